@@ -1,0 +1,465 @@
+"""Benchmark: DG time steps/s of the DGFS Couette workload on B200.
+
+Workload (the configuration the headline metric is quoted on): 2-D mesh of
+16 x 8 quadrilaterals at P = 3 (2048 DOFs), Nv = 24^3 velocities on
+[-6, 6]^3, VHS omega = 0.81, Nrho = 12, M = 12, diffuse walls at y = -+0.5
+moving at -+0.3 with T = 1, initial Maxwellian n = 1, T = 1, SSP-RK2
+(dgfs-tvd-rk2), dt = 5e-4, FP32 state, FP64 moments/projection.  A step is
+one full DG time step (two collision-operator evaluations of every DOF plus
+two FR advection stages), captured as one CUDA graph.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun every rank runs its own replica of the workload (no
+collective on the data path); value = total steps of all ranks / the
+slowest rank's device time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NONDIM = dict(T0=273.0, H0=1e-3, rho0=0.00011140244750324529, molarMass0=39.96e-3)
+WORK = dict(Nv=24, Nrho=12, M=12, dev=6, omega=0.81, order=3, nx=16, ny=8,
+            uw=0.3, dt=5e-4)
+METRIC = 'DG steps/s and Q evals/s: plain FP64 vs FP32 batched vs surrogate at stated L2 err'
+
+
+def couette_ini(precision='single', w=WORK):
+    import numpy as np
+    u0 = np.sqrt(2 * 8.3144598 / NONDIM['molarMass0'] * NONDIM['T0'])
+    rho0, T0 = NONDIM['rho0'], NONDIM['T0']
+    walls = ''.join(f"""
+[soln-bcs-{name}]
+type = dgfs-wall-diffuse
+rho = {rho0}
+T = {T0}
+ux = {sgn * w['uw'] * u0}
+uy = 0
+uz = 0
+""" for name, sgn in (('y-', -1), ('y+', 1)))
+    return f"""
+[backend]
+precision = {precision}
+[constants]
+Nv = {w['Nv']}
+Nrho = {w['Nrho']}
+[non-dim]
+T0 = {T0}
+H0 = {NONDIM['H0']}
+rho0 = {rho0}
+molarMass0 = {NONDIM['molarMass0']}
+[velocity-mesh]
+dev = {w['dev']}
+cmax = 0
+Tmax = {T0}
+[spherical-design-rule]
+ssrule = womersley
+M = {w['M']}
+[scattering-model]
+type = vhs-gll
+omega = {w['omega']}
+dRef = 4.17e-10
+Tref = {T0}
+[solver]
+system = dgfs
+order = {w['order']}
+[solver-time-integrator]
+scheme = dgfs-tvd-rk2
+controller = none
+tstart = 0.0
+tend = 0.1
+dt = {w['dt']}
+[soln-ics]
+type = maxwellian
+rho = {rho0}
+T = {T0}
+ux = 0
+uy = 0
+uz = 0
+{walls}"""
+
+
+def q_flops_per_eval(Nv, Nrho, M):
+    """Algorithmic FLOP of one collision-operator evaluation (packed
+    algorithm): (M*Nrho + Nrho + 2) complex FFTs at 5 n log2 n plus the
+    per-(p,q) multiplier/product work 8 n, n = Nv^3."""
+    import math
+    n = Nv**3
+    return (M * Nrho + Nrho + 2) * 5.0 * n * math.log2(n) + 8.0 * M * Nrho * n
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+
+    def start(self):
+        q = ('clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,'
+             'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+             'clocks_event_reasons.sw_power_cap')
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(self.index), f'--query-gpu={q}',
+                 '--format=csv,noheader,nounits', '-lms', '200'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(',')])
+
+    def stop(self):
+        if self.proc is None:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        import statistics
+        sm = [float(r[0]) for r in self.rows if len(r) >= 7 and r[0].replace('.', '').isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) >= 7 and r[1].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({names[k] for r in self.rows if len(r) >= 7
+                          for k in range(4) if r[3 + k].lower() == 'active'})
+        return {'sm_mhz': statistics.median(sm) if sm else None,
+                'sm_max_mhz': max(mx) if mx else None, 'reasons': reasons,
+                'samples': len(sm)}
+
+
+def dist_init():
+    import torch
+    ws = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = 'nccl' if torch.cuda.is_available() else 'gloo'
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return ws, rank, local
+
+
+def reduce_max(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64,
+                     device='cuda' if torch.cuda.is_available() else 'cpu')
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------- CPU legs
+_ORC = None
+
+
+def _oracle_init(Nv, Nrho, sz, dev, omega):
+    """Pool initializer: build the reference-algorithm tables once per worker."""
+    global _ORC
+    sys.path.insert(0, ROOT)
+    from oracle.velocitymesh import VelocityMesh
+    from oracle.vhs import VHSOracle
+    vm = VelocityMesh(Nv, Nrho, sz, cmax=0.0, Tmax=NONDIM['T0'], dev=dev, **NONDIM)
+    _ORC = VHSOracle(vm, omega, 4.17e-10, NONDIM['T0'])
+
+
+def _oracle_q_worker(F):
+    import numpy as np
+    if len(F) == 0:
+        return np.zeros((0, 0))
+    return np.stack([_ORC.Q(f) for f in F])
+
+
+def make_pool(ncores, Nv, Nrho, sz, dev, omega):
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    pool = ProcessPoolExecutor(max_workers=ncores, mp_context=mp.get_context('spawn'),
+                               initializer=_oracle_init, initargs=(Nv, Nrho, sz, dev, omega))
+    list(pool.map(_oracle_q_worker, [[] for _ in range(ncores)]))   # start workers
+    return pool
+
+
+def cpu_reference_step_time(F_sample, fr_state, ndof_total, pool, ncores):
+    """Time of one full DG step of the reference algorithm on the host cores,
+    from a bounded sample: Q of the sample DOFs spread over the pool (wall
+    time), and the FR operator on the full mesh."""
+    import numpy as np
+    chunks = [c for c in np.array_split(F_sample, ncores) if len(c)]
+    t0 = time.perf_counter()
+    outs = list(pool.map(_oracle_q_worker, chunks))
+    tq = time.perf_counter() - t0
+    Q = np.concatenate(outs)
+    orc_fr, u = fr_state
+    t1 = time.perf_counter()
+    orc_fr.rhs(u)
+    tfr = time.perf_counter() - t1
+    # per step: 2 stages x (Q over all DOFs + one FR operator)
+    t_step = 2.0 * (tq * ndof_total / len(F_sample) + tfr)
+    return t_step, Q, tq, tfr
+
+
+def make_fr_oracle(system):
+    import numpy as np
+    from oracle.fr import FROracle
+    shp = system.geo.shape
+    ops = {'M0': shp.opmat('M0'), 'M132': shp.opmat('M1 - M3*M2'), 'M3': shp.opmat('M3')}
+    walls = [(system.walls.uwall[w].double().cpu().numpy(),
+              system.walls.fw[w].double().cpu().numpy()) for w in range(system.walls.fw.shape[0])]
+    return FROracle(ops, system.geo, system.vm.c0(), system.vm.cw(), walls)
+
+
+def run_reference(args):
+    """--impl reference: the reference's algorithm (FP64 CPU restatement,
+    oracle/) timed on all host cores; each step a bounded sample."""
+    import numpy as np
+    ws, rank, local = int(os.environ.get('WORLD_SIZE', '1')), int(os.environ.get('RANK', '0')), 0
+    if rank != 0:
+        return
+    ncores = os.cpu_count() or 1
+    from frfs_b200.inifile import Inifile
+    from frfs_b200.velocitymesh import DGFSVelocityMesh
+    from frfs_b200.mesh import StructuredMesh, ElementGeometry
+    from oracle.fr import FROracle
+    cfg = Inifile(couette_ini('double'))
+    vm = DGFSVelocityMesh(None, cfg)
+    mesh = StructuredMesh((WORK['nx'], WORK['ny']), (0.0, -0.5), (2.0, 0.5), periodic='x')
+    geo = ElementGeometry(mesh, WORK['order'])
+    shp = geo.shape
+    from frfs_b200.initcond import DGFSMaxwellianInitCondition
+    walls = []
+    for name in geo.wall_names:
+        bc = DGFSMaxwellianInitCondition(None, cfg, vm, f'soln-bcs-{name}')
+        walls.append((bc.unondim()[:, 0], bc.get_init_vals()))
+    ic = DGFSMaxwellianInitCondition(None, cfg, vm, 'soln-ics').get_init_vals()
+    u = np.broadcast_to(ic, (geo.neles, geo.nupts, vm.vsize())).copy()
+    orc_fr = FROracle({'M0': shp.opmat('M0'), 'M132': shp.opmat('M1 - M3*M2'),
+                       'M3': shp.opmat('M3')}, geo, vm.c0(), vm.cw(), walls)
+    nsample = 8 * ncores
+    rng = np.random.default_rng(0)
+    F = u.reshape(-1, vm.vsize())[:nsample] * (1 + 0.01 * rng.uniform(-1, 1, (nsample, vm.vsize())))
+    pool = make_pool(ncores, WORK['Nv'], WORK['Nrho'], vm.sz(), WORK['dev'], WORK['omega'])
+    times = []
+    for i in range(args.warmup + args.steps):
+        t, _, tq, tfr = cpu_reference_step_time(F, (orc_fr, u), geo.neles * geo.nupts, pool,
+                                                ncores)
+        if i >= args.warmup:
+            times.append(t)
+    pool.shutdown()
+    mean = sum(times) / len(times)
+    v = 1.0 / mean
+    sample = (f'{nsample} of {geo.neles * geo.nupts} DOFs for Q (3+3*M*Nrho FFTs each, '
+              f'FP64 pocketfft) + FR operator on the full mesh, extrapolated per DOF to 1 step')
+    line = {'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': 'DG steps/s',
+            'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': mean * 1e3, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'config': config_block(args.gpus),
+            'q_evals_per_s': geo.neles * geo.nupts * 2 / mean,
+            'cpu_baseline': {'value': v, 'unit': 'DG steps/s', 'cores': ncores,
+                             'kind': 'port', 'sample': sample},
+            'e2e': {'value': v, 'unit': 'DG steps/s', 'h2d_bytes_per_step': 0,
+                    'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config_block(n):
+    return {'workload': ('couette-2d: 16x8 quads P3 (2048 DOFs), Nv=24^3 on [-6,6]^3, '
+                         'VHS omega=0.81, Nrho=12, M=12, diffuse walls +-0.3, SSP-RK2 dt=5e-4'),
+            'ndof': 2048, 'Nv': 24, 'Nrho': 12, 'M': 12, 'order': 3, 'mesh': [16, 8],
+            'parallelism': f'replicas x{n}' if n > 1 else 'single GPU',
+            'l2': 'flushed before every timed step (256 MiB write); step working set 452 MB > L2'}
+
+
+# ---------------------------------------------------------------- GPU leg
+def run_gpu(args):
+    import numpy as np
+    import torch
+    ws, rank, local = dist_init()
+    # CPU baseline pool before any GPU work (spawned workers)
+    pool = None
+    ncores = os.cpu_count() or 1
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        from frfs_b200.sphericaldesign import half_sphere_design
+        pool = make_pool(ncores, WORK['Nv'], WORK['Nrho'], half_sphere_design(WORK['M']),
+                         WORK['dev'], WORK['omega'])
+    from frfs_b200 import _lib
+    from frfs_b200.backend import CUDABackend
+    from frfs_b200.inifile import Inifile
+    from frfs_b200.integrators import get_integrator
+    from frfs_b200.mesh import StructuredMesh
+    from frfs_b200.system import DGFSSystem
+    cfg = Inifile(couette_ini('single'))
+    be = CUDABackend(cfg)
+    dev = be.device
+    mesh = StructuredMesh((WORK['nx'], WORK['ny']), (0.0, -0.5), (2.0, 0.5), periodic='x')
+    system = DGFSSystem(be, mesh, cfg, nreg=3)
+    integ = get_integrator(be, system, cfg)
+    ndof = system.ele.neles * system.ele.nupts
+    dt = WORK['dt']
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    # ---------------- device-timed steps (graph replay, inputs resident)
+    for _ in range(max(args.warmup, 3)):
+        integ.step(integ.tcurr, dt)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    barrier(ws)
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    evs = []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        integ.step(integ.tcurr, dt)
+        e1.record(st)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    barrier(ws)
+    clocks = sampler.stop() if sampler else None
+    t_dev = sum(a.elapsed_time(b) for a, b in evs) / 1e3          # seconds, this rank
+    t_max = reduce_max(t_dev, ws)
+    value = ws * args.steps / t_max
+    ms_per_step = t_max / args.steps * 1e3
+    # ---------------- dominant kernel: Q alone, events on its stream
+    fin = system.eles_scal_upts_inb_full[0]
+    qout = system.eles_scal_upts_inb_full[2]
+    for _ in range(2):
+        system.sm.collide(fin, qout)
+    torch.cuda.synchronize()
+    qt = []
+    for _ in range(5):
+        flush.fill_(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        system.sm.collide(fin, qout)
+        b.record(st)
+        qt.append((a, b))
+    torch.cuda.synchronize()
+    q_ms = sum(x.elapsed_time(y) for x, y in qt) / len(qt)
+    flop = q_flops_per_eval(WORK['Nv'], WORK['Nrho'], WORK['M']) * ndof
+    achieved = flop / (q_ms * 1e-3) / 1e12
+    # measured FP32 FMA peak on this GPU (probe kernel in libbdgfs)
+    probe = torch.zeros(1, device=dev)
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    iters = 4096
+    _lib.check(_lib.lib().bdgfs_fma_probe(_lib.ptr(probe), nsm * 8, 64, _lib.stream_ptr()), 'probe')
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    _lib.check(_lib.lib().bdgfs_fma_probe(_lib.ptr(probe), nsm * 8, iters, _lib.stream_ptr()), 'probe')
+    b.record(st)
+    torch.cuda.synchronize()
+    pk_ms = a.elapsed_time(b)
+    peak = nsm * 8 * 256 * iters * 16 * 8 * 2 / (pk_ms * 1e-3) / 1e12
+    # ---------------- e2e: host buffers, copies inside the timed region
+    nbytes = fin.numel() * fin.element_size()
+    host_in = torch.empty(fin.shape, dtype=fin.dtype, pin_memory=True)
+    host_out = torch.empty(fin.shape, dtype=fin.dtype, pin_memory=True)
+    host_in.copy_(fin)
+    torch.cuda.synchronize()
+    e2e_ev = []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        fin.copy_(host_in, non_blocking=True)
+        integ.step(integ.tcurr, dt)
+        host_out.copy_(fin, non_blocking=True)
+        b.record(st)
+        e2e_ev.append((a, b))
+    torch.cuda.synchronize()
+    t_e2e = reduce_max(sum(x.elapsed_time(y) for x, y in e2e_ev) / 1e3, ws)
+    e2e = ws * args.steps / t_e2e
+    # ---------------- CPU baseline (rank 0, N = 1): reference algorithm sample
+    cpu = None
+    qerr = None
+    if pool is not None:
+        f_host = fin.reshape(-1, system.vm.vsize()).double().cpu().numpy()
+        rng = np.random.default_rng(1)
+        idx = rng.choice(ndof, size=min(ndof, 32 * ncores), replace=False)
+        F = f_host[idx]
+        orc_fr = make_fr_oracle(system)
+        u_host = fin.double().cpu().numpy()
+        t_step, Qo, tq, tfr = cpu_reference_step_time(F, (orc_fr, u_host), ndof, pool, ncores)
+        # L2 error of the FP32 GPU operator vs the FP64 reference algorithm on the sample
+        system.sm.collide(fin, qout, project=False)
+        qg = qout.reshape(-1, system.vm.vsize())[torch.as_tensor(idx, device=dev)].double().cpu().numpy()
+        qerr = float(np.linalg.norm(qg - Qo) / np.linalg.norm(Qo))
+        cpu = {'value': 1.0 / t_step, 'unit': 'DG steps/s', 'cores': ncores, 'kind': 'port',
+               'sample': (f'Q of {len(idx)} random DOFs of the same state (reference algorithm, '
+                          f'3+3*M*Nrho FP64 FFTs each, {tq:.1f} s on {ncores} processes) + FR '
+                          f'operator on the full mesh ({tfr:.2f} s), extrapolated to one step')}
+        pool.shutdown()
+    # gpu launches per step: 2 x (collide + disu + bc_update + rhs)
+    launches = 8 * args.steps
+    line = {
+        'metric': METRIC, 'value': value, 'unit': 'DG steps/s', 'n_gpus': ws,
+        'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms_per_step,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
+        'data': 'synthetic', 'config': config_block(ws),
+        'q_evals_per_s': ws * 2 * ndof * args.steps / t_max,
+        'q_rel_l2_err_vs_fp64_reference': qerr,
+        'roofline': {'bound': 'fp32', 'kernel': 'bdgfs::vhs_collide_kernel',
+                     'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
+                     'frac': achieved / peak,
+                     'peak_source': 'measured FP32 FMA probe on this GPU (MEASURED_PEAKS.json has '
+                                    'no FP32 CUDA-core figure)',
+                     'flop_per_launch': flop, 'launch_ms': q_ms, 'traffic': None},
+        'e2e': {'value': e2e, 'unit': 'DG steps/s', 'h2d_bytes_per_step': nbytes,
+                'd2h_bytes_per_step': nbytes},
+        'gpu_launches': launches,
+        'clocks': clocks,
+        'cpu_baseline': cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='frfs_b200', choices=['frfs_b200', 'reference'])
+    ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
+    args = ap.parse_args()
+    if args.impl == 'reference':
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,107 @@
+"""ctypes binding of ``libbdgfs.so`` (the C ABI declared in include/bdgfs.h).
+
+The library is loaded from the package's ``_lib`` directory.  There is no
+fallback: every product entry point raises if the library is missing or a
+call returns a non-zero status.
+"""
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(_HERE, '_lib', 'libbdgfs.so')
+
+BDGFS_OK = 0
+_ERRORS = {-1: 'invalid argument', -2: 'CUDA error', -3: 'unsupported grid/precision',
+           -4: 'bounded device wait timed out', -5: 'scratch buffer too small'}
+
+# Every symbol include/bdgfs.h declares (tests check the export list).
+EXPORTS = (
+    'bdgfs_vhs_scratch_bytes', 'bdgfs_vhs_collide', 'bdgfs_fma_probe',
+    'bdgfs_fr_disu', 'bdgfs_fr_bc_update', 'bdgfs_fr_rhs',
+    'bdgfs_moments', 'bdgfs_residual', 'bdgfs_status_check',
+)
+
+
+class BdgfsError(RuntimeError):
+    pass
+
+
+class VhsGrid(C.Structure):
+    _fields_ = [('Nv', C.c_int32), ('Nrho', C.c_int32), ('M', C.c_int32),
+                ('fp64', C.c_int32), ('prefac', C.c_double), ('cw', C.c_double),
+                ('phase', C.c_void_p), ('gw', C.c_void_p), ('bb2', C.c_void_p),
+                ('c0', C.c_void_p), ('ginv', C.c_void_p)]
+
+
+class VhsBatch(C.Structure):
+    _fields_ = [('grid', C.c_int32), ('pad_', C.c_int32), ('ndof', C.c_int64),
+                ('f', C.c_void_p), ('Q', C.c_void_p), ('moments', C.c_void_p)]
+
+
+class FrEles(C.Structure):
+    _fields_ = [('ndims', C.c_int32), ('nupts', C.c_int32), ('nfpts', C.c_int32),
+                ('neles', C.c_int32), ('nv', C.c_int64), ('Nv', C.c_int32),
+                ('fp64', C.c_int32),
+                ('m0', C.c_void_p), ('dcorr', C.c_void_p), ('m3', C.c_void_p),
+                ('smats', C.c_void_p), ('rcpdjac', C.c_void_p), ('pnorm', C.c_void_p),
+                ('magn', C.c_void_p), ('nbr', C.c_void_p), ('c0', C.c_void_p)]
+
+
+class FrWall(C.Structure):
+    _fields_ = [('nwall', C.c_int32), ('nbc', C.c_int32),
+                ('fpt', C.c_void_p), ('bcid', C.c_void_p), ('uwall', C.c_void_p),
+                ('fw', C.c_void_p), ('bcv', C.c_void_p), ('cw', C.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libbdgfs.so once; raise if it is absent."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise BdgfsError(f'{LIBPATH} not built: run python -m frfs_b200.build')
+        L = C.CDLL(LIBPATH)
+        L.bdgfs_vhs_scratch_bytes.restype = C.c_size_t
+        L.bdgfs_vhs_scratch_bytes.argtypes = [C.POINTER(VhsGrid), C.c_int32, C.c_int32]
+        L.bdgfs_vhs_collide.restype = C.c_int32
+        L.bdgfs_vhs_collide.argtypes = [C.POINTER(VhsGrid), C.c_int32, C.POINTER(VhsBatch),
+                                        C.c_int32, C.c_int32, C.c_void_p, C.c_size_t,
+                                        C.c_void_p, C.c_void_p]
+        L.bdgfs_fma_probe.restype = C.c_int32
+        L.bdgfs_fma_probe.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]
+        vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+        sig = {
+            'bdgfs_fr_disu': [vp, vp, vp, vp],
+            'bdgfs_fr_bc_update': [vp, vp, vp, vp],
+            'bdgfs_fr_rhs': [vp, vp, vp, vp, vp, dbl, dbl, vp, dbl, vp, dbl, vp],
+            'bdgfs_moments': [vp, i64, i32, i32, vp, dbl, vp, vp],
+            'bdgfs_residual': [vp, vp, i64, i32, vp, vp],
+            'bdgfs_status_check': [vp, i64, i32, vp, vp],
+        }
+        for name, at in sig.items():
+            fn = getattr(L, name)
+            fn.restype = C.c_int32
+            fn.argtypes = at
+        _lib = L
+    return _lib
+
+
+def check(rc, what):
+    if rc != BDGFS_OK:
+        raise BdgfsError(f'{what}: {_ERRORS.get(rc, rc)} (status {rc})')
+
+
+def stream_ptr(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
+
+
+def ref(struct):
+    return C.c_void_p(C.addressof(struct))

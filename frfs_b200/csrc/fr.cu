@@ -1,0 +1,459 @@
+// Flux-reconstruction advection of the distribution function, all Nv^3
+// velocities at once (no velocity batching).
+//
+// Reference path (per velocity batch, frfs/solvers/dgfs/system.py:140-196):
+//   disu        u_f = M0 u                       (solvers/dgfs/elements.py:56-59)
+//   tdisf       F~_i = smats[i][k] c_k u          (kernels/tflux.mako, flux.mako)
+//   tdivtpcorf  R = (M1 - M3 M2) F~               (elements.py:79-82)
+//   comm_flux   upwind flux at interfaces / diffuse walls
+//               (kernels/intcflux.mako, rsolvers/rusanov.mako, bccflux.mako,
+//                bcs/dgfs-wall-diffuse.mako)
+//   tdivtconf   R += M3 Fhat                      (elements.py:85-88)
+//   negdivconf  R = -R / |J|                      (kernels/negdivconf.mako)
+//   axnpby      RK update                         (backends/cuda/kernels/axnpby.mako)
+//   update_bc   diffuse-wall mass balance sums    (kernels/bccupdate.mako,
+//               bcs/dgfs-wall-diffuse-update.mako)
+//
+// Layout: state u[e][upt][v], face values uf[e][fpt][v], v = (x*Nv+y)*Nv+z
+// contiguous, so every global access below is coalesced across the threads
+// of a block (one thread per velocity).  bdgfs_fr_rhs fuses tdisf,
+// tdivtpcorf, both comm_flux kernels, tdivtconf, negdivconf and the RK
+// combination out = a*u + b*L(u) + c1*x1 + c2*x2 in one pass; the common
+// flux of an interior face point is evaluated by both neighbours (each with
+// its own outward normal), which equals the reference's lhs-computed value
+// with the sign flip of intcflux.mako:21-23.
+#include "common.cuh"
+
+namespace bdgfs {
+
+template <typename T>
+struct FrSmem {
+    T* dT;      // [ND*NU][NU]  (M1 - M3 M2) transposed
+    T* m3T;     // [NF][NU]
+    T* m0;      // [NF][NU]
+};
+
+// velocity components of index v
+template <typename T>
+__device__ __forceinline__ void vel(const T* c0, int Nv, int64_t v, T (&c)[3])
+{
+    const int iz = int(v % Nv);
+    const int iy = int((v / Nv) % Nv);
+    const int ix = int(v / (int64_t(Nv) * Nv));
+    c[0] = c0[ix];
+    c[1] = c0[iy];
+    c[2] = c0[iz];
+}
+
+template <typename T, int NU, int NF>
+__global__ void __launch_bounds__(128) disu_kernel(const bdgfs_fr_eles el, const T* __restrict__ u,
+                                                   T* __restrict__ uf)
+{
+    __shared__ T m0[NF * NU];
+    const T* gm0 = static_cast<const T*>(el.m0);
+    for (int i = threadIdx.x; i < NF * NU; i += blockDim.x) m0[i] = gm0[i];
+    __syncthreads();
+    const int64_t nv = el.nv;
+    const int64_t e = blockIdx.y;
+    for (int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < nv;
+         v += int64_t(gridDim.x) * blockDim.x) {
+        T uu[NU];
+#pragma unroll
+        for (int i = 0; i < NU; ++i) uu[i] = u[(e * NU + i) * nv + v];
+#pragma unroll 4
+        for (int f = 0; f < NF; ++f) {
+            T acc = T(0);
+#pragma unroll
+            for (int i = 0; i < NU; ++i) acc += m0[f * NU + i] * uu[i];
+            uf[(e * NF + f) * nv + v] = acc;
+        }
+    }
+}
+
+template <typename T, int ND, int NU, int NF>
+__global__ void __launch_bounds__(128) rhs_kernel(const bdgfs_fr_eles el, const bdgfs_fr_walls wl,
+                                                  const T* __restrict__ u, const T* __restrict__ uf,
+                                                  T* out, T a, T b, const T* x1, T c1, const T* x2,
+                                                  T c2)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* dT = reinterpret_cast<T*>(smraw);               // [ND*NU][NU]
+    T* m3T = dT + ND * NU * NU;                         // [NF][NU]
+    T* sm = m3T + NF * NU;                              // [NU][ND][ND]
+    T* rj = sm + NU * ND * ND;                          // [NU]
+    T* pn = rj + NU;                                    // [NF][ND]
+    T* mg = pn + NF * ND;                               // [NF]
+    int* nb = reinterpret_cast<int*>(mg + NF);          // [NF]
+    const int64_t e = blockIdx.y;
+    {
+        const T* gd = static_cast<const T*>(el.dcorr);   // [NU][ND*NU]
+        for (int i = threadIdx.x; i < ND * NU * NU; i += blockDim.x) {
+            const int col = i / NU, row = i % NU;
+            dT[i] = gd[row * ND * NU + col];
+        }
+        const T* gm3 = static_cast<const T*>(el.m3);     // [NU][NF]
+        for (int i = threadIdx.x; i < NF * NU; i += blockDim.x) {
+            const int f = i / NU, row = i % NU;
+            m3T[i] = gm3[row * NF + f];
+        }
+        const T* gs = static_cast<const T*>(el.smats) + e * NU * ND * ND;
+        for (int i = threadIdx.x; i < NU * ND * ND; i += blockDim.x) sm[i] = gs[i];
+        const T* gr = static_cast<const T*>(el.rcpdjac) + e * NU;
+        for (int i = threadIdx.x; i < NU; i += blockDim.x) rj[i] = gr[i];
+        const T* gp = static_cast<const T*>(el.pnorm) + e * NF * ND;
+        for (int i = threadIdx.x; i < NF * ND; i += blockDim.x) pn[i] = gp[i];
+        const T* gg = static_cast<const T*>(el.magn) + e * NF;
+        for (int i = threadIdx.x; i < NF; i += blockDim.x) {
+            mg[i] = gg[i];
+            nb[i] = el.nbr[e * NF + i];
+        }
+    }
+    __syncthreads();
+    const int64_t nv = el.nv;
+    const T* c0 = static_cast<const T*>(el.c0);
+    const T* uw = static_cast<const T*>(wl.uwall);
+    const T* fw = static_cast<const T*>(wl.fw);
+    const T* bcv = static_cast<const T*>(wl.bcv);
+    for (int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < nv;
+         v += int64_t(gridDim.x) * blockDim.x) {
+        T c[3];
+        vel(c0, el.Nv, v, c);
+        T uu[NU], R[NU];
+#pragma unroll
+        for (int i = 0; i < NU; ++i) {
+            uu[i] = u[(e * NU + i) * nv + v];
+            R[i] = T(0);
+        }
+        // volume: R += (M1 - M3 M2) F~,  F~[d][j] = (sum_k smats[j][d][k] c_k) u_j
+#pragma unroll 1
+        for (int j = 0; j < NU; ++j) {
+#pragma unroll
+            for (int d = 0; d < ND; ++d) {
+                T al = T(0);
+#pragma unroll
+                for (int k = 0; k < ND; ++k) al += sm[(j * ND + d) * ND + k] * c[k];
+                const T ft = al * uu[j];
+                const T* col = dT + (d * NU + j) * NU;
+#pragma unroll
+                for (int i = 0; i < NU; ++i) R[i] += col[i] * ft;
+            }
+        }
+        // surface: common normal flux at each face point, lifted by M3
+#pragma unroll 1
+        for (int f = 0; f < NF; ++f) {
+            const T ul = uf[(e * NF + f) * nv + v];
+            T nc = T(0);
+#pragma unroll
+            for (int d = 0; d < ND; ++d) nc += pn[f * ND + d] * c[d];
+            const int n = nb[f];
+            T ur;
+            if (n >= 0) {
+                ur = uf[int64_t(n) * nv + v];
+            } else {
+                const int w = -1 - n;
+                const int bid = wl.bcid[w];
+                T fac = T(0);
+#pragma unroll
+                for (int d = 0; d < ND; ++d) fac += (c[d] - uw[bid * 3 + d]) * pn[f * ND + d];
+                ur = (fac < T(0)) ? fw[int64_t(bid) * nv + v] * (-bcv[2 * w] / bcv[2 * w + 1]) : ul;
+            }
+            const T fn = T(0.5) * nc * (ul + ur) + T(0.5) * fabs(nc) * (ul - ur);
+            const T fh = mg[f] * fn;
+            const T* col = m3T + f * NU;
+#pragma unroll
+            for (int i = 0; i < NU; ++i) R[i] += col[i] * fh;
+        }
+#pragma unroll
+        for (int i = 0; i < NU; ++i) {
+            const int64_t idx = (e * NU + i) * nv + v;
+            T r = a * uu[i] + b * (-rj[i] * R[i]);
+            if (x1) r += c1 * x1[idx];
+            if (x2) r += c2 * x2[idx];
+            out[idx] = r;
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) bc_update_kernel(const bdgfs_fr_eles el,
+                                                        const bdgfs_fr_walls wl,
+                                                        const T* __restrict__ uf)
+{
+    __shared__ double red[2 * 8];
+    const int w = blockIdx.x;
+    const int e = wl.fpt[2 * w], f = wl.fpt[2 * w + 1];
+    const int bid = wl.bcid[w];
+    const int ND = el.ndims;
+    const T* pn = static_cast<const T*>(el.pnorm) + (int64_t(e) * el.nfpts + f) * ND;
+    const T* uw = static_cast<const T*>(wl.uwall) + bid * 3;
+    const T* fw = static_cast<const T*>(wl.fw) + int64_t(bid) * el.nv;
+    const T* ul = uf + (int64_t(e) * el.nfpts + f) * el.nv;
+    const T* c0 = static_cast<const T*>(el.c0);
+    double s0 = 0.0, s1 = 0.0;
+    for (int64_t v = threadIdx.x; v < el.nv; v += blockDim.x) {
+        T c[3];
+        vel(c0, el.Nv, v, c);
+        T fac = T(0);
+        for (int d = 0; d < ND; ++d) fac += (c[d] - uw[d]) * pn[d];
+        if (fac >= T(0)) s0 += double(fac * ul[v]);
+        else s1 += double(fac * fw[v]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) { red[2 * warp] = s0; red[2 * warp + 1] = s1; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a0 = 0.0, a1 = 0.0;
+        for (int i = 0; i < int(blockDim.x >> 5); ++i) { a0 += red[2 * i]; a1 += red[2 * i + 1]; }
+        T* out = static_cast<T*>(wl.bcv);
+        out[2 * w] = T(a0 * wl.cw);
+        out[2 * w + 1] = T(a1 * wl.cw);
+    }
+}
+
+// raw FP64 velocity moments of each distribution:
+// sum f, sum c f (3), sum c_i c_j f (6: xx xy xz yy yz zz), sum |c|^2 c f (3)
+template <typename T>
+__global__ void __launch_bounds__(256) moments_kernel(const T* __restrict__ f, int Nv,
+                                                      const double* __restrict__ c0, double cw,
+                                                      double* __restrict__ out)
+{
+    __shared__ double red[13 * 8];
+    const int64_t n = int64_t(Nv) * Nv * Nv;
+    const T* fd = f + int64_t(blockIdx.x) * n;
+    double m[13];
+#pragma unroll
+    for (int j = 0; j < 13; ++j) m[j] = 0.0;
+    for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
+        const double cx = c0[v / (int64_t(Nv) * Nv)], cy = c0[(v / Nv) % Nv], cz = c0[v % Nv];
+        const double fv = double(fd[v]);
+        const double c2 = cx * cx + cy * cy + cz * cz;
+        m[0] += fv;
+        m[1] += cx * fv; m[2] += cy * fv; m[3] += cz * fv;
+        m[4] += cx * cx * fv; m[5] += cx * cy * fv; m[6] += cx * cz * fv;
+        m[7] += cy * cy * fv; m[8] += cy * cz * fv; m[9] += cz * cz * fv;
+        m[10] += c2 * cx * fv; m[11] += c2 * cy * fv; m[12] += c2 * cz * fv;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < 13; ++j) {
+        double x = m[j];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) red[warp * 13 + j] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 13) {
+        double s = 0.0;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) s += red[w * 13 + threadIdx.x];
+        out[int64_t(blockIdx.x) * 13 + threadIdx.x] = s * cw;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) residual_kernel(const T* __restrict__ a,
+                                                       const T* __restrict__ b, int64_t n,
+                                                       double* out)
+{
+    __shared__ double red[2 * 8];
+    double s0 = 0.0, s1 = 0.0;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const double x = double(a[i]), y = double(b[i]);
+        s0 += (x - y) * (x - y);
+        s1 += y * y;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) { red[2 * warp] = s0; red[2 * warp + 1] = s1; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a0 = 0.0, a1 = 0.0;
+        for (int i = 0; i < int(blockDim.x >> 5); ++i) { a0 += red[2 * i]; a1 += red[2 * i + 1]; }
+        atomicAdd(out, a0);
+        atomicAdd(out + 1, a1);
+    }
+}
+
+// status word check: any non-finite or negative-density flag set by the
+// scan below (NaN/Inf detection of the state, read back after graph replay)
+template <typename T>
+__global__ void __launch_bounds__(256) status_kernel(const T* __restrict__ a, int64_t n,
+                                                     int32_t* status)
+{
+    int bad = 0;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const T x = a[i];
+        if (!isfinite(x)) bad |= 1;
+    }
+    bad = __reduce_or_sync(0xffffffffu, bad);
+    if (bad && (threadIdx.x & 31) == 0) atomicOr(status, bad);
+}
+
+static int grid_v(int64_t nv, int neles, dim3* g)
+{
+    int64_t bx = (nv + 127) / 128;
+    if (bx > 65535) bx = 65535;
+    if (neles > 65535 || neles < 1) return BDGFS_EINVAL;
+    *g = dim3(unsigned(bx), unsigned(neles));
+    return BDGFS_OK;
+}
+
+template <typename T, int ND, int NU, int NF>
+static int rhs_launch(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl, const void* u,
+                      const void* uf, void* out, double a, double b, const void* x1, double c1,
+                      const void* x2, double c2, cudaStream_t st)
+{
+    dim3 g;
+    if (grid_v(el->nv, el->neles, &g) != BDGFS_OK) return BDGFS_EINVAL;
+    const size_t smem = sizeof(T) * (ND * NU * NU + NF * NU + NU * ND * ND + NU + NF * ND + NF)
+                        + sizeof(int) * NF + 16;
+    auto k = rhs_kernel<T, ND, NU, NF>;
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+        return BDGFS_ECUDA;
+    bdgfs_fr_walls w0{};
+    k<<<g, 128, smem, st>>>(*el, wl ? *wl : w0, static_cast<const T*>(u),
+                            static_cast<const T*>(uf), static_cast<T*>(out), T(a), T(b),
+                            static_cast<const T*>(x1), T(c1), static_cast<const T*>(x2), T(c2));
+    return cuda_status(cudaGetLastError());
+}
+
+template <typename T, int NU, int NF>
+static int disu_launch(const bdgfs_fr_eles* el, const void* u, void* uf, cudaStream_t st)
+{
+    dim3 g;
+    if (grid_v(el->nv, el->neles, &g) != BDGFS_OK) return BDGFS_EINVAL;
+    disu_kernel<T, NU, NF><<<g, 128, 0, st>>>(*el, static_cast<const T*>(u), static_cast<T*>(uf));
+    return cuda_status(cudaGetLastError());
+}
+
+#define BDGFS_FR_SHAPES(X)                                                          \
+    X(2, 4, 8) X(2, 9, 12) X(2, 16, 16) X(2, 25, 20) X(3, 8, 24) X(3, 27, 54)
+
+static bool shape_ok(const bdgfs_fr_eles* el)
+{
+#define CHK(D, U, F) if (el->ndims == D && el->nupts == U && el->nfpts == F) return true;
+    BDGFS_FR_SHAPES(CHK)
+#undef CHK
+    return false;
+}
+
+static int check_eles(const bdgfs_fr_eles* el)
+{
+    if (!el || el->nv < 1 || el->neles < 1 || el->Nv < 1 ||
+        int64_t(el->Nv) * el->Nv * el->Nv != el->nv)
+        return BDGFS_EINVAL;
+    if (!el->m0 || !el->dcorr || !el->m3 || !el->smats || !el->rcpdjac || !el->pnorm ||
+        !el->magn || !el->nbr || !el->c0)
+        return BDGFS_EINVAL;
+    return shape_ok(el) ? BDGFS_OK : BDGFS_EUNSUPPORTED;
+}
+
+}  // namespace bdgfs
+
+using namespace bdgfs;
+
+extern "C" int32_t bdgfs_fr_disu(const bdgfs_fr_eles* el, const void* u, void* uf, void* stream)
+{
+    int rc = check_eles(el);
+    if (rc != BDGFS_OK) return rc;
+    if (!u || !uf) return BDGFS_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+#define GO(D, U, F)                                                                         \
+    if (el->ndims == D && el->nupts == U && el->nfpts == F)                                 \
+        return el->fp64 ? disu_launch<double, U, F>(el, u, uf, st)                          \
+                        : disu_launch<float, U, F>(el, u, uf, st);
+    BDGFS_FR_SHAPES(GO)
+#undef GO
+    return BDGFS_EUNSUPPORTED;
+}
+
+extern "C" int32_t bdgfs_fr_bc_update(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl,
+                                      const void* uf, void* stream)
+{
+    int rc = check_eles(el);
+    if (rc != BDGFS_OK) return rc;
+    if (!wl || !uf) return BDGFS_EINVAL;
+    if (wl->nwall == 0) return BDGFS_OK;
+    if (wl->nwall < 0 || !wl->fpt || !wl->bcid || !wl->uwall || !wl->fw || !wl->bcv)
+        return BDGFS_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (el->fp64)
+        bc_update_kernel<double><<<wl->nwall, 256, 0, st>>>(*el, *wl, static_cast<const double*>(uf));
+    else
+        bc_update_kernel<float><<<wl->nwall, 256, 0, st>>>(*el, *wl, static_cast<const float*>(uf));
+    return cuda_status(cudaGetLastError());
+}
+
+extern "C" int32_t bdgfs_fr_rhs(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl, const void* u,
+                                const void* uf, void* out, double a, double b, const void* x1,
+                                double c1, const void* x2, double c2, void* stream)
+{
+    int rc = check_eles(el);
+    if (rc != BDGFS_OK) return rc;
+    if (!u || !uf || !out) return BDGFS_EINVAL;
+    if (wl && wl->nwall > 0 && (!wl->bcid || !wl->uwall || !wl->fw || !wl->bcv))
+        return BDGFS_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+#define GO(D, U, F)                                                                          \
+    if (el->ndims == D && el->nupts == U && el->nfpts == F)                                  \
+        return el->fp64 ? rhs_launch<double, D, U, F>(el, wl, u, uf, out, a, b, x1, c1, x2, c2, st) \
+                        : rhs_launch<float, D, U, F>(el, wl, u, uf, out, a, b, x1, c1, x2, c2, st);
+    BDGFS_FR_SHAPES(GO)
+#undef GO
+    return BDGFS_EUNSUPPORTED;
+}
+
+extern "C" int32_t bdgfs_moments(const void* f, int64_t ndof, int32_t Nv, int32_t fp64,
+                                 const double* c0, double cw, double* out, void* stream)
+{
+    if (!f || !c0 || !out || ndof < 0 || Nv < 1) return BDGFS_EINVAL;
+    if (ndof == 0) return BDGFS_OK;
+    if (ndof > 2147483647LL) return BDGFS_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (fp64)
+        moments_kernel<double><<<unsigned(ndof), 256, 0, st>>>(static_cast<const double*>(f), Nv, c0, cw, out);
+    else
+        moments_kernel<float><<<unsigned(ndof), 256, 0, st>>>(static_cast<const float*>(f), Nv, c0, cw, out);
+    return cuda_status(cudaGetLastError());
+}
+
+extern "C" int32_t bdgfs_residual(const void* a, const void* b, int64_t n, int32_t fp64,
+                                  double* out2, void* stream)
+{
+    if (!a || !b || !out2 || n < 0) return BDGFS_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(out2, 0, 2 * sizeof(double), st) != cudaSuccess) return BDGFS_ECUDA;
+    if (n == 0) return BDGFS_OK;
+    int64_t blocks = (n + 255) / 256;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (fp64)
+        residual_kernel<double><<<unsigned(blocks), 256, 0, st>>>(static_cast<const double*>(a),
+                                                                  static_cast<const double*>(b), n, out2);
+    else
+        residual_kernel<float><<<unsigned(blocks), 256, 0, st>>>(static_cast<const float*>(a),
+                                                                 static_cast<const float*>(b), n, out2);
+    return cuda_status(cudaGetLastError());
+}
+
+extern "C" int32_t bdgfs_status_check(const void* a, int64_t n, int32_t fp64, int32_t* status,
+                                      void* stream)
+{
+    if (!a || !status || n < 0) return BDGFS_EINVAL;
+    if (n == 0) return BDGFS_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int64_t blocks = (n + 255) / 256;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (fp64)
+        status_kernel<double><<<unsigned(blocks), 256, 0, st>>>(static_cast<const double*>(a), n, status);
+    else
+        status_kernel<float><<<unsigned(blocks), 256, 0, st>>>(static_cast<const float*>(a), n, status);
+    return cuda_status(cudaGetLastError());
+}

@@ -1,0 +1,148 @@
+"""DGFS time integrators: controller x stepper, CUDA-graph replay.
+
+Mirrors frfs/integrators: ``get_integrator`` (integrators/__init__.py:9-44)
+composes a controller ('none', integrators/std/controllers.py:54-73) with a
+stepper chosen by ``[solver-time-integrator] scheme``:
+
+* 'dgfs-euler'   (steppers.py:20-99):  u <- u + dt (L + Q)(u)
+* 'dgfs-tvd-rk2' (steppers.py:103-225): u1 = u + dt (L+Q)(u);
+                 u <- u/2 + u1/2 + dt/2 (L+Q)(u1)
+
+Each stage is one ``collide`` launch (all DOFs) plus the disu / bc-update /
+fused-rhs launches; the register banks are those of the reference (r0, r1,
+r2) and the result lands back in r0, so one step is captured once as a CUDA
+graph and replayed.  Per-step hooks: NaN check (plugins/nancheck.py) through
+a device status word, FP64 residual (plugins/dgfsresidualstd.py).
+"""
+import torch
+
+from . import _lib
+
+
+class BaseDGFSStepper:
+    stepper_name = None
+    nregs = 2
+
+    def __init__(self, backend, system, cfg):
+        self.backend, self.system, self.cfg = backend, system, cfg
+        sect = 'solver-time-integrator'
+        self.tstart = cfg.getfloat(sect, 'tstart', 0.0)
+        self.tend = cfg.getfloat(sect, 'tend')
+        self._dt = cfg.getfloat(sect, 'dt')
+        self.tcurr = self.tstart
+        self.nacptsteps = 0
+        self._idxcurr = 0
+        self._graph = None
+        self.use_graph = cfg.getbool(sect, 'cuda-graph', True)
+        self.nancheck_nsteps = cfg.getint('soln-plugin-nancheck', 'nsteps', 0)
+        self.resid_nsteps = cfg.getint('soln-plugin-dgfsresidualstd', 'nsteps', 0)
+        self._status = torch.zeros(1, dtype=torch.int32, device=backend.device)
+        self.residuals = []
+
+    @property
+    def soln(self):
+        return self.system.eles_scal_upts_inb_full[self._idxcurr]
+
+    def _step_kernels(self, t, dt):
+        raise NotImplementedError
+
+    def step(self, t, dt):
+        if not self.use_graph:
+            self._step_kernels(t, dt)
+            return
+        if self._graph is None or self._graph_dt != dt:
+            # warm-up launch on a side stream (sets kernel attributes), then capture
+            s = torch.cuda.Stream(device=self.backend.device)
+            s.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(s):
+                self._step_kernels(t, dt)
+            torch.cuda.current_stream().wait_stream(s)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._step_kernels(t, dt)
+            self._graph, self._graph_dt = g, dt
+            # the warm-up advanced the state: undo by replaying nothing -- the
+            # warm-up step is counted as a real step
+            self._warm_stepped = True
+            return
+        self._graph.replay()
+
+    def advance_to(self, t):
+        while self.tcurr < t - 1e-12 * max(1.0, abs(t)):
+            dt = min(self._dt, t - self.tcurr)
+            need_resid = self.resid_nsteps and (self.nacptsteps + 1) % self.resid_nsteps == 0
+            if need_resid:
+                prev = self.soln.clone()
+            self.step(self.tcurr, dt)
+            self.tcurr += dt
+            self.nacptsteps += 1
+            if need_resid:
+                self.residuals.append((self.tcurr, self._residual(prev)))
+            if self.nancheck_nsteps and self.nacptsteps % self.nancheck_nsteps == 0:
+                self.nancheck()
+        return self.tcurr
+
+    def run(self):
+        return self.advance_to(self.tend)
+
+    def _residual(self, prev):
+        out = torch.zeros(2, dtype=torch.float64, device=self.backend.device)
+        cur = self.soln
+        _lib.check(_lib.lib().bdgfs_residual(cur.data_ptr(), prev.data_ptr(), cur.numel(),
+                                             int(cur.dtype == torch.float64), out.data_ptr(),
+                                             _lib.stream_ptr()), 'bdgfs_residual')
+        o = out.cpu()
+        return float((o[0] / o[1]).sqrt())
+
+    def nancheck(self):
+        """Raise if the state holds NaN/Inf (plugins/nancheck.py:17-22)."""
+        self._status.zero_()
+        u = self.soln
+        _lib.check(_lib.lib().bdgfs_status_check(u.data_ptr(), u.numel(),
+                                                 int(u.dtype == torch.float64),
+                                                 self._status.data_ptr(), _lib.stream_ptr()),
+                   'bdgfs_status_check')
+        if int(self._status.item()):
+            raise RuntimeError(f'NaNs detected at t = {self.tcurr}')
+
+
+class StdEulerDGFSStepper(BaseDGFSStepper):
+    stepper_name = 'dgfs-euler'
+    nregs = 2
+    order = 1
+
+    def _step_kernels(self, t, dt):
+        s = self.system
+        s.collide(t, 0, 1)                                   # r1 = Q(r0)
+        s.advect_combine(t, 0, 0, a=1.0, b=dt, x1=1, c1=dt)  # r0 += dt (L + Q)
+
+
+class StdTVDRK2DGFSStepper(BaseDGFSStepper):
+    stepper_name = 'dgfs-tvd-rk2'
+    nregs = 3
+    order = 2
+
+    def _step_kernels(self, t, dt):
+        s = self.system
+        s.collide(t, 0, 1)                                        # r1 = Q(r0)
+        s.advect_combine(t, 0, 1, a=1.0, b=dt, x1=1, c1=dt)       # r1 = r0 + dt (L+Q)(r0)
+        s.collide(t + dt, 1, 2)                                   # r2 = Q(r1)
+        s.advect_combine(t + dt, 1, 0, a=0.5, b=0.5 * dt,         # r0 = r0/2 + r1/2
+                         x1=2, c1=0.5 * dt, x2=0, c2=0.5)         #      + dt/2 (L+Q)(r1)
+
+
+STEPPERS = {c.stepper_name: c for c in (StdEulerDGFSStepper, StdTVDRK2DGFSStepper)}
+
+
+def get_integrator(backend, system_or_factory, cfg):
+    """Controller 'none' x stepper by scheme name (integrators/__init__.py)."""
+    sect = 'solver-time-integrator'
+    ctrl = cfg.get(sect, 'controller', 'none')
+    if ctrl != 'none':
+        raise ValueError(f'unsupported controller {ctrl}')
+    scheme = cfg.get(sect, 'scheme')
+    if scheme not in STEPPERS:
+        raise ValueError(f'unsupported scheme {scheme}; have {sorted(STEPPERS)}')
+    cls = STEPPERS[scheme]
+    system = system_or_factory(cls.nregs) if callable(system_or_factory) else system_or_factory
+    return cls(backend, system, cfg)

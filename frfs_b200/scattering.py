@@ -1,0 +1,196 @@
+"""Scattering-model plugins: the fast-spectral VHS collision operator.
+
+Drop-in for ``DGFSScatteringModel`` / ``DGFSVHSGLLScatteringModel``
+(frfs/solvers/dgfs/scattering.py:16-286): registered by
+``scattering_model = 'vhs-gll'``, constructed as ``(backend, cfg, vm)``,
+with ``fs(d_arr_in, d_arr_out, elem, upt)`` for one DOF.  The batched
+``collide(fin, fout)`` evaluates every DOF in one persistent launch of
+``bdgfs_vhs_collide`` (hand-written sm_100a kernel, libbdgfs.so).
+
+Host precompute (FP64, then cast to the state precision):
+  prefactor  scattering.py:50-65
+  phase      exp(i (pi/L)(qz_p/2) s_{q,a} l0[k]) per axis: the separable
+             factors of exp(i a_pq) with a_pq = (pi/L)(qz_p/2)(l . s_q)
+             (vhs-gll.mako:45-69)
+  gw, bb2    (2 qw_p sw / n) bb1_p and bb2 (vhs-gll.mako:71-101, 172-207);
+             sinc(s) = sin(s + 1e-15)/(s + 1e-15) as in vhs-gll.mako:11-14
+"""
+from math import gamma
+
+import numpy as np
+import torch
+
+from . import _lib
+from .util import subclass_where  # noqa: F401  (registry helper re-export)
+
+
+class DGFSScatteringModel:
+    scattering_model = None
+
+    def __init__(self, backend, cfg, velocitymesh):
+        self.backend = backend
+        self.cfg = cfg
+        self.vm = velocitymesh
+        self.load_parameters()
+        self.perform_precomputation()
+
+    def load_parameters(self):
+        raise NotImplementedError
+
+    def perform_precomputation(self):
+        raise NotImplementedError
+
+    def fs(self, d_arr_in, d_arr_out, elem, upt):
+        raise NotImplementedError
+
+
+def _sinc_ref(s):
+    return np.sin(s + 1e-15) / (s + 1e-15)
+
+
+def vhs_prefactor(vm, omega, dRef, Tref, alpha=1.0, mass=1.0):
+    """scattering.py:50-65.  For a species of (normalised) mass ``mass`` the
+    self-collision form of frfs/solvers/dgfsbi/scattering.py:81-91 with
+    p = q, which reduces to the single-species formula at mass 1."""
+    gam = 2.0 * (1 - omega)
+    invKn = (vm.H0() * np.sqrt(2.0) * np.pi * vm.n0() * dRef * dRef
+             * (Tref / vm.T0())**(omega - 0.5))
+    mu = mass / 2.0
+    pref = invKn * alpha / (np.sqrt(2.0) * mu**(omega - 0.5)
+                            * 2.0**(1 + alpha) * gamma(2.5 - omega) * np.pi)
+    return gam, pref, 1.0 / invKn
+
+
+def vhs_tables(Nv, L, qz, qw, sz, sw, gam):
+    """Kernel tables in FP64 numpy (layouts of include/bdgfs.h)."""
+    N = Nv
+    NH = N // 2 + 1
+    n = N**3
+    l0 = np.concatenate((np.arange(0, N // 2), np.arange(-N // 2, 0))).astype(np.float64)
+    Nrho, M = len(qz), sz.shape[0]
+    beta = np.pi / L * qz / 2.0                                    # [Nrho]
+    arg = beta[:, None, None, None] * sz[None, :, :, None] * l0[None, None, None, :]
+    phase = np.exp(1j * arg)                                       # [Nrho][M][3][N]
+    # |l| on the [kz][kx][ky] index order
+    kz, kx, ky = np.meshgrid(l0, l0, l0, indexing='ij')
+    lmag = np.sqrt(kx * kx + ky * ky + kz * kz)                    # [kz][kx][ky]
+    gw = np.empty((Nrho, N, NH, N))
+    bb2 = np.zeros((N, N, N))
+    for p in range(Nrho):
+        bb1 = qz[p]**(gam + 2.0) * 4 * np.pi * _sinc_ref(np.pi / L * qz[p] / 2.0 * lmag)
+        gw[p] = (2.0 * qw[p] * sw / n) * bb1[:, :NH, :]
+        bb2 += qw[p] * qz[p]**(gam + 2.0) * 16 * np.pi * np.pi * \
+            _sinc_ref(np.pi / L * qz[p] * lmag)
+    return phase, gw, bb2
+
+
+def gram_inverse(c0, ndims_vel=3):
+    """Inverse Gram matrix of phi = {1, cx, cy, cz, |c|^2} over the grid."""
+    N = len(c0)
+    cx, cy, cz = np.meshgrid(c0, c0, c0, indexing='ij')
+    phi = np.stack([np.ones_like(cx), cx, cy, cz, cx * cx + cy * cy + cz * cz]).reshape(5, -1)
+    G = phi @ phi.T
+    return np.linalg.inv(G)
+
+
+class VHSGrid:
+    """Device-resident tables of one velocity grid (owned by the caller of
+    the C ABI; the kernel never allocates)."""
+
+    def __init__(self, Nv, L, qz, qw, sz, sw, gam, prefac, cw, c0, dtype, device):
+        self.Nv, self.Nrho, self.M = Nv, len(qz), sz.shape[0]
+        self.dtype = dtype
+        phase, gw, bb2 = vhs_tables(Nv, L, qz, qw, sz, sw, gam)
+        cdt = torch.complex64 if dtype == torch.float32 else torch.complex128
+        self.phase = torch.from_numpy(phase).to(cdt).to(device).contiguous()
+        self.gw = torch.from_numpy(gw).to(dtype).to(device).contiguous()
+        self.bb2 = torch.from_numpy(bb2).to(dtype).to(device).contiguous()
+        self.c0 = torch.from_numpy(np.asarray(c0, np.float64)).to(device)
+        self.ginv = torch.from_numpy(gram_inverse(c0)).to(device).contiguous()
+        self.prefac, self.cw = float(prefac), float(cw)
+        self.struct = _lib.VhsGrid(
+            Nv, self.Nrho, self.M, int(dtype == torch.float64), self.prefac, self.cw,
+            self.phase.data_ptr(), self.gw.data_ptr(), self.bb2.data_ptr(),
+            self.c0.data_ptr(), self.ginv.data_ptr())
+
+
+class VHSCollider:
+    """Owns scratch and the work counter for one set of grids and runs
+    ``bdgfs_vhs_collide`` (one persistent launch over all batches)."""
+
+    def __init__(self, grids, device):
+        self.grids = list(grids)
+        self.device = device
+        arr = (_lib.VhsGrid * len(self.grids))(*[g.struct for g in self.grids])
+        self._garr = arr
+        L = _lib.lib()
+        nbytes = L.bdgfs_vhs_scratch_bytes(arr, len(self.grids), 0)
+        if nbytes == 0:
+            raise _lib.BdgfsError('unsupported velocity grid set for bdgfs_vhs_collide')
+        self.scratch = torch.empty(nbytes, dtype=torch.uint8, device=device)
+        self.counter = torch.zeros(1, dtype=torch.int64, device=device)
+
+    def __call__(self, batches, project=True, exact=False, stream=None):
+        """batches: list of (grid_index, f[ndof, n], Q[ndof, n], moments|None)."""
+        L = _lib.lib()
+        bs = (_lib.VhsBatch * len(batches))()
+        for i, (gi, f, Q, mom) in enumerate(batches):
+            g = self.grids[gi]
+            n3 = g.Nv**3
+            if f.dtype != g.dtype or Q.dtype != g.dtype:
+                raise TypeError('state dtype does not match the grid tables')
+            if not (f.is_contiguous() and Q.is_contiguous()):
+                raise ValueError('f and Q must be contiguous [ndof][Nv^3]')
+            if f.numel() % n3 or Q.numel() != f.numel():
+                raise ValueError('f/Q sizes must be a multiple of Nv^3 and equal')
+            if mom is not None and (mom.dtype != torch.float64
+                                    or mom.numel() < 10 * (f.numel() // n3)):
+                raise ValueError('moments must be float64 [ndof][10]')
+            bs[i] = _lib.VhsBatch(gi, 0, f.numel() // n3, f.data_ptr(), Q.data_ptr(),
+                                  mom.data_ptr() if mom is not None else 0)
+        rc = L.bdgfs_vhs_collide(self._garr, len(self.grids), bs, len(batches),
+                                 (1 if project else 0) | (2 if exact else 0),
+                                 _lib.ptr(self.scratch),
+                                 self.scratch.numel(), _lib.ptr(self.counter),
+                                 _lib.stream_ptr(stream))
+        _lib.check(rc, 'bdgfs_vhs_collide')
+
+
+class DGFSVHSGLLScatteringModel(DGFSScatteringModel):
+    """'vhs-gll' (scattering.py:44-286) on the B200 kernel."""
+    scattering_model = 'vhs-gll'
+
+    def load_parameters(self):
+        cfg = self.cfg
+        self._omega = cfg.getfloat('scattering-model', 'omega')
+        self._dRef = cfg.getfloat('scattering-model', 'dRef')
+        self._Tref = cfg.getfloat('scattering-model', 'Tref')
+        self._mass = cfg.getfloat('scattering-model', 'mass', 1.0)
+        self._gamma, self._prefactor, self._Kn = vhs_prefactor(
+            self.vm, self._omega, self._dRef, self._Tref, mass=self._mass)
+        self._project = cfg.getbool('scattering-model', 'conservation-projection', True)
+        # exact Nyquist-plane treatment: default on for FP64 state
+        self._exact = cfg.getbool('scattering-model', 'exact-nyquist',
+                                  self.backend.fpdtype == torch.float64)
+
+    def perform_precomputation(self):
+        vm, be = self.vm, self.backend
+        self.grid = VHSGrid(vm.Nv(), vm.L(), vm.qz(), vm.qw(), vm.sz(), vm.sw(),
+                            self._gamma, self._prefactor, vm.cw(), vm.c0(),
+                            be.fpdtype, be.device)
+        self.collider = VHSCollider([self.grid], be.device)
+
+    def prefactor(self):
+        return self._prefactor
+
+    def collide(self, fin, fout, moments=None, project=None, exact=None):
+        """Q for every DOF: fin/fout [ndof][Nv^3] (any leading shape)."""
+        n3 = self.vm.vsize()
+        self.collider([(0, fin.reshape(-1, n3), fout.reshape(-1, n3), moments)],
+                      project=self._project if project is None else project,
+                      exact=self._exact if exact is None else exact)
+
+    def fs(self, d_arr_in, d_arr_out, elem, upt):
+        """One DOF (elem, upt) of a [neles][nupts][Nv^3] bank (per-DOF shim
+        of scattering.py:227)."""
+        self.collide(d_arr_in[elem, upt], d_arr_out[elem, upt])

@@ -1,0 +1,256 @@
+"""The DGFS system: state banks, FR operators, diffuse walls and Q.
+
+Drop-in for ``DGFSSystem`` (frfs/solvers/dgfs/system.py:17-231, name
+'dgfs') on the path the steppers use: ``rhs``, ``updatebc``, ``collide``,
+``invmass`` and the kernel registry ``_kernels`` keyed like
+``BaseSystem._gen_kernels`` (frfs/solvers/base/system.py:167-176).
+
+Differences of layout, not of meaning:
+* the state bank of one element type is a device tensor
+  ``[neles][nupts][Nv^3]`` (velocity contiguous) instead of the
+  reference's AoSoA ``(nupts, Nv^3, neles)``;
+* every velocity is advected in one pass, so ``batch``/``varidx`` are
+  accepted and ignored (the reference's NvBatchSize loop and its
+  copy_to/from_reg kernels disappear);
+* ('eles','tdisf'), ('eles','tdivtpcorf'), ('iint','comm_flux'),
+  ('bcint','comm_flux'), ('eles','tdivtconf') and ('eles','negdivconf')
+  are fused into one launch of ``bdgfs_fr_rhs``; in the registry the first
+  five resolve to no-ops and ``('eles','negdivconf')`` runs the fused
+  kernel, so a caller that runs them in the reference's order gets the
+  reference's result.
+"""
+import numpy as np
+import torch
+
+from . import _lib
+from .initcond import DGFSInitCondition, DGFSMaxwellianInitCondition
+from .mesh import ElementGeometry
+from .scattering import DGFSScatteringModel
+from .util import subclass_where
+from .velocitymesh import DGFSVelocityMesh
+
+
+class DGFSElements:
+    """Device-resident operators and metrics of one element type."""
+
+    def __init__(self, backend, geo, vm):
+        self.be, self.geo, self.vm = backend, geo, vm
+        shp = geo.shape
+        dt = backend.fpdtype
+        c = lambda a: backend.const(np.ascontiguousarray(a), dtype=dt)
+        self.neles, self.nupts, self.nfpts, self.ndims = geo.neles, geo.nupts, geo.nfpts, geo.ndims
+        self.m0 = c(shp.opmat('M0'))
+        self.dcorr = c(shp.opmat('M1 - M3*M2'))
+        self.m3 = c(shp.opmat('M3'))
+        self.smats = c(geo.smats)
+        self.rcpdjac = c(geo.rcpdjac)
+        self.pnorm = c(geo.norm_pnorm)
+        self.magn = c(geo.mag_pnorm)
+        self.nbr = backend.const(geo.nbr, dtype=torch.int32)
+        self.c0 = c(vm.c0())
+        self.struct = _lib.FrEles(
+            geo.ndims, geo.nupts, geo.nfpts, geo.neles, vm.vsize(), vm.Nv(),
+            int(dt == torch.float64),
+            self.m0.data_ptr(), self.dcorr.data_ptr(), self.m3.data_ptr(),
+            self.smats.data_ptr(), self.rcpdjac.data_ptr(), self.pnorm.data_ptr(),
+            self.magn.data_ptr(), self.nbr.data_ptr(), self.c0.data_ptr())
+
+    def ploc_at_np(self, name):
+        return {'upts': self.geo.plocupts, 'fpts': self.geo.plocfpts}[name]
+
+
+class DGFSWallDiffuseBCInters:
+    """Diffuse walls ('dgfs-wall-diffuse', frfs/solvers/dgfs/inters.py:175-229):
+    wall Maxwellian f_w and wall velocity per boundary, bc0/bc1 per wall
+    face point."""
+    type = 'dgfs-wall-diffuse'
+
+    def __init__(self, backend, geo, vm, cfg, bcsects):
+        self.be = backend
+        dt = backend.fpdtype
+        fws, uws = [], []
+        for sect in bcsects:
+            bc = DGFSMaxwellianInitCondition(backend, cfg, vm, sect)
+            fws.append(bc.get_init_vals())
+            uws.append(bc.unondim()[:, 0])
+        nw = len(geo.wall_fpts)
+        self.nwall = nw
+        self.fw = backend.const(np.array(fws).reshape(len(fws), -1) if fws else np.zeros((1, 1)), dtype=dt)
+        self.uwall = backend.const(np.array(uws).reshape(-1, 3) if uws else np.zeros((1, 3)), dtype=dt)
+        self.fpt = backend.const(geo.wall_fpts.reshape(-1, 2) if nw else np.zeros((1, 2)),
+                                 dtype=torch.int32)
+        self.bcid = backend.const(geo.wall_bcid if nw else np.zeros(1), dtype=torch.int32)
+        self.bcv = backend.zeros(max(nw, 1), 2)
+        self.struct = _lib.FrWall(nw, len(fws), self.fpt.data_ptr(), self.bcid.data_ptr(),
+                                  self.uwall.data_ptr(), self.fw.data_ptr(), self.bcv.data_ptr(),
+                                  float(vm.cw()))
+
+
+class DGFSSystem:
+    name = 'dgfs'
+    elementscls = DGFSElements
+    velocitymeshcls = DGFSVelocityMesh
+    scatteringcls = DGFSScatteringModel
+
+    def __init__(self, backend, mesh, cfg, nreg=3, initsoln=None):
+        self.backend, self.cfg, self.mesh = backend, cfg, mesh
+        self.vm = self.velocitymeshcls(backend, cfg)
+        order = cfg.getint('solver', 'order')
+        self.geo = ElementGeometry(mesh, order)
+        self.ele = self.elementscls(backend, self.geo, self.vm)
+        self.ndims = self.geo.ndims
+        # boundary conditions: every named boundary must be a configured wall
+        sects = []
+        for name in self.geo.wall_names:
+            sect = f'soln-bcs-{name}'
+            bctype = cfg.get(sect, 'type')
+            if bctype != 'dgfs-wall-diffuse':
+                raise ValueError(f'unsupported boundary condition {bctype} on {name}')
+            sects.append(sect)
+        self.walls = DGFSWallDiffuseBCInters(backend, self.geo, self.vm, cfg, sects)
+        # time-step estimate (system.py:50-66)
+        advmax = self.vm.L()
+        self.unitCFLdt = np.sqrt(np.min(self.geo.djac)) / advmax / self.ndims
+        # collision model by name (system.py:68-72)
+        smn = cfg.get('scattering-model', 'type')
+        self.sm = subclass_where(self.scatteringcls, scattering_model=smn)(backend, cfg, self.vm)
+        # register banks [neles][nupts][Nv^3]
+        E, U, nv = self.ele.neles, self.ele.nupts, self.vm.vsize()
+        self.eles_scal_upts_inb_full = [backend.empty(E, U, nv) for _ in range(nreg)]
+        self._uf = backend.empty(E, self.ele.nfpts, nv)
+        if initsoln is not None:
+            self.eles_scal_upts_inb_full[0].copy_(torch.as_tensor(initsoln).to(
+                self.eles_scal_upts_inb_full[0]))
+        else:
+            icn = cfg.get('soln-ics', 'type')
+            ic = subclass_where(DGFSInitCondition, model=icn)(backend, cfg, self.vm, 'soln-ics')
+            f0 = backend.const(ic.get_init_vals())
+            self.eles_scal_upts_inb_full[0].copy_(f0.expand(E, U, nv))
+        self._gen_kernels()
+
+    # -- kernel registry ------------------------------------------------
+    def _gen_kernels(self):
+        noop = lambda **kw: None
+        self._kernels = {
+            ('eles', 'disu'): self._disu,
+            ('eles', 'tdisf'): noop, ('eles', 'tdivtpcorf'): noop,
+            ('iint', 'comm_flux'): noop, ('bcint', 'comm_flux'): noop,
+            ('eles', 'tdivtconf'): noop,
+            ('eles', 'negdivconf'): self._fused_rhs,
+            ('bcint', 'update_bc'): self._update_bc,
+        }
+        self._active = (0, 1)
+
+    def _bank(self, i):
+        return self.eles_scal_upts_inb_full[i]
+
+    def _disu(self, **kw):
+        u = self._bank(self._active[0])
+        _lib.check(_lib.lib().bdgfs_fr_disu(_lib.ref(self.ele.struct), _lib.ptr(u),
+                                            _lib.ptr(self._uf), _lib.stream_ptr()),
+                   'bdgfs_fr_disu')
+
+    def _update_bc(self, **kw):
+        _lib.check(_lib.lib().bdgfs_fr_bc_update(_lib.ref(self.ele.struct),
+                                                 _lib.ref(self.walls.struct),
+                                                 _lib.ptr(self._uf), _lib.stream_ptr()),
+                   'bdgfs_fr_bc_update')
+
+    def _fused_rhs(self, a=0.0, b=1.0, x1=None, c1=0.0, x2=None, c2=0.0, out=None, **kw):
+        u = self._bank(self._active[0])
+        out = self._bank(self._active[1]) if out is None else out
+        L = _lib.lib()
+        rc = L.bdgfs_fr_rhs(_lib.ref(self.ele.struct), _lib.ref(self.walls.struct),
+                            u.data_ptr(), self._uf.data_ptr(), out.data_ptr(), float(a), float(b),
+                            x1.data_ptr() if x1 is not None else None, float(c1),
+                            x2.data_ptr() if x2 is not None else None, float(c2),
+                            _lib.stream_ptr())
+        _lib.check(rc, 'bdgfs_fr_rhs')
+
+    # -- reference system methods ----------------------------------------
+    def rhs(self, t, uinbank, foutbank, batch=None, varidx=None):
+        """foutbank <- -div F(uinbank) (system.py:140-177); uses the bc0/bc1
+        left by the last ``updatebc``."""
+        self._active = (uinbank, foutbank)
+        k = self._kernels
+        k['eles', 'disu']()
+        for name in (('eles', 'tdisf'), ('eles', 'tdivtpcorf'), ('iint', 'comm_flux'),
+                     ('bcint', 'comm_flux'), ('eles', 'tdivtconf')):
+            k[name](t=t, varidx=varidx)
+        k['eles', 'negdivconf'](t=t)
+
+    def updatebc(self, t, uinbank, foutbank, batch=None, varidx=None):
+        """disu + update_bc over all velocities (system.py:180-196)."""
+        self._active = (uinbank, foutbank)
+        self._kernels['eles', 'disu']()
+        self._kernels['bcint', 'update_bc'](t=t)
+
+    def collide(self, t, uinbank, foutbank):
+        """foutbank <- Q(uinbank) for every DOF in one launch (system.py:199-218)."""
+        self.sm.collide(self._bank(uinbank), self._bank(foutbank))
+
+    def invmass(self, uinbank, foutbank):
+        raise NotImplementedError('invmass is unused by the DGFS steppers')
+
+    # -- fused stage used by the steppers ---------------------------------
+    def advect_combine(self, t, uinbank, outbank, a, b, x1=None, c1=0.0, x2=None, c2=0.0):
+        """out = a*u + b*L(u) + c1*x1 + c2*x2 (bc update included)."""
+        self._active = (uinbank, outbank)
+        self._disu()
+        if self.walls.nwall:
+            self._update_bc()
+        self._fused_rhs(a=a, b=b, x1=self._bank(x1) if x1 is not None else None, c1=c1,
+                        x2=self._bank(x2) if x2 is not None else None, c2=c2)
+
+    # -- diagnostics ------------------------------------------------------
+    def moments(self, bank):
+        """Non-dimensional rho, U, T, q, P per DOF (FP64 on the GPU)."""
+        return macroscopic(self._bank(bank), self.vm)
+
+    def residual(self, a, b):
+        out = torch.zeros(2, dtype=torch.float64, device=self.backend.device)
+        x, y = self._bank(a), self._bank(b)
+        L = _lib.lib()
+        _lib.check(L.bdgfs_residual(x.data_ptr(), y.data_ptr(), x.numel(),
+                                    int(x.dtype == torch.float64), out.data_ptr(),
+                                    _lib.stream_ptr()), 'bdgfs_residual')
+        return out
+
+
+def raw_moments(f, vm):
+    """FP64 raw moments [ndof][13] (bdgfs_moments)."""
+    n3 = vm.vsize()
+    f2 = f.reshape(-1, n3)
+    out = torch.empty(f2.shape[0], 13, dtype=torch.float64, device=f.device)
+    c0 = torch.as_tensor(vm.c0(), dtype=torch.float64, device=f.device)
+    L = _lib.lib()
+    _lib.check(L.bdgfs_moments(f2.data_ptr(), f2.shape[0], vm.Nv(), int(f.dtype == torch.float64),
+                               c0.data_ptr(), float(vm.cw()), out.data_ptr(), _lib.stream_ptr()),
+               'bdgfs_moments')
+    return out
+
+
+def macroscopic(f, vm):
+    """rho, U[3], T, q[3], P[6] per DOF from the FP64 raw moments, with the
+    definitions of frfs/plugins/dgfsmomwriterstd.py:151-213 (3-D, mr = 1)."""
+    m = raw_moments(f, vm)
+    rho = m[:, 0]
+    U = m[:, 1:4] / rho[:, None]
+    Sxx = m[:, 4:10]                                   # xx xy xz yy yz zz
+    ij = ((0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2))
+    P = torch.stack([2.0 * (Sxx[:, k] - rho * U[:, a] * U[:, b]) for k, (a, b) in enumerate(ij)], 1)
+    tr = (P[:, 0] + P[:, 3] + P[:, 5]) / 2.0          # sum f |c-U|^2 cw
+    T = tr * (2.0 / 3.0) / rho
+    # q_a = sum f |c-U|^2 (c-U)_a cw from raw moments
+    S = torch.zeros(m.shape[0], 3, 3, dtype=torch.float64, device=m.device)
+    for k, (a, b) in enumerate(ij):
+        S[:, a, b] = Sxx[:, k]
+        S[:, b, a] = Sxx[:, k]
+    trS = S[:, 0, 0] + S[:, 1, 1] + S[:, 2, 2]
+    U2 = (U * U).sum(1)
+    m1 = m[:, 1:4]
+    # |c-U|^2 (c-U) expanded: M3 - tr(S) U - 2 S U + 2 U (U.m1) + |U|^2 m1 - rho |U|^2 U
+    q = (m[:, 10:13] - trS[:, None] * U - 2.0 * torch.einsum('nab,nb->na', S, U)
+         + 2.0 * U * (U * m1).sum(1, keepdim=True) + U2[:, None] * m1
+         - (rho * U2)[:, None] * U)
+    return rho, U, T, q, P

@@ -1,0 +1,168 @@
+/*
+ * bdgfs: B200-native DGFS hot path (fast-spectral Boltzmann collision
+ * operator and flux-reconstruction advection) behind a plain C ABI.
+ *
+ * Every entry point takes device pointers, sizes and a CUDA stream passed
+ * as void*, returns an int32 status (0 = ok, negative = error), never
+ * allocates device memory and never synchronises the host, so a sequence
+ * of calls can be captured in a CUDA graph.  Buffers and scratch are owned
+ * by the caller.
+ */
+#ifndef BDGFS_H
+#define BDGFS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BDGFS_OK 0
+#define BDGFS_EINVAL (-1)       /* bad argument / size / layout             */
+#define BDGFS_ECUDA (-2)        /* a CUDA runtime call failed               */
+#define BDGFS_EUNSUPPORTED (-3) /* grid size / precision not compiled in    */
+#define BDGFS_ETIMEOUT (-4)     /* a bounded device wait gave up            */
+#define BDGFS_ESCRATCH (-5)     /* caller-provided scratch is too small     */
+
+/* ------------------------------------------------------------------------
+ * Fast-spectral VHS collision operator Q(f, f)
+ * ---------------------------------------------------------------------- */
+
+/* One velocity grid (Nv^3 cube) with its precomputed tables.  All table
+ * pointers are device pointers; "real" means float when fp64 == 0 and
+ * double when fp64 == 1, "complex" the matching (re, im) pair. */
+typedef struct bdgfs_vhs_grid {
+    int32_t Nv;          /* points per axis: 8, 12, 16, 24 or 32            */
+    int32_t Nrho;        /* radial Gauss-Jacobi points                      */
+    int32_t M;           /* half-sphere directions                          */
+    int32_t fp64;        /* 0: FP32 state/tables, 1: FP64                   */
+    double prefac;       /* VHS prefactor                                   */
+    double cw;           /* velocity cell volume (2L/Nv)^3                  */
+    const void* phase;   /* complex [Nrho][M][3][Nv]:
+                            exp(i*(pi/L)*(qz_p/2)*s_{q,a}*l0[k])            */
+    const void* gw;      /* real [Nrho][Nv][Nv/2+1][Nv], index [p][kz][kx][ky]:
+                            (2*qw_p*sw/Nv^3) * bb1_p(k)                     */
+    const void* bb2;     /* real [Nv][Nv][Nv], index [kz][kx][ky]            */
+    const double* c0;    /* [Nv] cell-centre velocities                     */
+    const double* ginv;  /* [5][5] inverse Gram matrix of {1,cx,cy,cz,|c|^2} */
+} bdgfs_vhs_grid;
+
+/* A batch of distributions living on one grid. */
+typedef struct bdgfs_vhs_batch {
+    int32_t grid;        /* index into the grids array                      */
+    int32_t pad_;
+    int64_t ndof;        /* number of distributions                         */
+    const void* f;       /* real [ndof][Nv^3], velocity index (x*Nv+y)*Nv+z  */
+    void* Q;             /* real [ndof][Nv^3]                               */
+    double* moments;     /* optional [ndof][10]: C.Q before (0..4) and after
+                            (5..9) the projection, in FP64, C = cw*{1,c,|c|^2} */
+} bdgfs_vhs_batch;
+
+/* Bytes of device scratch bdgfs_vhs_collide needs for nctas resident CTAs
+ * (nctas <= 0: one per SM of the current device). */
+size_t bdgfs_vhs_scratch_bytes(const bdgfs_vhs_grid* grids, int32_t ngrids,
+                               int32_t nctas);
+
+#define BDGFS_PROJECT 1  /* FP64 minimal-norm conservation projection      */
+#define BDGFS_EXACT 2    /* also carry the second-order Nyquist-plane term  */
+
+/* Q for every distribution of every batch, in one persistent launch.
+ * flags & BDGFS_PROJECT applies the FP64 minimal-norm conservation
+ * projection Q <- Q - phi^T G^{-1} (phi Q); flags & BDGFS_EXACT runs a
+ * second transform per (p, q) so that the result equals the reference's
+ * complex-square form to rounding (2x the work).  work_counter: one device uint64 that this
+ * call resets (stream-ordered) and uses to hand out distributions.
+ * Replaces DGFSVHSGLLScatteringModel.fs (frfs/solvers/dgfs/scattering.py:227)
+ * called for every (elem, upt) by DGFSSystem.collide
+ * (frfs/solvers/dgfs/system.py:199-218). */
+int32_t bdgfs_vhs_collide(const bdgfs_vhs_grid* grids, int32_t ngrids,
+                          const bdgfs_vhs_batch* batches, int32_t nbatch,
+                          int32_t flags, void* scratch, size_t scratch_bytes,
+                          uint64_t* work_counter, void* stream);
+
+/* Measured FP32 FMA throughput probe: runs iters dependent-free FMA chains
+ * per thread on nblocks x 256 threads and writes a checksum to out[0]. */
+int32_t bdgfs_fma_probe(float* out, int32_t nblocks, int32_t iters,
+                        void* stream);
+
+/* ------------------------------------------------------------------------
+ * Flux-reconstruction advection (all Nv^3 velocities per launch)
+ * ---------------------------------------------------------------------- */
+
+/* One element type.  State u[e][upt][v], face values uf[e][fpt][v],
+ * v = (x*Nv + y)*Nv + z.  "real" is float (fp64 == 0) or double. */
+typedef struct bdgfs_fr_eles {
+    int32_t ndims;       /* 2 (quad) or 3 (hex)                            */
+    int32_t nupts;       /* solution points per element                    */
+    int32_t nfpts;       /* flux points per element                        */
+    int32_t neles;
+    int64_t nv;          /* Nv^3                                           */
+    int32_t Nv;
+    int32_t fp64;
+    const void* m0;      /* real [nfpts][nupts]        M0                  */
+    const void* dcorr;   /* real [nupts][ndims*nupts]  M1 - M3*M2          */
+    const void* m3;      /* real [nupts][nfpts]        M3                  */
+    const void* smats;   /* real [neles][nupts][ndims][ndims]              */
+    const void* rcpdjac; /* real [neles][nupts]                            */
+    const void* pnorm;   /* real [neles][nfpts][ndims] unit outward normal */
+    const void* magn;    /* real [neles][nfpts]        |J J^-T n|          */
+    const int32_t* nbr;  /* [neles][nfpts]: e'*nfpts+f' of the neighbour
+                            face point, or -1 - (wall face-point index)     */
+    const void* c0;      /* real [Nv] cell-centre velocities               */
+} bdgfs_fr_eles;
+
+/* Diffuse-wall face points. */
+typedef struct bdgfs_fr_walls {
+    int32_t nwall;       /* wall face points                               */
+    int32_t nbc;         /* wall boundary conditions                       */
+    const int32_t* fpt;  /* [nwall][2] (element, flux point)               */
+    const int32_t* bcid; /* [nwall] boundary condition of each point       */
+    const void* uwall;   /* real [nbc][3] wall velocity                    */
+    const void* fw;      /* real [nbc][nv] wall Maxwellian                 */
+    void* bcv;           /* real [nwall][2] bc0, bc1 (written by bc_update) */
+    double cw;           /* velocity cell volume                           */
+} bdgfs_fr_walls;
+
+/* uf = M0 u.  Replaces kernels['eles', 'disu'] (solvers/dgfs/elements.py:56-59). */
+int32_t bdgfs_fr_disu(const bdgfs_fr_eles* el, const void* u, void* uf,
+                      void* stream);
+
+/* bc0/bc1 of every diffuse-wall face point from uf.  Replaces
+ * kernels['bcint', 'update_bc'] (solvers/dgfs/inters.py:221-229,
+ * kernels/bccupdate.mako, kernels/bcs/dgfs-wall-diffuse-update.mako),
+ * summed over all velocities in one pass. */
+int32_t bdgfs_fr_bc_update(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl,
+                           const void* uf, void* stream);
+
+/* out = a*u + b*L(u) + c1*x1 + c2*x2 with L(u) = -div F (FR, upwind
+ * interfaces, diffuse walls).  x1/x2 may be NULL; out may alias u, x1 or
+ * x2.  Replaces kernels ('eles','tdisf'), ('eles','tdivtpcorf'),
+ * ('iint','comm_flux'), ('bcint','comm_flux'), ('eles','tdivtconf'),
+ * ('eles','negdivconf') of DGFSSystem.rhs (solvers/dgfs/system.py:140-177)
+ * and the stepper's axnpby (backends/cuda/blasext.py:14-43). */
+int32_t bdgfs_fr_rhs(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl,
+                     const void* u, const void* uf, void* out, double a,
+                     double b, const void* x1, double c1, const void* x2,
+                     double c2, void* stream);
+
+/* FP64 raw velocity moments of ndof distributions, out[ndof][13]:
+ * cw*sum{f, c f (3), c_i c_j f (xx xy xz yy yz zz), |c|^2 c f (3)}.
+ * Feeds the macroscopic fields of plugins/dgfsmomwriterstd.py:14-313. */
+int32_t bdgfs_moments(const void* f, int64_t ndof, int32_t Nv, int32_t fp64,
+                      const double* c0, double cw, double* out, void* stream);
+
+/* out2[0] = sum (a-b)^2, out2[1] = sum b^2 in FP64 (residual norm of
+ * plugins/dgfsresidualstd.py:34-80). */
+int32_t bdgfs_residual(const void* a, const void* b, int64_t n, int32_t fp64,
+                       double* out2, void* stream);
+
+/* *status |= 1 if any of the n values is NaN or Inf (plugins/nancheck.py). */
+int32_t bdgfs_status_check(const void* a, int64_t n, int32_t fp64,
+                           int32_t* status, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BDGFS_H */

@@ -1,0 +1,24 @@
+"""CPU oracle for the DGFS hot path.
+
+TEST INFRASTRUCTURE ONLY.  Nothing in the product package (``frfs_b200``)
+imports, links or runs anything from this directory; only ``tests/``,
+``__graft_entry__.smoke()`` and the ``cpu_baseline`` / ``--impl reference``
+legs of ``bench.py`` use it, and only as the checker or as the timed CPU
+restatement of the reference algorithm.
+
+Every function restates, in FP64 numpy, the reference algorithm of
+jaisw7/frfs for one row of the hot path and cites the reference file:line
+it follows.  The restatement keeps the reference's own operation order and
+normalisations (cuFFT Z2Z conventions: forward exp(-2*pi*i*jk/n),
+inverse exp(+2*pi*i*jk/n), both unnormalised).
+
+Parity pins: FR operator matrices, quadrature rules and spherical designs
+are pinned against fixtures produced by the reference's own Python modules
+(``tests/golden/make_golden.py``); the VHS precompute tables are pinned
+against the reference's own numpy formulation of them (the docstring block
+in ``frfs/solvers/dgfs/scattering.py:94-126``, executed by the same
+script).  The collision operator itself cannot be run from the reference
+here (it needs PyCUDA, Mako and cuFFT), so Q is pinned by known-answer
+tests instead: Q(Maxwellian) ~ 0, conservation of mass/momentum/energy,
+and the Bobylev-Krook-Wu analytic solution for Maxwell molecules.
+"""

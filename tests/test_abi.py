@@ -1,0 +1,68 @@
+"""The C ABI library loads, exports every symbol include/bdgfs.h declares,
+and the ctypes mirrors of its structs have the C layout (checked against
+offsetof/sizeof from a C program compiled with the header)."""
+import os
+import re
+import shutil
+import subprocess
+
+import pytest
+
+from frfs_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, 'include', 'bdgfs.h')
+
+
+def _declared():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r'\b(bdgfs_\w+)\s*\(', txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    names = _declared()
+    assert len(names) >= 9
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) == set(_lib.EXPORTS) | set(n for n in names if n not in _lib.EXPORTS) \
+        and set(_lib.EXPORTS) <= set(names)
+
+
+STRUCTS = {
+    'bdgfs_vhs_grid': _lib.VhsGrid,
+    'bdgfs_vhs_batch': _lib.VhsBatch,
+    'bdgfs_fr_eles': _lib.FrEles,
+    'bdgfs_fr_walls': _lib.FrWall,
+}
+
+
+@pytest.mark.skipif(shutil.which('gcc') is None, reason='no C compiler')
+def test_struct_layouts_match_header(tmp_path):
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"',
+             'int main(void) {']
+    for cname, cls in STRUCTS.items():
+        lines.append(f'printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ['return 0;', '}']
+    src = tmp_path / 'off.c'
+    src.write_text('\n'.join(lines))
+    exe = tmp_path / 'off'
+    subprocess.check_call(['gcc', str(src), '-o', str(exe)])
+    out = subprocess.check_output([str(exe)], text=True)
+    for line in out.splitlines():
+        cname, field, val = line.split()
+        cls = STRUCTS[cname]
+        if field == 'sizeof':
+            assert __import__('ctypes').sizeof(cls) == int(val), cname
+        else:
+            assert getattr(cls, field).offset == int(val), (cname, field)
+
+
+def test_invalid_arguments_return_status_not_crash():
+    L = _lib.lib()
+    assert L.bdgfs_vhs_collide(None, 0, None, 0, 0, None, 0, None, None) == -1
+    assert L.bdgfs_fr_disu(None, None, None, None) == -1
+    assert L.bdgfs_residual(None, None, 0, 0, None, None) == -1
+    assert L.bdgfs_vhs_scratch_bytes(None, 0, 1) == 0

@@ -1,0 +1,132 @@
+"""The oracle against the reference's own outputs (golden fixtures) and
+known-answer properties of the collision operator."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle.velocitymesh import VelocityMesh, gauss_jacobi
+from oracle.vhs import VHSOracle, precompute, vhs_prefactor
+
+from helpers import NONDIM, maxwellian, mixed_maxwellians, rel_l2
+
+GOLD = os.path.join(os.path.dirname(__file__), 'golden')
+
+
+def _vm(name):
+    g = np.load(f'{GOLD}/vmesh_{name}.npz')
+    dev = {'c1': 5, 'nv8': 5, 'm16': 6}[name]
+    vm = VelocityMesh(int(g['Nv']), int(g['Nrho']), g['sz'], cmax=0.0, Tmax=NONDIM['T0'],
+                      dev=dev, **NONDIM)
+    return vm, g
+
+
+@pytest.mark.parametrize('name', ['c1', 'nv8', 'm16'])
+def test_velocity_mesh_matches_reference(name):
+    vm, g = _vm(name)
+    assert np.array_equal(vm.cv, g['cv'])
+    assert vm.cw == float(g['cw']) and vm.L == float(g['L'])
+    assert np.allclose(vm.qz, g['qz'], rtol=0, atol=1e-14)
+    assert np.allclose(vm.qw, g['qw'], rtol=0, atol=1e-14)
+    assert vm.sw == float(g['sw'])
+    assert np.isclose(vm.u0, float(g['u0'])) and np.isclose(vm.n0, float(g['n0']))
+
+
+def test_gauss_jacobi_matches_reference():
+    d = np.load(f'{GOLD}/sphdesign.npz')
+    for n in (8, 12):
+        z, w = gauss_jacobi(n)
+        assert np.allclose(z, d[f'gj{n}_z'], atol=1e-14)
+        assert np.allclose(w, d[f'gj{n}_w'], atol=1e-14)
+
+
+def test_vhs_tables_match_reference_numpy_formulation():
+    vm, _ = _vm('nv8')
+    p = np.load(f'{GOLD}/vhs_precompute_nv8.npz')
+    aa, bb1, bb2 = precompute(vm, float(p['gamma']))
+    assert np.abs(aa.ravel() - p['aa']).max() < 1e-13
+    assert np.abs(bb1.ravel() - p['bb1']).max() < 1e-13 * np.abs(p['bb1']).max()
+    assert np.abs(bb2 - p['bb2']).max() < 1e-13 * np.abs(p['bb2']).max()
+
+
+def test_maxwellian_and_bkw_initial_values_match_reference():
+    from oracle.fr import velocities
+    vm, g = _vm('c1')
+    ic = np.load(f'{GOLD}/initcond.npz')
+    f = maxwellian(vm.cv, float(ic['rho']), ic['u'], float(ic['T']))
+    assert np.allclose(f, ic['maxwellian'], rtol=1e-13, atol=0)
+    K = 1.0 - np.exp(-float(ic['bkw_t0']) / 6.0)
+    c2 = np.sum(vm.cv**2, axis=0)
+    bkw = 1 / (2 * (2 * np.pi * K)**1.5) * np.exp(-c2 / (2 * K)) * ((5 * K - 3) / K + (1 - K) / K**2 * c2)
+    assert np.allclose(bkw, ic['bkw'], rtol=1e-13, atol=1e-300)
+
+
+@pytest.fixture(scope='module')
+def c1_oracle():
+    vm, _ = _vm('c1')
+    return vm, VHSOracle(vm, 0.5, 4.17e-10, 273.0)
+
+
+def test_prefactor_formula(c1_oracle):
+    vm, orc = c1_oracle
+    gam, pref, Kn = vhs_prefactor(vm, 0.81, 4.17e-10, 273.0)
+    assert np.isclose(gam, 0.38) and Kn > 0 and pref > 0
+    # hard sphere: gamma = 1
+    assert np.isclose(orc.gamma, 1.0)
+
+
+def test_q_maxwellian_is_spectrally_small(c1_oracle):
+    vm, orc = c1_oracle
+    f = maxwellian(vm.cv, 1.0, [0.1, -0.05, 0.0], 1.0)
+    gain, loss = orc.gain_loss(f)
+    assert np.linalg.norm(orc.Q(f)) < 1e-3 * np.linalg.norm(loss)
+
+
+def test_q_conserves_mass_momentum_energy(c1_oracle):
+    vm, orc = c1_oracle
+    rng = np.random.default_rng(0)
+    f = mixed_maxwellians(vm.cv, rng, k=2, nrange=(0.5, 1.5), umax=0.5, Trange=(0.7, 1.3),
+                          noise=0.0)
+    q = orc.Q(f)
+    gain, loss = orc.gain_loss(f)
+    scale = np.abs(loss).sum() * vm.cw
+    c2 = np.sum(vm.cv**2, axis=0)
+    for phi in (np.ones_like(c2), vm.cv[0], vm.cv[1], vm.cv[2], c2):
+        assert abs(np.sum(phi * q) * vm.cw) < 2e-3 * scale * (1 + np.abs(phi).max())
+
+
+def test_q_commutes_with_axis_reflection(c1_oracle):
+    """Reflecting c_y -> -c_y maps the icosahedral half-sphere design onto
+    itself (up to antipodes), so Q commutes with the reflection up to the
+    reference's Nyquist-plane asymmetry (l0 holds -N/2 but not +N/2)."""
+    vm, orc = c1_oracle
+    rng = np.random.default_rng(4)
+    N = vm.Nv
+    f = mixed_maxwellians(vm.cv, rng, k=2, nrange=(0.5, 1.5), umax=0.5, Trange=(0.7, 1.3),
+                          noise=0.0)
+    fr = f.reshape(N, N, N)[:, ::-1, :].ravel()        # c_y -> -c_y
+    q = orc.Q(f).reshape(N, N, N)[:, ::-1, :].ravel()
+    assert rel_l2(orc.Q(fr), q) < 1e-4
+
+
+def test_bkw_known_answer():
+    """Maxwell molecules (omega = 1, gamma = 0): Q(f_BKW(t)) is the time
+    derivative of the BKW solution for the operator's own time scale.  With
+    the reference normalisation, Q(f) / (df/dt) is one constant; check that
+    Q is proportional to the analytic derivative to 2%."""
+    dev = 7
+    sz = np.load(f'{GOLD}/vmesh_c1.npz')['sz']
+    vm = VelocityMesh(24, 12, sz, cmax=0.0, Tmax=NONDIM['T0'], dev=dev, **NONDIM)
+    orc = VHSOracle(vm, 1.0, 4.17e-10, 273.0)
+    c2 = np.sum(vm.cv**2, axis=0)
+
+    def bkw(t):
+        K = 1.0 - np.exp(-t / 6.0)
+        return (1 / (2 * (2 * np.pi * K)**1.5) * np.exp(-c2 / (2 * K))
+                * ((5 * K - 3) / K + (1 - K) / K**2 * c2))
+    t0, h = 5.5, 1e-4
+    dfdt = (bkw(t0 + h) - bkw(t0 - h)) / (2 * h)
+    q = orc.Q(bkw(t0))
+    scale = np.dot(q, dfdt) / np.dot(dfdt, dfdt)
+    assert scale > 0
+    assert rel_l2(q, scale * dfdt) < 2e-2

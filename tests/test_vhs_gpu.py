@@ -1,0 +1,95 @@
+"""GPU parity of the collision operator (bdgfs_vhs_collide through the
+C ABI) against the FP64 oracle of the reference algorithm."""
+import numpy as np
+import pytest
+import torch
+
+from frfs_b200.backend import CUDABackend
+from frfs_b200.scattering import DGFSVHSGLLScatteringModel
+from frfs_b200.velocitymesh import DGFSVelocityMesh
+
+from helpers import vhs_cfg, oracle_for, mixed_maxwellians, rel_l2, maxwellian
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(Nv, Nrho, M, dev, precision):
+    cfg = vhs_cfg(Nv, Nrho, M, dev, precision=precision)
+    be = CUDABackend(cfg)
+    vm = DGFSVelocityMesh(be, cfg)
+    sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
+    return be, vm, sm, oracle_for(vm)
+
+
+# (Nv, Nrho, M, dev, precision, exact, tol): tolerance is relative L2 of Q
+CASES = [
+    (8, 4, 6, 5, "double", True, 1e-10),
+    (12, 6, 6, 5, "double", True, 1e-10),
+    (16, 8, 6, 5, "double", True, 1e-10),
+    (8, 4, 6, 5, "single", True, 2e-4),
+    (16, 8, 6, 5, 'single', False, 2e-4),
+    (24, 12, 12, 6, 'single', False, 2e-4),
+    (32, 16, 12, 6, 'single', False, 2e-4),
+]
+
+
+@pytest.mark.parametrize('Nv,Nrho,M,dev,prec,exact,tol', CASES)
+def test_q_parity(cuda, Nv, Nrho, M, dev, prec, exact, tol):
+    be, vm, sm, orc = _setup(Nv, Nrho, M, dev, prec)
+    rng = np.random.default_rng(100 + Nv)
+    ndof = 3
+    F = np.stack([mixed_maxwellians(vm.cv(), rng) for _ in range(ndof)])
+    fin = torch.from_numpy(F).to(be.fpdtype).to(be.device)
+    fout = torch.empty_like(fin)
+    sm.collide(fin, fout, project=False, exact=exact)
+    torch.cuda.synchronize()
+    Qg = fout.double().cpu().numpy()
+    for i in range(ndof):
+        Fi = fin[i].double().cpu().numpy()      # the state the kernel saw
+        Qo = orc.Q(Fi)
+        err = rel_l2(Qg[i], Qo)
+        assert err < tol, (i, err)
+
+
+def test_q_conservation_projection(cuda):
+    be, vm, sm, orc = _setup(24, 12, 12, 6, 'single')
+    rng = np.random.default_rng(7)
+    F = np.stack([mixed_maxwellians(vm.cv(), rng) for _ in range(4)])
+    fin = torch.from_numpy(F).float().to(be.device)
+    q0 = torch.empty_like(fin)
+    q1 = torch.empty_like(fin)
+    mom = torch.zeros(4, 10, dtype=torch.float64, device=be.device)
+    sm.collide(fin, q0, project=False)
+    sm.collide(fin, q1, moments=mom, project=True)
+    torch.cuda.synchronize()
+    m = mom.cpu().numpy()
+    # projection exactness in FP64 before the cast: |C.Qc| / |C.Q| small
+    scale = np.abs(m[:, :5]).max(axis=1) + 1e-300
+    assert np.all(np.abs(m[:, 5:]).max(axis=1) <= 1e-12 * np.maximum(scale, 1.0))
+    # the correction is small relative to Q
+    a, b = q1.double().cpu().numpy(), q0.double().cpu().numpy()
+    assert rel_l2(a, b) < 1e-2
+
+
+def test_q_maxwellian_is_small(cuda):
+    be, vm, sm, orc = _setup(24, 12, 12, 6, 'single')
+    f = maxwellian(vm.cv(), 1.0, [0.1, -0.2, 0.05], 1.0)
+    fin = torch.from_numpy(f[None]).float().to(be.device)
+    q = torch.empty_like(fin)
+    sm.collide(fin, q, project=False)
+    gain_loss = orc.gain_loss(fin[0].double().cpu().numpy())
+    qn = np.linalg.norm(q.double().cpu().numpy())
+    assert qn < 1e-4 * np.linalg.norm(gain_loss[1])
+
+
+def test_q_batch_order_independent(cuda):
+    be, vm, sm, orc = _setup(16, 8, 6, 5, 'single')
+    rng = np.random.default_rng(3)
+    F = np.stack([mixed_maxwellians(vm.cv(), rng) for _ in range(300)])
+    fin = torch.from_numpy(F).float().to(be.device)
+    q = torch.empty_like(fin)
+    sm.collide(fin, q, project=True)
+    q2 = torch.empty_like(fin)
+    perm = torch.randperm(300, generator=torch.Generator().manual_seed(0)).to(be.device)
+    sm.collide(fin[perm].contiguous(), q2, project=True)
+    assert torch.equal(q[perm], q2)
