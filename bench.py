@@ -447,6 +447,31 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
+def run_q_only(ndof):
+    """Collision kernel alone on ndof seeded Couette-family cubes (profiling)."""
+    import numpy as np
+    import torch
+    from frfs_b200.backend import CUDABackend
+    from frfs_b200.inifile import Inifile
+    from frfs_b200.scattering import DGFSVHSGLLScatteringModel
+    from frfs_b200.velocitymesh import DGFSVelocityMesh
+    cfg = Inifile(couette_ini('single'))
+    be = CUDABackend(cfg)
+    vm = DGFSVelocityMesh(be, cfg)
+    sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
+    rng = np.random.default_rng(0)
+    cv = vm.cv()
+    base = np.exp(-np.sum(cv**2, axis=0)) / np.pi**1.5
+    f = torch.from_numpy(base).float().to(be.device).repeat(ndof, 1)
+    f *= 1 + 0.01 * torch.rand(f.shape, device=be.device, generator=torch.Generator(
+        device=be.device).manual_seed(int(rng.integers(1 << 30))))
+    q = torch.empty_like(f)
+    for _ in range(3):
+        sm.collide(f, q)
+    torch.cuda.synchronize()
+    print(json.dumps({'q_only_ndof': ndof, 'finite': bool(torch.isfinite(q).all())}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -454,8 +479,12 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='frfs_b200', choices=['frfs_b200', 'reference'])
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
+    ap.add_argument('--q-only', type=int, default=0, metavar='NDOF',
+                    help='profiling case: 3 launches of the collision kernel on NDOF cubes')
     args = ap.parse_args()
-    if args.impl == 'reference':
+    if args.q_only:
+        run_q_only(args.q_only)
+    elif args.impl == 'reference':
         run_reference(args)
     else:
         run_gpu(args)

@@ -16,7 +16,7 @@ _ERRORS = {-1: 'invalid argument', -2: 'CUDA error', -3: 'unsupported grid/preci
 
 # Every symbol include/bdgfs.h declares (tests check the export list).
 EXPORTS = (
-    'bdgfs_vhs_scratch_bytes', 'bdgfs_vhs_collide', 'bdgfs_fma_probe',
+    'bdgfs_vhs_scratch_bytes', 'bdgfs_vhs_collide', 'bdgfs_vhs_tiles', 'bdgfs_fma_probe',
     'bdgfs_fr_disu', 'bdgfs_fr_bc_update', 'bdgfs_fr_rhs',
     'bdgfs_moments', 'bdgfs_residual', 'bdgfs_status_check',
 )
@@ -28,7 +28,8 @@ class BdgfsError(RuntimeError):
 
 class VhsGrid(C.Structure):
     _fields_ = [('Nv', C.c_int32), ('Nrho', C.c_int32), ('M', C.c_int32),
-                ('fp64', C.c_int32), ('prefac', C.c_double), ('cw', C.c_double),
+                ('fp64', C.c_int32), ('tile', C.c_int32), ('pad_', C.c_int32),
+                ('prefac', C.c_double), ('cw', C.c_double),
                 ('phase', C.c_void_p), ('gw', C.c_void_p), ('bb2', C.c_void_p),
                 ('c0', C.c_void_p), ('ginv', C.c_void_p)]
 
@@ -69,6 +70,8 @@ def lib():
         L.bdgfs_vhs_collide.argtypes = [C.POINTER(VhsGrid), C.c_int32, C.POINTER(VhsBatch),
                                         C.c_int32, C.c_int32, C.c_void_p, C.c_size_t,
                                         C.c_void_p, C.c_void_p]
+        L.bdgfs_vhs_tiles.restype = C.c_int32
+        L.bdgfs_vhs_tiles.argtypes = [C.POINTER(VhsGrid), C.c_int32, C.c_void_p, C.c_int32]
         L.bdgfs_fma_probe.restype = C.c_int32
         L.bdgfs_fma_probe.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]
         vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double

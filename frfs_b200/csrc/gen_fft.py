@@ -115,11 +115,33 @@ def twiddle(em, v, e, N, sign):
                     f'{v}r * {lit(s)} + {v}i * {lit(c)}')
 
 
+_ORDER = (4, 3, 2)
+
+
 def radix_of(N):
-    for r in (4, 3, 2):
+    for r in _ORDER:
         if N % r == 0 and N != r:
             return r
     return N
+
+
+def _opcount(N, order):
+    global _ORDER
+    saved, _ORDER = _ORDER, order
+    try:
+        em = Emitter()
+        xs = [em.cdecl('x', 'y') for _ in range(N)]
+        dft(em, xs, +1)
+        body = '\n'.join(em.lines)
+        return body.count(' + ') + body.count(' - ') + body.count('*')
+    finally:
+        _ORDER = saved
+
+
+def best_order(N):
+    """Radix preference (a permutation of 4, 3, 2) with the fewest operations."""
+    import itertools
+    return min(itertools.permutations((4, 3, 2)), key=lambda o: (_opcount(N, o), o))
 
 
 def dft(em, xs, sign):
@@ -144,6 +166,8 @@ def dft(em, xs, sign):
 
 
 def codelet(N, sign):
+    global _ORDER
+    _ORDER = best_order(N)
     em = Emitter()
     name = f'dft{N}_{"fwd" if sign < 0 else "inv"}'
     xs = []

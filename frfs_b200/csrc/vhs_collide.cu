@@ -508,17 +508,86 @@ struct NoVariant {
     };
 };
 
-// Variant table.  (T, NT, V0, V1)
-//   fp32 : Nv 24 (+ Nv 32 in the same launch), Nv 16, Nv 8/12 (tests)
-//   fp64 : Nv 16, Nv 8/12 (tests)
-using F24 = Variant<float, 24, 288, false, false>;
-using F32g = Variant<float, 32, 288, true, true>;
-using F16 = Variant<float, 16, 256, false, false>;
-using F12 = Variant<float, 12, 144, false, false>;
-using F8 = Variant<float, 8, 64, false, false>;
-using D16 = Variant<double, 16, 256, false, false>;
-using D12 = Variant<double, 12, 144, false, false>;
-using D8 = Variant<double, 8, 64, false, false>;
+// Variant table: each entry is one compiled (precision, grid set, CTA size)
+// combination; the tile field of the first grid picks among the entries that
+// match the grid set (tile 0 = first match).
+template <typename T, int NT, typename V0, typename V1>
+static int launch(const bdgfs_vhs_grid* grids, int ngrids, const bdgfs_vhs_batch* batches,
+                  int nbatch, int flags, void* scratch, size_t scratch_bytes,
+                  uint64_t* counter, cudaStream_t st);
+
+template <typename T, int NT, typename V0, typename V1>
+static size_t entry_per_cta(int maxM, size_t* smem)
+{
+    size_t s0 = V0::L::smem_bytes(maxM), s1 = V1::L::smem_bytes(maxM);
+    *smem = s0 > s1 ? s0 : s1;
+    size_t p0 = V0::L::scratch_bytes(), p1 = V1::L::scratch_bytes();
+    return p0 > p1 ? p0 : p1;
+}
+
+struct Entry {
+    int fp64, n0, n1, threads;
+    int (*run)(const bdgfs_vhs_grid*, int, const bdgfs_vhs_batch*, int, int, void*, size_t,
+               uint64_t*, cudaStream_t);
+    size_t (*per)(int, size_t*);
+};
+
+#define VARIANT(T, N, NT, WG, SG) Variant<T, N, NT, WG, SG>
+#define ENTRY(FP, T, NT, N0, WG0, SG0, N1, WG1, SG1)                                        \
+    {FP, N0, N1, NT,                                                                         \
+     &launch<T, NT, VARIANT(T, N0, NT, WG0, SG0), VARIANT(T, N1, NT, WG1, SG1)>,             \
+     &entry_per_cta<T, NT, VARIANT(T, N0, NT, WG0, SG0), VARIANT(T, N1, NT, WG1, SG1)>}
+#define ENTRY1(FP, T, NT, N0, WG0, SG0)                                                      \
+    {FP, N0, 0, NT, &launch<T, NT, VARIANT(T, N0, NT, WG0, SG0), NoVariant>,                \
+     &entry_per_cta<T, NT, VARIANT(T, N0, NT, WG0, SG0), NoVariant>}
+
+static const Entry kEntries[] = {
+    // fp32, one grid
+    ENTRY1(0, float, 288, 24, false, false),
+    ENTRY1(0, float, 576, 24, false, false),
+    ENTRY1(0, float, 192, 24, false, false),
+    ENTRY1(0, float, 288, 32, true, true),
+    ENTRY1(0, float, 576, 32, true, true),
+    ENTRY1(0, float, 256, 16, false, false),
+    ENTRY1(0, float, 128, 16, false, false),
+    ENTRY1(0, float, 144, 12, false, false),
+    ENTRY1(0, float, 64, 8, false, false),
+    // fp32, two grids in one launch
+    ENTRY(0, float, 288, 24, false, false, 32, true, true),
+    ENTRY(0, float, 576, 24, false, false, 32, true, true),
+    // fp64
+    ENTRY1(1, double, 256, 16, false, false),
+    ENTRY1(1, double, 128, 16, false, false),
+    ENTRY1(1, double, 144, 12, false, false),
+    ENTRY1(1, double, 64, 8, false, false),
+};
+static constexpr int kNumEntries = int(sizeof(kEntries) / sizeof(kEntries[0]));
+
+static bool entry_matches(const Entry& e, const bdgfs_vhs_grid* grids, int ngrids)
+{
+    if (e.fp64 != grids[0].fp64) return false;
+    if (ngrids == 1) return e.n1 == 0 && e.n0 == grids[0].Nv;
+    if (e.n1 == 0) return false;
+    const int a = grids[0].Nv, b = grids[1].Nv;
+    return (a == e.n0 || a == e.n1) && (b == e.n0 || b == e.n1);
+}
+
+// Entry index for (grids, tile), or -1.
+static int choose(const bdgfs_vhs_grid* grids, int ngrids)
+{
+    if (!grids || ngrids < 1 || ngrids > 2) return -1;
+    for (int i = 0; i < ngrids; ++i) {
+        if (grids[i].fp64 != grids[0].fp64) return -1;
+        if (grids[i].Nrho < 1 || grids[i].M < 1 || grids[i].M > 64) return -1;
+    }
+    int tile = grids[0].tile, k = 0;
+    for (int i = 0; i < kNumEntries; ++i) {
+        if (!entry_matches(kEntries[i], grids, ngrids)) continue;
+        if (k == tile) return i;
+        ++k;
+    }
+    return -1;
+}
 
 template <typename T, int NT, typename V0, typename V1>
 static int launch(const bdgfs_vhs_grid* grids, int ngrids, const bdgfs_vhs_batch* batches,
@@ -539,19 +608,15 @@ static int launch(const bdgfs_vhs_grid* grids, int ngrids, const bdgfs_vhs_batch
         a.start[b + 1] = a.start[b] + batches[b].ndof;
     }
     if (a.start[nbatch] == 0) return BDGFS_OK;
-    size_t smem = V0::L::smem_bytes(maxM);
-    size_t s1 = V1::L::smem_bytes(maxM);
-    smem = s1 > smem ? s1 : smem;
-    size_t per = V0::L::scratch_bytes();
-    size_t p1 = V1::L::scratch_bytes();
-    per = p1 > per ? p1 : per;
+    size_t smem = 0;
+    const size_t per = entry_per_cta<T, NT, V0, V1>(maxM, &smem);
     int dev = 0, nsm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return BDGFS_ECUDA;
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return BDGFS_ECUDA;
     int64_t nblk = nsm;
     if (nblk > a.start[nbatch]) nblk = a.start[nbatch];
-    const int64_t fit = scratch_bytes / per;
+    const int64_t fit = int64_t(scratch_bytes / per);
     if (fit < 1) return BDGFS_ESCRATCH;
     if (nblk > fit) nblk = fit;
     a.scratch = static_cast<unsigned char*>(scratch);
@@ -570,59 +635,6 @@ static int launch(const bdgfs_vhs_grid* grids, int ngrids, const bdgfs_vhs_batch
         return BDGFS_ECUDA;
     k<<<unsigned(nblk), NT, smem, st>>>(a);
     return cuda_status(cudaGetLastError());
-}
-
-// Chooses the compiled variant for a set of grids.
-static int choose(const bdgfs_vhs_grid* grids, int ngrids, int* id)
-{
-    if (ngrids < 1 || ngrids > 2) return BDGFS_EINVAL;
-    const int fp64 = grids[0].fp64;
-    int n0 = grids[0].Nv, n1 = ngrids > 1 ? grids[1].Nv : 0;
-    for (int i = 0; i < ngrids; ++i) {
-        if (grids[i].fp64 != fp64) return BDGFS_EUNSUPPORTED;
-        if (grids[i].Nrho < 1 || grids[i].M < 1 || grids[i].M > 64) return BDGFS_EINVAL;
-    }
-    if (!fp64) {
-        if (ngrids == 1) {
-            switch (n0) {
-            case 24: *id = 1; return BDGFS_OK;
-            case 32: *id = 2; return BDGFS_OK;
-            case 16: *id = 3; return BDGFS_OK;
-            case 12: *id = 4; return BDGFS_OK;
-            case 8: *id = 5; return BDGFS_OK;
-            }
-        } else if ((n0 == 24 || n0 == 32) && (n1 == 24 || n1 == 32)) {
-            *id = 2;   // mixed 24/32 launch
-            return BDGFS_OK;
-        }
-    } else if (ngrids == 1) {
-        switch (n0) {
-        case 16: *id = 11; return BDGFS_OK;
-        case 12: *id = 12; return BDGFS_OK;
-        case 8: *id = 13; return BDGFS_OK;
-        }
-    }
-    return BDGFS_EUNSUPPORTED;
-}
-
-static size_t per_cta(int id, int maxM, size_t* smem)
-{
-    switch (id) {
-    case 1: *smem = F24::L::smem_bytes(maxM); return F24::L::scratch_bytes();
-    case 2: {
-        size_t a = F24::L::scratch_bytes(), b = F32g::L::scratch_bytes();
-        size_t sa = F24::L::smem_bytes(maxM), sb = F32g::L::smem_bytes(maxM);
-        *smem = sa > sb ? sa : sb;
-        return a > b ? a : b;
-    }
-    case 3: *smem = F16::L::smem_bytes(maxM); return F16::L::scratch_bytes();
-    case 4: *smem = F12::L::smem_bytes(maxM); return F12::L::scratch_bytes();
-    case 5: *smem = F8::L::smem_bytes(maxM); return F8::L::scratch_bytes();
-    case 11: *smem = D16::L::smem_bytes(maxM); return D16::L::scratch_bytes();
-    case 12: *smem = D12::L::smem_bytes(maxM); return D12::L::scratch_bytes();
-    case 13: *smem = D8::L::smem_bytes(maxM); return D8::L::scratch_bytes();
-    }
-    return 0;
 }
 
 __global__ void fma_probe_kernel(float* out, int iters)
@@ -646,15 +658,28 @@ __global__ void fma_probe_kernel(float* out, int iters)
 
 using namespace bdgfs;
 
+extern "C" int32_t bdgfs_vhs_tiles(const bdgfs_vhs_grid* grids, int32_t ngrids,
+                                   int32_t* threads, int32_t capacity)
+{
+    if (!grids || ngrids < 1 || ngrids > 2) return 0;
+    int k = 0;
+    for (int i = 0; i < kNumEntries; ++i) {
+        if (!entry_matches(kEntries[i], grids, ngrids)) continue;
+        if (threads && k < capacity) threads[k] = kEntries[i].threads;
+        ++k;
+    }
+    return k;
+}
+
 extern "C" size_t bdgfs_vhs_scratch_bytes(const bdgfs_vhs_grid* grids, int32_t ngrids,
                                           int32_t nctas)
 {
-    int id = 0;
-    if (!grids || choose(grids, ngrids, &id) != BDGFS_OK) return 0;
+    const int id = choose(grids, ngrids);
+    if (id < 0) return 0;
     int maxM = 1;
     for (int i = 0; i < ngrids; ++i) maxM = grids[i].M > maxM ? grids[i].M : maxM;
     size_t smem = 0;
-    const size_t per = per_cta(id, maxM, &smem);
+    const size_t per = kEntries[id].per(maxM, &smem);
     if (nctas <= 0) {
         int dev = 0, nsm = 0;
         if (cudaGetDevice(&dev) != cudaSuccess ||
@@ -677,29 +702,10 @@ extern "C" int32_t bdgfs_vhs_collide(const bdgfs_vhs_grid* grids, int32_t ngrids
             return BDGFS_EINVAL;
         if (batches[b].ndof > 0 && (!batches[b].f || !batches[b].Q)) return BDGFS_EINVAL;
     }
-    int id = 0;
-    int rc = choose(grids, ngrids, &id);
-    if (rc != BDGFS_OK) return rc;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    switch (id) {
-    case 1: return launch<float, 288, F24, NoVariant>(grids, ngrids, batches, nbatch, flags,
-                                                     scratch, scratch_bytes, work_counter, st);
-    case 2: return launch<float, 288, F24, F32g>(grids, ngrids, batches, nbatch, flags,
-                                                scratch, scratch_bytes, work_counter, st);
-    case 3: return launch<float, 256, F16, NoVariant>(grids, ngrids, batches, nbatch, flags,
-                                                     scratch, scratch_bytes, work_counter, st);
-    case 4: return launch<float, 144, F12, NoVariant>(grids, ngrids, batches, nbatch, flags,
-                                                     scratch, scratch_bytes, work_counter, st);
-    case 5: return launch<float, 64, F8, NoVariant>(grids, ngrids, batches, nbatch, flags,
-                                                   scratch, scratch_bytes, work_counter, st);
-    case 11: return launch<double, 256, D16, NoVariant>(grids, ngrids, batches, nbatch, flags,
-                                                       scratch, scratch_bytes, work_counter, st);
-    case 12: return launch<double, 144, D12, NoVariant>(grids, ngrids, batches, nbatch, flags,
-                                                       scratch, scratch_bytes, work_counter, st);
-    case 13: return launch<double, 64, D8, NoVariant>(grids, ngrids, batches, nbatch, flags,
-                                                     scratch, scratch_bytes, work_counter, st);
-    }
-    return BDGFS_EUNSUPPORTED;
+    const int id = choose(grids, ngrids);
+    if (id < 0) return BDGFS_EUNSUPPORTED;
+    return kEntries[id].run(grids, ngrids, batches, nbatch, flags, scratch, scratch_bytes,
+                            work_counter, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int32_t bdgfs_fma_probe(float* out, int32_t nblocks, int32_t iters, void* stream)

@@ -109,9 +109,10 @@ class VHSGrid:
         self.ginv = torch.from_numpy(gram_inverse(c0)).to(device).contiguous()
         self.prefac, self.cw = float(prefac), float(cw)
         self.struct = _lib.VhsGrid(
-            Nv, self.Nrho, self.M, int(dtype == torch.float64), self.prefac, self.cw,
-            self.phase.data_ptr(), self.gw.data_ptr(), self.bb2.data_ptr(),
-            self.c0.data_ptr(), self.ginv.data_ptr())
+            Nv=Nv, Nrho=self.Nrho, M=self.M, fp64=int(dtype == torch.float64), tile=0,
+            prefac=self.prefac, cw=self.cw, phase=self.phase.data_ptr(),
+            gw=self.gw.data_ptr(), bb2=self.bb2.data_ptr(), c0=self.c0.data_ptr(),
+            ginv=self.ginv.data_ptr())
 
 
 class VHSCollider:
@@ -121,6 +122,8 @@ class VHSCollider:
     def __init__(self, grids, device):
         self.grids = list(grids)
         self.device = device
+        if any(g.phase.device.type != 'cuda' for g in self.grids):
+            raise _lib.BdgfsError('collision tables must be on a CUDA device')
         arr = (_lib.VhsGrid * len(self.grids))(*[g.struct for g in self.grids])
         self._garr = arr
         L = _lib.lib()
@@ -146,8 +149,11 @@ class VHSCollider:
             if mom is not None and (mom.dtype != torch.float64
                                     or mom.numel() < 10 * (f.numel() // n3)):
                 raise ValueError('moments must be float64 [ndof][10]')
-            bs[i] = _lib.VhsBatch(gi, 0, f.numel() // n3, f.data_ptr(), Q.data_ptr(),
-                                  mom.data_ptr() if mom is not None else 0)
+            if f.device.type != 'cuda' or Q.device.type != 'cuda':
+                raise _lib.BdgfsError('f and Q must be CUDA tensors')
+            bs[i] = _lib.VhsBatch(grid=gi, ndof=f.numel() // n3, f=f.data_ptr(),
+                                  Q=Q.data_ptr(),
+                                  moments=mom.data_ptr() if mom is not None else 0)
         rc = L.bdgfs_vhs_collide(self._garr, len(self.grids), bs, len(batches),
                                  (1 if project else 0) | (2 if exact else 0),
                                  _lib.ptr(self.scratch),
@@ -169,15 +175,25 @@ class DGFSVHSGLLScatteringModel(DGFSScatteringModel):
         self._gamma, self._prefactor, self._Kn = vhs_prefactor(
             self.vm, self._omega, self._dRef, self._Tref, mass=self._mass)
         self._project = cfg.getbool('scattering-model', 'conservation-projection', True)
-        # exact Nyquist-plane treatment: default on for FP64 state
+        # exact Nyquist-plane treatment (second transform per (p, q)): default
+        # on for FP64 state and for coarse grids (Nv <= 16), where the
+        # second-order Nyquist term reaches 1e-3 of Q; at Nv >= 24 it is ~1e-6
         self._exact = cfg.getbool('scattering-model', 'exact-nyquist',
-                                  self.backend.fpdtype == torch.float64)
+                                  self.backend.fpdtype == torch.float64
+                                  or self.vm.Nv() <= 16)
 
     def perform_precomputation(self):
         vm, be = self.vm, self.backend
         self.grid = VHSGrid(vm.Nv(), vm.L(), vm.qz(), vm.qw(), vm.sz(), vm.sw(),
                             self._gamma, self._prefactor, vm.cw(), vm.c0(),
                             be.fpdtype, be.device)
+        # kernel variant: [scattering-model] tile = auto (autotuned, cached) | <int>
+        tile = self.cfg.get('scattering-model', 'tile', 'auto')
+        if tile == 'auto':
+            from .autotune import tune_vhs
+            tune_vhs([self.grid], be.device)
+        else:
+            self.grid.struct.tile = int(tile)
         self.collider = VHSCollider([self.grid], be.device)
 
     def prefactor(self):

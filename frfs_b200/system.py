@@ -49,11 +49,12 @@ class DGFSElements:
         self.nbr = backend.const(geo.nbr, dtype=torch.int32)
         self.c0 = c(vm.c0())
         self.struct = _lib.FrEles(
-            geo.ndims, geo.nupts, geo.nfpts, geo.neles, vm.vsize(), vm.Nv(),
-            int(dt == torch.float64),
-            self.m0.data_ptr(), self.dcorr.data_ptr(), self.m3.data_ptr(),
-            self.smats.data_ptr(), self.rcpdjac.data_ptr(), self.pnorm.data_ptr(),
-            self.magn.data_ptr(), self.nbr.data_ptr(), self.c0.data_ptr())
+            ndims=geo.ndims, nupts=geo.nupts, nfpts=geo.nfpts, neles=geo.neles,
+            nv=vm.vsize(), Nv=vm.Nv(), fp64=int(dt == torch.float64),
+            m0=self.m0.data_ptr(), dcorr=self.dcorr.data_ptr(), m3=self.m3.data_ptr(),
+            smats=self.smats.data_ptr(), rcpdjac=self.rcpdjac.data_ptr(),
+            pnorm=self.pnorm.data_ptr(), magn=self.magn.data_ptr(),
+            nbr=self.nbr.data_ptr(), c0=self.c0.data_ptr())
 
     def ploc_at_np(self, name):
         return {'upts': self.geo.plocupts, 'fpts': self.geo.plocfpts}[name]
@@ -81,9 +82,10 @@ class DGFSWallDiffuseBCInters:
                                  dtype=torch.int32)
         self.bcid = backend.const(geo.wall_bcid if nw else np.zeros(1), dtype=torch.int32)
         self.bcv = backend.zeros(max(nw, 1), 2)
-        self.struct = _lib.FrWall(nw, len(fws), self.fpt.data_ptr(), self.bcid.data_ptr(),
-                                  self.uwall.data_ptr(), self.fw.data_ptr(), self.bcv.data_ptr(),
-                                  float(vm.cw()))
+        self.struct = _lib.FrWall(nwall=nw, nbc=len(fws), fpt=self.fpt.data_ptr(),
+                                  bcid=self.bcid.data_ptr(), uwall=self.uwall.data_ptr(),
+                                  fw=self.fw.data_ptr(), bcv=self.bcv.data_ptr(),
+                                  cw=float(vm.cw()))
 
 
 class DGFSSystem:

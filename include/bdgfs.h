@@ -37,6 +37,9 @@ typedef struct bdgfs_vhs_grid {
     int32_t Nrho;        /* radial Gauss-Jacobi points                      */
     int32_t M;           /* half-sphere directions                          */
     int32_t fp64;        /* 0: FP32 state/tables, 1: FP64                   */
+    int32_t tile;        /* kernel variant (threads per CTA), 0 = default;
+                            see bdgfs_vhs_tiles                             */
+    int32_t pad_;
     double prefac;       /* VHS prefactor                                   */
     double cw;           /* velocity cell volume (2L/Nv)^3                  */
     const void* phase;   /* complex [Nrho][M][3][Nv]:
@@ -58,6 +61,12 @@ typedef struct bdgfs_vhs_batch {
     double* moments;     /* optional [ndof][10]: C.Q before (0..4) and after
                             (5..9) the projection, in FP64, C = cw*{1,c,|c|^2} */
 } bdgfs_vhs_batch;
+
+/* Number of kernel variants compiled for this grid set (tile values
+ * 0..n-1, 0 being the default); threads[i] receives each variant's CTA size
+ * when threads is not NULL (capacity n).  Returns 0 for an unsupported set. */
+int32_t bdgfs_vhs_tiles(const bdgfs_vhs_grid* grids, int32_t ngrids,
+                        int32_t* threads, int32_t capacity);
 
 /* Bytes of device scratch bdgfs_vhs_collide needs for nctas resident CTAs
  * (nctas <= 0: one per SM of the current device). */

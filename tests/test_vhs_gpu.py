@@ -21,15 +21,18 @@ def _setup(Nv, Nrho, M, dev, precision):
     return be, vm, sm, oracle_for(vm)
 
 
-# (Nv, Nrho, M, dev, precision, exact, tol): tolerance is relative L2 of Q
+# (Nv, Nrho, M, dev, precision, exact, tol): tol is the relative L2 error of Q
+# against the FP64 reference algorithm.  FP64: rounding only.  FP32: the
+# stated bound of 1e-3 (FP32 rounding amplified by the gain-loss cancellation
+# of Q; relative to the loss term the error is below 1e-5, checked too).
 CASES = [
     (8, 4, 6, 5, "double", True, 1e-10),
     (12, 6, 6, 5, "double", True, 1e-10),
     (16, 8, 6, 5, "double", True, 1e-10),
-    (8, 4, 6, 5, "single", True, 2e-4),
-    (16, 8, 6, 5, 'single', False, 2e-4),
-    (24, 12, 12, 6, 'single', False, 2e-4),
-    (32, 16, 12, 6, 'single', False, 2e-4),
+    (8, 4, 6, 5, "single", True, 1e-3),
+    (16, 8, 6, 5, 'single', True, 1e-3),
+    (24, 12, 12, 6, 'single', False, 1e-3),
+    (32, 16, 12, 6, 'single', False, 1e-3),
 ]
 
 
@@ -49,6 +52,9 @@ def test_q_parity(cuda, Nv, Nrho, M, dev, prec, exact, tol):
         Qo = orc.Q(Fi)
         err = rel_l2(Qg[i], Qo)
         assert err < tol, (i, err)
+        loss = orc.gain_loss(Fi)[1]
+        assert np.linalg.norm(Qg[i] - Qo) < (1e-5 if prec == 'single' else 1e-12) * \
+            np.linalg.norm(loss)
 
 
 def test_q_conservation_projection(cuda):
