@@ -17,6 +17,7 @@ _ERRORS = {-1: 'invalid argument', -2: 'CUDA error', -3: 'unsupported grid/preci
 # Every symbol include/bdgfs.h declares (tests check the export list).
 EXPORTS = (
     'bdgfs_vhs_scratch_bytes', 'bdgfs_vhs_collide', 'bdgfs_vhs_tiles', 'bdgfs_fma_probe',
+    'bdgfs_vhs_collide_static',
     'bdgfs_fr_disu', 'bdgfs_fr_bc_update', 'bdgfs_fr_rhs',
     'bdgfs_moments', 'bdgfs_residual', 'bdgfs_status_check',
 )
@@ -70,6 +71,10 @@ def lib():
         L.bdgfs_vhs_collide.argtypes = [C.POINTER(VhsGrid), C.c_int32, C.POINTER(VhsBatch),
                                         C.c_int32, C.c_int32, C.c_void_p, C.c_size_t,
                                         C.c_void_p, C.c_void_p]
+        L.bdgfs_vhs_collide_static.restype = C.c_int32
+        L.bdgfs_vhs_collide_static.argtypes = [C.POINTER(VhsGrid), C.c_int32,
+                                               C.POINTER(VhsBatch), C.c_int32, C.c_int32,
+                                               C.c_void_p]
         L.bdgfs_vhs_tiles.restype = C.c_int32
         L.bdgfs_vhs_tiles.argtypes = [C.POINTER(VhsGrid), C.c_int32, C.c_void_p, C.c_int32]
         L.bdgfs_fma_probe.restype = C.c_int32

@@ -708,6 +708,70 @@ extern "C" int32_t bdgfs_vhs_collide(const bdgfs_vhs_grid* grids, int32_t ngrids
                             work_counter, static_cast<cudaStream_t>(stream));
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free entry point.
+//
+// Some callers cannot allocate device memory at the point where they need the
+// collision operator: a host application whose device memory is owned by
+// another allocator (a caching allocator or a fixed arena handed out at
+// start-up), a time loop that must not allocate once it is running, or a
+// plugin whose host only passes it input and output pointers.  For them
+// bdgfs_vhs_collide_static takes its scratch and its work counter from one
+// file-scope device array instead of a caller-provided buffer.
+//
+// Layout of the array: bytes [0, 256) hold the 64-bit work counter, the rest
+// is per-CTA scratch.  Its size is fixed (BDGFS_STATIC_SCRATCH_BYTES); every
+// GPU that loads this library holds it until the process exits.  When one
+// CTA's scratch for the given grids does not fit, the call fails with
+// BDGFS_ESCRATCH; when fewer CTAs than SMs fit, fewer run (slower, same
+// result).  Calls share the array and it keeps the last call's contents:
+// the counter is cleared (stream-ordered) on every call and every other
+// scratch word is written before it is read, but calls that overlap on the
+// GPU (different streams, or different host threads) race on it.
+#define BDGFS_STATIC_SCRATCH_BYTES (size_t(16) << 20)
+static __device__ __align__(256) unsigned char g_vhs_static_scratch[BDGFS_STATIC_SCRATCH_BYTES];
+
+// Device address of the array, looked up once per device (the array's name
+// is only a host-side stand-in in host code).
+static void* static_scratch_addr(int dev)
+{
+    constexpr int kMaxDev = 64;
+    static void* addr[kMaxDev] = {};
+    if (dev < 0 || dev >= kMaxDev) return nullptr;
+    if (!addr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_vhs_static_scratch) != cudaSuccess) return nullptr;
+        addr[dev] = p;
+    }
+    return addr[dev];
+}
+
+extern "C" int32_t bdgfs_vhs_collide_static(const bdgfs_vhs_grid* grids, int32_t ngrids,
+                                            const bdgfs_vhs_batch* batches, int32_t nbatch,
+                                            int32_t flags, void* stream)
+{
+    if (!grids || !batches || nbatch < 1 || nbatch > 4) return BDGFS_EINVAL;
+    for (int b = 0; b < nbatch; ++b) {
+        if (batches[b].grid < 0 || batches[b].grid >= ngrids || batches[b].ndof < 0)
+            return BDGFS_EINVAL;
+        if (batches[b].ndof > 0 && (!batches[b].f || !batches[b].Q)) return BDGFS_EINVAL;
+    }
+    const int id = choose(grids, ngrids);
+    if (id < 0) return BDGFS_EUNSUPPORTED;
+    int maxM = 1;
+    for (int i = 0; i < ngrids; ++i) maxM = grids[i].M > maxM ? grids[i].M : maxM;
+    size_t smem = 0;
+    const size_t per = kEntries[id].per(maxM, &smem);
+    const size_t capacity = BDGFS_STATIC_SCRATCH_BYTES - 256;
+    if (per > capacity) return BDGFS_ESCRATCH;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return BDGFS_ECUDA;
+    unsigned char* base = static_cast<unsigned char*>(static_scratch_addr(dev));
+    if (!base) return BDGFS_ECUDA;
+    return kEntries[id].run(grids, ngrids, batches, nbatch, flags, base + 256, capacity,
+                            reinterpret_cast<uint64_t*>(base), static_cast<cudaStream_t>(stream));
+}
+
 extern "C" int32_t bdgfs_fma_probe(float* out, int32_t nblocks, int32_t iters, void* stream)
 {
     if (!out || nblocks < 1 || iters < 1) return BDGFS_EINVAL;

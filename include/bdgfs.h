@@ -90,6 +90,18 @@ int32_t bdgfs_vhs_collide(const bdgfs_vhs_grid* grids, int32_t ngrids,
                           int32_t flags, void* scratch, size_t scratch_bytes,
                           uint64_t* work_counter, void* stream);
 
+/* Same as bdgfs_vhs_collide, for callers that cannot allocate device memory
+ * (their device memory belongs to another allocator or a fixed arena, or they
+ * must not allocate once running): scratch and work counter come from one
+ * file-scope device array of 16 MiB held by every GPU that loads the library.
+ * No counterpart in the reference.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  Returns BDGFS_ESCRATCH if one CTA's scratch for these
+ * grids exceeds the array; calls that overlap on the GPU race on the array. */
+int32_t bdgfs_vhs_collide_static(const bdgfs_vhs_grid* grids, int32_t ngrids,
+                                 const bdgfs_vhs_batch* batches, int32_t nbatch,
+                                 int32_t flags, void* stream);
+
 /* Measured FP32 FMA throughput probe: runs iters dependent-free FMA chains
  * per thread on nblocks x 256 threads and writes a checksum to out[0]. */
 int32_t bdgfs_fma_probe(float* out, int32_t nblocks, int32_t iters,
