@@ -297,6 +297,138 @@ def config_block(n):
             'l2': 'flushed before every timed step (256 MiB write); step working set 452 MB > L2'}
 
 
+# ---------------------------------------------------------------- other configs
+BATCHED = dict(n24=24576, n32=8192, Nrho=16, M=12, dev=6, omega=0.81, mass2=2.0)
+SMALL64 = dict(Nv=16, Nrho=8, M=6, dev=5, omega=0.5, order=2, nx=4, ny=4, dt=1e-3)
+
+
+def batched_q(flush, reps=3):
+    """Two species on uneven grids (24^3 and 32^3, mass ratio 2) in one
+    persistent launch captured in a CUDA graph; returns Q evals/s and the
+    FP32 arrays for the error check."""
+    import numpy as np
+    import torch
+    from frfs_b200.backend import CUDABackend
+    from frfs_b200.inifile import Inifile
+    from frfs_b200.scattering import VHSGrid, VHSCollider, vhs_prefactor
+    from frfs_b200.velocitymesh import DGFSVelocityMesh
+    from frfs_b200.autotune import tune_vhs
+    w = BATCHED
+    grids, fs = [], []
+    gen = torch.Generator(device='cuda').manual_seed(7)
+    for Nv, ndof, mass in ((24, w['n24'], 1.0), (32, w['n32'], w['mass2'])):
+        cfg = Inifile(couette_ini('single', dict(WORK, Nv=Nv, Nrho=w['Nrho'], M=w['M'])))
+        be = CUDABackend(cfg)
+        vm = DGFSVelocityMesh(be, cfg)
+        gam, pref, _ = vhs_prefactor(vm, w['omega'], 4.17e-10, NONDIM['T0'], mass=mass)
+        g = VHSGrid(Nv, vm.L(), vm.qz(), vm.qw(), vm.sz(), vm.sw(), gam, pref, vm.cw(), vm.c0(),
+                    torch.float32, be.device)
+        grids.append(g)
+        # seeded sums of 1-3 Maxwellians (n ~ U(0.2,2), |u| < 1, T ~ U(0.5,2)) + 1% noise,
+        # generated on the device from per-distribution parameters
+        c0 = torch.as_tensor(vm.c0(), dtype=torch.float32, device=be.device)
+        cx, cy, cz = c0.view(-1, 1, 1), c0.view(1, -1, 1), c0.view(1, 1, -1)
+        f = torch.zeros(ndof, Nv, Nv, Nv, device=be.device)
+        k = torch.randint(1, 4, (ndof,), generator=gen, device=be.device)
+        for j in range(3):
+            n = 0.2 + 1.8 * torch.rand(ndof, generator=gen, device=be.device)
+            d = torch.randn(ndof, 3, generator=gen, device=be.device)
+            d = d / d.norm(dim=1, keepdim=True) * torch.rand(ndof, 1, generator=gen,
+                                                            device=be.device).pow(1 / 3)
+            T = 0.5 + 1.5 * torch.rand(ndof, generator=gen, device=be.device)
+            on = (k > j).float() * n / (torch.pi * T)**1.5
+            for i0 in range(0, ndof, 2048):
+                sl = slice(i0, i0 + 2048)
+                r2 = ((cx[None] - d[sl, 0, None, None, None])**2
+                      + (cy[None] - d[sl, 1, None, None, None])**2
+                      + (cz[None] - d[sl, 2, None, None, None])**2)
+                f[sl] += on[sl, None, None, None] * torch.exp(-r2 / T[sl, None, None, None])
+        f *= 1 + 0.01 * (2 * torch.rand(f.shape, generator=gen, device=be.device) - 1)
+        fs.append(f.reshape(ndof, -1).contiguous())
+    tune_vhs(grids, grids[0].phase.device)
+    col = VHSCollider(grids, grids[0].phase.device)
+    qs = [torch.empty_like(f) for f in fs]
+    batches = [(1, fs[1], qs[1], None), (0, fs[0], qs[0], None)]   # expensive grid first
+    col(batches)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        col(batches)
+    torch.cuda.current_stream().wait_stream(s)
+    with torch.cuda.graph(g):
+        col(batches)
+    st = torch.cuda.current_stream()
+    ms = []
+    for _ in range(reps):
+        flush.fill_(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        g.replay()
+        b.record(st)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    t = sum(ms) / len(ms)
+    ndof = w['n24'] + w['n32']
+    return {'workload': 'two species, 24576 x 24^3 + 8192 x 32^3, mass ratio 2, Nrho=16, M=12, '
+                        'one persistent launch in a CUDA graph, FP32 + FP64 projection',
+            'q_evals_per_s': ndof / (t * 1e-3), 'ms_per_launch': t,
+            'tiles': [int(x.struct.tile) for x in grids]}, (grids, fs, qs)
+
+
+def small_fp64(flush, steps=20):
+    """Plain FP64 method: 4x4 periodic quads P2 (144 DOFs), Nv=16, hard
+    spheres, Nrho=8, M=6, two seeded Maxwellians per DOF, SSP-RK2 dt=1e-3."""
+    import numpy as np
+    import torch
+    from frfs_b200.backend import CUDABackend
+    from frfs_b200.inifile import Inifile
+    from frfs_b200.integrators import get_integrator
+    from frfs_b200.mesh import StructuredMesh
+    from frfs_b200.system import DGFSSystem
+    w = SMALL64
+    ini = couette_ini('double', dict(WORK, Nv=w['Nv'], Nrho=w['Nrho'], M=w['M'], dev=w['dev'],
+                                     omega=w['omega'], order=w['order'], dt=w['dt']))
+    cfg = Inifile(ini)
+    be = CUDABackend(cfg)
+    mesh = StructuredMesh((w['nx'], w['ny']), (0.0, 0.0), (1.0, 1.0), periodic='xy')
+    s = DGFSSystem(be, mesh, cfg, nreg=3)
+    rng = np.random.default_rng(2)
+    cv = s.vm.cv()
+    u = s.eles_scal_upts_inb_full[0]
+    F = np.empty(u.shape)
+    for e in range(u.shape[0]):
+        for j in range(u.shape[1]):
+            f = 0.0
+            for _ in range(2):
+                d = rng.normal(size=3)
+                d = d / np.linalg.norm(d) * 0.5 * rng.uniform()**(1 / 3)
+                T = rng.uniform(0.7, 1.3)
+                f = f + rng.uniform(0.5, 1.5) / (np.pi * T)**1.5 * np.exp(
+                    -np.sum((cv - d[:, None])**2, axis=0) / T)
+            F[e, j] = f
+    u.copy_(torch.from_numpy(F))
+    integ = get_integrator(be, s, cfg)
+    for _ in range(3):
+        integ.step(0.0, w['dt'])
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    tot = 0.0
+    for _ in range(steps):
+        flush.fill_(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        integ.step(0.0, w['dt'])
+        b.record(st)
+        torch.cuda.synchronize()
+        tot += a.elapsed_time(b)
+    return {'workload': '4x4 periodic quads P2 (144 DOFs), Nv=16^3 on [-5,5]^3, hard sphere, '
+                        'Nrho=8, M=6, SSP-RK2 dt=1e-3, FP64 (exact-Nyquist collision operator)',
+            'dg_steps_per_s': steps / (tot * 1e-3), 'ms_per_step': tot / steps,
+            'dtype': 'f64'}
+
+
 # ---------------------------------------------------------------- GPU leg
 def run_gpu(args):
     import numpy as np
@@ -419,6 +551,12 @@ def run_gpu(args):
                           f'3+3*M*Nrho FP64 FFTs each, {tq:.1f} s on {ncores} processes) + FR '
                           f'operator on the full mesh ({tfr:.2f} s), extrapolated to one step')}
         pool.shutdown()
+    # other measured configurations of the metric (rank 0, single GPU)
+    extra = {}
+    if ws == 1 and not args.no_extra:
+        extra['plain_fp64_small'] = small_fp64(flush)
+        bq, _ = batched_q(flush)
+        extra['batched_q'] = bq
     # gpu launches per step: 2 x (collide + disu + bc_update + rhs)
     launches = 8 * args.steps
     line = {
@@ -439,6 +577,7 @@ def run_gpu(args):
         'gpu_launches': launches,
         'clocks': clocks,
         'cpu_baseline': cpu,
+        **extra,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -479,6 +618,8 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='frfs_b200', choices=['frfs_b200', 'reference'])
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
+    ap.add_argument('--no-extra', action='store_true',
+                    help='skip the FP64 small and batched-collision measurements')
     ap.add_argument('--q-only', type=int, default=0, metavar='NDOF',
                     help='profiling case: 3 launches of the collision kernel on NDOF cubes')
     args = ap.parse_args()

@@ -20,6 +20,7 @@ EXPORTS = (
     'bdgfs_vhs_collide_static',
     'bdgfs_fr_disu', 'bdgfs_fr_bc_update', 'bdgfs_fr_rhs',
     'bdgfs_moments', 'bdgfs_residual', 'bdgfs_status_check',
+    'bdgfs_gemm', 'bdgfs_colsum', 'bdgfs_adamw',
 )
 
 
@@ -55,6 +56,18 @@ class FrWall(C.Structure):
                 ('fw', C.c_void_p), ('bcv', C.c_void_p), ('cw', C.c_double)]
 
 
+class GemmArgs(C.Structure):
+    _fields_ = [('M', C.c_int64), ('N', C.c_int64), ('K', C.c_int64),
+                ('A', C.c_void_p), ('sam', C.c_int64), ('sak', C.c_int64),
+                ('B', C.c_void_p), ('sbn', C.c_int64), ('sbk', C.c_int64),
+                ('a_bf16', C.c_int32), ('b_bf16', C.c_int32),
+                ('alpha', C.c_float), ('beta', C.c_float),
+                ('bias', C.c_void_p), ('act', C.c_int32), ('engine', C.c_int32),
+                ('cf32', C.c_void_p), ('cbf16', C.c_void_p), ('ldc', C.c_int64),
+                ('zout', C.c_void_p), ('zin', C.c_void_p), ('ldz', C.c_int64),
+                ('status', C.c_void_p), ('pad_', C.c_int32)]
+
+
 _lib = None
 
 
@@ -87,6 +100,10 @@ def lib():
             'bdgfs_moments': [vp, i64, i32, i32, vp, dbl, vp, vp],
             'bdgfs_residual': [vp, vp, i64, i32, vp, vp],
             'bdgfs_status_check': [vp, i64, i32, vp, vp],
+            'bdgfs_gemm': [C.c_void_p, vp],
+            'bdgfs_colsum': [vp, i64, i64, vp, vp],
+            'bdgfs_adamw': [vp, vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float,
+                            C.c_float, C.c_float, i64, vp],
         }
         for name, at in sig.items():
             fn = getattr(L, name)

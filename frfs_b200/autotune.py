@@ -58,7 +58,10 @@ def tune_vhs(grids, device, reps=3, force=False, record=None):
     key = _key(grids, props.multi_processor_count)
     cache = _load()
     if key in cache and not force:
-        return int(cache[key]['tile'])
+        tile = int(cache[key]['tile'])
+        for g in grids:
+            g.struct.tile = tile
+        return tile
     threads = variants(grids)
     if len(threads) <= 1:
         return 0
@@ -97,7 +100,7 @@ def tune_vhs(grids, device, reps=3, force=False, record=None):
     for g in grids:
         g.struct.tile = tile
     cache[key] = {'tile': tile, 'threads': threads[tile],
-                  'ms': {str(threads[i]): times[i] for i in range(len(times))}}
+                  'ms': {f'tile{i}-{threads[i]}thr': times[i] for i in range(len(times))}}
     _store(cache)
     if record is not None:
         record.update(cache[key])

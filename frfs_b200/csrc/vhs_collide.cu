@@ -77,7 +77,10 @@ struct QLayout {
     }
 };
 
-template <typename T, int N, int NT, bool WG, bool SG>
+// GR > 0: the z- and y-passes of each inverse transform are done by GR
+// groups of NT/GR threads, group g owning the kx-slabs [g*N/GR, (g+1)*N/GR);
+// the two passes then only synchronise within the group (named barrier).
+template <typename T, int N, int NT, bool WG, bool SG, int GR = 0>
 __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
                             T* __restrict__ Qout, double* mom, int flags,
                             unsigned char* smem, unsigned char* scratch)
@@ -120,6 +123,30 @@ __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
     (void)Sg;
 
     auto widx = [](int i, int j, int k) { return (i * N + j) * WS + k; };
+    // pencil mapping of the first two inverse passes (kx-major pencils)
+    static_assert(GR == 0 || (N % GR == 0 && NT % GR == 0 && (NT / GR) % 32 == 0
+                              && ((N / GR) * N) % (NT / GR) == 0), "bad slab groups");
+    constexpr int TG = GR ? NT / GR : NT;
+    constexpr int P12 = GR ? (N / GR) * N / TG : (NP + NT - 1) / NT;
+    const int grp = GR ? tid / TG : 0, lt = GR ? tid % TG : tid;
+    auto pencil12 = [&](int r, int& a, int& b) -> bool {
+        const int pl = lt + r * TG;
+        if (GR) {
+            a = grp * (N / (GR ? GR : 1)) + pl / N;
+            b = pl % N;
+            return true;
+        }
+        if (pl >= NP) return false;
+        a = pl / N;
+        b = pl % N;
+        return true;
+    };
+    auto sync12 = [&]() {
+        if constexpr (GR > 0)
+            asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(TG) : "memory");
+        else
+            __syncthreads();
+    };
     const T inv_n = T(1) / T(L::n);
 
     // ---- Fh = FFT(f) / n, stored for kx <= N/2 ----
@@ -175,8 +202,10 @@ __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
             const int q = qt / ntr, tr = qt % ntr;   // tr = 1: Nyquist term
             const cpx<T>* ep = ph + q * 3 * N;
             // ---- pass 1: spectrum * m_pq, inverse along z ----
-            for (int pid = tid; pid < NP; pid += NT) {
-                const int kx = pid / N, ky = pid % N;
+#pragma unroll 1
+            for (int r = 0; r < P12; ++r) {
+                int kx, ky;
+                if (!pencil12(r, kx, ky)) break;
                 const cpx<T> Ex = ep[kx], Ey = ep[N + ky];
                 const cpx<T> Pxy = cmul(Ex, Ey);
                 const bool direct = kx < NH;
@@ -236,10 +265,12 @@ __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
 #pragma unroll
                 for (int z = 0; z < N; ++z) W[widx(kx, ky, z)] = v[z];
             }
-            __syncthreads();
+            sync12();
             // ---- pass 2: inverse along y ----
-            for (int pid = tid; pid < NP; pid += NT) {
-                const int kx = pid / N, z = pid % N;
+#pragma unroll 1
+            for (int r = 0; r < P12; ++r) {
+                int kx, z;
+                if (!pencil12(r, kx, z)) break;
                 cpx<T> v[N];
 #pragma unroll
                 for (int j = 0; j < N; ++j) v[j] = W[widx(kx, j, z)];
@@ -456,11 +487,12 @@ struct KArgs {
     unsigned long long* counter;
 };
 
-template <typename T, int N, int NT, bool WG, bool SG>
+template <typename T, int N, int NT, bool WG, bool SG, int GR = 0>
 struct Variant {
     using L = QLayout<T, N, NT, WG, SG>;
     static constexpr int n = N;
     static constexpr bool wg = WG, sg = SG;
+    static constexpr int gr = GR;
 };
 
 // Kernel over a set of grid variants; a distribution of a batch on a grid
@@ -488,11 +520,11 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
         T* Q = static_cast<T*>(bt.Q) + dof * n3;
         double* mom = bt.moments ? bt.moments + dof * 10 : nullptr;
         if (g.Nv == V0::n) {
-            collide_one<T, V0::n, NT, V0::wg, V0::sg>(
+            collide_one<T, V0::n, NT, V0::wg, V0::sg, V0::gr>(
                 g, f, Q, mom, a.flags, smem, scratch);
         } else if constexpr (V1::n > 0) {
             if (g.Nv == V1::n)
-                collide_one<T, V1::n, NT, V1::wg, V1::sg>(
+                collide_one<T, V1::n, NT, V1::wg, V1::sg, V1::gr>(
                     g, f, Q, mom, a.flags, smem, scratch);
         }
     }
@@ -501,6 +533,7 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
 struct NoVariant {
     static constexpr int n = 0;
     static constexpr bool wg = false, sg = false;
+    static constexpr int gr = 0;
     struct L {
         static constexpr int WS = 0;
         static size_t smem_bytes(int) { return 0; }
@@ -533,6 +566,10 @@ struct Entry {
 };
 
 #define VARIANT(T, N, NT, WG, SG) Variant<T, N, NT, WG, SG>
+#define VARIANTG(T, N, NT, GR) Variant<T, N, NT, false, false, GR>
+#define ENTRYG(FP, T, NT, N0, GR)                                                            \
+    {FP, N0, 0, NT, &launch<T, NT, VARIANTG(T, N0, NT, GR), NoVariant>,                     \
+     &entry_per_cta<T, NT, VARIANTG(T, N0, NT, GR), NoVariant>}
 #define ENTRY(FP, T, NT, N0, WG0, SG0, N1, WG1, SG1)                                        \
     {FP, N0, N1, NT,                                                                         \
      &launch<T, NT, VARIANT(T, N0, NT, WG0, SG0), VARIANT(T, N1, NT, WG1, SG1)>,             \
@@ -546,10 +583,13 @@ static const Entry kEntries[] = {
     ENTRY1(0, float, 288, 24, false, false),
     ENTRY1(0, float, 576, 24, false, false),
     ENTRY1(0, float, 192, 24, false, false),
+    ENTRYG(0, float, 288, 24, 3),
+    ENTRYG(0, float, 576, 24, 6),
     ENTRY1(0, float, 288, 32, true, true),
     ENTRY1(0, float, 576, 32, true, true),
     ENTRY1(0, float, 256, 16, false, false),
     ENTRY1(0, float, 128, 16, false, false),
+    ENTRYG(0, float, 256, 16, 2),
     ENTRY1(0, float, 144, 12, false, false),
     ENTRY1(0, float, 64, 8, false, false),
     // fp32, two grids in one launch
@@ -558,6 +598,7 @@ static const Entry kEntries[] = {
     // fp64
     ENTRY1(1, double, 256, 16, false, false),
     ENTRY1(1, double, 128, 16, false, false),
+    ENTRYG(1, double, 256, 16, 2),
     ENTRY1(1, double, 144, 12, false, false),
     ENTRY1(1, double, 64, 8, false, false),
 };

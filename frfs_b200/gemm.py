@@ -1,0 +1,66 @@
+"""Host wrappers of the surrogate's GEMMs (``bdgfs_gemm``): tensor-core
+(tcgen05, bf16 operands, FP32 accumulation) and FP32 CUDA-core engines."""
+import ctypes as C
+
+import torch
+
+from . import _lib
+
+ACT_NONE, ACT_GELU, ACT_GELU_GRAD = 0, 1, 2
+
+
+def _operand(t, trans):
+    """(pointer, row stride, k stride, is_bf16) of a 2-D operand viewed as
+    [rows][K] (trans=False) or as the transpose of a [K][rows] tensor."""
+    if t.dim() != 2:
+        raise ValueError('GEMM operands are 2-D')
+    if t.dtype not in (torch.float32, torch.bfloat16):
+        raise TypeError('GEMM operands are float32 or bfloat16')
+    s0, s1 = t.stride()
+    return (t.data_ptr(), s1, s0, t.dtype == torch.bfloat16) if trans else \
+        (t.data_ptr(), s0, s1, t.dtype == torch.bfloat16)
+
+
+def gemm(a, b, *, ta=False, tb=False, alpha=1.0, beta=0.0, bias=None, act=ACT_NONE,
+         out=None, out_bf16=None, zout=None, zin=None, engine=0, status=None, stream=None):
+    """out[m][n] = alpha * sum_k A(m,k) B(n,k) (+ beta*out) (+ bias) -> act.
+    A = a (M x K) or a^T if ta; B = b (N x K) or b^T if tb."""
+    pa, sam, sak, abf = _operand(a, ta)
+    pb, sbn, sbk, bbf = _operand(b, tb)
+    M = a.shape[1] if ta else a.shape[0]
+    K = a.shape[0] if ta else a.shape[1]
+    N = b.shape[1] if tb else b.shape[0]
+    if (b.shape[0] if tb else b.shape[1]) != K:
+        raise ValueError('inner dimensions differ')
+    for t in (out, out_bf16, zout, zin, bias):
+        if t is not None and (not t.is_cuda or not t.is_contiguous()):
+            raise ValueError('outputs/bias must be contiguous CUDA tensors')
+    ldc = N
+    if out is not None and out.shape != (M, N):
+        raise ValueError('out shape')
+    if out_bf16 is not None and out_bf16.shape != (M, N):
+        raise ValueError('out_bf16 shape')
+    args = _lib.GemmArgs(M=M, N=N, K=K, A=pa, sam=sam, sak=sak, B=pb, sbn=sbn, sbk=sbk,
+                         a_bf16=int(abf), b_bf16=int(bbf), alpha=float(alpha), beta=float(beta),
+                         bias=bias.data_ptr() if bias is not None else 0, act=int(act),
+                         engine=int(engine),
+                         cf32=out.data_ptr() if out is not None else 0,
+                         cbf16=out_bf16.data_ptr() if out_bf16 is not None else 0, ldc=ldc,
+                         zout=zout.data_ptr() if zout is not None else 0,
+                         zin=zin.data_ptr() if zin is not None else 0, ldz=N,
+                         status=status.data_ptr() if status is not None else 0)
+    _lib.check(_lib.lib().bdgfs_gemm(C.byref(args), _lib.stream_ptr(stream)), 'bdgfs_gemm')
+    return out if out is not None else out_bf16
+
+
+def colsum(x, out):
+    _lib.check(_lib.lib().bdgfs_colsum(x.data_ptr(), x.shape[0], x.shape[1], out.data_ptr(),
+                                       _lib.stream_ptr()), 'bdgfs_colsum')
+    return out
+
+
+def adamw(p, g, m1, m2, p_bf16, step, lr=3e-4, betas=(0.9, 0.999), eps=1e-8, wd=0.01):
+    _lib.check(_lib.lib().bdgfs_adamw(p.data_ptr(), g.data_ptr(), m1.data_ptr(), m2.data_ptr(),
+                                      p_bf16.data_ptr() if p_bf16 is not None else None,
+                                      p.numel(), lr, betas[0], betas[1], eps, wd, int(step),
+                                      _lib.stream_ptr()), 'bdgfs_adamw')

@@ -191,7 +191,7 @@ class DGFSVHSGLLScatteringModel(DGFSScatteringModel):
         tile = self.cfg.get('scattering-model', 'tile', 'auto')
         if tile == 'auto':
             from .autotune import tune_vhs
-            tune_vhs([self.grid], be.device)
+            self.grid.struct.tile = tune_vhs([self.grid], be.device)
         else:
             self.grid.struct.tile = int(tile)
         self.collider = VHSCollider([self.grid], be.device)

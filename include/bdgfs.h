@@ -182,6 +182,52 @@ int32_t bdgfs_residual(const void* a, const void* b, int64_t n, int32_t fp64,
 int32_t bdgfs_status_check(const void* a, int64_t n, int32_t fp64,
                            int32_t* status, void* stream);
 
+/* ------------------------------------------------------------------------
+ * GEMMs of the learned collision-operator surrogate (no counterpart in the
+ * reference, whose collision operator is spectral only)
+ * ---------------------------------------------------------------------- */
+
+/* C[m][n] = alpha * sum_k A(m,k) B(n,k) [+ beta*C] [+ bias[n]] -> act,
+ * A(m,k) = A[m*sam + k*sak], B(n,k) = B[n*sbn + k*sbk].
+ * engine 0: tcgen05 tensor cores, bf16 operands (float sources are rounded
+ *           to bf16), FP32 accumulation, beta must be 0;
+ * engine 1: FP32 CUDA cores (float sources only, no bias/act).
+ * act 0: none; 1: GELU (erf form); 2: multiply by GELU'(zin[m][n]).
+ * zout (optional, float, leading dim ldz) receives the pre-activation. */
+typedef struct bdgfs_gemm_args {
+    int64_t M, N, K;
+    const void* A;
+    int64_t sam, sak;
+    const void* B;
+    int64_t sbn, sbk;
+    int32_t a_bf16, b_bf16;
+    float alpha, beta;
+    const void* bias;    /* float [N] or NULL                            */
+    int32_t act;
+    int32_t engine;
+    void* cf32;          /* float output or NULL                         */
+    void* cbf16;         /* bf16 output or NULL                          */
+    int64_t ldc;
+    void* zout;          /* float pre-activation output or NULL          */
+    const void* zin;     /* float pre-activation input (act == 2)        */
+    int64_t ldz;
+    int32_t* status;     /* receives BDGFS_ETIMEOUT if a wait expired    */
+    int32_t pad_;
+} bdgfs_gemm_args;
+
+int32_t bdgfs_gemm(const bdgfs_gemm_args* args, void* stream);
+
+/* out[n] = sum_m X[m][n] (bias gradients). */
+int32_t bdgfs_colsum(const float* X, int64_t M, int64_t N, float* out,
+                     void* stream);
+
+/* AdamW step on FP32 master weights p (n values) with moments m1, m2;
+ * writes a bf16 copy to p_bf16 when not NULL.  step counts from 1. */
+int32_t bdgfs_adamw(float* p, const float* grad, float* m1, float* m2,
+                    void* p_bf16, int64_t n, float lr, float beta1,
+                    float beta2, float eps, float weight_decay, int64_t step,
+                    void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -34,6 +34,7 @@ STRUCTS = {
     'bdgfs_vhs_batch': _lib.VhsBatch,
     'bdgfs_fr_eles': _lib.FrEles,
     'bdgfs_fr_walls': _lib.FrWall,
+    'bdgfs_gemm_args': _lib.GemmArgs,
 }
 
 

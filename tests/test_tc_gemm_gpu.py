@@ -1,0 +1,68 @@
+"""tcgen05 tensor-core GEMM and FP32 GEMM against a torch FP32 reference of
+the same operation (operands rounded to bf16 for the tensor-core engine)."""
+import math
+
+import pytest
+import torch
+
+from frfs_b200.gemm import ACT_GELU, ACT_GELU_GRAD, gemm
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref(A, B, alpha=1.0, bias=None):
+    r = alpha * (A.double() @ B.double().T)
+    if bias is not None:
+        r = r + bias.double()
+    return r
+
+
+def _rel(x, y):
+    return float((x.double() - y.double()).norm() / y.double().norm())
+
+
+@pytest.mark.parametrize('M,N,K', [(128, 128, 64), (64, 40, 16), (300, 200, 130),
+                                   (1024, 1024, 512), (257, 513, 1000)])
+def test_tc_gemm_matches_fp32_reference(cuda, M, N, K):
+    g = torch.Generator(device=cuda).manual_seed(M + N + K)
+    A = torch.randn(M, K, device=cuda, generator=g).bfloat16()
+    B = torch.randn(N, K, device=cuda, generator=g).bfloat16()
+    C = torch.empty(M, N, device=cuda)
+    gemm(A, B, out=C)
+    torch.cuda.synchronize()
+    assert _rel(C, _ref(A, B)) < 1e-5
+
+
+def test_tc_gemm_strided_float_operands_bias_gelu(cuda):
+    g = torch.Generator(device=cuda).manual_seed(5)
+    At = torch.randn(96, 200, device=cuda, generator=g)       # A = At^T  (200 x 96)
+    Bt = torch.randn(96, 150, device=cuda, generator=g)       # B = Bt^T  (150 x 96)
+    bias = torch.randn(150, device=cuda, generator=g)
+    C = torch.empty(200, 150, device=cuda)
+    Z = torch.empty(200, 150, device=cuda)
+    Cb = torch.empty(200, 150, device=cuda, dtype=torch.bfloat16)
+    gemm(At, Bt, ta=True, tb=True, alpha=0.5, bias=bias, act=ACT_GELU, out=C, out_bf16=Cb, zout=Z)
+    torch.cuda.synchronize()
+    Ar, Br = At.bfloat16().float().T, Bt.bfloat16().float().T
+    z = _ref(Ar, Br, 0.5, bias)
+    assert _rel(Z, z) < 1e-5
+    h = 0.5 * z * (1 + torch.erf(z / math.sqrt(2)))
+    assert _rel(C, h) < 1e-5
+    assert _rel(Cb.float(), h) < 1e-2
+    # GELU-derivative epilogue
+    D = torch.empty(200, 150, device=cuda)
+    gemm(At, Bt, ta=True, tb=True, act=ACT_GELU_GRAD, zin=Z, out=D)
+    torch.cuda.synchronize()
+    phi = torch.exp(-0.5 * z * z) / math.sqrt(2 * math.pi)
+    cdf = 0.5 * (1 + torch.erf(z / math.sqrt(2)))
+    assert _rel(D, _ref(Ar, Br) * (cdf + z * phi)) < 1e-5
+
+
+def test_f32_gemm_engine(cuda):
+    g = torch.Generator(device=cuda).manual_seed(9)
+    A = torch.randn(333, 777, device=cuda, generator=g)
+    B = torch.randn(129, 777, device=cuda, generator=g)
+    C = torch.ones(333, 129, device=cuda)
+    gemm(A, B, alpha=2.0, beta=1.0, out=C, engine=1)
+    torch.cuda.synchronize()
+    assert _rel(C, 2.0 * _ref(A, B) + 1.0) < 1e-6

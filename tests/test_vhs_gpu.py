@@ -99,3 +99,57 @@ def test_q_batch_order_independent(cuda):
     perm = torch.randperm(300, generator=torch.Generator().manual_seed(0)).to(be.device)
     sm.collide(fin[perm].contiguous(), q2, project=True)
     assert torch.equal(q[perm], q2)
+
+
+@pytest.mark.parametrize('Nv,Nrho,M,dev,prec', [(24, 12, 12, 6, 'single'), (16, 8, 6, 5, 'single'),
+                                                (16, 8, 6, 5, 'double'), (32, 16, 12, 6, 'single')])
+def test_every_kernel_variant_agrees(cuda, Nv, Nrho, M, dev, prec):
+    """Every compiled variant (CTA size, slab groups) computes the same
+    per-distribution arithmetic, so all agree to FP rounding."""
+    from frfs_b200.autotune import variants
+    from frfs_b200.scattering import VHSCollider
+    be, vm, sm, orc = _setup(Nv, Nrho, M, dev, prec)
+    rng = np.random.default_rng(11)
+    F = np.stack([mixed_maxwellians(vm.cv(), rng) for _ in range(40)])
+    fin = torch.from_numpy(F).to(be.fpdtype).to(be.device)
+    outs = []
+    nvar = len(variants([sm.grid]))
+    assert nvar >= 2
+    for t in range(nvar):
+        sm.grid.struct.tile = t
+        col = VHSCollider([sm.grid], be.device)
+        q = torch.empty_like(fin)
+        col([(0, fin, q, None)], project=True, exact=(Nv <= 16))
+        outs.append(q)
+    torch.cuda.synchronize()
+    ref = outs[0].double()
+    for t, q in enumerate(outs[1:], 1):
+        err = float((q.double() - ref).norm() / ref.norm())
+        assert err < (1e-12 if prec == 'double' else 1e-6), (t, err)
+
+
+def test_two_grids_one_launch_equals_separate(cuda):
+    """24^3 and 32^3 batches (two species, different masses) in one
+    persistent launch give the same Q as separate launches."""
+    from frfs_b200.scattering import VHSCollider, VHSGrid, vhs_prefactor
+    out = []
+    grids, fs = [], []
+    for Nv, mass in ((24, 1.0), (32, 2.0)):
+        be, vm, sm, orc = _setup(Nv, 16, 12, 6, 'single')
+        gam, pref, _ = vhs_prefactor(vm, 0.81, 4.17e-10, 273.0, mass=mass)
+        g = VHSGrid(Nv, vm.L(), vm.qz(), vm.qw(), vm.sz(), vm.sw(), gam, pref, vm.cw(),
+                    vm.c0(), torch.float32, be.device)
+        rng = np.random.default_rng(Nv)
+        F = np.stack([mixed_maxwellians(vm.cv(), rng) for _ in range(20)])
+        grids.append(g)
+        fs.append(torch.from_numpy(F).float().to(be.device))
+    both = VHSCollider(grids, be.device)
+    qa = [torch.empty_like(f) for f in fs]
+    both([(1, fs[1], qa[1], None), (0, fs[0], qa[0], None)])
+    for i in range(2):
+        one = VHSCollider([grids[i]], be.device)
+        qb = torch.empty_like(fs[i])
+        one([(0, fs[i], qb, None)])
+        torch.cuda.synchronize()
+        err = float((qa[i].double() - qb.double()).norm() / qb.double().norm())
+        assert err < 1e-6, (i, err)
