@@ -20,7 +20,8 @@ EXPORTS = (
     'bdgfs_vhs_collide_static',
     'bdgfs_fr_disu', 'bdgfs_fr_bc_update', 'bdgfs_fr_rhs',
     'bdgfs_moments', 'bdgfs_residual', 'bdgfs_status_check',
-    'bdgfs_gemm', 'bdgfs_colsum', 'bdgfs_adamw',
+    'bdgfs_gemm', 'bdgfs_colsum', 'bdgfs_adamw', 'bdgfs_relmse',
+    'bdgfs_hybrid_classify', 'bdgfs_hybrid_project', 'bdgfs_hybrid_scatter',
 )
 
 
@@ -38,7 +39,8 @@ class VhsGrid(C.Structure):
 
 class VhsBatch(C.Structure):
     _fields_ = [('grid', C.c_int32), ('pad_', C.c_int32), ('ndof', C.c_int64),
-                ('f', C.c_void_p), ('Q', C.c_void_p), ('moments', C.c_void_p)]
+                ('f', C.c_void_p), ('Q', C.c_void_p), ('moments', C.c_void_p),
+                ('index', C.c_void_p), ('count', C.c_void_p)]
 
 
 class FrEles(C.Structure):
@@ -65,7 +67,18 @@ class GemmArgs(C.Structure):
                 ('bias', C.c_void_p), ('act', C.c_int32), ('engine', C.c_int32),
                 ('cf32', C.c_void_p), ('cbf16', C.c_void_p), ('ldc', C.c_int64),
                 ('zout', C.c_void_p), ('zin', C.c_void_p), ('ldz', C.c_int64),
-                ('status', C.c_void_p), ('pad_', C.c_int32)]
+                ('status', C.c_void_p), ('pad_', C.c_int32),
+                ('arow', C.c_void_p), ('crow', C.c_void_p), ('row_scale', C.c_void_p),
+                ('mcount', C.c_void_p)]
+
+
+class HybridArgs(C.Structure):
+    _fields_ = [('ndof', C.c_int64), ('Nv', C.c_int32), ('fp64', C.c_int32),
+                ('c0', C.c_void_p), ('ginv', C.c_void_p), ('cw', C.c_double),
+                ('threshold', C.c_float), ('recheck', C.c_float), ('seed', C.c_uint64),
+                ('counts', C.c_void_p), ('sur_idx', C.c_void_p), ('sur_inv_rho', C.c_void_p),
+                ('sur_rho2', C.c_void_p), ('spec_idx', C.c_void_p), ('flag', C.c_void_p),
+                ('eps', C.c_void_p), ('recheck_err', C.c_void_p)]
 
 
 _lib = None
@@ -101,6 +114,10 @@ def lib():
             'bdgfs_residual': [vp, vp, i64, i32, vp, vp],
             'bdgfs_status_check': [vp, i64, i32, vp, vp],
             'bdgfs_gemm': [C.c_void_p, vp],
+            'bdgfs_relmse': [vp, vp, i64, i64, C.c_float, vp, vp, vp],
+            'bdgfs_hybrid_classify': [vp, vp, vp],
+            'bdgfs_hybrid_project': [vp, vp, vp],
+            'bdgfs_hybrid_scatter': [vp, vp, vp, vp],
             'bdgfs_colsum': [vp, i64, i64, vp, vp],
             'bdgfs_adamw': [vp, vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float,
                             C.c_float, C.c_float, i64, vp],

@@ -126,18 +126,19 @@ __device__ __forceinline__ float to_f<__nv_bfloat16>(__nv_bfloat16 x) { return _
 template <typename S>
 __device__ __forceinline__ void load_tile(unsigned char* dst, const S* src, int64_t rows,
                                           int64_t K, int64_t srow, int64_t sk, int64_t r0,
-                                          int64_t k0)
+                                          int64_t k0, const int32_t* rowmap)
 {
     // 128 rows x 8 k-groups = 1024 (row, kgroup) pairs, 8 per thread
     for (int p = threadIdx.x; p < BM * (BK / 8); p += THREADS) {
         const int r = p / (BK / 8), kg = p % (BK / 8);
         const int64_t gr = r0 + r;
+        const int64_t sr = (gr < rows && rowmap) ? int64_t(rowmap[gr]) : gr;
         __align__(16) __nv_bfloat16 h[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             const int64_t gk = k0 + kg * 8 + j;
             float x = 0.f;
-            if (gr < rows && gk < K) x = to_f<S>(src[gr * srow + gk * sk]);
+            if (gr < rows && gk < K) x = to_f<S>(src[sr * srow + gk * sk]);
             h[j] = __float2bfloat16_rn(x);
         }
         unsigned char* d = dst + ((r / 8) * (BK / 8) + kg) * 128 + (r % 8) * 16;
@@ -170,6 +171,13 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t m0 = int64_t(blockIdx.y) * BM, n0 = int64_t(blockIdx.x) * BN;
+    // rows beyond a device-side count: nothing to do (uniform per CTA)
+    int64_t Mrows = g.M;
+    if (g.mcount) {
+        const int64_t c = *g.mcount;
+        Mrows = c < g.M ? (c < 0 ? 0 : c) : g.M;
+    }
+    if (m0 >= Mrows) return;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -198,8 +206,8 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
             phase[s] ^= 1;
         }
         if (!__syncthreads_and(ok)) break;
-        load_tile<SA>(sA[s], A, g.M, g.K, g.sam, g.sak, m0, kt * BK);
-        load_tile<SB>(sB[s], B, g.N, g.K, g.sbn, g.sbk, n0, kt * BK);
+        load_tile<SA>(sA[s], A, Mrows, g.K, g.sam, g.sak, m0, kt * BK, g.arow);
+        load_tile<SB>(sB[s], B, g.N, g.K, g.sbn, g.sbk, n0, kt * BK, nullptr);
         fence_async_smem();
         __syncthreads();
         if (warp == 0) {
@@ -231,28 +239,29 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
     if (!abort_s) {
         // epilogue: warp w holds rows 32w + lane, 16 columns per load
         const int64_t row = m0 + warp * 32 + lane;
-        const float alpha = g.alpha;
+        const int64_t orow = (row < Mrows && g.crow) ? int64_t(g.crow[row]) : row;
+        const float alpha = g.alpha * ((row < Mrows && g.row_scale) ? g.row_scale[row] : 1.f);
         const float* bias = static_cast<const float*>(g.bias);
         for (int c = 0; c < BN; c += 16) {
             float v[16];
             tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c), v);
-            if (row >= g.M) continue;
+            if (row >= Mrows) continue;
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
                 const int64_t col = n0 + c + j;
                 if (col >= g.N) break;
                 float x = alpha * v[j];
                 if (bias) x += bias[col];
-                if (g.zout) static_cast<float*>(g.zout)[row * g.ldz + col] = x;
+                if (g.zout) static_cast<float*>(g.zout)[orow * g.ldz + col] = x;
                 if (g.act == 1) {
                     x = gelu(x);
                 } else if (g.act == 2) {
-                    const float z = static_cast<const float*>(g.zin)[row * g.ldz + col];
+                    const float z = static_cast<const float*>(g.zin)[orow * g.ldz + col];
                     x *= gelu_grad(z);
                 }
-                if (g.cf32) static_cast<float*>(g.cf32)[row * g.ldc + col] = x;
+                if (g.cf32) static_cast<float*>(g.cf32)[orow * g.ldc + col] = x;
                 if (g.cbf16)
-                    static_cast<__nv_bfloat16*>(g.cbf16)[row * g.ldc + col] = __float2bfloat16_rn(x);
+                    static_cast<__nv_bfloat16*>(g.cbf16)[orow * g.ldc + col] = __float2bfloat16_rn(x);
             }
         }
     } else if (threadIdx.x == 0 && g.status) {
@@ -337,6 +346,29 @@ __global__ void adamw_kernel(float* p, const float* gr, float* m1, float* m2, __
     if (pb) pb[i] = __float2bfloat16_rn(w);
 }
 
+// Per-row relative squared error and its gradient:
+//   L = (1/M) sum_m |y_m - t_m|^2 / (|t_m|^2 + delta),  dy = dL/dy.
+__global__ void __launch_bounds__(256) relmse_kernel(const float* y, const float* t, int64_t M,
+                                                     int64_t N, float delta, float* dy,
+                                                     double* loss)
+{
+    __shared__ double red[2 * 8];
+    const int64_t m = blockIdx.x;
+    const float* ym = y + m * N;
+    const float* tm = t + m * N;
+    double e[2] = {0, 0};
+    for (int64_t j = threadIdx.x; j < N; j += blockDim.x) {
+        const double d = double(ym[j]) - double(tm[j]);
+        e[0] += d * d;
+        e[1] += double(tm[j]) * double(tm[j]);
+    }
+    block_sum<2>(e, red);
+    const double den = e[1] + double(delta);
+    const float sc = float(2.0 / (den * double(M)));
+    for (int64_t j = threadIdx.x; j < N; j += blockDim.x) dy[m * N + j] = sc * (ym[j] - tm[j]);
+    if (threadIdx.x == 0 && loss) atomicAdd(loss, e[0] / den / double(M));
+}
+
 }  // namespace bdgfs
 
 using namespace bdgfs;
@@ -349,7 +381,9 @@ extern "C" int32_t bdgfs_gemm(const bdgfs_gemm_args* g, void* stream)
     if (g->M == 0 || g->N == 0) return BDGFS_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (g->engine == 1) {           // FP32 SIMT
-        if (g->a_bf16 || g->b_bf16 || !g->cf32 || g->act || g->bias) return BDGFS_EUNSUPPORTED;
+        if (g->a_bf16 || g->b_bf16 || !g->cf32 || g->act || g->bias || g->arow || g->crow ||
+            g->row_scale || g->mcount)
+            return BDGFS_EUNSUPPORTED;
         dim3 grid(unsigned((g->N + 63) / 64), unsigned((g->M + 63) / 64));
         f32_gemm_kernel<<<grid, 256, 0, st>>>(*g, static_cast<const float*>(g->A),
                                               static_cast<const float*>(g->B));
@@ -401,5 +435,16 @@ extern "C" int32_t bdgfs_adamw(float* p, const float* grad, float* m1, float* m2
     adamw_kernel<<<unsigned((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         p, grad, m1, m2, static_cast<__nv_bfloat16*>(p_bf16), n, lr, beta1, beta2, eps,
         weight_decay, bc1, bc2);
+    return cuda_status(cudaGetLastError());
+}
+
+extern "C" int32_t bdgfs_relmse(const float* y, const float* t, int64_t M, int64_t N, float delta,
+                                float* dy, double* loss, void* stream)
+{
+    if (!y || !t || !dy || M < 0 || N < 1 || M > 2147483647LL) return BDGFS_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (loss && cudaMemsetAsync(loss, 0, sizeof(double), st) != cudaSuccess) return BDGFS_ECUDA;
+    if (M == 0) return BDGFS_OK;
+    relmse_kernel<<<unsigned(M), 256, 0, st>>>(y, t, M, N, delta, dy, loss);
     return cuda_status(cudaGetLastError());
 }

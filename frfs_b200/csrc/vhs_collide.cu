@@ -502,8 +502,22 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int64_t s_item;
+    __shared__ int64_t s_start[5];
     unsigned char* scratch = a.scratch + size_t(blockIdx.x) * a.scratch_per_cta;
-    const int64_t total = a.start[a.nbatch];
+    if (threadIdx.x == 0) {
+        // per-batch counts: the host size, or a device count when given
+        s_start[0] = 0;
+        for (int b = 0; b < a.nbatch; ++b) {
+            int64_t c = a.batches[b].ndof;
+            if (a.batches[b].count) {
+                const int64_t d = *a.batches[b].count;
+                c = d < 0 ? 0 : (d < c ? d : c);
+            }
+            s_start[b + 1] = s_start[b] + c;
+        }
+    }
+    __syncthreads();
+    const int64_t total = s_start[a.nbatch];
     for (;;) {
         if (threadIdx.x == 0) s_item = int64_t(atomicAdd(a.counter, 1ull));
         __syncthreads();
@@ -511,10 +525,12 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
         __syncthreads();
         if (item >= total) break;
         int b = 0;
-        while (item >= a.start[b + 1]) ++b;
+        while (item >= s_start[b + 1]) ++b;
         const bdgfs_vhs_batch& bt = a.batches[b];
         const bdgfs_vhs_grid& g = a.grids[bt.grid];
-        const int64_t dof = item - a.start[b];
+        const int64_t pos = item - s_start[b];
+        const int64_t dof = bt.index ? int64_t(bt.index[pos]) : pos;
+        if (dof < 0 || dof >= bt.ndof) continue;   // malformed index list: skip
         const int64_t n3 = int64_t(g.Nv) * g.Nv * g.Nv;
         const T* f = static_cast<const T*>(bt.f) + dof * n3;
         T* Q = static_cast<T*>(bt.Q) + dof * n3;

@@ -22,13 +22,17 @@ def _operand(t, trans):
 
 
 def gemm(a, b, *, ta=False, tb=False, alpha=1.0, beta=0.0, bias=None, act=ACT_NONE,
-         out=None, out_bf16=None, zout=None, zin=None, engine=0, status=None, stream=None):
-    """out[m][n] = alpha * sum_k A(m,k) B(n,k) (+ beta*out) (+ bias) -> act.
-    A = a (M x K) or a^T if ta; B = b (N x K) or b^T if tb."""
+         out=None, out_bf16=None, zout=None, zin=None, engine=0, status=None, stream=None,
+         arow=None, crow=None, row_scale=None, mcount=None, M=None):
+    """out[m][n] = alpha * row_scale[m] * sum_k A(m,k) B(n,k) (+ beta*out)
+    (+ bias) -> act.  A = a (M x K) or a^T if ta; B = b (N x K) or b^T if tb.
+    arow gathers rows of A, crow scatters rows of the outputs, mcount is a
+    device row count (rows beyond it are skipped)."""
     pa, sam, sak, abf = _operand(a, ta)
     pb, sbn, sbk, bbf = _operand(b, tb)
-    M = a.shape[1] if ta else a.shape[0]
     K = a.shape[0] if ta else a.shape[1]
+    if M is None:
+        M = a.shape[1] if ta else a.shape[0]
     N = b.shape[1] if tb else b.shape[0]
     if (b.shape[0] if tb else b.shape[1]) != K:
         raise ValueError('inner dimensions differ')
@@ -36,10 +40,15 @@ def gemm(a, b, *, ta=False, tb=False, alpha=1.0, beta=0.0, bias=None, act=ACT_NO
         if t is not None and (not t.is_cuda or not t.is_contiguous()):
             raise ValueError('outputs/bias must be contiguous CUDA tensors')
     ldc = N
-    if out is not None and out.shape != (M, N):
-        raise ValueError('out shape')
-    if out_bf16 is not None and out_bf16.shape != (M, N):
-        raise ValueError('out_bf16 shape')
+    if crow is None:
+        if out is not None and out.shape != (M, N):
+            raise ValueError('out shape')
+        if out_bf16 is not None and out_bf16.shape != (M, N):
+            raise ValueError('out_bf16 shape')
+    for t, dt in ((arow, torch.int32), (crow, torch.int32), (row_scale, torch.float32),
+                  (mcount, torch.int64)):
+        if t is not None and (t.dtype != dt or not t.is_cuda):
+            raise TypeError('index/scale/count tensors: int32 rows, float32 scale, int64 count')
     args = _lib.GemmArgs(M=M, N=N, K=K, A=pa, sam=sam, sak=sak, B=pb, sbn=sbn, sbk=sbk,
                          a_bf16=int(abf), b_bf16=int(bbf), alpha=float(alpha), beta=float(beta),
                          bias=bias.data_ptr() if bias is not None else 0, act=int(act),
@@ -48,7 +57,11 @@ def gemm(a, b, *, ta=False, tb=False, alpha=1.0, beta=0.0, bias=None, act=ACT_NO
                          cbf16=out_bf16.data_ptr() if out_bf16 is not None else 0, ldc=ldc,
                          zout=zout.data_ptr() if zout is not None else 0,
                          zin=zin.data_ptr() if zin is not None else 0, ldz=N,
-                         status=status.data_ptr() if status is not None else 0)
+                         status=status.data_ptr() if status is not None else 0,
+                         arow=arow.data_ptr() if arow is not None else 0,
+                         crow=crow.data_ptr() if crow is not None else 0,
+                         row_scale=row_scale.data_ptr() if row_scale is not None else 0,
+                         mcount=mcount.data_ptr() if mcount is not None else 0)
     _lib.check(_lib.lib().bdgfs_gemm(C.byref(args), _lib.stream_ptr(stream)), 'bdgfs_gemm')
     return out if out is not None else out_bf16
 

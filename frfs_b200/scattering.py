@@ -133,8 +133,10 @@ class VHSCollider:
         self.scratch = torch.empty(nbytes, dtype=torch.uint8, device=device)
         self.counter = torch.zeros(1, dtype=torch.int64, device=device)
 
-    def __call__(self, batches, project=True, exact=False, stream=None):
-        """batches: list of (grid_index, f[ndof, n], Q[ndof, n], moments|None)."""
+    def __call__(self, batches, project=True, exact=False, stream=None, index=None, count=None):
+        """batches: list of (grid_index, f[ndof, n], Q[ndof, n], moments|None).
+        index (int32, device) / count (int64 device scalar) restrict the first
+        batch to f[index[i]], i < count (read by the kernel)."""
         L = _lib.lib()
         bs = (_lib.VhsBatch * len(batches))()
         for i, (gi, f, Q, mom) in enumerate(batches):
@@ -154,6 +156,14 @@ class VHSCollider:
             bs[i] = _lib.VhsBatch(grid=gi, ndof=f.numel() // n3, f=f.data_ptr(),
                                   Q=Q.data_ptr(),
                                   moments=mom.data_ptr() if mom is not None else 0)
+            if i == 0 and index is not None:
+                if index.dtype != torch.int32 or not index.is_cuda:
+                    raise TypeError('index must be an int32 CUDA tensor')
+                bs[i].index = index.data_ptr()
+            if i == 0 and count is not None:
+                if count.dtype != torch.int64 or not count.is_cuda:
+                    raise TypeError('count must be an int64 CUDA tensor')
+                bs[i].count = count.data_ptr()
         rc = L.bdgfs_vhs_collide(self._garr, len(self.grids), bs, len(batches),
                                  (1 if project else 0) | (2 if exact else 0),
                                  _lib.ptr(self.scratch),

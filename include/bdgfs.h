@@ -60,6 +60,10 @@ typedef struct bdgfs_vhs_batch {
     void* Q;             /* real [ndof][Nv^3]                               */
     double* moments;     /* optional [ndof][10]: C.Q before (0..4) and after
                             (5..9) the projection, in FP64, C = cw*{1,c,|c|^2} */
+    const int32_t* index;  /* optional: distribution i is f[index[i]] (and
+                              Q/moments at the same position)              */
+    const int64_t* count;  /* optional device count of distributions to
+                              process (<= ndof), read by the kernel          */
 } bdgfs_vhs_batch;
 
 /* Number of kernel variants compiled for this grid set (tile values
@@ -213,6 +217,10 @@ typedef struct bdgfs_gemm_args {
     int64_t ldz;
     int32_t* status;     /* receives BDGFS_ETIMEOUT if a wait expired    */
     int32_t pad_;
+    const int32_t* arow; /* optional: row m of A is row arow[m] (gather) */
+    const int32_t* crow; /* optional: row m of C/zout is crow[m] (scatter) */
+    const float* row_scale;   /* optional: acc of row m scaled by row_scale[m] */
+    const int64_t* mcount;    /* optional device row count (<= M)        */
 } bdgfs_gemm_args;
 
 int32_t bdgfs_gemm(const bdgfs_gemm_args* args, void* stream);
@@ -221,12 +229,53 @@ int32_t bdgfs_gemm(const bdgfs_gemm_args* args, void* stream);
 int32_t bdgfs_colsum(const float* X, int64_t M, int64_t N, float* out,
                      void* stream);
 
+/* Mean per-row relative squared error of y against t and its gradient dy
+ * (loss of the surrogate's training). */
+int32_t bdgfs_relmse(const float* y, const float* t, int64_t M, int64_t N,
+                     float delta, float* dy, double* loss, void* stream);
+
 /* AdamW step on FP32 master weights p (n values) with moments m1, m2;
  * writes a bf16 copy to p_bf16 when not NULL.  step counts from 1. */
 int32_t bdgfs_adamw(float* p, const float* grad, float* m1, float* m2,
                     void* p_bf16, int64_t n, float lr, float beta1,
                     float beta2, float eps, float weight_decay, int64_t step,
                     void* stream);
+
+/* ------------------------------------------------------------------------
+ * Surrogate/spectral hybrid collision step (no counterpart in the reference)
+ * ---------------------------------------------------------------------- */
+typedef struct bdgfs_hybrid_args {
+    int64_t ndof;            /* distributions of the state (rows)          */
+    int32_t Nv;
+    int32_t fp64;
+    const double* c0;        /* [Nv] cell-centre velocities                */
+    const double* ginv;      /* [5][5] inverse Gram matrix of {1,c,|c|^2}  */
+    double cw;
+    float threshold;         /* Maxwellian deviation below which the
+                                surrogate is used                          */
+    float recheck;           /* fraction of surrogate cells re-checked     */
+    uint64_t seed;           /* re-check sampling seed (e.g. step number)  */
+    int64_t* counts;         /* [3] device: surrogate, spectral (incl.
+                                re-checks), re-checked                     */
+    int32_t* sur_idx;        /* [ndof] surrogate cells                     */
+    float* sur_inv_rho;      /* [ndof] 1/rho of each surrogate row         */
+    float* sur_rho2;         /* [ndof] rho^2 of each surrogate row         */
+    int32_t* spec_idx;       /* [ndof] spectral cells                      */
+    uint8_t* flag;           /* [ndof] 0 spectral, 1 surrogate, 2 re-checked */
+    float* eps;              /* optional [ndof] indicator values           */
+    double* recheck_err;     /* optional [2]: sum |Qs-Qspec|^2, sum |Qspec|^2 */
+} bdgfs_hybrid_args;
+
+/* Indicator eps = |f - M[f]| / |f| per distribution and device-side lists. */
+int32_t bdgfs_hybrid_classify(const bdgfs_hybrid_args* h, const void* f,
+                              void* stream);
+/* FP64 conservation projection of the first counts[0] compact rows of Qc. */
+int32_t bdgfs_hybrid_project(const bdgfs_hybrid_args* h, void* Qc,
+                             void* stream);
+/* Compact surrogate rows -> Q[sur_idx[m]], except re-checked cells (kept
+ * spectral; their surrogate error is accumulated in recheck_err). */
+int32_t bdgfs_hybrid_scatter(const bdgfs_hybrid_args* h, const void* Qc,
+                             void* Q, void* stream);
 
 #ifdef __cplusplus
 }

@@ -35,6 +35,7 @@ STRUCTS = {
     'bdgfs_fr_eles': _lib.FrEles,
     'bdgfs_fr_walls': _lib.FrWall,
     'bdgfs_gemm_args': _lib.GemmArgs,
+    'bdgfs_hybrid_args': _lib.HybridArgs,
 }
 
 
