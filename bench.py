@@ -429,6 +429,121 @@ def small_fp64(flush, steps=20):
             'dtype': 'f64'}
 
 
+def surrogate_legs(flush, log=None):
+    """Config 4 (surrogate trained on the Couette family, evaluated on 50000
+    held-out seeded distributions) and config 5 (8^3 hex P2 lid-driven
+    cavity: plain FP32 spectral vs surrogate hybrid, DG steps/s)."""
+    import time
+    import torch
+    from frfs_b200.backend import CUDABackend
+    from frfs_b200.inifile import Inifile
+    from frfs_b200.integrators import get_integrator
+    from frfs_b200.mesh import StructuredMesh
+    from frfs_b200.scattering import DGFSVHSGLLScatteringModel
+    from frfs_b200.surrogate import HybridCollider, QSurrogate, sample_family
+    from frfs_b200.system import DGFSSystem
+    from frfs_b200.velocitymesh import DGFSVelocityMesh
+    cfg = Inifile(couette_ini('single'))
+    be = CUDABackend(cfg)
+    vm = DGFSVelocityMesh(be, cfg)
+    sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
+    t0 = time.time()
+    q = QSurrogate(sm.grid, nmodes=512, width=1024)
+    q.fit(nsamples=200000, ntest=50000, epochs=20, lr=3e-4, batch=1024, seed=0)
+    t_fit = time.time() - t0
+    # surrogate vs spectral throughput on near-equilibrium cells
+    gen = torch.Generator(device=be.device).manual_seed(3)
+    f = sample_family(vm.c0(), 8192, gen, be.device)
+    out = torch.empty_like(f)
+    h = HybridCollider(q, threshold=float('inf'), recheck=0.0)
+    st = torch.cuda.current_stream()
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(reps):
+            flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            fn()
+            b.record(st)
+            torch.cuda.synchronize()
+            tot += a.elapsed_time(b)
+        return tot / reps
+    t_sur = timed(lambda: h(f, out))
+    t_spec = timed(lambda: sm.collide(f, out, project=True, exact=False))
+    c4 = {'workload': ('surrogate of Q on Nv=24^3 (M=Nrho=12): 512-mode bases (randomised SVD), '
+                       '4-layer GELU MLP width 1024, BF16 weights / FP32 accumulation on tcgen05, '
+                       'AdamW lr 3e-4, 20 epochs, 200000 training / 50000 held-out seeded '
+                       'distributions of the Couette family, FP64 conservation projection'),
+          'modes': q.k, 'train_steps': q.steps, 'train_s': q.train_seconds,
+          'data_s': q.data_seconds, 'fit_s_total': t_fit,
+          'final_loss': q.history[-1], 'first_epoch_loss': q.history[0],
+          'heldout_rel_l2_vs_spectral_q': q.test_err,
+          'surrogate_q_evals_per_s': 8192 / (t_sur * 1e-3),
+          'spectral_q_evals_per_s': 8192 / (t_spec * 1e-3)}
+    # ---- config 5: lid-driven cavity
+    import numpy as np
+    u0 = np.sqrt(2 * 8.3144598 / NONDIM['molarMass0'] * NONDIM['T0'])
+    ini = couette_ini('single', dict(WORK, order=2)).split('[soln-bcs-y-]')[0]
+    ini += f"""
+[soln-bcs-lid]
+type = dgfs-wall-diffuse
+rho = {NONDIM['rho0']}
+T = {NONDIM['T0']}
+ux = {0.5 * u0}
+uy = 0
+uz = 0
+[soln-bcs-walls]
+type = dgfs-wall-diffuse
+rho = {NONDIM['rho0']}
+T = {NONDIM['T0']}
+ux = 0
+uy = 0
+uz = 0
+"""
+    names = {'x-': 'walls', 'x+': 'walls', 'y-': 'walls', 'y+': 'lid', 'z-': 'walls',
+             'z+': 'walls'}
+    res = {}
+    for mode in ('plain', 'hybrid'):
+        c5cfg = Inifile(ini)
+        c5cfg.set('solver-time-integrator', 'dt', '2e-4')
+        be5 = CUDABackend(c5cfg)
+        mesh = StructuredMesh((8, 8, 8), (0, 0, 0), (1, 1, 1), periodic='', bcnames=names)
+        s5 = DGFSSystem(be5, mesh, c5cfg, nreg=3)
+        hc = None
+        if mode == 'hybrid':
+            hc = HybridCollider(q, threshold=0.05, recheck=0.02)
+            n3 = s5.vm.vsize()
+            s5.sm.collide = lambda fin, fout, **kw: hc(fin.reshape(-1, n3), fout.reshape(-1, n3))
+        integ = get_integrator(be5, s5, c5cfg)
+        for _ in range(3):
+            integ.step(0.0, 2e-4)
+        torch.cuda.synchronize()
+        steps = 10
+        tot = 0.0
+        for _ in range(steps):
+            flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            integ.step(0.0, 2e-4)
+            b.record(st)
+            torch.cuda.synchronize()
+            tot += a.elapsed_time(b)
+        res[mode] = {'dg_steps_per_s': steps / (tot * 1e-3), 'ms_per_step': tot / steps}
+        if hc is not None:
+            res[mode].update(hc.stats())
+        del s5, integ, hc
+        torch.cuda.empty_cache()
+    c5 = {'workload': ('3-D lid-driven cavity: 8^3 hex P2 (13824 DOFs), Nv=24^3, VHS 0.81, '
+                       'Nrho=M=12, lid 0.5, diffuse walls T=1, uniform Maxwellian start, SSP-RK2 '
+                       'dt=2e-4; hybrid threshold 0.05, 2% spectral re-check every call'),
+          'plain_fp32_spectral': res['plain'], 'hybrid': res['hybrid'],
+          'speedup': res['hybrid']['dg_steps_per_s'] / res['plain']['dg_steps_per_s']}
+    return c4, c5
+
+
 # ---------------------------------------------------------------- GPU leg
 def run_gpu(args):
     import numpy as np
@@ -557,6 +672,10 @@ def run_gpu(args):
         extra['plain_fp64_small'] = small_fp64(flush)
         bq, _ = batched_q(flush)
         extra['batched_q'] = bq
+    if ws == 1 and not args.no_surrogate:
+        c4, c5 = surrogate_legs(flush)
+        extra['surrogate'] = c4
+        extra['hybrid_lid_cavity'] = c5
     # gpu launches per step: 2 x (collide + disu + bc_update + rhs)
     launches = 8 * args.steps
     line = {
@@ -618,6 +737,8 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='frfs_b200', choices=['frfs_b200', 'reference'])
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline leg')
+    ap.add_argument('--no-surrogate', action='store_true',
+                    help='skip the surrogate training and hybrid lid-cavity legs')
     ap.add_argument('--no-extra', action='store_true',
                     help='skip the FP64 small and batched-collision measurements')
     ap.add_argument('--q-only', type=int, default=0, metavar='NDOF',

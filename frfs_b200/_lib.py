@@ -78,7 +78,7 @@ class HybridArgs(C.Structure):
                 ('threshold', C.c_float), ('recheck', C.c_float), ('seed', C.c_uint64),
                 ('counts', C.c_void_p), ('sur_idx', C.c_void_p), ('sur_inv_rho', C.c_void_p),
                 ('sur_rho2', C.c_void_p), ('spec_idx', C.c_void_p), ('flag', C.c_void_p),
-                ('eps', C.c_void_p), ('recheck_err', C.c_void_p)]
+                ('eps', C.c_void_p), ('recheck_err', C.c_void_p), ('seed_dev', C.c_void_p)]
 
 
 _lib = None

@@ -68,7 +68,8 @@ __global__ void __launch_bounds__(256) indicator_kernel(const bdgfs_hybrid_args 
         const double eps = (ok && e[1] > 0.0) ? sqrt(e[0] / e[1]) : 1e30;
         if (h.eps) h.eps[dof] = float(eps);
         const bool sur = eps < double(h.threshold);
-        const bool re = sur && (double(mix32(h.seed * 0x100000001B3ull + uint64_t(dof))) <
+        const uint64_t seed = h.seed_dev ? *h.seed_dev : h.seed;
+        const bool re = sur && (double(mix32(seed * 0x100000001B3ull + uint64_t(dof))) <
                                 double(h.recheck) * 4294967296.0);
         if (h.flag) h.flag[dof] = uint8_t(sur ? (re ? 2 : 1) : 0);
         if (sur) {
@@ -128,6 +129,7 @@ __global__ void __launch_bounds__(256) scatter_kernel(const bdgfs_hybrid_args h,
 {
     __shared__ double red[2 * 8];
     const int64_t row = blockIdx.x;
+    if (row == 0 && threadIdx.x == 0 && h.seed_dev) *h.seed_dev += 1;   // next step's sample
     const int64_t cnt = *h.counts;
     if (row >= cnt) return;
     const int64_t n = int64_t(h.Nv) * h.Nv * h.Nv;

@@ -348,6 +348,8 @@ __global__ void adamw_kernel(float* p, const float* gr, float* m1, float* m2, __
 
 // Per-row relative squared error and its gradient:
 //   L = (1/M) sum_m |y_m - t_m|^2 / (|t_m|^2 + delta),  dy = dL/dy.
+// delta floors the denominator (rows with tiny targets are weighted by
+// their absolute error).
 __global__ void __launch_bounds__(256) relmse_kernel(const float* y, const float* t, int64_t M,
                                                      int64_t N, float delta, float* dy,
                                                      double* loss)

@@ -220,3 +220,48 @@ class DGFSVHSGLLScatteringModel(DGFSScatteringModel):
         """One DOF (elem, upt) of a [neles][nupts][Nv^3] bank (per-DOF shim
         of scattering.py:227)."""
         self.collide(d_arr_in[elem, upt], d_arr_out[elem, upt])
+
+
+class DGFSVHSGLLHybridScatteringModel(DGFSVHSGLLScatteringModel):
+    """'vhs-gll-hybrid': the spectral operator of 'vhs-gll' plus the learned
+    surrogate on near-equilibrium cells (``frfs_b200.surrogate``).
+
+    [scattering-model] keys (besides those of 'vhs-gll'):
+      surrogate-threshold  Maxwellian deviation below which the surrogate
+                           is used (default 0.05)
+      surrogate-recheck    fraction of surrogate cells re-checked by the
+                           spectral operator every call (default 0.02)
+      surrogate-file       trained model to load (torch.save of state_dict);
+                           trained and saved there when absent
+      surrogate-nsamples / -epochs / -modes / -width / -lr / -seed
+                           training settings (200000 / 20 / 512 / 1024 /
+                           3e-4 / 0)
+    """
+    scattering_model = 'vhs-gll-hybrid'
+
+    def perform_precomputation(self):
+        import os
+        from .surrogate import HybridCollider, QSurrogate
+        super().perform_precomputation()
+        cfg, sect = self.cfg, 'scattering-model'
+        self.surrogate = QSurrogate(self.grid,
+                                    nmodes=cfg.getint(sect, 'surrogate-modes', 512),
+                                    width=cfg.getint(sect, 'surrogate-width', 1024))
+        path = cfg.get(sect, 'surrogate-file', '')
+        if path and os.path.exists(path):
+            self.surrogate.load_state_dict(torch.load(path, map_location='cpu'))
+        else:
+            self.surrogate.fit(nsamples=cfg.getint(sect, 'surrogate-nsamples', 200000),
+                               epochs=cfg.getint(sect, 'surrogate-epochs', 20),
+                               lr=cfg.getfloat(sect, 'surrogate-lr', 3e-4),
+                               seed=cfg.getint(sect, 'surrogate-seed', 0))
+            if path:
+                torch.save(self.surrogate.state_dict(), path)
+        self.hybrid = HybridCollider(self.surrogate,
+                                     threshold=cfg.getfloat(sect, 'surrogate-threshold', 0.05),
+                                     recheck=cfg.getfloat(sect, 'surrogate-recheck', 0.02),
+                                     project=self._project)
+
+    def collide(self, fin, fout, moments=None, project=None, exact=None):
+        n3 = self.vm.vsize()
+        self.hybrid(fin.reshape(-1, n3), fout.reshape(-1, n3))

@@ -74,47 +74,40 @@ def sample_family(vm_c0, n, gen, device, dtype=torch.float32, amp=(0.0, 0.3)):
 
 
 # ------------------------------------------------------------------ basis
-def _cholqr(Z, reps=2):
-    """Orthonormal columns of Z (n x r), CholQR2 with FP32 GEMMs on the
-    device and the r x r Cholesky factor in FP64 on the host."""
-    for _ in range(reps):
-        r = Z.shape[1]
-        G = torch.empty(r, r, device=Z.device)
-        gemm(Z, Z, ta=True, tb=True, out=G, engine=1)           # Z^T Z
-        Gh = G.double().cpu().numpy()
-        Gh = 0.5 * (Gh + Gh.T) + 1e-12 * np.trace(Gh) / r * np.eye(r)
-        L = np.linalg.cholesky(Gh)
-        Linv_t = torch.from_numpy(np.linalg.inv(L).T.copy()).float().to(Z.device)
-        Zn = torch.empty_like(Z)
-        gemm(Z, Linv_t, tb=True, out=Zn, engine=1)               # Z L^{-T}
-        Z = Zn
-    return Z
+def _orth(Z):
+    """Orthonormal columns spanning Z (n x r, device): Householder QR of the
+    tall-skinny block in FP64 on the host (r is a few hundred)."""
+    q, _ = np.linalg.qr(Z.double().cpu().numpy())
+    return torch.from_numpy(q).float().to(Z.device).contiguous()
 
 
 def fit_basis(X, k, oversample=64, power=2, gen=None):
-    """Top-k right singular vectors (k x n, orthonormal rows) of the sample
-    matrix X (ns x n, FP32, device) by a randomised SVD."""
+    """Leading right singular vectors (at most k, orthonormal rows) of the
+    sample matrix X (ns x n, FP32, device) by a randomised SVD."""
     ns, n = X.shape
     r = min(k + oversample, ns, n)
     Om = torch.randn(n, r, device=X.device, generator=gen)
     Y = torch.empty(ns, r, device=X.device)
     gemm(X, Om, tb=True, out=Y, engine=1)                        # X Omega
-    V = torch.empty(n, r, device=X.device)
     for it in range(power):
+        V = torch.empty(n, Y.shape[1], device=X.device)
         gemm(X, Y, ta=True, tb=True, out=V, engine=1)            # X^T Y
-        V = _cholqr(V)
+        V = _orth(V)
         if it < power - 1:
+            Y = torch.empty(ns, V.shape[1], device=X.device)
             gemm(X, V, tb=True, out=Y, engine=1)                 # X V
+    r = V.shape[1]
     B = torch.empty(ns, r, device=X.device)
     gemm(X, V, tb=True, out=B, engine=1)
     Cm = torch.empty(r, r, device=X.device)
     gemm(B, B, ta=True, tb=True, out=Cm, engine=1)               # B^T B
     w, U = np.linalg.eigh(Cm.double().cpu().numpy())
-    order = np.argsort(w)[::-1][:k]
+    order = np.argsort(w)[::-1]
+    order = order[w[order] > 1e-12 * w[order[0]]][:k]
     Uk = torch.from_numpy(U[:, order].copy()).float().to(X.device)
-    Vk = torch.empty(n, k, device=X.device)
+    Vk = torch.empty(n, Uk.shape[1], device=X.device)
     gemm(V, Uk, tb=True, out=Vk, engine=1)                       # V U_k
-    Vk = _cholqr(Vk, reps=1)
+    Vk = _orth(Vk)
     sv = np.sqrt(np.maximum(w[order], 0.0))
     return Vk.t().contiguous(), sv
 
@@ -221,6 +214,9 @@ class QSurrogate:
         Xq = (Qb / (rho * rho)[:, None].float()).contiguous()
         self.Bf, self.svf = fit_basis(Xf, self.k, gen=gen)
         self.Bq, self.svq = fit_basis(Xq, self.k, gen=gen)
+        # the data may support fewer modes than requested
+        self.k = min(self.Bf.shape[0], self.Bq.shape[0])
+        self.Bf, self.Bq = self.Bf[:self.k].contiguous(), self.Bq[:self.k].contiguous()
         # basis truncation error on the fit sample (relative L2 of Q)
         cq = torch.empty(nbasis, self.k, device=dev)
         gemm(Xq, self.Bq, out=cq, engine=1)
@@ -242,6 +238,8 @@ class QSurrogate:
         self.cscale = float(Cc.pow(2).mean().sqrt())
         X = ((A - self.mu) / self.sigma).bfloat16().contiguous()
         Tt = (Cc / self.cscale).contiguous()
+        # loss floor: 1% of the mean target energy
+        self.loss_delta = 0.01 * float(Tt.pow(2).sum(1).mean())
         del A, Cc
         t_data = time.time() - t0
         # 3. training (AdamW, relative MSE per sample)
@@ -252,19 +250,17 @@ class QSurrogate:
         t1 = time.time()
         for ep in range(epochs):
             perm = torch.randperm(nsamples, generator=gen, device=dev)
-            tot = 0.0
             nb = 0
             for i0 in range(0, nsamples - batch + 1, batch):
                 idx = perm[i0:i0 + batch]
                 xb, tb = X[idx].contiguous(), Tt[idx].contiguous()
                 y = self.forward_train(xb)
                 _lib.check(_lib.lib().bdgfs_relmse(y.data_ptr(), tb.data_ptr(), batch, self.k,
-                                                   1e-12, dy.data_ptr(), loss.data_ptr(),
+                                                   self.loss_delta, dy.data_ptr(), loss.data_ptr(),
                                                    _lib.stream_ptr()), 'bdgfs_relmse')
                 self.backward_train(dy)
                 step += 1
                 self.step(step, lr)
-                tot += float(loss.item()) if (nb % 50 == 0) else 0.0
                 nb += 1
             self.history.append(float(loss.item()))
             if log:
@@ -343,7 +339,7 @@ class QSurrogate:
         e = torch.cat(errs).numpy()
         return {'mean': float(e.mean()), 'median': float(np.median(e)),
                 'p90': float(np.percentile(e, 90)), 'aggregate': math.sqrt(num / den),
-                'n': int(nsamples)}
+                'n': int(nsamples), 'basis_truncation_q': getattr(self, 'basis_err_q', None)}
 
     def state_dict(self):
         keys = ('Bf', 'Bq', 'mu', 'sigma')
@@ -377,7 +373,6 @@ class HybridCollider:
         self.threshold, self.recheck, self.project = float(threshold), float(recheck), project
         self.spectral = VHSCollider([self.grid], model.device)
         self._n = 0
-        self.step_seed = 0
 
     def _alloc(self, ndof):
         if self._n >= ndof:
@@ -391,18 +386,22 @@ class HybridCollider:
         self.flag = torch.zeros(ndof, dtype=torch.uint8, device=dev)
         self.eps = torch.zeros(ndof, device=dev)
         self.recheck_err = torch.zeros(2, dtype=torch.float64, device=dev)
+        self.seed_dev = torch.zeros(1, dtype=torch.int64, device=dev)
         self.Qc = torch.empty(ndof, self.model.n, device=dev, dtype=self.grid.dtype)
         self._n = ndof
 
     def _args(self, ndof, seed):
+        """seed None: the re-check sample follows a device step counter
+        (advanced every call, also under CUDA-graph replay)."""
         g = self.grid
         return _lib.HybridArgs(
             ndof=ndof, Nv=g.Nv, fp64=int(g.dtype == torch.float64), c0=g.c0.data_ptr(),
             ginv=g.ginv.data_ptr(), cw=g.cw, threshold=self.threshold, recheck=self.recheck,
-            seed=seed, counts=self.counts.data_ptr(), sur_idx=self.sur_idx.data_ptr(),
+            seed=int(seed or 0), counts=self.counts.data_ptr(), sur_idx=self.sur_idx.data_ptr(),
             sur_inv_rho=self.inv_rho.data_ptr(), sur_rho2=self.rho2.data_ptr(),
             spec_idx=self.spec_idx.data_ptr(), flag=self.flag.data_ptr(),
-            eps=self.eps.data_ptr(), recheck_err=self.recheck_err.data_ptr())
+            eps=self.eps.data_ptr(), recheck_err=self.recheck_err.data_ptr(),
+            seed_dev=self.seed_dev.data_ptr() if seed is None else 0)
 
     def __call__(self, fin, fout, seed=None):
         """Q for every distribution of fin [ndof][n] into fout."""
@@ -410,8 +409,6 @@ class HybridCollider:
         f2, q2 = fin.reshape(-1, n), fout.reshape(-1, n)
         ndof = f2.shape[0]
         self._alloc(ndof)
-        seed = self.step_seed if seed is None else seed
-        self.step_seed += 1
         L = _lib.lib()
         args = self._args(ndof, seed)
         _lib.check(L.bdgfs_hybrid_classify(C.byref(args), f2.data_ptr(), _lib.stream_ptr()),

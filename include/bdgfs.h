@@ -264,6 +264,8 @@ typedef struct bdgfs_hybrid_args {
     uint8_t* flag;           /* [ndof] 0 spectral, 1 surrogate, 2 re-checked */
     float* eps;              /* optional [ndof] indicator values           */
     double* recheck_err;     /* optional [2]: sum |Qs-Qspec|^2, sum |Qspec|^2 */
+    uint64_t* seed_dev;      /* optional device step counter: used instead of
+                                seed, advanced by bdgfs_hybrid_scatter      */
 } bdgfs_hybrid_args;
 
 /* Indicator eps = |f - M[f]| / |f| per distribution and device-side lists. */
