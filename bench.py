@@ -10,9 +10,10 @@ two FR advection stages), captured as one CUDA graph.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Under torchrun every rank runs its own replica of the workload (no
-collective on the data path); value = total steps of all ranks / the
-slowest rank's device time.
+Under torchrun with N ranks the channel is N times longer, each rank owns
+one 16 x 8 slab (2048 DOFs, the single-GPU workload) and neighbouring slabs
+exchange face values over NCCL every stage (weak scaling); value = N *
+steps / the slowest rank's device time.
 """
 import argparse
 import json
@@ -293,7 +294,8 @@ def config_block(n):
     return {'workload': ('couette-2d: 16x8 quads P3 (2048 DOFs), Nv=24^3 on [-6,6]^3, '
                          'VHS omega=0.81, Nrho=12, M=12, diffuse walls +-0.3, SSP-RK2 dt=5e-4'),
             'ndof': 2048, 'Nv': 24, 'Nrho': 12, 'M': 12, 'order': 3, 'mesh': [16, 8],
-            'parallelism': f'replicas x{n}' if n > 1 else 'single GPU',
+            'parallelism': (f'{n} slabs of a {16 * n}x8 channel, NCCL face-value halo '
+                            'exchange per stage (weak scaling)') if n > 1 else 'single GPU',
             'l2': 'flushed before every timed step (256 MiB write); step working set 452 MB > L2'}
 
 
@@ -565,9 +567,21 @@ def run_gpu(args):
     cfg = Inifile(couette_ini('single'))
     be = CUDABackend(cfg)
     dev = be.device
-    mesh = StructuredMesh((WORK['nx'], WORK['ny']), (0.0, -0.5), (2.0, 0.5), periodic='x')
-    system = DGFSSystem(be, mesh, cfg, nreg=3)
+    if ws == 1:
+        mesh = StructuredMesh((WORK['nx'], WORK['ny']), (0.0, -0.5), (2.0, 0.5), periodic='x')
+        system = DGFSSystem(be, mesh, cfg, nreg=3)
+    else:
+        # weak scaling: a ws-times longer channel, one 16 x 8 slab per rank,
+        # face values of neighbouring slabs exchanged over NCCL every stage
+        from frfs_b200.partition import NCCLTransport, slab_partition
+        mesh = StructuredMesh((WORK['nx'] * ws, WORK['ny']), (0.0, -0.5), (2.0 * ws, 0.5),
+                              periodic='x')
+        parts = slab_partition(mesh, ws)
+        system = DGFSSystem(be, mesh, cfg, nreg=3, partition=(parts, rank),
+                            transport=NCCLTransport())
     integ = get_integrator(be, system, cfg)
+    if ws > 1:
+        integ.use_graph = False       # NCCL exchange inside the step: eager launches
     ndof = system.ele.neles * system.ele.nupts
     dt = WORK['dt']
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)

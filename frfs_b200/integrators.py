@@ -91,6 +91,9 @@ class BaseDGFSStepper:
         _lib.check(_lib.lib().bdgfs_residual(cur.data_ptr(), prev.data_ptr(), cur.numel(),
                                              int(cur.dtype == torch.float64), out.data_ptr(),
                                              _lib.stream_ptr()), 'bdgfs_residual')
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+            dist.all_reduce(out)                   # partitioned state: global norms
         o = out.cpu()
         return float((o[0] / o[1]).sqrt())
 
@@ -102,6 +105,9 @@ class BaseDGFSStepper:
                                                  int(u.dtype == torch.float64),
                                                  self._status.data_ptr(), _lib.stream_ptr()),
                    'bdgfs_status_check')
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+            dist.all_reduce(self._status, op=dist.ReduceOp.MAX)
         if int(self._status.item()):
             raise RuntimeError(f'NaNs detected at t = {self.tcurr}')
 

@@ -94,11 +94,20 @@ class DGFSSystem:
     velocitymeshcls = DGFSVelocityMesh
     scatteringcls = DGFSScatteringModel
 
-    def __init__(self, backend, mesh, cfg, nreg=3, initsoln=None):
+    def __init__(self, backend, mesh, cfg, nreg=3, initsoln=None, partition=None,
+                 transport=None):
+        """partition = (parts, rank): this system owns the elements
+        parts[rank] of the mesh (frfs_b200.partition); transport exchanges
+        the face values of neighbouring parts after disu."""
         self.backend, self.cfg, self.mesh = backend, cfg, mesh
         self.vm = self.velocitymeshcls(backend, cfg)
         order = cfg.getint('solver', 'order')
         self.geo = ElementGeometry(mesh, order)
+        self.domain = None
+        if partition is not None:
+            from .partition import LocalDomain
+            self.domain = self.geo = LocalDomain(self.geo, *partition)
+        self.transport = transport
         self.ele = self.elementscls(backend, self.geo, self.vm)
         self.ndims = self.geo.ndims
         # boundary conditions: every named boundary must be a configured wall
@@ -119,7 +128,14 @@ class DGFSSystem:
         # register banks [neles][nupts][Nv^3]
         E, U, nv = self.ele.neles, self.ele.nupts, self.vm.vsize()
         self.eles_scal_upts_inb_full = [backend.empty(E, U, nv) for _ in range(nreg)]
-        self._uf = backend.empty(E, self.ele.nfpts, nv)
+        nghost = self.domain.nghost if self.domain is not None else 0
+        self._uf_rows = backend.empty(E * self.ele.nfpts + nghost, nv)
+        self._uf = self._uf_rows[:E * self.ele.nfpts].view(E, self.ele.nfpts, nv)
+        self._send_rows = {}
+        if self.domain is not None:
+            for r, rows in self.domain.send.items():
+                self._send_rows[r] = torch.as_tensor(rows, dtype=torch.int64,
+                                                     device=backend.device)
         if initsoln is not None:
             self.eles_scal_upts_inb_full[0].copy_(torch.as_tensor(initsoln).to(
                 self.eles_scal_upts_inb_full[0]))
@@ -158,12 +174,16 @@ class DGFSSystem:
                                                  _lib.ptr(self._uf), _lib.stream_ptr()),
                    'bdgfs_fr_bc_update')
 
+    def _exchange(self):
+        if self.transport is not None:
+            self.transport.exchange(self)
+
     def _fused_rhs(self, a=0.0, b=1.0, x1=None, c1=0.0, x2=None, c2=0.0, out=None, **kw):
         u = self._bank(self._active[0])
         out = self._bank(self._active[1]) if out is None else out
         L = _lib.lib()
         rc = L.bdgfs_fr_rhs(_lib.ref(self.ele.struct), _lib.ref(self.walls.struct),
-                            u.data_ptr(), self._uf.data_ptr(), out.data_ptr(), float(a), float(b),
+                            u.data_ptr(), self._uf_rows.data_ptr(), out.data_ptr(), float(a), float(b),
                             x1.data_ptr() if x1 is not None else None, float(c1),
                             x2.data_ptr() if x2 is not None else None, float(c2),
                             _lib.stream_ptr())
@@ -176,6 +196,7 @@ class DGFSSystem:
         self._active = (uinbank, foutbank)
         k = self._kernels
         k['eles', 'disu']()
+        self._exchange()
         for name in (('eles', 'tdisf'), ('eles', 'tdivtpcorf'), ('iint', 'comm_flux'),
                      ('bcint', 'comm_flux'), ('eles', 'tdivtconf')):
             k[name](t=t, varidx=varidx)
@@ -197,8 +218,17 @@ class DGFSSystem:
     # -- fused stage used by the steppers ---------------------------------
     def advect_combine(self, t, uinbank, outbank, a, b, x1=None, c1=0.0, x2=None, c2=0.0):
         """out = a*u + b*L(u) + c1*x1 + c2*x2 (bc update included)."""
+        self.advect_begin(uinbank, outbank)
+        self.advect_end(t, a, b, x1, c1, x2, c2)
+
+    def advect_begin(self, uinbank, outbank):
+        """First half of a stage: face values of the stage input."""
         self._active = (uinbank, outbank)
         self._disu()
+
+    def advect_end(self, t, a, b, x1=None, c1=0.0, x2=None, c2=0.0):
+        """Second half: halo exchange, wall update, fused FR + combination."""
+        self._exchange()
         if self.walls.nwall:
             self._update_bc()
         self._fused_rhs(a=a, b=b, x1=self._bank(x1) if x1 is not None else None, c1=c1,

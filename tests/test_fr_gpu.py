@@ -137,3 +137,28 @@ def test_moments_and_residual(cuda):
     s.eles_scal_upts_inb_full[1].copy_(s.eles_scal_upts_inb_full[0] * 1.01)
     r = s.residual(1, 0).cpu().numpy()
     assert abs(np.sqrt(r[0] / r[1]) - 0.01) < 1e-10
+
+
+def test_partitioned_virtual_ranks_equal_single_domain(cuda):
+    """Three parts of a slab-partitioned mesh, stepped stage by stage with the
+    in-process halo exchange, reproduce the single-domain steps exactly."""
+    from frfs_b200.partition import LocalTransport, slab_partition, step_rk2_virtual
+    cfg, be, mesh, s = _system('quad', 3, 'single', Nv=16, Nrho=8, M=6, dev=5, shape=(6, 2))
+    _perturb(s, 4)
+    parts = slab_partition(mesh, 3)
+    systems = [DGFSSystem(be, mesh, cfg, nreg=3, partition=(parts, r)) for r in range(3)]
+    tr = LocalTransport(systems)
+    for r, sy in enumerate(systems):
+        sy.transport = tr
+        idx = torch.as_tensor(parts[r], device=be.device)
+        sy.eles_scal_upts_inb_full[0].copy_(s.eles_scal_upts_inb_full[0].index_select(0, idx))
+    integ = get_integrator(be, s, cfg)
+    integ.use_graph = False
+    for _ in range(2):
+        integ.step(0.0, 5e-4)
+        step_rk2_virtual(systems, 5e-4)
+    torch.cuda.synchronize()
+    for r, sy in enumerate(systems):
+        idx = torch.as_tensor(parts[r], device=be.device)
+        assert torch.equal(sy.eles_scal_upts_inb_full[0],
+                           s.eles_scal_upts_inb_full[0].index_select(0, idx)), r
