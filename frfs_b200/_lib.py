@@ -22,6 +22,7 @@ EXPORTS = (
     'bdgfs_moments', 'bdgfs_residual', 'bdgfs_status_check',
     'bdgfs_gemm', 'bdgfs_colsum', 'bdgfs_adamw', 'bdgfs_relmse',
     'bdgfs_hybrid_classify', 'bdgfs_hybrid_project', 'bdgfs_hybrid_scatter',
+    'bdgfs_hybrid_project_scatter', 'bdgfs_hybrid_heads',
 )
 
 
@@ -78,7 +79,9 @@ class HybridArgs(C.Structure):
                 ('threshold', C.c_float), ('recheck', C.c_float), ('seed', C.c_uint64),
                 ('counts', C.c_void_p), ('sur_idx', C.c_void_p), ('sur_inv_rho', C.c_void_p),
                 ('sur_rho2', C.c_void_p), ('spec_idx', C.c_void_p), ('flag', C.c_void_p),
-                ('eps', C.c_void_p), ('recheck_err', C.c_void_p), ('seed_dev', C.c_void_p)]
+                ('eps', C.c_void_p), ('recheck_err', C.c_void_p), ('seed_dev', C.c_void_p),
+                ('dev_rows', C.c_void_p), ('feat', C.c_void_p), ('feat_ld', C.c_int64),
+                ('sur_s', C.c_void_p)]
 
 
 _lib = None
@@ -118,6 +121,8 @@ def lib():
             'bdgfs_hybrid_classify': [vp, vp, vp],
             'bdgfs_hybrid_project': [vp, vp, vp],
             'bdgfs_hybrid_scatter': [vp, vp, vp, vp],
+            'bdgfs_hybrid_project_scatter': [vp, vp, vp, vp],
+            'bdgfs_hybrid_heads': [vp, vp, C.c_int64, C.c_int64, C.c_int32, vp, C.c_int64, vp],
             'bdgfs_colsum': [vp, i64, i64, vp, vp],
             'bdgfs_adamw': [vp, vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float,
                             C.c_float, C.c_float, i64, vp],

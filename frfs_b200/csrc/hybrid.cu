@@ -13,6 +13,8 @@
 // scatter: compact surrogate rows -> state-indexed Q, except on re-checked
 //   cells, which keep the spectral result; there the surrogate's error is
 //   accumulated (FP64 sums of |Qs - Qspec|^2 and |Qspec|^2).
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 
 namespace bdgfs {
@@ -64,8 +66,10 @@ __global__ void __launch_bounds__(256) indicator_kernel(const bdgfs_hybrid_args 
         }
     }
     block_sum<2>(e, red);
+    __shared__ int64_t s_pos;
     if (threadIdx.x == 0) {
         const double eps = (ok && e[1] > 0.0) ? sqrt(e[0] / e[1]) : 1e30;
+        s_pos = -1;
         if (h.eps) h.eps[dof] = float(eps);
         const bool sur = eps < double(h.threshold);
         const uint64_t seed = h.seed_dev ? *h.seed_dev : h.seed;
@@ -77,12 +81,36 @@ __global__ void __launch_bounds__(256) indicator_kernel(const bdgfs_hybrid_args 
             h.sur_idx[p] = int32_t(dof);
             h.sur_inv_rho[p] = float(1.0 / rho);
             h.sur_rho2[p] = float(rho * rho);
+            s_pos = p;
+            if (h.sur_s) h.sur_s[p] = float(sqrt(e[0]) / rho);
+            if (h.feat) {
+                __nv_bfloat16* fr = static_cast<__nv_bfloat16*>(h.feat) + p * h.feat_ld;
+                fr[0] = __float2bfloat16_rn(float(ux));
+                fr[1] = __float2bfloat16_rn(float(uy));
+                fr[2] = __float2bfloat16_rn(float(uz));
+                fr[3] = __float2bfloat16_rn(float(Tt - 1.0));
+            }
         }
         if (!sur || re) {
             const int64_t p = int64_t(atomicAdd(reinterpret_cast<unsigned long long*>(h.counts + 1), 1ull));
             h.spec_idx[p] = int32_t(dof);
         }
         if (re) atomicAdd(reinterpret_cast<unsigned long long*>(h.counts + 2), 1ull);
+    }
+    __syncthreads();
+    const int64_t p = s_pos;
+    if (p >= 0 && h.dev_rows) {
+        // (f - M[f]) / |f - M[f]|_2: direction of the deviation from the
+        // local Maxwellian (its size, at unit density, is sur_s)
+        __nv_bfloat16* out = static_cast<__nv_bfloat16*>(h.dev_rows) + p * n;
+        const double a = ok ? rho / pow(3.141592653589793 * Tt, 1.5) : 0.0, it = ok ? 1.0 / Tt : 0.0;
+        const double inv = (ok && e[0] > 0.0) ? 1.0 / sqrt(e[0]) : 0.0;
+        for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
+            const double cx = c0[v / (int64_t(Nv) * Nv)] - ux, cy = c0[(v / Nv) % Nv] - uy,
+                         cz = c0[v % Nv] - uz;
+            const double d = ok ? double(fd[v]) - a * exp(-(cx * cx + cy * cy + cz * cz) * it) : 0.0;
+            out[v] = __float2bfloat16_rn(float(d * inv));
+        }
     }
 }
 
@@ -153,6 +181,84 @@ __global__ void __launch_bounds__(256) scatter_kernel(const bdgfs_hybrid_args h,
     }
 }
 
+// Conservation projection of compact row `row` fused with its scatter:
+// the corrected values go straight to Q[sur_idx[row]] (or, on a re-checked
+// cell, are compared with the spectral values already there).
+template <typename T>
+__global__ void __launch_bounds__(256) project_scatter_kernel(const bdgfs_hybrid_args h,
+                                                              const T* __restrict__ Qc, T* __restrict__ Q)
+{
+    __shared__ double red[5 * 8];
+    const int64_t row = blockIdx.x;
+    if (row == 0 && threadIdx.x == 0 && h.seed_dev) *h.seed_dev += 1;   // next step's sample
+    const int64_t cnt = *h.counts;
+    if (row >= cnt) return;
+    const int Nv = h.Nv;
+    const int64_t n = int64_t(Nv) * Nv * Nv;
+    const T* src = Qc + row * n;
+    const int64_t dof = h.sur_idx[row];
+    T* dst = Q + dof * n;
+    const double* c0 = h.c0;
+    double m[5] = {0, 0, 0, 0, 0};
+    for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
+        const double cx = c0[v / (int64_t(Nv) * Nv)], cy = c0[(v / Nv) % Nv], cz = c0[v % Nv];
+        const double x = double(src[v]);
+        m[0] += x;
+        m[1] += cx * x;
+        m[2] += cy * x;
+        m[3] += cz * x;
+        m[4] += (cx * cx + cy * cy + cz * cz) * x;
+    }
+    block_sum<5>(m, red);
+    double lam[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        double t = 0.0;
+#pragma unroll
+        for (int j = 0; j < 5; ++j) t += h.ginv[i * 5 + j] * m[j];
+        lam[i] = t;
+    }
+    const bool re = h.flag[dof] == 2;
+    double e[2] = {0, 0};
+    for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
+        const double cx = c0[v / (int64_t(Nv) * Nv)], cy = c0[(v / Nv) % Nv], cz = c0[v % Nv];
+        const double c2 = cx * cx + cy * cy + cz * cz;
+        const T q = T(double(src[v]) - (lam[0] + lam[1] * cx + lam[2] * cy + lam[3] * cz + lam[4] * c2));
+        if (!re) {
+            dst[v] = q;
+        } else {
+            const double d = double(q) - double(dst[v]);
+            e[0] += d * d;
+            e[1] += double(dst[v]) * double(dst[v]);
+        }
+    }
+    if (!re) return;                                   // uniform per block
+    block_sum<2>(e, red);
+    if (threadIdx.x == 0 && h.recheck_err) {
+        atomicAdd(h.recheck_err, e[0]);
+        atomicAdd(h.recheck_err + 1, e[1]);
+    }
+}
+
+// out[m][j] = sum_i s_m^i Y[m][i*k + j]
+__global__ void __launch_bounds__(128) heads_kernel(const bdgfs_hybrid_args h, const float* __restrict__ Y,
+                                                    int64_t ldy, int64_t k, int nheads,
+                                                    __nv_bfloat16* __restrict__ out, int64_t ldo)
+{
+    const int64_t row = blockIdx.x;
+    if (row >= *h.counts) return;
+    const float s = h.sur_s[row];
+    const float* y = Y + row * ldy;
+    for (int64_t j = threadIdx.x; j < k; j += blockDim.x) {
+        float acc = 0.f, p = 1.f;
+        for (int i = 0; i < nheads; ++i) {
+            acc += p * y[i * k + j];
+            p *= s;
+        }
+        out[row * ldo + j] = __float2bfloat16_rn(acc);
+    }
+}
+
 }  // namespace bdgfs
 
 using namespace bdgfs;
@@ -211,5 +317,35 @@ extern "C" int32_t bdgfs_hybrid_scatter(const bdgfs_hybrid_args* h, const void* 
     else
         scatter_kernel<float><<<unsigned(h->ndof), 256, 0, st>>>(*h, static_cast<const float*>(Qc),
                                                                  static_cast<float*>(Q));
+    return cuda_status(cudaGetLastError());
+}
+
+extern "C" int32_t bdgfs_hybrid_project_scatter(const bdgfs_hybrid_args* h, const void* Qc, void* Q,
+                                                void* stream)
+{
+    int rc = check_h(h);
+    if (rc) return rc;
+    if (!Qc || !Q || !h->counts || !h->sur_idx || !h->flag || !h->ginv) return BDGFS_EINVAL;
+    if (h->ndof == 0) return BDGFS_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (h->fp64)
+        project_scatter_kernel<double><<<unsigned(h->ndof), 256, 0, st>>>(
+            *h, static_cast<const double*>(Qc), static_cast<double*>(Q));
+    else
+        project_scatter_kernel<float><<<unsigned(h->ndof), 256, 0, st>>>(
+            *h, static_cast<const float*>(Qc), static_cast<float*>(Q));
+    return cuda_status(cudaGetLastError());
+}
+
+extern "C" int32_t bdgfs_hybrid_heads(const bdgfs_hybrid_args* h, const float* Y, int64_t ldy, int64_t k,
+                                      int32_t nheads, void* out, int64_t ldo, void* stream)
+{
+    int rc = check_h(h);
+    if (rc) return rc;
+    if (!Y || !out || !h->counts || !h->sur_s || k < 1 || nheads < 1 || ldy < nheads * k || ldo < k)
+        return BDGFS_EINVAL;
+    if (h->ndof == 0) return BDGFS_OK;
+    heads_kernel<<<unsigned(h->ndof), 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        *h, Y, ldy, k, nheads, static_cast<__nv_bfloat16*>(out), ldo);
     return cuda_status(cudaGetLastError());
 }

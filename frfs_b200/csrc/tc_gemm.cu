@@ -21,6 +21,8 @@
 #include <cuda_bf16.h>
 
 #include "common.cuh"
+#include "tc_gemm.cuh"
+#include "tcgen05.cuh"
 
 namespace bdgfs {
 
@@ -30,88 +32,18 @@ constexpr int BM = 128, BN = 128, BK = 64;
 constexpr int THREADS = 128;
 constexpr int TILE_BYTES = BM * BK * 2;          // 16 KB per operand per stage
 constexpr uint32_t kWaitLimit = 1u << 26;        // bounded mbarrier polls
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p)
-{
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// K-major, no-swizzle smem descriptor (sm_100 matrix descriptor, version 1).
-__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
-{
-    uint64_t d = 0;
-    d |= uint64_t((saddr >> 4) & 0x3FFFu);
-    d |= uint64_t((lbo >> 4) & 0x3FFFu) << 16;
-    d |= uint64_t((sbo >> 4) & 0x3FFFu) << 32;
-    d |= uint64_t(1) << 46;                           // version (sm_100)
-    // base offset 0, lbo mode 0, layout type 0 (no swizzle)
-    return d;
-}
-
-// Instruction descriptor: D f32, A/B bf16, both K-major, M=128, N=128.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t(BN) >> 3) << 17) |
-                            ((uint32_t(BM) >> 4) << 24);
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
+constexpr uint32_t kIdesc = idesc_bf16(BM, BN);
 
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase)
 {
-    const uint32_t a = smem_u32(bar);
-    for (uint32_t it = 0; it < kWaitLimit; ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(a), "r"(phase)
-            : "memory");
-        if (done) return true;
-    }
+    for (uint32_t it = 0; it < kWaitLimit; ++it)
+        if (mbar_try(bar, phase)) return true;
     return false;
 }
 
-__device__ __forceinline__ void fence_async_smem()
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
 {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accum)
-{
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-        :
-        : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accum), "r"(0u), "r"(0u),
-          "r"(0u), "r"(0u)
-        : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar)
-{
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                     smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t addr, float (&v)[16])
-{
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-          "=r"(r[14]), "=r"(r[15])
-        : "r"(addr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+    return smem_desc(saddr, lbo, sbo, 0);
 }
 
 template <typename S>
@@ -144,15 +76,6 @@ __device__ __forceinline__ void load_tile(unsigned char* dst, const S* src, int6
         unsigned char* d = dst + ((r / 8) * (BK / 8) + kg) * 128 + (r % 8) * 16;
         *reinterpret_cast<uint4*>(d) = *reinterpret_cast<const uint4*>(h);
     }
-}
-
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
-__device__ __forceinline__ float gelu_grad(float x)
-{
-    // d/dx [x Phi(x)] = Phi(x) + x phi(x)
-    const float cdf = 0.5f * (1.f + erff(x * 0.70710678118654752f));
-    const float pdf = 0.3989422804014327f * __expf(-0.5f * x * x);
-    return cdf + x * pdf;
 }
 
 }  // namespace tc
@@ -218,7 +141,7 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
                 for (int ks = 0; ks < BK / 16; ++ks) {
                     const uint64_t ad = make_desc(a0 + ks * 256, 128, 1024);
                     const uint64_t bd = make_desc(b0 + ks * 256, 128, 1024);
-                    mma_bf16(tmem, ad, bd, (kt > 0 || ks > 0) ? 1u : 0u);
+                    mma_bf16(tmem, ad, bd, kIdesc, (kt > 0 || ks > 0) ? 1u : 0u);
                 }
                 mma_commit(&bar[s]);
             }
@@ -390,6 +313,10 @@ extern "C" int32_t bdgfs_gemm(const bdgfs_gemm_args* g, void* stream)
         f32_gemm_kernel<<<grid, 256, 0, st>>>(*g, static_cast<const float*>(g->A),
                                               static_cast<const float*>(g->B));
         return cuda_status(cudaGetLastError());
+    }
+    if (g->engine == 0) {           // TMA-fed persistent engine when the operands qualify
+        const int rc = tma_gemm(*g, st);
+        if (rc != BDGFS_EUNSUPPORTED) return rc;
     }
     if (g->beta != 0.f) return BDGFS_EUNSUPPORTED;
     const int64_t gy = (g->M + tc::BM - 1) / tc::BM, gx = (g->N + tc::BN - 1) / tc::BN;

@@ -23,7 +23,7 @@ def _operand(t, trans):
 
 def gemm(a, b, *, ta=False, tb=False, alpha=1.0, beta=0.0, bias=None, act=ACT_NONE,
          out=None, out_bf16=None, zout=None, zin=None, engine=0, status=None, stream=None,
-         arow=None, crow=None, row_scale=None, mcount=None, M=None):
+         arow=None, crow=None, row_scale=None, mcount=None, M=None, ldc=None):
     """out[m][n] = alpha * row_scale[m] * sum_k A(m,k) B(n,k) (+ beta*out)
     (+ bias) -> act.  A = a (M x K) or a^T if ta; B = b (N x K) or b^T if tb.
     arow gathers rows of A, crow scatters rows of the outputs, mcount is a
@@ -36,15 +36,22 @@ def gemm(a, b, *, ta=False, tb=False, alpha=1.0, beta=0.0, bias=None, act=ACT_NO
     N = b.shape[1] if tb else b.shape[0]
     if (b.shape[0] if tb else b.shape[1]) != K:
         raise ValueError('inner dimensions differ')
-    for t in (out, out_bf16, zout, zin, bias):
-        if t is not None and (not t.is_cuda or not t.is_contiguous()):
-            raise ValueError('outputs/bias must be contiguous CUDA tensors')
-    ldc = N
-    if crow is None:
-        if out is not None and out.shape != (M, N):
-            raise ValueError('out shape')
-        if out_bf16 is not None and out_bf16.shape != (M, N):
-            raise ValueError('out_bf16 shape')
+    if bias is not None and (not bias.is_cuda or not bias.is_contiguous()):
+        raise ValueError('bias must be a contiguous CUDA tensor')
+    # outputs: 2-D row-major views (unit column stride); one leading
+    # dimension for out/out_bf16 and one for zout/zin
+    lds = {}
+    for name, t in (('c', out), ('c', out_bf16), ('z', zout), ('z', zin)):
+        if t is None:
+            continue
+        if not t.is_cuda or t.dim() != 2 or t.stride(1) != 1 or t.shape[1] != N:
+            raise ValueError('outputs are 2-D CUDA views with N columns and unit column stride')
+        if crow is None and t.shape[0] != M:
+            raise ValueError('output rows differ from M')
+        if lds.setdefault(name, t.stride(0)) != t.stride(0):
+            raise ValueError('out and out_bf16 (zout and zin) must share a leading dimension')
+    ldc = lds.get('c', N) if ldc is None else int(ldc)
+    ldz = lds.get('z', N)
     for t, dt in ((arow, torch.int32), (crow, torch.int32), (row_scale, torch.float32),
                   (mcount, torch.int64)):
         if t is not None and (t.dtype != dt or not t.is_cuda):
@@ -56,7 +63,7 @@ def gemm(a, b, *, ta=False, tb=False, alpha=1.0, beta=0.0, bias=None, act=ACT_NO
                          cf32=out.data_ptr() if out is not None else 0,
                          cbf16=out_bf16.data_ptr() if out_bf16 is not None else 0, ldc=ldc,
                          zout=zout.data_ptr() if zout is not None else 0,
-                         zin=zin.data_ptr() if zin is not None else 0, ldz=N,
+                         zin=zin.data_ptr() if zin is not None else 0, ldz=ldz,
                          status=status.data_ptr() if status is not None else 0,
                          arow=arow.data_ptr() if arow is not None else 0,
                          crow=crow.data_ptr() if crow is not None else 0,

@@ -194,8 +194,13 @@ int32_t bdgfs_status_check(const void* a, int64_t n, int32_t fp64,
 /* C[m][n] = alpha * sum_k A(m,k) B(n,k) [+ beta*C] [+ bias[n]] -> act,
  * A(m,k) = A[m*sam + k*sak], B(n,k) = B[n*sbn + k*sbk].
  * engine 0: tcgen05 tensor cores, bf16 operands (float sources are rounded
- *           to bf16), FP32 accumulation, beta must be 0;
- * engine 1: FP32 CUDA cores (float sources only, no bias/act).
+ *           to bf16), FP32 accumulation, beta must be 0.  bf16 A and B with
+ *           unit K stride, K, sam, sbn multiples of 8, 16-byte aligned and
+ *           no arow run on the persistent TMA-fed engine (128x256 tiles);
+ *           everything else on the general loader (128x128 tiles);
+ * engine 1: FP32 CUDA cores (float sources only, no bias/act);
+ * engine 2: the general tcgen05 loader only (same results as engine 0 up
+ *           to FP32 summation order).
  * act 0: none; 1: GELU (erf form); 2: multiply by GELU'(zin[m][n]).
  * zout (optional, float, leading dim ldz) receives the pre-activation. */
 typedef struct bdgfs_gemm_args {
@@ -266,6 +271,14 @@ typedef struct bdgfs_hybrid_args {
     double* recheck_err;     /* optional [2]: sum |Qs-Qspec|^2, sum |Qspec|^2 */
     uint64_t* seed_dev;      /* optional device step counter: used instead of
                                 seed, advanced by bdgfs_hybrid_scatter      */
+    void* dev_rows;          /* optional bf16 [ndof][Nv^3]: for surrogate row p,
+                                d / |d|_2 with d = f/rho - M[f]/rho (the
+                                deviation from the local Maxwellian at unit
+                                density; zero when d = 0)                   */
+    void* feat;              /* optional bf16 rows with stride feat_ld: row p
+                                gets (u_x, u_y, u_z, T - 1) at columns 0..3 */
+    int64_t feat_ld;
+    float* sur_s;            /* optional [ndof]: |d|_2 of surrogate row p   */
 } bdgfs_hybrid_args;
 
 /* Indicator eps = |f - M[f]| / |f| per distribution and device-side lists. */
@@ -278,6 +291,16 @@ int32_t bdgfs_hybrid_project(const bdgfs_hybrid_args* h, void* Qc,
  * spectral; their surrogate error is accumulated in recheck_err). */
 int32_t bdgfs_hybrid_scatter(const bdgfs_hybrid_args* h, const void* Qc,
                              void* Q, void* stream);
+/* bdgfs_hybrid_project and bdgfs_hybrid_scatter in one pass (Qc is read,
+ * projected on the fly and written to Q; Qc itself is left unchanged). */
+int32_t bdgfs_hybrid_project_scatter(const bdgfs_hybrid_args* h,
+                                     const void* Qc, void* Q, void* stream);
+/* Combine the network's output heads of the first counts[0] rows:
+ * out[m][j] = sum_{i<nheads} sur_s[m]^i * Y[m][i*k + j]
+ * (Y float, leading dimension ldy; out bf16, leading dimension ldo). */
+int32_t bdgfs_hybrid_heads(const bdgfs_hybrid_args* h, const float* Y,
+                           int64_t ldy, int64_t k, int32_t nheads,
+                           void* out, int64_t ldo, void* stream);
 
 #ifdef __cplusplus
 }

@@ -66,3 +66,60 @@ def test_f32_gemm_engine(cuda):
     gemm(A, B, alpha=2.0, beta=1.0, out=C, engine=1)
     torch.cuda.synchronize()
     assert _rel(C, 2.0 * _ref(A, B) + 1.0) < 1e-6
+
+
+@pytest.mark.parametrize('M,N,K', [(2048, 2560, 256),      # 160 tiles: >1 tile per CTA
+                                   (300, 528, 13824),       # long K, ragged N
+                                   (1, 8, 8), (129, 257, 72)])
+def test_tma_engine_matches_general_engine(cuda, M, N, K):
+    """The persistent TMA-fed engine (engine 0 on contiguous bf16 operands)
+    against the general loader (engine 2) and an FP64 reference, with every
+    epilogue option: bias, GELU, pre-activation, bf16 copy, row scale,
+    scattered output rows and a device row count."""
+    g = torch.Generator(device=cuda).manual_seed(M * 7 + N + K)
+    Abig = torch.randn(M, K + 24, device=cuda, generator=g).bfloat16()
+    A = Abig[:, 8:8 + K]                                   # row stride K+24, 16-byte aligned start
+    B = torch.randn(N, K, device=cuda, generator=g).bfloat16()
+    bias = torch.randn(N, device=cuda, generator=g)
+    scale = torch.rand(M, device=cuda, generator=g) + 0.5
+    crow = torch.randperm(M, device=cuda, generator=g).to(torch.int32)
+    cnt = torch.tensor([max(1, M - 37)], dtype=torch.int64, device=cuda)
+    outs = []
+    for eng in (0, 2):
+        C = torch.zeros(M, N, device=cuda)
+        Cb = torch.zeros(M, N, device=cuda, dtype=torch.bfloat16)
+        Z = torch.zeros(M, N, device=cuda)
+        gemm(A, B, alpha=0.75, bias=bias, act=ACT_GELU, out=C, out_bf16=Cb, zout=Z,
+             row_scale=scale, crow=crow, mcount=cnt, engine=eng)
+        outs.append((C, Cb, Z))
+    torch.cuda.synchronize()
+    c = int(cnt.item())
+    z = 0.75 * scale[:c, None].double() * (A[:c].double() @ B.double().T) + bias.double()
+    h = 0.5 * z * (1 + torch.erf(z / math.sqrt(2)))
+    rows = crow[:c].long()
+    for C, Cb, Z in outs:
+        assert _rel(Z[rows], z) < 1e-5
+        assert _rel(C[rows], h) < 1e-5
+        assert _rel(Cb[rows].float(), h) < 1e-2
+        # rows past the device count are untouched
+        rest = torch.ones(M, dtype=torch.bool, device=cuda)
+        rest[rows] = False
+        assert float(C[rest].abs().sum()) == 0.0
+    assert _rel(outs[0][0][rows], outs[1][0][rows]) < 1e-5
+
+
+def test_tma_engine_gelu_grad_and_plain(cuda):
+    g = torch.Generator(device=cuda).manual_seed(3)
+    A = torch.randn(640, 1024, device=cuda, generator=g).bfloat16()
+    B = torch.randn(768, 1024, device=cuda, generator=g).bfloat16()
+    Z = torch.randn(640, 768, device=cuda, generator=g)
+    D = torch.empty(640, 768, device=cuda)
+    gemm(A, B, act=ACT_GELU_GRAD, zin=Z, out=D)
+    P = torch.empty(640, 768, device=cuda)
+    gemm(A, B, out=P)
+    torch.cuda.synchronize()
+    z = Z.double()
+    phi = torch.exp(-0.5 * z * z) / math.sqrt(2 * math.pi)
+    cdf = 0.5 * (1 + torch.erf(z / math.sqrt(2)))
+    assert _rel(D, _ref(A, B) * (cdf + z * phi)) < 1e-5
+    assert _rel(P, _ref(A, B)) < 1e-5
