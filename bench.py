@@ -17,6 +17,7 @@ steps / the slowest rank's device time.
 """
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -442,7 +443,7 @@ def surrogate_legs(flush, log=None):
     from frfs_b200.integrators import get_integrator
     from frfs_b200.mesh import StructuredMesh
     from frfs_b200.scattering import DGFSVHSGLLScatteringModel
-    from frfs_b200.surrogate import HybridCollider, QSurrogate, sample_family
+    from frfs_b200.surrogate import CAVITY, HybridCollider, QSurrogate, sample_family
     from frfs_b200.system import DGFSSystem
     from frfs_b200.velocitymesh import DGFSVelocityMesh
     cfg = Inifile(couette_ini('single'))
@@ -475,11 +476,23 @@ def surrogate_legs(flush, log=None):
         return tot / reps
     t_sur = timed(lambda: h(f, out))
     t_spec = timed(lambda: sm.collide(f, out, project=True, exact=False))
-    c4 = {'workload': ('surrogate of Q on Nv=24^3 (M=Nrho=12): 512-mode bases (randomised SVD), '
-                       '4-layer GELU MLP width 1024, BF16 weights / FP32 accumulation on tcgen05, '
+    # what the hidden layers add: the same model with only its linear skip path
+    saved = q.W[3].clone()
+    q.W[3][:, :q.w] = 0.0
+    q._fold()
+    lin = q.evaluate(10000, seed=1)
+    q.W[3].copy_(saved)
+    q._fold()
+    c4 = {'workload': ('surrogate of Q on Nv=24^3 (M=Nrho=12): 512-mode bases (randomised SVD) '
+                       'of the Maxwellian-deviation direction and of Q/rho^2, 4-layer GELU MLP '
+                       'width 1024 with a linear skip and 3 output heads '
+                       '(Q/rho^2 = y0 + s y1 + s^2 y2, s the deviation size), BF16 weights / '
+                       'FP32 accumulation on tcgen05, least-squares start of the skip path, '
                        'AdamW lr 3e-4, 20 epochs, 200000 training / 50000 held-out seeded '
                        'distributions of the Couette family, FP64 conservation projection'),
           'modes': q.k, 'train_steps': q.steps, 'train_s': q.train_seconds,
+          'ridge_start_train_rel_residual': q.ridge_residual,
+          'heldout_rel_l2_linear_skip_only': lin,
           'data_s': q.data_seconds, 'fit_s_total': t_fit,
           'final_loss': q.history[-1], 'first_epoch_loss': q.history[0],
           'heldout_rel_l2_vs_spectral_q': q.test_err,
@@ -507,7 +520,13 @@ uz = 0
 """
     names = {'x-': 'walls', 'x+': 'walls', 'y-': 'walls', 'y+': 'lid', 'z-': 'walls',
              'z+': 'walls'}
-    res = {}
+    # surrogate for the cavity's near-equilibrium cells (CAVITY family)
+    t0 = time.time()
+    qc = QSurrogate(sm.grid, nmodes=512, width=1024, family=CAVITY)
+    qc.fit(nsamples=200000, ntest=20000, epochs=20, lr=3e-4, batch=1024, seed=10)
+    t_fit_c = time.time() - t0
+    res, fields = {}, {}
+    nsteps, nwarm = 40, 3
     for mode in ('plain', 'hybrid'):
         c5cfg = Inifile(ini)
         c5cfg.set('solver-time-integrator', 'dt', '2e-4')
@@ -516,16 +535,17 @@ uz = 0
         s5 = DGFSSystem(be5, mesh, c5cfg, nreg=3)
         hc = None
         if mode == 'hybrid':
-            hc = HybridCollider(q, threshold=0.05, recheck=0.02)
+            hc = HybridCollider(qc, threshold=0.05, recheck=0.02)
             n3 = s5.vm.vsize()
             s5.sm.collide = lambda fin, fout, **kw: hc(fin.reshape(-1, n3), fout.reshape(-1, n3))
         integ = get_integrator(be5, s5, c5cfg)
-        for _ in range(3):
+        for _ in range(nwarm):
             integ.step(0.0, 2e-4)
         torch.cuda.synchronize()
-        steps = 10
         tot = 0.0
-        for _ in range(steps):
+        sur = rec = 0
+        num = den = 0.0
+        for _ in range(nsteps - nwarm):
             flush.fill_(1)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(st)
@@ -533,16 +553,36 @@ uz = 0
             b.record(st)
             torch.cuda.synchronize()
             tot += a.elapsed_time(b)
-        res[mode] = {'dg_steps_per_s': steps / (tot * 1e-3), 'ms_per_step': tot / steps}
+            if hc is not None:                       # stats of the step's last collide call
+                sst = hc.stats()
+                sur += sst['surrogate_cells']
+                rec += sst['rechecked_cells']
+                e = hc.recheck_err.cpu().tolist()
+                num += e[0]
+                den += e[1]
+        k = nsteps - nwarm
+        res[mode] = {'dg_steps_per_s': k / (tot * 1e-3), 'ms_per_step': tot / k}
         if hc is not None:
-            res[mode].update(hc.stats())
+            res[mode].update({'surrogate_cells_per_call': sur / k, 'rechecked_cells_per_call': rec / k,
+                              'spectral_cells_per_call': hc.stats()['spectral_cells'],
+                              'recheck_rel_l2': math.sqrt(num / den) if den > 0 else None})
+        rho, U, T, _, _ = s5.moments(integ._idxcurr)
+        fields[mode] = (rho.cpu(), U.cpu(), T.cpu())
         del s5, integ, hc
         torch.cuda.empty_cache()
+    (rp, up, Tp), (rh, uh, Th) = fields['plain'], fields['hybrid']
     c5 = {'workload': ('3-D lid-driven cavity: 8^3 hex P2 (13824 DOFs), Nv=24^3, VHS 0.81, '
                        'Nrho=M=12, lid 0.5, diffuse walls T=1, uniform Maxwellian start, SSP-RK2 '
-                       'dt=2e-4; hybrid threshold 0.05, 2% spectral re-check every call'),
+                       f'dt=2e-4, {nsteps} steps ({nwarm} untimed); hybrid threshold 0.05, 2% '
+                       'spectral re-check every call; surrogate trained on the cavity family'),
+          'surrogate_fit_s': t_fit_c, 'surrogate_heldout_rel_l2': qc.test_err,
           'plain_fp32_spectral': res['plain'], 'hybrid': res['hybrid'],
-          'speedup': res['hybrid']['dg_steps_per_s'] / res['plain']['dg_steps_per_s']}
+          'speedup': res['hybrid']['dg_steps_per_s'] / res['plain']['dg_steps_per_s'],
+          'fields_after_steps': nsteps,
+          'hybrid_vs_plain_max_abs_diff': {
+              'rho_rel': float(((rh - rp).abs() / rp).max()),
+              'U_over_lid_speed': float((uh - up).abs().max() / 0.5),
+              'T_rel': float(((Th - Tp).abs() / Tp).max())}}
     return c4, c5
 
 

@@ -233,6 +233,8 @@ class DGFSVHSGLLHybridScatteringModel(DGFSVHSGLLScatteringModel):
                            spectral operator every call (default 0.02)
       surrogate-file       trained model to load (torch.save of state_dict);
                            trained and saved there when absent
+      surrogate-family     training distributions: 'couette' (default) or
+                           'cavity' (see frfs_b200.surrogate)
       surrogate-nsamples / -epochs / -modes / -width / -lr / -seed
                            training settings (200000 / 20 / 512 / 1024 /
                            3e-4 / 0)
@@ -241,12 +243,17 @@ class DGFSVHSGLLHybridScatteringModel(DGFSVHSGLLScatteringModel):
 
     def perform_precomputation(self):
         import os
-        from .surrogate import HybridCollider, QSurrogate
+        from .surrogate import CAVITY, COUETTE, HybridCollider, QSurrogate
         super().perform_precomputation()
         cfg, sect = self.cfg, 'scattering-model'
+        fams = {'couette': COUETTE, 'cavity': CAVITY}
+        fam = cfg.get(sect, 'surrogate-family', 'couette')
+        if fam not in fams:
+            raise ValueError(f'surrogate-family {fam!r}: expected one of {sorted(fams)}')
         self.surrogate = QSurrogate(self.grid,
                                     nmodes=cfg.getint(sect, 'surrogate-modes', 512),
-                                    width=cfg.getint(sect, 'surrogate-width', 1024))
+                                    width=cfg.getint(sect, 'surrogate-width', 1024),
+                                    family=fams[fam])
         path = cfg.get(sect, 'surrogate-file', '')
         if path and os.path.exists(path):
             self.surrogate.load_state_dict(torch.load(path, map_location='cpu'))

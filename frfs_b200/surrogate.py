@@ -3,25 +3,40 @@
 The reference has no learned component; this module adds one on top of the
 spectral operator (``scattering.py``), which stays the fallback.
 
-Model (per distribution f on an Nv^3 grid, n = Nv^3):
-  rho   = sum(f) cw                                   (FP64 moments kernel)
-  a     = Bf (f / rho)                                 Bf: nmodes x n basis
-  y     = MLP((a - mu) / sigma)                        4 layers, GELU, width W
-  Q     = rho^2 * s * Bq^T y                           Bq: nmodes x n basis
-  Q    <- Q - phi^T G^{-1} (phi Q)                     FP64 conservation
-Q(lambda f) = lambda^2 Q(f) is used exactly (density normalisation).  The
-bases are fitted by a randomised SVD (Halko, Martinsson, Tropp 2011) whose
-GEMMs are the project's FP32 kernels; every training GEMM (forward and
-backward) runs on the tcgen05 tensor cores with BF16 operands and FP32
-accumulation; AdamW and the loss are project kernels too.
+Model (per distribution f on an Nv^3 grid, n = Nv^3).  With rho, u, T the
+FP64 moments of f and M the Maxwellian with those moments, the deviation
+at unit density d = f/rho - M/rho splits into its size s = |d|_2 and its
+direction d^ = d/s.  Q is bilinear, so exactly
+    Q(f)/rho^2 = Q(M/rho) + s 2 Q(M/rho, d^) + s^2 Q(d^, d^)
+               =   y0(u,T) + s y1(d^; u,T)  + s^2 y2(d^),
+and the network predicts the three heads from (d^, u, T):
+  x   = [(Bd d^ - mu)/sigma, u_x, u_y, u_z, T - 1, 0...]   Bd: k x n basis
+  h   = GELU layers 1..3 (width W) of x
+  Y   = W4 [h, x] + b4        (3 heads of k output modes; [h, x] is a linear
+                               skip from the input to the output layer)
+  y   = Y0 + s Y1 + s^2 Y2
+  Q   = rho^2 Bq^T (cscale y)                              Bq: k x n basis
+  Q  <- Q - phi^T G^{-1} (phi Q)                           FP64 conservation
+The bases are fitted by a randomised SVD (Halko, Martinsson, Tropp 2011)
+whose GEMMs are the project's FP32 kernels.  Inference and the training
+inputs run through the same kernels: the indicator kernel writes d^ (bf16),
+s, rho^2 and (u, T - 1); one tcgen05 GEMM projects d^ onto Bd/sigma with
+bias -mu/sigma; GELU layers, output heads, head combination and the
+reconstruction are tcgen05 GEMMs plus one small kernel; the FP64
+projection is fused with the scatter to the state's rows.  Training:
+least-squares start of the linear (skip) part, then AdamW on all
+parameters with the project's GEMM / GELU-gradient / loss / AdamW kernels.
 
-Training family (the Couette workload's distributions): Maxwellians with
-rho ~ U(0.8, 1.2), u_x ~ U(-0.35, 0.35), u_y, u_z ~ U(-0.05, 0.05),
-T ~ U(0.85, 1.2), multiplied by 1 + A P(xi), xi = (c - u)/sqrt(T), with P a
-random unit combination of the Grad-type shear-stress and heat-flux
-polynomials (xi_i xi_j, xi_i^2 - xi_j^2, xi_i (|xi|^2 - 5/2)), which leave
-rho, u and T unchanged, and A ~ U(0, 0.3); negative values are clipped.
-Labels are the FP32 spectral Q with the conservation projection.
+Families of training distributions (``Family``): Maxwellians with seeded
+rho, u, T multiplied by 1 + A P(xi), xi = (c - u)/sqrt(T), with P a random
+unit combination of the Grad-type shear-stress and heat-flux polynomials
+(xi_i xi_j, xi_i^2 - xi_j^2, xi_i (|xi|^2 - 5/2)), which leave rho, u and T
+unchanged, and negative values clipped.  ``COUETTE``: rho ~ U(0.8, 1.2),
+u_x ~ U(-0.35, 0.35), u_y, u_z ~ U(-0.05, 0.05), T ~ U(0.85, 1.2),
+A ~ U(0, 0.3).  ``CAVITY``: rho ~ U(0.9, 1.1), u_x ~ U(-0.55, 0.55),
+u_y, u_z ~ U(-0.3, 0.3), T ~ U(0.9, 1.1), log A ~ U(log 1e-4, log 0.15)
+(near-equilibrium cells of a lid-driven cavity).  Labels are the FP32
+spectral Q with the conservation projection.
 
 Hybrid step (``HybridCollider``): the Maxwellian-deviation indicator routes
 cells with eps < threshold to the surrogate and the rest to the spectral
@@ -33,6 +48,7 @@ hybrid step is captured in one CUDA graph.
 import ctypes as C
 import math
 import time
+from dataclasses import dataclass
 
 import numpy as np
 import torch
@@ -40,23 +56,39 @@ import torch
 from . import _lib
 from .gemm import ACT_GELU, ACT_GELU_GRAD, adamw, colsum, gemm
 
+NFEAT = 4            # (u_x, u_y, u_z, T - 1)
+NHEADS = 3           # y = Y0 + s Y1 + s^2 Y2
+
 
 # ------------------------------------------------------------------ data
-GRAD_POLYS = ('xy', 'xz', 'yz', 'xx-yy', 'yy-zz', 'qx', 'qy', 'qz')
+@dataclass(frozen=True)
+class Family:
+    rho: tuple = (0.8, 1.2)
+    ux: float = 0.35                  # half-ranges of the drift components
+    uy: float = 0.05
+    uz: float = 0.05
+    T: tuple = (0.85, 1.2)
+    amp: tuple = (0.0, 0.3)
+    log_amp: bool = False
 
 
-def sample_family(vm_c0, n, gen, device, dtype=torch.float32, amp=(0.0, 0.3)):
-    """n distributions of the Couette-type family on the grid with cell
-    centres vm_c0 (FP32 on the device)."""
+COUETTE = Family()
+CAVITY = Family(rho=(0.9, 1.1), ux=0.55, uy=0.3, uz=0.3, T=(0.9, 1.1), amp=(1e-4, 0.15),
+                log_amp=True)
+
+
+def sample_family(vm_c0, n, gen, device, dtype=torch.float32, amp=None, family=COUETTE):
+    """n distributions of a family on the grid with cell centres vm_c0."""
     c0 = torch.as_tensor(vm_c0, dtype=torch.float32, device=device)
     N = c0.numel()
     cx, cy, cz = c0.view(1, -1, 1, 1), c0.view(1, 1, -1, 1), c0.view(1, 1, 1, -1)
     U = lambda lo, hi, *s: lo + (hi - lo) * torch.rand(*s, generator=gen, device=device)
-    rho = U(0.8, 1.2, n).view(-1, 1, 1, 1)
-    ux = U(-0.35, 0.35, n).view(-1, 1, 1, 1)
-    uy = U(-0.05, 0.05, n).view(-1, 1, 1, 1)
-    uz = U(-0.05, 0.05, n).view(-1, 1, 1, 1)
-    T = U(0.85, 1.2, n).view(-1, 1, 1, 1)
+    fam = family
+    rho = U(*fam.rho, n).view(-1, 1, 1, 1)
+    ux = U(-fam.ux, fam.ux, n).view(-1, 1, 1, 1)
+    uy = U(-fam.uy, fam.uy, n).view(-1, 1, 1, 1)
+    uz = U(-fam.uz, fam.uz, n).view(-1, 1, 1, 1)
+    T = U(*fam.T, n).view(-1, 1, 1, 1)
     s = T.sqrt()
     xx, xy, xz = (cx - ux) / s, (cy - uy) / s, (cz - uz) / s
     x2 = xx * xx + xy * xy + xz * xz
@@ -66,7 +98,11 @@ def sample_family(vm_c0, n, gen, device, dtype=torch.float32, amp=(0.0, 0.3)):
              xz * (x2 - 2.5) / math.sqrt(2.5)]
     coef = torch.randn(n, len(polys), generator=gen, device=device)
     coef = coef / coef.norm(dim=1, keepdim=True)
-    A = U(amp[0], amp[1], n).view(-1, 1, 1, 1)
+    lo, hi = amp if amp is not None else fam.amp
+    if fam.log_amp and amp is None:
+        A = torch.exp(U(math.log(lo), math.log(hi), n)).view(-1, 1, 1, 1)
+    else:
+        A = U(lo, hi, n).view(-1, 1, 1, 1)
     P = sum(coef[:, i].view(-1, 1, 1, 1) * p for i, p in enumerate(polys))
     f = rho / (math.pi * T)**1.5 * torch.exp(-((cx - ux)**2 + (cy - uy)**2 + (cz - uz)**2) / T)
     f = f * torch.clamp(1.0 + A * P, min=0.0)
@@ -114,28 +150,41 @@ def fit_basis(X, k, oversample=64, power=2, gen=None):
 
 # ------------------------------------------------------------------ model
 class QSurrogate:
-    """Basis projection + MLP (BF16 weights, FP32 accumulation) for Q."""
+    """Basis projection + MLP with output heads (BF16 weights, FP32
+    accumulation on the tensor cores) for Q."""
 
-    def __init__(self, grid, nmodes=512, width=1024, device=None):
+    def __init__(self, grid, nmodes=512, width=1024, device=None, family=COUETTE):
         self.grid = grid                    # scattering.VHSGrid (tables, c0, ginv)
         self.Nv = grid.Nv
         self.n = grid.Nv**3
         self.k = nmodes
         self.w = width
+        self.family = family
         self.device = device or grid.phase.device
         self.trained = False
         self.history = []
 
+    @property
+    def kin(self):
+        """Input width: k deviation modes, NFEAT features, zero padding to a
+        multiple of 16."""
+        return (self.k + NFEAT + 15) // 16 * 16
+
+    @property
+    def ldx(self):
+        """Row length of the layer-4 input buffer [h3 (w) | x (kin)]."""
+        return self.w + self.kin
+
     # parameters ------------------------------------------------------
     def _init_params(self, gen):
-        dims = [(self.w, self.k), (self.w, self.w), (self.w, self.w), (self.k, self.w)]
+        dims = [(self.w, self.kin), (self.w, self.w), (self.w, self.w), (NHEADS * self.k, self.ldx)]
         self.W, self.b = [], []
         for (o, i) in dims:
             W = torch.randn(o, i, device=self.device, generator=gen) * math.sqrt(2.0 / i)
             self.W.append(W.contiguous())
             self.b.append(torch.zeros(o, device=self.device))
-        self.W[-1] *= 0.1
-        self.Wb = [W.bfloat16() for W in self.W]
+        self.W[3] *= 0.02
+        self._sync_bf16()
         self.mW = [torch.zeros_like(W) for W in self.W]
         self.vW = [torch.zeros_like(W) for W in self.W]
         self.mb = [torch.zeros_like(b) for b in self.b]
@@ -143,35 +192,42 @@ class QSurrogate:
         self.gW = [torch.zeros_like(W) for W in self.W]
         self.gb = [torch.zeros_like(b) for b in self.b]
 
+    def _sync_bf16(self):
+        self.Wb = [W.bfloat16() for W in self.W]
+
     # training forward / backward (project kernels) ---------------------
-    def forward_train(self, x_bf16):
-        """x (B x k, bf16, standardised) -> y (B x k FP32); keeps activations."""
-        B = x_bf16.shape[0]
+    def forward_train(self, xc):
+        """xc (B x ldx bf16; columns [w, ldx) hold the input x) -> heads Y
+        (B x 3k FP32).  Layer 3 writes its output into xc[:, :w]."""
+        B = xc.shape[0]
         dev = self.device
-        self._acts = [x_bf16]
+        x = xc[:, self.w:]
+        self._xc = xc
+        self._acts = [x]
         self._z = []
-        h = x_bf16
+        h = x
         for l in range(3):
             z = torch.empty(B, self.w, device=dev)
-            hn = torch.empty(B, self.w, device=dev, dtype=torch.bfloat16)
+            hn = xc[:, :self.w] if l == 2 else torch.empty(B, self.w, device=dev, dtype=torch.bfloat16)
             gemm(h, self.Wb[l], bias=self.b[l], act=ACT_GELU, zout=z, out_bf16=hn)
             self._z.append(z)
             self._acts.append(hn)
             h = hn
-        y = torch.empty(B, self.k, device=dev)
-        gemm(h, self.Wb[3], bias=self.b[3], out=y)
-        return y
+        Y = torch.empty(B, NHEADS * self.k, device=dev)
+        gemm(xc, self.Wb[3], bias=self.b[3], out=Y)
+        return Y
 
-    def backward_train(self, dy):
-        """Gradients of all parameters from dL/dy (B x k FP32)."""
-        g = dy
+    def backward_train(self, dY):
+        """Gradients of all parameters from dL/dY (B x 3k FP32)."""
+        g = dY
         for l in (3, 2, 1, 0):
-            h = self._acts[l]
+            h = self._xc if l == 3 else self._acts[l]
             gemm(g, h, ta=True, tb=True, out=self.gW[l])          # dW = g^T h
             colsum(g, self.gb[l])
             if l > 0:
                 gn = torch.empty(g.shape[0], self.w, device=self.device)
-                gemm(g, self.Wb[l], tb=True, act=ACT_GELU_GRAD, zin=self._z[l - 1], out=gn)
+                gemm(g, self.Wb[l][:, :self.w], tb=True, act=ACT_GELU_GRAD, zin=self._z[l - 1],
+                     out=gn)
                 g = gn
 
     def step(self, t, lr, wd=0.01):
@@ -179,90 +235,111 @@ class QSurrogate:
             adamw(self.W[l], self.gW[l], self.mW[l], self.vW[l], self.Wb[l], t, lr=lr, wd=wd)
             adamw(self.b[l], self.gb[l], self.mb[l], self.vb[l], None, t, lr=lr, wd=0.0)
 
-    # data -> coefficients ------------------------------------------------
+    @staticmethod
+    def combine(Y, s, k):
+        """y = Y0 + s Y1 + s^2 Y2 (training-side combination of the heads)."""
+        s = s[:, None]
+        return Y[:, :k] + s * Y[:, k:2 * k] + (s * s) * Y[:, 2 * k:3 * k]
+
+    def train_step(self, xc, s, t, dp, loss, step, lr):
+        """One AdamW step on a batch: xc input rows (x in columns [w, ldx)),
+        s deviation sizes, t targets.  Returns the combined prediction."""
+        B = xc.shape[0]
+        Y = self.forward_train(xc)
+        p = self.combine(Y, s, self.k).contiguous()
+        _lib.check(_lib.lib().bdgfs_relmse(p.data_ptr(), t.data_ptr(), B, self.k, self.loss_delta,
+                                           dp.data_ptr(), loss.data_ptr(), _lib.stream_ptr()),
+                   'bdgfs_relmse')
+        s1 = s[:, None]
+        self.backward_train(torch.cat([dp, s1 * dp, (s1 * s1) * dp], dim=1))
+        self.step(step, lr)
+        return p
+
+    # data ------------------------------------------------------------------
     def _labels(self, f, collider):
         Q = torch.empty_like(f)
         collider([(0, f, Q, None)], project=True, exact=False)
         return Q
 
-    def _coeffs(self, f, Q):
-        """FP32 coefficients a = Bf f/rho, c = Bq Q/rho^2 of a chunk."""
-        from .system import raw_moments
-        rho = (f.double().sum(1) * self.grid.cw).float()
-        a = torch.empty(f.shape[0], self.k, device=self.device)
-        c = torch.empty(f.shape[0], self.k, device=self.device)
-        gemm(f, self.Bf, out=a, engine=1)
-        gemm(Q, self.Bq, out=c, engine=1)
-        a /= rho[:, None]
-        c /= (rho * rho)[:, None]
-        return a, c
-
     def fit(self, nsamples=200000, ntest=50000, epochs=20, lr=3e-4, batch=1024, seed=0,
-            nbasis=16384, chunk=8192, log=None):
-        """Generate data, fit the bases, train the MLP (all on the device)."""
+            nbasis=16384, chunk=8192, log=None, ridge=1e-6):
+        """Generate data, fit the bases, train the network (all on the
+        device)."""
         from .scattering import VHSCollider
         dev = self.device
         gen = torch.Generator(device=dev).manual_seed(seed)
         col = VHSCollider([self.grid], dev)
         c0 = self.grid.c0.double().cpu().numpy()
+        enc = HybridCollider(self, threshold=float('inf'), recheck=0.0)
         t0 = time.time()
-        # 1. bases from a sample
-        fb = sample_family(c0, nbasis, gen, dev)
+        # 1. bases from a sample: deviation directions and Q / rho^2
+        fb = sample_family(c0, nbasis, gen, dev, family=self.family)
         Qb = self._labels(fb, col)
-        rho = fb.double().sum(1) * self.grid.cw
-        Xf = (fb / rho[:, None].float()).contiguous()
-        Xq = (Qb / (rho * rho)[:, None].float()).contiguous()
-        self.Bf, self.svf = fit_basis(Xf, self.k, gen=gen)
+        enc.classify(fb)
+        m = nbasis
+        idx = enc.sur_idx[:m].long()
+        Xd = enc.dev_rows[:m].float()
+        Xq = (Qb.index_select(0, idx) / enc.rho2[:m, None]).contiguous()
+        self.Bd, self.svd_ = fit_basis(Xd, self.k, gen=gen)
         self.Bq, self.svq = fit_basis(Xq, self.k, gen=gen)
-        # the data may support fewer modes than requested
-        self.k = min(self.Bf.shape[0], self.Bq.shape[0])
-        self.Bf, self.Bq = self.Bf[:self.k].contiguous(), self.Bq[:self.k].contiguous()
-        # basis truncation error on the fit sample (relative L2 of Q)
-        cq = torch.empty(nbasis, self.k, device=dev)
+        self.k = min(self.Bd.shape[0], self.Bq.shape[0])
+        self.Bd, self.Bq = self.Bd[:self.k].contiguous(), self.Bq[:self.k].contiguous()
+        # input standardisation of the deviation modes (folded into the
+        # projection: x = (Bd/sigma) d^ - mu/sigma)
+        a = torch.empty(m, self.k, device=dev)
+        gemm(Xd, self.Bd, out=a, engine=1)
+        self.mu = a.mean(0)
+        sd = a.std(0)
+        self.sigma = sd.clamp_min(1e-3 * float(sd.max()))
+        self._fold_input()
+        # basis truncation error of Q on the fit sample (relative L2)
+        cq = torch.empty(m, self.k, device=dev)
         gemm(Xq, self.Bq, out=cq, engine=1)
         Xr = torch.empty_like(Xq)
         gemm(cq, self.Bq, tb=True, out=Xr, engine=1)
         self.basis_err_q = float((Xr - Xq).norm() / Xq.norm())
-        del fb, Qb, Xf, Xq, Xr
-        # 2. training coefficients
-        A = torch.empty(nsamples, self.k, device=dev)
+        del fb, Qb, Xd, Xq, Xr, a, cq
+        # 2. training data through the inference encoder
+        X = torch.zeros(nsamples, self.kin, device=dev, dtype=torch.bfloat16)
+        S = torch.empty(nsamples, device=dev)
         Cc = torch.empty(nsamples, self.k, device=dev)
         for i0 in range(0, nsamples, chunk):
             m = min(chunk, nsamples - i0)
-            f = sample_family(c0, m, gen, dev)
-            a, c = self._coeffs(f, self._labels(f, col))
-            A[i0:i0 + m] = a
-            Cc[i0:i0 + m] = c
-        self.mu = A.mean(0)
-        self.sigma = A.std(0).clamp_min(1e-6 * float(A.std(0).max()))
+            f = sample_family(c0, m, gen, dev, family=self.family)
+            Q = self._labels(f, col)
+            x, s, rho2, idx = self.encode(f, enc)
+            X[i0:i0 + m] = x
+            S[i0:i0 + m] = s
+            Qs = (Q.index_select(0, idx.long()) / rho2[:, None]).contiguous()
+            gemm(Qs, self.Bq, out=Cc[i0:i0 + m], engine=1)
         self.cscale = float(Cc.pow(2).mean().sqrt())
-        X = ((A - self.mu) / self.sigma).bfloat16().contiguous()
         Tt = (Cc / self.cscale).contiguous()
-        # loss floor: 1% of the mean target energy
-        self.loss_delta = 0.01 * float(Tt.pow(2).sum(1).mean())
-        del A, Cc
+        del Cc
+        # per-row relative loss, floored at 1e-4 of the mean target energy
+        self.loss_delta = 1e-4 * float(Tt.pow(2).sum(1).mean())
         t_data = time.time() - t0
-        # 3. training (AdamW, relative MSE per sample)
+        # 3. parameters: random MLP, least-squares start of the skip path
         self._init_params(gen)
-        loss = torch.zeros(1, dtype=torch.float64, device=dev)
-        dy = torch.empty(batch, self.k, device=dev)
-        step = 0
         t1 = time.time()
+        self.ridge_residual = self._ridge_init(X, S, Tt, ridge)
+        # 4. AdamW on the per-row relative squared error of y
+        loss = torch.zeros(1, dtype=torch.float64, device=dev)
+        tot = torch.zeros(1, dtype=torch.float64, device=dev)
+        xc = torch.zeros(batch, self.ldx, device=dev, dtype=torch.bfloat16)
+        dp = torch.empty(batch, self.k, device=dev)
+        step = 0
         for ep in range(epochs):
             perm = torch.randperm(nsamples, generator=gen, device=dev)
+            tot.zero_()
             nb = 0
             for i0 in range(0, nsamples - batch + 1, batch):
-                idx = perm[i0:i0 + batch]
-                xb, tb = X[idx].contiguous(), Tt[idx].contiguous()
-                y = self.forward_train(xb)
-                _lib.check(_lib.lib().bdgfs_relmse(y.data_ptr(), tb.data_ptr(), batch, self.k,
-                                                   self.loss_delta, dy.data_ptr(), loss.data_ptr(),
-                                                   _lib.stream_ptr()), 'bdgfs_relmse')
-                self.backward_train(dy)
+                idb = perm[i0:i0 + batch]
+                xc[:, self.w:] = X[idb]
                 step += 1
-                self.step(step, lr)
+                self.train_step(xc, S[idb], Tt[idb].contiguous(), dp, loss, step, lr)
+                tot += loss
                 nb += 1
-            self.history.append(float(loss.item()))
+            self.history.append(float(tot.item()) / max(nb, 1))
             if log:
                 log(f'epoch {ep}: loss {self.history[-1]:.4e}')
         torch.cuda.synchronize(dev)
@@ -271,49 +348,90 @@ class QSurrogate:
         self.steps = step
         self._fold()
         self.trained = True
-        # 4. held-out evaluation against the spectral operator
+        # 5. held-out evaluation against the spectral operator
         self.test_err = self.evaluate(ntest, seed=seed + 1, chunk=chunk)
         return self
 
+    def _ridge_init(self, X, S, Tt, lam):
+        """Least-squares start: the output layer's skip columns and bias
+        solve min |[x, 1, s x, s, s^2 x, s^2] Theta - t|^2 (+ lam |Theta|^2)
+        over the training set (normal equations on the FP32 GEMM engine,
+        FP64 solve on the host).  Returns the relative residual."""
+        dev = self.device
+        k, kin, w = self.k, self.kin, self.w
+        ns = X.shape[0]
+        nf = NHEADS * (kin + 1)
+        G = torch.zeros(nf, nf, device=dev, dtype=torch.float64)
+        R = torch.zeros(nf, k, device=dev, dtype=torch.float64)
+        ch = 16384
+        for i0 in range(0, ns, ch):
+            x = X[i0:i0 + ch].float()
+            s = S[i0:i0 + ch, None]
+            one = torch.ones_like(s)
+            F = torch.cat([x, one, s * x, s, s * s * x, s * s], dim=1).contiguous()
+            g = torch.empty(nf, nf, device=dev)
+            gemm(F, F, ta=True, tb=True, out=g, engine=1)
+            r = torch.empty(nf, k, device=dev)
+            gemm(F, Tt[i0:i0 + ch], ta=True, tb=True, out=r, engine=1)
+            G += g.double()
+            R += r.double()
+        Gh, Rh = G.cpu().numpy(), R.cpu().numpy()
+        Gh += lam * np.trace(Gh) / nf * np.eye(nf)
+        Th = np.linalg.solve(Gh, Rh)                      # nf x k
+        tt = float(Tt.double().pow(2).sum())
+        res = float(np.sum(Th * (Gh @ Th)) - 2 * np.sum(Th * Rh)) + tt
+        Th = torch.from_numpy(Th).float().to(dev)
+        for hd in range(NHEADS):
+            blk = Th[hd * (kin + 1):(hd + 1) * (kin + 1)]
+            self.W[3][hd * k:(hd + 1) * k, w:] = blk[:kin].t()
+            self.b[3][hd * k:(hd + 1) * k] = blk[kin]
+        self._sync_bf16()
+        return math.sqrt(max(res, 0.0) / tt)
+
+    def _fold_input(self):
+        self.BdT_bf16 = (self.Bd / self.sigma[:, None]).bfloat16().contiguous()     # k x n
+        self.bias_in = (-self.mu / self.sigma).contiguous()
+
     def _fold(self):
-        """Fold input standardisation into layer 1 and the output scale into
-        the reconstruction basis (exact rewrites of the trained model)."""
-        W1 = self.W[0] / self.sigma[None, :]
-        b1 = self.b[0] - W1 @ self.mu
-        self.inf_W = [W1.bfloat16().contiguous()] + [w.bfloat16().contiguous() for w in self.W[1:]]
-        self.inf_b = [b1.contiguous()] + [b.contiguous() for b in self.b[1:]]
-        self.BfT_bf16 = self.Bf.bfloat16().contiguous()                 # k x n
+        """Inference copies: bf16 weights; output scale folded into the
+        reconstruction basis."""
+        self._fold_input()
+        self.inf_W = [w.bfloat16().contiguous() for w in self.W]
+        self.inf_b = [b.contiguous() for b in self.b]
         self.BqT_bf16 = (self.Bq.t() * self.cscale).bfloat16().contiguous()   # n x k
 
     # inference ------------------------------------------------------------
-    def infer(self, f, rows, inv_rho, rho2, out, count=None, M=None):
-        """Compact surrogate Q: out[m] = Q of f[rows[m]] (m < count) on the
-        tensor cores; no conservation projection here."""
-        M = M if M is not None else rows.numel()
-        dev = self.device
-        bufs = self._bufs(M)
-        gemm(f, self.BfT_bf16, arow=rows, row_scale=inv_rho, mcount=count, M=M,
-             out_bf16=bufs[0])
-        h = bufs[0]
+    def encode(self, f, enc):
+        """Classify every row of f as surrogate (threshold inf) and return
+        the network input x (bf16, compact order), s, rho^2 and the row map."""
+        enc.classify(f)
+        m = f.shape[0]
+        self.project_input(enc, m)
+        return enc.xc[:m, self.w:], enc.sur_s[:m], enc.rho2[:m], enc.sur_idx[:m]
+
+    def project_input(self, enc, M):
+        gemm(enc.dev_rows[:M], self.BdT_bf16, bias=self.bias_in, mcount=enc.counts[0:1],
+             out_bf16=enc.xc[:M, self.w:self.w + self.k])
+
+    def infer(self, enc, M):
+        """Compact surrogate Q of the rows the indicator selected (device
+        count) into enc.Qc; no conservation projection here."""
+        cnt = enc.counts[0:1]
+        self.project_input(enc, M)
+        xc = enc.xc[:M]
+        h = xc[:, self.w:]
         for l in range(3):
-            gemm(h, self.inf_W[l], bias=self.inf_b[l], act=ACT_GELU, mcount=count,
-                 out_bf16=bufs[1 + (l % 2)])
-            h = bufs[1 + (l % 2)]
-        gemm(h, self.inf_W[3], bias=self.inf_b[3], mcount=count, out_bf16=bufs[3])
-        gemm(bufs[3], self.BqT_bf16, row_scale=rho2, mcount=count, out=out)
-        return out
+            hn = xc[:, :self.w] if l == 2 else enc.h[l][:M]
+            gemm(h, self.inf_W[l], bias=self.inf_b[l], act=ACT_GELU, mcount=cnt, out_bf16=hn)
+            h = hn
+        gemm(xc, self.inf_W[3], bias=self.inf_b[3], mcount=cnt, out=enc.Y[:M])
+        _lib.check(_lib.lib().bdgfs_hybrid_heads(C.byref(enc.args), enc.Y.data_ptr(),
+                                                 NHEADS * self.k, self.k, NHEADS,
+                                                 enc.yb.data_ptr(), self.k, _lib.stream_ptr()),
+                   'bdgfs_hybrid_heads')
+        gemm(enc.yb[:M], self.BqT_bf16, row_scale=enc.rho2, mcount=cnt, out=enc.Qc[:M])
 
-    def _bufs(self, M):
-        if getattr(self, '_buf_M', 0) < M:
-            dev = self.device
-            self._buf = [torch.empty(M, self.k, device=dev, dtype=torch.bfloat16),
-                         torch.empty(M, self.w, device=dev, dtype=torch.bfloat16),
-                         torch.empty(M, self.w, device=dev, dtype=torch.bfloat16),
-                         torch.empty(M, self.k, device=dev, dtype=torch.bfloat16)]
-            self._buf_M = M
-        return [b[:M] for b in self._buf]
-
-    def evaluate(self, nsamples, seed=1, chunk=8192):
+    def evaluate(self, nsamples, seed=1, chunk=8192, family=None):
         """Relative L2 error of the surrogate (with conservation projection)
         against the FP32 spectral Q on seeded held-out distributions:
         returns dict(mean, median, p90, aggregate)."""
@@ -327,7 +445,7 @@ class QSurrogate:
         h = HybridCollider(self, threshold=float('inf'), recheck=0.0)
         for i0 in range(0, nsamples, chunk):
             m = min(chunk, nsamples - i0)
-            f = sample_family(c0, m, gen, dev)
+            f = sample_family(c0, m, gen, dev, family=family or self.family)
             Qs = self._labels(f, col)
             Qh = torch.empty_like(f)
             h.collide_surrogate_only(f, Qh)
@@ -342,7 +460,7 @@ class QSurrogate:
                 'n': int(nsamples), 'basis_truncation_q': getattr(self, 'basis_err_q', None)}
 
     def state_dict(self):
-        keys = ('Bf', 'Bq', 'mu', 'sigma')
+        keys = ('Bd', 'Bq', 'mu', 'sigma')
         d = {k: getattr(self, k).cpu() for k in keys}
         d.update(W=[w.cpu() for w in self.W], b=[b.cpu() for b in self.b], cscale=self.cscale,
                  k=self.k, w=self.w, Nv=self.Nv)
@@ -350,11 +468,13 @@ class QSurrogate:
 
     def load_state_dict(self, d):
         dev = self.device
-        for k in ('Bf', 'Bq', 'mu', 'sigma'):
+        for k in ('Bd', 'Bq', 'mu', 'sigma'):
             setattr(self, k, d[k].to(dev))
+        self.k, self.w = int(d['k']), int(d['w'])
         self.W = [w.to(dev) for w in d['W']]
         self.b = [b.to(dev) for b in d['b']]
         self.cscale = float(d['cscale'])
+        self._sync_bf16()
         self._fold()
         self.trained = True
         return self
@@ -373,27 +493,42 @@ class HybridCollider:
         self.threshold, self.recheck, self.project = float(threshold), float(recheck), project
         self.spectral = VHSCollider([self.grid], model.device)
         self._n = 0
+        self._net = None
 
     def _alloc(self, ndof):
-        if self._n >= ndof:
-            return
-        dev = self.model.device
-        self.counts = torch.zeros(3, dtype=torch.int64, device=dev)
-        self.sur_idx = torch.zeros(ndof, dtype=torch.int32, device=dev)
-        self.spec_idx = torch.zeros(ndof, dtype=torch.int32, device=dev)
-        self.inv_rho = torch.zeros(ndof, device=dev)
-        self.rho2 = torch.zeros(ndof, device=dev)
-        self.flag = torch.zeros(ndof, dtype=torch.uint8, device=dev)
-        self.eps = torch.zeros(ndof, device=dev)
-        self.recheck_err = torch.zeros(2, dtype=torch.float64, device=dev)
-        self.seed_dev = torch.zeros(1, dtype=torch.int64, device=dev)
-        self.Qc = torch.empty(ndof, self.model.n, device=dev, dtype=self.grid.dtype)
-        self._n = ndof
+        if self._n < ndof:
+            dev = self.model.device
+            n = self.model.n
+            self.counts = torch.zeros(3, dtype=torch.int64, device=dev)
+            self.sur_idx = torch.zeros(ndof, dtype=torch.int32, device=dev)
+            self.spec_idx = torch.zeros(ndof, dtype=torch.int32, device=dev)
+            self.inv_rho = torch.zeros(ndof, device=dev)
+            self.rho2 = torch.zeros(ndof, device=dev)
+            self.sur_s = torch.zeros(ndof, device=dev)
+            self.flag = torch.zeros(ndof, dtype=torch.uint8, device=dev)
+            self.eps = torch.zeros(ndof, device=dev)
+            self.recheck_err = torch.zeros(2, dtype=torch.float64, device=dev)
+            self.seed_dev = torch.zeros(1, dtype=torch.int64, device=dev)
+            self.dev_rows = torch.zeros(ndof, n, device=dev, dtype=torch.bfloat16)
+            self._n = ndof
+            self._net = None
+        m = self.model
+        shape = (self._n, m.k, m.w, m.kin)
+        if self._net != shape:
+            dev = m.device
+            ndof = self._n
+            self.xc = torch.zeros(ndof, m.ldx, device=dev, dtype=torch.bfloat16)
+            self.h = [torch.empty(ndof, m.w, device=dev, dtype=torch.bfloat16) for _ in range(2)]
+            self.Y = torch.empty(ndof, NHEADS * m.k, device=dev)
+            self.yb = torch.empty(ndof, m.k, device=dev, dtype=torch.bfloat16)
+            self.Qc = torch.empty(ndof, m.n, device=dev, dtype=self.grid.dtype)
+            self._net = shape
 
     def _args(self, ndof, seed):
         """seed None: the re-check sample follows a device step counter
         (advanced every call, also under CUDA-graph replay)."""
-        g = self.grid
+        g, m = self.grid, self.model
+        feat = self.xc.data_ptr() + 2 * (m.w + m.k)          # columns [w+k, w+k+4) of xc
         return _lib.HybridArgs(
             ndof=ndof, Nv=g.Nv, fp64=int(g.dtype == torch.float64), c0=g.c0.data_ptr(),
             ginv=g.ginv.data_ptr(), cw=g.cw, threshold=self.threshold, recheck=self.recheck,
@@ -401,29 +536,33 @@ class HybridCollider:
             sur_inv_rho=self.inv_rho.data_ptr(), sur_rho2=self.rho2.data_ptr(),
             spec_idx=self.spec_idx.data_ptr(), flag=self.flag.data_ptr(),
             eps=self.eps.data_ptr(), recheck_err=self.recheck_err.data_ptr(),
-            seed_dev=self.seed_dev.data_ptr() if seed is None else 0)
+            seed_dev=self.seed_dev.data_ptr() if seed is None else 0,
+            dev_rows=self.dev_rows.data_ptr(), feat=feat, feat_ld=m.ldx,
+            sur_s=self.sur_s.data_ptr())
+
+    def classify(self, fin, seed=None):
+        f2 = fin.reshape(-1, self.model.n)
+        ndof = f2.shape[0]
+        self._alloc(ndof)
+        self.args = self._args(ndof, seed)
+        _lib.check(_lib.lib().bdgfs_hybrid_classify(C.byref(self.args), f2.data_ptr(),
+                                                    _lib.stream_ptr()), 'bdgfs_hybrid_classify')
+        return ndof
 
     def __call__(self, fin, fout, seed=None):
         """Q for every distribution of fin [ndof][n] into fout."""
         n = self.model.n
         f2, q2 = fin.reshape(-1, n), fout.reshape(-1, n)
-        ndof = f2.shape[0]
-        self._alloc(ndof)
+        ndof = self.classify(f2, seed)
         L = _lib.lib()
-        args = self._args(ndof, seed)
-        _lib.check(L.bdgfs_hybrid_classify(C.byref(args), f2.data_ptr(), _lib.stream_ptr()),
-                   'bdgfs_hybrid_classify')
         # spectral cells (incl. re-checks): index list + device count
         self.spectral([(0, f2, q2, None)], project=self.project, exact=False,
                       index=self.spec_idx, count=self.counts[1:2])
-        # surrogate cells: compact rows, projection, scatter
-        self.model.infer(f2, self.sur_idx, self.inv_rho, self.rho2, self.Qc[:ndof],
-                         count=self.counts[0:1], M=ndof)
-        if self.project:
-            _lib.check(L.bdgfs_hybrid_project(C.byref(args), self.Qc.data_ptr(), _lib.stream_ptr()),
-                       'bdgfs_hybrid_project')
-        _lib.check(L.bdgfs_hybrid_scatter(C.byref(args), self.Qc.data_ptr(), q2.data_ptr(),
-                                          _lib.stream_ptr()), 'bdgfs_hybrid_scatter')
+        # surrogate cells: compact rows, then projection fused with the scatter
+        self.model.infer(self, ndof)
+        fn = L.bdgfs_hybrid_project_scatter if self.project else L.bdgfs_hybrid_scatter
+        _lib.check(fn(C.byref(self.args), self.Qc.data_ptr(), q2.data_ptr(), _lib.stream_ptr()),
+                   'bdgfs_hybrid_project_scatter')
 
     def collide_surrogate_only(self, fin, fout):
         """Every cell through the surrogate (evaluation helper)."""

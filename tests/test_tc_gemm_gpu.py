@@ -97,15 +97,16 @@ def test_tma_engine_matches_general_engine(cuda, M, N, K):
     z = 0.75 * scale[:c, None].double() * (A[:c].double() @ B.double().T) + bias.double()
     h = 0.5 * z * (1 + torch.erf(z / math.sqrt(2)))
     rows = crow[:c].long()
+    tol = 1e-5 * max(1.0, math.sqrt(K / 1024))     # FP32 accumulation over K
     for C, Cb, Z in outs:
-        assert _rel(Z[rows], z) < 1e-5
-        assert _rel(C[rows], h) < 1e-5
+        assert _rel(Z[rows], z) < tol
+        assert _rel(C[rows], h) < tol
         assert _rel(Cb[rows].float(), h) < 1e-2
         # rows past the device count are untouched
         rest = torch.ones(M, dtype=torch.bool, device=cuda)
         rest[rows] = False
         assert float(C[rest].abs().sum()) == 0.0
-    assert _rel(outs[0][0][rows], outs[1][0][rows]) < 1e-5
+    assert _rel(outs[0][0][rows], outs[1][0][rows]) < tol
 
 
 def test_tma_engine_gelu_grad_and_plain(cuda):
