@@ -492,6 +492,7 @@ def surrogate_legs(flush, log=None):
                        'distributions of the Couette family, FP64 conservation projection'),
           'modes': q.k, 'train_steps': q.steps, 'train_s': q.train_seconds,
           'ridge_start_train_rel_residual': q.ridge_residual,
+          'basis_truncation_heads': q.basis_err_heads,
           'heldout_rel_l2_linear_skip_only': lin,
           'data_s': q.data_seconds, 'fit_s_total': t_fit,
           'final_loss': q.history[-1], 'first_epoch_loss': q.history[0],
@@ -576,6 +577,8 @@ uz = 0
                        f'dt=2e-4, {nsteps} steps ({nwarm} untimed); hybrid threshold 0.05, 2% '
                        'spectral re-check every call; surrogate trained on the cavity family'),
           'surrogate_fit_s': t_fit_c, 'surrogate_heldout_rel_l2': qc.test_err,
+          'surrogate_basis_truncation_heads': qc.basis_err_heads,
+          'surrogate_final_loss': qc.history[-1], 'surrogate_first_epoch_loss': qc.history[0],
           'plain_fp32_spectral': res['plain'], 'hybrid': res['hybrid'],
           'speedup': res['hybrid']['dg_steps_per_s'] / res['plain']['dg_steps_per_s'],
           'fields_after_steps': nsteps,

@@ -29,18 +29,34 @@ __device__ __forceinline__ uint32_t mix32(uint64_t x)
     return uint32_t(x >> 32);
 }
 
+constexpr int kMaxNv = 64;
+
+// velocity index v = (ix*Nv + iy)*Nv + iz, 32-bit arithmetic
+__device__ __forceinline__ void vsplit(uint32_t v, uint32_t Nv, uint32_t& ix, uint32_t& iy, uint32_t& iz)
+{
+    const uint32_t q = v / Nv;
+    iz = v - q * Nv;
+    ix = q / Nv;
+    iy = q - ix * Nv;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) indicator_kernel(const bdgfs_hybrid_args h, const T* __restrict__ f)
 {
     __shared__ double red[8 * 8];
+    __shared__ double cs[kMaxNv], ex[3][kMaxNv];
+    __shared__ int64_t s_pos;
     const int64_t dof = blockIdx.x;
     const int Nv = h.Nv;
-    const int64_t n = int64_t(Nv) * Nv * Nv;
-    const T* fd = f + dof * n;
-    const double* c0 = h.c0;
+    const int n = Nv * Nv * Nv;
+    const T* fd = f + dof * int64_t(n);
+    for (int i = threadIdx.x; i < Nv; i += blockDim.x) cs[i] = h.c0[i];
+    __syncthreads();
     double m[5] = {0, 0, 0, 0, 0};
-    for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
-        const double cx = c0[v / (int64_t(Nv) * Nv)], cy = c0[(v / Nv) % Nv], cz = c0[v % Nv];
+    for (int v = threadIdx.x; v < n; v += blockDim.x) {
+        uint32_t ix, iy, iz;
+        vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
+        const double cx = cs[ix], cy = cs[iy], cz = cs[iz];
         const double x = double(fd[v]);
         m[0] += x;
         m[1] += cx * x;
@@ -52,21 +68,30 @@ __global__ void __launch_bounds__(256) indicator_kernel(const bdgfs_hybrid_args 
     const double rho = m[0] * h.cw;
     const double ux = m[1] / m[0], uy = m[2] / m[0], uz = m[3] / m[0];
     const double Tt = (m[4] / m[0] - (ux * ux + uy * uy + uz * uz)) * (2.0 / 3.0);
-    double e[2] = {0, 0};
     const bool ok = rho > 0.0 && Tt > 0.0;
+    // separable Maxwellian: M = a * ex[0][ix] * ex[1][iy] * ex[2][iz]
+    const double a = ok ? rho / pow(3.141592653589793 * Tt, 1.5) : 0.0;
     if (ok) {
-        const double a = rho / pow(3.141592653589793 * Tt, 1.5), it = 1.0 / Tt;
-        for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
-            const double cx = c0[v / (int64_t(Nv) * Nv)] - ux, cy = c0[(v / Nv) % Nv] - uy,
-                         cz = c0[v % Nv] - uz;
+        const double it = 1.0 / Tt;
+        for (int i = threadIdx.x; i < 3 * Nv; i += blockDim.x) {
+            const int d = i / Nv, j = i - d * Nv;
+            const double c = cs[j] - (d == 0 ? ux : d == 1 ? uy : uz);
+            ex[d][j] = exp(-c * c * it);
+        }
+    }
+    __syncthreads();
+    double e[2] = {0, 0};
+    if (ok) {
+        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+            uint32_t ix, iy, iz;
+            vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
             const double x = double(fd[v]);
-            const double d = x - a * exp(-(cx * cx + cy * cy + cz * cz) * it);
+            const double d = x - a * ex[0][ix] * ex[1][iy] * ex[2][iz];
             e[0] += d * d;
             e[1] += x * x;
         }
     }
     block_sum<2>(e, red);
-    __shared__ int64_t s_pos;
     if (threadIdx.x == 0) {
         const double eps = (ok && e[1] > 0.0) ? sqrt(e[0] / e[1]) : 1e30;
         s_pos = -1;
@@ -102,13 +127,12 @@ __global__ void __launch_bounds__(256) indicator_kernel(const bdgfs_hybrid_args 
     if (p >= 0 && h.dev_rows) {
         // (f - M[f]) / |f - M[f]|_2: direction of the deviation from the
         // local Maxwellian (its size, at unit density, is sur_s)
-        __nv_bfloat16* out = static_cast<__nv_bfloat16*>(h.dev_rows) + p * n;
-        const double a = ok ? rho / pow(3.141592653589793 * Tt, 1.5) : 0.0, it = ok ? 1.0 / Tt : 0.0;
+        __nv_bfloat16* out = static_cast<__nv_bfloat16*>(h.dev_rows) + p * int64_t(n);
         const double inv = (ok && e[0] > 0.0) ? 1.0 / sqrt(e[0]) : 0.0;
-        for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
-            const double cx = c0[v / (int64_t(Nv) * Nv)] - ux, cy = c0[(v / Nv) % Nv] - uy,
-                         cz = c0[v % Nv] - uz;
-            const double d = ok ? double(fd[v]) - a * exp(-(cx * cx + cy * cy + cz * cz) * it) : 0.0;
+        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+            uint32_t ix, iy, iz;
+            vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
+            const double d = ok ? double(fd[v]) - a * ex[0][ix] * ex[1][iy] * ex[2][iz] : 0.0;
             out[v] = __float2bfloat16_rn(float(d * inv));
         }
     }
@@ -126,8 +150,10 @@ __global__ void __launch_bounds__(256) project_kernel(const bdgfs_hybrid_args h,
     T* q = Qc + row * n;
     const double* c0 = h.c0;
     double m[5] = {0, 0, 0, 0, 0};
-    for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
-        const double cx = c0[v / (int64_t(Nv) * Nv)], cy = c0[(v / Nv) % Nv], cz = c0[v % Nv];
+    for (int v = threadIdx.x; v < int(n); v += blockDim.x) {
+        uint32_t ix, iy, iz;
+        vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
+        const double cx = c0[ix], cy = c0[iy], cz = c0[iz];
         const double x = double(q[v]);
         m[0] += x;
         m[1] += cx * x;
@@ -144,8 +170,10 @@ __global__ void __launch_bounds__(256) project_kernel(const bdgfs_hybrid_args h,
         for (int j = 0; j < 5; ++j) s += h.ginv[i * 5 + j] * m[j];
         lam[i] = s;
     }
-    for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
-        const double cx = c0[v / (int64_t(Nv) * Nv)], cy = c0[(v / Nv) % Nv], cz = c0[v % Nv];
+    for (int v = threadIdx.x; v < int(n); v += blockDim.x) {
+        uint32_t ix, iy, iz;
+        vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
+        const double cx = c0[ix], cy = c0[iy], cz = c0[iz];
         const double c2 = cx * cx + cy * cy + cz * cz;
         q[v] = T(double(q[v]) - (lam[0] + lam[1] * cx + lam[2] * cy + lam[3] * cz + lam[4] * c2));
     }
@@ -200,8 +228,10 @@ __global__ void __launch_bounds__(256) project_scatter_kernel(const bdgfs_hybrid
     T* dst = Q + dof * n;
     const double* c0 = h.c0;
     double m[5] = {0, 0, 0, 0, 0};
-    for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
-        const double cx = c0[v / (int64_t(Nv) * Nv)], cy = c0[(v / Nv) % Nv], cz = c0[v % Nv];
+    for (int v = threadIdx.x; v < int(n); v += blockDim.x) {
+        uint32_t ix, iy, iz;
+        vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
+        const double cx = c0[ix], cy = c0[iy], cz = c0[iz];
         const double x = double(src[v]);
         m[0] += x;
         m[1] += cx * x;
@@ -220,8 +250,10 @@ __global__ void __launch_bounds__(256) project_scatter_kernel(const bdgfs_hybrid
     }
     const bool re = h.flag[dof] == 2;
     double e[2] = {0, 0};
-    for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
-        const double cx = c0[v / (int64_t(Nv) * Nv)], cy = c0[(v / Nv) % Nv], cz = c0[v % Nv];
+    for (int v = threadIdx.x; v < int(n); v += blockDim.x) {
+        uint32_t ix, iy, iz;
+        vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
+        const double cx = c0[ix], cy = c0[iy], cz = c0[iz];
         const double c2 = cx * cx + cy * cy + cz * cz;
         const T q = T(double(src[v]) - (lam[0] + lam[1] * cx + lam[2] * cy + lam[3] * cz + lam[4] * c2));
         if (!re) {
@@ -240,7 +272,7 @@ __global__ void __launch_bounds__(256) project_scatter_kernel(const bdgfs_hybrid
     }
 }
 
-// out[m][j] = sum_i s_m^i Y[m][i*k + j]
+// out[m][i*k + j] = s_m^i Y[m][i*k + j]
 __global__ void __launch_bounds__(128) heads_kernel(const bdgfs_hybrid_args h, const float* __restrict__ Y,
                                                     int64_t ldy, int64_t k, int nheads,
                                                     __nv_bfloat16* __restrict__ out, int64_t ldo)
@@ -249,13 +281,11 @@ __global__ void __launch_bounds__(128) heads_kernel(const bdgfs_hybrid_args h, c
     if (row >= *h.counts) return;
     const float s = h.sur_s[row];
     const float* y = Y + row * ldy;
-    for (int64_t j = threadIdx.x; j < k; j += blockDim.x) {
-        float acc = 0.f, p = 1.f;
-        for (int i = 0; i < nheads; ++i) {
-            acc += p * y[i * k + j];
-            p *= s;
-        }
-        out[row * ldo + j] = __float2bfloat16_rn(acc);
+    float p = 1.f;
+    for (int i = 0; i < nheads; ++i) {
+        for (int64_t j = threadIdx.x; j < k; j += blockDim.x)
+            out[row * ldo + i * k + j] = __float2bfloat16_rn(p * y[i * k + j]);
+        p *= s;
     }
 }
 
@@ -265,7 +295,7 @@ using namespace bdgfs;
 
 static int check_h(const bdgfs_hybrid_args* h)
 {
-    if (!h || h->ndof < 0 || h->Nv < 1 || !h->c0) return BDGFS_EINVAL;
+    if (!h || h->ndof < 0 || h->Nv < 1 || h->Nv > kMaxNv || !h->c0) return BDGFS_EINVAL;
     if (h->ndof > 2147483647LL) return BDGFS_EINVAL;
     return BDGFS_OK;
 }
@@ -342,7 +372,8 @@ extern "C" int32_t bdgfs_hybrid_heads(const bdgfs_hybrid_args* h, const float* Y
 {
     int rc = check_h(h);
     if (rc) return rc;
-    if (!Y || !out || !h->counts || !h->sur_s || k < 1 || nheads < 1 || ldy < nheads * k || ldo < k)
+    if (!Y || !out || !h->counts || !h->sur_s || k < 1 || nheads < 1 || ldy < nheads * k ||
+        ldo < nheads * k)
         return BDGFS_EINVAL;
     if (h->ndof == 0) return BDGFS_OK;
     heads_kernel<<<unsigned(h->ndof), 128, 0, static_cast<cudaStream_t>(stream)>>>(

@@ -14,18 +14,29 @@ and the network predicts the three heads from (d^, u, T):
   h   = GELU layers 1..3 (width W) of x
   Y   = W4 [h, x] + b4        (3 heads of k output modes; [h, x] is a linear
                                skip from the input to the output layer)
-  y   = Y0 + s Y1 + s^2 Y2
-  Q   = rho^2 Bq^T (cscale y)                              Bq: k x n basis
+  Q   = rho^2 (Bq0^T Y0 + s Bq1^T Y1 + s^2 Bq2^T Y2)       Bqh: k x n bases
   Q  <- Q - phi^T G^{-1} (phi Q)                           FP64 conservation
 The bases are fitted by a randomised SVD (Halko, Martinsson, Tropp 2011)
 whose GEMMs are the project's FP32 kernels.  Inference and the training
 inputs run through the same kernels: the indicator kernel writes d^ (bf16),
 s, rho^2 and (u, T - 1); one tcgen05 GEMM projects d^ onto Bd/sigma with
-bias -mu/sigma; GELU layers, output heads, head combination and the
-reconstruction are tcgen05 GEMMs plus one small kernel; the FP64
-projection is fused with the scatter to the state's rows.  Training:
-least-squares start of the linear (skip) part, then AdamW on all
-parameters with the project's GEMM / GELU-gradient / loss / AdamW kernels.
+bias -mu/sigma; GELU layers, output heads and the reconstruction (one
+GEMM over the three heads, scaled by 1, s, s^2 in a small kernel) run on
+the tensor cores; the FP64
+projection is fused with the scatter to the state's rows.
+
+Training targets are the heads themselves: with M the Maxwellian of a
+sample f and d^ its (bf16) deviation direction, bilinearity gives, for any
+probe size a,
+    y0 = Q(M)/rho^2,  y1 = (Q+ - Q-)/(2 a rho^2),  y2 = (Q+ + Q- - 2 Q(M))/(2 a^2 rho^2)
+with Q+- = Q(M +- a rho d^) (spectral, FP32, conservation-projected), so
+every head is supervised at a fixed scale whatever the sample's own s.
+Each head has its own output basis; the heads' coefficients, each divided
+by its RMS, are fitted by a least-squares start of the linear (skip) part
+and then AdamW (linear warm-up, cosine decay) on all parameters with the
+project's GEMM / GELU-gradient / loss / AdamW kernels (per-row relative
+squared error over the three heads); the head scales are folded into the
+output layer afterwards.
 
 Families of training distributions (``Family``): Maxwellians with seeded
 rho, u, T multiplied by 1 + A P(xi), xi = (c - u)/sqrt(T), with P a random
@@ -58,6 +69,7 @@ from .gemm import ACT_GELU, ACT_GELU_GRAD, adamw, colsum, gemm
 
 NFEAT = 4            # (u_x, u_y, u_z, T - 1)
 NHEADS = 3           # y = Y0 + s Y1 + s^2 Y2
+PROBE = 0.1          # deviation size a of the head-label probes M +- a rho d^
 
 
 # ------------------------------------------------------------------ data
@@ -236,30 +248,64 @@ class QSurrogate:
             adamw(self.b[l], self.gb[l], self.mb[l], self.vb[l], None, t, lr=lr, wd=0.0)
 
     @staticmethod
-    def combine(Y, s, k):
-        """y = Y0 + s Y1 + s^2 Y2 (training-side combination of the heads)."""
+    def scale_heads(Y, s, k):
+        """[Y0, s Y1, s^2 Y2] (what bdgfs_hybrid_heads computes)."""
         s = s[:, None]
-        return Y[:, :k] + s * Y[:, k:2 * k] + (s * s) * Y[:, 2 * k:3 * k]
+        return torch.cat([Y[:, :k], s * Y[:, k:2 * k], (s * s) * Y[:, 2 * k:3 * k]], dim=1)
 
-    def train_step(self, xc, s, t, dp, loss, step, lr):
+    def train_step(self, xc, t, dY, loss, step, lr):
         """One AdamW step on a batch: xc input rows (x in columns [w, ldx)),
-        s deviation sizes, t targets.  Returns the combined prediction."""
+        t the scaled head targets (B x 3k).  Returns the heads."""
         B = xc.shape[0]
         Y = self.forward_train(xc)
-        p = self.combine(Y, s, self.k).contiguous()
-        _lib.check(_lib.lib().bdgfs_relmse(p.data_ptr(), t.data_ptr(), B, self.k, self.loss_delta,
-                                           dp.data_ptr(), loss.data_ptr(), _lib.stream_ptr()),
-                   'bdgfs_relmse')
-        s1 = s[:, None]
-        self.backward_train(torch.cat([dp, s1 * dp, (s1 * s1) * dp], dim=1))
+        _lib.check(_lib.lib().bdgfs_relmse(Y.data_ptr(), t.data_ptr(), B, NHEADS * self.k,
+                                           self.loss_delta, dY.data_ptr(), loss.data_ptr(),
+                                           _lib.stream_ptr()), 'bdgfs_relmse')
+        self.backward_train(dY)
         self.step(step, lr)
-        return p
+        return Y
 
     # data ------------------------------------------------------------------
     def _labels(self, f, collider):
         Q = torch.empty_like(f)
         collider([(0, f, Q, None)], project=True, exact=False)
         return Q
+
+    def _maxwellian(self, f):
+        """FP64 density and the Maxwellian with the density, velocity and
+        temperature of each row of f (training-data preparation)."""
+        Nv, g = self.Nv, self.grid
+        c0 = g.c0.double()
+        F = f.double().view(-1, Nv, Nv, Nv)
+        cx, cy, cz = c0.view(1, -1, 1, 1), c0.view(1, 1, -1, 1), c0.view(1, 1, 1, -1)
+        m0 = F.sum((1, 2, 3))
+        ux = (F * cx).sum((1, 2, 3)) / m0
+        uy = (F * cy).sum((1, 2, 3)) / m0
+        uz = (F * cz).sum((1, 2, 3)) / m0
+        T = ((F * (cx * cx + cy * cy + cz * cz)).sum((1, 2, 3)) / m0
+             - (ux * ux + uy * uy + uz * uz)) * (2.0 / 3.0)
+        rho = m0 * g.cw
+        v = lambda t: t.view(-1, 1, 1, 1)
+        M = v(rho) / (math.pi * v(T))**1.5 * torch.exp(
+            -((cx - v(ux))**2 + (cy - v(uy))**2 + (cz - v(uz))**2) / v(T))
+        return rho, M.reshape(f.shape[0], -1).float()
+
+    def _head_labels(self, f, dev_rows, col):
+        """(y0, y1, y2) rows (FP32, n wide each) of the distributions f
+        whose deviation directions (bf16, as the network sees them) are
+        dev_rows."""
+        rho, M = self._maxwellian(f)
+        d = dev_rows.float()
+        d = d / d.norm(dim=1, keepdim=True).clamp_min(1e-30)
+        r = (PROBE * rho).float()[:, None]
+        Q0 = self._labels(M, col)
+        Qp = self._labels((M + r * d).contiguous(), col)
+        Qm = self._labels((M - r * d).contiguous(), col)
+        r2 = (rho * rho).float()[:, None]
+        y0 = Q0 / r2
+        y1 = (Qp - Qm) / (2 * PROBE * r2)
+        y2 = (Qp + Qm - 2 * Q0) / (2 * PROBE * PROBE * r2)
+        return y0, y1, y2
 
     def fit(self, nsamples=200000, ntest=50000, epochs=20, lr=3e-4, batch=1024, seed=0,
             nbasis=16384, chunk=8192, log=None, ridge=1e-6):
@@ -272,18 +318,20 @@ class QSurrogate:
         c0 = self.grid.c0.double().cpu().numpy()
         enc = HybridCollider(self, threshold=float('inf'), recheck=0.0)
         t0 = time.time()
-        # 1. bases from a sample: deviation directions and Q / rho^2
+        # 1. bases from a sample: deviation directions and the three heads
         fb = sample_family(c0, nbasis, gen, dev, family=self.family)
-        Qb = self._labels(fb, col)
         enc.classify(fb)
         m = nbasis
         idx = enc.sur_idx[:m].long()
+        fb = fb.index_select(0, idx)
         Xd = enc.dev_rows[:m].float()
-        Xq = (Qb.index_select(0, idx) / enc.rho2[:m, None]).contiguous()
-        self.Bd, self.svd_ = fit_basis(Xd, self.k, gen=gen)
-        self.Bq, self.svq = fit_basis(Xq, self.k, gen=gen)
-        self.k = min(self.Bd.shape[0], self.Bq.shape[0])
-        self.Bd, self.Bq = self.Bd[:self.k].contiguous(), self.Bq[:self.k].contiguous()
+        heads = self._head_labels(fb, enc.dev_rows[:m], col)
+        del fb
+        self.Bd, _ = fit_basis(Xd, self.k, gen=gen)
+        Bq = [fit_basis(h.contiguous(), self.k, gen=gen)[0] for h in heads]
+        self.k = min([self.Bd.shape[0]] + [b.shape[0] for b in Bq])
+        self.Bd = self.Bd[:self.k].contiguous()
+        self.Bq = torch.cat([b[:self.k] for b in Bq]).contiguous()           # 3k x n
         # input standardisation of the deviation modes (folded into the
         # projection: x = (Bd/sigma) d^ - mu/sigma)
         a = torch.empty(m, self.k, device=dev)
@@ -292,42 +340,49 @@ class QSurrogate:
         sd = a.std(0)
         self.sigma = sd.clamp_min(1e-3 * float(sd.max()))
         self._fold_input()
-        # basis truncation error of Q on the fit sample (relative L2)
-        cq = torch.empty(m, self.k, device=dev)
-        gemm(Xq, self.Bq, out=cq, engine=1)
-        Xr = torch.empty_like(Xq)
-        gemm(cq, self.Bq, tb=True, out=Xr, engine=1)
-        self.basis_err_q = float((Xr - Xq).norm() / Xq.norm())
-        del fb, Qb, Xd, Xq, Xr, a, cq
-        # 2. training data through the inference encoder
+        # basis truncation error of each head on the fit sample (relative L2)
+        self.basis_err_heads = []
+        for hd, y in enumerate(heads):
+            B = self.Bq[hd * self.k:(hd + 1) * self.k]
+            cq = torch.empty(m, self.k, device=dev)
+            gemm(y.contiguous(), B, out=cq, engine=1)
+            yr = torch.empty_like(y)
+            gemm(cq, B, tb=True, out=yr, engine=1)
+            self.basis_err_heads.append(float((yr - y).norm() / y.norm()))
+        self.basis_err_q = max(self.basis_err_heads)
+        del Xd, heads, a, cq, yr
+        # 2. training data through the inference encoder; head coefficients
+        K3 = NHEADS * self.k
         X = torch.zeros(nsamples, self.kin, device=dev, dtype=torch.bfloat16)
-        S = torch.empty(nsamples, device=dev)
-        Cc = torch.empty(nsamples, self.k, device=dev)
+        Cc = torch.empty(nsamples, K3, device=dev)
         for i0 in range(0, nsamples, chunk):
             m = min(chunk, nsamples - i0)
             f = sample_family(c0, m, gen, dev, family=self.family)
-            Q = self._labels(f, col)
-            x, s, rho2, idx = self.encode(f, enc)
+            x, _, _, idx = self.encode(f, enc)
             X[i0:i0 + m] = x
-            S[i0:i0 + m] = s
-            Qs = (Q.index_select(0, idx.long()) / rho2[:, None]).contiguous()
-            gemm(Qs, self.Bq, out=Cc[i0:i0 + m], engine=1)
-        self.cscale = float(Cc.pow(2).mean().sqrt())
-        Tt = (Cc / self.cscale).contiguous()
+            heads = self._head_labels(f.index_select(0, idx.long()), enc.dev_rows[:m], col)
+            for hd, y in enumerate(heads):
+                gemm(y.contiguous(), self.Bq[hd * self.k:(hd + 1) * self.k],
+                     out=Cc[i0:i0 + m, hd * self.k:(hd + 1) * self.k], engine=1)
+        self.hscale = Cc.view(nsamples, NHEADS, self.k).pow(2).mean((0, 2)).sqrt()
+        Tt = (Cc.view(nsamples, NHEADS, self.k) / self.hscale[None, :, None]).view(nsamples, K3)
+        Tt = Tt.contiguous()
         del Cc
-        # per-row relative loss, floored at 1e-4 of the mean target energy
-        self.loss_delta = 1e-4 * float(Tt.pow(2).sum(1).mean())
+        # per-row relative loss, floored at 1% of the mean target energy
+        self.loss_delta = 1e-2 * float(Tt.pow(2).sum(1).mean())
         t_data = time.time() - t0
         # 3. parameters: random MLP, least-squares start of the skip path
         self._init_params(gen)
         t1 = time.time()
-        self.ridge_residual = self._ridge_init(X, S, Tt, ridge)
-        # 4. AdamW on the per-row relative squared error of y
+        self.ridge_residual = self._ridge_init(X, Tt, ridge)
+        # 4. AdamW
         loss = torch.zeros(1, dtype=torch.float64, device=dev)
         tot = torch.zeros(1, dtype=torch.float64, device=dev)
         xc = torch.zeros(batch, self.ldx, device=dev, dtype=torch.bfloat16)
-        dp = torch.empty(batch, self.k, device=dev)
+        dY = torch.empty(batch, K3, device=dev)
         step = 0
+        nsteps = epochs * (nsamples // batch)
+        warm = max(1, min(200, nsteps // 20))
         for ep in range(epochs):
             perm = torch.randperm(nsamples, generator=gen, device=dev)
             tot.zero_()
@@ -336,7 +391,11 @@ class QSurrogate:
                 idb = perm[i0:i0 + batch]
                 xc[:, self.w:] = X[idb]
                 step += 1
-                self.train_step(xc, S[idb], Tt[idb].contiguous(), dp, loss, step, lr)
+                # linear warm-up, cosine decay to lr/100
+                lr_t = lr * (step / warm if step <= warm else
+                             0.01 + 0.99 * 0.5 * (1 + math.cos(math.pi * (step - warm) /
+                                                                max(1, nsteps - warm))))
+                self.train_step(xc, Tt[idb].contiguous(), dY, loss, step, lr_t)
                 tot += loss
                 nb += 1
             self.history.append(float(tot.item()) / max(nb, 1))
@@ -352,39 +411,35 @@ class QSurrogate:
         self.test_err = self.evaluate(ntest, seed=seed + 1, chunk=chunk)
         return self
 
-    def _ridge_init(self, X, S, Tt, lam):
+    def _ridge_init(self, X, Tt, lam):
         """Least-squares start: the output layer's skip columns and bias
-        solve min |[x, 1, s x, s, s^2 x, s^2] Theta - t|^2 (+ lam |Theta|^2)
-        over the training set (normal equations on the FP32 GEMM engine,
-        FP64 solve on the host).  Returns the relative residual."""
+        solve min |[x, 1] Theta - t|^2 (+ lam |Theta|^2) over the training
+        set for all heads (normal equations on the FP32 GEMM engine, FP64
+        solve on the host).  Returns the relative residual."""
         dev = self.device
-        k, kin, w = self.k, self.kin, self.w
-        ns = X.shape[0]
-        nf = NHEADS * (kin + 1)
+        kin, w = self.kin, self.w
+        ns, K3 = Tt.shape
+        nf = kin + 1
         G = torch.zeros(nf, nf, device=dev, dtype=torch.float64)
-        R = torch.zeros(nf, k, device=dev, dtype=torch.float64)
+        R = torch.zeros(nf, K3, device=dev, dtype=torch.float64)
         ch = 16384
         for i0 in range(0, ns, ch):
             x = X[i0:i0 + ch].float()
-            s = S[i0:i0 + ch, None]
-            one = torch.ones_like(s)
-            F = torch.cat([x, one, s * x, s, s * s * x, s * s], dim=1).contiguous()
+            F = torch.cat([x, torch.ones(x.shape[0], 1, device=dev)], dim=1).contiguous()
             g = torch.empty(nf, nf, device=dev)
             gemm(F, F, ta=True, tb=True, out=g, engine=1)
-            r = torch.empty(nf, k, device=dev)
+            r = torch.empty(nf, K3, device=dev)
             gemm(F, Tt[i0:i0 + ch], ta=True, tb=True, out=r, engine=1)
             G += g.double()
             R += r.double()
         Gh, Rh = G.cpu().numpy(), R.cpu().numpy()
         Gh += lam * np.trace(Gh) / nf * np.eye(nf)
-        Th = np.linalg.solve(Gh, Rh)                      # nf x k
+        Th = np.linalg.solve(Gh, Rh)                      # nf x 3k
         tt = float(Tt.double().pow(2).sum())
         res = float(np.sum(Th * (Gh @ Th)) - 2 * np.sum(Th * Rh)) + tt
         Th = torch.from_numpy(Th).float().to(dev)
-        for hd in range(NHEADS):
-            blk = Th[hd * (kin + 1):(hd + 1) * (kin + 1)]
-            self.W[3][hd * k:(hd + 1) * k, w:] = blk[:kin].t()
-            self.b[3][hd * k:(hd + 1) * k] = blk[kin]
+        self.W[3][:, w:] = Th[:kin].t()
+        self.b[3][:] = Th[kin]
         self._sync_bf16()
         return math.sqrt(max(res, 0.0) / tt)
 
@@ -393,12 +448,15 @@ class QSurrogate:
         self.bias_in = (-self.mu / self.sigma).contiguous()
 
     def _fold(self):
-        """Inference copies: bf16 weights; output scale folded into the
-        reconstruction basis."""
+        """Inference copies: bf16 weights, head scales folded into the
+        output layer."""
         self._fold_input()
-        self.inf_W = [w.bfloat16().contiguous() for w in self.W]
-        self.inf_b = [b.contiguous() for b in self.b]
-        self.BqT_bf16 = (self.Bq.t() * self.cscale).bfloat16().contiguous()   # n x k
+        sc = self.hscale.repeat_interleave(self.k)[:, None]
+        W3 = self.W[3] * sc
+        b3 = self.b[3] * sc[:, 0]
+        self.inf_W = [w.bfloat16().contiguous() for w in self.W[:3]] + [W3.bfloat16().contiguous()]
+        self.inf_b = [b.contiguous() for b in self.b[:3]] + [b3.contiguous()]
+        self.BqT_bf16 = self.Bq.t().bfloat16().contiguous()                    # n x 3k
 
     # inference ------------------------------------------------------------
     def encode(self, f, enc):
@@ -427,8 +485,8 @@ class QSurrogate:
         gemm(xc, self.inf_W[3], bias=self.inf_b[3], mcount=cnt, out=enc.Y[:M])
         _lib.check(_lib.lib().bdgfs_hybrid_heads(C.byref(enc.args), enc.Y.data_ptr(),
                                                  NHEADS * self.k, self.k, NHEADS,
-                                                 enc.yb.data_ptr(), self.k, _lib.stream_ptr()),
-                   'bdgfs_hybrid_heads')
+                                                 enc.yb.data_ptr(), NHEADS * self.k,
+                                                 _lib.stream_ptr()), 'bdgfs_hybrid_heads')
         gemm(enc.yb[:M], self.BqT_bf16, row_scale=enc.rho2, mcount=cnt, out=enc.Qc[:M])
 
     def evaluate(self, nsamples, seed=1, chunk=8192, family=None):
@@ -460,20 +518,19 @@ class QSurrogate:
                 'n': int(nsamples), 'basis_truncation_q': getattr(self, 'basis_err_q', None)}
 
     def state_dict(self):
-        keys = ('Bd', 'Bq', 'mu', 'sigma')
+        keys = ('Bd', 'Bq', 'mu', 'sigma', 'hscale')
         d = {k: getattr(self, k).cpu() for k in keys}
-        d.update(W=[w.cpu() for w in self.W], b=[b.cpu() for b in self.b], cscale=self.cscale,
+        d.update(W=[w.cpu() for w in self.W], b=[b.cpu() for b in self.b],
                  k=self.k, w=self.w, Nv=self.Nv)
         return d
 
     def load_state_dict(self, d):
         dev = self.device
-        for k in ('Bd', 'Bq', 'mu', 'sigma'):
+        for k in ('Bd', 'Bq', 'mu', 'sigma', 'hscale'):
             setattr(self, k, d[k].to(dev))
         self.k, self.w = int(d['k']), int(d['w'])
         self.W = [w.to(dev) for w in d['W']]
         self.b = [b.to(dev) for b in d['b']]
-        self.cscale = float(d['cscale'])
         self._sync_bf16()
         self._fold()
         self.trained = True
@@ -520,7 +577,7 @@ class HybridCollider:
             self.xc = torch.zeros(ndof, m.ldx, device=dev, dtype=torch.bfloat16)
             self.h = [torch.empty(ndof, m.w, device=dev, dtype=torch.bfloat16) for _ in range(2)]
             self.Y = torch.empty(ndof, NHEADS * m.k, device=dev)
-            self.yb = torch.empty(ndof, m.k, device=dev, dtype=torch.bfloat16)
+            self.yb = torch.empty(ndof, NHEADS * m.k, device=dev, dtype=torch.bfloat16)
             self.Qc = torch.empty(ndof, m.n, device=dev, dtype=self.grid.dtype)
             self._net = shape
 

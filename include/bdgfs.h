@@ -251,7 +251,7 @@ int32_t bdgfs_adamw(float* p, const float* grad, float* m1, float* m2,
  * ---------------------------------------------------------------------- */
 typedef struct bdgfs_hybrid_args {
     int64_t ndof;            /* distributions of the state (rows)          */
-    int32_t Nv;
+    int32_t Nv;              /* 1..64                                      */
     int32_t fp64;
     const double* c0;        /* [Nv] cell-centre velocities                */
     const double* ginv;      /* [5][5] inverse Gram matrix of {1,c,|c|^2}  */
@@ -295,8 +295,8 @@ int32_t bdgfs_hybrid_scatter(const bdgfs_hybrid_args* h, const void* Qc,
  * projected on the fly and written to Q; Qc itself is left unchanged). */
 int32_t bdgfs_hybrid_project_scatter(const bdgfs_hybrid_args* h,
                                      const void* Qc, void* Q, void* stream);
-/* Combine the network's output heads of the first counts[0] rows:
- * out[m][j] = sum_{i<nheads} sur_s[m]^i * Y[m][i*k + j]
+/* Scale the network's output heads of the first counts[0] rows:
+ * out[m][i*k + j] = sur_s[m]^i * Y[m][i*k + j], i < nheads, j < k
  * (Y float, leading dimension ldy; out bf16, leading dimension ldo). */
 int32_t bdgfs_hybrid_heads(const bdgfs_hybrid_args* h, const float* Y,
                            int64_t ldy, int64_t k, int32_t nheads,

@@ -3,9 +3,8 @@
 Restates, in numpy FP64, the network the surrogate trains on the GPU:
   h1 = GELU(x W1^T + b1), h2 = GELU(h1 W2^T + b2), h3 = GELU(h2 W3^T + b3)
   Y  = [h3, x] W4^T + b4                  (W4: 3k x (w + kin), skip from x)
-  p  = Y[:, :k] + s Y[:, k:2k] + s^2 Y[:, 2k:]
 with GELU(z) = z Phi(z) (erf form) and the per-row relative squared error
-L = (1/B) sum_b |p_b - t_b|^2 / (|t_b|^2 + delta).  There is no learned
+of the heads L = (1/B) sum_b |Y_b - t_b|^2 / (|t_b|^2 + delta).  There is no learned
 component in the reference; this oracle checks the project's own gradient
 kernels.
 """
@@ -23,7 +22,7 @@ def gelu_grad(z):
     return 0.5 * (1.0 + _verf(z / sqrt(2.0))) + z * np.exp(-0.5 * z * z) / sqrt(2.0 * pi)
 
 
-def forward(x, s, W, b):
+def forward(x, W, b):
     acts, zs = [x], []
     h = x
     for l in range(3):
@@ -32,22 +31,23 @@ def forward(x, s, W, b):
         h = gelu(z)
         acts.append(h)
     xc = np.concatenate([h, x], axis=1)
-    Y = xc @ W[3].T + b[3]
+    return xc @ W[3].T + b[3], acts, zs, xc
+
+
+def combine(Y, s):
+    """y = Y0 + s Y1 + s^2 Y2 (heads of equal width)."""
     k = Y.shape[1] // 3
     s1 = s[:, None]
-    p = Y[:, :k] + s1 * Y[:, k:2 * k] + s1 * s1 * Y[:, 2 * k:]
-    return p, acts, zs, xc
+    return Y[:, :k] + s1 * Y[:, k:2 * k] + s1 * s1 * Y[:, 2 * k:]
 
 
-def loss_and_grads(x, s, t, W, b, delta=1e-12):
-    p, acts, zs, xc = forward(x, s, W, b)
+def loss_and_grads(x, t, W, b, delta=1e-12):
+    Y, acts, zs, xc = forward(x, W, b)
     B = x.shape[0]
     w = W[0].shape[0]
     den = (t * t).sum(1, keepdims=True) + delta
-    L = float((((p - t)**2).sum(1, keepdims=True) / den).mean())
-    dp = 2.0 * (p - t) / (den * B)
-    s1 = s[:, None]
-    g = np.concatenate([dp, s1 * dp, s1 * s1 * dp], axis=1)
+    L = float((((Y - t)**2).sum(1, keepdims=True) / den).mean())
+    g = 2.0 * (Y - t) / (den * B)
     gW, gb = [None] * 4, [None] * 4
     for l in (3, 2, 1, 0):
         gW[l] = g.T @ (xc if l == 3 else acts[l])

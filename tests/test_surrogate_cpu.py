@@ -13,9 +13,8 @@ def test_oracle_gradients_match_finite_differences():
          rng.normal(size=(w, w)) * 0.4, rng.normal(size=(3 * k, w + kin)) * 0.4]
     b = [rng.normal(size=w) * 0.1, rng.normal(size=w) * 0.1, rng.normal(size=w) * 0.1,
          rng.normal(size=3 * k) * 0.1]
-    x, t = rng.normal(size=(B, kin)), rng.normal(size=(B, k))
-    s = rng.uniform(0.1, 1.0, size=B)
-    L, gW, gb = loss_and_grads(x, s, t, W, b)
+    x, t = rng.normal(size=(B, kin)), rng.normal(size=(B, 3 * k))
+    L, gW, gb = loss_and_grads(x, t, W, b)
     h = 1e-6
     for l in range(4):
         for (i, j) in ((0, 0), (1, 2), (W[l].shape[0] - 1, W[l].shape[1] - 1)):
@@ -23,14 +22,14 @@ def test_oracle_gradients_match_finite_differences():
             Wp[l][i, j] += h
             Wm = [m.copy() for m in W]
             Wm[l][i, j] -= h
-            fd = (loss_and_grads(x, s, t, Wp, b)[0] - loss_and_grads(x, s, t, Wm, b)[0]) / (2 * h)
+            fd = (loss_and_grads(x, t, Wp, b)[0] - loss_and_grads(x, t, Wm, b)[0]) / (2 * h)
             assert abs(fd - gW[l][i, j]) < 1e-6 * max(1.0, abs(fd))
         for i in (1, b[l].shape[0] - 1):
             bp = [v.copy() for v in b]
             bp[l][i] += h
             bm = [v.copy() for v in b]
             bm[l][i] -= h
-            fd = (loss_and_grads(x, s, t, W, bp)[0] - loss_and_grads(x, s, t, W, bm)[0]) / (2 * h)
+            fd = (loss_and_grads(x, t, W, bp)[0] - loss_and_grads(x, t, W, bm)[0]) / (2 * h)
             assert abs(fd - gb[l][i]) < 1e-6 * max(1.0, abs(fd))
 
 

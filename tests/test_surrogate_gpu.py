@@ -40,15 +40,14 @@ def test_training_gradients_match_fp64_oracle(cuda):
     xc = torch.zeros(B, q.ldx, device=be.device, dtype=torch.bfloat16)
     xc[:, q.w:] = torch.randn(B, q.kin, device=be.device, generator=gen).bfloat16()
     x = xc[:, q.w:].double().cpu().numpy()
-    s = torch.rand(B, device=be.device, generator=gen) + 0.1
-    t = torch.randn(B, 64, device=be.device, generator=gen)
-    dp = torch.empty(B, 64, device=be.device)
+    t = torch.randn(B, 3 * 64, device=be.device, generator=gen)
+    dY = torch.empty(B, 3 * 64, device=be.device)
     loss = torch.zeros(1, dtype=torch.float64, device=be.device)
     W = [w.bfloat16().double().cpu().numpy() for w in q.W]
     b = [bb.double().cpu().numpy() for bb in q.b]
-    q.train_step(xc, s, t, dp, loss, 1, lr=0.0)      # lr 0: gradients only
+    q.train_step(xc, t, dY, loss, 1, lr=0.0)         # lr 0: gradients only
     torch.cuda.synchronize()
-    L, gW, gb = loss_and_grads(x, s.double().cpu().numpy(), t.double().cpu().numpy(), W, b)
+    L, gW, gb = loss_and_grads(x, t.double().cpu().numpy(), W, b)
     assert abs(float(loss) - L) < 2e-2 * L
     for l in range(4):
         e = np.linalg.norm(q.gW[l].double().cpu().numpy() - gW[l]) / np.linalg.norm(gW[l])
@@ -87,13 +86,13 @@ def test_indicator_rows_features_and_heads(cuda):
     feat = h.xc[:m, q.w + q.k:q.w + q.k + 4].double()
     ref = torch.cat([u, (T - 1)[:, None]], dim=1)
     assert float((feat - ref).abs().max()) < 4e-3
-    # heads: out = Y0 + s Y1 + s^2 Y2
+    # heads: out = [Y0, s Y1, s^2 Y2]
     Y = torch.randn(m, 3 * q.k, device=be.device, generator=gen)
     h.Y[:m] = Y
     _lib.check(_lib.lib().bdgfs_hybrid_heads(C.byref(h.args), h.Y.data_ptr(), 3 * q.k, q.k, 3,
-                                             h.yb.data_ptr(), q.k, _lib.stream_ptr()), 'heads')
+                                             h.yb.data_ptr(), 3 * q.k, _lib.stream_ptr()), 'heads')
     torch.cuda.synchronize()
-    yr = q.combine(Y.double(), h.sur_s[:m].double(), q.k)
+    yr = q.scale_heads(Y.double(), h.sur_s[:m].double(), q.k)
     assert float((h.yb[:m].double() - yr).norm() / yr.norm()) < 4e-3
     # fused projection + scatter == projection then scatter
     Qc = torch.randn(m, vm.vsize(), device=be.device, generator=gen)
@@ -108,6 +107,28 @@ def test_indicator_rows_features_and_heads(cuda):
                                                _lib.stream_ptr()), 's')
     torch.cuda.synchronize()
     assert torch.equal(out1, out2)
+
+
+def test_head_labels_recombine_to_q(cuda):
+    """Bilinearity: the head labels from the probes M +- a rho d^ recombine,
+    at each sample's own deviation size s, to the spectral Q of the sample
+    (up to FP32 rounding and the bf16 rounding of d^)."""
+    from frfs_b200.scattering import VHSCollider
+    be, vm, sm, q = _model(k=64, w=128)
+    gen = torch.Generator(device=be.device).manual_seed(12)
+    f = sample_family(vm.c0(), 64, gen, be.device)
+    h = HybridCollider(q, threshold=float('inf'), recheck=0.0)
+    h.classify(f)
+    idx = h.sur_idx[:64].long()
+    fc = f.index_select(0, idx)
+    col = VHSCollider([q.grid], be.device)
+    y0, y1, y2 = q._head_labels(fc, h.dev_rows[:64], col)
+    s = h.sur_s[:64, None]
+    Q = q._labels(fc, col) / h.rho2[:64, None]
+    p = y0 + s * y1 + s * s * y2
+    torch.cuda.synchronize()
+    err = (p - Q).norm(dim=1) / Q.norm(dim=1)
+    assert float(err.max()) < 1e-2, float(err.max())
 
 
 @pytest.fixture(scope='module')
