@@ -40,7 +40,62 @@ __device__ __forceinline__ void vsplit(uint32_t v, uint32_t Nv, uint32_t& ix, ui
     iy = q - ix * Nv;
 }
 
-template <typename T>
+// Four consecutive values (same x, y; z..z+3) of a row: one 16-byte load
+// for float, two for double (VEC = 4), or one scalar (VEC = 1).
+template <typename T, int VEC>
+struct Chunk {
+    T v[VEC];
+    __device__ __forceinline__ void load(const T* p)
+    {
+        if constexpr (VEC == 4 && sizeof(T) == 4) {
+            const float4 x = *reinterpret_cast<const float4*>(p);
+            v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+        } else if constexpr (VEC == 4) {
+            const double2 a = reinterpret_cast<const double2*>(p)[0];
+            const double2 b = reinterpret_cast<const double2*>(p)[1];
+            v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+        } else {
+            v[0] = *p;
+        }
+    }
+    __device__ __forceinline__ void store(T* p) const
+    {
+        if constexpr (VEC == 4 && sizeof(T) == 4) {
+            *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+        } else if constexpr (VEC == 4) {
+            reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+            reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+        } else {
+            *p = v[0];
+        }
+    }
+};
+
+// FP64 raw moments {sum x, sum c x, sum |c|^2 x} of one row (block-wide)
+template <typename T, int VEC>
+__device__ __forceinline__ void row_moments(const T* __restrict__ row, int n, int Nv, const double* cs,
+                                            double (&m)[5])
+{
+#pragma unroll 2
+    for (int v = threadIdx.x * VEC; v < n; v += blockDim.x * VEC) {
+        Chunk<T, VEC> c;
+        c.load(row + v);
+        uint32_t ix, iy, iz;
+        vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
+        const double cx = cs[ix], cy = cs[iy], b = cx * cx + cy * cy;
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) {
+            const double x = double(c.v[j]), cz = cs[iz + j];
+            m[0] += x;
+            m[1] += cx * x;
+            m[2] += cy * x;
+            m[3] += cz * x;
+            m[4] += (b + cz * cz) * x;
+        }
+    }
+}
+
+template <typename T, int VEC>
 __global__ void __launch_bounds__(256) indicator_kernel(const bdgfs_hybrid_args h, const T* __restrict__ f)
 {
     __shared__ double red[8 * 8];
@@ -53,17 +108,7 @@ __global__ void __launch_bounds__(256) indicator_kernel(const bdgfs_hybrid_args 
     for (int i = threadIdx.x; i < Nv; i += blockDim.x) cs[i] = h.c0[i];
     __syncthreads();
     double m[5] = {0, 0, 0, 0, 0};
-    for (int v = threadIdx.x; v < n; v += blockDim.x) {
-        uint32_t ix, iy, iz;
-        vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
-        const double cx = cs[ix], cy = cs[iy], cz = cs[iz];
-        const double x = double(fd[v]);
-        m[0] += x;
-        m[1] += cx * x;
-        m[2] += cy * x;
-        m[3] += cz * x;
-        m[4] += (cx * cx + cy * cy + cz * cz) * x;
-    }
+    row_moments<T, VEC>(fd, n, Nv, cs, m);
     block_sum<5>(m, red);
     const double rho = m[0] * h.cw;
     const double ux = m[1] / m[0], uy = m[2] / m[0], uz = m[3] / m[0];
@@ -82,13 +127,20 @@ __global__ void __launch_bounds__(256) indicator_kernel(const bdgfs_hybrid_args 
     __syncthreads();
     double e[2] = {0, 0};
     if (ok) {
-        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+#pragma unroll 2
+        for (int v = threadIdx.x * VEC; v < n; v += blockDim.x * VEC) {
+            Chunk<T, VEC> c;
+            c.load(fd + v);
             uint32_t ix, iy, iz;
             vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
-            const double x = double(fd[v]);
-            const double d = x - a * ex[0][ix] * ex[1][iy] * ex[2][iz];
-            e[0] += d * d;
-            e[1] += x * x;
+            const double axy = a * ex[0][ix] * ex[1][iy];
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) {
+                const double x = double(c.v[j]);
+                const double d = x - axy * ex[2][iz + j];
+                e[0] += d * d;
+                e[1] += x * x;
+            }
         }
     }
     block_sum<2>(e, red);
@@ -129,11 +181,24 @@ __global__ void __launch_bounds__(256) indicator_kernel(const bdgfs_hybrid_args 
         // local Maxwellian (its size, at unit density, is sur_s)
         __nv_bfloat16* out = static_cast<__nv_bfloat16*>(h.dev_rows) + p * int64_t(n);
         const double inv = (ok && e[0] > 0.0) ? 1.0 / sqrt(e[0]) : 0.0;
-        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+#pragma unroll 2
+        for (int v = threadIdx.x * VEC; v < n; v += blockDim.x * VEC) {
+            Chunk<T, VEC> c;
+            c.load(fd + v);
             uint32_t ix, iy, iz;
             vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
-            const double d = ok ? double(fd[v]) - a * ex[0][ix] * ex[1][iy] * ex[2][iz] : 0.0;
-            out[v] = __float2bfloat16_rn(float(d * inv));
+            const double axy = a * ex[0][ix] * ex[1][iy];
+            float d[VEC];
+#pragma unroll
+            for (int j = 0; j < VEC; ++j)
+                d[j] = ok ? float((double(c.v[j]) - axy * ex[2][iz + j]) * inv) : 0.f;
+            if constexpr (VEC == 4) {
+                __align__(8) __nv_bfloat162 hv[2] = {__floats2bfloat162_rn(d[0], d[1]),
+                                                     __floats2bfloat162_rn(d[2], d[3])};
+                *reinterpret_cast<uint2*>(out + v) = *reinterpret_cast<const uint2*>(hv);
+            } else {
+                out[v] = __float2bfloat16_rn(d[0]);
+            }
         }
     }
 }
@@ -212,33 +277,25 @@ __global__ void __launch_bounds__(256) scatter_kernel(const bdgfs_hybrid_args h,
 // Conservation projection of compact row `row` fused with its scatter:
 // the corrected values go straight to Q[sur_idx[row]] (or, on a re-checked
 // cell, are compared with the spectral values already there).
-template <typename T>
+template <typename T, int VEC>
 __global__ void __launch_bounds__(256) project_scatter_kernel(const bdgfs_hybrid_args h,
                                                               const T* __restrict__ Qc, T* __restrict__ Q)
 {
     __shared__ double red[5 * 8];
+    __shared__ double cs[kMaxNv];
     const int64_t row = blockIdx.x;
     if (row == 0 && threadIdx.x == 0 && h.seed_dev) *h.seed_dev += 1;   // next step's sample
     const int64_t cnt = *h.counts;
     if (row >= cnt) return;
     const int Nv = h.Nv;
-    const int64_t n = int64_t(Nv) * Nv * Nv;
-    const T* src = Qc + row * n;
+    const int n = Nv * Nv * Nv;
+    const T* src = Qc + row * int64_t(n);
     const int64_t dof = h.sur_idx[row];
-    T* dst = Q + dof * n;
-    const double* c0 = h.c0;
+    T* dst = Q + dof * int64_t(n);
+    for (int i = threadIdx.x; i < Nv; i += blockDim.x) cs[i] = h.c0[i];
+    __syncthreads();
     double m[5] = {0, 0, 0, 0, 0};
-    for (int v = threadIdx.x; v < int(n); v += blockDim.x) {
-        uint32_t ix, iy, iz;
-        vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
-        const double cx = c0[ix], cy = c0[iy], cz = c0[iz];
-        const double x = double(src[v]);
-        m[0] += x;
-        m[1] += cx * x;
-        m[2] += cy * x;
-        m[3] += cz * x;
-        m[4] += (cx * cx + cy * cy + cz * cz) * x;
-    }
+    row_moments<T, VEC>(src, n, Nv, cs, m);
     block_sum<5>(m, red);
     double lam[5];
 #pragma unroll
@@ -250,18 +307,30 @@ __global__ void __launch_bounds__(256) project_scatter_kernel(const bdgfs_hybrid
     }
     const bool re = h.flag[dof] == 2;
     double e[2] = {0, 0};
-    for (int v = threadIdx.x; v < int(n); v += blockDim.x) {
+#pragma unroll 2
+    for (int v = threadIdx.x * VEC; v < n; v += blockDim.x * VEC) {
+        Chunk<T, VEC> c;
+        c.load(src + v);
         uint32_t ix, iy, iz;
         vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
-        const double cx = c0[ix], cy = c0[iy], cz = c0[iz];
-        const double c2 = cx * cx + cy * cy + cz * cz;
-        const T q = T(double(src[v]) - (lam[0] + lam[1] * cx + lam[2] * cy + lam[3] * cz + lam[4] * c2));
+        const double cx = cs[ix], cy = cs[iy];
+        const double lxy = lam[0] + lam[1] * cx + lam[2] * cy + lam[4] * (cx * cx + cy * cy);
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) {
+            const double cz = cs[iz + j];
+            c.v[j] = T(double(c.v[j]) - (lxy + lam[3] * cz + lam[4] * cz * cz));
+        }
         if (!re) {
-            dst[v] = q;
+            c.store(dst + v);
         } else {
-            const double d = double(q) - double(dst[v]);
-            e[0] += d * d;
-            e[1] += double(dst[v]) * double(dst[v]);
+            Chunk<T, VEC> sp;
+            sp.load(dst + v);
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) {
+                const double d = double(c.v[j]) - double(sp.v[j]);
+                e[0] += d * d;
+                e[1] += double(sp.v[j]) * double(sp.v[j]);
+            }
         }
     }
     if (!re) return;                                   // uniform per block
@@ -312,10 +381,19 @@ extern "C" int32_t bdgfs_hybrid_classify(const bdgfs_hybrid_args* h, const void*
     if (h->recheck_err && cudaMemsetAsync(h->recheck_err, 0, 2 * sizeof(double), st) != cudaSuccess)
         return BDGFS_ECUDA;
     if (h->ndof == 0) return BDGFS_OK;
-    if (h->fp64)
-        indicator_kernel<double><<<unsigned(h->ndof), 256, 0, st>>>(*h, static_cast<const double*>(f));
-    else
-        indicator_kernel<float><<<unsigned(h->ndof), 256, 0, st>>>(*h, static_cast<const float*>(f));
+    const bool v4 = h->Nv % 4 == 0 && (reinterpret_cast<uintptr_t>(f) & 15u) == 0 &&
+                    (!h->dev_rows || (reinterpret_cast<uintptr_t>(h->dev_rows) & 7u) == 0);
+    if (h->fp64) {
+        if (v4)
+            indicator_kernel<double, 4><<<unsigned(h->ndof), 256, 0, st>>>(*h, static_cast<const double*>(f));
+        else
+            indicator_kernel<double, 1><<<unsigned(h->ndof), 256, 0, st>>>(*h, static_cast<const double*>(f));
+    } else {
+        if (v4)
+            indicator_kernel<float, 4><<<unsigned(h->ndof), 256, 0, st>>>(*h, static_cast<const float*>(f));
+        else
+            indicator_kernel<float, 1><<<unsigned(h->ndof), 256, 0, st>>>(*h, static_cast<const float*>(f));
+    }
     return cuda_status(cudaGetLastError());
 }
 
@@ -358,12 +436,23 @@ extern "C" int32_t bdgfs_hybrid_project_scatter(const bdgfs_hybrid_args* h, cons
     if (!Qc || !Q || !h->counts || !h->sur_idx || !h->flag || !h->ginv) return BDGFS_EINVAL;
     if (h->ndof == 0) return BDGFS_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (h->fp64)
-        project_scatter_kernel<double><<<unsigned(h->ndof), 256, 0, st>>>(
-            *h, static_cast<const double*>(Qc), static_cast<double*>(Q));
-    else
-        project_scatter_kernel<float><<<unsigned(h->ndof), 256, 0, st>>>(
-            *h, static_cast<const float*>(Qc), static_cast<float*>(Q));
+    const bool v4 = h->Nv % 4 == 0 && (reinterpret_cast<uintptr_t>(Qc) & 15u) == 0 &&
+                    (reinterpret_cast<uintptr_t>(Q) & 15u) == 0;
+    if (h->fp64) {
+        if (v4)
+            project_scatter_kernel<double, 4><<<unsigned(h->ndof), 256, 0, st>>>(
+                *h, static_cast<const double*>(Qc), static_cast<double*>(Q));
+        else
+            project_scatter_kernel<double, 1><<<unsigned(h->ndof), 256, 0, st>>>(
+                *h, static_cast<const double*>(Qc), static_cast<double*>(Q));
+    } else {
+        if (v4)
+            project_scatter_kernel<float, 4><<<unsigned(h->ndof), 256, 0, st>>>(
+                *h, static_cast<const float*>(Qc), static_cast<float*>(Q));
+        else
+            project_scatter_kernel<float, 1><<<unsigned(h->ndof), 256, 0, st>>>(
+                *h, static_cast<const float*>(Qc), static_cast<float*>(Q));
+    }
     return cuda_status(cudaGetLastError());
 }
 

@@ -106,7 +106,19 @@ def test_indicator_rows_features_and_heads(cuda):
     _lib.check(_lib.lib().bdgfs_hybrid_scatter(C.byref(h.args), h.Qc.data_ptr(), out2.data_ptr(),
                                                _lib.stream_ptr()), 's')
     torch.cuda.synchronize()
-    assert torch.equal(out1, out2)
+    assert torch.allclose(out1, out2, rtol=1e-5, atol=1e-6 * float(out2.abs().max()))
+    # unaligned rows take the scalar path: same lists, rows and features
+    buf = torch.empty(f.numel() + 1, device=be.device)
+    fu = buf[1:].view_as(f)
+    fu.copy_(f)
+    ref = (h.sur_s[:m].clone(), h.dev_rows[:m].clone(), h.xc[:m].clone(), h.sur_idx[:m].clone())
+    h.classify(fu)
+    torch.cuda.synchronize()
+    order = torch.argsort(h.sur_idx[:m])
+    order0 = torch.argsort(ref[3])
+    assert torch.equal(h.sur_idx[:m][order], ref[3][order0])
+    assert torch.allclose(h.sur_s[:m][order], ref[0][order0], rtol=1e-6)
+    assert float((h.dev_rows[:m][order].float() - ref[1][order0].float()).abs().max()) < 1e-2
 
 
 def test_head_labels_recombine_to_q(cuda):
