@@ -23,6 +23,7 @@ EXPORTS = (
     'bdgfs_gemm', 'bdgfs_colsum', 'bdgfs_adamw', 'bdgfs_relmse',
     'bdgfs_hybrid_classify', 'bdgfs_hybrid_project', 'bdgfs_hybrid_scatter',
     'bdgfs_hybrid_project_scatter', 'bdgfs_hybrid_heads',
+    'bdgfs_bgk_moments', 'bdgfs_bgk_maxwellian', 'bdgfs_ars_stage',
 )
 
 
@@ -84,6 +85,16 @@ class HybridArgs(C.Structure):
                 ('sur_s', C.c_void_p)]
 
 
+class ArsArgs(C.Structure):
+    _fields_ = [('ndof', C.c_int64), ('Nv', C.c_int32), ('fp64', C.c_int32),
+                ('c0', C.c_void_p), ('cw', C.c_double),
+                ('prefac', C.c_double), ('omega', C.c_double), ('dt', C.c_double),
+                ('stage', C.c_int32), ('flags', C.c_int32),
+                ('ae', C.c_double * 4), ('ai', C.c_double * 4),
+                ('f', C.c_void_p * 4), ('fout', C.c_void_p), ('L', C.c_void_p * 4),
+                ('U', C.c_void_p * 5), ('LU', C.c_void_p * 4)]
+
+
 _lib = None
 
 
@@ -123,6 +134,9 @@ def lib():
             'bdgfs_hybrid_scatter': [vp, vp, vp, vp],
             'bdgfs_hybrid_project_scatter': [vp, vp, vp, vp],
             'bdgfs_hybrid_heads': [vp, vp, C.c_int64, C.c_int64, C.c_int32, vp, C.c_int64, vp],
+            'bdgfs_bgk_moments': [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_double, vp, vp],
+            'bdgfs_bgk_maxwellian': [vp, C.c_int64, C.c_int32, C.c_int32, vp, vp, vp],
+            'bdgfs_ars_stage': [vp, vp],
             'bdgfs_colsum': [vp, i64, i64, vp, vp],
             'bdgfs_adamw': [vp, vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float,
                             C.c_float, C.c_float, i64, vp],

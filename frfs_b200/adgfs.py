@@ -1,0 +1,175 @@
+"""The 'adgfs' system: FR advection with the BGK relaxation operator,
+advanced by the ARS IMEX steppers.
+
+Mirrors frfs/solvers/adgfs/system.py (ADGFSSystem, name 'adgfs') and
+frfs/solvers/adgfs/scattering.py (ADGFSBGKDirectGLLScatteringModel,
+``scattering_model = 'bgk-direct-gll'``), with the reference's method
+names (``moment``, ``constructMaxwellian``, ``updateMomentARS``,
+``updateDistARS``, ``get_nregs_moms``) on top of the fused stage entry
+``bdgfs_ars_stage`` that the project's ARS steppers use.  Moment rows are
+FP64 ``[ndof][5]`` = (rho, rho u, E) as in the reference
+(nalph = 5).
+"""
+import ctypes as C
+
+import torch
+
+from . import _lib
+from .system import DGFSSystem
+from .util import subclass_where  # noqa: F401
+
+ARS_MOM0, ARS_MOML, ARS_MOMU, ARS_DIST = 1, 2, 4, 8
+R0 = 8.3144598
+NA = 6.0221409e+23
+
+
+class ADGFSScatteringModel:
+    """Registry base (scattering.py: ADGFSScatteringModel)."""
+    scattering_model = None
+
+    def __init__(self, backend, cfg, velocitymesh):
+        self.backend, self.cfg, self.vm = backend, cfg, velocitymesh
+        self.load_parameters()
+        self.perform_precomputation()
+
+    def collide(self, *args, **kwargs):
+        raise RuntimeError('Not valid for asymptotic systems')
+
+
+class ADGFSBGKDirectGLLScatteringModel(ADGFSScatteringModel):
+    """BGK relaxation nu (M[f] - f), nu = prefac rho T^(1 - omega), Pr = 1."""
+    scattering_model = 'bgk-direct-gll'
+    nalph = 5
+
+    def load_parameters(self):
+        cfg, vm = self.cfg, self.vm
+        omega = cfg.getfloat('scattering-model', 'omega')
+        muRef = cfg.getfloat('scattering-model', 'muRef')
+        Tref = cfg.getfloat('scattering-model', 'Tref')
+        t0 = vm.H0() / vm.u0()                           # time scale
+        visc = muRef * (vm.T0() / Tref)**omega           # viscosity at T0
+        p0 = vm.n0() * R0 / NA * vm.T0()                 # pressure scale
+        self._prefactor = t0 * p0 / visc
+        self._omega = omega
+        self._Pr = 1.0
+
+    def nu(self, rho, T):
+        return self._prefactor * rho * T**(1 - self._omega)
+
+    def perform_precomputation(self):
+        dev = self.backend.device
+        self.c0 = torch.as_tensor(self.vm.c0(), dtype=torch.float64, device=dev).contiguous()
+        self.cw = float(self.vm.cw())
+        self.fp64 = int(self.backend.fpdtype == torch.float64)
+
+    # reference kernels ---------------------------------------------------
+    def moment(self, f, U):
+        """U[dof] <- (rho, rho u, E) of f[dof] (FP64)."""
+        n = self.vm.vsize()
+        _lib.check(_lib.lib().bdgfs_bgk_moments(f.data_ptr(), f.numel() // n, self.vm.Nv(),
+                                                self.fp64, self.c0.data_ptr(), self.cw,
+                                                U.data_ptr(), _lib.stream_ptr()),
+                   'bdgfs_bgk_moments')
+
+    def constructMaxwellian(self, U, M):
+        n = self.vm.vsize()
+        _lib.check(_lib.lib().bdgfs_bgk_maxwellian(U.data_ptr(), M.numel() // n, self.vm.Nv(),
+                                                   self.fp64, self.c0.data_ptr(), M.data_ptr(),
+                                                   _lib.stream_ptr()), 'bdgfs_bgk_maxwellian')
+
+    def ars_stage(self, ndof, dt, ar, flags, ae, ai, f, fout, L, U, LU):
+        """One fused ARS stage (bdgfs_ars_stage) over ndof distributions;
+        f, L, U, LU are lists of tensors (None where the flags do not need
+        them)."""
+        p = lambda t: t.data_ptr() if t is not None else None
+        a = _lib.ArsArgs(ndof=int(ndof),
+                         Nv=self.vm.Nv(), fp64=self.fp64, c0=self.c0.data_ptr(), cw=self.cw,
+                         prefac=self._prefactor, omega=self._omega, dt=float(dt), stage=ar,
+                         flags=flags)
+        for j, x in enumerate(ae):
+            a.ae[j] = x
+        for j, x in enumerate(ai):
+            a.ai[j] = x
+        for j, t in enumerate(f):
+            a.f[j] = p(t)
+        a.fout = p(fout)
+        for j, t in enumerate(L):
+            a.L[j] = p(t)
+        for j, t in enumerate(U):
+            a.U[j] = p(t)
+        for j, t in enumerate(LU):
+            a.LU[j] = p(t)
+        _lib.check(_lib.lib().bdgfs_ars_stage(C.byref(a), _lib.stream_ptr()), 'bdgfs_ars_stage')
+
+
+class ADGFSSystem(DGFSSystem):
+    """'adgfs' (system.py:17-121): FR advection plus BGK relaxation."""
+    name = 'adgfs'
+    scatteringcls = ADGFSScatteringModel
+
+    def __init__(self, *args, **kwargs):
+        super().__init__(*args, **kwargs)
+        self.nreg_moms = None
+
+    @property
+    def ndof(self):
+        return self.ele.neles * self.ele.nupts
+
+    def get_nregs_moms(self, nreg_moms):
+        """Moment banks [ndof][5] FP64 (system.py:31-52)."""
+        if self.nreg_moms is not None and self.nreg_moms != nreg_moms:
+            raise RuntimeError('moment registers already allocated with another count')
+        if self.nreg_moms is None:
+            dev = self.backend.device
+            self.eles_scal_upts_inb_moms = [
+                torch.zeros(self.ndof, self.sm.nalph, dtype=torch.float64, device=dev)
+                for _ in range(nreg_moms)]
+            self.nreg_moms = nreg_moms
+            self.nalph = self.sm.nalph
+        return list(range(nreg_moms))
+
+    def _mom(self, i):
+        return self.eles_scal_upts_inb_moms[i] if isinstance(i, int) else i
+
+    def _ref(self, i):
+        return self._bank(i) if isinstance(i, int) else i
+
+    def collide(self, *args, **kwargs):
+        raise RuntimeError('Not valid for asymptotic systems')
+
+    # reference methods (system.py:62-121) --------------------------------
+    def moment(self, t, finbank, momoutbank, fscratchbank=None):
+        self.sm.moment(self._bank(finbank), self._mom(momoutbank))
+
+    def constructMaxwellian(self, t, mominbank, Mcoeffbank, momscratchbank=None):
+        self.sm.constructMaxwellian(self._mom(mominbank), self._bank(Mcoeffbank))
+
+    def updateMomentARS(self, dt, *args):
+        """args = _A[ar][0:ar], A[ar][1:ar+1], LU_0..LU_{ar-1}, U_0..U_ar."""
+        ar = (len(args) - 1) // 4
+        if len(args) != 4 * ar + 1:
+            raise ValueError('updateMomentARS: inconsistent number of arguments')
+        ae, ai = args[:ar], args[ar:2 * ar]
+        LU = [self._mom(x) for x in args[2 * ar:3 * ar]]
+        U = [self._mom(x) for x in args[3 * ar:]]
+        self.sm.ars_stage(self.ndof, dt, ar, ARS_MOMU, ae, ai, [None] * ar, None, [None] * ar, U,
+                          LU)
+
+    def updateDistARS(self, dt, *args):
+        """args = _A[ar][0:ar], A[ar][1:ar+1], L_0..L_{ar-1}, U_0..U_ar,
+        M_1..M_ar (unused: the Maxwellians are rebuilt from U on the fly),
+        f_0..f_ar (f_ar is the output)."""
+        q = (len(args) - 2) // 6
+        if len(args) != 6 * q + 2:
+            raise ValueError('updateDistARS: inconsistent number of arguments')
+        ae, ai = args[:q], args[q:2 * q]
+        L = [self._ref(x) for x in args[2 * q:3 * q]]
+        U = [self._mom(x) for x in args[3 * q:4 * q + 1]]
+        F = [self._ref(x) for x in args[5 * q + 1:]]
+        self.sm.ars_stage(self.ndof, dt, q, ARS_DIST, ae, ai, F[:q], F[q], L, U, [None] * q)
+
+    # fused stage used by the project's ARS steppers ------------------------
+    def ars_stage(self, dt, ar, flags, ae, ai, fbanks, foutbank, Lbanks, Umoms, LUmoms):
+        self.sm.ars_stage(self.ndof, dt, ar, flags, ae, ai, [self._bank(b) for b in fbanks],
+                          self._bank(foutbank), [self._bank(b) for b in Lbanks],
+                          [self._mom(m) for m in Umoms], [self._mom(m) for m in LUmoms])

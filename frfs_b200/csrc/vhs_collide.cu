@@ -93,7 +93,8 @@ __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
     constexpr int FS = L::FS;
     constexpr int NP = N * N;                 // pencils per pass
     constexpr int NPT = (NP + NT - 1) / NT;   // pencils per thread
-    static_assert(SG || NP % NT == 0, "register S_p needs whole x-pencils per thread");
+    // register S_p: thread tid owns x-pencils tid + r*NT (r < NPT; the last
+    // round is partial when NT does not divide N*N)
     const int tid = threadIdx.x;
     const int M = g.M, Nrho = g.Nrho;
 
@@ -299,6 +300,7 @@ __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
 #pragma unroll
                 for (int r = 0; r < NPT; ++r) {
                     const int pid = tid + r * NT;
+                    if (NP % NT != 0 && pid >= NP) break;
                     const int y = pid / N, z = pid % N;
                     cpx<T> v[N];
 #pragma unroll
@@ -333,6 +335,7 @@ __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
 #pragma unroll
             for (int r = 0; r < NPT; ++r) {
                 const int pid = tid + r * NT;
+                if (NP % NT != 0 && pid >= NP) break;
                 const int y = pid / N, z = pid % N;
                 cpx<T> v[N];
 #pragma unroll
@@ -617,6 +620,8 @@ static const Entry kEntries[] = {
     ENTRYG(1, double, 256, 16, 2),
     ENTRY1(1, double, 144, 12, false, false),
     ENTRY1(1, double, 64, 8, false, false),
+    // appended variants (earlier tile indices stay valid)
+    ENTRY1(0, float, 384, 24, false, false),
 };
 static constexpr int kNumEntries = int(sizeof(kEntries) / sizeof(kEntries[0]));
 

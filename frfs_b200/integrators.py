@@ -7,6 +7,9 @@ stepper chosen by ``[solver-time-integrator] scheme``:
 * 'dgfs-euler'   (steppers.py:20-99):  u <- u + dt (L + Q)(u)
 * 'dgfs-tvd-rk2' (steppers.py:103-225): u1 = u + dt (L+Q)(u);
                  u <- u/2 + u1/2 + dt/2 (L+Q)(u1)
+* 'adgfs-ars-111/222/443' (steppers.py:489-670): IMEX Runge-Kutta with the
+                 FR advection explicit and the BGK relaxation implicit
+                 ('adgfs' system, frfs_b200.adgfs)
 
 Each stage is one ``collide`` launch (all DOFs) plus the disu / bc-update /
 fused-rhs launches; the register banks are those of the reference (r0, r1,
@@ -137,7 +140,77 @@ class StdTVDRK2DGFSStepper(BaseDGFSStepper):
                          x1=2, c1=0.5 * dt, x2=0, c2=0.5)         #      + dt/2 (L+Q)(r1)
 
 
-STEPPERS = {c.stepper_name: c for c in (StdEulerDGFSStepper, StdTVDRK2DGFSStepper)}
+class ARSabcAstdStepper(BaseDGFSStepper):
+    """a-stage explicit, b-stage implicit, c-order ARS IMEX schemes for the
+    'adgfs' system (steppers.py:500-585): the explicit part is the FR
+    advection L(f) = -div(c f) (bc update included), the implicit part the
+    BGK relaxation.  Per stage i (ar = i+1): L_i = L(F_i), then one fused
+    launch forms LU_i, U_ar and F_ar (bdgfs_ars_stage).  Banks: F_0 (the
+    solution; the last stage updates it in place), F_1..F_{s-1}, L_0..L_{s-1};
+    moment rows U_0..U_s, LU_0..LU_{s-1}."""
+    _A = A = None
+
+    @classmethod
+    def nstages(cls):
+        return len(cls._A) - 1
+
+    def __init__(self, backend, system, cfg):
+        super().__init__(backend, system, cfg)
+        s = self.nstages()
+        moms = system.get_nregs_moms(2 * s + 1)
+        self._U, self._LU = moms[:s + 1], moms[s + 1:]
+        self._F = [0] + list(range(1, s)) + [0]
+        self._L = list(range(s, 2 * s))
+
+    def _step_kernels(self, t, dt):
+        from .adgfs import ARS_DIST, ARS_MOM0, ARS_MOML, ARS_MOMU
+        sysm, s = self.system, self.nstages()
+        for i in range(s):
+            ar = i + 1
+            sysm.advect_combine(t, self._F[i], self._L[i], a=0.0, b=1.0)     # L_i = L(F_i)
+            flags = ARS_MOML | ARS_MOMU | ARS_DIST | (ARS_MOM0 if i == 0 else 0)
+            sysm.ars_stage(dt, ar, flags, self._A_expl(ar), self._A_impl(ar), self._F[:ar],
+                           self._F[ar], self._L[:ar], self._U[:ar + 1], self._LU[:ar])
+
+    @classmethod
+    def _A_expl(cls, ar):
+        return cls._A[ar][:ar]
+
+    @classmethod
+    def _A_impl(cls, ar):
+        return cls.A[ar][1:ar + 1]
+
+
+class ARS111AstdStepper(ARSabcAstdStepper):
+    stepper_name = 'adgfs-ars-111'
+    order = 1
+    _A = [[0., 0.], [1., 0.]]
+    A = [[0., 0.], [0., 1.]]
+    nregs = 2
+
+
+class ARS222AstdStepper(ARSabcAstdStepper):
+    stepper_name = 'adgfs-ars-222'
+    order = 2
+    gamma = 1. - (2.**0.5) / 2.
+    delta = 1. - 1. / (2. * gamma)
+    _A = [[0., 0., 0.], [gamma, 0., 0.], [delta, 1 - delta, 0.]]
+    A = [[0., 0., 0.], [0., gamma, 0.], [0., 1 - gamma, gamma]]
+    nregs = 4
+
+
+class ARS443AstdStepper(ARSabcAstdStepper):
+    stepper_name = 'adgfs-ars-443'
+    order = 3
+    _A = [[0., 0., 0., 0., 0.], [1. / 2., 0., 0., 0., 0.], [11. / 18., 1. / 18., 0., 0., 0.],
+          [5. / 6., -5. / 6., 1. / 2., 0., 0.], [1. / 4., 7. / 4., 3. / 4., -7. / 4., 0.]]
+    A = [[0., 0., 0., 0., 0.], [0., 1. / 2., 0., 0., 0.], [0., 1. / 6., 1. / 2., 0., 0.],
+         [0., -1. / 2., 1. / 2., 1. / 2., 0.], [0., 3. / 2., -3. / 2., 1. / 2., 1. / 2.]]
+    nregs = 8
+
+
+STEPPERS = {c.stepper_name: c for c in (StdEulerDGFSStepper, StdTVDRK2DGFSStepper,
+                                        ARS111AstdStepper, ARS222AstdStepper, ARS443AstdStepper)}
 
 
 def get_integrator(backend, system_or_factory, cfg):

@@ -302,6 +302,53 @@ int32_t bdgfs_hybrid_heads(const bdgfs_hybrid_args* h, const float* Y,
                            int64_t ldy, int64_t k, int32_t nheads,
                            void* out, int64_t ldo, void* stream);
 
+/* ------------------------------------------------------------------------
+ * BGK relaxation ('bgk-direct-gll') and the ARS IMEX stage update of the
+ * 'adgfs' system (frfs/solvers/adgfs/scattering.py,
+ * frfs/solvers/adgfs/kernels/scattering/bgk-direct-gll.mako,
+ * linear-common-direct-gll.mako, frfs/integrators/std/steppers.py:489-670).
+ * Moment rows U[dof][5] = (rho, rho u_x, rho u_y, rho u_z, E), FP64,
+ * E = sum |c|^2 f cw; T = (E - |rho u|^2/rho) / (1.5 rho);
+ * nu = prefac * rho * T^(1 - omega); M = rho/(pi T)^1.5 exp(-|c-u|^2/T).
+ * ---------------------------------------------------------------------- */
+#define BDGFS_ARS_MOM0 1   /* U[0]      <- moments of f[0]                  */
+#define BDGFS_ARS_MOML 2   /* LU[ar-1]  <- moments of L[ar-1]               */
+#define BDGFS_ARS_MOMU 4   /* U[ar]     <- U[0] + dt sum_j ae[j] LU[j]      */
+#define BDGFS_ARS_DIST 8   /* fout      <- (f0 + sum_j ae[j] dt L_j
+                                + sum_{j=1}^{ar-1} ai[j-1] dt nu_j (M_j - f_j)
+                                + ai[ar-1] dt nu_ar M_ar)
+                               / (1 + ai[ar-1] dt nu_ar)                    */
+
+typedef struct bdgfs_ars_args {
+    int64_t ndof;            /* distributions (rows)                        */
+    int32_t Nv;              /* 1..64                                       */
+    int32_t fp64;
+    const double* c0;        /* [Nv]                                        */
+    double cw;
+    double prefac, omega, dt;
+    int32_t stage;           /* ar = 1..4                                   */
+    int32_t flags;           /* BDGFS_ARS_*                                 */
+    double ae[4];            /* explicit row _A[ar][0..ar-1]                */
+    double ai[4];            /* implicit row A[ar][1..ar]                   */
+    const void* f[4];        /* f_0 .. f_{ar-1}                             */
+    void* fout;              /* f_ar (may be f_0: updated in place)         */
+    const void* L[4];        /* L_0 .. L_{ar-1} (explicit FR parts)          */
+    double* U[5];            /* moment rows U_0 .. U_ar                     */
+    double* LU[4];           /* moment rows of L_0 .. L_{ar-1}              */
+} bdgfs_ars_args;
+
+/* U[dof] = moments of f[dof]: ADGFSBGKDirectGLLScatteringModel.moment. */
+int32_t bdgfs_bgk_moments(const void* f, int64_t ndof, int32_t Nv, int32_t fp64,
+                          const double* c0, double cw, double* U, void* stream);
+/* M[dof] = Maxwellian of U[dof]: cmaxwellian (bgk-direct-gll.mako:4-50). */
+int32_t bdgfs_bgk_maxwellian(const double* U, int64_t ndof, int32_t Nv,
+                             int32_t fp64, const double* c0, void* M,
+                             void* stream);
+/* One ARS stage (the flagged parts, in the order MOM0, MOML, MOMU, DIST):
+ * updateMom{ar}_ARS + cmaxwellian + updateDistribution{ar}_ARS in one
+ * launch, the Maxwellians computed on the fly. */
+int32_t bdgfs_ars_stage(const bdgfs_ars_args* a, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,92 @@
+"""Oracle: BGK relaxation ('bgk-direct-gll') and the ARS IMEX steppers (FP64).
+
+Restates, in numpy, for test use only:
+  prefactor     t0 p0 / visc, t0 = H0/u0, visc = muRef (T0/Tref)^omega,
+                p0 = n0 R0/NA T0           (frfs/solvers/adgfs/scattering.py,
+                                            ADGFSBGKDirectGLLScatteringModel.load_parameters)
+  moments       U = (sum f, sum c f, sum |c|^2 f) cw  (mat of perform_precomputation)
+  Maxwellian    T = (U4 - |U1:3|^2/U0)/(1.5 U0), M = U0/(pi T)^1.5 exp(-|c-u|^2/T)
+                                           (kernels/scattering/bgk-direct-gll.mako:4-50)
+  nu            prefac U0 T^(1-omega)      (linear-common-direct-gll.mako:121-130)
+  ARS stage ar  U_ar = U_0 + dt sum_{j<ar} _A[ar][j] LU_j        (updateMom{ar}_ARS)
+                f_ar = (f_0 + sum_{j<ar} _A[ar][j] dt L_j
+                        + sum_{j=1}^{ar-1} A[ar][j] dt nu_j (M_j - f_j)
+                        + A[ar][ar] dt nu_ar M_ar) / (1 + A[ar][ar] dt nu_ar)
+                                           (updateDistribution{ar}_ARS,
+                                            linear-common-direct-gll.mako:90-145)
+  stepper       ARSabcAstdStepper.step     (frfs/integrators/std/steppers.py:531-585)
+                with the tables of ARS-111/222/443 (steppers.py:589-670).
+Distributions are arrays [..., nv]; moments [..., 5].
+"""
+import numpy as np
+
+R0 = 8.3144598
+NA = 6.0221409e+23
+
+_g = 1.0 - 2.0**0.5 / 2.0
+_d = 1.0 - 1.0 / (2.0 * _g)
+ARS = {
+    'adgfs-ars-111': ([[0., 0.], [1., 0.]],
+                      [[0., 0.], [0., 1.]]),
+    'adgfs-ars-222': ([[0., 0., 0.], [_g, 0., 0.], [_d, 1 - _d, 0.]],
+                      [[0., 0., 0.], [0., _g, 0.], [0., 1 - _g, _g]]),
+    'adgfs-ars-443': ([[0., 0., 0., 0., 0.], [1 / 2, 0., 0., 0., 0.],
+                       [11 / 18, 1 / 18, 0., 0., 0.], [5 / 6, -5 / 6, 1 / 2, 0., 0.],
+                       [1 / 4, 7 / 4, 3 / 4, -7 / 4, 0.]],
+                      [[0., 0., 0., 0., 0.], [0., 1 / 2, 0., 0., 0.],
+                       [0., 1 / 6, 1 / 2, 0., 0.], [0., -1 / 2, 1 / 2, 1 / 2, 0.],
+                       [0., 3 / 2, -3 / 2, 1 / 2, 1 / 2]]),
+}
+
+
+def bgk_prefactor(H0, u0, T0, n0, omega, muRef, Tref):
+    t0 = H0 / u0
+    visc = muRef * (T0 / Tref)**omega
+    p0 = n0 * R0 / NA * T0
+    return t0 * p0 / visc
+
+
+def moments5(f, cv, cw):
+    c2 = np.sum(cv * cv, axis=0)
+    return np.stack([f.sum(-1), f @ cv[0], f @ cv[1], f @ cv[2], f @ c2], axis=-1) * cw
+
+
+def _state(U):
+    rho = U[..., 0]
+    u = U[..., 1:4] / rho[..., None]
+    T = (U[..., 4] - np.sum(U[..., 1:4]**2, axis=-1) / rho) / (1.5 * rho)
+    return rho, u, T
+
+
+def maxwellian(U, cv):
+    rho, u, T = _state(U)
+    d2 = sum((cv[k][None] - u.reshape(-1, 3)[:, k:k + 1])**2 for k in range(3))
+    d2 = d2.reshape(U.shape[:-1] + (cv.shape[1],))
+    return (rho / (np.pi * T)**1.5)[..., None] * np.exp(-d2 / T[..., None])
+
+
+def nu(U, prefac, omega):
+    rho, _, T = _state(U)
+    return prefac * rho * T**(1.0 - omega)
+
+
+def step_ars(f0, dt, L, scheme, prefac, omega, cv, cw):
+    """One ARS step of df/dt = L(f) + nu (M[f] - f); L(f) is the explicit
+    (advection) part, a callable on arrays shaped like f0."""
+    _A, A = ARS[scheme]
+    s = len(_A) - 1
+    F, Ls, LU = [f0], [], []
+    U = [moments5(f0, cv, cw)]
+    for i in range(s):
+        ar = i + 1
+        Ls.append(L(F[i]))
+        LU.append(moments5(Ls[i], cv, cw))
+        U.append(U[0] + dt * sum(_A[ar][j] * LU[j] for j in range(ar)))
+        num = F[0] + sum(_A[ar][j] * dt * Ls[j] for j in range(ar))
+        for j in range(1, ar):
+            num = num + A[ar][j] * dt * nu(U[j], prefac, omega)[..., None] * (
+                maxwellian(U[j], cv) - F[j])
+        nar = nu(U[ar], prefac, omega)[..., None]
+        num = num + A[ar][ar] * dt * nar * maxwellian(U[ar], cv)
+        F.append(num / (1.0 + A[ar][ar] * dt * nar))
+    return F[s]

@@ -36,6 +36,7 @@ STRUCTS = {
     'bdgfs_fr_walls': _lib.FrWall,
     'bdgfs_gemm_args': _lib.GemmArgs,
     'bdgfs_hybrid_args': _lib.HybridArgs,
+    'bdgfs_ars_args': _lib.ArsArgs,
 }
 
 
