@@ -432,6 +432,70 @@ def small_fp64(flush, steps=20):
             'dtype': 'f64'}
 
 
+def ars_bgk(flush, steps=20):
+    """adgfs system: the Couette workload's mesh and velocity grid (16 x 8
+    quads P3, Nv=24^3, FP32) with BGK relaxation (omega 0.81) and the
+    ARS-222 IMEX stepper; DG steps/s and the HBM roofline of the fused
+    ARS stage kernel (stage 2: reads f0, L0, L1, f1 and L1 once more for
+    its moments, writes f2)."""
+    import torch
+    from frfs_b200.adgfs import ARS_DIST, ARS_MOML, ARS_MOMU, ADGFSSystem
+    from frfs_b200.backend import CUDABackend
+    from frfs_b200.inifile import Inifile
+    from frfs_b200.integrators import get_integrator
+    from frfs_b200.mesh import StructuredMesh
+    cfg = Inifile(couette_ini('single'))
+    for k, v in (('type', 'bgk-direct-gll'), ('muRef', '2.117e-5'), ('Tref', '273')):
+        cfg.set('scattering-model', k, v)
+    cfg.set('solver', 'system', 'adgfs')
+    cfg.set('solver-time-integrator', 'scheme', 'adgfs-ars-222')
+    be = CUDABackend(cfg)
+    mesh = StructuredMesh((WORK['nx'], WORK['ny']), (0.0, -0.5), (2.0, 0.5), periodic='x')
+    s = ADGFSSystem(be, mesh, cfg, nreg=4)
+    integ = get_integrator(be, s, cfg)
+    dt = WORK['dt']
+    for _ in range(3):
+        integ.step(0.0, dt)
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    tot = 0.0
+    for _ in range(steps):
+        flush.fill_(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        integ.step(0.0, dt)
+        b.record(st)
+        torch.cuda.synchronize()
+        tot += a.elapsed_time(b)
+    # the stage-2 kernel alone (same banks as inside the step)
+    Ae, Ai = integ._A_expl(2), integ._A_impl(2)
+    kt = 0.0
+    reps = 10
+    for _ in range(reps):
+        flush.fill_(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        s.ars_stage(dt, 2, ARS_MOML | ARS_MOMU | ARS_DIST, Ae, Ai, integ._F[:2], integ._F[2],
+                    integ._L[:2], integ._U[:3], integ._LU[:2])
+        b.record(st)
+        torch.cuda.synchronize()
+        kt += a.elapsed_time(b)
+    kt /= reps
+    elems = s.ndof * s.vm.vsize()
+    nbytes = elems * 4 * 6                       # 5 reads + 1 write of FP32 rows
+    peak = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                                       'MEASURED_PEAKS.json')))['hbm_gbs'] \
+        if os.path.exists(os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                                       'MEASURED_PEAKS.json')) else 6650.0
+    ach = nbytes / (kt * 1e-3) / 1e9
+    return {'workload': ('adgfs: 16x8 quads P3 (2048 DOFs), Nv=24^3, BGK (bgk-direct-gll, '
+                         'omega 0.81), ARS-222, dt=5e-4, FP32 state / FP64 moments'),
+            'dg_steps_per_s': steps / (tot * 1e-3), 'ms_per_step': tot / steps,
+            'stage_kernel': {'kernel': 'bdgfs::ars_kernel (stage 2)', 'ms': kt,
+                             'bytes': nbytes, 'achieved_gbs': ach, 'peak_gbs': peak,
+                             'frac': ach / peak, 'bound': 'hbm'}}
+
+
 def surrogate_legs(flush, log=None):
     """Config 4 (surrogate trained on the Couette family, evaluated on 50000
     held-out seeded distributions) and config 5 (8^3 hex P2 lid-driven
@@ -729,6 +793,7 @@ def run_gpu(args):
         extra['plain_fp64_small'] = small_fp64(flush)
         bq, _ = batched_q(flush)
         extra['batched_q'] = bq
+        extra['ars_bgk'] = ars_bgk(flush)
     if ws == 1 and not args.no_surrogate:
         c4, c5 = surrogate_legs(flush)
         extra['surrogate'] = c4
@@ -787,6 +852,55 @@ def run_q_only(ndof):
     print(json.dumps({'q_only_ndof': ndof, 'finite': bool(torch.isfinite(q).all())}))
 
 
+def run_surrogate_call(ndof, reps=2):
+    """Profiling case: all-surrogate hybrid calls on ndof Couette-family
+    cells with a randomly initialised 512-mode / width-1024 network (the
+    kernels and shapes of inference; timing only)."""
+    import torch
+    from frfs_b200.backend import CUDABackend
+    from frfs_b200.inifile import Inifile
+    from frfs_b200.scattering import DGFSVHSGLLScatteringModel
+    from frfs_b200.surrogate import HybridCollider, QSurrogate, sample_family
+    from frfs_b200.velocitymesh import DGFSVelocityMesh
+    cfg = Inifile(couette_ini('single'))
+    be = CUDABackend(cfg)
+    vm = DGFSVelocityMesh(be, cfg)
+    sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
+    q = QSurrogate(sm.grid, nmodes=512, width=1024)
+    dev = be.device
+    g = torch.Generator(device=dev).manual_seed(0)
+    n = q.n
+    q.Bd = torch.linalg.qr(torch.randn(n, 512, device=dev, generator=g))[0].t().contiguous()
+    q.Bq = torch.linalg.qr(torch.randn(n, 1536, device=dev, generator=g))[0].t().contiguous()
+    q.mu = torch.zeros(512, device=dev)
+    q.sigma = torch.full((512,), 0.05, device=dev)
+    q.hscale = torch.full((3,), 1e-3, device=dev)
+    q._init_params(g)
+    q._fold()
+    f = sample_family(vm.c0(), ndof, g, dev)
+    out = torch.empty_like(f)
+    h = HybridCollider(q, threshold=float('inf'), recheck=0.0)
+    for _ in range(2):
+        h(f, out)
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(reps):
+        h(f, out)
+    b.record(st)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    print(json.dumps({'surrogate_call_ndof': ndof, 'ms': ms, 'q_evals_per_s': ndof / ms * 1e3}))
+
+
+def run_ars_only():
+    """The adgfs ARS-222 leg alone (profiling case)."""
+    import torch
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device='cuda')
+    print(json.dumps(ars_bgk(flush)))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -800,9 +914,17 @@ def main():
                     help='skip the FP64 small and batched-collision measurements')
     ap.add_argument('--q-only', type=int, default=0, metavar='NDOF',
                     help='profiling case: 3 launches of the collision kernel on NDOF cubes')
+    ap.add_argument('--surrogate-call', type=int, default=0, metavar='NDOF',
+                    help='profiling case: all-surrogate hybrid calls on NDOF cells')
+    ap.add_argument('--ars-only', action='store_true',
+                    help='profiling case: the adgfs ARS-222 leg alone')
     args = ap.parse_args()
     if args.q_only:
         run_q_only(args.q_only)
+    elif args.surrogate_call:
+        run_surrogate_call(args.surrogate_call)
+    elif args.ars_only:
+        run_ars_only()
     elif args.impl == 'reference':
         run_reference(args)
     else:
