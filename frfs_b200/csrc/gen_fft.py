@@ -9,12 +9,15 @@ natural input and output order:
                                                         or +1 (inverse)
 
 which are the sign/normalisation conventions of a Z2Z FFT (forward and
-inverse both unnormalised).  The factorisation is the textbook
-Cooley-Tukey mixed-radix split N = N1*N2 (input index n = N2*n1 + n2,
-output index k = k1 + N1*k2), applied recursively with hand-written
-radix-2/3/4 butterflies; twiddles exp(sign*2*pi*i*e/N) are evaluated in
-FP64 by numpy here and emitted as literals, with the trivial ones
-(e = 0, N/4, N/2, 3N/4 and the odd multiples of N/8) specialised.
+inverse both unnormalised).  Lengths with a coprime factor 3 (12 = 3*4,
+24 = 3*8) use the Good-Thomas prime-factor split (Good 1958; Thomas 1963):
+CRT index maps, no twiddle factors between the stages.  Otherwise the
+factorisation is the textbook Cooley-Tukey mixed-radix split N = N1*N2
+(input index n = N2*n1 + n2, output index k = k1 + N1*k2), applied
+recursively with hand-written radix-2/3/4 butterflies; twiddles
+exp(sign*2*pi*i*e/N) are evaluated in FP64 by numpy here and emitted as
+literals, with the trivial ones (e = 0, N/4, N/2, 3N/4 and the odd
+multiples of N/8) specialised.
 """
 import os
 
@@ -144,10 +147,37 @@ def best_order(N):
     return min(itertools.permutations((4, 3, 2)), key=lambda o: (_opcount(N, o), o))
 
 
+def coprime_split(N):
+    """(N1, N2) with N = N1*N2, gcd = 1, N1 the factor 3 (24 = 3*8,
+    12 = 3*4), or None."""
+    from math import gcd
+    if N % 3 == 0 and N > 3 and gcd(3, N // 3) == 1:
+        return 3, N // 3
+    return None
+
+
+def pfa(em, xs, sign, N1, N2):
+    """Good-Thomas prime-factor split for coprime N1, N2 (no twiddles):
+    n = (N2 n1 + N1 n2) mod N, k = (N2 t1 k1 + N1 t2 k2) mod N with
+    t1 = N2^-1 mod N1, t2 = N1^-1 mod N2."""
+    N = N1 * N2
+    t1, t2 = pow(N2, -1, N1), pow(N1, -1, N2)
+    A = [dft(em, [xs[(N2 * n1 + N1 * n2) % N] for n1 in range(N1)], sign) for n2 in range(N2)]
+    X = [None] * N
+    for k1 in range(N1):
+        out = dft(em, [A[n2][k1] for n2 in range(N2)], sign)
+        for k2 in range(N2):
+            X[(N2 * t1 * k1 + N1 * t2 * k2) % N] = out[k2]
+    return X
+
+
 def dft(em, xs, sign):
     N = len(xs)
     if N <= 4:
         return butterfly(em, xs, sign)
+    sp = coprime_split(N)
+    if sp is not None:
+        return pfa(em, xs, sign, *sp)
     N1 = radix_of(N)
     N2 = N // N1
     # step 1: N2 DFTs of size N1 over x[N2*n1 + n2]

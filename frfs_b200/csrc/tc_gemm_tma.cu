@@ -6,7 +6,8 @@
 // chain: projection of the Maxwellian-deviation rows onto the input basis,
 // the MLP layers, reconstruction from the output basis).
 //
-// Tile 128 x 256 x 64.  One CTA per SM walks the output tiles
+// Tile 128 x 256 x 64 (128 x 128 x 64 for GEMMs whose 256-wide tiles
+// would occupy fewer than half the SMs).  One CTA per SM walks the output tiles
 // (n-fastest, so CTAs that share an A row-block run together and the
 // second read of it hits L2).  Warp roles:
 //   warp 0      one thread issues the TMA loads of A (128 x 64) and
@@ -40,15 +41,25 @@ namespace tma {
 
 using namespace tc;
 
-constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;
+constexpr int BM = 128, BK = 64;
 constexpr int THREADS = 192;
-constexpr uint32_t A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
-constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES;            // 48 KB
-constexpr uint32_t TMEM_COLS = 2 * BN;                          // two accumulators
-constexpr size_t SMEM_BYTES = size_t(STAGES) * STAGE_BYTES + 1024;   // + alignment slack
-constexpr uint32_t kIdesc = idesc_bf16(BM, BN);
+constexpr uint32_t A_BYTES = BM * BK * 2;
 constexpr uint32_t kPollLimit = 1u << 26;
 
+// Tile shape by BN (output columns per tile): 256 (48 KB stages, 4 deep)
+// or 128 (32 KB stages, 6 deep) for GEMMs with too few 256-wide tiles to
+// fill the SMs.
+template <int BN>
+struct Cfg {
+    static constexpr int STAGES = BN == 256 ? 4 : 6;
+    static constexpr uint32_t B_BYTES = BN * BK * 2;
+    static constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES;
+    static constexpr uint32_t TMEM_COLS = 2 * BN;                 // two accumulators
+    static constexpr size_t SMEM_BYTES = size_t(STAGES) * STAGE_BYTES + 1024;
+    static constexpr uint32_t IDESC = idesc_bf16(BM, BN);
+};
+
+template <int STAGES>
 struct Ctl {
     uint64_t full[STAGES], empty[STAGES], accf[2], acce[2], drain;
     uint32_t tmem;
@@ -136,12 +147,16 @@ __device__ __forceinline__ void store_row32(const bdgfs_gemm_args& g, int64_t or
     }
 }
 
+template <int BN>
 __global__ void __launch_bounds__(THREADS, 1)
     tma_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                     const bdgfs_gemm_args g)
 {
+    using C = Cfg<BN>;
+    constexpr int STAGES = C::STAGES;
+    constexpr uint32_t STAGE_BYTES = C::STAGE_BYTES, TMEM_COLS = C::TMEM_COLS, kIdesc = C::IDESC;
     extern __shared__ unsigned char smraw[];
-    __shared__ Ctl ctl;
+    __shared__ Ctl<STAGES> ctl;
     // stage buffers on a 1024-byte boundary (the 128-byte swizzle pattern)
     const uint32_t raw = smem_u32(smraw);
     unsigned char* sm = smraw + ((1024u - (raw & 1023u)) & 1023u);
@@ -309,22 +324,15 @@ int sm_count()
 
 }  // namespace tma
 
-int tma_gemm(const bdgfs_gemm_args& g, cudaStream_t st)
+namespace {
+
+template <int BN>
+int launch_bn(const bdgfs_gemm_args& g, cudaStream_t st, const CUtensorMap& ma, int nsm)
 {
     using namespace tma;
-    const auto a16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
-    if (g.engine != 0 || !g.a_bf16 || !g.b_bf16 || g.sak != 1 || g.sbk != 1 || g.arow || g.beta != 0.f)
-        return BDGFS_EUNSUPPORTED;
-    if (g.K % 8 || g.sam % 8 || g.sbn % 8 || g.sam < g.K || g.sbn < g.K || !a16(g.A) || !a16(g.B))
-        return BDGFS_EUNSUPPORTED;
-    if (g.M > (int64_t(1) << 31) - BM || g.N > (int64_t(1) << 31) - BN || g.K > (int64_t(1) << 31))
-        return BDGFS_EUNSUPPORTED;
-    if (g.act == 2 && !g.zin) return BDGFS_EINVAL;
-    CUtensorMap ma, mb;
-    if (!make_map(&ma, g.A, g.M, g.K, g.sam, BM) || !make_map(&mb, g.B, g.N, g.K, g.sbn, BN))
-        return BDGFS_EUNSUPPORTED;
-    const int nsm = sm_count();
-    if (nsm <= 0) return BDGFS_ECUDA;
+    using C = Cfg<BN>;
+    CUtensorMap mb;
+    if (!make_map(&mb, g.B, g.N, g.K, g.sbn, BN)) return BDGFS_EUNSUPPORTED;
     const int64_t tiles = ((g.M + BM - 1) / BM) * ((g.N + BN - 1) / BN);
     const unsigned grid = unsigned(tiles < nsm ? tiles : nsm);
     // dynamic shared-memory opt-in, once per device
@@ -335,14 +343,39 @@ int tma_gemm(const bdgfs_gemm_args& g, cudaStream_t st)
     {
         std::lock_guard<std::mutex> lock(mu);
         if (!attr_set[dev]) {
-            if (cudaFuncSetAttribute(tma_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int(SMEM_BYTES)) != cudaSuccess)
+            if (cudaFuncSetAttribute(tma_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(C::SMEM_BYTES)) != cudaSuccess)
                 return BDGFS_ECUDA;
             attr_set[dev] = true;
         }
     }
-    tma_gemm_kernel<<<grid, THREADS, SMEM_BYTES, st>>>(ma, mb, g);
+    tma_gemm_kernel<BN><<<grid, THREADS, C::SMEM_BYTES, st>>>(ma, mb, g);
     return cuda_status(cudaGetLastError());
+}
+
+}  // namespace
+
+int tma_gemm(const bdgfs_gemm_args& g, cudaStream_t st)
+{
+    using namespace tma;
+    const auto a16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+    if (g.engine != 0 || !g.a_bf16 || !g.b_bf16 || g.sak != 1 || g.sbk != 1 || g.arow || g.beta != 0.f)
+        return BDGFS_EUNSUPPORTED;
+    if (g.K % 8 || g.sam % 8 || g.sbn % 8 || g.sam < g.K || g.sbn < g.K || !a16(g.A) || !a16(g.B))
+        return BDGFS_EUNSUPPORTED;
+    if (g.M > (int64_t(1) << 31) - BM || g.N > (int64_t(1) << 31) - 256 || g.K > (int64_t(1) << 31))
+        return BDGFS_EUNSUPPORTED;
+    if (g.act == 2 && !g.zin) return BDGFS_EINVAL;
+    CUtensorMap ma;
+    if (!make_map(&ma, g.A, g.M, g.K, g.sam, BM)) return BDGFS_EUNSUPPORTED;
+    const int nsm = sm_count();
+    if (nsm <= 0) return BDGFS_ECUDA;
+    // 256-wide tiles unless they would occupy fewer than half the SMs (128-wide
+    // tiles double the A traffic and run the MMA at half width: measured
+    // slower whenever the 256-wide grid covers most SMs)
+    const int64_t tiles256 = ((g.M + BM - 1) / BM) * ((g.N + 255) / 256);
+    if (2 * tiles256 < int64_t(nsm)) return launch_bn<128>(g, st, ma, nsm);
+    return launch_bn<256>(g, st, ma, nsm);
 }
 
 }  // namespace bdgfs

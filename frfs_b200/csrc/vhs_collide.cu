@@ -64,6 +64,7 @@ struct QLayout {
         if (!WG) b += w_elems * sizeof(cpx<T>);
         b += fh_elems * sizeof(cpx<T>);
         b += size_t(M) * 3 * N * sizeof(cpx<T>);
+        b += size_t(M) * N * sizeof(cpx<T>);      // (Ez.x + Ez.y, Ez.x - Ez.y) per direction
         b += 10 * (NT / 32) * sizeof(double) + 16;
         return b;
     }
@@ -109,6 +110,8 @@ __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
     sp += L::fh_elems * sizeof(cpx<T>);
     cpx<T>* ph = reinterpret_cast<cpx<T>*>(sp);
     sp += size_t(M) * 3 * N * sizeof(cpx<T>);
+    cpx<T>* phab = reinterpret_cast<cpx<T>*>(sp);       // [q][kz]: (Ez.x + Ez.y, Ez.x - Ez.y)
+    sp += size_t(M) * N * sizeof(cpx<T>);
     double* red = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(sp) + 15) & ~uintptr_t(15));
 
     cpx<T>* Gh = reinterpret_cast<cpx<T>*>(scratch);   // [kz][kx<NH][ky]
@@ -195,8 +198,12 @@ __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
     }
 
     for (int p = 0; p < Nrho; ++p) {
-        for (int e = tid; e < M * 3 * N; e += NT)
-            ph[e] = phase[size_t(p) * M * 3 * N + e];
+        for (int e = tid; e < M * 3 * N; e += NT) {
+            const cpx<T> v = phase[size_t(p) * M * 3 * N + e];
+            ph[e] = v;
+            const int q = e / (3 * N), r = e - q * 3 * N;
+            if (r >= 2 * N) phab[q * N + (r - 2 * N)] = {v.x + v.y, v.x - v.y};
+        }
         __syncthreads();
 
         for (int qt = 0; qt < M * ntr; ++qt) {
@@ -232,18 +239,22 @@ __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
                         v[kz] = {-ms * F.y, ms * F.x};
                     }
                 } else if (!nyq) {
+                    // off the Nyquist planes m = Re(E) + Im(E), E = Pxy * Ez,
+                    // = Pxy.x (Ez.x + Ez.y) + Pxy.y (Ez.x - Ez.y)
                     const cpx<T> Pb = conjc(Pxy);
+                    const cpx<T>* ab = phab + (qt / ntr) * N;
 #pragma unroll
                     for (int kz = 0; kz < N; ++kz) {
                         cpx<T> F = direct ? fp[kz] : conjc(fp[(N - kz) % N]);
-                        const cpx<T> Ez = ep[2 * N + kz];
-                        const cpx<T> E = cmul(Pxy, Ez);
                         T m;
                         if (kz == N / 2) {
+                            const cpx<T> Ez = ep[2 * N + kz];
+                            const cpx<T> E = cmul(Pxy, Ez);
                             const cpx<T> Eb = cmul(Pb, Ez);
                             m = T(0.5) * (E.x + E.y + Eb.x - Eb.y);
                         } else {
-                            m = E.x + E.y;
+                            const cpx<T> w = ab[kz];
+                            m = Pxy.x * w.x + Pxy.y * w.y;
                         }
                         v[kz] = {m * F.x, m * F.y};
                     }
