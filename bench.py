@@ -894,6 +894,71 @@ def run_surrogate_call(ndof, reps=2):
     print(json.dumps({'surrogate_call_ndof': ndof, 'ms': ms, 'q_evals_per_s': ndof / ms * 1e3}))
 
 
+def run_fr_only(kind, reps=10):
+    """Profiling case: the FR kernels of one SSP-RK2 stage (disu, wall
+    update, fused rhs with two combination operands) on the Couette
+    (16x8 quads P3) or lid-cavity (8^3 hex P2) mesh, Nv=24^3, FP32; device
+    time per kernel and the fused rhs kernel's HBM roofline."""
+    import torch
+    from frfs_b200.backend import CUDABackend
+    from frfs_b200.inifile import Inifile
+    from frfs_b200.mesh import StructuredMesh
+    from frfs_b200.system import DGFSSystem
+    if kind == 'couette':
+        cfg = Inifile(couette_ini('single'))
+        mesh = StructuredMesh((WORK['nx'], WORK['ny']), (0.0, -0.5), (2.0, 0.5), periodic='x')
+    else:
+        ini = couette_ini('single', dict(WORK, order=2)).split('[soln-bcs-y-]')[0]
+        ini += """
+[soln-bcs-walls]
+type = dgfs-wall-diffuse
+rho = {rho}
+T = {T}
+ux = 0
+uy = 0
+uz = 0
+""".format(rho=NONDIM['rho0'], T=NONDIM['T0'])
+        cfg = Inifile(ini)
+        mesh = StructuredMesh((8, 8, 8), (0, 0, 0), (1, 1, 1), periodic='',
+                              bcnames={k: 'walls' for k in ('x-', 'x+', 'y-', 'y+', 'z-', 'z+')})
+    be = CUDABackend(cfg)
+    s = DGFSSystem(be, mesh, cfg, nreg=3)
+    st = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=be.device)
+    x1, x2 = s._bank(1), s._bank(2)
+    x1.copy_(s._bank(0))
+    x2.copy_(s._bank(0))
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(reps):
+            flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            fn()
+            b.record(st)
+            torch.cuda.synchronize()
+            tot += a.elapsed_time(b)
+        return tot / reps
+    s._active = (0, 1)
+    t_disu = timed(s._disu)
+    t_bc = timed(s._update_bc) if s.walls.nwall else 0.0
+    out = s._bank(1).clone()
+    t_rhs = timed(lambda: s._fused_rhs(a=0.5, b=2.5e-4, x1=x1, c1=2.5e-4, x2=x2, c2=0.5,
+                                       out=out))
+    E, U, F, nv = s.ele.neles, s.ele.nupts, s.ele.nfpts, s.vm.vsize()
+    nbytes = 4 * nv * E * (4 * U + 2 * F)          # u, x1, x2 in + out; own and neighbour faces
+    peak = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                                       'MEASURED_PEAKS.json')))['hbm_gbs']
+    print(json.dumps({'fr_only': kind, 'neles': E, 'nupts': U, 'nfpts': F, 'nv': nv,
+                      'disu_ms': t_disu, 'bc_update_ms': t_bc, 'rhs_ms': t_rhs,
+                      'rhs_bytes': nbytes, 'rhs_gbs': nbytes / (t_rhs * 1e-3) / 1e9,
+                      'rhs_frac_of_hbm': nbytes / (t_rhs * 1e-3) / 1e9 / peak,
+                      'disu_gbs': 4 * nv * E * (U + F) / (t_disu * 1e-3) / 1e9}))
+
+
 def run_ars_only():
     """The adgfs ARS-222 leg alone (profiling case)."""
     import torch
@@ -918,6 +983,8 @@ def main():
                     help='profiling case: all-surrogate hybrid calls on NDOF cells')
     ap.add_argument('--ars-only', action='store_true',
                     help='profiling case: the adgfs ARS-222 leg alone')
+    ap.add_argument('--fr-only', choices=['couette', 'cavity'],
+                    help='profiling case: the FR kernels of one RK stage')
     args = ap.parse_args()
     if args.q_only:
         run_q_only(args.q_only)
@@ -925,6 +992,8 @@ def main():
         run_surrogate_call(args.surrogate_call)
     elif args.ars_only:
         run_ars_only()
+    elif args.fr_only:
+        run_fr_only(args.fr_only)
     elif args.impl == 'reference':
         run_reference(args)
     else:

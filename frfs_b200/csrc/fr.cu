@@ -37,64 +37,167 @@ struct FrSmem {
 template <typename T>
 __device__ __forceinline__ void vel(const T* c0, int Nv, int64_t v, T (&c)[3])
 {
-    const int iz = int(v % Nv);
-    const int iy = int((v / Nv) % Nv);
-    const int ix = int(v / (int64_t(Nv) * Nv));
+    // v < Nv^3 <= 2^18: 32-bit arithmetic
+    const uint32_t vv = uint32_t(v), n = uint32_t(Nv);
+    const uint32_t q = vv / n, iz = vv - q * n;
+    const uint32_t ix = q / n, iy = q - ix * n;
     c[0] = c0[ix];
     c[1] = c0[iy];
     c[2] = c0[iz];
 }
 
-template <typename T, int NU, int NF>
-__global__ void __launch_bounds__(128) disu_kernel(const bdgfs_fr_eles el, const T* __restrict__ u,
-                                                   T* __restrict__ uf)
+// VB consecutive values of a velocity row (one vector access when aligned)
+template <typename T, int VB>
+struct Vec {
+    T v[VB];
+    __device__ __forceinline__ void load(const T* __restrict__ p)
+    {
+        if constexpr (VB == 4 && sizeof(T) == 4) {
+            const float4 x = *reinterpret_cast<const float4*>(p);
+            v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+        } else if constexpr (VB == 2 && sizeof(T) == 4) {
+            const float2 x = *reinterpret_cast<const float2*>(p);
+            v[0] = x.x; v[1] = x.y;
+        } else if constexpr (VB == 2 && sizeof(T) == 8) {
+            const double2 x = *reinterpret_cast<const double2*>(p);
+            v[0] = x.x; v[1] = x.y;
+        } else {
+#pragma unroll
+            for (int q = 0; q < VB; ++q) v[q] = p[q];
+        }
+    }
+    __device__ __forceinline__ void store(T* __restrict__ p) const
+    {
+        if constexpr (VB == 4 && sizeof(T) == 4) {
+            *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+        } else if constexpr (VB == 2 && sizeof(T) == 4) {
+            *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+        } else if constexpr (VB == 2 && sizeof(T) == 8) {
+            *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < VB; ++q) p[q] = v[q];
+        }
+    }
+};
+
+// y[i] += col[i] * s[q] for i < NU, col a shared-memory column padded to a
+// multiple of 4 (read as 16-byte broadcasts for float)
+template <typename T, int NU, int NUP, int VB>
+__device__ __forceinline__ void axpy_col(const T* __restrict__ col, const T (&s)[VB], T (&R)[VB][NU])
 {
-    __shared__ T m0[NF * NU];
-    const T* gm0 = static_cast<const T*>(el.m0);
-    for (int i = threadIdx.x; i < NF * NU; i += blockDim.x) m0[i] = gm0[i];
-    __syncthreads();
-    const int64_t nv = el.nv;
-    const int64_t e = blockIdx.y;
-    for (int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < nv;
-         v += int64_t(gridDim.x) * blockDim.x) {
-        T uu[NU];
 #pragma unroll
-        for (int i = 0; i < NU; ++i) uu[i] = u[(e * NU + i) * nv + v];
-#pragma unroll 4
-        for (int f = 0; f < NF; ++f) {
-            T acc = T(0);
+    for (int i4 = 0; i4 < NUP; i4 += 4) {
+        T w[4];
+        if constexpr (sizeof(T) == 4) {
+            const float4 x = *reinterpret_cast<const float4*>(col + i4);
+            w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
+        } else {
+            const double2 x0 = *reinterpret_cast<const double2*>(col + i4);
+            const double2 x1 = *reinterpret_cast<const double2*>(col + i4 + 2);
+            w[0] = x0.x; w[1] = x0.y; w[2] = x1.x; w[3] = x1.y;
+        }
 #pragma unroll
-            for (int i = 0; i < NU; ++i) acc += m0[f * NU + i] * uu[i];
-            uf[(e * NF + f) * nv + v] = acc;
+        for (int t = 0; t < 4; ++t) {
+            if (i4 + t < NU) {
+#pragma unroll
+                for (int q = 0; q < VB; ++q) R[q][i4 + t] += w[t] * s[q];
+            }
         }
     }
 }
 
-template <typename T, int ND, int NU, int NF>
-__global__ void __launch_bounds__(128) rhs_kernel(const bdgfs_fr_eles el, const bdgfs_fr_walls wl,
+// u_f = M0 u.  Each CTA (128 threads) owns one element and a chunk of
+// velocities, each thread VB consecutive velocities per step.  When every
+// row of M0 is a unit vector (flux points on solution points, as with GLL
+// points) the product is a gather: uf[f] = u[sel[f]], pure data movement;
+// otherwise the dense product with the operator read from shared memory.
+template <typename T, int NU, int NF, int VB>
+__global__ void __launch_bounds__(128) disu_kernel(const bdgfs_fr_eles el, const T* __restrict__ u,
+                                                   T* __restrict__ uf, int64_t chunk)
+{
+    __shared__ T m0[NF * NU];
+    __shared__ int sel[NF];
+    __shared__ int gather;
+    const T* gm0 = static_cast<const T*>(el.m0);                                  // [NF][NU]
+    for (int i = threadIdx.x; i < NF * NU; i += blockDim.x) m0[i] = gm0[i];
+    if (threadIdx.x == 0) gather = 1;
+    __syncthreads();
+    for (int f = threadIdx.x; f < NF; f += blockDim.x) {
+        int nz = 0, at = -1;
+        bool unit = true;
+        for (int i = 0; i < NU; ++i) {
+            const T x = m0[f * NU + i];
+            if (x != T(0)) {
+                ++nz;
+                at = i;
+                unit = unit && x == T(1);
+            }
+        }
+        sel[f] = at;
+        if (nz != 1 || !unit) atomicAnd(&gather, 0);
+    }
+    __syncthreads();
+    const int64_t nv = el.nv;
+    const int64_t e = blockIdx.y;
+    const int64_t v1 = (int64_t(blockIdx.x) + 1) * chunk < nv ? (int64_t(blockIdx.x) + 1) * chunk : nv;
+    const int64_t vs = int64_t(blockIdx.x) * chunk + int64_t(threadIdx.x) * VB;
+    if (gather) {
+        for (int64_t v0 = vs; v0 < v1; v0 += int64_t(blockDim.x) * VB) {
+#pragma unroll 6
+            for (int f = 0; f < NF; ++f) {
+                Vec<T, VB> x;
+                x.load(u + (e * NU + sel[f]) * nv + v0);
+                x.store(uf + (e * NF + f) * nv + v0);
+            }
+        }
+        return;
+    }
+    for (int64_t v0 = vs; v0 < v1; v0 += int64_t(blockDim.x) * VB) {
+#pragma unroll
+        for (int q = 0; q < VB; ++q) {
+            T uu[NU];
+#pragma unroll
+            for (int i = 0; i < NU; ++i) uu[i] = u[(e * NU + i) * nv + v0 + q];
+#pragma unroll 4
+            for (int f = 0; f < NF; ++f) {
+                T acc = T(0);
+#pragma unroll
+                for (int i = 0; i < NU; ++i) acc += m0[f * NU + i] * uu[i];
+                uf[(e * NF + f) * nv + v0 + q] = acc;
+            }
+        }
+    }
+}
+
+template <typename T, int ND, int NU, int NF, int VB>
+__global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, const bdgfs_fr_walls wl,
                                                   const T* __restrict__ u, const T* __restrict__ uf,
                                                   T* out, T a, T b, const T* x1, T c1, const T* x2,
-                                                  T c2)
+                                                  T c2, int64_t chunk)
 {
+    constexpr int NUP = (NU + 3) / 4 * 4;
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* dT = reinterpret_cast<T*>(smraw);               // [ND*NU][NU]
-    T* m3T = dT + ND * NU * NU;                         // [NF][NU]
-    T* sm = m3T + NF * NU;                              // [NU][ND][ND]
+    T* dT = reinterpret_cast<T*>(smraw);               // [ND*NU][NUP]  (M1 - M3 M2) transposed
+    T* m3T = dT + ND * NU * NUP;                        // [NF][NUP]
+    T* sm = m3T + NF * NUP;                             // [NU][ND][ND]
     T* rj = sm + NU * ND * ND;                          // [NU]
     T* pn = rj + NU;                                    // [NF][ND]
     T* mg = pn + NF * ND;                               // [NF]
     int* nb = reinterpret_cast<int*>(mg + NF);          // [NF]
     const int64_t e = blockIdx.y;
     {
-        const T* gd = static_cast<const T*>(el.dcorr);   // [NU][ND*NU]
-        for (int i = threadIdx.x; i < ND * NU * NU; i += blockDim.x) {
-            const int col = i / NU, row = i % NU;
-            dT[i] = gd[row * ND * NU + col];
+        for (int i = threadIdx.x; i < (ND * NU + NF) * NUP; i += blockDim.x) dT[i] = T(0);
+        __syncthreads();
+        const T* gd = static_cast<const T*>(el.dcorr);   // [NU][ND*NU], read coalesced
+        for (int i = threadIdx.x; i < NU * ND * NU; i += blockDim.x) {
+            const int row = i / (ND * NU), col = i - row * (ND * NU);
+            dT[col * NUP + row] = gd[i];
         }
         const T* gm3 = static_cast<const T*>(el.m3);     // [NU][NF]
-        for (int i = threadIdx.x; i < NF * NU; i += blockDim.x) {
-            const int f = i / NU, row = i % NU;
-            m3T[i] = gm3[row * NF + f];
+        for (int i = threadIdx.x; i < NU * NF; i += blockDim.x) {
+            const int row = i / NF, f = i - row * NF;
+            m3T[f * NUP + row] = gm3[i];
         }
         const T* gs = static_cast<const T*>(el.smats) + e * NU * ND * ND;
         for (int i = threadIdx.x; i < NU * ND * ND; i += blockDim.x) sm[i] = gs[i];
@@ -114,62 +217,109 @@ __global__ void __launch_bounds__(128) rhs_kernel(const bdgfs_fr_eles el, const 
     const T* uw = static_cast<const T*>(wl.uwall);
     const T* fw = static_cast<const T*>(wl.fw);
     const T* bcv = static_cast<const T*>(wl.bcv);
-    for (int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < nv;
-         v += int64_t(gridDim.x) * blockDim.x) {
-        T c[3];
-        vel(c0, el.Nv, v, c);
-        T uu[NU], R[NU];
+    const int64_t v1 = (int64_t(blockIdx.x) + 1) * chunk < nv ? (int64_t(blockIdx.x) + 1) * chunk : nv;
+    for (int64_t v0 = int64_t(blockIdx.x) * chunk + int64_t(threadIdx.x) * VB; v0 < v1;
+         v0 += int64_t(blockDim.x) * VB) {
+        T c[VB][3];
 #pragma unroll
-        for (int i = 0; i < NU; ++i) {
-            uu[i] = u[(e * NU + i) * nv + v];
-            R[i] = T(0);
-        }
+        for (int q = 0; q < VB; ++q) vel(c0, el.Nv, v0 + q, c[q]);
+        T R[VB][NU];
+#pragma unroll
+        for (int q = 0; q < VB; ++q)
+#pragma unroll
+            for (int i = 0; i < NU; ++i) R[q][i] = T(0);
         // volume: R += (M1 - M3 M2) F~,  F~[d][j] = (sum_k smats[j][d][k] c_k) u_j
+        Vec<T, VB> uj;
+        uj.load(u + (e * NU) * nv + v0);
 #pragma unroll 1
         for (int j = 0; j < NU; ++j) {
+            Vec<T, VB> un;                                  // prefetch u_{j+1}
+            if (j + 1 < NU) un.load(u + (e * NU + j + 1) * nv + v0);
 #pragma unroll
             for (int d = 0; d < ND; ++d) {
-                T al = T(0);
+                T ft[VB];
 #pragma unroll
-                for (int k = 0; k < ND; ++k) al += sm[(j * ND + d) * ND + k] * c[k];
-                const T ft = al * uu[j];
-                const T* col = dT + (d * NU + j) * NU;
+                for (int q = 0; q < VB; ++q) {
+                    T al = T(0);
 #pragma unroll
-                for (int i = 0; i < NU; ++i) R[i] += col[i] * ft;
+                    for (int k = 0; k < ND; ++k) al += sm[(j * ND + d) * ND + k] * c[q][k];
+                    ft[q] = al * uj.v[q];
+                }
+                axpy_col<T, NU, NUP, VB>(dT + (d * NU + j) * NUP, ft, R);
             }
+            uj = un;
         }
         // surface: common normal flux at each face point, lifted by M3
+        // face values: ul and the neighbour's (or the wall Maxwellian's) row,
+        // prefetched one face ahead
+        auto rsrc = [&](int f) -> const T* {
+            const int n = nb[f];
+            return n >= 0 ? uf + int64_t(n) * nv + v0 : fw + int64_t(wl.bcid[-1 - n]) * nv + v0;
+        };
+        Vec<T, VB> ulp, urp;
+        ulp.load(uf + (e * NF) * nv + v0);
+        urp.load(rsrc(0));
 #pragma unroll 1
         for (int f = 0; f < NF; ++f) {
-            const T ul = uf[(e * NF + f) * nv + v];
-            T nc = T(0);
-#pragma unroll
-            for (int d = 0; d < ND; ++d) nc += pn[f * ND + d] * c[d];
+            Vec<T, VB> ul = ulp, ur = urp;
+            if (f + 1 < NF) {
+                ulp.load(uf + (e * NF + f + 1) * nv + v0);
+                urp.load(rsrc(f + 1));
+            }
             const int n = nb[f];
-            T ur;
-            if (n >= 0) {
-                ur = uf[int64_t(n) * nv + v];
-            } else {
+            T nc[VB];
+#pragma unroll
+            for (int q = 0; q < VB; ++q) {
+                nc[q] = T(0);
+#pragma unroll
+                for (int d = 0; d < ND; ++d) nc[q] += pn[f * ND + d] * c[q][d];
+            }
+            if (n < 0) {                                     // diffuse wall: ur holds f_w
                 const int w = -1 - n;
                 const int bid = wl.bcid[w];
-                T fac = T(0);
+                const T sc = -bcv[2 * w] / bcv[2 * w + 1];
 #pragma unroll
-                for (int d = 0; d < ND; ++d) fac += (c[d] - uw[bid * 3 + d]) * pn[f * ND + d];
-                ur = (fac < T(0)) ? fw[int64_t(bid) * nv + v] * (-bcv[2 * w] / bcv[2 * w + 1]) : ul;
+                for (int q = 0; q < VB; ++q) {
+                    T fac = T(0);
+#pragma unroll
+                    for (int d = 0; d < ND; ++d) fac += (c[q][d] - uw[bid * 3 + d]) * pn[f * ND + d];
+                    ur.v[q] = (fac < T(0)) ? ur.v[q] * sc : ul.v[q];
+                }
             }
-            const T fn = T(0.5) * nc * (ul + ur) + T(0.5) * fabs(nc) * (ul - ur);
-            const T fh = mg[f] * fn;
-            const T* col = m3T + f * NU;
+            T fh[VB];
 #pragma unroll
-            for (int i = 0; i < NU; ++i) R[i] += col[i] * fh;
+            for (int q = 0; q < VB; ++q) {
+                const T fn = T(0.5) * nc[q] * (ul.v[q] + ur.v[q]) + T(0.5) * fabs(nc[q]) * (ul.v[q] - ur.v[q]);
+                fh[q] = mg[f] * fn;
+            }
+            axpy_col<T, NU, NUP, VB>(m3T + f * NUP, fh, R);
         }
+        // combination rows u, x1, x2, loaded one row ahead
+        Vec<T, VB> u0n, y1n, y2n;
+        u0n.load(u + (e * NU) * nv + v0);
+        if (x1) y1n.load(x1 + (e * NU) * nv + v0);
+        if (x2) y2n.load(x2 + (e * NU) * nv + v0);
 #pragma unroll
         for (int i = 0; i < NU; ++i) {
-            const int64_t idx = (e * NU + i) * nv + v;
-            T r = a * uu[i] + b * (-rj[i] * R[i]);
-            if (x1) r += c1 * x1[idx];
-            if (x2) r += c2 * x2[idx];
-            out[idx] = r;
+            const int64_t idx = (e * NU + i) * nv + v0;
+            const Vec<T, VB> ui = u0n, y1 = y1n, y2 = y2n;
+            if (i + 1 < NU) {
+                u0n.load(u + idx + nv);
+                if (x1) y1n.load(x1 + idx + nv);
+                if (x2) y2n.load(x2 + idx + nv);
+            }
+            Vec<T, VB> o;
+#pragma unroll
+            for (int q = 0; q < VB; ++q) o.v[q] = a * ui.v[q] + b * (-rj[i] * R[q][i]);
+            if (x1) {
+#pragma unroll
+                for (int q = 0; q < VB; ++q) o.v[q] += c1 * y1.v[q];
+            }
+            if (x2) {
+#pragma unroll
+                for (int q = 0; q < VB; ++q) o.v[q] += c2 * y2.v[q];
+            }
+            o.store(out + idx);
         }
     }
 }
@@ -190,7 +340,25 @@ __global__ void __launch_bounds__(256) bc_update_kernel(const bdgfs_fr_eles el,
     const T* ul = uf + (int64_t(e) * el.nfpts + f) * el.nv;
     const T* c0 = static_cast<const T*>(el.c0);
     double s0 = 0.0, s1 = 0.0;
-    for (int64_t v = threadIdx.x; v < el.nv; v += blockDim.x) {
+    // four velocities per step (16-byte loads) when rows are aligned
+    const bool v4 = sizeof(T) == 4 && el.nv % 4 == 0 && (reinterpret_cast<uintptr_t>(ul) & 15u) == 0 &&
+                    (reinterpret_cast<uintptr_t>(fw) & 15u) == 0;
+    const int64_t nv4 = v4 ? el.nv : 0;
+    for (int64_t v0 = int64_t(threadIdx.x) * 4; v0 < nv4; v0 += int64_t(blockDim.x) * 4) {
+        Vec<T, 4> a, b;
+        a.load(ul + v0);
+        b.load(fw + v0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            T c[3];
+            vel(c0, el.Nv, v0 + q, c);
+            T fac = T(0);
+            for (int d = 0; d < ND; ++d) fac += (c[d] - uw[d]) * pn[d];
+            if (fac >= T(0)) s0 += double(fac * a.v[q]);
+            else s1 += double(fac * b.v[q]);
+        }
+    }
+    for (int64_t v = nv4 + threadIdx.x; v < el.nv; v += blockDim.x) {
         T c[3];
         vel(c0, el.Nv, v, c);
         T fac = T(0);
@@ -296,13 +464,58 @@ __global__ void __launch_bounds__(256) status_kernel(const T* __restrict__ a, in
     if (bad && (threadIdx.x & 31) == 0) atomicOr(status, bad);
 }
 
-static int grid_v(int64_t nv, int neles, dim3* g)
+// Velocity chunk per CTA (a multiple of 128*VB).
+static int64_t fr_chunk(int64_t nv, int neles, int VB)
 {
-    int64_t bx = (nv + 127) / 128;
-    if (bx > 65535) bx = 65535;
-    if (neles > 65535 || neles < 1) return BDGFS_EINVAL;
+    // one 128*VB velocity step per CTA: staging the operators costs ~40
+    // instructions per thread against ~20k of work, and short CTAs balance
+    // the waves; longer chunks only when the grid's x extent would overflow
+    const int64_t step = 128 * int64_t(VB);
+    int64_t chunk = step;
+    while ((nv + chunk - 1) / chunk > 65535) chunk *= 2;
+    (void)neles;
+    return chunk;
+}
+
+static int grid_v(int64_t nv, int neles, int64_t chunk, dim3* g)
+{
+    const int64_t bx = (nv + chunk - 1) / chunk;
+    if (bx > 65535 || neles > 65535 || neles < 1) return BDGFS_EINVAL;
     *g = dim3(unsigned(bx), unsigned(neles));
     return BDGFS_OK;
+}
+
+// VB velocities per thread when every row is VB-aligned
+template <typename T>
+static int vec_width(int64_t nv, const void* const* ptrs, int n)
+{
+    const int VB = sizeof(T) == 4 ? 4 : 2;
+    if (nv % VB) return 1;
+    for (int i = 0; i < n; ++i)
+        if (ptrs[i] && (reinterpret_cast<uintptr_t>(ptrs[i]) % (VB * sizeof(T)))) return 1;
+    return VB;
+}
+
+template <typename T, int ND, int NU, int NF, int VB>
+static int rhs_launch_vb(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl, const void* u,
+                         const void* uf, void* out, double a, double b, const void* x1, double c1,
+                         const void* x2, double c2, cudaStream_t st)
+{
+    constexpr int NUP = (NU + 3) / 4 * 4;
+    const int64_t chunk = fr_chunk(el->nv, el->neles, VB);
+    dim3 g;
+    if (grid_v(el->nv, el->neles, chunk, &g) != BDGFS_OK) return BDGFS_EINVAL;
+    const size_t smem = sizeof(T) * ((ND * NU + NF) * NUP + NU * ND * ND + NU + NF * ND + NF)
+                        + sizeof(int) * NF + 16;
+    auto k = rhs_kernel<T, ND, NU, NF, VB>;
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+        return BDGFS_ECUDA;
+    bdgfs_fr_walls w0{};
+    k<<<g, 128, smem, st>>>(*el, wl ? *wl : w0, static_cast<const T*>(u), static_cast<const T*>(uf),
+                            static_cast<T*>(out), T(a), T(b), static_cast<const T*>(x1), T(c1),
+                            static_cast<const T*>(x2), T(c2), chunk);
+    return cuda_status(cudaGetLastError());
 }
 
 template <typename T, int ND, int NU, int NF>
@@ -310,28 +523,33 @@ static int rhs_launch(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl, const v
                       const void* uf, void* out, double a, double b, const void* x1, double c1,
                       const void* x2, double c2, cudaStream_t st)
 {
+    const void* ptrs[] = {u, uf, out, x1, x2, wl ? wl->fw : nullptr};
+    // 4 velocities per thread for float (each operator column read from
+    // shared memory feeds 4 x 4 FMAs; measured faster than 2 also for NU = 27)
+    constexpr int VBW = sizeof(T) == 4 ? 4 : 2;
+    if (vec_width<T>(el->nv, ptrs, 6) >= VBW)
+        return rhs_launch_vb<T, ND, NU, NF, VBW>(el, wl, u, uf, out, a, b, x1, c1, x2, c2, st);
+    return rhs_launch_vb<T, ND, NU, NF, 1>(el, wl, u, uf, out, a, b, x1, c1, x2, c2, st);
+}
+
+template <typename T, int NU, int NF, int VB>
+static int disu_launch_vb(const bdgfs_fr_eles* el, const void* u, void* uf, cudaStream_t st)
+{
+    const int64_t chunk = fr_chunk(el->nv, el->neles, VB);
     dim3 g;
-    if (grid_v(el->nv, el->neles, &g) != BDGFS_OK) return BDGFS_EINVAL;
-    const size_t smem = sizeof(T) * (ND * NU * NU + NF * NU + NU * ND * ND + NU + NF * ND + NF)
-                        + sizeof(int) * NF + 16;
-    auto k = rhs_kernel<T, ND, NU, NF>;
-    if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
-        return BDGFS_ECUDA;
-    bdgfs_fr_walls w0{};
-    k<<<g, 128, smem, st>>>(*el, wl ? *wl : w0, static_cast<const T*>(u),
-                            static_cast<const T*>(uf), static_cast<T*>(out), T(a), T(b),
-                            static_cast<const T*>(x1), T(c1), static_cast<const T*>(x2), T(c2));
+    if (grid_v(el->nv, el->neles, chunk, &g) != BDGFS_OK) return BDGFS_EINVAL;
+    disu_kernel<T, NU, NF, VB><<<g, 128, 0, st>>>(*el, static_cast<const T*>(u), static_cast<T*>(uf),
+                                                  chunk);
     return cuda_status(cudaGetLastError());
 }
 
 template <typename T, int NU, int NF>
 static int disu_launch(const bdgfs_fr_eles* el, const void* u, void* uf, cudaStream_t st)
 {
-    dim3 g;
-    if (grid_v(el->nv, el->neles, &g) != BDGFS_OK) return BDGFS_EINVAL;
-    disu_kernel<T, NU, NF><<<g, 128, 0, st>>>(*el, static_cast<const T*>(u), static_cast<T*>(uf));
-    return cuda_status(cudaGetLastError());
+    const void* ptrs[] = {u, uf};
+    constexpr int VBW = sizeof(T) == 4 ? 4 : 2;
+    if (vec_width<T>(el->nv, ptrs, 2) == VBW) return disu_launch_vb<T, NU, NF, VBW>(el, u, uf, st);
+    return disu_launch_vb<T, NU, NF, 1>(el, u, uf, st);
 }
 
 #define BDGFS_FR_SHAPES(X)                                                          \
@@ -347,7 +565,7 @@ static bool shape_ok(const bdgfs_fr_eles* el)
 
 static int check_eles(const bdgfs_fr_eles* el)
 {
-    if (!el || el->nv < 1 || el->neles < 1 || el->Nv < 1 ||
+    if (!el || el->nv < 1 || el->neles < 1 || el->Nv < 1 || el->Nv > 1024 ||
         int64_t(el->Nv) * el->Nv * el->Nv != el->nv)
         return BDGFS_EINVAL;
     if (!el->m0 || !el->dcorr || !el->m3 || !el->smats || !el->rcpdjac || !el->pnorm ||
