@@ -51,7 +51,8 @@ class FrEles(C.Structure):
                 ('fp64', C.c_int32),
                 ('m0', C.c_void_p), ('dcorr', C.c_void_p), ('m3', C.c_void_p),
                 ('smats', C.c_void_p), ('rcpdjac', C.c_void_p), ('pnorm', C.c_void_p),
-                ('magn', C.c_void_p), ('nbr', C.c_void_p), ('c0', C.c_void_p)]
+                ('magn', C.c_void_p), ('nbr', C.c_void_p), ('c0', C.c_void_p),
+                ('engine', C.c_int32), ('pad_', C.c_int32)]
 
 
 class FrWall(C.Structure):

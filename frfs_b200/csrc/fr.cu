@@ -23,6 +23,7 @@
 // its own outward normal), which equals the reference's lhs-computed value
 // with the sign flip of intcflux.mako:21-23.
 #include "common.cuh"
+#include "fr_tc.cuh"
 
 namespace bdgfs {
 
@@ -620,6 +621,11 @@ extern "C" int32_t bdgfs_fr_rhs(const bdgfs_fr_eles* el, const bdgfs_fr_walls* w
     if (wl && wl->nwall > 0 && (!wl->bcid || !wl->uwall || !wl->fw || !wl->bcv))
         return BDGFS_EINVAL;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!el->fp64 && el->engine == 1) {          // tensor-core engine when the shape has one
+        const bdgfs_fr_walls w0{};
+        const int tc = fr_rhs_tc(*el, wl ? *wl : w0, u, uf, out, a, b, x1, c1, x2, c2, st);
+        if (tc != BDGFS_EUNSUPPORTED) return tc;
+    }
 #define GO(D, U, F)                                                                          \
     if (el->ndims == D && el->nupts == U && el->nfpts == F)                                  \
         return el->fp64 ? rhs_launch<double, D, U, F>(el, wl, u, uf, out, a, b, x1, c1, x2, c2, st) \

@@ -135,6 +135,11 @@ typedef struct bdgfs_fr_eles {
     const int32_t* nbr;  /* [neles][nfpts]: e'*nfpts+f' of the neighbour
                             face point, or -1 - (wall face-point index)     */
     const void* c0;      /* real [Nv] cell-centre velocities               */
+    int32_t engine;      /* bdgfs_fr_rhs: 0 = CUDA cores (default);
+                            1 = tensor cores (tcgen05 kind::tf32, 3xTF32
+                            products keep FP32 accuracy; FP32 state and the
+                            tabulated shapes only, else CUDA cores)        */
+    int32_t pad_;
 } bdgfs_fr_eles;
 
 /* Diffuse-wall face points. */

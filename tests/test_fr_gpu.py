@@ -162,3 +162,27 @@ def test_partitioned_virtual_ranks_equal_single_domain(cuda):
         idx = torch.as_tensor(parts[r], device=be.device)
         assert torch.equal(sy.eles_scal_upts_inb_full[0],
                            s.eles_scal_upts_inb_full[0].index_select(0, idx)), r
+
+
+@pytest.mark.parametrize('kind,order', [('quad', 3), ('hex', 2), ('quad', 2)])
+def test_tensor_core_rhs_matches_cuda_core_rhs(cuda, kind, order):
+    """The tcgen05 (3xTF32) FR residual against the CUDA-core kernel on the
+    same FP32 state: agreement to FP32 rounding, with walls and with the
+    RK combination operands."""
+    cfg, be, mesh, s = _system(kind, order, 'single', shape=(3, 2) if kind == 'quad' else (2, 2, 2))
+    _perturb(s, 7)
+    x1 = s.eles_scal_upts_inb_full[0] * 1.5
+    x2 = s.eles_scal_upts_inb_full[0] * 0.5
+    s.updatebc(0.0, 0, 1)
+    outs = []
+    for eng in (1, 0):                  # tensor cores, CUDA cores
+        s.ele.struct.engine = eng
+        o = torch.empty_like(x1)
+        s._active = (0, 1)
+        s._fused_rhs(a=0.5, b=2.0, x1=x1, c1=0.25, x2=x2, c2=-0.5, out=o)
+        outs.append(o)
+    s.ele.struct.engine = 0
+    torch.cuda.synchronize()
+    # 3xTF32 keeps ~22 significant bits per product; the residual is a sum with
+    # cancellation: within the FP32 tolerance of the FR parity tests
+    assert rel_l2(outs[0].double().cpu().numpy(), outs[1].double().cpu().numpy()) < 2e-5
