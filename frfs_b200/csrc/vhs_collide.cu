@@ -49,7 +49,76 @@ __device__ __forceinline__ cpx<T> cmul(cpx<T> a, cpx<T> b)
 template <typename T>
 __device__ __forceinline__ cpx<T> conjc(cpx<T> a) { return {a.x, -a.y}; }
 
-template <typename T, int N, int NT, bool WG, bool SG>
+// z-pencil (kx, ky) of the spectrum m_pq * Fh (tr = 0), or of the Nyquist
+// correction term i * m_s * Fh (tr = 1).  Fh holds kx <= N/2 at innermost
+// stride FS; kx > N/2 follows from Hermitian symmetry.  ep: the direction's
+// phase factors [Ex | Ey | Ez]; ab[kz] = (Ez.x + Ez.y, Ez.x - Ez.y).
+template <typename T, int N, int FS>
+__device__ __forceinline__ void pencil_spectrum(int kx, int ky, int tr, const cpx<T>* ep,
+                                                const cpx<T>* ab, const cpx<T>* Fh,
+                                                cpx<T> (&v)[N])
+{
+    constexpr int NH = N / 2 + 1;
+    const cpx<T> Ex = ep[kx], Ey = ep[N + ky];
+    const cpx<T> Pxy = cmul(Ex, Ey);
+    const bool direct = kx < NH;
+    const int pkx = direct ? kx : N - kx;
+    const int pky = direct ? ky : (N - ky) % N;
+    const cpx<T>* fp = Fh + (pkx * N + pky) * FS;
+    const bool nyq = (kx == N / 2) || (ky == N / 2);
+    if (tr == 1) {
+        // second-order Nyquist term: spectrum i * m_s * Fh with
+        // m_s = [sin a + sin abar - cos a + cos abar] / 2
+        const cpx<T> Ebx = (kx == N / 2) ? Ex : conjc(Ex);
+        const cpx<T> Eby = (ky == N / 2) ? Ey : conjc(Ey);
+        const cpx<T> Pb = cmul(Ebx, Eby);
+#pragma unroll
+        for (int kz = 0; kz < N; ++kz) {
+            cpx<T> F = direct ? fp[kz] : conjc(fp[(N - kz) % N]);
+            const cpx<T> Ez = ep[2 * N + kz];
+            const cpx<T> Ebz = (kz == N / 2) ? Ez : conjc(Ez);
+            const cpx<T> E = cmul(Pxy, Ez);
+            const cpx<T> Eb = cmul(Pb, Ebz);
+            const T ms = T(0.5) * (E.y + Eb.y - E.x + Eb.x);
+            v[kz] = {-ms * F.y, ms * F.x};
+        }
+    } else if (!nyq) {
+        // off the Nyquist planes m = Re(E) + Im(E), E = Pxy * Ez,
+        // = Pxy.x (Ez.x + Ez.y) + Pxy.y (Ez.x - Ez.y)
+        const cpx<T> Pb = conjc(Pxy);
+#pragma unroll
+        for (int kz = 0; kz < N; ++kz) {
+            cpx<T> F = direct ? fp[kz] : conjc(fp[(N - kz) % N]);
+            T m;
+            if (kz == N / 2) {
+                const cpx<T> Ez = ep[2 * N + kz];
+                const cpx<T> E = cmul(Pxy, Ez);
+                const cpx<T> Eb = cmul(Pb, Ez);
+                m = T(0.5) * (E.x + E.y + Eb.x - Eb.y);
+            } else {
+                const cpx<T> w = ab[kz];
+                m = Pxy.x * w.x + Pxy.y * w.y;
+            }
+            v[kz] = {m * F.x, m * F.y};
+        }
+    } else {
+        const cpx<T> Ebx = (kx == N / 2) ? Ex : conjc(Ex);
+        const cpx<T> Eby = (ky == N / 2) ? Ey : conjc(Ey);
+        const cpx<T> Pb = cmul(Ebx, Eby);
+#pragma unroll
+        for (int kz = 0; kz < N; ++kz) {
+            cpx<T> F = direct ? fp[kz] : conjc(fp[(N - kz) % N]);
+            const cpx<T> Ez = ep[2 * N + kz];
+            const cpx<T> Ebz = (kz == N / 2) ? Ez : conjc(Ez);
+            const cpx<T> E = cmul(Pxy, Ez);
+            const cpx<T> Eb = cmul(Pb, Ebz);
+            const T m = T(0.5) * (E.x + E.y + Eb.x - Eb.y);
+            v[kz] = {m * F.x, m * F.y};
+        }
+    }
+}
+
+template <typename T, int N, int NT, bool WG, bool SG, bool SL = false>
 struct QLayout {
     static constexpr int NH = N / 2 + 1;
     static constexpr int n = N * N * N;
@@ -57,7 +126,9 @@ struct QLayout {
     static constexpr int FS = N + 1;            // innermost stride of Fh
     static constexpr size_t w_elems = size_t(N) * N * WS;
     static constexpr size_t fh_elems = size_t(NH) * N * FS;
-    // shared memory: [W (if smem)] [Fh] [phase M*3*N] [reduction]
+    static constexpr size_t slab_elems = SL ? size_t(NT / 32) * N * (N + 1) : 0;
+    // shared memory: [W (if smem)] [Fh] [phase M*3*N] [phab M*N] [warp slabs]
+    // [reduction]
     static size_t smem_bytes(int M)
     {
         size_t b = 0;
@@ -65,6 +136,7 @@ struct QLayout {
         b += fh_elems * sizeof(cpx<T>);
         b += size_t(M) * 3 * N * sizeof(cpx<T>);
         b += size_t(M) * N * sizeof(cpx<T>);      // (Ez.x + Ez.y, Ez.x - Ez.y) per direction
+        b += slab_elems * sizeof(cpx<T>);
         b += 10 * (NT / 32) * sizeof(double) + 16;
         return b;
     }
@@ -81,14 +153,20 @@ struct QLayout {
 // GR > 0: the z- and y-passes of each inverse transform are done by GR
 // groups of NT/GR threads, group g owning the kx-slabs [g*N/GR, (g+1)*N/GR);
 // the two passes then only synchronise within the group (named barrier).
-template <typename T, int N, int NT, bool WG, bool SG, int GR = 0>
+// SL (W in global scratch, N = 32): warp w owns the kx-slabs w, w + NT/32, ...
+// of each inverse transform and does their z- and y-passes in a private
+// shared-memory slab (lane = pencil, no CTA barrier); only the finished slab
+// goes to the global W, which the x-pass then reads.  Per transform the
+// global traffic is one write and one read of W instead of two of each.
+template <typename T, int N, int NT, bool WG, bool SG, int GR = 0, bool SL = false>
 __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
                             T* __restrict__ Qout, double* mom, int flags,
                             unsigned char* smem, unsigned char* scratch)
 {
     const int project = flags & BDGFS_PROJECT;
     const int ntr = (flags & BDGFS_EXACT) ? 2 : 1;
-    using L = QLayout<T, N, NT, WG, SG>;
+    using L = QLayout<T, N, NT, WG, SG, SL>;
+    static_assert(!SL || (WG && N == 32 && GR == 0), "warp slabs: W in global scratch, N = 32");
     constexpr int NH = L::NH;
     constexpr int WS = L::WS;
     constexpr int FS = L::FS;
@@ -112,6 +190,9 @@ __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
     sp += size_t(M) * 3 * N * sizeof(cpx<T>);
     cpx<T>* phab = reinterpret_cast<cpx<T>*>(sp);       // [q][kz]: (Ez.x + Ez.y, Ez.x - Ez.y)
     sp += size_t(M) * N * sizeof(cpx<T>);
+    cpx<T>* slab = reinterpret_cast<cpx<T>*>(sp);       // [warp][ky][z], stride N+1
+    sp += L::slab_elems * sizeof(cpx<T>);
+    (void)slab;
     double* red = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(sp) + 15) & ~uintptr_t(15));
 
     cpx<T>* Gh = reinterpret_cast<cpx<T>*>(scratch);   // [kz][kx<NH][ky]
@@ -209,86 +290,50 @@ __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
         for (int qt = 0; qt < M * ntr; ++qt) {
             const int q = qt / ntr, tr = qt % ntr;   // tr = 1: Nyquist term
             const cpx<T>* ep = ph + q * 3 * N;
-            // ---- pass 1: spectrum * m_pq, inverse along z ----
+            if constexpr (SL) {
+                // ---- passes 1 and 2 per kx-slab in the warp's shared slab ----
+                const int lane = tid & 31;
+                cpx<T>* sl = slab + (tid >> 5) * N * (N + 1);
 #pragma unroll 1
-            for (int r = 0; r < P12; ++r) {
-                int kx, ky;
-                if (!pencil12(r, kx, ky)) break;
-                const cpx<T> Ex = ep[kx], Ey = ep[N + ky];
-                const cpx<T> Pxy = cmul(Ex, Ey);
-                const bool direct = kx < NH;
-                const int pkx = direct ? kx : N - kx;
-                const int pky = direct ? ky : (N - ky) % N;
-                const cpx<T>* fp = Fh + (pkx * N + pky) * FS;
-                cpx<T> v[N];
-                const bool nyq = (kx == N / 2) || (ky == N / 2);
-                if (tr == 1) {
-                    // second-order Nyquist term: spectrum i * m_s * Fh with
-                    // m_s = [sin a + sin abar - cos a + cos abar] / 2
-                    const cpx<T> Ebx = (kx == N / 2) ? Ex : conjc(Ex);
-                    const cpx<T> Eby = (ky == N / 2) ? Ey : conjc(Ey);
-                    const cpx<T> Pb = cmul(Ebx, Eby);
+                for (int kx = tid >> 5; kx < N; kx += NT / 32) {
+                    cpx<T> v[N];
+                    pencil_spectrum<T, N, FS>(kx, lane, tr, ep, phab + q * N, Fh, v);
+                    dft<N, +1>(v);
 #pragma unroll
-                    for (int kz = 0; kz < N; ++kz) {
-                        cpx<T> F = direct ? fp[kz] : conjc(fp[(N - kz) % N]);
-                        const cpx<T> Ez = ep[2 * N + kz];
-                        const cpx<T> Ebz = (kz == N / 2) ? Ez : conjc(Ez);
-                        const cpx<T> E = cmul(Pxy, Ez);
-                        const cpx<T> Eb = cmul(Pb, Ebz);
-                        const T ms = T(0.5) * (E.y + Eb.y - E.x + Eb.x);
-                        v[kz] = {-ms * F.y, ms * F.x};
-                    }
-                } else if (!nyq) {
-                    // off the Nyquist planes m = Re(E) + Im(E), E = Pxy * Ez,
-                    // = Pxy.x (Ez.x + Ez.y) + Pxy.y (Ez.x - Ez.y)
-                    const cpx<T> Pb = conjc(Pxy);
-                    const cpx<T>* ab = phab + (qt / ntr) * N;
+                    for (int z = 0; z < N; ++z) sl[lane * (N + 1) + z] = v[z];
+                    __syncwarp();
 #pragma unroll
-                    for (int kz = 0; kz < N; ++kz) {
-                        cpx<T> F = direct ? fp[kz] : conjc(fp[(N - kz) % N]);
-                        T m;
-                        if (kz == N / 2) {
-                            const cpx<T> Ez = ep[2 * N + kz];
-                            const cpx<T> E = cmul(Pxy, Ez);
-                            const cpx<T> Eb = cmul(Pb, Ez);
-                            m = T(0.5) * (E.x + E.y + Eb.x - Eb.y);
-                        } else {
-                            const cpx<T> w = ab[kz];
-                            m = Pxy.x * w.x + Pxy.y * w.y;
-                        }
-                        v[kz] = {m * F.x, m * F.y};
-                    }
-                } else {
-                    const cpx<T> Ebx = (kx == N / 2) ? Ex : conjc(Ex);
-                    const cpx<T> Eby = (ky == N / 2) ? Ey : conjc(Ey);
-                    const cpx<T> Pb = cmul(Ebx, Eby);
+                    for (int j = 0; j < N; ++j) v[j] = sl[j * (N + 1) + lane];
+                    dft<N, +1>(v);
 #pragma unroll
-                    for (int kz = 0; kz < N; ++kz) {
-                        cpx<T> F = direct ? fp[kz] : conjc(fp[(N - kz) % N]);
-                        const cpx<T> Ez = ep[2 * N + kz];
-                        const cpx<T> Ebz = (kz == N / 2) ? Ez : conjc(Ez);
-                        const cpx<T> E = cmul(Pxy, Ez);
-                        const cpx<T> Eb = cmul(Pb, Ebz);
-                        const T m = T(0.5) * (E.x + E.y + Eb.x - Eb.y);
-                        v[kz] = {m * F.x, m * F.y};
-                    }
+                    for (int j = 0; j < N; ++j) W[widx(kx, j, lane)] = v[j];
+                    __syncwarp();
                 }
-                dft<N, +1>(v);
-#pragma unroll
-                for (int z = 0; z < N; ++z) W[widx(kx, ky, z)] = v[z];
-            }
-            sync12();
-            // ---- pass 2: inverse along y ----
+            } else {
+                // ---- pass 1: spectrum * m_pq, inverse along z ----
 #pragma unroll 1
-            for (int r = 0; r < P12; ++r) {
-                int kx, z;
-                if (!pencil12(r, kx, z)) break;
-                cpx<T> v[N];
+                for (int r = 0; r < P12; ++r) {
+                    int kx, ky;
+                    if (!pencil12(r, kx, ky)) break;
+                    cpx<T> v[N];
+                    pencil_spectrum<T, N, FS>(kx, ky, tr, ep, phab + q * N, Fh, v);
+                    dft<N, +1>(v);
 #pragma unroll
-                for (int j = 0; j < N; ++j) v[j] = W[widx(kx, j, z)];
-                dft<N, +1>(v);
+                    for (int z = 0; z < N; ++z) W[widx(kx, ky, z)] = v[z];
+                }
+                sync12();
+                // ---- pass 2: inverse along y ----
+#pragma unroll 1
+                for (int r = 0; r < P12; ++r) {
+                    int kx, z;
+                    if (!pencil12(r, kx, z)) break;
+                    cpx<T> v[N];
 #pragma unroll
-                for (int j = 0; j < N; ++j) W[widx(kx, j, z)] = v[j];
+                    for (int j = 0; j < N; ++j) v[j] = W[widx(kx, j, z)];
+                    dft<N, +1>(v);
+#pragma unroll
+                    for (int j = 0; j < N; ++j) W[widx(kx, j, z)] = v[j];
+                }
             }
             __syncthreads();
             // ---- pass 3: inverse along x, S_p += Re(w^2) ----
@@ -501,11 +546,11 @@ struct KArgs {
     unsigned long long* counter;
 };
 
-template <typename T, int N, int NT, bool WG, bool SG, int GR = 0>
+template <typename T, int N, int NT, bool WG, bool SG, int GR = 0, bool SL = false>
 struct Variant {
-    using L = QLayout<T, N, NT, WG, SG>;
+    using L = QLayout<T, N, NT, WG, SG, SL>;
     static constexpr int n = N;
-    static constexpr bool wg = WG, sg = SG;
+    static constexpr bool wg = WG, sg = SG, sl = SL;
     static constexpr int gr = GR;
 };
 
@@ -550,11 +595,11 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
         T* Q = static_cast<T*>(bt.Q) + dof * n3;
         double* mom = bt.moments ? bt.moments + dof * 10 : nullptr;
         if (g.Nv == V0::n) {
-            collide_one<T, V0::n, NT, V0::wg, V0::sg, V0::gr>(
+            collide_one<T, V0::n, NT, V0::wg, V0::sg, V0::gr, V0::sl>(
                 g, f, Q, mom, a.flags, smem, scratch);
         } else if constexpr (V1::n > 0) {
             if (g.Nv == V1::n)
-                collide_one<T, V1::n, NT, V1::wg, V1::sg, V1::gr>(
+                collide_one<T, V1::n, NT, V1::wg, V1::sg, V1::gr, V1::sl>(
                     g, f, Q, mom, a.flags, smem, scratch);
         }
     }
@@ -562,7 +607,7 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
 
 struct NoVariant {
     static constexpr int n = 0;
-    static constexpr bool wg = false, sg = false;
+    static constexpr bool wg = false, sg = false, sl = false;
     static constexpr int gr = 0;
     struct L {
         static constexpr int WS = 0;
@@ -597,6 +642,7 @@ struct Entry {
 
 #define VARIANT(T, N, NT, WG, SG) Variant<T, N, NT, WG, SG>
 #define VARIANTG(T, N, NT, GR) Variant<T, N, NT, false, false, GR>
+#define VARIANTS(T, NT) Variant<T, 32, NT, true, false, 0, true>
 #define ENTRYG(FP, T, NT, N0, GR)                                                            \
     {FP, N0, 0, NT, &launch<T, NT, VARIANTG(T, N0, NT, GR), NoVariant>,                     \
      &entry_per_cta<T, NT, VARIANTG(T, N0, NT, GR), NoVariant>}
@@ -633,6 +679,12 @@ static const Entry kEntries[] = {
     ENTRY1(1, double, 64, 8, false, false),
     // appended variants (earlier tile indices stay valid)
     ENTRY1(0, float, 384, 24, false, false),
+    // 32^3 with warp slabs in shared memory, S_p in registers
+    {0, 32, 0, 256, &launch<float, 256, VARIANTS(float, 256), NoVariant>,
+     &entry_per_cta<float, 256, VARIANTS(float, 256), NoVariant>},
+    {0, 24, 32, 256,
+     &launch<float, 256, VARIANT(float, 24, 256, false, false), VARIANTS(float, 256)>,
+     &entry_per_cta<float, 256, VARIANT(float, 24, 256, false, false), VARIANTS(float, 256)>},
 };
 static constexpr int kNumEntries = int(sizeof(kEntries) / sizeof(kEntries[0]));
 

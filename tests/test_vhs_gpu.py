@@ -143,13 +143,22 @@ def test_two_grids_one_launch_equals_separate(cuda):
         F = np.stack([mixed_maxwellians(vm.cv(), rng) for _ in range(20)])
         grids.append(g)
         fs.append(torch.from_numpy(F).float().to(be.device))
-    both = VHSCollider(grids, be.device)
-    qa = [torch.empty_like(f) for f in fs]
-    both([(1, fs[1], qa[1], None), (0, fs[0], qa[0], None)])
+    from frfs_b200.autotune import variants
+    qb = []
     for i in range(2):
+        grids[i].struct.tile = 0
         one = VHSCollider([grids[i]], be.device)
-        qb = torch.empty_like(fs[i])
-        one([(0, fs[i], qb, None)])
+        qb.append(torch.empty_like(fs[i]))
+        one([(0, fs[i], qb[i], None)])
+    nvar = len(variants(grids))
+    assert nvar >= 2
+    for t in range(nvar):          # every two-grid variant (tile of the first grid)
+        grids[0].struct.tile = t
+        both = VHSCollider(grids, be.device)
+        qa = [torch.empty_like(f) for f in fs]
+        both([(1, fs[1], qa[1], None), (0, fs[0], qa[0], None)])
         torch.cuda.synchronize()
-        err = float((qa[i].double() - qb.double()).norm() / qb.double().norm())
-        assert err < 1e-6, (i, err)
+        for i in range(2):
+            err = float((qa[i].double() - qb[i].double()).norm() / qb[i].double().norm())
+            assert err < 1e-6, (t, i, err)
+    grids[0].struct.tile = 0
