@@ -213,6 +213,157 @@ def codelet(N, sign):
             f'{name}(cpx<T> (&x)[{N}])\n{{\n{body}\n}}\n')
 
 
+# ---------------------------------------------------------------------------
+# Packed codelets: two transforms at once on float2 registers (re[k] holds
+# the real parts of x_A[k] and x_B[k], im[k] the imaginary parts), every
+# operation one sm_100 f32x2 instruction (add / fma / mul on both lanes).
+#
+# The scalar codelet's statements are linear in earlier temporaries, so each
+# is parsed into a linear form {name: coefficient}.  Values are kept lazily
+# as (register, scale): a scale of -1 or a constant factor is carried to the
+# next sum instead of being applied, where it becomes the multiplier of one
+# fused multiply-add, so that negations and twiddle constants cost nothing
+# until an output needs a scale other than 1.
+
+def _tokens(expr):
+    import re
+    return re.findall(r'T\([^)]*\)|x\[\d+\]\.[xy]|t\d+[ri]|[-+*()]', expr)
+
+
+def parse_linear(expr):
+    """Linear form {name: coef} of a codelet expression."""
+    toks = _tokens(expr)
+    pos = [0]
+
+    def peek():
+        return toks[pos[0]] if pos[0] < len(toks) else None
+
+    def take():
+        pos[0] += 1
+        return toks[pos[0] - 1]
+
+    def add(a, b, s):
+        out = dict(a)
+        for k, v in b.items():
+            out[k] = out.get(k, 0.0) + s * v
+        return {k: v for k, v in out.items() if v != 0.0}
+
+    def expr_():
+        v = term()
+        while peek() in ('+', '-'):
+            s = 1.0 if take() == '+' else -1.0
+            v = add(v, term(), s)
+        return v
+
+    def term():
+        v = factor()
+        while peek() == '*':
+            take()
+            w = factor()
+            if '1' in v and len(v) == 1:
+                v = {k: c * v['1'] for k, c in w.items()}
+            elif '1' in w and len(w) == 1:
+                v = {k: c * w['1'] for k, c in v.items()}
+            else:
+                raise ValueError('non-linear ' + expr)
+        return v
+
+    def factor():
+        t = take()
+        if t == '+':
+            return factor()
+        if t == '-':
+            return {k: -c for k, c in factor().items()}
+        if t == '(':
+            v = expr_()
+            assert take() == ')'
+            return v
+        if t.startswith('T('):
+            return {'1': float(t[2:-1])}
+        return {t: 1.0}
+
+    v = expr_()
+    assert pos[0] == len(toks), expr
+    return v
+
+
+def _f(c):
+    return f'{float(c)!r}f'.replace('inf', 'INFINITY')
+
+
+def _pair(c):
+    return f'make_float2({_f(c)}, {_f(c)})'
+
+
+def packed_codelet(N, sign):
+    """float2 version of codelet(N, sign); returns (source, op count)."""
+    import re
+    src = codelet(N, sign)
+    body = src[src.index('{') + 1:src.rindex('}')]
+    stmts = [s.strip() for line in body.strip().splitlines() for s in line.split(';') if s.strip()]
+    alias = {}          # scalar name -> (register, scale)
+    lines, nops, nreg = [], 0, [0]
+
+    def reg():
+        nreg[0] += 1
+        return f'p{nreg[0]}'
+
+    def resolve(form):
+        terms = {}
+        for k, c in form.items():
+            r, g = alias[k]
+            terms[r] = terms.get(r, 0.0) + c * g
+        return [(r, c) for r, c in terms.items() if c != 0.0]
+
+    for st in stmts:
+        m = re.match(r'const T (t\d+[ri]) = (.*)$', st)
+        if m:
+            name, ex = m.groups()
+            mi = re.match(r'x\[(\d+)\]\.([xy])$', ex)
+            if mi:
+                r = reg()
+                arr = 're' if mi.group(2) == 'x' else 'im'
+                lines.append(f'const float2 {r} = {arr}[{mi.group(1)}];')
+                alias[name] = (r, 1.0)
+                continue
+            terms = resolve(parse_linear(ex))
+            if len(terms) == 1:
+                alias[name] = terms[0]
+                continue
+            assert len(terms) == 2, st
+            (pa, ca), (pb, cb) = terms
+            if abs(ca) != 1.0 and abs(cb) == 1.0:
+                (pa, ca), (pb, cb) = (pb, cb), (pa, ca)
+            ratio = cb / ca
+            if abs(abs(ratio) - 1.0) < 1e-12:     # exact in FP32
+                ratio = float(np.sign(ratio))
+            r = reg()
+            if ratio == 1.0:
+                lines.append(f'const float2 {r} = __fadd2_rn({pa}, {pb});')
+            else:
+                lines.append(f'const float2 {r} = __ffma2_rn({pb}, {_pair(ratio)}, {pa});')
+            nops += 1
+            alias[name] = (r, ca)
+            continue
+        m = re.match(r'x\[(\d+)\]\.([xy]) = (t\d+[ri])$', st)
+        assert m, st
+        k, comp, name = m.groups()
+        arr = 're' if comp == 'x' else 'im'
+        r, g = alias[name]
+        if abs(g - 1.0) < 1e-12:
+            g = 1.0
+        if g == 1.0:
+            lines.append(f'{arr}[{k}] = {r};')
+        else:
+            lines.append(f'{arr}[{k}] = __fmul2_rn({r}, {_pair(g)});')
+            nops += 1
+    name = f'dft{N}_{"fwd" if sign < 0 else "inv"}_p2'
+    text = ('__device__ __forceinline__ void '
+            f'{name}(float2 (&re)[{N}], float2 (&im)[{N}])\n{{\n'
+            + '\n'.join('    ' + l for l in lines) + '\n}\n')
+    return text, nops
+
+
 def main():
     out = ['// Generated by gen_fft.py: unnormalised in-register DFT codelets.',
            '// Do not edit by hand.',
@@ -227,11 +378,26 @@ def main():
         disp.append(f'    if constexpr (N == {N}) {{ if constexpr (SIGN < 0) '
                     f'dft{N}_fwd<T>(x); else dft{N}_inv<T>(x); }}')
     disp.append('}')
+    out += disp + ['']
+    # packed (two transforms per thread) codelets, sm_100 f32x2 arithmetic
+    for N in SIZES:
+        for sg in (-1, 1):
+            out.append(packed_codelet(N, sg)[0])
+    disp = ['template <int N, int SIGN>',
+            '__device__ __forceinline__ void dft_p2(float2 (&re)[N], float2 (&im)[N])', '{']
+    for N in SIZES:
+        disp.append(f'    if constexpr (N == {N}) {{ if constexpr (SIGN < 0) '
+                    f'dft{N}_fwd_p2(re, im); else dft{N}_inv_p2(re, im); }}')
+    disp.append('}')
     out += disp + ['', '}  // namespace bdgfs', '']
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)),
                         'fft_codelets.cuh')
     with open(path, 'w') as fh:
         fh.write('\n'.join(out))
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                        'vhs_p2_tables.cuh')
+    with open(path, 'w') as fh:
+        fh.write(p2_header())
 
 
 def reference_check():
@@ -264,6 +430,143 @@ def reference_check():
             assert err < 1e-13, (N, sign, err)
 
 
+# ---------------------------------------------------------------------------
+# Lane tables of the packed Nv = 24 collision kernel (288 threads, two
+# pencils per thread).  Work cube planes Wr/Wi: element (i, j, k) at
+# i*P2_PS + j*P2_RS + k (floats).  Shared-memory banks are 4 bytes, 32 of
+# them; a warp's 8-byte accesses are served per half-warp, one wavefront per
+# distinct 8-byte slot mod 16 in the worst bank.
+#
+# z-pass table: thread t owns pencil A = (kxA, kyA) (kxA <= N/2, read from
+# the Hermitian half Fh) and pencil B = its conjugate partner (N-kxA, N-kyA),
+# except the last two threads, which own the self-conjugate pencils
+# (0,0)+(0,N/2) and (N/2,0)+(N/2,N/2).  Threads are ordered so that each
+# half-warp's z-pair stores of A, of B and its Fh loads fall into distinct
+# slots as far as a greedy pass finds.
+# x-pass table: thread t owns the x-pencils (y, 2m), (y, 2m+1), ordered so
+# that each half-warp's loads Wr[i*PS + y*RS + 2m] hit distinct slots.
+P2_N, P2_PS, P2_RS, P2_FS = 24, 632, 26, 25
+
+
+def p2_tables():
+    import collections
+    import random
+    N, H = P2_N, P2_N // 2
+    base = [((kx, ky), (N - kx, (N - ky) % N)) for kx in range(1, H) for ky in range(N)]
+    base += [((kx, ky), (kx, N - ky)) for kx in (0, H) for ky in range(1, H)]
+    singles = [((0, 0), (0, H)), ((H, 0), (H, H))]
+    keys = (lambda pr: ((pr[0][0] * P2_PS + pr[0][1] * P2_RS) // 2) % 16,
+            lambda pr: ((pr[1][0] * P2_PS + pr[1][1] * P2_RS) // 2) % 16,
+            lambda pr: ((pr[0][0] * N + pr[0][1]) * P2_FS) % 16)
+
+    def greedy(order):
+        left, out = list(order), []
+        while left:
+            cap = 16 if len(out) < len(base) + 2 - 16 else 14
+            used, pick = [set() for _ in keys], []
+            for slack in range(len(keys) + 1):
+                for pr in list(left):
+                    if pr in pick:
+                        continue
+                    ks = [k(pr) for k in keys]
+                    if sum(k in u for k, u in zip(ks, used)) <= slack:
+                        pick.append(pr)
+                        for k, u in zip(ks, used):
+                            u.add(k)
+                        if len(pick) == cap:
+                            break
+                if len(pick) == cap:
+                    break
+            for pr in pick:
+                left.remove(pr)
+            out += pick
+        return out + singles
+
+    def cost(tab):
+        return sum(max(collections.Counter(k(pr) for pr in tab[h:h + 16]).values())
+                   for h in range(0, len(tab), 16) for k in keys)
+
+    best = None
+    for seed in range(64):
+        order = list(base)
+        random.Random(seed).shuffle(order)
+        tab = greedy(order)
+        if best is None or cost(tab) < best[0]:
+            best = (cost(tab), tab)
+    zt = best[1]
+    slot = lambda y, m: ((y * P2_RS + 2 * m) // 2) % 16
+    left, xt = [(y, m) for y in range(N) for m in range(H)], []
+    while left:
+        used, pick = set(), []
+        for pr in list(left):
+            if slot(*pr) not in used:
+                used.add(slot(*pr))
+                pick.append(pr)
+                if len(pick) == 16:
+                    break
+        for pr in list(left):
+            if len(pick) == 16:
+                break
+            if pr not in pick:
+                pick.append(pr)
+        for pr in pick:
+            left.remove(pr)
+        xt += pick
+    # every pencil exactly once
+    assert sorted(p for pr in zt for p in pr) == [(a, b) for a in range(N) for b in range(N)]
+    assert sorted(xt) == [(y, m) for y in range(N) for m in range(H)]
+    assert all(pr[0][0] <= H for pr in zt)
+    return zt, xt
+
+
+def p2_header():
+    zt, xt = p2_tables()
+    z = ', '.join('{%d, %d, %d, %d}' % (a[0], a[1], b[0], b[1]) for a, b in zt)
+    x = ', '.join('{%d, %d}' % p for p in xt)
+    return '\n'.join([
+        '// Generated by gen_fft.py: lane tables of the packed Nv = 24 collision',
+        '// kernel.  Do not edit by hand.',
+        '#pragma once', '', 'namespace bdgfs {', 'namespace p2tab {', '',
+        f'constexpr int N = {P2_N}, PS = {P2_PS}, RS = {P2_RS}, FS = {P2_FS};',
+        '// z-pass: {kxA, kyA, kxB, kyB}; the last two entries are the self-conjugate pairs',
+        f'__constant__ unsigned char zpen[{len(zt)}][4] = {{{z}}};',
+        '// x-pass: {y, m} for the x-pencils (y, 2m), (y, 2m+1)',
+        f'__constant__ unsigned char xpen[{len(xt)}][2] = {{{x}}};',
+        '', '}  // namespace p2tab', '}  // namespace bdgfs', ''])
+
+
+def packed_check():
+    """Execute the packed codelets in numpy (two random transforms at once)."""
+    import re
+    for N in SIZES:
+        for sign in (-1, 1):
+            text, _ = packed_codelet(N, sign)
+            body = text[text.index('{') + 1:text.rindex('}')]
+            py = []
+            for line in body.strip().splitlines():
+                stmt = line.strip().rstrip(';')
+                stmt = re.sub(r'^const float2 ', '', stmt)
+                stmt = re.sub(r'(\d)f\b', r'\1', stmt)
+                py.append(stmt)
+            rng = np.random.default_rng(100 + N)
+            xa = rng.standard_normal(N) + 1j * rng.standard_normal(N)
+            xb = rng.standard_normal(N) + 1j * rng.standard_normal(N)
+            re_ = [np.array([xa[k].real, xb[k].real]) for k in range(N)]
+            im_ = [np.array([xa[k].imag, xb[k].imag]) for k in range(N)]
+            env = {'re': re_, 'im': im_,
+                   '__fadd2_rn': lambda a, b: a + b,
+                   '__ffma2_rn': lambda a, b, c: a * b + c,
+                   '__fmul2_rn': lambda a, b: a * b,
+                   'make_float2': lambda a, b: np.array([a, b])}
+            exec('\n'.join(py), env)
+            for lane, x in ((0, xa), (1, xb)):
+                got = np.array([env['re'][k][lane] + 1j * env['im'][k][lane] for k in range(N)])
+                ref = (np.fft.fft(x) if sign < 0 else np.fft.ifft(x) * N)
+                err = np.abs(got - ref).max() / np.abs(ref).max()
+                assert err < 1e-13, (N, sign, lane, err)
+
+
 if __name__ == '__main__':
     reference_check()
+    packed_check()
     main()

@@ -38,6 +38,8 @@
 #include "common.cuh"
 #include "cpx.cuh"
 #include "fft_codelets.cuh"
+#include "vhs_p2_tables.cuh"
+#include "tcgen05.cuh"
 
 namespace bdgfs {
 
@@ -535,6 +537,455 @@ __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
     __syncthreads();   // Qs/red reuse by the next distribution
 }
 
+// ---------------------------------------------------------------------------
+// Packed variant, Nv = 24, FP32, 288 threads.
+//
+// Every thread carries two pencils through each pass as float2 pairs: re[k]
+// holds the real parts of both pencils' k-th element, im[k] the imaginary
+// parts, and the DFT codelets (dft_p2) issue one sm_100 f32x2 instruction
+// per operation on both pencils.  The FP32 pipe does the same work as with
+// scalar code; the instruction stream halves.  576 pencils per pass are
+// exactly 288 pairs (no idle second round), and the work cube lives as two
+// float planes Wr/Wi (element (i, j, k) at i*PS + j*RS + k), so that the y-
+// and x-passes, which pair pencils along k, load and store 8-byte pairs.
+//
+// z-passes (first pass of each inverse transform, the spectrum built from
+// the Hermitian half Fh) pair pencil A = (kx, ky), kx <= N/2, with its
+// conjugate partner B = (N - kx, N - ky): F_B(kz) = conj(F_A(N - kz)), so one
+// Fh pencil feeds both.  The multiplier of either pencil, Nyquist planes
+// included, is m(kz) = al*Ez.x + be*Ez.y (be2 at kz = N/2), with per-pencil
+// al, be, be2 from Ex(kx), Ey(ky) and their Hermitian-partner counterparts:
+// no per-pencil branches.  Lane tables (vhs_p2_tables.cuh) order the pencil
+// pairs so that shared-memory accesses spread over the banks.
+//
+// S_p (48 floats per thread) lives in tensor memory: with 9 warps per CTA
+// three share an SM sub-partition, which caps registers at 168, and the
+// x-pass needs 96 for its two pencils.  Warp w owns TMEM lanes
+// 32*(w%4).. and columns 48*(w/4).. of a 256-column allocation.
+namespace p2 {
+constexpr int N = p2tab::N, NH = N / 2 + 1, NP2 = N / 2, NT = 288;
+constexpr uint32_t TMEM_COLS = 256;
+static_assert(2 * N * ((NT / 32 + 3) / 4) <= int(TMEM_COLS), "TMEM columns");
+constexpr int PS = p2tab::PS, RS = p2tab::RS, FS = p2tab::FS;
+constexpr int WF = N * PS;                      // floats per plane set
+static_assert(NT == N * NP2 && PS >= N * RS && PS % 2 == 0 && RS % 2 == 0, "packed layout");
+}  // namespace p2
+
+struct QLayoutP2 {
+    static size_t smem_bytes(int M)
+    {
+        size_t b = 2 * size_t(p2::WF) * sizeof(float);                     // Wr, Wi
+        b += size_t(p2::NH) * p2::N * p2::FS * sizeof(cpx<float>);        // Fh
+        b += size_t(M) * 3 * p2::N * sizeof(cpx<float>);                  // phase
+        b += size_t(M) * p2::N * sizeof(float4);                          // (Ez.x, Ez.x, Ez.y, Ez.y)
+        b += 10 * (p2::NT / 32) * sizeof(double) + 16;
+        return b;
+    }
+    // global scratch per CTA: Gh as two float planes [kz][kx <= N/2][ky]
+    static size_t scratch_bytes()
+    {
+        const size_t b = 2 * size_t(p2::N) * p2::NH * p2::N * sizeof(float);
+        return (b + 255) & ~size_t(255);
+    }
+};
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 ld2(const float* p) { return *reinterpret_cast<const float2*>(p); }
+__device__ __forceinline__ void st2(float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
+
+// Multiplier coefficients of pencil (kx, ky) for direction phases ep:
+// m(kz) = a*Ez.x + b*Ez.y (kz != N/2), a*Ez.x + b2*Ez.y (kz = N/2); tr = 1
+// gives those of the Nyquist correction term m_s.  Derived from
+// m = [E.x + E.y + Eb.x - Eb.y]/2, m_s = [E.y + Eb.y - E.x + Eb.x]/2 with
+// E = Ex Ey Ez and Eb the same product at the Hermitian-partner wavenumber.
+__device__ __forceinline__ void p2_coef(const cpx<float>* ep, int kx, int ky, int tr, float& a,
+                                        float& b, float& b2)
+{
+    constexpr int N = p2::N;
+    const cpx<float> Ex = ep[kx], Ey = ep[N + ky];
+    const cpx<float> P = cmul(Ex, Ey);
+    const cpx<float> Pb = cmul(kx == N / 2 ? Ex : conjc(Ex), ky == N / 2 ? Ey : conjc(Ey));
+    if (tr == 0) {
+        a = 0.5f * ((P.x + P.y) + (Pb.x - Pb.y));
+        b = 0.5f * ((P.x - P.y) + (Pb.x + Pb.y));
+        b2 = 0.5f * ((P.x - P.y) - (Pb.x + Pb.y));
+    } else {
+        a = 0.5f * ((P.y - P.x) + (Pb.x + Pb.y));
+        b = 0.5f * ((P.x + P.y) + (Pb.y - Pb.x));
+        b2 = 0.5f * ((P.x + P.y) + (Pb.x - Pb.y));
+    }
+}
+
+// Spectrum of the pencil pair at kz for multipliers m = (m_A, m_B):
+// m * F (tr = 0) or i * m * F (tr = 1).
+__device__ __forceinline__ void p2_spec(int tr, float2 m, cpx<float> FA, cpx<float> FB, float2& vr,
+                                        float2& vi)
+{
+    if (tr == 0) {
+        vr = f2(m.x * FA.x, m.y * FB.x);
+        vi = f2(m.x * FA.y, m.y * FB.y);
+    } else {
+        vr = f2(-m.x * FA.y, -m.y * FB.y);
+        vi = f2(m.x * FA.x, m.y * FB.x);
+    }
+}
+
+// z-pass spectrum of the thread's pencil pair; SINGLES: some lanes of this
+// warp own two self-conjugate pencils (B read from its own Fh pencil).
+template <bool SINGLES>
+__device__ __forceinline__ void p2_pass1_spectrum(int tr, const float4* ez, float2 al, float2 be,
+                                                  float2 be2, const cpx<float>* fa,
+                                                  const cpx<float>* fb, bool single,
+                                                  float2 (&vr)[p2::N], float2 (&vi)[p2::N])
+{
+    constexpr int N = p2::N;
+    auto mval = [&](int kz) {
+        const float4 e = ez[kz];
+        return __ffma2_rn(al, f2(e.x, e.y), __fmul2_rn(kz == N / 2 ? be2 : be, f2(e.z, e.w)));
+    };
+#pragma unroll
+    for (int kz = 0; kz <= N / 2; ++kz) {
+        const int kn = (N - kz) % N;
+        const cpx<float> F0 = fa[kz], F1 = fa[kn];
+        cpx<float> B0 = conjc(F1), B1 = conjc(F0);
+        if constexpr (SINGLES) {
+            if (single) {
+                B0 = fb[kz];
+                B1 = fb[kn];
+            }
+        }
+        p2_spec(tr, mval(kz), F0, B0, vr[kz], vi[kz]);
+        if (kn != kz) p2_spec(tr, mval(kn), F1, B1, vr[kn], vi[kn]);
+    }
+}
+
+__device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict__ f,
+                               float* __restrict__ Qout, double* mom, int flags,
+                               unsigned char* smem, unsigned char* scratch, uint32_t tmem)
+{
+    using namespace p2;
+    const int project = flags & BDGFS_PROJECT;
+    const int ntr = (flags & BDGFS_EXACT) ? 2 : 1;
+    const int tid = threadIdx.x, M = g.M, Nrho = g.Nrho;
+
+    float* Wr = reinterpret_cast<float*>(smem);
+    float* Wi = Wr + WF;
+    cpx<float>* Fh = reinterpret_cast<cpx<float>*>(Wi + WF);
+    cpx<float>* ph = Fh + NH * N * FS;
+    float4* ezz = reinterpret_cast<float4*>(ph + M * 3 * N);
+    double* red = reinterpret_cast<double*>(ezz + M * N);
+    float* Ghr = reinterpret_cast<float*>(scratch);       // [kz][kx <= N/2][ky]
+    float* Ghi = Ghr + N * NH * N;
+
+    // lane tables: z-pass pencil pair, y-pass pair (natural), x-pass pair
+    const int kxA = p2tab::zpen[tid][0], kyA = p2tab::zpen[tid][1];
+    const int kxB = p2tab::zpen[tid][2], kyB = p2tab::zpen[tid][3];
+    const bool single = tid >= NT - 2;
+    const bool single_warp = (tid >> 5) == (NT - 1) / 32;
+    const int offA = kxA * PS + kyA * RS, offB = kxB * PS + kyB * RS;
+    const cpx<float>* fa = Fh + (kxA * N + kyA) * FS;
+    const cpx<float>* fb = Fh + (kxB < NH ? kxB * N + kyB : 0) * FS;
+    const int ybase = (tid / NP2) * PS + 2 * (tid % NP2);      // + j*RS
+    const int xbase = p2tab::xpen[tid][0] * RS + 2 * p2tab::xpen[tid][1];   // + i*PS
+    const float inv_n = 1.f / float(N * N * N);
+    const int warp = tid >> 5;
+    const uint32_t ts = tmem + (uint32_t(32 * (warp & 3)) << 16) + uint32_t(2 * N * (warp >> 2));
+
+    // ---- Fh = FFT(f) / n (kx <= N/2) ----
+    {
+        const int y = tid / NP2, z = 2 * (tid % NP2);      // x-pass, real input
+        float2 vr[N], vi[N];
+#pragma unroll
+        for (int x = 0; x < N; ++x) {
+            const float* fp = f + (x * N + y) * N + z;
+            vr[x] = f2(fp[0], fp[1]);
+            vi[x] = f2(0.f, 0.f);
+        }
+        dft_p2<N, -1>(vr, vi);
+#pragma unroll
+        for (int kx = 0; kx < NH; ++kx) {
+            st2(Wr + kx * PS + y * RS + z, vr[kx]);
+            st2(Wi + kx * PS + y * RS + z, vi[kx]);
+        }
+    }
+    __syncthreads();
+    if (tid < NH * NP2) {                                   // y-pass
+        float2 vr[N], vi[N];
+#pragma unroll
+        for (int j = 0; j < N; ++j) { vr[j] = ld2(Wr + ybase + j * RS); vi[j] = ld2(Wi + ybase + j * RS); }
+        dft_p2<N, -1>(vr, vi);
+#pragma unroll
+        for (int j = 0; j < N; ++j) { st2(Wr + ybase + j * RS, vr[j]); st2(Wi + ybase + j * RS, vi[j]); }
+    }
+    __syncthreads();
+    if (tid < NH * NP2) {                                   // z-pass -> Fh
+        const int kx = tid / NP2, ky = 2 * (tid % NP2);
+        const int b0 = kx * PS + ky * RS;
+        float2 vr[N], vi[N];
+#pragma unroll
+        for (int kz = 0; kz < N; ++kz) {
+            vr[kz] = f2(Wr[b0 + kz], Wr[b0 + RS + kz]);
+            vi[kz] = f2(Wi[b0 + kz], Wi[b0 + RS + kz]);
+        }
+        dft_p2<N, -1>(vr, vi);
+        cpx<float>* F0 = Fh + (kx * N + ky) * FS;
+#pragma unroll
+        for (int kz = 0; kz < N; ++kz) {
+            F0[kz] = {vr[kz].x * inv_n, vi[kz].x * inv_n};
+            F0[FS + kz] = {vr[kz].y * inv_n, vi[kz].y * inv_n};
+        }
+    }
+    // (the first phase staging below is followed by a barrier)
+
+    const cpx<float>* phase = static_cast<const cpx<float>*>(g.phase);
+    const float* gw = static_cast<const float*>(g.gw);
+
+    for (int p = 0; p < Nrho; ++p) {
+        for (int e = tid; e < M * 3 * N; e += NT) {
+            const cpx<float> v = phase[size_t(p) * M * 3 * N + e];
+            ph[e] = v;
+            const int q = e / (3 * N), r = e - q * 3 * N;
+            if (r >= 2 * N) ezz[q * N + (r - 2 * N)] = make_float4(v.x, v.x, v.y, v.y);
+        }
+        __syncthreads();
+
+        for (int qt = 0; qt < M * ntr; ++qt) {
+            const int q = qt / ntr, tr = qt % ntr;
+            const cpx<float>* ep = ph + q * 3 * N;
+            // ---- pass 1: spectrum, inverse along z (pencil pairs of the table) ----
+            {
+                float aA, bA, cA, aB, bB, cB;
+                p2_coef(ep, kxA, kyA, tr, aA, bA, cA);
+                p2_coef(ep, kxB, kyB, tr, aB, bB, cB);
+                float2 vr[N], vi[N];
+                if (single_warp)
+                    p2_pass1_spectrum<true>(tr, ezz + q * N, f2(aA, aB), f2(bA, bB), f2(cA, cB),
+                                            fa, fb, single, vr, vi);
+                else
+                    p2_pass1_spectrum<false>(tr, ezz + q * N, f2(aA, aB), f2(bA, bB), f2(cA, cB),
+                                             fa, fb, single, vr, vi);
+                dft_p2<N, +1>(vr, vi);
+#pragma unroll
+                for (int z = 0; z < N; z += 2) {
+                    st2(Wr + offA + z, f2(vr[z].x, vr[z + 1].x));
+                    st2(Wi + offA + z, f2(vi[z].x, vi[z + 1].x));
+                    st2(Wr + offB + z, f2(vr[z].y, vr[z + 1].y));
+                    st2(Wi + offB + z, f2(vi[z].y, vi[z + 1].y));
+                }
+            }
+            __syncthreads();
+            // ---- pass 2: inverse along y ----
+            {
+                float2 vr[N], vi[N];
+#pragma unroll
+                for (int j = 0; j < N; ++j) { vr[j] = ld2(Wr + ybase + j * RS); vi[j] = ld2(Wi + ybase + j * RS); }
+                dft_p2<N, +1>(vr, vi);
+#pragma unroll
+                for (int j = 0; j < N; ++j) { st2(Wr + ybase + j * RS, vr[j]); st2(Wi + ybase + j * RS, vi[j]); }
+            }
+            __syncthreads();
+            // ---- pass 3: inverse along x, S_p += Re(w^2) = (re + im)(re - im) ----
+            {
+                float2 vr[N], vi[N];
+#pragma unroll
+                for (int i = 0; i < N; ++i) { vr[i] = ld2(Wr + i * PS + xbase); vi[i] = ld2(Wi + i * PS + xbase); }
+                dft_p2<N, +1>(vr, vi);
+                const float2 m1 = f2(-1.f, -1.f);
+                tc::tmem_wait_st();
+#pragma unroll
+                for (int c = 0; c < N / 8; ++c) {
+                    uint32_t r[16];
+                    if (qt > 0) {
+                        tc::tmem_ld16_issue(ts + 16 * c, r);
+                        tc::tmem_wait();
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 16; ++k) r[k] = 0u;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        const int x = 8 * c + k;
+                        const float2 d = tr == 0 ? __ffma2_rn(vi[x], m1, vr[x]) : __ffma2_rn(vr[x], m1, vi[x]);
+                        const float2 sv = __ffma2_rn(__fadd2_rn(vr[x], vi[x]), d,
+                                                     f2(__uint_as_float(r[2 * k]), __uint_as_float(r[2 * k + 1])));
+                        r[2 * k] = __float_as_uint(sv.x);
+                        r[2 * k + 1] = __float_as_uint(sv.y);
+                    }
+                    tc::tmem_st16(ts + 16 * c, r);
+                }
+            }
+            __syncthreads();
+        }
+
+        // ---- Gh += gw_p * FFT(S_p) (kx <= N/2) ----
+        {
+            float2 vr[N], vi[N];                            // x-pass, real input
+            tc::tmem_wait_st();
+#pragma unroll
+            for (int c = 0; c < N / 8; ++c) {
+                uint32_t r[16];
+                tc::tmem_ld16_issue(ts + 16 * c, r);
+                tc::tmem_wait();
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    vr[8 * c + k] = f2(__uint_as_float(r[2 * k]), __uint_as_float(r[2 * k + 1]));
+                    vi[8 * c + k] = f2(0.f, 0.f);
+                }
+            }
+            dft_p2<N, -1>(vr, vi);
+#pragma unroll
+            for (int kx = 0; kx < NH; ++kx) { st2(Wr + kx * PS + xbase, vr[kx]); st2(Wi + kx * PS + xbase, vi[kx]); }
+        }
+        __syncthreads();
+        if (tid < NH * NP2) {                               // y-pass
+            float2 vr[N], vi[N];
+#pragma unroll
+            for (int j = 0; j < N; ++j) { vr[j] = ld2(Wr + ybase + j * RS); vi[j] = ld2(Wi + ybase + j * RS); }
+            dft_p2<N, -1>(vr, vi);
+#pragma unroll
+            for (int j = 0; j < N; ++j) { st2(Wr + ybase + j * RS, vr[j]); st2(Wi + ybase + j * RS, vi[j]); }
+        }
+        __syncthreads();
+        if (tid < NH * NP2) {                               // z-pass, accumulate
+            const int kx = tid / NP2, ky = 2 * (tid % NP2);
+            const int b0 = kx * PS + ky * RS;
+            float2 vr[N], vi[N];
+#pragma unroll
+            for (int kz = 0; kz < N; ++kz) {
+                vr[kz] = f2(Wr[b0 + kz], Wr[b0 + RS + kz]);
+                vi[kz] = f2(Wi[b0 + kz], Wi[b0 + RS + kz]);
+            }
+            dft_p2<N, -1>(vr, vi);
+            const float* gwp = gw + size_t(p) * N * NH * N + kx * N + ky;
+#pragma unroll
+            for (int kz = 0; kz < N; ++kz) {
+                const float2 w = __ldg(reinterpret_cast<const float2*>(gwp + kz * NH * N));
+                const int gi = (kz * NH + kx) * N + ky;
+                if (p == 0) {
+                    st2(Ghr + gi, __fmul2_rn(w, vr[kz]));
+                    st2(Ghi + gi, __fmul2_rn(w, vi[kz]));
+                } else {
+                    st2(Ghr + gi, __ffma2_rn(w, vr[kz], ld2(Ghr + gi)));
+                    st2(Ghi + gi, __ffma2_rn(w, vi[kz], ld2(Ghi + gi)));
+                }
+            }
+        }
+        // the next iteration's phase staging ends with a barrier
+    }
+    __syncthreads();
+
+    // ---- QG + i*fC = IFFT(Gh + i*bb2*Fh) ----
+    const float* bb2 = static_cast<const float*>(g.bb2);
+    {
+        auto spec = [&](int kx, int ky, int kz) -> cpx<float> {
+            const bool direct = kx < NH;
+            const int pkx = direct ? kx : N - kx;
+            const int pky = direct ? ky : (N - ky) % N;
+            const int pkz = direct ? kz : (N - kz) % N;
+            const int gi = (pkz * NH + pkx) * N + pky;
+            cpx<float> G = {Ghr[gi], Ghi[gi]};
+            cpx<float> F = Fh[(pkx * N + pky) * FS + pkz];
+            if (!direct) { G.y = -G.y; F.y = -F.y; }
+            const float b = ldg(bb2 + (kz * N + kx) * N + ky);
+            return {G.x - b * F.y, G.y + b * F.x};
+        };
+        float2 vr[N], vi[N];
+#pragma unroll
+        for (int kz = 0; kz < N; ++kz) {
+            const cpx<float> a = spec(kxA, kyA, kz), b = spec(kxB, kyB, kz);
+            vr[kz] = f2(a.x, b.x);
+            vi[kz] = f2(a.y, b.y);
+        }
+        dft_p2<N, +1>(vr, vi);
+#pragma unroll
+        for (int z = 0; z < N; z += 2) {
+            st2(Wr + offA + z, f2(vr[z].x, vr[z + 1].x));
+            st2(Wi + offA + z, f2(vi[z].x, vi[z + 1].x));
+            st2(Wr + offB + z, f2(vr[z].y, vr[z + 1].y));
+            st2(Wi + offB + z, f2(vi[z].y, vi[z + 1].y));
+        }
+    }
+    __syncthreads();
+    {
+        float2 vr[N], vi[N];
+#pragma unroll
+        for (int j = 0; j < N; ++j) { vr[j] = ld2(Wr + ybase + j * RS); vi[j] = ld2(Wi + ybase + j * RS); }
+        dft_p2<N, +1>(vr, vi);
+#pragma unroll
+        for (int j = 0; j < N; ++j) { st2(Wr + ybase + j * RS, vr[j]); st2(Wi + ybase + j * RS, vi[j]); }
+    }
+    __syncthreads();
+
+    const float prefac = float(g.prefac);
+    const bool need_m = project || mom;
+    float* Qs = reinterpret_cast<float*>(Fh);          // Fh is free from here on
+    double m[5] = {0, 0, 0, 0, 0};
+    {
+        const int y = tid / NP2, z = 2 * (tid % NP2);
+        float2 vr[N], vi[N];
+#pragma unroll
+        for (int i = 0; i < N; ++i) { vr[i] = ld2(Wr + i * PS + y * RS + z); vi[i] = ld2(Wi + i * PS + y * RS + z); }
+        dft_p2<N, +1>(vr, vi);
+        const double cy = need_m ? g.c0[y] : 0.0;
+        const double cz0 = need_m ? g.c0[z] : 0.0, cz1 = need_m ? g.c0[z + 1] : 0.0;
+#pragma unroll
+        for (int x = 0; x < N; ++x) {
+            const int idx = (x * N + y) * N + z;
+            const float q0 = prefac * (vr[x].x - f[idx] * vi[x].x);
+            const float q1 = prefac * (vr[x].y - f[idx + 1] * vi[x].y);
+            float* dst = project ? Qs : Qout;
+            dst[idx] = q0;
+            dst[idx + 1] = q1;
+            if (need_m) {
+                const double cx = g.c0[x], d0 = double(q0), d1 = double(q1);
+                m[0] += d0 + d1;
+                m[1] += cx * (d0 + d1);
+                m[2] += cy * (d0 + d1);
+                m[3] += cz0 * d0 + cz1 * d1;
+                m[4] += (cx * cx + cy * cy + cz0 * cz0) * d0 + (cx * cx + cy * cy + cz1 * cz1) * d1;
+            }
+        }
+    }
+    if (!need_m) return;
+    block_sum<5>(m, red);
+    double m2[5] = {0, 0, 0, 0, 0};
+    if (project) {
+        double lam[5];
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+            double s = 0.0;
+#pragma unroll
+            for (int j = 0; j < 5; ++j) s += g.ginv[i * 5 + j] * m[j];
+            lam[i] = s;
+        }
+        for (int pid = tid; pid < N * N; pid += NT) {
+            const int y = pid / N, z = pid % N;
+            const double cy = g.c0[y], cz = g.c0[z];
+            for (int x = 0; x < N; ++x) {
+                const int idx = (x * N + y) * N + z;
+                const double cx = g.c0[x];
+                const double c2 = cx * cx + cy * cy + cz * cz;
+                const double qc = double(Qs[idx]) - (lam[0] + lam[1] * cx + lam[2] * cy
+                                                     + lam[3] * cz + lam[4] * c2);
+                Qout[idx] = float(qc);
+                m2[0] += qc;
+                m2[1] += cx * qc;
+                m2[2] += cy * qc;
+                m2[3] += cz * qc;
+                m2[4] += c2 * qc;
+            }
+        }
+        if (mom) block_sum<5>(m2, red);
+    }
+    if (mom && tid == 0) {
+        for (int j = 0; j < 5; ++j) {
+            mom[j] = m[j] * g.cw;
+            mom[5 + j] = project ? m2[j] * g.cw : m[j] * g.cw;
+        }
+    }
+    __syncthreads();   // Qs/red reuse by the next distribution
+}
+
 struct KArgs {
     bdgfs_vhs_grid grids[2];
     bdgfs_vhs_batch batches[4];
@@ -550,8 +1001,16 @@ template <typename T, int N, int NT, bool WG, bool SG, int GR = 0, bool SL = fal
 struct Variant {
     using L = QLayout<T, N, NT, WG, SG, SL>;
     static constexpr int n = N;
-    static constexpr bool wg = WG, sg = SG, sl = SL;
+    static constexpr bool wg = WG, sg = SG, sl = SL, pk = false;
     static constexpr int gr = GR;
+};
+
+// packed Nv = 24 FP32 variant (288 threads)
+struct VariantP2 {
+    using L = QLayoutP2;
+    static constexpr int n = p2::N;
+    static constexpr bool wg = false, sg = false, sl = false, pk = true;
+    static constexpr int gr = 0;
 };
 
 // Kernel over a set of grid variants; a distribution of a batch on a grid
@@ -562,6 +1021,12 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int64_t s_item;
     __shared__ int64_t s_start[5];
+    __shared__ uint32_t s_tmem;
+    constexpr bool kPacked = V0::pk || V1::pk;
+    if constexpr (kPacked) {
+        if (threadIdx.x < 32) tc::tmem_alloc(&s_tmem, p2::TMEM_COLS);
+        tc::tc_fence_before();
+    }
     unsigned char* scratch = a.scratch + size_t(blockIdx.x) * a.scratch_per_cta;
     if (threadIdx.x == 0) {
         // per-batch counts: the host size, or a device count when given
@@ -576,6 +1041,11 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
         }
     }
     __syncthreads();
+    uint32_t tmem = 0;
+    if constexpr (kPacked) {
+        tc::tc_fence_after();
+        tmem = s_tmem;
+    }
     const int64_t total = s_start[a.nbatch];
     for (;;) {
         if (threadIdx.x == 0) s_item = int64_t(atomicAdd(a.counter, 1ull));
@@ -595,19 +1065,35 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
         T* Q = static_cast<T*>(bt.Q) + dof * n3;
         double* mom = bt.moments ? bt.moments + dof * 10 : nullptr;
         if (g.Nv == V0::n) {
-            collide_one<T, V0::n, NT, V0::wg, V0::sg, V0::gr, V0::sl>(
-                g, f, Q, mom, a.flags, smem, scratch);
-        } else if constexpr (V1::n > 0) {
-            if (g.Nv == V1::n)
-                collide_one<T, V1::n, NT, V1::wg, V1::sg, V1::gr, V1::sl>(
+            if constexpr (V0::pk)
+                collide_one_p2(g, f, Q, mom, a.flags, smem, scratch, tmem);
+            else
+                collide_one<T, V0::n, NT, V0::wg, V0::sg, V0::gr, V0::sl>(
                     g, f, Q, mom, a.flags, smem, scratch);
+        } else if constexpr (V1::n > 0) {
+            if (g.Nv == V1::n) {
+                if constexpr (V1::pk)
+                    collide_one_p2(g, f, Q, mom, a.flags, smem, scratch, tmem);
+                else
+                    collide_one<T, V1::n, NT, V1::wg, V1::sg, V1::gr, V1::sl>(
+                        g, f, Q, mom, a.flags, smem, scratch);
+            }
+        }
+    }
+    if constexpr (kPacked) {
+        tc::tmem_wait_st();
+        tc::tc_fence_before();
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            tc::tc_fence_after();
+            tc::tmem_dealloc(tmem, p2::TMEM_COLS);
         }
     }
 }
 
 struct NoVariant {
     static constexpr int n = 0;
-    static constexpr bool wg = false, sg = false, sl = false;
+    static constexpr bool wg = false, sg = false, sl = false, pk = false;
     static constexpr int gr = 0;
     struct L {
         static constexpr int WS = 0;
@@ -685,6 +1171,9 @@ static const Entry kEntries[] = {
     {0, 24, 32, 256,
      &launch<float, 256, VARIANT(float, 24, 256, false, false), VARIANTS(float, 256)>,
      &entry_per_cta<float, 256, VARIANT(float, 24, 256, false, false), VARIANTS(float, 256)>},
+    // 24^3 packed: two pencils per thread on f32x2 arithmetic
+    {0, 24, 0, 288, &launch<float, 288, VariantP2, NoVariant>,
+     &entry_per_cta<float, 288, VariantP2, NoVariant>},
 };
 static constexpr int kNumEntries = int(sizeof(kEntries) / sizeof(kEntries[0]));
 

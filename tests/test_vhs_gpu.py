@@ -57,6 +57,36 @@ def test_q_parity(cuda, Nv, Nrho, M, dev, prec, exact, tol):
             np.linalg.norm(loss)
 
 
+@pytest.mark.parametrize('exact', [False, True])
+def test_every_variant_q_parity_24(cuda, exact):
+    """Every Nv=24 FP32 variant (scalar CTA sizes, slab groups and the packed
+    two-pencils-per-thread f32x2 variant, whose Nyquist-plane multipliers
+    and association order differ) against the FP64 reference algorithm,
+    with and without the exact Nyquist correction."""
+    from frfs_b200.autotune import variants
+    from frfs_b200.scattering import VHSCollider
+    be, vm, sm, orc = _setup(24, 12, 12, 6, 'single')
+    rng = np.random.default_rng(124)            # the distributions of test_q_parity
+    F = np.stack([mixed_maxwellians(vm.cv(), rng) for _ in range(3)])
+    fin = torch.from_numpy(F).float().to(be.device)
+    F = fin.double().cpu().numpy()              # the state the kernel sees
+    Qo = [orc.Q(F[i]) for i in range(3)]
+    loss = [np.linalg.norm(orc.gain_loss(F[i])[1]) for i in range(3)]
+    threads = variants([sm.grid])
+    assert 288 in threads
+    for t in range(len(threads)):
+        sm.grid.struct.tile = t
+        col = VHSCollider([sm.grid], be.device)
+        q = torch.empty_like(fin)
+        col([(0, fin, q, None)], project=False, exact=exact)
+        torch.cuda.synchronize()
+        Qg = q.double().cpu().numpy()
+        for i in range(3):
+            assert rel_l2(Qg[i], Qo[i]) < 1e-3, (t, i)
+            assert np.linalg.norm(Qg[i] - Qo[i]) < 1e-5 * loss[i], (t, i)
+    sm.grid.struct.tile = 0
+
+
 def test_q_conservation_projection(cuda):
     be, vm, sm, orc = _setup(24, 12, 12, 6, 'single')
     rng = np.random.default_rng(7)
@@ -104,8 +134,11 @@ def test_q_batch_order_independent(cuda):
 @pytest.mark.parametrize('Nv,Nrho,M,dev,prec', [(24, 12, 12, 6, 'single'), (16, 8, 6, 5, 'single'),
                                                 (16, 8, 6, 5, 'double'), (32, 16, 12, 6, 'single')])
 def test_every_kernel_variant_agrees(cuda, Nv, Nrho, M, dev, prec):
-    """Every compiled variant (CTA size, slab groups) computes the same
-    per-distribution arithmetic, so all agree to FP rounding."""
+    """Every compiled variant (CTA size, slab groups, warp slabs, the packed
+    f32x2 variant) computes the same per-distribution algorithm, so all agree
+    to rounding.  FP32: the packed variant associates sums differently, and
+    Q's gain-loss cancellation turns ~1e-8 relative rounding of the terms
+    into ~1e-5 relative to Q; the bound is 5e-5 (the oracle bound is 1e-3)."""
     from frfs_b200.autotune import variants
     from frfs_b200.scattering import VHSCollider
     be, vm, sm, orc = _setup(Nv, Nrho, M, dev, prec)
@@ -125,7 +158,7 @@ def test_every_kernel_variant_agrees(cuda, Nv, Nrho, M, dev, prec):
     ref = outs[0].double()
     for t, q in enumerate(outs[1:], 1):
         err = float((q.double() - ref).norm() / ref.norm())
-        assert err < (1e-12 if prec == 'double' else 1e-6), (t, err)
+        assert err < (1e-12 if prec == 'double' else 5e-5), (t, err)
 
 
 def test_two_grids_one_launch_equals_separate(cuda):
