@@ -439,13 +439,17 @@ def reference_check():
 #
 # z-pass table: thread t owns pencil A = (kxA, kyA) (kxA <= N/2, read from
 # the Hermitian half Fh) and pencil B = its conjugate partner (N-kxA, N-kyA),
-# except the last two threads, which own the self-conjugate pencils
-# (0,0)+(0,N/2) and (N/2,0)+(N/2,N/2).  Threads are ordered so that each
+# except threads P2_SINGLE_AT and P2_SINGLE_AT + 1, which own the
+# self-conjugate pencils (0,0)+(0,N/2) and (N/2,0)+(N/2,N/2).  Threads are ordered so that each
 # half-warp's z-pair stores of A, of B and its Fh loads fall into distinct
 # slots as far as a greedy pass finds.
 # x-pass table: thread t owns the x-pencils (y, 2m), (y, 2m+1), ordered so
 # that each half-warp's loads Wr[i*PS + y*RS + 2m] hit distinct slots.
 P2_N, P2_PS, P2_RS, P2_FS = 24, 632, 26, 25
+# the two self-conjugate pairs sit at the end of warp 1: with 9 warps, SM
+# sub-partition 0 runs three (0, 4, 8), so the extra loads of these lanes go
+# to a sub-partition with two
+P2_SINGLE_AT = 62
 
 
 def p2_tables():
@@ -462,7 +466,7 @@ def p2_tables():
     def greedy(order):
         left, out = list(order), []
         while left:
-            cap = 16 if len(out) < len(base) + 2 - 16 else 14
+            cap = 14 if len(out) == P2_SINGLE_AT - 14 else 16
             used, pick = [set() for _ in keys], []
             for slack in range(len(keys) + 1):
                 for pr in list(left):
@@ -480,7 +484,7 @@ def p2_tables():
             for pr in pick:
                 left.remove(pr)
             out += pick
-        return out + singles
+        return out[:P2_SINGLE_AT] + singles + out[P2_SINGLE_AT:]
 
     def cost(tab):
         return sum(max(collections.Counter(k(pr) for pr in tab[h:h + 16]).values())
@@ -528,7 +532,8 @@ def p2_header():
         '// kernel.  Do not edit by hand.',
         '#pragma once', '', 'namespace bdgfs {', 'namespace p2tab {', '',
         f'constexpr int N = {P2_N}, PS = {P2_PS}, RS = {P2_RS}, FS = {P2_FS};',
-        '// z-pass: {kxA, kyA, kxB, kyB}; the last two entries are the self-conjugate pairs',
+        f'constexpr int SINGLE_AT = {P2_SINGLE_AT};   // threads SINGLE_AT, SINGLE_AT + 1',
+        '// z-pass: {kxA, kyA, kxB, kyB}; two entries hold the self-conjugate pairs',
         f'__constant__ unsigned char zpen[{len(zt)}][4] = {{{z}}};',
         '// x-pass: {y, m} for the x-pencils (y, 2m), (y, 2m+1)',
         f'__constant__ unsigned char xpen[{len(xt)}][2] = {{{x}}};',

@@ -680,8 +680,9 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
     // lane tables: z-pass pencil pair, y-pass pair (natural), x-pass pair
     const int kxA = p2tab::zpen[tid][0], kyA = p2tab::zpen[tid][1];
     const int kxB = p2tab::zpen[tid][2], kyB = p2tab::zpen[tid][3];
-    const bool single = tid >= NT - 2;
-    const bool single_warp = (tid >> 5) == (NT - 1) / 32;
+    const bool single = tid == p2tab::SINGLE_AT || tid == p2tab::SINGLE_AT + 1;
+    const bool single_warp = (tid >> 5) == p2tab::SINGLE_AT / 32;
+    static_assert(p2tab::SINGLE_AT % 32 < 31, "self-conjugate pairs in one warp");
     const int offA = kxA * PS + kyA * RS, offB = kxB * PS + kyB * RS;
     const cpx<float>* fa = Fh + (kxA * N + kyA) * FS;
     const cpx<float>* fb = Fh + (kxB < NH ? kxB * N + kyB : 0) * FS;
