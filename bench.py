@@ -305,10 +305,11 @@ BATCHED = dict(n24=24576, n32=8192, Nrho=16, M=12, dev=6, omega=0.81, mass2=2.0)
 SMALL64 = dict(Nv=16, Nrho=8, M=6, dev=5, omega=0.5, order=2, nx=4, ny=4, dt=1e-3)
 
 
-def batched_q(flush, reps=3):
+def batched_q(flush, reps=3, sizes=None):
     """Two species on uneven grids (24^3 and 32^3, mass ratio 2) in one
     persistent launch captured in a CUDA graph; returns Q evals/s and the
-    FP32 arrays for the error check."""
+    FP32 arrays for the error check.  sizes: (n24, n32) instead of the
+    workload's (profiling case)."""
     import numpy as np
     import torch
     from frfs_b200.backend import CUDABackend
@@ -316,7 +317,9 @@ def batched_q(flush, reps=3):
     from frfs_b200.scattering import VHSGrid, VHSCollider, vhs_prefactor
     from frfs_b200.velocitymesh import DGFSVelocityMesh
     from frfs_b200.autotune import tune_vhs
-    w = BATCHED
+    w = dict(BATCHED)
+    if sizes is not None:
+        w['n24'], w['n32'] = sizes
     grids, fs = [], []
     gen = torch.Generator(device='cuda').manual_seed(7)
     for Nv, ndof, mass in ((24, w['n24'], 1.0), (32, w['n32'], w['mass2'])):
@@ -374,7 +377,7 @@ def batched_q(flush, reps=3):
         ms.append(a.elapsed_time(b))
     t = sum(ms) / len(ms)
     ndof = w['n24'] + w['n32']
-    return {'workload': 'two species, 24576 x 24^3 + 8192 x 32^3, mass ratio 2, Nrho=16, M=12, '
+    return {'workload': f"two species, {w['n24']} x 24^3 + {w['n32']} x 32^3, mass ratio 2, Nrho=16, M=12, "
                         'one persistent launch in a CUDA graph, FP32 + FP64 projection',
             'q_evals_per_s': ndof / (t * 1e-3), 'ms_per_launch': t,
             'tiles': [int(x.struct.tile) for x in grids]}, (grids, fs, qs)
@@ -981,6 +984,9 @@ def main():
                     help='profiling case: 3 launches of the collision kernel on NDOF cubes')
     ap.add_argument('--surrogate-call', type=int, default=0, metavar='NDOF',
                     help='profiling case: all-surrogate hybrid calls on NDOF cells')
+    ap.add_argument('--q-batched', type=int, default=0, metavar='NDOF24',
+                    help='profiling case: the two-species collision launch on NDOF24 24^3 and '
+                         'NDOF24/3 32^3 cubes')
     ap.add_argument('--ars-only', action='store_true',
                     help='profiling case: the adgfs ARS-222 leg alone')
     ap.add_argument('--fr-only', choices=['couette', 'cavity'],
@@ -990,6 +996,11 @@ def main():
         run_q_only(args.q_only)
     elif args.surrogate_call:
         run_surrogate_call(args.surrogate_call)
+    elif args.q_batched:
+        import torch
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device='cuda')
+        res, _ = batched_q(flush, reps=2, sizes=(args.q_batched, args.q_batched // 3))
+        print(json.dumps(res))
     elif args.ars_only:
         run_ars_only()
     elif args.fr_only:
