@@ -199,6 +199,71 @@ def _oracle_q_worker(F):
     return np.stack([_ORC.Q(f) for f in F])
 
 
+def _oracle_init_multi(grids):
+    """Pool initializer: one reference-algorithm oracle per (key, Nv, Nrho, sz,
+    dev, omega, scale) entry; scale multiplies Q (species mass)."""
+    global _ORCS
+    sys.path.insert(0, ROOT)
+    from oracle.velocitymesh import VelocityMesh
+    from oracle.vhs import VHSOracle
+    _ORCS = {}
+    for key, Nv, Nrho, sz, dev, omega, scale in grids:
+        vm = VelocityMesh(Nv, Nrho, sz, cmax=0.0, Tmax=NONDIM['T0'], dev=dev, **NONDIM)
+        _ORCS[key] = (VHSOracle(vm, omega, 4.17e-10, NONDIM['T0']), scale)
+
+
+def _oracle_q_keyed(item):
+    import numpy as np
+    key, F = item
+    orc, scale = _ORCS[key]
+    return key, np.stack([scale * orc.Q(f) for f in F])
+
+
+def batched_q_error(arrays, per_grid=16, seed=5):
+    """Relative L2 error of the batched launch's Q against the FP64 reference
+    algorithm on a seeded sample of per_grid distributions of each grid
+    (host cores, spawned pool)."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    import numpy as np
+    from frfs_b200.scattering import vhs_prefactor
+    from frfs_b200.sphericaldesign import half_sphere_design
+    grids, fs, qs = arrays
+    w = BATCHED
+    rng = np.random.default_rng(seed)
+    cfgs, items, picks = [], [], {}
+    for gi, (g, mass) in enumerate(zip(grids, (1.0, w['mass2']))):
+        key = f'Nv{g.Nv}'
+        from frfs_b200.inifile import Inifile
+        from frfs_b200.velocitymesh import DGFSVelocityMesh
+        from frfs_b200.backend import CUDABackend
+        cfg = Inifile(couette_ini('single', dict(WORK, Nv=g.Nv, Nrho=w['Nrho'], M=w['M'])))
+        vm = DGFSVelocityMesh(CUDABackend(cfg), cfg)
+        scale = (vhs_prefactor(vm, w['omega'], 4.17e-10, NONDIM['T0'], mass=mass)[1]
+                 / vhs_prefactor(vm, w['omega'], 4.17e-10, NONDIM['T0'], mass=1.0)[1])
+        cfgs.append((key, g.Nv, w['Nrho'], half_sphere_design(w['M']), WORK['dev'], w['omega'], scale))
+        idx = np.sort(rng.choice(fs[gi].shape[0], size=per_grid, replace=False))
+        picks[key] = (gi, idx)
+        F = fs[gi][idx].double().cpu().numpy()
+        items += [(key, c) for c in np.array_split(F, max(1, per_grid // 2))]
+    ncores = min(os.cpu_count() or 1, len(items))
+    with ProcessPoolExecutor(max_workers=ncores, mp_context=mp.get_context('spawn'),
+                             initializer=_oracle_init_multi, initargs=(cfgs,)) as pool:
+        outs = list(pool.map(_oracle_q_keyed, items))
+    err = {}
+    for key, (gi, idx) in picks.items():
+        Qo = np.concatenate([q for k, q in outs if k == key])
+        # the same conservation projection as the kernel, applied in FP64
+        c0 = grids[gi].c0.double().cpu().numpy()
+        cx, cy, cz = np.meshgrid(c0, c0, c0, indexing='ij')
+        Phi = np.stack([np.ones_like(cx), cx, cy, cz, cx * cx + cy * cy + cz * cz]).reshape(5, -1)
+        lam = np.linalg.solve(Phi @ Phi.T, Phi @ Qo.T)
+        Qo = Qo - (Phi.T @ lam).T
+        Qg = qs[gi][idx].double().cpu().numpy()
+        err[key] = float(np.linalg.norm(Qg - Qo) / np.linalg.norm(Qo))
+    return err
+
+
 def make_pool(ncores, Nv, Nrho, sz, dev, omega):
     import multiprocessing as mp
     from concurrent.futures import ProcessPoolExecutor
@@ -302,6 +367,9 @@ def config_block(n):
 
 # ---------------------------------------------------------------- other configs
 BATCHED = dict(n24=24576, n32=8192, Nrho=16, M=12, dev=6, omega=0.81, mass2=2.0)
+# DRAM bytes (read + write) of one collision launch on the 2048-DOF Couette
+# state, from an ncu capture of the packed Nv=24 variant (114.6 MB + 99.5 MB)
+Q_LAUNCH_DRAM_BYTES = 114.58e6 + 99.50e6
 SMALL64 = dict(Nv=16, Nrho=8, M=6, dev=5, omega=0.5, order=2, nx=4, ny=4, dt=1e-3)
 
 
@@ -794,8 +862,13 @@ def run_gpu(args):
     extra = {}
     if ws == 1 and not args.no_extra:
         extra['plain_fp64_small'] = small_fp64(flush)
-        bq, _ = batched_q(flush)
+        bq, arrays = batched_q(flush)
+        bq['q_rel_l2_err_vs_fp64_reference'] = batched_q_error(arrays)
+        bq['error_sample'] = ('16 seeded distributions per grid, FP64 reference algorithm on the '
+                              'host cores followed by the same conservation projection as the '
+                              'kernel (applied in FP64)')
         extra['batched_q'] = bq
+        del arrays
         extra['ars_bgk'] = ars_bgk(flush)
     if ws == 1 and not args.no_surrogate:
         c4, c5 = surrogate_legs(flush)
@@ -815,7 +888,11 @@ def run_gpu(args):
                      'frac': achieved / peak,
                      'peak_source': 'measured FP32 FMA probe on this GPU (MEASURED_PEAKS.json has '
                                     'no FP32 CUDA-core figure)',
-                     'flop_per_launch': flop, 'launch_ms': q_ms, 'traffic': None},
+                     'flop_per_launch': flop, 'launch_ms': q_ms,
+                     # dram__bytes_read.sum + dram__bytes_write.sum of one captured launch
+                     # of the same kernel variant on 2048 Nv=24 cubes (ncu --set full);
+                     # algorithmic: f in + Q out = 2 x 113 MB
+                     'traffic': Q_LAUNCH_DRAM_BYTES, 'traffic_alg': 2 * 4 * ndof * 24**3},
         'e2e': {'value': e2e, 'unit': 'DG steps/s', 'h2d_bytes_per_step': nbytes,
                 'd2h_bytes_per_step': nbytes},
         'gpu_launches': launches,
