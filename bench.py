@@ -1032,11 +1032,28 @@ uz = 0
     nbytes = 4 * nv * E * (4 * U + 2 * F)          # u, x1, x2 in + out; own and neighbour faces
     peak = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)),
                                        'MEASURED_PEAKS.json')))['hbm_gbs']
-    print(json.dumps({'fr_only': kind, 'neles': E, 'nupts': U, 'nfpts': F, 'nv': nv,
-                      'disu_ms': t_disu, 'bc_update_ms': t_bc, 'rhs_ms': t_rhs,
-                      'rhs_bytes': nbytes, 'rhs_gbs': nbytes / (t_rhs * 1e-3) / 1e9,
-                      'rhs_frac_of_hbm': nbytes / (t_rhs * 1e-3) / 1e9 / peak,
-                      'disu_gbs': 4 * nv * E * (U + F) / (t_disu * 1e-3) / 1e9}))
+    res = {'fr_only': kind, 'neles': E, 'nupts': U, 'nfpts': F, 'nv': nv,
+           'disu_ms': t_disu, 'bc_update_ms': t_bc, 'rhs_ms': t_rhs,
+           'rhs_bytes': nbytes, 'rhs_gbs': nbytes / (t_rhs * 1e-3) / 1e9,
+           'rhs_frac_of_hbm': nbytes / (t_rhs * 1e-3) / 1e9 / peak,
+           'disu_gbs': 4 * nv * E * (U + F) / (t_disu * 1e-3) / 1e9}
+    if s.ele.fsel is not None:
+        # face values read from the state (no disu): u, x1, x2 in + out, neighbour faces
+        from frfs_b200 import _lib
+        L, fsel = _lib.lib(), s.ele.fsel.data_ptr()
+        u = s._bank(0)
+        t_bcg = timed(lambda: L.bdgfs_fr_bc_update_gather(
+            _lib.ref(s.ele.struct), _lib.ref(s.walls.struct), fsel, u.data_ptr(),
+            _lib.stream_ptr())) if s.walls.nwall else 0.0
+        t_rg = timed(lambda: L.bdgfs_fr_rhs_gather(
+            _lib.ref(s.ele.struct), _lib.ref(s.walls.struct), fsel, u.data_ptr(), out.data_ptr(),
+            0.5, 2.5e-4, x1.data_ptr(), 2.5e-4, x2.data_ptr(), 0.5, _lib.stream_ptr()))
+        gbytes = 4 * nv * E * (4 * U + F)
+        res.update({'gather_bc_update_ms': t_bcg, 'gather_rhs_ms': t_rg, 'gather_rhs_bytes': gbytes,
+                    'gather_rhs_frac_of_hbm': gbytes / (t_rg * 1e-3) / 1e9 / peak,
+                    'stage_ms_disu_path': t_disu + t_bc + t_rhs,
+                    'stage_ms_gather_path': t_bcg + t_rg})
+    print(json.dumps(res))
 
 
 def run_ars_only():

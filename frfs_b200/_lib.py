@@ -18,7 +18,8 @@ _ERRORS = {-1: 'invalid argument', -2: 'CUDA error', -3: 'unsupported grid/preci
 EXPORTS = (
     'bdgfs_vhs_scratch_bytes', 'bdgfs_vhs_collide', 'bdgfs_vhs_tiles', 'bdgfs_fma_probe',
     'bdgfs_vhs_collide_static',
-    'bdgfs_fr_disu', 'bdgfs_fr_bc_update', 'bdgfs_fr_rhs',
+    'bdgfs_fr_disu', 'bdgfs_fr_bc_update', 'bdgfs_fr_rhs', 'bdgfs_fr_rhs_gather',
+    'bdgfs_fr_bc_update_gather',
     'bdgfs_moments', 'bdgfs_residual', 'bdgfs_status_check',
     'bdgfs_gemm', 'bdgfs_colsum', 'bdgfs_adamw', 'bdgfs_relmse',
     'bdgfs_hybrid_classify', 'bdgfs_hybrid_project', 'bdgfs_hybrid_scatter',
@@ -125,6 +126,8 @@ def lib():
             'bdgfs_fr_disu': [vp, vp, vp, vp],
             'bdgfs_fr_bc_update': [vp, vp, vp, vp],
             'bdgfs_fr_rhs': [vp, vp, vp, vp, vp, dbl, dbl, vp, dbl, vp, dbl, vp],
+            'bdgfs_fr_rhs_gather': [vp, vp, vp, vp, vp, dbl, dbl, vp, dbl, vp, dbl, vp],
+            'bdgfs_fr_bc_update_gather': [vp, vp, vp, vp, vp],
             'bdgfs_moments': [vp, i64, i32, i32, vp, dbl, vp, vp],
             'bdgfs_residual': [vp, vp, i64, i32, vp, vp],
             'bdgfs_status_check': [vp, i64, i32, vp, vp],

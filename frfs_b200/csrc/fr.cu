@@ -171,9 +171,14 @@ __global__ void __launch_bounds__(128) disu_kernel(const bdgfs_fr_eles el, const
     }
 }
 
-template <typename T, int ND, int NU, int NF, int VB>
+// GATHER: no face-value array; the face value of face point f of element e
+// is the solution-point row u[e][fsel[f]] (M0 rows are unit vectors, as with
+// GLL points), and a neighbour entry e'*NF + f' of nbr reads u[e'][fsel[f']].
+// out must not alias u then (other CTAs read u's face rows).
+template <typename T, int ND, int NU, int NF, int VB, bool GATHER = false>
 __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, const bdgfs_fr_walls wl,
                                                   const T* __restrict__ u, const T* __restrict__ uf,
+                                                  const int32_t* __restrict__ fsel,
                                                   T* out, T a, T b, const T* x1, T c1, const T* x2,
                                                   T c2, int64_t chunk)
 {
@@ -186,6 +191,7 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
     T* pn = rj + NU;                                    // [NF][ND]
     T* mg = pn + NF * ND;                               // [NF]
     int* nb = reinterpret_cast<int*>(mg + NF);          // [NF]
+    int* fs = nb + NF;                                  // [NF] (GATHER)
     const int64_t e = blockIdx.y;
     {
         for (int i = threadIdx.x; i < (ND * NU + NF) * NUP; i += blockDim.x) dT[i] = T(0);
@@ -210,6 +216,7 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
         for (int i = threadIdx.x; i < NF; i += blockDim.x) {
             mg[i] = gg[i];
             nb[i] = el.nbr[e * NF + i];
+            if constexpr (GATHER) fs[i] = fsel[i];
         }
     }
     __syncthreads();
@@ -253,18 +260,29 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
         // surface: common normal flux at each face point, lifted by M3
         // face values: ul and the neighbour's (or the wall Maxwellian's) row,
         // prefetched one face ahead
+        auto lsrc = [&](int f) -> const T* {
+            if constexpr (GATHER) return u + (e * NU + fs[f]) * nv + v0;
+            else return uf + (e * NF + f) * nv + v0;
+        };
         auto rsrc = [&](int f) -> const T* {
             const int n = nb[f];
-            return n >= 0 ? uf + int64_t(n) * nv + v0 : fw + int64_t(wl.bcid[-1 - n]) * nv + v0;
+            if (n < 0) return fw + int64_t(wl.bcid[-1 - n]) * nv + v0;
+            if constexpr (GATHER) {
+                const int en = n / NF;
+                if (en >= el.neles) return lsrc(f);     // outside this state: no flux
+                return u + (int64_t(en) * NU + fs[n - en * NF]) * nv + v0;
+            } else {
+                return uf + int64_t(n) * nv + v0;
+            }
         };
         Vec<T, VB> ulp, urp;
-        ulp.load(uf + (e * NF) * nv + v0);
+        ulp.load(lsrc(0));
         urp.load(rsrc(0));
 #pragma unroll 1
         for (int f = 0; f < NF; ++f) {
             Vec<T, VB> ul = ulp, ur = urp;
             if (f + 1 < NF) {
-                ulp.load(uf + (e * NF + f + 1) * nv + v0);
+                ulp.load(lsrc(f + 1));
                 urp.load(rsrc(f + 1));
             }
             const int n = nb[f];
@@ -325,10 +343,13 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
     }
 }
 
+// uf: face-value rows [E][NF]; or, with fsel, the solution-point rows of u
+// ([E][NU]) read at row fsel[f] (GATHER, M0 rows unit vectors)
 template <typename T>
 __global__ void __launch_bounds__(256) bc_update_kernel(const bdgfs_fr_eles el,
                                                         const bdgfs_fr_walls wl,
-                                                        const T* __restrict__ uf)
+                                                        const T* __restrict__ uf,
+                                                        const int32_t* __restrict__ fsel)
 {
     __shared__ double red[2 * 8];
     const int w = blockIdx.x;
@@ -338,7 +359,8 @@ __global__ void __launch_bounds__(256) bc_update_kernel(const bdgfs_fr_eles el,
     const T* pn = static_cast<const T*>(el.pnorm) + (int64_t(e) * el.nfpts + f) * ND;
     const T* uw = static_cast<const T*>(wl.uwall) + bid * 3;
     const T* fw = static_cast<const T*>(wl.fw) + int64_t(bid) * el.nv;
-    const T* ul = uf + (int64_t(e) * el.nfpts + f) * el.nv;
+    const T* ul = fsel ? uf + (int64_t(e) * el.nupts + fsel[f]) * el.nv
+                       : uf + (int64_t(e) * el.nfpts + f) * el.nv;
     const T* c0 = static_cast<const T*>(el.c0);
     double s0 = 0.0, s1 = 0.0;
     // four velocities per step (16-byte loads) when rows are aligned
@@ -499,38 +521,38 @@ static int vec_width(int64_t nv, const void* const* ptrs, int n)
 
 template <typename T, int ND, int NU, int NF, int VB>
 static int rhs_launch_vb(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl, const void* u,
-                         const void* uf, void* out, double a, double b, const void* x1, double c1,
-                         const void* x2, double c2, cudaStream_t st)
+                         const void* uf, const int32_t* fsel, void* out, double a, double b,
+                         const void* x1, double c1, const void* x2, double c2, cudaStream_t st)
 {
     constexpr int NUP = (NU + 3) / 4 * 4;
     const int64_t chunk = fr_chunk(el->nv, el->neles, VB);
     dim3 g;
     if (grid_v(el->nv, el->neles, chunk, &g) != BDGFS_OK) return BDGFS_EINVAL;
     const size_t smem = sizeof(T) * ((ND * NU + NF) * NUP + NU * ND * ND + NU + NF * ND + NF)
-                        + sizeof(int) * NF + 16;
-    auto k = rhs_kernel<T, ND, NU, NF, VB>;
+                        + sizeof(int) * 2 * NF + 16;
+    auto k = fsel ? rhs_kernel<T, ND, NU, NF, VB, true> : rhs_kernel<T, ND, NU, NF, VB, false>;
     if (smem > 48 * 1024 &&
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
         return BDGFS_ECUDA;
     bdgfs_fr_walls w0{};
     k<<<g, 128, smem, st>>>(*el, wl ? *wl : w0, static_cast<const T*>(u), static_cast<const T*>(uf),
-                            static_cast<T*>(out), T(a), T(b), static_cast<const T*>(x1), T(c1),
+                            fsel, static_cast<T*>(out), T(a), T(b), static_cast<const T*>(x1), T(c1),
                             static_cast<const T*>(x2), T(c2), chunk);
     return cuda_status(cudaGetLastError());
 }
 
 template <typename T, int ND, int NU, int NF>
 static int rhs_launch(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl, const void* u,
-                      const void* uf, void* out, double a, double b, const void* x1, double c1,
-                      const void* x2, double c2, cudaStream_t st)
+                      const void* uf, const int32_t* fsel, void* out, double a, double b,
+                      const void* x1, double c1, const void* x2, double c2, cudaStream_t st)
 {
     const void* ptrs[] = {u, uf, out, x1, x2, wl ? wl->fw : nullptr};
     // 4 velocities per thread for float (each operator column read from
     // shared memory feeds 4 x 4 FMAs; measured faster than 2 also for NU = 27)
     constexpr int VBW = sizeof(T) == 4 ? 4 : 2;
     if (vec_width<T>(el->nv, ptrs, 6) >= VBW)
-        return rhs_launch_vb<T, ND, NU, NF, VBW>(el, wl, u, uf, out, a, b, x1, c1, x2, c2, st);
-    return rhs_launch_vb<T, ND, NU, NF, 1>(el, wl, u, uf, out, a, b, x1, c1, x2, c2, st);
+        return rhs_launch_vb<T, ND, NU, NF, VBW>(el, wl, u, uf, fsel, out, a, b, x1, c1, x2, c2, st);
+    return rhs_launch_vb<T, ND, NU, NF, 1>(el, wl, u, uf, fsel, out, a, b, x1, c1, x2, c2, st);
 }
 
 template <typename T, int NU, int NF, int VB>
@@ -605,9 +627,28 @@ extern "C" int32_t bdgfs_fr_bc_update(const bdgfs_fr_eles* el, const bdgfs_fr_wa
         return BDGFS_EINVAL;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (el->fp64)
-        bc_update_kernel<double><<<wl->nwall, 256, 0, st>>>(*el, *wl, static_cast<const double*>(uf));
+        bc_update_kernel<double><<<wl->nwall, 256, 0, st>>>(*el, *wl, static_cast<const double*>(uf),
+                                                            nullptr);
     else
-        bc_update_kernel<float><<<wl->nwall, 256, 0, st>>>(*el, *wl, static_cast<const float*>(uf));
+        bc_update_kernel<float><<<wl->nwall, 256, 0, st>>>(*el, *wl, static_cast<const float*>(uf),
+                                                           nullptr);
+    return cuda_status(cudaGetLastError());
+}
+
+extern "C" int32_t bdgfs_fr_bc_update_gather(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl,
+                                             const int32_t* fsel, const void* u, void* stream)
+{
+    int rc = check_eles(el);
+    if (rc != BDGFS_OK) return rc;
+    if (!wl || !u || !fsel) return BDGFS_EINVAL;
+    if (wl->nwall == 0) return BDGFS_OK;
+    if (wl->nwall < 0 || !wl->fpt || !wl->bcid || !wl->uwall || !wl->fw || !wl->bcv)
+        return BDGFS_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (el->fp64)
+        bc_update_kernel<double><<<wl->nwall, 256, 0, st>>>(*el, *wl, static_cast<const double*>(u), fsel);
+    else
+        bc_update_kernel<float><<<wl->nwall, 256, 0, st>>>(*el, *wl, static_cast<const float*>(u), fsel);
     return cuda_status(cudaGetLastError());
 }
 
@@ -628,8 +669,28 @@ extern "C" int32_t bdgfs_fr_rhs(const bdgfs_fr_eles* el, const bdgfs_fr_walls* w
     }
 #define GO(D, U, F)                                                                          \
     if (el->ndims == D && el->nupts == U && el->nfpts == F)                                  \
-        return el->fp64 ? rhs_launch<double, D, U, F>(el, wl, u, uf, out, a, b, x1, c1, x2, c2, st) \
-                        : rhs_launch<float, D, U, F>(el, wl, u, uf, out, a, b, x1, c1, x2, c2, st);
+        return el->fp64 ? rhs_launch<double, D, U, F>(el, wl, u, uf, nullptr, out, a, b, x1, c1, x2, c2, st) \
+                        : rhs_launch<float, D, U, F>(el, wl, u, uf, nullptr, out, a, b, x1, c1, x2, c2, st);
+    BDGFS_FR_SHAPES(GO)
+#undef GO
+    return BDGFS_EUNSUPPORTED;
+}
+
+extern "C" int32_t bdgfs_fr_rhs_gather(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl,
+                                       const int32_t* fsel, const void* u, void* out, double a,
+                                       double b, const void* x1, double c1, const void* x2,
+                                       double c2, void* stream)
+{
+    int rc = check_eles(el);
+    if (rc != BDGFS_OK) return rc;
+    if (!u || !out || !fsel || out == u) return BDGFS_EINVAL;
+    if (wl && wl->nwall > 0 && (!wl->bcid || !wl->uwall || !wl->fw || !wl->bcv))
+        return BDGFS_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+#define GO(D, U, F)                                                                          \
+    if (el->ndims == D && el->nupts == U && el->nfpts == F)                                  \
+        return el->fp64 ? rhs_launch<double, D, U, F>(el, wl, u, nullptr, fsel, out, a, b, x1, c1, x2, c2, st) \
+                        : rhs_launch<float, D, U, F>(el, wl, u, nullptr, fsel, out, a, b, x1, c1, x2, c2, st);
     BDGFS_FR_SHAPES(GO)
 #undef GO
     return BDGFS_EUNSUPPORTED;

@@ -39,7 +39,12 @@ class DGFSElements:
         dt = backend.fpdtype
         c = lambda a: backend.const(np.ascontiguousarray(a), dtype=dt)
         self.neles, self.nupts, self.nfpts, self.ndims = geo.neles, geo.nupts, geo.nfpts, geo.ndims
-        self.m0 = c(shp.opmat('M0'))
+        m0 = np.asarray(shp.opmat('M0'))
+        self.m0 = c(m0)
+        # flux points on solution points (every row of M0 a unit vector, as
+        # with GLL points): face values are rows of the state itself
+        unit = np.all(np.count_nonzero(m0, axis=1) == 1) and np.all(m0.max(axis=1) == 1.0)
+        self.fsel = (backend.const(np.argmax(m0, axis=1), dtype=torch.int32) if unit else None)
         self.dcorr = c(shp.opmat('M1 - M3*M2'))
         self.m3 = c(shp.opmat('M3'))
         self.smats = c(geo.smats)
@@ -221,18 +226,41 @@ class DGFSSystem:
         self.advect_begin(uinbank, outbank)
         self.advect_end(t, a, b, x1, c1, x2, c2)
 
+    def _gathers(self):
+        """Face values straight from the state (bdgfs_fr_*_gather): GLL-type
+        flux points, one part (no halo rows) and out distinct from u."""
+        return (self.ele.fsel is not None and self.domain is None
+                and self._active[0] != self._active[1])
+
     def advect_begin(self, uinbank, outbank):
         """First half of a stage: face values of the stage input."""
         self._active = (uinbank, outbank)
-        self._disu()
+        if not self._gathers():
+            self._disu()
 
     def advect_end(self, t, a, b, x1=None, c1=0.0, x2=None, c2=0.0):
         """Second half: halo exchange, wall update, fused FR + combination."""
+        x1 = self._bank(x1) if x1 is not None else None
+        x2 = self._bank(x2) if x2 is not None else None
+        if self._gathers():
+            L = _lib.lib()
+            u, out = self._bank(self._active[0]), self._bank(self._active[1])
+            fsel = self.ele.fsel.data_ptr()
+            if self.walls.nwall:
+                _lib.check(L.bdgfs_fr_bc_update_gather(_lib.ref(self.ele.struct),
+                                                       _lib.ref(self.walls.struct), fsel,
+                                                       u.data_ptr(), _lib.stream_ptr()),
+                           'bdgfs_fr_bc_update_gather')
+            _lib.check(L.bdgfs_fr_rhs_gather(_lib.ref(self.ele.struct), _lib.ref(self.walls.struct),
+                                             fsel, u.data_ptr(), out.data_ptr(), float(a), float(b),
+                                             x1.data_ptr() if x1 is not None else None, float(c1),
+                                             x2.data_ptr() if x2 is not None else None, float(c2),
+                                             _lib.stream_ptr()), 'bdgfs_fr_rhs_gather')
+            return
         self._exchange()
         if self.walls.nwall:
             self._update_bc()
-        self._fused_rhs(a=a, b=b, x1=self._bank(x1) if x1 is not None else None, c1=c1,
-                        x2=self._bank(x2) if x2 is not None else None, c2=c2)
+        self._fused_rhs(a=a, b=b, x1=x1, c1=c1, x2=x2, c2=c2)
 
     # -- diagnostics ------------------------------------------------------
     def moments(self, bank):

@@ -176,6 +176,25 @@ int32_t bdgfs_fr_rhs(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl,
                      double b, const void* x1, double c1, const void* x2,
                      double c2, void* stream);
 
+/* Face points on solution points (every row of M0 a unit vector, as with
+ * GLL points): fsel[f] (int32 [nfpts], device) is the solution point of
+ * flux point f, and the face values are read from u itself, so no uf array
+ * and no bdgfs_fr_disu are needed.  bdgfs_fr_rhs_gather computes what
+ * bdgfs_fr_disu + bdgfs_fr_rhs compute (bitwise); nbr entries e'*nfpts + f'
+ * read u[e'][fsel[f']] (entries past the state, e.g. halo rows of a
+ * partitioned mesh, are not supported and read as the element's own face
+ * value).  out must not alias u (BDGFS_EINVAL): other
+ * elements read u's face rows during the launch.  bdgfs_fr_bc_update_gather
+ * is bdgfs_fr_disu + bdgfs_fr_bc_update. */
+int32_t bdgfs_fr_rhs_gather(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl,
+                            const int32_t* fsel, const void* u, void* out,
+                            double a, double b, const void* x1, double c1,
+                            const void* x2, double c2, void* stream);
+int32_t bdgfs_fr_bc_update_gather(const bdgfs_fr_eles* el,
+                                  const bdgfs_fr_walls* wl,
+                                  const int32_t* fsel, const void* u,
+                                  void* stream);
+
 /* FP64 raw velocity moments of ndof distributions, out[ndof][13]:
  * cw*sum{f, c f (3), c_i c_j f (xx xy xz yy yz zz), |c|^2 c f (3)}.
  * Feeds the macroscopic fields of plugins/dgfsmomwriterstd.py:14-313. */

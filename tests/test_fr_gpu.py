@@ -186,3 +186,55 @@ def test_tensor_core_rhs_matches_cuda_core_rhs(cuda, kind, order):
     # 3xTF32 keeps ~22 significant bits per product; the residual is a sum with
     # cancellation: within the FP32 tolerance of the FR parity tests
     assert rel_l2(outs[0].double().cpu().numpy(), outs[1].double().cpu().numpy()) < 2e-5
+
+
+@pytest.mark.parametrize('kind,order,prec', [('quad', 3, 'single'), ('hex', 2, 'single'),
+                                             ('hex', 2, 'double')])
+def test_gather_rhs_equals_disu_rhs(cuda, kind, order, prec):
+    """GLL flux points: bdgfs_fr_bc_update_gather / bdgfs_fr_rhs_gather read
+    the face values from the state itself and give bitwise the results of
+    bdgfs_fr_disu + bdgfs_fr_bc_update + bdgfs_fr_rhs; the aliasing guard
+    refuses out == u."""
+    from frfs_b200 import _lib
+    cfg, be, mesh, s = _system(kind, order, prec)
+    assert s.ele.fsel is not None
+    _perturb(s, 11)
+    u = s.eles_scal_upts_inb_full[0]
+    x1, x2 = u * 1.5, u * 0.5
+    s.updatebc(0.0, 0, 1)
+    bc_ref = s.walls.bcv.clone()
+    ref = torch.empty_like(u)
+    s._active = (0, 1)
+    s._fused_rhs(a=0.5, b=2.0, x1=x1, c1=0.25, x2=x2, c2=-0.5, out=ref)
+    s.walls.bcv.zero_()
+    L, fsel = _lib.lib(), s.ele.fsel.data_ptr()
+    _lib.check(L.bdgfs_fr_bc_update_gather(_lib.ref(s.ele.struct), _lib.ref(s.walls.struct), fsel,
+                                           u.data_ptr(), _lib.stream_ptr()), 'bc_update_gather')
+    out = torch.empty_like(u)
+    _lib.check(L.bdgfs_fr_rhs_gather(_lib.ref(s.ele.struct), _lib.ref(s.walls.struct), fsel,
+                                     u.data_ptr(), out.data_ptr(), 0.5, 2.0, x1.data_ptr(), 0.25,
+                                     x2.data_ptr(), -0.5, _lib.stream_ptr()), 'rhs_gather')
+    torch.cuda.synchronize()
+    assert torch.equal(s.walls.bcv, bc_ref)
+    assert torch.equal(out, ref)
+    assert L.bdgfs_fr_rhs_gather(_lib.ref(s.ele.struct), _lib.ref(s.walls.struct), fsel,
+                                 u.data_ptr(), u.data_ptr(), 0.5, 2.0, None, 0.0, None, 0.0,
+                                 _lib.stream_ptr()) == -1
+
+
+def test_stepper_gather_path_equals_disu_path(cuda):
+    """Two SSP-RK2 steps through the gather path (the default for one part
+    and GLL points) equal the same steps with the face-value array."""
+    outs = []
+    for gather in (True, False):
+        cfg, be, mesh, s = _system('hex', 2, 'single')
+        _perturb(s, 3)
+        if not gather:
+            s.ele.fsel = None
+        integ = get_integrator(be, s, cfg)
+        for _ in range(2):
+            integ.step(integ.tcurr, 1e-4)
+            integ.tcurr += 1e-4
+        torch.cuda.synchronize()
+        outs.append(s.eles_scal_upts_inb_full[0].clone())
+    assert torch.equal(outs[0], outs[1])
