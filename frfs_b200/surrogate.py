@@ -548,12 +548,17 @@ class HybridCollider:
     spectral elsewhere, spectral re-check of a seeded ``recheck`` fraction of
     the surrogate cells (their spectral result is kept)."""
 
-    def __init__(self, model, threshold=0.05, recheck=0.02, project=True):
+    def __init__(self, model, threshold=0.05, recheck=0.02, project=True, overlap=True):
+        """overlap: run the spectral launch on a side stream next to the
+        surrogate GEMMs (the GEMMs fill the SMs the persistent spectral
+        launch leaves idle in its last round); joined before the scatter."""
         from .scattering import VHSCollider
         self.model = model
         self.grid = model.grid
         self.threshold, self.recheck, self.project = float(threshold), float(recheck), project
         self.spectral = VHSCollider([self.grid], model.device)
+        self.overlap = overlap
+        self._side = None
         self._n = 0
         self._net = None
 
@@ -617,11 +622,23 @@ class HybridCollider:
         f2, q2 = fin.reshape(-1, n), fout.reshape(-1, n)
         ndof = self.classify(f2, seed)
         L = _lib.lib()
-        # spectral cells (incl. re-checks): index list + device count
-        self.spectral([(0, f2, q2, None)], project=self.project, exact=False,
-                      index=self.spec_idx, count=self.counts[1:2])
-        # surrogate cells: compact rows, then projection fused with the scatter
+        # spectral cells (incl. re-checks): index list + device count; the
+        # surrogate rows (compact GEMMs) meanwhile on the main stream
+        main = torch.cuda.current_stream()
+        if self.overlap:
+            if self._side is None:
+                self._side = torch.cuda.Stream(device=self.model.device)
+            self._side.wait_stream(main)
+            with torch.cuda.stream(self._side):
+                self.spectral([(0, f2, q2, None)], project=self.project, exact=False,
+                              index=self.spec_idx, count=self.counts[1:2])
+        else:
+            self.spectral([(0, f2, q2, None)], project=self.project, exact=False,
+                          index=self.spec_idx, count=self.counts[1:2])
         self.model.infer(self, ndof)
+        if self.overlap:
+            main.wait_stream(self._side)
+        # projection fused with the scatter (reads the re-checked spectral rows)
         fn = L.bdgfs_hybrid_project_scatter if self.project else L.bdgfs_hybrid_scatter
         _lib.check(fn(C.byref(self.args), self.Qc.data_ptr(), q2.data_ptr(), _lib.stream_ptr()),
                    'bdgfs_hybrid_project_scatter')

@@ -228,3 +228,34 @@ def test_surrogate_output_conserves(small_fit):
     m = out.double() @ phi.T * vm.cw()
     scale = out.double().abs().sum(1, keepdim=True) * vm.cw() * 36.0
     assert bool((m.abs() < 1e-5 * scale).all())     # FP32 storage of FP64-projected rows
+
+
+def test_hybrid_overlap_equals_serial_and_replays(small_fit):
+    """The spectral launch on a side stream next to the surrogate GEMMs gives
+    the serial result bitwise, eagerly and replayed from a CUDA graph."""
+    be, vm, sm, q = small_fit
+    gen = torch.Generator(device=be.device).manual_seed(12)
+    f = sample_family(vm.c0(), 400, gen, be.device)
+    outs = []
+    for overlap in (False, True):
+        h = HybridCollider(q, threshold=0.05, recheck=0.2, overlap=overlap)
+        o = torch.empty_like(f)
+        h(f, o, seed=3)
+        outs.append(o)
+    torch.cuda.synchronize()
+    assert torch.equal(outs[0], outs[1])
+    h = HybridCollider(q, threshold=0.05, recheck=0.2, overlap=True)
+    o = torch.empty_like(f)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        h(f, o, seed=3)                    # warm-up: allocations and kernel attributes
+    torch.cuda.current_stream().wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        h(f, o, seed=3)
+    o.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(o, outs[0])
+    del g
