@@ -108,6 +108,21 @@ __device__ __forceinline__ void axpy_col(const T* __restrict__ col, const T (&s)
     }
 }
 
+// asynchronous global -> shared copies of one thread (Ampere-style
+// cp.async; BYTES 4, 8 or 16, both addresses aligned to BYTES)
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* sdst, const void* gsrc)
+{
+    const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(sdst));
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gsrc) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(sa), "l"(gsrc), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // u_f = M0 u.  Each CTA (128 threads) owns one element and a chunk of
 // velocities, each thread VB consecutive velocities per step.  When every
 // row of M0 is a unit vector (flux points on solution points, as with GLL
@@ -175,7 +190,7 @@ __global__ void __launch_bounds__(128) disu_kernel(const bdgfs_fr_eles el, const
 // is the solution-point row u[e][fsel[f]] (M0 rows are unit vectors, as with
 // GLL points), and a neighbour entry e'*NF + f' of nbr reads u[e'][fsel[f']].
 // out must not alias u then (other CTAs read u's face rows).
-template <typename T, int ND, int NU, int NF, int VB, bool GATHER = false>
+template <typename T, int ND, int NU, int NF, int VB, bool GATHER = false, int RING = 8>
 __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, const bdgfs_fr_walls wl,
                                                   const T* __restrict__ u, const T* __restrict__ uf,
                                                   const int32_t* __restrict__ fsel,
@@ -184,7 +199,8 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
 {
     constexpr int NUP = (NU + 3) / 4 * 4;
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* dT = reinterpret_cast<T*>(smraw);               // [ND*NU][NUP]  (M1 - M3 M2) transposed
+    // [RING][128][VB] row ring (see below), then the operators
+    T* dT = reinterpret_cast<T*>(smraw) + RING * 128 * VB;   // [ND*NU][NUP]  (M1 - M3 M2) transposed
     T* m3T = dT + ND * NU * NUP;                        // [NF][NUP]
     T* sm = m3T + NF * NUP;                             // [NU][ND][ND]
     T* rj = sm + NU * ND * ND;                          // [NU]
@@ -225,6 +241,49 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
     const T* uw = static_cast<const T*>(wl.uwall);
     const T* fw = static_cast<const T*>(wl.fw);
     const T* bcv = static_cast<const T*>(wl.bcv);
+    // Every row the thread reads in one velocity step, in order, goes through
+    // a per-thread ring of RING slots in shared memory, filled by cp.async
+    // RING - 1 rows ahead (no registers held for the prefetch):
+    //   k < NU              u_k (volume)
+    //   k < NU + 2 NF       face f = (k - NU) / 2: own value, then the
+    //                       neighbour's (or the wall Maxwellian's)
+    //   k < NU + 2 NF + 3 NU  combination row i: u_i, x1_i, x2_i
+    constexpr int NR = NU + 2 * NF + 3 * NU;
+    T* ring = reinterpret_cast<T*>(smraw) + size_t(threadIdx.x) * VB;   // slot r at ring + r*128*VB
+    auto lsrc = [&](int f, int64_t v0) -> const T* {
+        if constexpr (GATHER) return u + (e * NU + fs[f]) * nv + v0;
+        else return uf + (e * NF + f) * nv + v0;
+    };
+    auto rsrc = [&](int f, int64_t v0) -> const T* {
+        const int n = nb[f];
+        if (n < 0) return fw + int64_t(wl.bcid[-1 - n]) * nv + v0;
+        if constexpr (GATHER) {
+            const int en = n / NF;
+            if (en >= el.neles) return lsrc(f, v0);     // outside this state: no flux
+            return u + (int64_t(en) * NU + fs[n - en * NF]) * nv + v0;
+        } else {
+            return uf + int64_t(n) * nv + v0;
+        }
+    };
+    auto rowptr = [&](int k, int64_t v0) -> const T* {
+        if (k < NU) return u + (e * NU + k) * nv + v0;
+        k -= NU;
+        if (k < 2 * NF) return (k & 1) ? rsrc(k >> 1, v0) : lsrc(k >> 1, v0);
+        k -= 2 * NF;
+        const int i = k / 3, w = k - 3 * (k / 3);
+        const T* base = w == 0 ? u : (w == 1 ? (x1 ? x1 : u) : (x2 ? x2 : u));
+        return base + (e * NU + i) * nv + v0;
+    };
+    auto issue = [&](int k, int64_t v0) {
+        if (k < NR) cp_async<VB * sizeof(T)>(ring + size_t(k % RING) * 128 * VB, rowptr(k, v0));
+        cp_async_commit();
+    };
+    auto take = [&](int k) {
+        cp_async_wait<RING - 1>();
+        Vec<T, VB> r;
+        r.load(ring + size_t(k % RING) * 128 * VB);
+        return r;
+    };
     const int64_t v1 = (int64_t(blockIdx.x) + 1) * chunk < nv ? (int64_t(blockIdx.x) + 1) * chunk : nv;
     for (int64_t v0 = int64_t(blockIdx.x) * chunk + int64_t(threadIdx.x) * VB; v0 < v1;
          v0 += int64_t(blockDim.x) * VB) {
@@ -236,13 +295,13 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
         for (int q = 0; q < VB; ++q)
 #pragma unroll
             for (int i = 0; i < NU; ++i) R[q][i] = T(0);
+#pragma unroll
+        for (int k = 0; k < RING - 1; ++k) issue(k, v0);
         // volume: R += (M1 - M3 M2) F~,  F~[d][j] = (sum_k smats[j][d][k] c_k) u_j
-        Vec<T, VB> uj;
-        uj.load(u + (e * NU) * nv + v0);
 #pragma unroll 1
         for (int j = 0; j < NU; ++j) {
-            Vec<T, VB> un;                                  // prefetch u_{j+1}
-            if (j + 1 < NU) un.load(u + (e * NU + j + 1) * nv + v0);
+            issue(j + RING - 1, v0);
+            const Vec<T, VB> uj = take(j);
 #pragma unroll
             for (int d = 0; d < ND; ++d) {
                 T ft[VB];
@@ -255,36 +314,15 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
                 }
                 axpy_col<T, NU, NUP, VB>(dT + (d * NU + j) * NUP, ft, R);
             }
-            uj = un;
         }
         // surface: common normal flux at each face point, lifted by M3
-        // face values: ul and the neighbour's (or the wall Maxwellian's) row,
-        // prefetched one face ahead
-        auto lsrc = [&](int f) -> const T* {
-            if constexpr (GATHER) return u + (e * NU + fs[f]) * nv + v0;
-            else return uf + (e * NF + f) * nv + v0;
-        };
-        auto rsrc = [&](int f) -> const T* {
-            const int n = nb[f];
-            if (n < 0) return fw + int64_t(wl.bcid[-1 - n]) * nv + v0;
-            if constexpr (GATHER) {
-                const int en = n / NF;
-                if (en >= el.neles) return lsrc(f);     // outside this state: no flux
-                return u + (int64_t(en) * NU + fs[n - en * NF]) * nv + v0;
-            } else {
-                return uf + int64_t(n) * nv + v0;
-            }
-        };
-        Vec<T, VB> ulp, urp;
-        ulp.load(lsrc(0));
-        urp.load(rsrc(0));
 #pragma unroll 1
         for (int f = 0; f < NF; ++f) {
-            Vec<T, VB> ul = ulp, ur = urp;
-            if (f + 1 < NF) {
-                ulp.load(lsrc(f + 1));
-                urp.load(rsrc(f + 1));
-            }
+            const int k = NU + 2 * f;
+            issue(k + RING - 1, v0);
+            const Vec<T, VB> ul = take(k);
+            issue(k + RING, v0);
+            Vec<T, VB> ur = take(k + 1);
             const int n = nb[f];
             T nc[VB];
 #pragma unroll
@@ -313,20 +351,16 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
             }
             axpy_col<T, NU, NUP, VB>(m3T + f * NUP, fh, R);
         }
-        // combination rows u, x1, x2, loaded one row ahead
-        Vec<T, VB> u0n, y1n, y2n;
-        u0n.load(u + (e * NU) * nv + v0);
-        if (x1) y1n.load(x1 + (e * NU) * nv + v0);
-        if (x2) y2n.load(x2 + (e * NU) * nv + v0);
+        // combination rows u, x1, x2: out = a u + b L(u) + c1 x1 + c2 x2
 #pragma unroll
         for (int i = 0; i < NU; ++i) {
-            const int64_t idx = (e * NU + i) * nv + v0;
-            const Vec<T, VB> ui = u0n, y1 = y1n, y2 = y2n;
-            if (i + 1 < NU) {
-                u0n.load(u + idx + nv);
-                if (x1) y1n.load(x1 + idx + nv);
-                if (x2) y2n.load(x2 + idx + nv);
-            }
+            const int k = NU + 2 * NF + 3 * i;
+            issue(k + RING - 1, v0);
+            const Vec<T, VB> ui = take(k);
+            issue(k + RING, v0);
+            const Vec<T, VB> y1 = take(k + 1);
+            issue(k + RING + 1, v0);
+            const Vec<T, VB> y2 = take(k + 2);
             Vec<T, VB> o;
 #pragma unroll
             for (int q = 0; q < VB; ++q) o.v[q] = a * ui.v[q] + b * (-rj[i] * R[q][i]);
@@ -338,7 +372,7 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
 #pragma unroll
                 for (int q = 0; q < VB; ++q) o.v[q] += c2 * y2.v[q];
             }
-            o.store(out + idx);
+            o.store(out + (e * NU + i) * nv + v0);
         }
     }
 }
@@ -528,9 +562,11 @@ static int rhs_launch_vb(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl, cons
     const int64_t chunk = fr_chunk(el->nv, el->neles, VB);
     dim3 g;
     if (grid_v(el->nv, el->neles, chunk, &g) != BDGFS_OK) return BDGFS_EINVAL;
-    const size_t smem = sizeof(T) * ((ND * NU + NF) * NUP + NU * ND * ND + NU + NF * ND + NF)
+    constexpr int RING = 8;
+    const size_t smem = sizeof(T) * (size_t(RING) * 128 * VB + (ND * NU + NF) * NUP + NU * ND * ND + NU
+                                     + NF * ND + NF)
                         + sizeof(int) * 2 * NF + 16;
-    auto k = fsel ? rhs_kernel<T, ND, NU, NF, VB, true> : rhs_kernel<T, ND, NU, NF, VB, false>;
+    auto k = fsel ? rhs_kernel<T, ND, NU, NF, VB, true, RING> : rhs_kernel<T, ND, NU, NF, VB, false, RING>;
     if (smem > 48 * 1024 &&
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
         return BDGFS_ECUDA;
