@@ -1026,8 +1026,10 @@ uz = 0
     t_disu = timed(s._disu)
     t_bc = timed(s._update_bc) if s.walls.nwall else 0.0
     out = s._bank(1).clone()
-    t_rhs = timed(lambda: s._fused_rhs(a=0.5, b=2.5e-4, x1=x1, c1=2.5e-4, x2=x2, c2=0.5,
-                                       out=out))
+    from frfs_b200 import _lib as _lb
+    t_rhs = timed(lambda: _lb.lib().bdgfs_fr_rhs(
+        _lb.ref(s.ele.struct), _lb.ref(s.walls.struct), s._bank(0).data_ptr(), s._uf_rows.data_ptr(),
+        out.data_ptr(), 0.5, 2.5e-4, x1.data_ptr(), 2.5e-4, x2.data_ptr(), 0.5, _lb.stream_ptr()))
     E, U, F, nv = s.ele.neles, s.ele.nupts, s.ele.nfpts, s.vm.vsize()
     nbytes = 4 * nv * E * (4 * U + 2 * F)          # u, x1, x2 in + out; own and neighbour faces
     peak = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)),
@@ -1053,6 +1055,15 @@ uz = 0
                     'gather_rhs_frac_of_hbm': gbytes / (t_rg * 1e-3) / 1e9 / peak,
                     'stage_ms_disu_path': t_disu + t_bc + t_rhs,
                     'stage_ms_gather_path': t_bcg + t_rg})
+        if s.ele.tensor is not None:
+            # factored residual R = M1 F~ + M3 (F^n - M2 F~) on the gather path
+            t_rt = timed(lambda: L.bdgfs_fr_rhs_tensor(
+                _lib.ref(s.ele.struct), _lib.ref(s.walls.struct), _lib.ref(s.ele.tensor),
+                u.data_ptr(), None, out.data_ptr(), 0.5, 2.5e-4, x1.data_ptr(), 2.5e-4, x2.data_ptr(), 0.5,
+                _lib.stream_ptr()))
+            res.update({'tensor_rhs_ms': t_rt,
+                        'tensor_rhs_frac_of_hbm': gbytes / (t_rt * 1e-3) / 1e9 / peak,
+                        'stage_ms_tensor_path': t_bcg + t_rt})
     print(json.dumps(res))
 
 

@@ -19,7 +19,7 @@ EXPORTS = (
     'bdgfs_vhs_scratch_bytes', 'bdgfs_vhs_collide', 'bdgfs_vhs_tiles', 'bdgfs_fma_probe',
     'bdgfs_vhs_collide_static',
     'bdgfs_fr_disu', 'bdgfs_fr_bc_update', 'bdgfs_fr_rhs', 'bdgfs_fr_rhs_gather',
-    'bdgfs_fr_bc_update_gather',
+    'bdgfs_fr_bc_update_gather', 'bdgfs_fr_rhs_tensor',
     'bdgfs_moments', 'bdgfs_residual', 'bdgfs_status_check',
     'bdgfs_gemm', 'bdgfs_colsum', 'bdgfs_adamw', 'bdgfs_relmse',
     'bdgfs_hybrid_classify', 'bdgfs_hybrid_project', 'bdgfs_hybrid_scatter',
@@ -54,6 +54,11 @@ class FrEles(C.Structure):
                 ('smats', C.c_void_p), ('rcpdjac', C.c_void_p), ('pnorm', C.c_void_p),
                 ('magn', C.c_void_p), ('nbr', C.c_void_p), ('c0', C.c_void_p),
                 ('engine', C.c_int32), ('pad_', C.c_int32)]
+
+
+class FrTensor(C.Structure):
+    _fields_ = [('fsel', C.c_void_p), ('fdim', C.c_void_p), ('fsgn', C.c_void_p),
+                ('m1line', C.c_void_p), ('p', C.c_int32), ('pad_', C.c_int32)]
 
 
 class FrWall(C.Structure):
@@ -128,6 +133,7 @@ def lib():
             'bdgfs_fr_rhs': [vp, vp, vp, vp, vp, dbl, dbl, vp, dbl, vp, dbl, vp],
             'bdgfs_fr_rhs_gather': [vp, vp, vp, vp, vp, dbl, dbl, vp, dbl, vp, dbl, vp],
             'bdgfs_fr_bc_update_gather': [vp, vp, vp, vp, vp],
+            'bdgfs_fr_rhs_tensor': [vp, vp, vp, vp, vp, vp, dbl, dbl, vp, dbl, vp, dbl, vp],
             'bdgfs_moments': [vp, i64, i32, i32, vp, dbl, vp, vp],
             'bdgfs_residual': [vp, vp, i64, i32, vp, vp],
             'bdgfs_status_check': [vp, i64, i32, vp, vp],

@@ -190,10 +190,17 @@ __global__ void __launch_bounds__(128) disu_kernel(const bdgfs_fr_eles el, const
 // is the solution-point row u[e][fsel[f]] (M0 rows are unit vectors, as with
 // GLL points), and a neighbour entry e'*NF + f' of nbr reads u[e'][fsel[f']].
 // out must not alias u then (other CTAs read u's face rows).
-template <typename T, int ND, int NU, int NF, int VB, bool GATHER = false, int RING = 8>
+// TPP > 0 (tensor-product points, TPP per line, flux points on solution
+// points, own face value of f equal to u[e][fsel[f]]): the residual is
+// applied factored, R = M1 F~ + M3 (F^n - M2 F~), with M1 along its lines
+// (tp.m1line, TPP nonzeros per column at compile-time rows) and M2 a
+// selection (row f: tp.fsgn[f] at column tp.fdim[f]*NU + fsel[f]), instead of
+// the dense M1 - M3 M2.
+template <typename T, int ND, int NU, int NF, int VB, bool GATHER = false, int RING = 8, int TPP = 0>
 __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, const bdgfs_fr_walls wl,
                                                   const T* __restrict__ u, const T* __restrict__ uf,
                                                   const int32_t* __restrict__ fsel,
+                                                  const bdgfs_fr_tensor tp,
                                                   T* out, T a, T b, const T* x1, T c1, const T* x2,
                                                   T c2, int64_t chunk)
 {
@@ -206,8 +213,11 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
     T* rj = sm + NU * ND * ND;                          // [NU]
     T* pn = rj + NU;                                    // [NF][ND]
     T* mg = pn + NF * ND;                               // [NF]
-    int* nb = reinterpret_cast<int*>(mg + NF);          // [NF]
+    T* m1l = mg + NF;                                   // [ND][NU][4] (TPP)
+    T* fsg = m1l + (TPP ? ND * NU * 4 : 0);             // [NF] (TPP)
+    int* nb = reinterpret_cast<int*>(fsg + (TPP ? NF : 0));   // [NF]
     int* fs = nb + NF;                                  // [NF] (GATHER)
+    int* fdm = fs + NF;                                 // [NF] (TPP)
     const int64_t e = blockIdx.y;
     {
         for (int i = threadIdx.x; i < (ND * NU + NF) * NUP; i += blockDim.x) dT[i] = T(0);
@@ -232,7 +242,17 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
         for (int i = threadIdx.x; i < NF; i += blockDim.x) {
             mg[i] = gg[i];
             nb[i] = el.nbr[e * NF + i];
-            if constexpr (GATHER) fs[i] = fsel[i];
+            // table entries clamped into range (a malformed table gives wrong
+            // values, never an out-of-range access)
+            if constexpr (GATHER || TPP > 0) fs[i] = min(max(fsel[i], 0), NU - 1);
+            if constexpr (TPP > 0) {
+                fdm[i] = min(max(tp.fdim[i], 0), ND - 1);
+                fsg[i] = static_cast<const T*>(tp.fsgn)[i];
+            }
+        }
+        if constexpr (TPP > 0) {
+            const T* gl = static_cast<const T*>(tp.m1line);
+            for (int i = threadIdx.x; i < ND * NU * 4; i += blockDim.x) m1l[i] = gl[i];
         }
     }
     __syncthreads();
@@ -297,6 +317,34 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
             for (int i = 0; i < NU; ++i) R[q][i] = T(0);
 #pragma unroll
         for (int k = 0; k < RING - 1; ++k) issue(k, v0);
+        if constexpr (TPP > 0) {
+            // volume: R += M1 F~ along the lines of M1 (rows known at compile time)
+#pragma unroll
+            for (int j = 0; j < NU; ++j) {
+                issue(j + RING - 1, v0);
+                const Vec<T, VB> uj = take(j);
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    T ft[VB];
+#pragma unroll
+                    for (int q = 0; q < VB; ++q) {
+                        T al = T(0);
+#pragma unroll
+                        for (int k = 0; k < ND; ++k) al += sm[(j * ND + d) * ND + k] * c[q][k];
+                        ft[q] = al * uj.v[q];
+                    }
+                    const int st = d == 0 ? 1 : (d == 1 ? TPP : TPP * TPP);
+                    const int base = j - ((j / st) % TPP) * st;
+                    const T* w = m1l + (d * NU + j) * 4;
+#pragma unroll
+                    for (int t = 0; t < TPP; ++t) {
+                        const T wt = w[t];
+#pragma unroll
+                        for (int q = 0; q < VB; ++q) R[q][base + t * st] += wt * ft[q];
+                    }
+                }
+            }
+        } else {
         // volume: R += (M1 - M3 M2) F~,  F~[d][j] = (sum_k smats[j][d][k] c_k) u_j
 #pragma unroll 1
         for (int j = 0; j < NU; ++j) {
@@ -314,6 +362,7 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
                 }
                 axpy_col<T, NU, NUP, VB>(dT + (d * NU + j) * NUP, ft, R);
             }
+        }
         }
         // surface: common normal flux at each face point, lifted by M3
 #pragma unroll 1
@@ -348,6 +397,17 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
             for (int q = 0; q < VB; ++q) {
                 const T fn = T(0.5) * nc[q] * (ul.v[q] + ur.v[q]) + T(0.5) * fabs(nc[q]) * (ul.v[q] - ur.v[q]);
                 fh[q] = mg[f] * fn;
+            }
+            if constexpr (TPP > 0) {                         // F^n - M2 F~ (ul is u at fsel[f])
+                const int jf = fs[f], df = fdm[f];
+                const T sg = fsg[f];
+#pragma unroll
+                for (int q = 0; q < VB; ++q) {
+                    T al = T(0);
+#pragma unroll
+                    for (int k = 0; k < ND; ++k) al += sm[(jf * ND + df) * ND + k] * c[q][k];
+                    fh[q] -= sg * al * ul.v[q];
+                }
             }
             axpy_col<T, NU, NUP, VB>(m3T + f * NUP, fh, R);
         }
@@ -553,10 +613,11 @@ static int vec_width(int64_t nv, const void* const* ptrs, int n)
     return VB;
 }
 
-template <typename T, int ND, int NU, int NF, int VB>
+template <typename T, int ND, int NU, int NF, int VB, int TPP = 0>
 static int rhs_launch_vb(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl, const void* u,
-                         const void* uf, const int32_t* fsel, void* out, double a, double b,
-                         const void* x1, double c1, const void* x2, double c2, cudaStream_t st)
+                         const void* uf, const int32_t* fsel, const bdgfs_fr_tensor* tp, void* out,
+                         double a, double b, const void* x1, double c1, const void* x2, double c2,
+                         cudaStream_t st)
 {
     constexpr int NUP = (NU + 3) / 4 * 4;
     const int64_t chunk = fr_chunk(el->nv, el->neles, VB);
@@ -564,31 +625,35 @@ static int rhs_launch_vb(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl, cons
     if (grid_v(el->nv, el->neles, chunk, &g) != BDGFS_OK) return BDGFS_EINVAL;
     constexpr int RING = 8;
     const size_t smem = sizeof(T) * (size_t(RING) * 128 * VB + (ND * NU + NF) * NUP + NU * ND * ND + NU
-                                     + NF * ND + NF)
-                        + sizeof(int) * 2 * NF + 16;
-    auto k = fsel ? rhs_kernel<T, ND, NU, NF, VB, true, RING> : rhs_kernel<T, ND, NU, NF, VB, false, RING>;
+                                     + NF * ND + NF + (TPP ? ND * NU * 4 + NF : 0))
+                        + sizeof(int) * 3 * NF + 16;
+    auto k = TPP ? (uf ? rhs_kernel<T, ND, NU, NF, VB, false, RING, TPP>
+                       : rhs_kernel<T, ND, NU, NF, VB, true, RING, TPP>)
+                 : (fsel ? rhs_kernel<T, ND, NU, NF, VB, true, RING> : rhs_kernel<T, ND, NU, NF, VB, false, RING>);
     if (smem > 48 * 1024 &&
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
         return BDGFS_ECUDA;
     bdgfs_fr_walls w0{};
+    const bdgfs_fr_tensor t0{};
     k<<<g, 128, smem, st>>>(*el, wl ? *wl : w0, static_cast<const T*>(u), static_cast<const T*>(uf),
-                            fsel, static_cast<T*>(out), T(a), T(b), static_cast<const T*>(x1), T(c1),
-                            static_cast<const T*>(x2), T(c2), chunk);
+                            fsel, tp ? *tp : t0, static_cast<T*>(out), T(a), T(b),
+                            static_cast<const T*>(x1), T(c1), static_cast<const T*>(x2), T(c2), chunk);
     return cuda_status(cudaGetLastError());
 }
 
-template <typename T, int ND, int NU, int NF>
+template <typename T, int ND, int NU, int NF, int TPP = 0>
 static int rhs_launch(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl, const void* u,
-                      const void* uf, const int32_t* fsel, void* out, double a, double b,
-                      const void* x1, double c1, const void* x2, double c2, cudaStream_t st)
+                      const void* uf, const int32_t* fsel, const bdgfs_fr_tensor* tp, void* out,
+                      double a, double b, const void* x1, double c1, const void* x2, double c2,
+                      cudaStream_t st)
 {
     const void* ptrs[] = {u, uf, out, x1, x2, wl ? wl->fw : nullptr};
     // 4 velocities per thread for float (each operator column read from
     // shared memory feeds 4 x 4 FMAs; measured faster than 2 also for NU = 27)
     constexpr int VBW = sizeof(T) == 4 ? 4 : 2;
     if (vec_width<T>(el->nv, ptrs, 6) >= VBW)
-        return rhs_launch_vb<T, ND, NU, NF, VBW>(el, wl, u, uf, fsel, out, a, b, x1, c1, x2, c2, st);
-    return rhs_launch_vb<T, ND, NU, NF, 1>(el, wl, u, uf, fsel, out, a, b, x1, c1, x2, c2, st);
+        return rhs_launch_vb<T, ND, NU, NF, VBW, TPP>(el, wl, u, uf, fsel, tp, out, a, b, x1, c1, x2, c2, st);
+    return rhs_launch_vb<T, ND, NU, NF, 1, TPP>(el, wl, u, uf, fsel, tp, out, a, b, x1, c1, x2, c2, st);
 }
 
 template <typename T, int NU, int NF, int VB>
@@ -705,8 +770,8 @@ extern "C" int32_t bdgfs_fr_rhs(const bdgfs_fr_eles* el, const bdgfs_fr_walls* w
     }
 #define GO(D, U, F)                                                                          \
     if (el->ndims == D && el->nupts == U && el->nfpts == F)                                  \
-        return el->fp64 ? rhs_launch<double, D, U, F>(el, wl, u, uf, nullptr, out, a, b, x1, c1, x2, c2, st) \
-                        : rhs_launch<float, D, U, F>(el, wl, u, uf, nullptr, out, a, b, x1, c1, x2, c2, st);
+        return el->fp64 ? rhs_launch<double, D, U, F>(el, wl, u, uf, nullptr, nullptr, out, a, b, x1, c1, x2, c2, st) \
+                        : rhs_launch<float, D, U, F>(el, wl, u, uf, nullptr, nullptr, out, a, b, x1, c1, x2, c2, st);
     BDGFS_FR_SHAPES(GO)
 #undef GO
     return BDGFS_EUNSUPPORTED;
@@ -725,9 +790,30 @@ extern "C" int32_t bdgfs_fr_rhs_gather(const bdgfs_fr_eles* el, const bdgfs_fr_w
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 #define GO(D, U, F)                                                                          \
     if (el->ndims == D && el->nupts == U && el->nfpts == F)                                  \
-        return el->fp64 ? rhs_launch<double, D, U, F>(el, wl, u, nullptr, fsel, out, a, b, x1, c1, x2, c2, st) \
-                        : rhs_launch<float, D, U, F>(el, wl, u, nullptr, fsel, out, a, b, x1, c1, x2, c2, st);
+        return el->fp64 ? rhs_launch<double, D, U, F>(el, wl, u, nullptr, fsel, nullptr, out, a, b, x1, c1, x2, c2, st) \
+                        : rhs_launch<float, D, U, F>(el, wl, u, nullptr, fsel, nullptr, out, a, b, x1, c1, x2, c2, st);
     BDGFS_FR_SHAPES(GO)
+#undef GO
+    return BDGFS_EUNSUPPORTED;
+}
+
+extern "C" int32_t bdgfs_fr_rhs_tensor(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl,
+                                       const bdgfs_fr_tensor* tp, const void* u, const void* uf,
+                                       void* out, double a, double b, const void* x1, double c1,
+                                       const void* x2, double c2, void* stream)
+{
+    int rc = check_eles(el);
+    if (rc != BDGFS_OK) return rc;
+    if (!tp || !tp->fsel || !tp->fdim || !tp->fsgn || !tp->m1line || !u || !out || (!uf && out == u))
+        return BDGFS_EINVAL;
+    if (wl && wl->nwall > 0 && (!wl->bcid || !wl->uwall || !wl->fw || !wl->bcv))
+        return BDGFS_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+#define GO(D, U, F, P)                                                                        \
+    if (el->ndims == D && el->nupts == U && el->nfpts == F && tp->p == P)                     \
+        return el->fp64 ? rhs_launch<double, D, U, F, P>(el, wl, u, uf, tp->fsel, tp, out, a, b, x1, c1, x2, c2, st) \
+                        : rhs_launch<float, D, U, F, P>(el, wl, u, uf, tp->fsel, tp, out, a, b, x1, c1, x2, c2, st);
+    GO(2, 4, 8, 2) GO(2, 9, 12, 3) GO(2, 16, 16, 4) GO(3, 8, 24, 2) GO(3, 27, 54, 3)
 #undef GO
     return BDGFS_EUNSUPPORTED;
 }

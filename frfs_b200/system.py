@@ -45,6 +45,7 @@ class DGFSElements:
         # with GLL points): face values are rows of the state itself
         unit = np.all(np.count_nonzero(m0, axis=1) == 1) and np.all(m0.max(axis=1) == 1.0)
         self.fsel = (backend.const(np.argmax(m0, axis=1), dtype=torch.int32) if unit else None)
+        self.tensor = self._tensor_form(shp, m0, c) if unit else None
         self.dcorr = c(shp.opmat('M1 - M3*M2'))
         self.m3 = c(shp.opmat('M3'))
         self.smats = c(geo.smats)
@@ -60,6 +61,42 @@ class DGFSElements:
             smats=self.smats.data_ptr(), rcpdjac=self.rcpdjac.data_ptr(),
             pnorm=self.pnorm.data_ptr(), magn=self.magn.data_ptr(),
             nbr=self.nbr.data_ptr(), c0=self.c0.data_ptr())
+
+    def _tensor_form(self, shp, m0, c):
+        """bdgfs_fr_tensor of the shape when its solution points form a
+        tensor product (p per line, first reference coordinate fastest), M1
+        acts along the lines and M2 selects one column per flux point; else
+        None."""
+        nd, nu, nf = self.ndims, self.nupts, self.nfpts
+        p = int(round(nu ** (1.0 / nd)))
+        if p ** nd != nu or not 2 <= p <= 4:
+            return None
+        m1, m2 = np.asarray(shp.opmat('M1')), np.asarray(shp.opmat('M2'))
+        fsel = np.argmax(m0, axis=1)
+        line = np.zeros((nd, nu, 4))
+        for d in range(nd):
+            st = p ** d
+            for j in range(nu):
+                col = m1[:, d * nu + j].copy()
+                base = j - ((j // st) % p) * st
+                for t in range(p):
+                    line[d, j, t] = col[base + t * st]
+                    col[base + t * st] = 0.0
+                if np.any(col != 0.0):
+                    return None
+        fdim = np.zeros(nf, dtype=np.int32)
+        fsgn = np.zeros(nf)
+        for f in range(nf):
+            nz = np.flatnonzero(m2[f])
+            if len(nz) != 1 or nz[0] % nu != fsel[f]:
+                return None
+            fdim[f], fsgn[f] = nz[0] // nu, m2[f, nz[0]]
+        self.tp_fdim = self.be.const(fdim, dtype=torch.int32)
+        self.tp_fsgn = c(fsgn)
+        self.tp_m1line = c(line)
+        self.tp_fsel = self.be.const(fsel, dtype=torch.int32)
+        return _lib.FrTensor(fsel=self.tp_fsel.data_ptr(), fdim=self.tp_fdim.data_ptr(),
+                             fsgn=self.tp_fsgn.data_ptr(), m1line=self.tp_m1line.data_ptr(), p=p)
 
     def ploc_at_np(self, name):
         return {'upts': self.geo.plocupts, 'fpts': self.geo.plocfpts}[name]
@@ -187,11 +224,16 @@ class DGFSSystem:
         u = self._bank(self._active[0])
         out = self._bank(self._active[1]) if out is None else out
         L = _lib.lib()
+        xs = (float(a), float(b), x1.data_ptr() if x1 is not None else None, float(c1),
+              x2.data_ptr() if x2 is not None else None, float(c2), _lib.stream_ptr())
+        if self.ele.tensor is not None and self.ele.struct.engine == 0:
+            rc = L.bdgfs_fr_rhs_tensor(_lib.ref(self.ele.struct), _lib.ref(self.walls.struct),
+                                       _lib.ref(self.ele.tensor), u.data_ptr(),
+                                       self._uf_rows.data_ptr(), out.data_ptr(), *xs)
+            _lib.check(rc, 'bdgfs_fr_rhs_tensor')
+            return
         rc = L.bdgfs_fr_rhs(_lib.ref(self.ele.struct), _lib.ref(self.walls.struct),
-                            u.data_ptr(), self._uf_rows.data_ptr(), out.data_ptr(), float(a), float(b),
-                            x1.data_ptr() if x1 is not None else None, float(c1),
-                            x2.data_ptr() if x2 is not None else None, float(c2),
-                            _lib.stream_ptr())
+                            u.data_ptr(), self._uf_rows.data_ptr(), out.data_ptr(), *xs)
         _lib.check(rc, 'bdgfs_fr_rhs')
 
     # -- reference system methods ----------------------------------------
@@ -251,11 +293,19 @@ class DGFSSystem:
                                                        _lib.ref(self.walls.struct), fsel,
                                                        u.data_ptr(), _lib.stream_ptr()),
                            'bdgfs_fr_bc_update_gather')
-            _lib.check(L.bdgfs_fr_rhs_gather(_lib.ref(self.ele.struct), _lib.ref(self.walls.struct),
-                                             fsel, u.data_ptr(), out.data_ptr(), float(a), float(b),
-                                             x1.data_ptr() if x1 is not None else None, float(c1),
-                                             x2.data_ptr() if x2 is not None else None, float(c2),
-                                             _lib.stream_ptr()), 'bdgfs_fr_rhs_gather')
+            xs = (x1.data_ptr() if x1 is not None else None, float(c1),
+                  x2.data_ptr() if x2 is not None else None, float(c2), _lib.stream_ptr())
+            if self.ele.tensor is not None:
+                _lib.check(L.bdgfs_fr_rhs_tensor(_lib.ref(self.ele.struct),
+                                                 _lib.ref(self.walls.struct),
+                                                 _lib.ref(self.ele.tensor), u.data_ptr(), None,
+                                                 out.data_ptr(), float(a), float(b), *xs),
+                           'bdgfs_fr_rhs_tensor')
+            else:
+                _lib.check(L.bdgfs_fr_rhs_gather(_lib.ref(self.ele.struct),
+                                                 _lib.ref(self.walls.struct), fsel, u.data_ptr(),
+                                                 out.data_ptr(), float(a), float(b), *xs),
+                           'bdgfs_fr_rhs_gather')
             return
         self._exchange()
         if self.walls.nwall:

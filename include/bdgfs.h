@@ -195,6 +195,32 @@ int32_t bdgfs_fr_bc_update_gather(const bdgfs_fr_eles* el,
                                   const int32_t* fsel, const void* u,
                                   void* stream);
 
+/* Tensor-product points (nupts = p^ndims, point index fastest in the first
+ * reference coordinate) with flux points on solution points: the residual
+ * factored as R = M1 F~ + M3 (F^n - M2 F~) instead of the dense
+ * (M1 - M3 M2) F~ + M3 F^n of the shape's operators. */
+typedef struct bdgfs_fr_tensor {
+    const int32_t* fsel;  /* [nfpts] solution point of flux point f (M0's 1)  */
+    const int32_t* fdim;  /* [nfpts] reference direction d of M2's only
+                             nonzero in row f, at column d*nupts + fsel[f]   */
+    const void* fsgn;     /* real [nfpts] that nonzero                       */
+    const void* m1line;   /* real [ndims][nupts][4]: M1 on the d-line through
+                             point j: M1[j + (t - j_d) p^d][d*nupts + j] for
+                             t < p (j_d the d-th coordinate index of j), 0
+                             for p <= t < 4; every other entry of M1 is 0    */
+    int32_t p;            /* points per line, 2..4                           */
+    int32_t pad_;
+} bdgfs_fr_tensor;
+
+/* bdgfs_fr_rhs (uf = the face values of bdgfs_fr_disu) or, with uf NULL,
+ * bdgfs_fr_rhs_gather (out must not alias u then), with the factored
+ * residual: equal to rounding, and bitwise the same with or without uf. */
+int32_t bdgfs_fr_rhs_tensor(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl,
+                            const bdgfs_fr_tensor* tp, const void* u,
+                            const void* uf, void* out, double a, double b,
+                            const void* x1, double c1, const void* x2,
+                            double c2, void* stream);
+
 /* FP64 raw velocity moments of ndof distributions, out[ndof][13]:
  * cw*sum{f, c f (3), c_i c_j f (xx xy xz yy yz zz), |c|^2 c f (3)}.
  * Feeds the macroscopic fields of plugins/dgfsmomwriterstd.py:14-313. */

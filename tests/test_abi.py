@@ -34,6 +34,7 @@ STRUCTS = {
     'bdgfs_vhs_batch': _lib.VhsBatch,
     'bdgfs_fr_eles': _lib.FrEles,
     'bdgfs_fr_walls': _lib.FrWall,
+    'bdgfs_fr_tensor': _lib.FrTensor,
     'bdgfs_gemm_args': _lib.GemmArgs,
     'bdgfs_hybrid_args': _lib.HybridArgs,
     'bdgfs_ars_args': _lib.ArsArgs,

@@ -204,10 +204,11 @@ def test_gather_rhs_equals_disu_rhs(cuda, kind, order, prec):
     s.updatebc(0.0, 0, 1)
     bc_ref = s.walls.bcv.clone()
     ref = torch.empty_like(u)
-    s._active = (0, 1)
-    s._fused_rhs(a=0.5, b=2.0, x1=x1, c1=0.25, x2=x2, c2=-0.5, out=ref)
-    s.walls.bcv.zero_()
     L, fsel = _lib.lib(), s.ele.fsel.data_ptr()
+    _lib.check(L.bdgfs_fr_rhs(_lib.ref(s.ele.struct), _lib.ref(s.walls.struct), u.data_ptr(),
+                              s._uf_rows.data_ptr(), ref.data_ptr(), 0.5, 2.0, x1.data_ptr(), 0.25,
+                              x2.data_ptr(), -0.5, _lib.stream_ptr()), 'rhs')
+    s.walls.bcv.zero_()
     _lib.check(L.bdgfs_fr_bc_update_gather(_lib.ref(s.ele.struct), _lib.ref(s.walls.struct), fsel,
                                            u.data_ptr(), _lib.stream_ptr()), 'bc_update_gather')
     out = torch.empty_like(u)
@@ -238,3 +239,43 @@ def test_stepper_gather_path_equals_disu_path(cuda):
         torch.cuda.synchronize()
         outs.append(s.eles_scal_upts_inb_full[0].clone())
     assert torch.equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize('kind,order,prec,tol', [('quad', 3, 'single', 2e-6), ('hex', 2, 'single', 2e-6),
+                                                 ('hex', 2, 'double', 1e-13), ('quad', 2, 'double', 1e-13)])
+def test_tensor_factored_rhs_matches_dense(cuda, kind, order, prec, tol):
+    """The factored residual R = M1 F~ + M3 (F^n - M2 F~) of
+    bdgfs_fr_rhs_tensor against bdgfs_fr_rhs_gather (dense M1 - M3 M2):
+    equal to rounding, with walls and the RK combination operands."""
+    from frfs_b200 import _lib
+    cfg, be, mesh, s = _system(kind, order, prec)
+    assert s.ele.tensor is not None
+    _perturb(s, 13)
+    u = s.eles_scal_upts_inb_full[0]
+    x1, x2 = u * 1.5, u * 0.5
+    s.updatebc(0.0, 0, 1)
+    L, fsel = _lib.lib(), s.ele.fsel.data_ptr()
+    outs = []
+    for tensor in (False, True):
+        o = torch.empty_like(u)
+        args = (u.data_ptr(), o.data_ptr(), 0.5, 2.0, x1.data_ptr(), 0.25, x2.data_ptr(), -0.5,
+                _lib.stream_ptr())
+        if tensor:
+            rc = L.bdgfs_fr_rhs_tensor(_lib.ref(s.ele.struct), _lib.ref(s.walls.struct),
+                                       _lib.ref(s.ele.tensor), args[0], None, *args[1:])
+        else:
+            rc = L.bdgfs_fr_rhs_gather(_lib.ref(s.ele.struct), _lib.ref(s.walls.struct), fsel, *args)
+        _lib.check(rc, 'rhs')
+        outs.append(o)
+    o = torch.empty_like(u)
+    s._disu()
+    _lib.check(L.bdgfs_fr_rhs_tensor(_lib.ref(s.ele.struct), _lib.ref(s.walls.struct),
+                                     _lib.ref(s.ele.tensor), u.data_ptr(), s._uf_rows.data_ptr(),
+                                     o.data_ptr(), 0.5, 2.0, x1.data_ptr(), 0.25, x2.data_ptr(), -0.5,
+                                     _lib.stream_ptr()), 'rhs_tensor_face_array')
+    torch.cuda.synchronize()
+    assert torch.equal(o, outs[1])          # face array or gather: the same arithmetic
+    # the residual part only: out - (a u + c1 x1 + c2 x2) = b L(u)
+    base = 0.5 * u + 0.25 * x1 - 0.5 * x2
+    la, lb = (outs[0] - base).double(), (outs[1] - base).double()
+    assert float((la - lb).norm() / la.norm()) < tol
