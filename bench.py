@@ -567,6 +567,82 @@ def ars_bgk(flush, steps=20):
                              'frac': ach / peak, 'bound': 'hbm'}}
 
 
+def cavity_ini():
+    """Config 5's .ini (8^3 hex P2, lid 0.5 at T=1, diffuse walls) and the
+    mesh boundary names."""
+    import numpy as np
+    u0 = np.sqrt(2 * 8.3144598 / NONDIM['molarMass0'] * NONDIM['T0'])
+    ini = couette_ini('single', dict(WORK, order=2)).split('[soln-bcs-y-]')[0]
+    ini += f"""
+[soln-bcs-lid]
+type = dgfs-wall-diffuse
+rho = {NONDIM['rho0']}
+T = {NONDIM['T0']}
+ux = {0.5 * u0}
+uy = 0
+uz = 0
+[soln-bcs-walls]
+type = dgfs-wall-diffuse
+rho = {NONDIM['rho0']}
+T = {NONDIM['T0']}
+ux = 0
+uy = 0
+uz = 0
+"""
+    names = {'x-': 'walls', 'x+': 'walls', 'y-': 'walls', 'y+': 'lid', 'z-': 'walls',
+             'z+': 'walls'}
+    return ini, names
+
+
+def run_hybrid_steps(nsteps, nwarm=3):
+    """Profiling case: SSP-RK2 steps of the lid-driven cavity with the
+    hybrid collision operator, the surrogate randomly initialised with its
+    head scales at zero (Q = 0 on surrogate cells; the kernels, shapes and
+    cell counts of the hybrid step; timing only)."""
+    import torch
+    from frfs_b200.backend import CUDABackend
+    from frfs_b200.inifile import Inifile
+    from frfs_b200.integrators import get_integrator
+    from frfs_b200.mesh import StructuredMesh
+    from frfs_b200.surrogate import HybridCollider, QSurrogate
+    from frfs_b200.system import DGFSSystem
+    ini, names = cavity_ini()
+    cfg = Inifile(ini)
+    cfg.set('solver-time-integrator', 'dt', '2e-4')
+    be = CUDABackend(cfg)
+    mesh = StructuredMesh((8, 8, 8), (0, 0, 0), (1, 1, 1), periodic='', bcnames=names)
+    s5 = DGFSSystem(be, mesh, cfg, nreg=3)
+    q = QSurrogate(s5.sm.grid, nmodes=512, width=1024)
+    dev = be.device
+    g = torch.Generator(device=dev).manual_seed(0)
+    n = q.n
+    q.Bd = torch.linalg.qr(torch.randn(n, 512, device=dev, generator=g))[0].t().contiguous()
+    q.Bq = torch.linalg.qr(torch.randn(n, 1536, device=dev, generator=g))[0].t().contiguous()
+    q.mu = torch.zeros(512, device=dev)
+    q.sigma = torch.full((512,), 0.05, device=dev)
+    q.hscale = torch.zeros(3, device=dev)
+    q._init_params(g)
+    q._fold()
+    hc = HybridCollider(q, threshold=0.05, recheck=0.02)
+    n3 = s5.vm.vsize()
+    s5.sm.collide = lambda fin, fout, **kw: hc(fin.reshape(-1, n3), fout.reshape(-1, n3))
+    integ = get_integrator(be, s5, cfg)
+    for _ in range(nwarm):
+        integ.step(0.0, 2e-4)
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(nsteps):
+        integ.step(0.0, 2e-4)
+    b.record(st)
+    torch.cuda.synchronize()
+    stt = hc.stats()
+    print(json.dumps({'hybrid_steps': nsteps, 'ms_per_step': a.elapsed_time(b) / nsteps,
+                      'spectral_cells_per_call': stt['spectral_cells'],
+                      'surrogate_cells_per_call': stt['surrogate_cells']}))
+
+
 def surrogate_legs(flush, log=None):
     """Config 4 (surrogate trained on the Couette family, evaluated on 50000
     held-out seeded distributions) and config 5 (8^3 hex P2 lid-driven
@@ -635,27 +711,7 @@ def surrogate_legs(flush, log=None):
           'surrogate_q_evals_per_s': 8192 / (t_sur * 1e-3),
           'spectral_q_evals_per_s': 8192 / (t_spec * 1e-3)}
     # ---- config 5: lid-driven cavity
-    import numpy as np
-    u0 = np.sqrt(2 * 8.3144598 / NONDIM['molarMass0'] * NONDIM['T0'])
-    ini = couette_ini('single', dict(WORK, order=2)).split('[soln-bcs-y-]')[0]
-    ini += f"""
-[soln-bcs-lid]
-type = dgfs-wall-diffuse
-rho = {NONDIM['rho0']}
-T = {NONDIM['T0']}
-ux = {0.5 * u0}
-uy = 0
-uz = 0
-[soln-bcs-walls]
-type = dgfs-wall-diffuse
-rho = {NONDIM['rho0']}
-T = {NONDIM['T0']}
-ux = 0
-uy = 0
-uz = 0
-"""
-    names = {'x-': 'walls', 'x+': 'walls', 'y-': 'walls', 'y+': 'lid', 'z-': 'walls',
-             'z+': 'walls'}
+    ini, names = cavity_ini()
     # surrogate for the cavity's near-equilibrium cells (CAVITY family)
     t0 = time.time()
     qc = QSurrogate(sm.grid, nmodes=512, width=1024, family=CAVITY)
@@ -1092,6 +1148,9 @@ def main():
     ap.add_argument('--q-batched', type=int, default=0, metavar='NDOF24',
                     help='profiling case: the two-species collision launch on NDOF24 24^3 and '
                          'NDOF24/3 32^3 cubes')
+    ap.add_argument('--hybrid-steps', type=int, default=0, metavar='N',
+                    help='profiling case: N hybrid SSP-RK2 steps of the lid-driven cavity '
+                         '(random surrogate with zero head scales)')
     ap.add_argument('--ars-only', action='store_true',
                     help='profiling case: the adgfs ARS-222 leg alone')
     ap.add_argument('--fr-only', choices=['couette', 'cavity'],
@@ -1101,6 +1160,8 @@ def main():
         run_q_only(args.q_only)
     elif args.surrogate_call:
         run_surrogate_call(args.surrogate_call)
+    elif args.hybrid_steps:
+        run_hybrid_steps(args.hybrid_steps)
     elif args.q_batched:
         import torch
         flush = torch.empty(256 << 20, dtype=torch.uint8, device='cuda')
