@@ -548,16 +548,23 @@ class HybridCollider:
     spectral elsewhere, spectral re-check of a seeded ``recheck`` fraction of
     the surrogate cells (their spectral result is kept)."""
 
-    def __init__(self, model, threshold=0.05, recheck=0.02, project=True, overlap=True):
+    def __init__(self, model, threshold=0.05, recheck=0.02, project=True, overlap=True,
+                 recheck_every=1):
         """overlap: run the spectral launch on a side stream next to the
         surrogate GEMMs (the GEMMs fill the SMs the persistent spectral
-        launch leaves idle in its last round); joined before the scatter."""
+        launch leaves idle in its last round); joined before the scatter.
+        recheck_every: re-check the ``recheck`` fraction on one call out of
+        this many (2 with SSP-RK2 re-checks once per time step: the first of
+        its two collide calls; under CUDA-graph capture the pattern is the
+        one captured)."""
         from .scattering import VHSCollider
         self.model = model
         self.grid = model.grid
         self.threshold, self.recheck, self.project = float(threshold), float(recheck), project
         self.spectral = VHSCollider([self.grid], model.device)
         self.overlap = overlap
+        self.recheck_every = max(1, int(recheck_every))
+        self._calls = 0
         self._side = None
         self._n = 0
         self._net = None
@@ -575,6 +582,7 @@ class HybridCollider:
             self.flag = torch.zeros(ndof, dtype=torch.uint8, device=dev)
             self.eps = torch.zeros(ndof, device=dev)
             self.recheck_err = torch.zeros(2, dtype=torch.float64, device=dev)
+            self.rc_counts = torch.zeros(3, dtype=torch.int64, device=dev)
             self.seed_dev = torch.zeros(1, dtype=torch.int64, device=dev)
             self.dev_rows = torch.zeros(ndof, n, device=dev, dtype=torch.bfloat16)
             self._n = ndof
@@ -591,27 +599,30 @@ class HybridCollider:
             self.Qc = torch.empty(ndof, m.n, device=dev, dtype=self.grid.dtype)
             self._net = shape
 
-    def _args(self, ndof, seed):
+    def _args(self, ndof, seed, recheck=None):
         """seed None: the re-check sample follows a device step counter
-        (advanced every call, also under CUDA-graph replay)."""
+        (advanced every call, also under CUDA-graph replay).  recheck: this
+        call's re-check fraction (default ``self.recheck``); with 0 the
+        re-check error of the last re-checking call is kept."""
         g, m = self.grid, self.model
+        rc = self.recheck if recheck is None else recheck
         feat = self.xc.data_ptr() + 2 * (m.w + m.k)          # columns [w+k, w+k+4) of xc
         return _lib.HybridArgs(
             ndof=ndof, Nv=g.Nv, fp64=int(g.dtype == torch.float64), c0=g.c0.data_ptr(),
-            ginv=g.ginv.data_ptr(), cw=g.cw, threshold=self.threshold, recheck=self.recheck,
+            ginv=g.ginv.data_ptr(), cw=g.cw, threshold=self.threshold, recheck=rc,
             seed=int(seed or 0), counts=self.counts.data_ptr(), sur_idx=self.sur_idx.data_ptr(),
             sur_inv_rho=self.inv_rho.data_ptr(), sur_rho2=self.rho2.data_ptr(),
             spec_idx=self.spec_idx.data_ptr(), flag=self.flag.data_ptr(),
-            eps=self.eps.data_ptr(), recheck_err=self.recheck_err.data_ptr(),
+            eps=self.eps.data_ptr(), recheck_err=self.recheck_err.data_ptr() if rc > 0 else 0,
             seed_dev=self.seed_dev.data_ptr() if seed is None else 0,
             dev_rows=self.dev_rows.data_ptr(), feat=feat, feat_ld=m.ldx,
             sur_s=self.sur_s.data_ptr())
 
-    def classify(self, fin, seed=None):
+    def classify(self, fin, seed=None, recheck=None):
         f2 = fin.reshape(-1, self.model.n)
         ndof = f2.shape[0]
         self._alloc(ndof)
-        self.args = self._args(ndof, seed)
+        self.args = self._args(ndof, seed, recheck)
         _lib.check(_lib.lib().bdgfs_hybrid_classify(C.byref(self.args), f2.data_ptr(),
                                                     _lib.stream_ptr()), 'bdgfs_hybrid_classify')
         return ndof
@@ -620,7 +631,11 @@ class HybridCollider:
         """Q for every distribution of fin [ndof][n] into fout."""
         n = self.model.n
         f2, q2 = fin.reshape(-1, n), fout.reshape(-1, n)
-        ndof = self.classify(f2, seed)
+        rc = self.recheck if self._calls % self.recheck_every == 0 else 0.0
+        self._calls += 1
+        ndof = self.classify(f2, seed, rc)
+        if rc > 0:
+            self.rc_counts.copy_(self.counts)          # counts of the last re-checking call
         L = _lib.lib()
         # spectral cells (incl. re-checks): index list + device count; the
         # surrogate rows (compact GEMMs) meanwhile on the main stream
@@ -653,7 +668,10 @@ class HybridCollider:
             self.threshold, self.recheck = saved
 
     def stats(self):
+        """Counts of the last call; re-checked cells and the re-check error
+        of the last call that re-checked."""
         c = self.counts.cpu().tolist()
+        r = self.rc_counts.cpu().tolist()
         e = self.recheck_err.cpu().tolist()
-        return {'surrogate_cells': c[0], 'spectral_cells': c[1], 'rechecked_cells': c[2],
+        return {'surrogate_cells': c[0], 'spectral_cells': c[1], 'rechecked_cells': r[2],
                 'recheck_rel_l2': math.sqrt(e[0] / e[1]) if e[1] > 0 else None}

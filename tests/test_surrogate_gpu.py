@@ -259,3 +259,28 @@ def test_hybrid_overlap_equals_serial_and_replays(small_fit):
     torch.cuda.synchronize()
     assert torch.equal(o, outs[0])
     del g
+
+
+def test_hybrid_recheck_every_second_call(small_fit):
+    """recheck_every=2: the first call re-checks (spectral result kept), the
+    second does not; the re-check statistics of the first call persist."""
+    be, vm, sm, q = small_fit
+    gen = torch.Generator(device=be.device).manual_seed(13)
+    f = sample_family(vm.c0(), 200, gen, be.device)
+    plain = torch.empty_like(f)
+    sm.collide(f, plain, project=True, exact=False)
+    sur_only = torch.empty_like(f)
+    HybridCollider(q, threshold=float('inf'), recheck=0.0)(f, sur_only)
+    h = HybridCollider(q, threshold=float('inf'), recheck=1.0, recheck_every=2)
+    o1, o2, o3 = torch.empty_like(f), torch.empty_like(f), torch.empty_like(f)
+    h(f, o1)
+    st1 = h.stats()
+    h(f, o2)
+    st2 = h.stats()
+    h(f, o3)
+    torch.cuda.synchronize()
+    assert torch.equal(o1, plain) and torch.equal(o3, plain)
+    assert torch.equal(o2, sur_only)
+    assert st1['rechecked_cells'] == 200 and st2['rechecked_cells'] == 200
+    assert st2['spectral_cells'] == 0
+    assert st2['recheck_rel_l2'] == st1['recheck_rel_l2']
