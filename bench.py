@@ -936,8 +936,11 @@ def run_gpu(args):
         c4, c5 = surrogate_legs(flush)
         extra['surrogate'] = c4
         extra['hybrid_lid_cavity'] = c5
-    # gpu launches per step: 2 x (collide + disu + bc_update + rhs)
-    launches = 8 * args.steps
+    # gpu launches per step: 2 stages x (collide [+ disu] [+ bc_update] + rhs); the
+    # one-part GLL system reads face values from the state (no disu)
+    gathers = system.ele.fsel is not None and system.domain is None
+    per_stage = 2 + (0 if gathers else 1) + (1 if system.walls.nwall else 0)
+    launches = 2 * per_stage * args.steps
     line = {
         'metric': METRIC, 'value': value, 'unit': 'DG steps/s', 'n_gpus': ws,
         'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms_per_step,
