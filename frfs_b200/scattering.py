@@ -230,7 +230,11 @@ class DGFSVHSGLLHybridScatteringModel(DGFSVHSGLLScatteringModel):
       surrogate-threshold  Maxwellian deviation below which the surrogate
                            is used (default 0.05)
       surrogate-recheck    fraction of surrogate cells re-checked by the
-                           spectral operator every call (default 0.02)
+                           spectral operator (default 0.02)
+      surrogate-recheck-every
+                           re-check on one collide call out of this many
+                           (default 1, every call; 2 with dgfs-tvd-rk2
+                           re-checks once per time step)
       surrogate-file       trained model to load (torch.save of state_dict);
                            trained and saved there when absent
       surrogate-family     training distributions: 'couette' (default) or
@@ -267,6 +271,7 @@ class DGFSVHSGLLHybridScatteringModel(DGFSVHSGLLScatteringModel):
         self.hybrid = HybridCollider(self.surrogate,
                                      threshold=cfg.getfloat(sect, 'surrogate-threshold', 0.05),
                                      recheck=cfg.getfloat(sect, 'surrogate-recheck', 0.02),
+                                     recheck_every=cfg.getint(sect, 'surrogate-recheck-every', 1),
                                      project=self._project)
 
     def collide(self, fin, fout, moments=None, project=None, exact=None):
