@@ -25,6 +25,7 @@ EXPORTS = (
     'bdgfs_hybrid_classify', 'bdgfs_hybrid_project', 'bdgfs_hybrid_scatter',
     'bdgfs_hybrid_project_scatter', 'bdgfs_hybrid_heads',
     'bdgfs_bgk_moments', 'bdgfs_bgk_maxwellian', 'bdgfs_ars_stage',
+    'bdgfs_esbgk_moments', 'bdgfs_esbgk_gaussian',
 )
 
 
@@ -99,7 +100,8 @@ class ArsArgs(C.Structure):
                 ('stage', C.c_int32), ('flags', C.c_int32),
                 ('ae', C.c_double * 4), ('ai', C.c_double * 4),
                 ('f', C.c_void_p * 4), ('fout', C.c_void_p), ('L', C.c_void_p * 4),
-                ('U', C.c_void_p * 5), ('LU', C.c_void_p * 4)]
+                ('U', C.c_void_p * 5), ('LU', C.c_void_p * 4),
+                ('model', C.c_int32), ('pad_', C.c_int32), ('Pr', C.c_double)]
 
 
 _lib = None
@@ -147,6 +149,8 @@ def lib():
             'bdgfs_bgk_moments': [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_double, vp, vp],
             'bdgfs_bgk_maxwellian': [vp, C.c_int64, C.c_int32, C.c_int32, vp, vp, vp],
             'bdgfs_ars_stage': [vp, vp],
+            'bdgfs_esbgk_moments': [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_double, vp, vp],
+            'bdgfs_esbgk_gaussian': [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_double, vp, vp],
             'bdgfs_colsum': [vp, i64, i64, vp, vp],
             'bdgfs_adamw': [vp, vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float,
                             C.c_float, C.c_float, i64, vp],

@@ -7,8 +7,10 @@ frfs/solvers/adgfs/scattering.py (ADGFSBGKDirectGLLScatteringModel,
 names (``moment``, ``constructMaxwellian``, ``updateMomentARS``,
 ``updateDistARS``, ``get_nregs_moms``) on top of the fused stage entry
 ``bdgfs_ars_stage`` that the project's ARS steppers use.  Moment rows are
-FP64 ``[ndof][5]`` = (rho, rho u, E) as in the reference
-(nalph = 5).
+FP64 ``[ndof][nalph]``: (rho, rho u, E) for BGK (nalph = 5) and, for
+ES-BGK (ADGFSESBGKDirectGLLScatteringModel, 'esbgk-direct-gll'), those
+followed by the raw second moments (xx, yy, zz, xy, yz, zx) (nalph = 11),
+as in the reference.
 """
 import ctypes as C
 
@@ -77,6 +79,8 @@ class ADGFSBGKDirectGLLScatteringModel(ADGFSScatteringModel):
                                                    self.fp64, self.c0.data_ptr(), M.data_ptr(),
                                                    _lib.stream_ptr()), 'bdgfs_bgk_maxwellian')
 
+    ars_model = 0          # BDGFS_ARS_BGK
+
     def ars_stage(self, ndof, dt, ar, flags, ae, ai, f, fout, L, U, LU):
         """One fused ARS stage (bdgfs_ars_stage) over ndof distributions;
         f, L, U, LU are lists of tensors (None where the flags do not need
@@ -85,7 +89,7 @@ class ADGFSBGKDirectGLLScatteringModel(ADGFSScatteringModel):
         a = _lib.ArsArgs(ndof=int(ndof),
                          Nv=self.vm.Nv(), fp64=self.fp64, c0=self.c0.data_ptr(), cw=self.cw,
                          prefac=self._prefactor, omega=self._omega, dt=float(dt), stage=ar,
-                         flags=flags)
+                         flags=flags, model=self.ars_model, Pr=self._Pr)
         for j, x in enumerate(ae):
             a.ae[j] = x
         for j, x in enumerate(ai):
@@ -102,6 +106,41 @@ class ADGFSBGKDirectGLLScatteringModel(ADGFSScatteringModel):
         _lib.check(_lib.lib().bdgfs_ars_stage(C.byref(a), _lib.stream_ptr()), 'bdgfs_ars_stage')
 
 
+class ADGFSESBGKDirectGLLScatteringModel(ADGFSBGKDirectGLLScatteringModel):
+    """ES-BGK relaxation nu (G[f] - f) towards the anisotropic Gaussian of
+    the ES tensor T_ij = T/Pr d_ij + 2 (1 - 1/Pr)(P_ij/rho - u_i u_j),
+    nu = prefac rho T^(1 - omega), prefac = t0 Pr p0 / visc, Pr from the
+    .ini (default 2/3) (scattering.py: ADGFSESBGKDirectGLLScatteringModel;
+    kernels/scattering/esbgk-direct-gll.mako)."""
+    scattering_model = 'esbgk-direct-gll'
+    nalph = 11
+    ars_model = 1          # BDGFS_ARS_ESBGK
+
+    def load_parameters(self):
+        super().load_parameters()
+        Pr = self.cfg.getfloat('scattering-model', 'Pr', 2.0 / 3.0)
+        if not Pr > 0:
+            raise ValueError('scattering-model: Pr must be positive')
+        self._prefactor *= Pr
+        self._Pr = Pr
+
+    def moment(self, f, U):
+        """U[dof] <- the 11 moments of f[dof] (FP64)."""
+        n = self.vm.vsize()
+        _lib.check(_lib.lib().bdgfs_esbgk_moments(f.data_ptr(), f.numel() // n, self.vm.Nv(),
+                                                  self.fp64, self.c0.data_ptr(), self.cw,
+                                                  U.data_ptr(), _lib.stream_ptr()),
+                   'bdgfs_esbgk_moments')
+
+    def constructMaxwellian(self, U, M):
+        """M[dof] <- the ES Gaussian of U[dof] (momentNorm + cmaxwellian)."""
+        n = self.vm.vsize()
+        _lib.check(_lib.lib().bdgfs_esbgk_gaussian(U.data_ptr(), M.numel() // n, self.vm.Nv(),
+                                                   self.fp64, self.c0.data_ptr(), self._Pr,
+                                                   M.data_ptr(), _lib.stream_ptr()),
+                   'bdgfs_esbgk_gaussian')
+
+
 class ADGFSSystem(DGFSSystem):
     """'adgfs' (system.py:17-121): FR advection plus BGK relaxation."""
     name = 'adgfs'
@@ -116,7 +155,7 @@ class ADGFSSystem(DGFSSystem):
         return self.ele.neles * self.ele.nupts
 
     def get_nregs_moms(self, nreg_moms):
-        """Moment banks [ndof][5] FP64 (system.py:31-52)."""
+        """Moment banks [ndof][nalph] FP64 (system.py:31-52)."""
         if self.nreg_moms is not None and self.nreg_moms != nreg_moms:
             raise RuntimeError('moment registers already allocated with another count')
         if self.nreg_moms is None:

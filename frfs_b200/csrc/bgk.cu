@@ -12,6 +12,13 @@
 // stage reduces the moments (FP64), forms the stage moments and updates f,
 // with each Maxwellian built on the fly from separable exponential tables
 // (3 Nv exponentials per Maxwellian instead of Nv^3).
+//
+// ES-BGK ('esbgk-direct-gll': ADGFSESBGKDirectGLLScatteringModel, kernels
+// momentNorm / cmaxwellian / updateMom{q}_ARS of esbgk-direct-gll.mako)
+// uses 11 moment rows (the five conserved ones and the six raw second
+// moments cx^2, cy^2, cz^2, cx cy, cy cz, cz cx) and relaxes to the
+// anisotropic Gaussian of the ES tensor; the Gaussian is not separable and
+// is evaluated per velocity.
 #include "common.cuh"
 #include "rows.cuh"
 
@@ -28,6 +35,111 @@ __device__ __forceinline__ void row_state(const double (&U)[5], double& rho, dou
     uy = U[2] / U[0];
     uz = U[3] / U[0];
     T = (U[4] - (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / U[0]) / (1.5 * U[0]);
+}
+
+// FP64 moments {1, c, |c|^2, cx^2, cy^2, cz^2, cx cy, cy cz, cz cx} . f of a
+// row (block-wide partial sums per thread)
+template <typename T, int VEC>
+__device__ __forceinline__ void row_moments11(const T* __restrict__ row, int n, int Nv, const double* cs,
+                                              double (&m)[11])
+{
+    for (int v = threadIdx.x * VEC; v < n; v += blockDim.x * VEC) {
+        Chunk<T, VEC> c;
+        c.load(row + v);
+        uint32_t ix, iy, iz;
+        vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
+        const double cx = cs[ix], cy = cs[iy];
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) {
+            const double x = double(c.v[j]), cz = cs[iz + j];
+            m[0] += x;
+            m[1] += cx * x;
+            m[2] += cy * x;
+            m[3] += cz * x;
+            m[4] += (cx * cx + cy * cy + cz * cz) * x;
+            m[5] += cx * cx * x;
+            m[6] += cy * cy * x;
+            m[7] += cz * cz * x;
+            m[8] += cx * cy * x;
+            m[9] += cy * cz * x;
+            m[10] += cz * cx * x;
+        }
+    }
+}
+
+// ES Gaussian of an 11-moment row: G(c) = g[0] exp(-q(c - u)), u = g[1..3],
+// q(d) = g[4] dx^2 + g[5] dy^2 + g[6] dz^2 + g[7] dx dy + g[8] dy dz + g[9] dz dx
+// (the inverse of T_ij = T/Pr delta_ij + 2 (1 - 1/Pr)(P_ij/rho - u_i u_j)).
+__device__ __forceinline__ void es_params(const double* U, double Pr, double (&g)[10])
+{
+    const double rho = U[0], ux = U[1] / rho, uy = U[2] / rho, uz = U[3] / rho;
+    const double T = (U[4] - rho * (ux * ux + uy * uy + uz * uz)) / (1.5 * rho);
+    const double k = 2.0 * (1.0 - 1.0 / Pr);
+    const double txx = T / Pr + k * (U[5] / rho - ux * ux);
+    const double tyy = T / Pr + k * (U[6] / rho - uy * uy);
+    const double tzz = T / Pr + k * (U[7] / rho - uz * uz);
+    const double txy = k * (U[8] / rho - ux * uy);
+    const double tyz = k * (U[9] / rho - uy * uz);
+    const double tzx = k * (U[10] / rho - uz * ux);
+    const double det = txx * (tyy * tzz - tyz * tyz) - txy * (txy * tzz - tyz * tzx)
+                       + tzx * (txy * tyz - tyy * tzx);
+    const double id = 1.0 / det;
+    g[0] = rho / (pow(kPi, 1.5) * sqrt(det));
+    g[1] = ux;
+    g[2] = uy;
+    g[3] = uz;
+    g[4] = (tyy * tzz - tyz * tyz) * id;
+    g[5] = (txx * tzz - tzx * tzx) * id;
+    g[6] = (txx * tyy - txy * txy) * id;
+    g[7] = 2.0 * (tyz * tzx - tzz * txy) * id;
+    g[8] = 2.0 * (txy * tzx - txx * tyz) * id;
+    g[9] = 2.0 * (txy * tyz - tzx * tyy) * id;
+}
+
+__device__ __forceinline__ double es_eval(const double* g, double cx, double cy, double cz)
+{
+    const double dx = cx - g[1], dy = cy - g[2], dz = cz - g[3];
+    const double q = g[4] * dx * dx + g[5] * dy * dy + g[6] * dz * dz + g[7] * dx * dy + g[8] * dy * dz
+                     + g[9] * dz * dx;
+    return g[0] * exp(-q);
+}
+
+template <typename T, int VEC>
+__global__ void __launch_bounds__(256) esbgk_moments_kernel(const T* __restrict__ f, int Nv, const double* c0,
+                                                            double cw, double* __restrict__ U)
+{
+    __shared__ double red[11 * 8];
+    __shared__ double cs[kMaxNv];
+    const int64_t dof = blockIdx.x;
+    const int n = Nv * Nv * Nv;
+    for (int i = threadIdx.x; i < Nv; i += blockDim.x) cs[i] = c0[i];
+    __syncthreads();
+    double m[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    row_moments11<T, VEC>(f + dof * int64_t(n), n, Nv, cs, m);
+    block_sum<11>(m, red);
+    if (threadIdx.x < 11) U[dof * 11 + threadIdx.x] = m[threadIdx.x] * cw;
+}
+
+template <typename T, int VEC>
+__global__ void __launch_bounds__(256) esbgk_gaussian_kernel(const double* __restrict__ U, int Nv,
+                                                             const double* c0, double Pr, T* __restrict__ M)
+{
+    __shared__ double cs[kMaxNv];
+    const int64_t dof = blockIdx.x;
+    const int n = Nv * Nv * Nv;
+    for (int i = threadIdx.x; i < Nv; i += blockDim.x) cs[i] = c0[i];
+    double g[10];
+    es_params(U + dof * 11, Pr, g);
+    __syncthreads();
+    T* row = M + dof * int64_t(n);
+    for (int v = threadIdx.x * VEC; v < n; v += blockDim.x * VEC) {
+        uint32_t ix, iy, iz;
+        vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
+        Chunk<T, VEC> c;
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) c.v[j] = T(es_eval(g, cs[ix], cs[iy], cs[iz + j]));
+        c.store(row + v);
+    }
 }
 
 template <typename T, int VEC>
@@ -77,12 +189,15 @@ __global__ void __launch_bounds__(256) bgk_maxwellian_kernel(const double* __res
     }
 }
 
-template <typename T, int VEC>
+// NA = 5: BGK (separable Maxwellians); NA = 11: ES-BGK (second moments
+// relaxed implicitly at nu/Pr, Gaussians evaluated per velocity).
+template <typename T, int VEC, int NA>
 __global__ void __launch_bounds__(256) ars_kernel(const bdgfs_ars_args g)
 {
-    __shared__ double red[5 * 8];
+    __shared__ double red[NA * 8];
     __shared__ double cs[kMaxNv];
-    __shared__ double ex[4][3][kMaxNv];
+    __shared__ double ex[NA == 5 ? 4 : 1][3][kMaxNv];
+    __shared__ double gp[NA == 11 ? 4 : 1][10];
     __shared__ double am[4], nu[4];
     const int64_t dof = blockIdx.x;
     const int Nv = g.Nv, ar = g.stage, flags = g.flags;
@@ -91,65 +206,121 @@ __global__ void __launch_bounds__(256) ars_kernel(const bdgfs_ars_args g)
     for (int i = threadIdx.x; i < Nv; i += blockDim.x) cs[i] = g.c0[i];
     __syncthreads();
 
-    double U0[5], LUl[5], Uar[5];
+    auto moments = [&](const T* row, double (&m)[NA]) {
+#pragma unroll
+        for (int i = 0; i < NA; ++i) m[i] = 0.0;
+        if constexpr (NA == 5) {
+            row_moments<T, VEC>(row, n, Nv, cs, m);
+        } else {
+            row_moments11<T, VEC>(row, n, Nv, cs, m);
+        }
+        block_sum<NA>(m, red);
+#pragma unroll
+        for (int i = 0; i < NA; ++i) m[i] *= g.cw;
+    };
+    // temperature-dependent relaxation rate of a moment row (conserved part)
+    auto rate = [&](const double* u) {
+        double rho, ux, uy, uz, Tt;
+        double u5[5] = {u[0], u[1], u[2], u[3], u[4]};
+        row_state(u5, rho, ux, uy, uz, Tt);
+        return g.prefac * rho * pow(Tt, 1.0 - g.omega);
+    };
+
+    double U0[NA], LUl[NA], Uar[NA];
     // ---- moments of f_0 (updateMom / moment)
     if (flags & BDGFS_ARS_MOM0) {
-        double m[5] = {0, 0, 0, 0, 0};
-        row_moments<T, VEC>(static_cast<const T*>(g.f[0]) + off, n, Nv, cs, m);
-        block_sum<5>(m, red);
-#pragma unroll
-        for (int i = 0; i < 5; ++i) U0[i] = m[i] * g.cw;
+        moments(static_cast<const T*>(g.f[0]) + off, U0);
         if (threadIdx.x == 0)
-            for (int i = 0; i < 5; ++i) g.U[0][dof * 5 + i] = U0[i];
+            for (int i = 0; i < NA; ++i) g.U[0][dof * NA + i] = U0[i];
     } else if (flags & BDGFS_ARS_MOMU) {
 #pragma unroll
-        for (int i = 0; i < 5; ++i) U0[i] = g.U[0][dof * 5 + i];
+        for (int i = 0; i < NA; ++i) U0[i] = g.U[0][dof * NA + i];
     }
     // ---- moments of the newest explicit part L_{ar-1}
     if (flags & BDGFS_ARS_MOML) {
-        double m[5] = {0, 0, 0, 0, 0};
-        row_moments<T, VEC>(static_cast<const T*>(g.L[ar - 1]) + off, n, Nv, cs, m);
-        block_sum<5>(m, red);
-#pragma unroll
-        for (int i = 0; i < 5; ++i) LUl[i] = m[i] * g.cw;
+        moments(static_cast<const T*>(g.L[ar - 1]) + off, LUl);
         if (threadIdx.x == 0)
-            for (int i = 0; i < 5; ++i) g.LU[ar - 1][dof * 5 + i] = LUl[i];
+            for (int i = 0; i < NA; ++i) g.LU[ar - 1][dof * NA + i] = LUl[i];
     }
-    // ---- stage moments U_ar = U_0 + dt sum_j ae_j LU_j (BGK conserves them)
+    // ---- stage moments: U_ar = U_0 + dt sum_j ae_j LU_j for the conserved
+    // five (BGK conserves them); ES-BGK's second moments relax implicitly
     if (flags & BDGFS_ARS_MOMU) {
 #pragma unroll
-        for (int i = 0; i < 5; ++i) {
+        for (int i = 0; i < NA; ++i) {
             double s = U0[i];
             for (int j = 0; j < ar; ++j) {
-                const double lu = (j == ar - 1 && (flags & BDGFS_ARS_MOML)) ? LUl[i] : g.LU[j][dof * 5 + i];
+                const double lu = (j == ar - 1 && (flags & BDGFS_ARS_MOML)) ? LUl[i] : g.LU[j][dof * NA + i];
                 s += g.dt * g.ae[j] * lu;
             }
             Uar[i] = s;
         }
+        if constexpr (NA == 11) {
+            // targets: the Maxwellian's second moments rho T/2 + rho u_i^2, rho u_i u_j
+            auto targets = [&](const double* u, double (&t)[6]) {
+                double rho, ux, uy, uz, Tt;
+                double u5[5] = {u[0], u[1], u[2], u[3], u[4]};
+                row_state(u5, rho, ux, uy, uz, Tt);
+                t[0] = 0.5 * rho * Tt + rho * ux * ux;
+                t[1] = 0.5 * rho * Tt + rho * uy * uy;
+                t[2] = 0.5 * rho * Tt + rho * uz * uz;
+                t[3] = rho * ux * uy;
+                t[4] = rho * uy * uz;
+                t[5] = rho * uz * ux;
+            };
+            double num[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) num[k] = Uar[5 + k];
+            for (int j = 1; j < ar; ++j) {
+                double uj[11], t[6];
+#pragma unroll
+                for (int i = 0; i < 11; ++i) uj[i] = g.U[j][dof * 11 + i];
+                targets(uj, t);
+                const double w = g.ai[j - 1] * g.dt * rate(uj) / g.Pr;
+#pragma unroll
+                for (int k = 0; k < 6; ++k) num[k] += w * (t[k] - uj[5 + k]);
+            }
+            double t[6];
+            targets(Uar, t);
+            const double w = g.ai[ar - 1] * g.dt * rate(Uar) / g.Pr;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) Uar[5 + k] = (num[k] + w * t[k]) / (1.0 + w);
+        }
         if (threadIdx.x == 0)
-            for (int i = 0; i < 5; ++i) g.U[ar][dof * 5 + i] = Uar[i];
+            for (int i = 0; i < NA; ++i) g.U[ar][dof * NA + i] = Uar[i];
     }
     if (!(flags & BDGFS_ARS_DIST)) return;
 
-    // ---- Maxwellians M_1..M_ar and collision frequencies of U_1..U_ar
+    // ---- relaxation targets M_1..M_ar (Maxwellians or ES Gaussians) and
+    // collision frequencies of U_1..U_ar
     for (int j = 1; j <= ar; ++j) {
-        double u[5];
+        double u[NA];
 #pragma unroll
-        for (int i = 0; i < 5; ++i) u[i] = (j == ar && (flags & BDGFS_ARS_MOMU)) ? Uar[i] : g.U[j][dof * 5 + i];
-        double rho, ux, uy, uz, Tt;
-        row_state(u, rho, ux, uy, uz, Tt);
-        if (threadIdx.x == 0) {
-            am[j - 1] = rho / pow(kPi * Tt, 1.5);
-            nu[j - 1] = g.prefac * rho * pow(Tt, 1.0 - g.omega);
-        }
-        const double it = 1.0 / Tt;
-        for (int i = threadIdx.x; i < 3 * Nv; i += blockDim.x) {
-            const int d = i / Nv, k = i - d * Nv;
-            const double c = cs[k] - (d == 0 ? ux : d == 1 ? uy : uz);
-            ex[j - 1][d][k] = exp(-c * c * it);
+        for (int i = 0; i < NA; ++i) u[i] = (j == ar && (flags & BDGFS_ARS_MOMU)) ? Uar[i] : g.U[j][dof * NA + i];
+        if (threadIdx.x == 0) nu[j - 1] = rate(u);
+        if constexpr (NA == 5) {
+            double rho, ux, uy, uz, Tt;
+            row_state(u, rho, ux, uy, uz, Tt);
+            if (threadIdx.x == 0) am[j - 1] = rho / pow(kPi * Tt, 1.5);
+            const double it = 1.0 / Tt;
+            for (int i = threadIdx.x; i < 3 * Nv; i += blockDim.x) {
+                const int d = i / Nv, k = i - d * Nv;
+                const double c = cs[k] - (d == 0 ? ux : d == 1 ? uy : uz);
+                ex[j - 1][d][k] = exp(-c * c * it);
+            }
+        } else {
+            if (threadIdx.x == 0) {
+                double gj[10];
+                es_params(u, g.Pr, gj);
+#pragma unroll
+                for (int i = 0; i < 10; ++i) gp[j - 1][i] = gj[i];
+            }
         }
     }
     __syncthreads();
+    auto target = [&](int j, uint32_t ix, uint32_t iy, uint32_t izq) -> double {
+        if constexpr (NA == 5) return am[j] * ex[j][0][ix] * ex[j][1][iy] * ex[j][2][izq];
+        else return es_eval(gp[j], cs[ix], cs[iy], cs[izq]);
+    };
     const double dt = g.dt;
     const double aii = g.ai[ar - 1] * dt * nu[ar - 1];
     const double inv = 1.0 / (1.0 + aii);
@@ -170,14 +341,12 @@ __global__ void __launch_bounds__(256) ars_kernel(const bdgfs_ars_args g)
         for (int j = 1; j < ar; ++j) {
             c.load(static_cast<const T*>(g.f[j]) + off + v);
             const double w = g.ai[j - 1] * dt * nu[j - 1];
-            const double axy = am[j - 1] * ex[j - 1][0][ix] * ex[j - 1][1][iy];
 #pragma unroll
-            for (int q = 0; q < VEC; ++q) acc[q] += w * (axy * ex[j - 1][2][iz + q] - double(c.v[q]));
+            for (int q = 0; q < VEC; ++q) acc[q] += w * (target(j - 1, ix, iy, iz + q) - double(c.v[q]));
         }
-        const double axy = am[ar - 1] * ex[ar - 1][0][ix] * ex[ar - 1][1][iy];
         Chunk<T, VEC> o;
 #pragma unroll
-        for (int q = 0; q < VEC; ++q) o.v[q] = T((acc[q] + aii * axy * ex[ar - 1][2][iz + q]) * inv);
+        for (int q = 0; q < VEC; ++q) o.v[q] = T((acc[q] + aii * target(ar - 1, ix, iy, iz + q)) * inv);
         o.store(static_cast<T*>(g.fout) + off + v);
     }
 }
@@ -233,7 +402,9 @@ extern "C" int32_t bdgfs_bgk_maxwellian(const double* U, int64_t ndof, int32_t N
 extern "C" int32_t bdgfs_ars_stage(const bdgfs_ars_args* a, void* stream)
 {
     if (!a || !a->c0 || a->ndof < 0 || a->ndof > 2147483647LL || a->Nv < 1 || a->Nv > kMaxNv ||
-        a->stage < 1 || a->stage > 4 || (a->flags & ~15))
+        a->stage < 1 || a->stage > 4 || (a->flags & ~15) ||
+        (a->model != BDGFS_ARS_BGK && a->model != BDGFS_ARS_ESBGK) ||
+        (a->model == BDGFS_ARS_ESBGK && !(a->Pr > 0.0)))
         return BDGFS_EINVAL;
     const int ar = a->stage, fl = a->flags;
     bool ok = true, v4 = a->Nv % 4 == 0;
@@ -256,6 +427,39 @@ extern "C" int32_t bdgfs_ars_stage(const bdgfs_ars_args* a, void* stream)
     }
     if (a->ndof == 0) return BDGFS_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (a->fp64) return launch_rows(v4, ars_kernel<double, 4>, ars_kernel<double, 1>, a->ndof, st, *a);
-    return launch_rows(v4, ars_kernel<float, 4>, ars_kernel<float, 1>, a->ndof, st, *a);
+    if (a->model == BDGFS_ARS_ESBGK) {
+        if (a->fp64) return launch_rows(v4, ars_kernel<double, 4, 11>, ars_kernel<double, 1, 11>, a->ndof, st, *a);
+        return launch_rows(v4, ars_kernel<float, 4, 11>, ars_kernel<float, 1, 11>, a->ndof, st, *a);
+    }
+    if (a->fp64) return launch_rows(v4, ars_kernel<double, 4, 5>, ars_kernel<double, 1, 5>, a->ndof, st, *a);
+    return launch_rows(v4, ars_kernel<float, 4, 5>, ars_kernel<float, 1, 5>, a->ndof, st, *a);
+}
+
+extern "C" int32_t bdgfs_esbgk_moments(const void* f, int64_t ndof, int32_t Nv, int32_t fp64,
+                                       const double* c0, double cw, double* U, void* stream)
+{
+    if (!f || !c0 || !U || ndof < 0 || ndof > 2147483647LL || Nv < 1 || Nv > kMaxNv) return BDGFS_EINVAL;
+    if (ndof == 0) return BDGFS_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool v4 = Nv % 4 == 0 && a16(f);
+    if (fp64)
+        return launch_rows(v4, esbgk_moments_kernel<double, 4>, esbgk_moments_kernel<double, 1>, ndof, st,
+                           static_cast<const double*>(f), int(Nv), c0, cw, U);
+    return launch_rows(v4, esbgk_moments_kernel<float, 4>, esbgk_moments_kernel<float, 1>, ndof, st,
+                       static_cast<const float*>(f), int(Nv), c0, cw, U);
+}
+
+extern "C" int32_t bdgfs_esbgk_gaussian(const double* U, int64_t ndof, int32_t Nv, int32_t fp64,
+                                        const double* c0, double Pr, void* M, void* stream)
+{
+    if (!U || !c0 || !M || ndof < 0 || ndof > 2147483647LL || Nv < 1 || Nv > kMaxNv || !(Pr > 0.0))
+        return BDGFS_EINVAL;
+    if (ndof == 0) return BDGFS_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool v4 = Nv % 4 == 0 && a16(M);
+    if (fp64)
+        return launch_rows(v4, esbgk_gaussian_kernel<double, 4>, esbgk_gaussian_kernel<double, 1>, ndof, st, U,
+                           int(Nv), c0, Pr, static_cast<double*>(M));
+    return launch_rows(v4, esbgk_gaussian_kernel<float, 4>, esbgk_gaussian_kernel<float, 1>, ndof, st, U,
+                       int(Nv), c0, Pr, static_cast<float*>(M));
 }

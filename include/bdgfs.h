@@ -383,9 +383,16 @@ typedef struct bdgfs_ars_args {
     const void* f[4];        /* f_0 .. f_{ar-1}                             */
     void* fout;              /* f_ar (may be f_0: updated in place)         */
     const void* L[4];        /* L_0 .. L_{ar-1} (explicit FR parts)          */
-    double* U[5];            /* moment rows U_0 .. U_ar                     */
+    double* U[5];            /* moment rows U_0 .. U_ar (5 or 11 per row)   */
     double* LU[4];           /* moment rows of L_0 .. L_{ar-1}              */
+    int32_t model;           /* BDGFS_ARS_BGK (5 moments, Maxwellian) or
+                                BDGFS_ARS_ESBGK (11 moments, ES Gaussian)   */
+    int32_t pad_;
+    double Pr;               /* Prandtl number (ES-BGK)                     */
 } bdgfs_ars_args;
+
+#define BDGFS_ARS_BGK 0
+#define BDGFS_ARS_ESBGK 1
 
 /* U[dof] = moments of f[dof]: ADGFSBGKDirectGLLScatteringModel.moment. */
 int32_t bdgfs_bgk_moments(const void* f, int64_t ndof, int32_t Nv, int32_t fp64,
@@ -394,6 +401,17 @@ int32_t bdgfs_bgk_moments(const void* f, int64_t ndof, int32_t Nv, int32_t fp64,
 int32_t bdgfs_bgk_maxwellian(const double* U, int64_t ndof, int32_t Nv,
                              int32_t fp64, const double* c0, void* M,
                              void* stream);
+/* ES-BGK ('esbgk-direct-gll', frfs/solvers/adgfs/scattering.py,
+ * ADGFSESBGKDirectGLLScatteringModel): U[dof][11] = moments of f[dof]
+ * {1, c, |c|^2, cx^2, cy^2, cz^2, cx cy, cy cz, cz cx} cw (the moment
+ * method), and M[dof] = the Gaussian of the ES tensor of U[dof]
+ * (momentNorm + cmaxwellian, esbgk-direct-gll.mako:4-120). */
+int32_t bdgfs_esbgk_moments(const void* f, int64_t ndof, int32_t Nv,
+                            int32_t fp64, const double* c0, double cw,
+                            double* U, void* stream);
+int32_t bdgfs_esbgk_gaussian(const double* U, int64_t ndof, int32_t Nv,
+                             int32_t fp64, const double* c0, double Pr,
+                             void* M, void* stream);
 /* One ARS stage (the flagged parts, in the order MOM0, MOML, MOMU, DIST):
  * updateMom{ar}_ARS + cmaxwellian + updateDistribution{ar}_ARS in one
  * launch, the Maxwellians computed on the fly. */

@@ -90,3 +90,97 @@ def step_ars(f0, dt, L, scheme, prefac, omega, cv, cw):
         num = num + A[ar][ar] * dt * nar * maxwellian(U[ar], cv)
         F.append(num / (1.0 + A[ar][ar] * dt * nar))
     return F[s]
+
+
+# ---------------------------------------------------------------------------
+# ES-BGK ('esbgk-direct-gll', frfs/solvers/adgfs/scattering.py,
+# ADGFSESBGKDirectGLLScatteringModel; kernels/scattering/esbgk-direct-gll.mako)
+#   moments     11: (sum f, sum c f, sum |c|^2 f, sum cx^2 f, sum cy^2 f,
+#               sum cz^2 f, sum cx cy f, sum cy cz f, sum cz cx f) cw
+#   prefactor   t0 Pr p0 / visc (nu = prefac rho T^(1-omega) as for BGK)
+#   Gaussian    (momentNorm, cmaxwellian) T_ii = T/Pr + 2 (1 - 1/Pr)
+#               (P_ii/rho - u_i^2), T_ij = 2 (1 - 1/Pr)(P_ij/rho - u_i u_j),
+#               G = rho / (pi^1.5 sqrt(det T)) exp(-(c-u)^T T^-1 (c-u))
+#   ARS moments (updateMom{ar}_ARS): the conserved five as for BGK; the six
+#               second moments relax implicitly at rate nu/Pr to the
+#               Maxwellian's (rho T/2 + rho u_i^2, rho u_i u_j).
+
+def esbgk_prefactor(H0, u0, T0, n0, omega, muRef, Tref, Pr):
+    return Pr * bgk_prefactor(H0, u0, T0, n0, omega, muRef, Tref)
+
+
+def moments11(f, cv, cw):
+    c2 = np.sum(cv * cv, axis=0)
+    cx, cy, cz = cv
+    rows = [np.ones_like(cx), cx, cy, cz, c2, cx * cx, cy * cy, cz * cz, cx * cy, cy * cz, cz * cx]
+    return np.stack([f @ r for r in rows], axis=-1) * cw
+
+
+def es_tensor(U, Pr):
+    """(rho, u[3], T, Tij[3x3]) of 11-moment rows."""
+    rho, u, T = _state(U)
+    k = 2.0 * (1.0 - 1.0 / Pr)
+    P = np.empty(U.shape[:-1] + (3, 3))
+    P[..., 0, 0], P[..., 1, 1], P[..., 2, 2] = U[..., 5], U[..., 6], U[..., 7]
+    P[..., 0, 1] = P[..., 1, 0] = U[..., 8]
+    P[..., 1, 2] = P[..., 2, 1] = U[..., 9]
+    P[..., 2, 0] = P[..., 0, 2] = U[..., 10]
+    Tij = k * (P / rho[..., None, None] - u[..., :, None] * u[..., None, :])
+    Tij = Tij + (T / Pr)[..., None, None] * np.eye(3)
+    return rho, u, T, Tij
+
+
+def es_gaussian(U, Pr, cv):
+    rho, u, T, Tij = es_tensor(U, Pr)
+    lead = U.shape[:-1]
+    flat = lambda a, s: a.reshape((-1,) + s)
+    rho_, u_, Tij_ = flat(rho, ()), flat(u, (3,)), flat(Tij, (3, 3))
+    out = np.empty((rho_.shape[0], cv.shape[1]))
+    for i in range(rho_.shape[0]):
+        d = cv - u_[i][:, None]
+        Ti = np.linalg.inv(Tij_[i])
+        q = np.einsum('av,ab,bv->v', d, Ti, d)
+        out[i] = rho_[i] / (np.pi**1.5 * np.sqrt(np.linalg.det(Tij_[i]))) * np.exp(-q)
+    return out.reshape(lead + (cv.shape[1],))
+
+
+def _es_targets(U):
+    """Second moments of the Maxwellian of U: rho T/2 + rho u_i^2, rho u_i u_j."""
+    rho, u, T = _state(U)
+    t = np.empty(U.shape[:-1] + (6,))
+    for k in range(3):
+        t[..., k] = 0.5 * rho * T + rho * u[..., k]**2
+    t[..., 3] = rho * u[..., 0] * u[..., 1]
+    t[..., 4] = rho * u[..., 1] * u[..., 2]
+    t[..., 5] = rho * u[..., 2] * u[..., 0]
+    return t
+
+
+def step_ars_es(f0, dt, L, scheme, prefac, omega, Pr, cv, cw):
+    """One ARS step of df/dt = L(f) + nu (G[f] - f) (ES-BGK)."""
+    _A, A = ARS[scheme]
+    s = len(_A) - 1
+    F, Ls, LU = [f0], [], []
+    U = [moments11(f0, cv, cw)]
+    for i in range(s):
+        ar = i + 1
+        Ls.append(L(F[i]))
+        LU.append(moments11(Ls[i], cv, cw))
+        Ua = U[0] + dt * sum(_A[ar][j] * LU[j] for j in range(ar))
+        # second moments: implicit relaxation at nu/Pr towards the Maxwellian's
+        rate = lambda Uj: nu(Uj, prefac, omega) / Pr
+        num = Ua[..., 5:].copy()
+        for j in range(1, ar):
+            num += A[ar][j] * dt * rate(U[j])[..., None] * (_es_targets(U[j]) - U[j][..., 5:])
+        ra = rate(Ua)[..., None]
+        num += A[ar][ar] * dt * ra * _es_targets(Ua)
+        Ua[..., 5:] = num / (1.0 + A[ar][ar] * dt * ra)
+        U.append(Ua)
+        num = F[0] + sum(_A[ar][j] * dt * Ls[j] for j in range(ar))
+        for j in range(1, ar):
+            num = num + A[ar][j] * dt * nu(U[j], prefac, omega)[..., None] * (
+                es_gaussian(U[j], Pr, cv) - F[j])
+        nar = nu(U[ar], prefac, omega)[..., None]
+        num = num + A[ar][ar] * dt * nar * es_gaussian(U[ar], Pr, cv)
+        F.append(num / (1.0 + A[ar][ar] * dt * nar))
+    return F[s]

@@ -61,3 +61,60 @@ def test_ars_tables_consistent():
         assert np.allclose(c_e, c_i), name          # same stage times
         assert np.isclose(Ae[-1].sum(), 1.0) and np.isclose(Ai[-1].sum(), 1.0)
     assert nu(np.array([1.0, 0, 0, 0, 1.5]), 2.0, 0.81) == pytest.approx(2.0)
+
+
+# ---------------------------------------------------------------------------
+# ES-BGK ('esbgk-direct-gll')
+
+def test_es_gaussian_is_maxwellian_at_pr_one_and_for_maxwellians():
+    from oracle.bgk import es_gaussian, es_tensor, moments11
+    cv, cw = _grid(16, 6.0)
+    f = _f0(cv, 2)[None]
+    U = moments11(f, cv, cw)
+    assert np.allclose(es_gaussian(U, 1.0, cv), maxwellian(U[..., :5], cv), rtol=1e-12, atol=0)
+    # a Maxwellian's ES tensor is T I for every Pr
+    M = maxwellian(U[..., :5], cv)
+    _, _, T, Tij = es_tensor(moments11(M, cv, cw), 2.0 / 3.0)
+    assert np.allclose(Tij[0], T[0] * np.eye(3), atol=1e-6)
+
+
+def test_esbgk_moments_follow_the_stage_moments():
+    """With L = 0, ARS-111: the 11 moments of f_1 equal the stage moments U_1
+    (second moments relaxed at nu/Pr) up to the grid's quadrature error, and
+    the deviatoric stress decays by 1/(1 + dt nu/Pr)."""
+    from oracle.bgk import _es_targets, moments11, step_ars_es
+    cv, cw = _grid(16, 6.0)
+    f = _f0(cv, 3)[None]
+    Pr, prefac, omega, dt = 2.0 / 3.0, 2.0, 0.81, 0.3
+    U0 = moments11(f, cv, cw)
+    f1 = step_ars_es(f, dt, lambda g: 0 * g, 'adgfs-ars-111', prefac, omega, Pr, cv, cw)
+    U1 = moments11(f1, cv, cw)
+    assert np.allclose(U1[..., :5], U0[..., :5], rtol=1e-6, atol=1e-8)
+    w = dt * nu(U0[..., :5], prefac, omega) / Pr
+    dev0 = U0[..., 5:] - _es_targets(U0)
+    dev1 = U1[..., 5:] - _es_targets(U1)
+    assert np.allclose(dev1, dev0 / (1 + w[..., None]), rtol=1e-4, atol=1e-7)
+
+
+@pytest.mark.parametrize('scheme,order', [('adgfs-ars-111', 1), ('adgfs-ars-222', 2)])
+def test_esbgk_ars_order(scheme, order):
+    from oracle.bgk import step_ars_es
+    cv, cw = _grid()
+    f0 = _f0(cv)[None]
+    L = lambda f: -0.7 * f
+    prefac, omega, T, Pr = 2.0, 0.81, 0.4, 2.0 / 3.0
+
+    def run(n):
+        f = f0.copy()
+        for _ in range(n):
+            f = step_ars_es(f, T / n, L, scheme, prefac, omega, Pr, cv, cw)
+        return f
+    ref = run(512)
+    rate = np.log2(np.linalg.norm(run(8) - ref) / np.linalg.norm(run(16) - ref))
+    assert rate > order - 0.3, rate
+
+
+def test_esbgk_prefactor():
+    from oracle.bgk import bgk_prefactor, esbgk_prefactor
+    a = (1e-3, 337.0, 273.0, 1e20, 0.81, 2.117e-5, 273.0)
+    assert esbgk_prefactor(*a, 2.0 / 3.0) == pytest.approx(bgk_prefactor(*a) * 2.0 / 3.0)
