@@ -25,7 +25,7 @@ EXPORTS = (
     'bdgfs_hybrid_classify', 'bdgfs_hybrid_project', 'bdgfs_hybrid_scatter',
     'bdgfs_hybrid_project_scatter', 'bdgfs_hybrid_heads',
     'bdgfs_bgk_moments', 'bdgfs_bgk_maxwellian', 'bdgfs_ars_stage',
-    'bdgfs_esbgk_moments', 'bdgfs_esbgk_gaussian',
+    'bdgfs_esbgk_moments', 'bdgfs_esbgk_gaussian', 'bdgfs_shakov_moments', 'bdgfs_shakov_target',
 )
 
 
@@ -151,6 +151,8 @@ def lib():
             'bdgfs_ars_stage': [vp, vp],
             'bdgfs_esbgk_moments': [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_double, vp, vp],
             'bdgfs_esbgk_gaussian': [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_double, vp, vp],
+            'bdgfs_shakov_moments': [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_double, vp, vp],
+            'bdgfs_shakov_target': [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_double, vp, vp],
             'bdgfs_colsum': [vp, i64, i64, vp, vp],
             'bdgfs_adamw': [vp, vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float,
                             C.c_float, C.c_float, i64, vp],

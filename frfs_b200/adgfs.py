@@ -10,7 +10,9 @@ names (``moment``, ``constructMaxwellian``, ``updateMomentARS``,
 FP64 ``[ndof][nalph]``: (rho, rho u, E) for BGK (nalph = 5) and, for
 ES-BGK (ADGFSESBGKDirectGLLScatteringModel, 'esbgk-direct-gll'), those
 followed by the raw second moments (xx, yy, zz, xy, yz, zx) (nalph = 11),
-as in the reference.
+and for Shakov (ADGFSShakovDirectGLLScatteringModel, 'shakov-direct-gll')
+the raw third moments |c|^2 c after them (nalph = 14), as in the
+reference.
 """
 import ctypes as C
 
@@ -139,6 +141,40 @@ class ADGFSESBGKDirectGLLScatteringModel(ADGFSBGKDirectGLLScatteringModel):
                                                    self.fp64, self.c0.data_ptr(), self._Pr,
                                                    M.data_ptr(), _lib.stream_ptr()),
                    'bdgfs_esbgk_gaussian')
+
+
+class ADGFSShakovDirectGLLScatteringModel(ADGFSBGKDirectGLLScatteringModel):
+    """Shakov relaxation nu (S[f] - f), S = M (1 + 2 (1 - Pr)/5 (q.d)/(rho T^2)
+    (2 |d|^2/T - 5)), d = c - u, q the heat flux; nu = prefac rho T^(1 - omega)
+    with the BGK prefactor t0 p0 / visc; Pr from the .ini (default 2/3)
+    (scattering.py: ADGFSShakovDirectGLLScatteringModel;
+    kernels/scattering/shakov-direct-gll.mako)."""
+    scattering_model = 'shakov-direct-gll'
+    nalph = 14
+    ars_model = 2          # BDGFS_ARS_SHAKOV
+
+    def load_parameters(self):
+        super().load_parameters()
+        Pr = self.cfg.getfloat('scattering-model', 'Pr', 2.0 / 3.0)
+        if not Pr > 0:
+            raise ValueError('scattering-model: Pr must be positive')
+        self._Pr = Pr
+
+    def moment(self, f, U):
+        """U[dof] <- the 14 moments of f[dof] (FP64)."""
+        n = self.vm.vsize()
+        _lib.check(_lib.lib().bdgfs_shakov_moments(f.data_ptr(), f.numel() // n, self.vm.Nv(),
+                                                   self.fp64, self.c0.data_ptr(), self.cw,
+                                                   U.data_ptr(), _lib.stream_ptr()),
+                   'bdgfs_shakov_moments')
+
+    def constructMaxwellian(self, U, M):
+        """M[dof] <- the Shakov distribution of U[dof] (momentNorm + cmaxwellian)."""
+        n = self.vm.vsize()
+        _lib.check(_lib.lib().bdgfs_shakov_target(U.data_ptr(), M.numel() // n, self.vm.Nv(),
+                                                  self.fp64, self.c0.data_ptr(), self._Pr,
+                                                  M.data_ptr(), _lib.stream_ptr()),
+                   'bdgfs_shakov_target')
 
 
 class ADGFSSystem(DGFSSystem):

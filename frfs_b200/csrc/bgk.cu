@@ -38,11 +38,13 @@ __device__ __forceinline__ void row_state(const double (&U)[5], double& rho, dou
 }
 
 // FP64 moments {1, c, |c|^2, cx^2, cy^2, cz^2, cx cy, cy cz, cz cx} . f of a
-// row (block-wide partial sums per thread)
-template <typename T, int VEC>
-__device__ __forceinline__ void row_moments11(const T* __restrict__ row, int n, int Nv, const double* cs,
-                                              double (&m)[11])
+// row (NA = 11), followed by {|c|^2 c} (NA = 14); block-wide partial sums
+// per thread
+template <typename T, int VEC, int NA>
+__device__ __forceinline__ void row_moments_hi(const T* __restrict__ row, int n, int Nv, const double* cs,
+                                               double (&m)[NA])
 {
+    static_assert(NA == 11 || NA == 14, "11 or 14 moment rows");
     for (int v = threadIdx.x * VEC; v < n; v += blockDim.x * VEC) {
         Chunk<T, VEC> c;
         c.load(row + v);
@@ -52,17 +54,23 @@ __device__ __forceinline__ void row_moments11(const T* __restrict__ row, int n, 
 #pragma unroll
         for (int j = 0; j < VEC; ++j) {
             const double x = double(c.v[j]), cz = cs[iz + j];
+            const double c2x = (cx * cx + cy * cy + cz * cz) * x;
             m[0] += x;
             m[1] += cx * x;
             m[2] += cy * x;
             m[3] += cz * x;
-            m[4] += (cx * cx + cy * cy + cz * cz) * x;
+            m[4] += c2x;
             m[5] += cx * cx * x;
             m[6] += cy * cy * x;
             m[7] += cz * cz * x;
             m[8] += cx * cy * x;
             m[9] += cy * cz * x;
             m[10] += cz * cx * x;
+            if constexpr (NA == 14) {
+                m[11] += cx * c2x;
+                m[12] += cy * c2x;
+                m[13] += cz * c2x;
+            }
         }
     }
 }
@@ -104,20 +112,84 @@ __device__ __forceinline__ double es_eval(const double* g, double cx, double cy,
     return g[0] * exp(-q);
 }
 
-template <typename T, int VEC>
-__global__ void __launch_bounds__(256) esbgk_moments_kernel(const T* __restrict__ f, int Nv, const double* c0,
-                                                            double cw, double* __restrict__ U)
+template <typename T, int VEC, int NA>
+__global__ void __launch_bounds__(256) hi_moments_kernel(const T* __restrict__ f, int Nv, const double* c0,
+                                                         double cw, double* __restrict__ U)
 {
-    __shared__ double red[11 * 8];
+    __shared__ double red[NA * 8];
     __shared__ double cs[kMaxNv];
     const int64_t dof = blockIdx.x;
     const int n = Nv * Nv * Nv;
     for (int i = threadIdx.x; i < Nv; i += blockDim.x) cs[i] = c0[i];
     __syncthreads();
-    double m[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    row_moments11<T, VEC>(f + dof * int64_t(n), n, Nv, cs, m);
-    block_sum<11>(m, red);
-    if (threadIdx.x < 11) U[dof * 11 + threadIdx.x] = m[threadIdx.x] * cw;
+    double m[NA];
+#pragma unroll
+    for (int i = 0; i < NA; ++i) m[i] = 0.0;
+    row_moments_hi<T, VEC, NA>(f + dof * int64_t(n), n, Nv, cs, m);
+    block_sum<NA>(m, red);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < NA; ++i) U[dof * NA + i] = m[i] * cw;
+    }
+}
+
+// Shakov target of a 14-moment row: S(c) = M(c) (1 + (k q . d)(2 |d|^2 / T - 5)),
+// d = c - u, k = 2 (1 - Pr) / (5 rho T^2), q the heat flux
+// q_i = Q_i - 2 P_ij u_j + rho u_i |u|^2 - 1.5 rho T u_i; s = {u, 1/T, k q}
+__device__ __forceinline__ void shakov_params(const double* U, double Pr, double (&s)[7])
+{
+    const double rho = U[0], ux = U[1] / rho, uy = U[2] / rho, uz = U[3] / rho;
+    const double u2 = ux * ux + uy * uy + uz * uz;
+    const double T = (U[4] - rho * u2) / (1.5 * rho);
+    const double qx = U[11] - 2.0 * (U[5] * ux + U[8] * uy + U[10] * uz) + rho * ux * u2 - 1.5 * rho * T * ux;
+    const double qy = U[12] - 2.0 * (U[8] * ux + U[6] * uy + U[9] * uz) + rho * uy * u2 - 1.5 * rho * T * uy;
+    const double qz = U[13] - 2.0 * (U[10] * ux + U[9] * uy + U[7] * uz) + rho * uz * u2 - 1.5 * rho * T * uz;
+    const double k = 2.0 * (1.0 - Pr) / (5.0 * rho * T * T);
+    s[0] = ux;
+    s[1] = uy;
+    s[2] = uz;
+    s[3] = 1.0 / T;
+    s[4] = k * qx;
+    s[5] = k * qy;
+    s[6] = k * qz;
+}
+
+// the Shakov factor 1 + (k q . d)(2 |d|^2 / T - 5) at velocity c
+__device__ __forceinline__ double shakov_factor(const double* s, double cx, double cy, double cz)
+{
+    const double dx = cx - s[0], dy = cy - s[1], dz = cz - s[2];
+    return 1.0 + (s[4] * dx + s[5] * dy + s[6] * dz) * (2.0 * (dx * dx + dy * dy + dz * dz) * s[3] - 5.0);
+}
+
+template <typename T, int VEC>
+__global__ void __launch_bounds__(256) shakov_target_kernel(const double* __restrict__ U, int Nv,
+                                                            const double* c0, double Pr, T* __restrict__ S)
+{
+    __shared__ double cs[kMaxNv];
+    __shared__ double ex[3][kMaxNv];
+    const int64_t dof = blockIdx.x;
+    const int n = Nv * Nv * Nv;
+    const double* u = U + dof * 14;
+    double sp[7];
+    shakov_params(u, Pr, sp);
+    const double am = u[0] / pow(kPi / sp[3], 1.5);
+    for (int i = threadIdx.x; i < 3 * Nv; i += blockDim.x) {
+        const int d = i / Nv, k = i - d * Nv;
+        if (d == 0) cs[k] = c0[k];
+        const double c = c0[k] - sp[d];
+        ex[d][k] = exp(-c * c * sp[3]);
+    }
+    __syncthreads();
+    T* row = S + dof * int64_t(n);
+    for (int v = threadIdx.x * VEC; v < n; v += blockDim.x * VEC) {
+        uint32_t ix, iy, iz;
+        vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
+        Chunk<T, VEC> c;
+#pragma unroll
+        for (int j = 0; j < VEC; ++j)
+            c.v[j] = T(am * ex[0][ix] * ex[1][iy] * ex[2][iz + j] * shakov_factor(sp, cs[ix], cs[iy], cs[iz + j]));
+        c.store(row + v);
+    }
 }
 
 template <typename T, int VEC>
@@ -189,15 +261,49 @@ __global__ void __launch_bounds__(256) bgk_maxwellian_kernel(const double* __res
     }
 }
 
+// second moments of the Maxwellian of a moment row: rho T/2 + rho u_i^2, rho u_i u_j
+__device__ __forceinline__ void maxwell_second(const double* u, double (&t)[6])
+{
+    double rho, ux, uy, uz, Tt;
+    double u5[5] = {u[0], u[1], u[2], u[3], u[4]};
+    row_state(u5, rho, ux, uy, uz, Tt);
+    t[0] = 0.5 * rho * Tt + rho * ux * ux;
+    t[1] = 0.5 * rho * Tt + rho * uy * uy;
+    t[2] = 0.5 * rho * Tt + rho * uz * uz;
+    t[3] = rho * ux * uy;
+    t[4] = rho * uy * uz;
+    t[5] = rho * uz * ux;
+}
+
+// explicit heat-flux relaxation target of a 14-moment row (Shakov):
+// Q(M)_i + (1 - Pr)(q_i - Q_i), Q(M)_i = rho u_i |u|^2 + 2.5 rho T u_i,
+// q_i - Q_i = -2 P_ij u_j + rho u_i |u|^2 - 1.5 rho T u_i
+__device__ __forceinline__ void shakov_heat(const double* u, double Pr, double (&h)[3])
+{
+    double rho, ux, uy, uz, Tt;
+    double u5[5] = {u[0], u[1], u[2], u[3], u[4]};
+    row_state(u5, rho, ux, uy, uz, Tt);
+    const double u2 = ux * ux + uy * uy + uz * uz;
+    const double v[3] = {ux, uy, uz};
+    const double Pu[3] = {u[5] * ux + u[8] * uy + u[10] * uz, u[8] * ux + u[6] * uy + u[9] * uz,
+                          u[10] * ux + u[9] * uy + u[7] * uz};
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        h[i] = rho * v[i] * u2 + 2.5 * rho * Tt * v[i]
+               + (1.0 - Pr) * (-2.0 * Pu[i] + rho * v[i] * u2 - 1.5 * rho * Tt * v[i]);
+}
+
 // NA = 5: BGK (separable Maxwellians); NA = 11: ES-BGK (second moments
-// relaxed implicitly at nu/Pr, Gaussians evaluated per velocity).
+// relaxed implicitly at nu/Pr, Gaussians evaluated per velocity); NA = 14:
+// Shakov (second moments at nu, heat flux at nu Pr, separable Maxwellians
+// times the heat-flux polynomial).
 template <typename T, int VEC, int NA>
 __global__ void __launch_bounds__(256) ars_kernel(const bdgfs_ars_args g)
 {
     __shared__ double red[NA * 8];
     __shared__ double cs[kMaxNv];
-    __shared__ double ex[NA == 5 ? 4 : 1][3][kMaxNv];
-    __shared__ double gp[NA == 11 ? 4 : 1][10];
+    __shared__ double ex[NA == 11 ? 1 : 4][3][kMaxNv];
+    __shared__ double gp[NA == 5 ? 1 : 4][10];
     __shared__ double am[4], nu[4];
     const int64_t dof = blockIdx.x;
     const int Nv = g.Nv, ar = g.stage, flags = g.flags;
@@ -212,13 +318,13 @@ __global__ void __launch_bounds__(256) ars_kernel(const bdgfs_ars_args g)
         if constexpr (NA == 5) {
             row_moments<T, VEC>(row, n, Nv, cs, m);
         } else {
-            row_moments11<T, VEC>(row, n, Nv, cs, m);
+            row_moments_hi<T, VEC, NA>(row, n, Nv, cs, m);
         }
         block_sum<NA>(m, red);
 #pragma unroll
         for (int i = 0; i < NA; ++i) m[i] *= g.cw;
     };
-    // temperature-dependent relaxation rate of a moment row (conserved part)
+    // temperature-dependent collision frequency of a moment row
     auto rate = [&](const double* u) {
         double rho, ux, uy, uz, Tt;
         double u5[5] = {u[0], u[1], u[2], u[3], u[4]};
@@ -242,8 +348,8 @@ __global__ void __launch_bounds__(256) ars_kernel(const bdgfs_ars_args g)
         if (threadIdx.x == 0)
             for (int i = 0; i < NA; ++i) g.LU[ar - 1][dof * NA + i] = LUl[i];
     }
-    // ---- stage moments: U_ar = U_0 + dt sum_j ae_j LU_j for the conserved
-    // five (BGK conserves them); ES-BGK's second moments relax implicitly
+    // ---- stage moments: U_ar = U_0 + dt sum_j ae_j LU_j (the relaxation
+    // conserves the first five); higher moments relax implicitly
     if (flags & BDGFS_ARS_MOMU) {
 #pragma unroll
         for (int i = 0; i < NA; ++i) {
@@ -254,52 +360,66 @@ __global__ void __launch_bounds__(256) ars_kernel(const bdgfs_ars_args g)
             }
             Uar[i] = s;
         }
-        if constexpr (NA == 11) {
-            // targets: the Maxwellian's second moments rho T/2 + rho u_i^2, rho u_i u_j
-            auto targets = [&](const double* u, double (&t)[6]) {
-                double rho, ux, uy, uz, Tt;
-                double u5[5] = {u[0], u[1], u[2], u[3], u[4]};
-                row_state(u5, rho, ux, uy, uz, Tt);
-                t[0] = 0.5 * rho * Tt + rho * ux * ux;
-                t[1] = 0.5 * rho * Tt + rho * uy * uy;
-                t[2] = 0.5 * rho * Tt + rho * uz * uz;
-                t[3] = rho * ux * uy;
-                t[4] = rho * uy * uz;
-                t[5] = rho * uz * ux;
-            };
+        if constexpr (NA >= 11) {
+            // second moments: rate nu/Pr (ES-BGK) or nu (Shakov) towards the Maxwellian's
+            const double s2 = NA == 11 ? 1.0 / g.Pr : 1.0;
             double num[6];
 #pragma unroll
             for (int k = 0; k < 6; ++k) num[k] = Uar[5 + k];
             for (int j = 1; j < ar; ++j) {
-                double uj[11], t[6];
-#pragma unroll
-                for (int i = 0; i < 11; ++i) uj[i] = g.U[j][dof * 11 + i];
-                targets(uj, t);
-                const double w = g.ai[j - 1] * g.dt * rate(uj) / g.Pr;
+                const double* uj = g.U[j] + dof * NA;
+                double t[6];
+                maxwell_second(uj, t);
+                const double w = g.ai[j - 1] * g.dt * rate(uj) * s2;
 #pragma unroll
                 for (int k = 0; k < 6; ++k) num[k] += w * (t[k] - uj[5 + k]);
             }
             double t[6];
-            targets(Uar, t);
-            const double w = g.ai[ar - 1] * g.dt * rate(Uar) / g.Pr;
+            maxwell_second(Uar, t);
+            const double w = g.ai[ar - 1] * g.dt * rate(Uar) * s2;
 #pragma unroll
             for (int k = 0; k < 6; ++k) Uar[5 + k] = (num[k] + w * t[k]) / (1.0 + w);
+        }
+        if constexpr (NA == 14) {
+            // heat flux: dQ/dt = nu (Q(M) + (1 - Pr)(q - Q) - Pr Q), -Pr Q implicit
+            double num[3] = {Uar[11], Uar[12], Uar[13]};
+            for (int j = 1; j < ar; ++j) {
+                const double* uj = g.U[j] + dof * NA;
+                double h[3];
+                shakov_heat(uj, g.Pr, h);
+                const double w = g.ai[j - 1] * g.dt * rate(uj);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) num[k] += w * (h[k] - g.Pr * uj[11 + k]);
+            }
+            double h[3];
+            shakov_heat(Uar, g.Pr, h);
+            const double w = g.ai[ar - 1] * g.dt * rate(Uar);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) Uar[11 + k] = (num[k] + w * h[k]) / (1.0 + g.Pr * w);
         }
         if (threadIdx.x == 0)
             for (int i = 0; i < NA; ++i) g.U[ar][dof * NA + i] = Uar[i];
     }
     if (!(flags & BDGFS_ARS_DIST)) return;
 
-    // ---- relaxation targets M_1..M_ar (Maxwellians or ES Gaussians) and
-    // collision frequencies of U_1..U_ar
+    // ---- relaxation targets of U_1..U_ar (Maxwellians, ES Gaussians or
+    // Shakov distributions) and their collision frequencies
     for (int j = 1; j <= ar; ++j) {
         double u[NA];
 #pragma unroll
         for (int i = 0; i < NA; ++i) u[i] = (j == ar && (flags & BDGFS_ARS_MOMU)) ? Uar[i] : g.U[j][dof * NA + i];
         if (threadIdx.x == 0) nu[j - 1] = rate(u);
-        if constexpr (NA == 5) {
+        if constexpr (NA == 11) {
+            if (threadIdx.x == 0) {
+                double gj[10];
+                es_params(u, g.Pr, gj);
+#pragma unroll
+                for (int i = 0; i < 10; ++i) gp[j - 1][i] = gj[i];
+            }
+        } else {
             double rho, ux, uy, uz, Tt;
-            row_state(u, rho, ux, uy, uz, Tt);
+            double u5[5] = {u[0], u[1], u[2], u[3], u[4]};
+            row_state(u5, rho, ux, uy, uz, Tt);
             if (threadIdx.x == 0) am[j - 1] = rho / pow(kPi * Tt, 1.5);
             const double it = 1.0 / Tt;
             for (int i = threadIdx.x; i < 3 * Nv; i += blockDim.x) {
@@ -307,19 +427,25 @@ __global__ void __launch_bounds__(256) ars_kernel(const bdgfs_ars_args g)
                 const double c = cs[k] - (d == 0 ? ux : d == 1 ? uy : uz);
                 ex[j - 1][d][k] = exp(-c * c * it);
             }
-        } else {
-            if (threadIdx.x == 0) {
-                double gj[10];
-                es_params(u, g.Pr, gj);
+            if constexpr (NA == 14) {
+                if (threadIdx.x == 0) {
+                    double sj[7];
+                    shakov_params(u, g.Pr, sj);
 #pragma unroll
-                for (int i = 0; i < 10; ++i) gp[j - 1][i] = gj[i];
+                    for (int i = 0; i < 7; ++i) gp[j - 1][i] = sj[i];
+                }
             }
         }
     }
     __syncthreads();
     auto target = [&](int j, uint32_t ix, uint32_t iy, uint32_t izq) -> double {
-        if constexpr (NA == 5) return am[j] * ex[j][0][ix] * ex[j][1][iy] * ex[j][2][izq];
-        else return es_eval(gp[j], cs[ix], cs[iy], cs[izq]);
+        if constexpr (NA == 11) {
+            return es_eval(gp[j], cs[ix], cs[iy], cs[izq]);
+        } else {
+            const double m = am[j] * ex[j][0][ix] * ex[j][1][iy] * ex[j][2][izq];
+            if constexpr (NA == 14) return m * shakov_factor(gp[j], cs[ix], cs[iy], cs[izq]);
+            else return m;
+        }
     };
     const double dt = g.dt;
     const double aii = g.ai[ar - 1] * dt * nu[ar - 1];
@@ -403,8 +529,8 @@ extern "C" int32_t bdgfs_ars_stage(const bdgfs_ars_args* a, void* stream)
 {
     if (!a || !a->c0 || a->ndof < 0 || a->ndof > 2147483647LL || a->Nv < 1 || a->Nv > kMaxNv ||
         a->stage < 1 || a->stage > 4 || (a->flags & ~15) ||
-        (a->model != BDGFS_ARS_BGK && a->model != BDGFS_ARS_ESBGK) ||
-        (a->model == BDGFS_ARS_ESBGK && !(a->Pr > 0.0)))
+        (a->model != BDGFS_ARS_BGK && a->model != BDGFS_ARS_ESBGK && a->model != BDGFS_ARS_SHAKOV) ||
+        (a->model != BDGFS_ARS_BGK && !(a->Pr > 0.0)))
         return BDGFS_EINVAL;
     const int ar = a->stage, fl = a->flags;
     bool ok = true, v4 = a->Nv % 4 == 0;
@@ -427,6 +553,10 @@ extern "C" int32_t bdgfs_ars_stage(const bdgfs_ars_args* a, void* stream)
     }
     if (a->ndof == 0) return BDGFS_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (a->model == BDGFS_ARS_SHAKOV) {
+        if (a->fp64) return launch_rows(v4, ars_kernel<double, 4, 14>, ars_kernel<double, 1, 14>, a->ndof, st, *a);
+        return launch_rows(v4, ars_kernel<float, 4, 14>, ars_kernel<float, 1, 14>, a->ndof, st, *a);
+    }
     if (a->model == BDGFS_ARS_ESBGK) {
         if (a->fp64) return launch_rows(v4, ars_kernel<double, 4, 11>, ars_kernel<double, 1, 11>, a->ndof, st, *a);
         return launch_rows(v4, ars_kernel<float, 4, 11>, ars_kernel<float, 1, 11>, a->ndof, st, *a);
@@ -443,9 +573,9 @@ extern "C" int32_t bdgfs_esbgk_moments(const void* f, int64_t ndof, int32_t Nv, 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const bool v4 = Nv % 4 == 0 && a16(f);
     if (fp64)
-        return launch_rows(v4, esbgk_moments_kernel<double, 4>, esbgk_moments_kernel<double, 1>, ndof, st,
+        return launch_rows(v4, hi_moments_kernel<double, 4, 11>, hi_moments_kernel<double, 1, 11>, ndof, st,
                            static_cast<const double*>(f), int(Nv), c0, cw, U);
-    return launch_rows(v4, esbgk_moments_kernel<float, 4>, esbgk_moments_kernel<float, 1>, ndof, st,
+    return launch_rows(v4, hi_moments_kernel<float, 4, 11>, hi_moments_kernel<float, 1, 11>, ndof, st,
                        static_cast<const float*>(f), int(Nv), c0, cw, U);
 }
 
@@ -462,4 +592,33 @@ extern "C" int32_t bdgfs_esbgk_gaussian(const double* U, int64_t ndof, int32_t N
                            int(Nv), c0, Pr, static_cast<double*>(M));
     return launch_rows(v4, esbgk_gaussian_kernel<float, 4>, esbgk_gaussian_kernel<float, 1>, ndof, st, U,
                        int(Nv), c0, Pr, static_cast<float*>(M));
+}
+
+extern "C" int32_t bdgfs_shakov_moments(const void* f, int64_t ndof, int32_t Nv, int32_t fp64,
+                                        const double* c0, double cw, double* U, void* stream)
+{
+    if (!f || !c0 || !U || ndof < 0 || ndof > 2147483647LL || Nv < 1 || Nv > kMaxNv) return BDGFS_EINVAL;
+    if (ndof == 0) return BDGFS_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool v4 = Nv % 4 == 0 && a16(f);
+    if (fp64)
+        return launch_rows(v4, hi_moments_kernel<double, 4, 14>, hi_moments_kernel<double, 1, 14>, ndof, st,
+                           static_cast<const double*>(f), int(Nv), c0, cw, U);
+    return launch_rows(v4, hi_moments_kernel<float, 4, 14>, hi_moments_kernel<float, 1, 14>, ndof, st,
+                       static_cast<const float*>(f), int(Nv), c0, cw, U);
+}
+
+extern "C" int32_t bdgfs_shakov_target(const double* U, int64_t ndof, int32_t Nv, int32_t fp64,
+                                       const double* c0, double Pr, void* S, void* stream)
+{
+    if (!U || !c0 || !S || ndof < 0 || ndof > 2147483647LL || Nv < 1 || Nv > kMaxNv || !(Pr > 0.0))
+        return BDGFS_EINVAL;
+    if (ndof == 0) return BDGFS_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool v4 = Nv % 4 == 0 && a16(S);
+    if (fp64)
+        return launch_rows(v4, shakov_target_kernel<double, 4>, shakov_target_kernel<double, 1>, ndof, st, U,
+                           int(Nv), c0, Pr, static_cast<double*>(S));
+    return launch_rows(v4, shakov_target_kernel<float, 4>, shakov_target_kernel<float, 1>, ndof, st, U,
+                       int(Nv), c0, Pr, static_cast<float*>(S));
 }

@@ -383,16 +383,18 @@ typedef struct bdgfs_ars_args {
     const void* f[4];        /* f_0 .. f_{ar-1}                             */
     void* fout;              /* f_ar (may be f_0: updated in place)         */
     const void* L[4];        /* L_0 .. L_{ar-1} (explicit FR parts)          */
-    double* U[5];            /* moment rows U_0 .. U_ar (5 or 11 per row)   */
+    double* U[5];            /* moment rows U_0 .. U_ar (5, 11 or 14)       */
     double* LU[4];           /* moment rows of L_0 .. L_{ar-1}              */
-    int32_t model;           /* BDGFS_ARS_BGK (5 moments, Maxwellian) or
-                                BDGFS_ARS_ESBGK (11 moments, ES Gaussian)   */
+    int32_t model;           /* BDGFS_ARS_BGK (5 moments, Maxwellian),
+                                BDGFS_ARS_ESBGK (11 moments, ES Gaussian) or
+                                BDGFS_ARS_SHAKOV (14 moments, Shakov)       */
     int32_t pad_;
-    double Pr;               /* Prandtl number (ES-BGK)                     */
+    double Pr;               /* Prandtl number (ES-BGK, Shakov)             */
 } bdgfs_ars_args;
 
 #define BDGFS_ARS_BGK 0
 #define BDGFS_ARS_ESBGK 1
+#define BDGFS_ARS_SHAKOV 2
 
 /* U[dof] = moments of f[dof]: ADGFSBGKDirectGLLScatteringModel.moment. */
 int32_t bdgfs_bgk_moments(const void* f, int64_t ndof, int32_t Nv, int32_t fp64,
@@ -412,6 +414,17 @@ int32_t bdgfs_esbgk_moments(const void* f, int64_t ndof, int32_t Nv,
 int32_t bdgfs_esbgk_gaussian(const double* U, int64_t ndof, int32_t Nv,
                              int32_t fp64, const double* c0, double Pr,
                              void* M, void* stream);
+/* Shakov ('shakov-direct-gll', frfs/solvers/adgfs/scattering.py,
+ * ADGFSShakovDirectGLLScatteringModel): U[dof][14] = the 11 ES-BGK moments
+ * followed by {|c|^2 c} cw, and S[dof] = M (1 + 2 (1 - Pr)/5 (q.d)/(rho T^2)
+ * (2 |d|^2/T - 5)) with q the heat flux of U[dof] (momentNorm + cmaxwellian,
+ * shakov-direct-gll.mako:4-95). */
+int32_t bdgfs_shakov_moments(const void* f, int64_t ndof, int32_t Nv,
+                             int32_t fp64, const double* c0, double cw,
+                             double* U, void* stream);
+int32_t bdgfs_shakov_target(const double* U, int64_t ndof, int32_t Nv,
+                            int32_t fp64, const double* c0, double Pr,
+                            void* S, void* stream);
 /* One ARS stage (the flagged parts, in the order MOM0, MOML, MOMU, DIST):
  * updateMom{ar}_ARS + cmaxwellian + updateDistribution{ar}_ARS in one
  * launch, the Maxwellians computed on the fly. */

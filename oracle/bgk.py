@@ -184,3 +184,106 @@ def step_ars_es(f0, dt, L, scheme, prefac, omega, Pr, cv, cw):
         num = num + A[ar][ar] * dt * nar * es_gaussian(U[ar], Pr, cv)
         F.append(num / (1.0 + A[ar][ar] * dt * nar))
     return F[s]
+
+
+# ---------------------------------------------------------------------------
+# Shakov ('shakov-direct-gll', frfs/solvers/adgfs/scattering.py,
+# ADGFSShakovDirectGLLScatteringModel; kernels/scattering/shakov-direct-gll.mako)
+#   moments     14: the 11 ES-BGK rows and |c|^2 c (x, y, z), times cw
+#   prefactor   t0 p0 / visc (as BGK), Pr from the .ini (default 2/3)
+#   heat flux   (momentNorm) q_i = Q_i - 2 P_ij u_j + rho u_i |u|^2 - 1.5 rho T u_i
+#   target      (cmaxwellian) S = M (1 + 2 (1 - Pr)/5 (q.d)/(rho T^2) (2|d|^2/T - 5)),
+#               d = c - u
+#   ARS moments (updateMom{ar}_ARS): the conserved five explicit; the six
+#               second moments relax implicitly at nu to the Maxwellian's;
+#               Q relaxes as dQ/dt = nu (Q(M) + (1 - Pr)(q - Q) - Pr Q), only
+#               the -Pr Q part implicit, with this stage's second moments.
+
+def shakov_prefactor(H0, u0, T0, n0, omega, muRef, Tref):
+    return bgk_prefactor(H0, u0, T0, n0, omega, muRef, Tref)
+
+
+def moments14(f, cv, cw):
+    c2 = np.sum(cv * cv, axis=0)
+    rows = [c2 * cv[0], c2 * cv[1], c2 * cv[2]]
+    return np.concatenate([moments11(f, cv, cw), np.stack([f @ r for r in rows], axis=-1) * cw],
+                          axis=-1)
+
+
+def _stress(U):
+    """Raw second moments of 14-moment rows as [..., 3, 3]."""
+    P = np.empty(U.shape[:-1] + (3, 3))
+    P[..., 0, 0], P[..., 1, 1], P[..., 2, 2] = U[..., 5], U[..., 6], U[..., 7]
+    P[..., 0, 1] = P[..., 1, 0] = U[..., 8]
+    P[..., 1, 2] = P[..., 2, 1] = U[..., 9]
+    P[..., 2, 0] = P[..., 0, 2] = U[..., 10]
+    return P
+
+
+def heat_flux(U):
+    rho, u, T = _state(U)
+    Pu = np.einsum('...ij,...j->...i', _stress(U), u)
+    u2 = np.sum(u * u, axis=-1)
+    return (U[..., 11:14] - 2.0 * Pu + (rho * u2)[..., None] * u
+            - 1.5 * (rho * T)[..., None] * u)
+
+
+def shakov_target(U, Pr, cv):
+    rho, u, T = _state(U)
+    q = heat_flux(U)
+    M = maxwellian(U[..., :5], cv)
+    lead = U.shape[:-1]
+    u_, q_ = u.reshape(-1, 3), q.reshape(-1, 3)
+    d = cv[None] - u_[:, :, None]                       # [n, 3, nv]
+    qd = np.einsum('ni,niv->nv', q_, d).reshape(lead + (cv.shape[1],))
+    d2 = np.sum(d * d, axis=1).reshape(lead + (cv.shape[1],))
+    k = 2.0 * (1.0 - Pr) / 5.0 / (rho * T * T)
+    return M * (1.0 + k[..., None] * qd * (2.0 * d2 / T[..., None] - 5.0))
+
+
+def _heat_targets(U, Pr):
+    """Q(M) + (1 - Pr)(q - Q): the explicit part of the heat-flux relaxation
+    (q - Q written out, as the reference does, so that Q cancels exactly)."""
+    rho, u, T = _state(U)
+    u2 = np.sum(u * u, axis=-1)
+    QM = (rho * u2)[..., None] * u + 2.5 * (rho * T)[..., None] * u
+    qmQ = (-2.0 * np.einsum('...ij,...j->...i', _stress(U), u) + (rho * u2)[..., None] * u
+           - 1.5 * (rho * T)[..., None] * u)
+    return QM + (1.0 - Pr) * qmQ
+
+
+def step_ars_sk(f0, dt, L, scheme, prefac, omega, Pr, cv, cw):
+    """One ARS step of df/dt = L(f) + nu (S[f] - f) (Shakov)."""
+    _A, A = ARS[scheme]
+    s = len(_A) - 1
+    F, Ls, LU = [f0], [], []
+    U = [moments14(f0, cv, cw)]
+    for i in range(s):
+        ar = i + 1
+        Ls.append(L(F[i]))
+        LU.append(moments14(Ls[i], cv, cw))
+        Ua = U[0] + dt * sum(_A[ar][j] * LU[j] for j in range(ar))
+        rate = lambda Uj: nu(Uj, prefac, omega)
+        ra = rate(Ua)[..., None]
+        num = Ua[..., 5:11].copy()
+        for j in range(1, ar):
+            num += A[ar][j] * dt * rate(U[j])[..., None] * (_es_targets(U[j]) - U[j][..., 5:11])
+        num += A[ar][ar] * dt * ra * _es_targets(Ua)
+        Ua[..., 5:11] = num / (1.0 + A[ar][ar] * dt * ra)
+        num = Ua[..., 11:14].copy()
+        for j in range(1, ar):
+            num += A[ar][j] * dt * rate(U[j])[..., None] * (
+                _heat_targets(U[j], Pr) - Pr * U[j][..., 11:14])
+        # this stage's heat-flux target uses the explicit Q_ar only through
+        # (1 - Pr)(q - Q), which does not depend on Q
+        num += A[ar][ar] * dt * ra * _heat_targets(Ua, Pr)
+        Ua[..., 11:14] = num / (1.0 + Pr * A[ar][ar] * dt * ra)
+        U.append(Ua)
+        num = F[0] + sum(_A[ar][j] * dt * Ls[j] for j in range(ar))
+        for j in range(1, ar):
+            num = num + A[ar][j] * dt * nu(U[j], prefac, omega)[..., None] * (
+                shakov_target(U[j], Pr, cv) - F[j])
+        nar = nu(U[ar], prefac, omega)[..., None]
+        num = num + A[ar][ar] * dt * nar * shakov_target(U[ar], Pr, cv)
+        F.append(num / (1.0 + A[ar][ar] * dt * nar))
+    return F[s]

@@ -118,3 +118,58 @@ def test_esbgk_prefactor():
     from oracle.bgk import bgk_prefactor, esbgk_prefactor
     a = (1e-3, 337.0, 273.0, 1e20, 0.81, 2.117e-5, 273.0)
     assert esbgk_prefactor(*a, 2.0 / 3.0) == pytest.approx(bgk_prefactor(*a) * 2.0 / 3.0)
+
+
+# ---------------------------------------------------------------------------
+# Shakov ('shakov-direct-gll')
+
+def test_shakov_target_moments():
+    """S keeps the conserved moments and the Maxwellian's second moments and
+    carries the heat flux (1 - Pr) q; at Pr = 1 it is the Maxwellian."""
+    from oracle.bgk import heat_flux, moments14, shakov_target
+    cv, cw = _grid(16, 6.0)
+    f = _f0(cv, 4)[None]
+    U = moments14(f, cv, cw)
+    Pr = 2.0 / 3.0
+    US = moments14(shakov_target(U, Pr, cv), cv, cw)
+    UM = moments14(maxwellian(U[..., :5], cv), cv, cw)
+    assert np.allclose(US[..., :11], UM[..., :11], rtol=0, atol=1e-7)
+    assert np.allclose(US[..., :5], U[..., :5], rtol=0, atol=2e-7)
+    assert np.allclose(heat_flux(US), (1 - Pr) * heat_flux(U), rtol=0, atol=3e-6)
+    assert abs(heat_flux(U)).max() > 1e-2
+    assert np.allclose(shakov_target(U, 1.0, cv), maxwellian(U[..., :5], cv), rtol=1e-13, atol=0)
+
+
+def test_shakov_heat_flux_relaxes_at_nu_pr():
+    """With L = 0, ARS-111: q decays by 1/(1 + dt nu Pr), the deviatoric
+    stress by 1/(1 + dt nu), and the moments of f_1 follow U_1."""
+    from oracle.bgk import _es_targets, heat_flux, moments14, step_ars_sk
+    cv, cw = _grid(16, 6.0)
+    f = _f0(cv, 5)[None]
+    Pr, prefac, omega, dt = 2.0 / 3.0, 2.0, 0.81, 0.3
+    U0 = moments14(f, cv, cw)
+    f1 = step_ars_sk(f, dt, lambda g: 0 * g, 'adgfs-ars-111', prefac, omega, Pr, cv, cw)
+    U1 = moments14(f1, cv, cw)
+    n0 = nu(U0[..., :5], prefac, omega)[..., None]
+    assert np.allclose(heat_flux(U1), heat_flux(U0) / (1 + dt * n0 * Pr), rtol=0, atol=3e-6)
+    dev0 = U0[..., 5:11] - _es_targets(U0)
+    dev1 = U1[..., 5:11] - _es_targets(U1)
+    assert np.allclose(dev1, dev0 / (1 + dt * n0), rtol=1e-4, atol=1e-7)
+
+
+@pytest.mark.parametrize('scheme,order', [('adgfs-ars-111', 1), ('adgfs-ars-222', 2)])
+def test_shakov_ars_order(scheme, order):
+    from oracle.bgk import step_ars_sk
+    cv, cw = _grid()
+    f0 = _f0(cv)[None]
+    L = lambda f: -0.7 * f
+    prefac, omega, T, Pr = 2.0, 0.81, 0.4, 2.0 / 3.0
+
+    def run(n):
+        f = f0.copy()
+        for _ in range(n):
+            f = step_ars_sk(f, T / n, L, scheme, prefac, omega, Pr, cv, cw)
+        return f
+    ref = run(512)
+    rate = np.log2(np.linalg.norm(run(8) - ref) / np.linalg.norm(run(16) - ref))
+    assert rate > order - 0.3, rate

@@ -196,3 +196,85 @@ def test_esbgk_single_precision_and_pr_one(cuda):
     ub = step_ars(u1, 2e-3, orc1.rhs, 'adgfs-ars-222', s1.sm._prefactor, s1.sm._omega, cv,
                   s1.vm.cw())
     assert rel_l2(s1.eles_scal_upts_inb_full[0].double().cpu().numpy(), ub) < 1e-11
+
+
+def _sk_cfg(scheme, precision='double', Nv=16, dt=2e-3, Pr=None):
+    cfg = _cfg(scheme, precision=precision, Nv=Nv, dt=dt)
+    cfg.set('scattering-model', 'type', 'shakov-direct-gll')
+    if Pr is not None:
+        cfg.set('scattering-model', 'Pr', str(Pr))
+    return cfg
+
+
+def test_shakov_moments_and_target_kernels(cuda):
+    """'shakov-direct-gll': 14 moments and the Shakov distribution (FP64) vs the oracle."""
+    from oracle.bgk import moments14, shakov_target
+    from oracle.fr import velocities
+    cfg = _sk_cfg('adgfs-ars-111')
+    be, s = _system(cfg, 2)
+    assert s.sm.nalph == 14 and abs(s.sm._Pr - 2.0 / 3.0) < 1e-15
+    _perturb(s, 3)
+    f = s.eles_scal_upts_inb_full[0]
+    s.get_nregs_moms(3)
+    s.moment(0.0, 0, 0)
+    s.constructMaxwellian(0.0, 0, 1)
+    torch.cuda.synchronize()
+    cv = velocities(s.vm.c0())
+    Uo = moments14(f.double().cpu().numpy().reshape(-1, cv.shape[1]), cv, s.vm.cw())
+    Ug = s.eles_scal_upts_inb_moms[0].cpu().numpy()
+    assert Ug.shape == Uo.shape
+    assert rel_l2(Ug, Uo) < 1e-13
+    So = shakov_target(Uo, s.sm._Pr, cv)
+    Sg = s.eles_scal_upts_inb_full[1].double().cpu().numpy().reshape(So.shape)
+    assert rel_l2(Sg, So) < 1e-12
+
+
+@pytest.mark.parametrize('scheme', ['adgfs-ars-111', 'adgfs-ars-222', 'adgfs-ars-443'])
+def test_shakov_ars_steps_match_oracle(cuda, scheme):
+    """Three graph-replayed Shakov ARS steps (FP64, Pr = 2/3) vs the oracle."""
+    from oracle.bgk import step_ars_sk
+    from oracle.fr import velocities
+    cfg = _sk_cfg(scheme)
+    nreg = {'adgfs-ars-111': 2, 'adgfs-ars-222': 4, 'adgfs-ars-443': 8}[scheme]
+    be, s = _system(cfg, nreg)
+    _perturb(s, 4)
+    orc = _fr_oracle(s, 'quad', 2)
+    cv = velocities(s.vm.c0())
+    u = s.eles_scal_upts_inb_full[0].double().cpu().numpy()
+    integ = get_integrator(be, s, cfg)
+    dt = 2e-3
+    for _ in range(3):
+        u = step_ars_sk(u, dt, orc.rhs, scheme, s.sm._prefactor, s.sm._omega, s.sm._Pr, cv,
+                        s.vm.cw())
+        integ.step(0.0, dt)
+    torch.cuda.synchronize()
+    g = s.eles_scal_upts_inb_full[0].double().cpu().numpy()
+    assert rel_l2(g, u) < 1e-11
+
+
+def test_shakov_single_precision_and_pr_one(cuda):
+    """FP32 Shakov ARS-222 vs the FP64 oracle; with Pr = 1 the Shakov stepper
+    gives the BGK result."""
+    from oracle.bgk import step_ars, step_ars_sk
+    from oracle.fr import velocities
+    cfg = _sk_cfg('adgfs-ars-222', precision='single', Pr=0.75)
+    be, s = _system(cfg, 4)
+    _perturb(s, 5)
+    orc = _fr_oracle(s, 'quad', 2)
+    cv = velocities(s.vm.c0())
+    u0 = s.eles_scal_upts_inb_full[0].double().cpu().numpy()
+    get_integrator(be, s, cfg).step(0.0, 2e-3)
+    torch.cuda.synchronize()
+    uo = step_ars_sk(u0, 2e-3, orc.rhs, 'adgfs-ars-222', s.sm._prefactor, s.sm._omega, 0.75,
+                     cv, s.vm.cw())
+    assert rel_l2(s.eles_scal_upts_inb_full[0].double().cpu().numpy(), uo) < 2e-5
+    cfg1 = _sk_cfg('adgfs-ars-222', Pr=1.0)
+    be1, s1 = _system(cfg1, 4)
+    _perturb(s1, 6)
+    orc1 = _fr_oracle(s1, 'quad', 2)
+    u1 = s1.eles_scal_upts_inb_full[0].double().cpu().numpy()
+    get_integrator(be1, s1, cfg1).step(0.0, 2e-3)
+    torch.cuda.synchronize()
+    ub = step_ars(u1, 2e-3, orc1.rhs, 'adgfs-ars-222', s1.sm._prefactor, s1.sm._omega, cv,
+                  s1.vm.cw())
+    assert rel_l2(s1.eles_scal_upts_inb_full[0].double().cpu().numpy(), ub) < 1e-11
