@@ -297,9 +297,8 @@ def make_fr_oracle(system):
     from oracle.fr import FROracle
     shp = system.geo.shape
     ops = {'M0': shp.opmat('M0'), 'M132': shp.opmat('M1 - M3*M2'), 'M3': shp.opmat('M3')}
-    walls = [(system.walls.uwall[w].double().cpu().numpy(),
-              system.walls.fw[w].double().cpu().numpy()) for w in range(system.walls.fw.shape[0])]
-    return FROracle(ops, system.geo, system.vm.c0(), system.vm.cw(), walls)
+    walls, rows = system.walls.oracle_walls()
+    return FROracle(ops, system.geo, system.vm.c0(), system.vm.cw(), walls, bcid=rows)
 
 
 def run_reference(args):
@@ -939,7 +938,7 @@ def run_gpu(args):
     # gpu launches per step: 2 stages x (collide [+ disu] [+ bc_update] + rhs); the
     # one-part GLL system reads face values from the state (no disu)
     gathers = system.ele.fsel is not None and system.domain is None
-    per_stage = 2 + (0 if gathers else 1) + (1 if system.walls.nwall else 0)
+    per_stage = 2 + (0 if gathers else 1) + (1 if system.walls.has_diffuse else 0)
     launches = 2 * per_stage * args.steps
     line = {
         'metric': METRIC, 'value': value, 'unit': 'DG steps/s', 'n_gpus': ws,
@@ -1089,7 +1088,7 @@ uz = 0
         return tot / reps
     s._active = (0, 1)
     t_disu = timed(s._disu)
-    t_bc = timed(s._update_bc) if s.walls.nwall else 0.0
+    t_bc = timed(s._update_bc) if s.walls.has_diffuse else 0.0
     out = s._bank(1).clone()
     from frfs_b200 import _lib as _lb
     t_rhs = timed(lambda: _lb.lib().bdgfs_fr_rhs(
@@ -1111,7 +1110,7 @@ uz = 0
         u = s._bank(0)
         t_bcg = timed(lambda: L.bdgfs_fr_bc_update_gather(
             _lib.ref(s.ele.struct), _lib.ref(s.walls.struct), fsel, u.data_ptr(),
-            _lib.stream_ptr())) if s.walls.nwall else 0.0
+            _lib.stream_ptr())) if s.walls.has_diffuse else 0.0
         t_rg = timed(lambda: L.bdgfs_fr_rhs_gather(
             _lib.ref(s.ele.struct), _lib.ref(s.walls.struct), fsel, u.data_ptr(), out.data_ptr(),
             0.5, 2.5e-4, x1.data_ptr(), 2.5e-4, x2.data_ptr(), 0.5, _lib.stream_ptr()))

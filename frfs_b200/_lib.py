@@ -65,7 +65,11 @@ class FrTensor(C.Structure):
 class FrWall(C.Structure):
     _fields_ = [('nwall', C.c_int32), ('nbc', C.c_int32),
                 ('fpt', C.c_void_p), ('bcid', C.c_void_p), ('uwall', C.c_void_p),
-                ('fw', C.c_void_p), ('bcv', C.c_void_p), ('cw', C.c_double)]
+                ('fw', C.c_void_p), ('bcv', C.c_void_p), ('cw', C.c_double),
+                ('kind', C.c_void_p), ('kinds_used', C.c_int32), ('pad_', C.c_int32)]
+
+
+BC_DIFFUSE, BC_INLET, BC_OUTLET, BC_SPECULAR_X, BC_SPECULAR_Y, BC_SPECULAR_Z = range(6)
 
 
 class GemmArgs(C.Structure):

@@ -196,6 +196,20 @@ __global__ void __launch_bounds__(128) disu_kernel(const bdgfs_fr_eles el, const
 // (tp.m1line, TPP nonzeros per column at compile-time rows) and M2 a
 // selection (row f: tp.fsgn[f] at column tp.fdim[f]*NU + fsel[f]), instead of
 // the dense M1 - M3 M2.
+// first velocity of the chunk of VB velocities that holds the mirror
+// images of v0 .. v0 + VB - 1 under c_d -> -c_d (the grid is symmetric:
+// c0[Nv - 1 - i] = -c0[i]); for the z axis the chunk holds them reversed.
+// Chunks never straddle a z line (VB divides Nv when a y or z mirror is
+// in use, checked on the host).
+__device__ __forceinline__ int64_t mirror_chunk(int64_t v0, int Nv, int kind, int VB)
+{
+    const int64_t N = Nv, N2 = N * N;
+    if (kind == BDGFS_BC_SPECULAR_X) return v0 + (N - 1 - 2 * (v0 / N2)) * N2;
+    if (kind == BDGFS_BC_SPECULAR_Y) return v0 + (N - 1 - 2 * ((v0 / N) % N)) * N;
+    const int64_t iz = v0 % N;
+    return v0 - iz + (N - iz - VB);
+}
+
 template <typename T, int ND, int NU, int NF, int VB, bool GATHER = false, int RING = 8, int TPP = 0>
 __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, const bdgfs_fr_walls wl,
                                                   const T* __restrict__ u, const T* __restrict__ uf,
@@ -276,7 +290,13 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
     };
     auto rsrc = [&](int f, int64_t v0) -> const T* {
         const int n = nb[f];
-        if (n < 0) return fw + int64_t(wl.bcid[-1 - n]) * nv + v0;
+        if (n < 0) {
+            const int bid = wl.bcid[-1 - n];
+            const int kd = wl.kind ? wl.kind[bid] : BDGFS_BC_DIFFUSE;
+            // specular: this face's own row at the mirrored velocities
+            if (kd >= BDGFS_BC_SPECULAR_X) return lsrc(f, mirror_chunk(v0, el.Nv, kd, VB));
+            return fw + int64_t(bid) * nv + v0;
+        }
         if constexpr (GATHER) {
             const int en = n / NF;
             if (en >= el.neles) return lsrc(f, v0);     // outside this state: no flux
@@ -380,16 +400,28 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
 #pragma unroll
                 for (int d = 0; d < ND; ++d) nc[q] += pn[f * ND + d] * c[q][d];
             }
-            if (n < 0) {                                     // diffuse wall: ur holds f_w
+            if (n < 0) {                                     // boundary: ur holds f_w or the mirrored row
                 const int w = -1 - n;
                 const int bid = wl.bcid[w];
-                const T sc = -bcv[2 * w] / bcv[2 * w + 1];
+                const int kd = wl.kind ? wl.kind[bid] : BDGFS_BC_DIFFUSE;
+                if (kd == BDGFS_BC_OUTLET) {
+                    ur = ul;
+                } else if (kd == BDGFS_BC_SPECULAR_Z) {      // mirrored chunk comes reversed
 #pragma unroll
-                for (int q = 0; q < VB; ++q) {
-                    T fac = T(0);
+                    for (int q = 0; q < VB / 2; ++q) {
+                        const T t = ur.v[q];
+                        ur.v[q] = ur.v[VB - 1 - q];
+                        ur.v[VB - 1 - q] = t;
+                    }
+                } else if (kd < BDGFS_BC_SPECULAR_X) {       // diffuse wall or inlet
+                    const T sc = kd == BDGFS_BC_DIFFUSE ? -bcv[2 * w] / bcv[2 * w + 1] : T(1);
 #pragma unroll
-                    for (int d = 0; d < ND; ++d) fac += (c[q][d] - uw[bid * 3 + d]) * pn[f * ND + d];
-                    ur.v[q] = (fac < T(0)) ? ur.v[q] * sc : ul.v[q];
+                    for (int q = 0; q < VB; ++q) {
+                        T fac = T(0);
+#pragma unroll
+                        for (int d = 0; d < ND; ++d) fac += (c[q][d] - uw[bid * 3 + d]) * pn[f * ND + d];
+                        ur.v[q] = (fac < T(0)) ? ur.v[q] * sc : ul.v[q];
+                    }
                 }
             }
             T fh[VB];
@@ -449,6 +481,14 @@ __global__ void __launch_bounds__(256) bc_update_kernel(const bdgfs_fr_eles el,
     const int w = blockIdx.x;
     const int e = wl.fpt[2 * w], f = wl.fpt[2 * w + 1];
     const int bid = wl.bcid[w];
+    if (wl.kind && wl.kind[bid] != BDGFS_BC_DIFFUSE) {        // nothing to balance
+        if (threadIdx.x == 0) {
+            T* out = static_cast<T*>(wl.bcv);
+            out[2 * w] = T(0);
+            out[2 * w + 1] = T(-1);
+        }
+        return;
+    }
     const int ND = el.ndims;
     const T* pn = static_cast<const T*>(el.pnorm) + (int64_t(e) * el.nfpts + f) * ND;
     const T* uw = static_cast<const T*>(wl.uwall) + bid * 3;
@@ -651,7 +691,9 @@ static int rhs_launch(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl, const v
     // 4 velocities per thread for float (each operator column read from
     // shared memory feeds 4 x 4 FMAs; measured faster than 2 also for NU = 27)
     constexpr int VBW = sizeof(T) == 4 ? 4 : 2;
-    if (vec_width<T>(el->nv, ptrs, 6) >= VBW)
+    const int ymask = (1 << BDGFS_BC_SPECULAR_Y) | (1 << BDGFS_BC_SPECULAR_Z);
+    const bool mirror_ok = !(wl && wl->kind && (wl->kinds_used & ymask)) || el->Nv % VBW == 0;
+    if (mirror_ok && vec_width<T>(el->nv, ptrs, 6) >= VBW)
         return rhs_launch_vb<T, ND, NU, NF, VBW, TPP>(el, wl, u, uf, fsel, tp, out, a, b, x1, c1, x2, c2, st);
     return rhs_launch_vb<T, ND, NU, NF, 1, TPP>(el, wl, u, uf, fsel, tp, out, a, b, x1, c1, x2, c2, st);
 }

@@ -173,10 +173,24 @@ __global__ void __launch_bounds__(THREADS) rhs_tc_kernel(const bdgfs_fr_eles el,
                     } else {
                         const int w = -1 - n;
                         const int bid = wl.bcid[w];
-                        float fac = 0.f;
+                        const int kd = wl.kind ? wl.kind[bid] : BDGFS_BC_DIFFUSE;
+                        if (kd == BDGFS_BC_OUTLET) {
+                            ur = ul;
+                        } else if (kd >= BDGFS_BC_SPECULAR_X) {  // own face row at the mirrored velocity
+                            const int64_t N = el.Nv;
+                            const int64_t ix = v / (N * N), iy = (v / N) % N, iz = v % N;
+                            const int64_t vm =
+                                kd == BDGFS_BC_SPECULAR_X ? v + (N - 1 - 2 * ix) * N * N
+                                : kd == BDGFS_BC_SPECULAR_Y ? v + (N - 1 - 2 * iy) * N
+                                                            : v + (N - 1 - 2 * iz);
+                            ur = uf[(e * NF + f) * nv + vm];
+                        } else {
+                            float fac = 0.f;
 #pragma unroll
-                        for (int m = 0; m < ND; ++m) fac += (c[m] - uw[bid * 3 + m]) * pn[f * ND + m];
-                        ur = fac < 0.f ? fw[int64_t(bid) * nv + v] * (-bcv[2 * w] / bcv[2 * w + 1]) : ul;
+                            for (int m = 0; m < ND; ++m) fac += (c[m] - uw[bid * 3 + m]) * pn[f * ND + m];
+                            const float sc = kd == BDGFS_BC_DIFFUSE ? -bcv[2 * w] / bcv[2 * w + 1] : 1.f;
+                            ur = fac < 0.f ? fw[int64_t(bid) * nv + v] * sc : ul;
+                        }
                     }
                     x = mg[f] * (0.5f * nc * (ul + ur) + 0.5f * fabsf(nc) * (ul - ur));
                 }

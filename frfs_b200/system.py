@@ -1,4 +1,4 @@
-"""The DGFS system: state banks, FR operators, diffuse walls and Q.
+"""The DGFS system: state banks, FR operators, boundary conditions and Q.
 
 Drop-in for ``DGFSSystem`` (frfs/solvers/dgfs/system.py:17-231, name
 'dgfs') on the path the steppers use: ``rhs``, ``updatebc``, ``collide``,
@@ -102,32 +102,190 @@ class DGFSElements:
         return {'upts': self.geo.plocupts, 'fpts': self.geo.plocfpts}[name]
 
 
-class DGFSWallDiffuseBCInters:
-    """Diffuse walls ('dgfs-wall-diffuse', frfs/solvers/dgfs/inters.py:175-229):
-    wall Maxwellian f_w and wall velocity per boundary, bc0/bc1 per wall
-    face point."""
+class DGFSBCInters:
+    """One boundary condition of the 'dgfs' system, selected by its .ini
+    ``type`` (frfs/solvers/dgfs/inters.py:115-480): its kernel kind and its
+    rows (U[3], f_w[nv]) -- one row, or one per face point -- for the face
+    points ``pts`` (indices into geo.wall_fpts) of the boundary."""
+    type = None
+    kind = _lib.BC_DIFFUSE
+    oracle_type = None
+
+    def __init__(self, backend, cfg, vm, sect, geo, pts):
+        self.be, self.cfg, self.vm, self.sect, self.geo, self.pts = backend, cfg, vm, sect, geo, pts
+        self.load()
+
+    def load(self):
+        self.rows = [(np.zeros(3), np.zeros(self.vm.vsize()))]
+
+    def point_rows(self):
+        return np.zeros(len(self.pts), dtype=np.int64)
+
+    def kind_of(self):
+        return self.kind
+
+    def _maxwellian(self):
+        bc = DGFSMaxwellianInitCondition(self.be, self.cfg, self.vm, self.sect)
+        return bc.unondim()[:, 0], bc.get_init_vals()
+
+
+class DGFSWallDiffuseBCInters(DGFSBCInters):
+    """'dgfs-wall-diffuse' (inters.py:175-229): u_R = f_w (-bc0/bc1) where
+    (c - U_w).n < 0, with the wall Maxwellian f_w of the section."""
     type = 'dgfs-wall-diffuse'
 
-    def __init__(self, backend, geo, vm, cfg, bcsects):
+    def load(self):
+        self.rows = [self._maxwellian()]
+
+
+class DGFSWallDiffuseCylBCInters(DGFSBCInters):
+    """'dgfs-wall-diffuse-cyl' (inters.py:446-500, bcs/dgfs-wall-diffuse-cyl
+    .mako): the diffuse wall with U_w and T_w given as expressions of the
+    face-point location (x, y, z and the [constants]); f_w = exp(-|c -
+    U_w|^2/T_w) per face point (its normalisation cancels in bc0/bc1)."""
+    type = 'dgfs-wall-diffuse-cyl'
+    oracle_type = 'dgfs-wall-diffuse'
+
+    def load(self):
+        cfg, vm, geo = self.cfg, self.vm, self.geo
+        subs = dict(cfg.items('constants'))
+        subs.update(abs='abs', pi=repr(np.pi))
+        x = np.zeros((3, len(self.pts)))
+        for i, w in enumerate(self.pts):
+            e, f = geo.wall_fpts[w]
+            x[:geo.ndims, i] = geo.plocfpts[e, f]
+        env = {'x': x[0], 'y': x[1], 'z': x[2], 'abs': np.abs, 'exp': np.exp, 'sin': np.sin,
+               'cos': np.cos, 'tanh': np.tanh, 'sqrt': np.sqrt, 'log': np.log, 'pi': np.pi}
+
+        def ev(k):
+            v = eval(cfg.getexpr(self.sect, k, subs={c: v for c, v in subs.items()
+                                                      if c not in ('abs', 'pi')}),
+                     {'__builtins__': {}}, env)
+            return np.broadcast_to(np.asarray(v, dtype=np.float64), (len(self.pts),))
+        U = np.stack([ev('ux'), ev('uy'), ev('uz')]) / vm.u0()
+        T = ev('T') / vm.T0()
+        cv = vm.cv()
+        self.rows = []
+        for i in range(len(self.pts)):
+            d2 = np.sum((cv - U[:, i:i + 1])**2, axis=0)
+            self.rows.append((U[:, i].copy(), np.exp(-d2 / T[i])))
+
+    def point_rows(self):
+        return np.arange(len(self.pts), dtype=np.int64)
+
+
+class DGFSWallSpecularBCInters(DGFSBCInters):
+    """'dgfs-wall-specular' (inters.py:232-311): u_R(c) = u_L(c - 2 (c.n) n).
+    The kernels mirror one velocity index, so the wall must be normal to a
+    coordinate axis (every wall of a structured box mesh is)."""
+    type = 'dgfs-wall-specular'
+
+    def kind_of(self):
+        geo = self.geo
+        axes = set()
+        for w in self.pts:
+            e, f = geo.wall_fpts[w]
+            n = np.asarray(geo.norm_pnorm[e, f], dtype=np.float64)
+            a = int(np.argmax(np.abs(n)))
+            if not np.allclose(np.delete(n, a), 0.0, atol=1e-12):
+                raise ValueError(f'{self.sect}: specular walls must be normal to a coordinate axis')
+            axes.add(a)
+        if len(axes) > 1:
+            raise ValueError(f'{self.sect}: a specular boundary must be one plane')
+        c0 = np.asarray(self.vm.c0())
+        if not np.allclose(c0[::-1], -c0, rtol=0, atol=1e-12 * np.abs(c0).max()):
+            raise ValueError('specular walls need a velocity grid symmetric about 0')
+        return _lib.BC_SPECULAR_X + (axes.pop() if axes else 0)
+
+
+class DGFSInletBCInters(DGFSBCInters):
+    """'dgfs-inlet' (inters.py:312-351): u_R = f_in where (c - U_in).n < 0."""
+    type = 'dgfs-inlet'
+    kind = _lib.BC_INLET
+
+    def load(self):
+        self.rows = [self._maxwellian()]
+
+
+class DGFSInletNormalShockBCInters(DGFSBCInters):
+    """'dgfs-inlet-normalshock' (inters.py:353-384): u_R = f_in where c.n < 0."""
+    type = 'dgfs-inlet-normalshock'
+    kind = _lib.BC_INLET
+
+    def load(self):
+        self.rows = [(np.zeros(3), self._maxwellian()[1])]
+
+
+class DGFSOutletBCInters(DGFSBCInters):
+    """'dgfs-outlet' (inters.py:386-414): u_R = u_L."""
+    type = 'dgfs-outlet'
+    kind = _lib.BC_OUTLET
+
+
+class DGFSVanishBCInters(DGFSBCInters):
+    """'dgfs-vanish' (inters.py:416-444): u_R = 0 where c.n < 0."""
+    type = 'dgfs-vanish'
+    kind = _lib.BC_INLET
+
+
+class DGFSBoundaries:
+    """Every boundary face point of the system in one bdgfs_fr_walls: the
+    rows of all boundary conditions, each face point's row and each row's
+    kind."""
+
+    def __init__(self, backend, geo, vm, cfg, names):
         self.be = backend
         dt = backend.fpdtype
-        fws, uws = [], []
-        for sect in bcsects:
-            bc = DGFSMaxwellianInitCondition(backend, cfg, vm, sect)
-            fws.append(bc.get_init_vals())
-            uws.append(bc.unondim()[:, 0])
         nw = len(geo.wall_fpts)
         self.nwall = nw
-        self.fw = backend.const(np.array(fws).reshape(len(fws), -1) if fws else np.zeros((1, 1)), dtype=dt)
-        self.uwall = backend.const(np.array(uws).reshape(-1, 3) if uws else np.zeros((1, 3)), dtype=dt)
+        bcs = []
+        for bid, name in enumerate(names):
+            sect = f'soln-bcs-{name}'
+            bctype = cfg.get(sect, 'type')
+            try:
+                cls = subclass_where(DGFSBCInters, type=bctype)
+            except KeyError:
+                raise ValueError(f'unsupported boundary condition {bctype} on {name}') from None
+            pts = np.nonzero(np.asarray(geo.wall_bcid) == bid)[0]
+            bcs.append(cls(backend, cfg, vm, sect, geo, pts))
+        self.bcs = bcs
+        rows, kinds, types = [], [], []
+        bcid = np.zeros(nw, dtype=np.int64)
+        for bc in bcs:
+            base = len(rows)
+            k = bc.kind_of()
+            for r in bc.rows:
+                rows.append(r)
+                kinds.append(k)
+                types.append(bc.oracle_type or bc.type)
+            bcid[bc.pts] = base + bc.point_rows()
+        if not rows:
+            rows, kinds, types = [(np.zeros(3), np.zeros(vm.vsize()))], [0], ['dgfs-wall-diffuse']
+        self.types = types
+        self.row_of_point = bcid
+        self.fw = backend.const(np.stack([r[1] for r in rows]), dtype=dt)
+        self.uwall = backend.const(np.stack([r[0] for r in rows]), dtype=dt)
         self.fpt = backend.const(geo.wall_fpts.reshape(-1, 2) if nw else np.zeros((1, 2)),
                                  dtype=torch.int32)
-        self.bcid = backend.const(geo.wall_bcid if nw else np.zeros(1), dtype=torch.int32)
+        self.bcid = backend.const(bcid if nw else np.zeros(1), dtype=torch.int32)
+        self.kind = backend.const(np.array(kinds), dtype=torch.int32)
+        self.kinds_used = int(sum(1 << k for k in set(kinds)))
         self.bcv = backend.zeros(max(nw, 1), 2)
-        self.struct = _lib.FrWall(nwall=nw, nbc=len(fws), fpt=self.fpt.data_ptr(),
+        self.struct = _lib.FrWall(nwall=nw, nbc=len(rows), fpt=self.fpt.data_ptr(),
                                   bcid=self.bcid.data_ptr(), uwall=self.uwall.data_ptr(),
                                   fw=self.fw.data_ptr(), bcv=self.bcv.data_ptr(),
-                                  cw=float(vm.cw()))
+                                  cw=float(vm.cw()), kind=self.kind.data_ptr(),
+                                  kinds_used=self.kinds_used)
+
+    @property
+    def has_diffuse(self):
+        return bool(self.kinds_used & (1 << _lib.BC_DIFFUSE)) and self.nwall > 0
+
+    def oracle_walls(self):
+        """(rows as (U, f_w, type), row of each face point) for oracle.fr."""
+        rows = [(self.uwall[i].double().cpu().numpy(), self.fw[i].double().cpu().numpy(), t)
+                for i, t in enumerate(self.types)]
+        return rows, self.row_of_point
 
 
 class DGFSSystem:
@@ -152,15 +310,8 @@ class DGFSSystem:
         self.transport = transport
         self.ele = self.elementscls(backend, self.geo, self.vm)
         self.ndims = self.geo.ndims
-        # boundary conditions: every named boundary must be a configured wall
-        sects = []
-        for name in self.geo.wall_names:
-            sect = f'soln-bcs-{name}'
-            bctype = cfg.get(sect, 'type')
-            if bctype != 'dgfs-wall-diffuse':
-                raise ValueError(f'unsupported boundary condition {bctype} on {name}')
-            sects.append(sect)
-        self.walls = DGFSWallDiffuseBCInters(backend, self.geo, self.vm, cfg, sects)
+        # boundary conditions by the .ini type of every named boundary
+        self.walls = DGFSBoundaries(backend, self.geo, self.vm, cfg, self.geo.wall_names)
         # time-step estimate (system.py:50-66)
         advmax = self.vm.L()
         self.unitCFLdt = np.sqrt(np.min(self.geo.djac)) / advmax / self.ndims
@@ -288,7 +439,7 @@ class DGFSSystem:
             L = _lib.lib()
             u, out = self._bank(self._active[0]), self._bank(self._active[1])
             fsel = self.ele.fsel.data_ptr()
-            if self.walls.nwall:
+            if self.walls.has_diffuse:
                 _lib.check(L.bdgfs_fr_bc_update_gather(_lib.ref(self.ele.struct),
                                                        _lib.ref(self.walls.struct), fsel,
                                                        u.data_ptr(), _lib.stream_ptr()),
@@ -308,7 +459,7 @@ class DGFSSystem:
                            'bdgfs_fr_rhs_gather')
             return
         self._exchange()
-        if self.walls.nwall:
+        if self.walls.has_diffuse:
             self._update_bc()
         self._fused_rhs(a=a, b=b, x1=x1, c1=c1, x2=x2, c2=c2)
 

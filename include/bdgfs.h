@@ -142,16 +142,39 @@ typedef struct bdgfs_fr_eles {
     int32_t pad_;
 } bdgfs_fr_eles;
 
-/* Diffuse-wall face points. */
+/* Boundary face points (walls, inlets, outlets, symmetry planes).  The
+ * ghost state u_R of a boundary face point, by the kind of its boundary
+ * condition (frfs/solvers/dgfs/kernels/bcs/<type>.mako):
+ *   BDGFS_BC_DIFFUSE   u_R = f_w (-bc0/bc1) where (c - U).n < 0, else u_L
+ *                      (dgfs-wall-diffuse, dgfs-wall-diffuse-cyl)
+ *   BDGFS_BC_INLET     u_R = f_w where (c - U).n < 0, else u_L (dgfs-inlet;
+ *                      dgfs-inlet-normalshock with U = 0; dgfs-vanish with
+ *                      U = 0 and f_w = 0)
+ *   BDGFS_BC_OUTLET    u_R = u_L (dgfs-outlet)
+ *   BDGFS_BC_SPECULAR_X/Y/Z  u_R(c) = u_L(c mirrored in the plane normal to
+ *                      that axis) (dgfs-wall-specular on axis-aligned walls;
+ *                      the velocity grid is symmetric about 0)
+ * with U = uwall[bid] and f_w = fw[bid]. */
+#define BDGFS_BC_DIFFUSE 0
+#define BDGFS_BC_INLET 1
+#define BDGFS_BC_OUTLET 2
+#define BDGFS_BC_SPECULAR_X 3
+#define BDGFS_BC_SPECULAR_Y 4
+#define BDGFS_BC_SPECULAR_Z 5
 typedef struct bdgfs_fr_walls {
-    int32_t nwall;       /* wall face points                               */
-    int32_t nbc;         /* wall boundary conditions                       */
+    int32_t nwall;       /* boundary face points                           */
+    int32_t nbc;         /* boundary conditions                            */
     const int32_t* fpt;  /* [nwall][2] (element, flux point)               */
     const int32_t* bcid; /* [nwall] boundary condition of each point       */
-    const void* uwall;   /* real [nbc][3] wall velocity                    */
-    const void* fw;      /* real [nbc][nv] wall Maxwellian                 */
-    void* bcv;           /* real [nwall][2] bc0, bc1 (written by bc_update) */
+    const void* uwall;   /* real [nbc][3] wall / inlet velocity U          */
+    const void* fw;      /* real [nbc][nv] wall / inlet Maxwellian f_w     */
+    void* bcv;           /* real [nwall][2] bc0, bc1 (written by bc_update;
+                            diffuse walls only)                            */
     double cw;           /* velocity cell volume                           */
+    const int32_t* kind; /* [nbc] BDGFS_BC_* of each condition (device);
+                            NULL: every condition is a diffuse wall        */
+    int32_t kinds_used;  /* bit (1 << kind) set for every kind in kind[]   */
+    int32_t pad_;
 } bdgfs_fr_walls;
 
 /* uf = M0 u.  Replaces kernels['eles', 'disu'] (solvers/dgfs/elements.py:56-59). */

@@ -14,6 +14,12 @@ Restates, interface by interface as the reference does:
               bc1 = sum_{(c-Uw).n < 0} (c-Uw).n f_w cw
                                                  (bccupdate.mako:8-23,
                                                   bcs/dgfs-wall-diffuse-update.mako:4-38)
+  other BCs   ghost uR by the boundary's type (kernels/bcs/<type>.mako):
+              dgfs-inlet: f_in if (c-U).n < 0 else uL; dgfs-inlet-normalshock:
+              f_in if c.n < 0 else uL; dgfs-vanish: 0 if c.n < 0 else uL;
+              dgfs-outlet: uL; dgfs-wall-specular: uL at the grid velocity
+              nearest to c - 2 (c.n) n (inters.py:232-311); dgfs-wall-diffuse-cyl
+              is the diffuse wall with a per-point f_w (its own U, T)
   tdivtconf   R += M3 Fhat                       (elements.py:85-88)
   negdivconf  R = -rcpdjac R                     (kernels/negdivconf.mako:5-13)
 and the steppers dgfs-euler / dgfs-tvd-rk2 (frfs/integrators/std/steppers.py:20-225).
@@ -32,15 +38,32 @@ class FROracle:
     """ops: dict with M0, M132, M3 (reference operator matrices);
     geo: object with smats[e][u][i][k], rcpdjac[e][u], norm_pnorm[e][f][d],
     mag_pnorm[e][f], nbr[e][f] (>= 0: e'*nfpts + f'; < 0: -1 - wall index),
-    wall_fpts[w] = (e, f), wall_bcid[w]; walls: list of (Uw[3], f_w[nv])."""
+    wall_fpts[w] = (e, f), wall_bcid[w]; walls: list of (Uw[3], f_w[nv]) or
+    (Uw[3], f_w[nv], type) rows (type: the .ini boundary type, default
+    'dgfs-wall-diffuse'); bcid[w]: the row of wall point w (default
+    geo.wall_bcid)."""
 
-    def __init__(self, ops, geo, c0, cw, walls=()):
+    def __init__(self, ops, geo, c0, cw, walls=(), bcid=None):
         self.M0, self.M132, self.M3 = ops['M0'], ops['M132'], ops['M3']
         self.geo = geo
-        self.cv = velocities(np.asarray(c0, np.float64))
+        self.c0 = np.asarray(c0, np.float64)
+        self.cv = velocities(self.c0)
         self.cw = cw
-        self.walls = list(walls)
+        self.walls = [w if len(w) == 3 else (w[0], w[1], 'dgfs-wall-diffuse') for w in walls]
+        self.bcid = np.asarray(geo.wall_bcid if bcid is None else bcid)
         self.ndims = geo.smats.shape[2]
+
+    def mirror(self, n):
+        """Index map of the specular reflection c -> c - 2 (c.n) n onto the
+        nearest grid velocity (inters.py:232-311: argmin of the squared
+        distance, which on the tensor-product grid is the nearest c0 per
+        component)."""
+        n3 = np.zeros(3)
+        n3[:len(n)] = n
+        cr = self.cv - 2.0 * (n3 @ self.cv)[None, :] * n3[:, None]
+        idx = [np.argmin(np.abs(cr[d][:, None] - self.c0[None, :]), axis=1) for d in range(3)]
+        N = len(self.c0)
+        return (idx[0] * N + idx[1]) * N + idx[2]
 
     def disu(self, u):
         return np.einsum('fu,euv->efv', self.M0, u)
@@ -51,7 +74,10 @@ class FROracle:
         nw = len(g.wall_fpts)
         bc = np.zeros((nw, 2))
         for w, (e, f) in enumerate(g.wall_fpts):
-            Uw, fw = self.walls[g.wall_bcid[w]]
+            Uw, fw, kind = self.walls[self.bcid[w]]
+            if kind != 'dgfs-wall-diffuse':
+                bc[w] = (0.0, -1.0)
+                continue
             n = g.norm_pnorm[e, f]
             fac = sum((self.cv[j] - Uw[j]) * n[j] for j in range(d))
             ul = uf[e, f]
@@ -93,9 +119,23 @@ class FROracle:
                     done[e2, f2] = True
                 else:
                     w = -1 - int(nb)
-                    Uw, fw = self.walls[g.wall_bcid[w]]
+                    Uw, fw, kind = self.walls[self.bcid[w]]
                     fac = sum((self.cv[j] - Uw[j]) * n[j] for j in range(d))
-                    ur = np.where(fac < 0, fw * (-bc[w, 0] / bc[w, 1]), ul)
+                    cn = sum(self.cv[j] * n[j] for j in range(d))
+                    if kind == 'dgfs-wall-diffuse':
+                        ur = np.where(fac < 0, fw * (-bc[w, 0] / bc[w, 1]), ul)
+                    elif kind == 'dgfs-inlet':
+                        ur = np.where(fac < 0, fw, ul)
+                    elif kind == 'dgfs-inlet-normalshock':
+                        ur = np.where(cn < 0, fw, ul)
+                    elif kind == 'dgfs-vanish':
+                        ur = np.where(cn < 0, 0.0, ul)
+                    elif kind == 'dgfs-outlet':
+                        ur = ul
+                    elif kind == 'dgfs-wall-specular':
+                        ur = ul[self.mirror(n)]
+                    else:
+                        raise ValueError(kind)
                     Fh[e, f] = mag * self._rusanov(ul, ur, n)
                 done[e, f] = True
         R = R + np.einsum('uf,efv->euv', self.M3, Fh)

@@ -111,3 +111,43 @@ uy = 0
 uz = 0
 {extra}
 """)
+
+
+def bc_cfg(Nv, order, bcs, precision='single', scheme='dgfs-tvd-rk2', dt=5e-4, Nrho=8, M=6,
+           dev=5):
+    """A config whose named boundaries ('x-', 'x+', ...) carry the boundary
+    types of ``bcs``: inlets at 0.2 u0 into the domain along x with 1.2 T0,
+    diffuse walls at rest, 'dgfs-wall-diffuse-cyl' with a wall temperature
+    and tangential speed that vary along the wall."""
+    u0 = np.sqrt(2 * 8.3144598 / NONDIM['molarMass0'] * NONDIM['T0'])
+    rho0, T0 = NONDIM['rho0'], NONDIM['T0']
+    sects = []
+    for name, t in bcs.items():
+        if t == 'dgfs-wall-diffuse-cyl':
+            body = (f"rho = {rho0}\nT = {T0} * (1.0 + 0.2 * (x < 0.5) * x)\n"
+                    f"ux = {0.1 * u0} * (1 + y)\nuy = 0\nuz = {0.05 * u0} * abs(x - 0.5)")
+        elif t in ('dgfs-inlet', 'dgfs-inlet-normalshock'):
+            body = f"rho = {1.1 * rho0}\nT = {1.2 * T0}\nux = {0.2 * u0}\nuy = 0\nuz = 0"
+        elif t == 'dgfs-wall-diffuse':
+            body = f"rho = {rho0}\nT = {T0}\nux = 0\nuy = 0\nuz = 0"
+        else:
+            body = ''
+        sects.append(f"[soln-bcs-{name}]\ntype = {t}\n{body}\n")
+    return vhs_cfg(Nv, Nrho, M, dev, precision=precision, extra=f"""
+[solver]
+system = dgfs
+order = {order}
+[solver-time-integrator]
+scheme = {scheme}
+controller = none
+tstart = 0.0
+tend = 1.0
+dt = {dt}
+[soln-ics]
+type = maxwellian
+rho = {rho0}
+T = {T0}
+ux = 0
+uy = 0
+uz = 0
+""" + '\n'.join(sects))

@@ -44,11 +44,8 @@ def _perturb(sys_, seed):
 
 def _fr_oracle(sys_, kind, order):
     from oracle.fr import FROracle
-    walls = []
-    for w in range(sys_.walls.fw.shape[0]):
-        walls.append((sys_.walls.uwall[w].double().cpu().numpy(),
-                      sys_.walls.fw[w].double().cpu().numpy()))
-    return FROracle(_ops(kind, order), sys_.geo, sys_.vm.c0(), sys_.vm.cw(), walls)
+    walls, rows = sys_.walls.oracle_walls()
+    return FROracle(_ops(kind, order), sys_.geo, sys_.vm.c0(), sys_.vm.cw(), walls, bcid=rows)
 
 
 @pytest.mark.parametrize('kind,order,prec,tol', [

@@ -47,7 +47,7 @@ def test_vhs_grid_struct_fields():
 
 
 def test_fr_structs_fields():
-    from frfs_b200.system import DGFSElements, DGFSWallDiffuseBCInters
+    from frfs_b200.system import DGFSBoundaries, DGFSElements
     cfg = couette_cfg(16, 8, 6, 5, 2)
     be = _CPUBackend()
     vm = DGFSVelocityMesh(be, cfg)
@@ -57,8 +57,9 @@ def test_fr_structs_fields():
     s = el.struct
     assert (s.ndims, s.nupts, s.nfpts, s.neles, s.nv, s.Nv, s.fp64) == (2, 9, 12, 6, 4096, 16, 0)
     assert s.m0 == el.m0.data_ptr() and s.nbr == el.nbr.data_ptr() and s.c0 == el.c0.data_ptr()
-    w = DGFSWallDiffuseBCInters(be, geo, vm, cfg, ['soln-bcs-y+', 'soln-bcs-y-'])
+    w = DGFSBoundaries(be, geo, vm, cfg, geo.wall_names)
     ws = w.struct
     assert (ws.nwall, ws.nbc) == (len(geo.wall_fpts), 2)
     assert ws.bcv == w.bcv.data_ptr() and ws.cw == vm.cw()
+    assert ws.kind == w.kind.data_ptr() and ws.kinds_used == 1
     assert w.fw.shape == (2, 4096)
