@@ -6,8 +6,15 @@ u read from the section and divided by rho0, T0, u0), with the reference's
 moment-consistency check (raises ``ValueError`` when the grid cannot
 represent the state to 1e-5).  ``DGFSBKWInitCondition``
 (initcond.py:120-140): the Bobylev-Krook-Wu solution at t0.
+``DGFSMaxwellianExprInitCondition`` (initcond.py:143-212): a Maxwellian per
+solution point whose rho, u, T are expressions of x, y, z and the
+[constants]; built on the device from its moment rows.
 """
 import numpy as np
+import torch
+
+from . import _lib
+from .util import npeval
 
 
 class DGFSInitCondition:
@@ -71,3 +78,53 @@ class DGFSBKWInitCondition(DGFSInitCondition):
 
     def unondim(self):
         raise ValueError('Not defined for bkw')
+
+
+class DGFSMaxwellianExprInitCondition(DGFSInitCondition):
+    model = 'maxwellianExpr'
+
+    def load_parameters(self, name):
+        self._vars = self.cfg.items_as('constants', float)
+        self.name = name
+        if any(d in self._vars for d in 'xyz'):
+            raise ValueError('Invalid constants (x, y, or z) in config file')
+
+    def perform_precomputation(self):
+        pass
+
+    def unondim(self):
+        raise ValueError('this model depends on spatial coordinates!')
+
+    def get_init_vals(self):
+        raise ValueError('this model depends on spatial coordinates!')
+
+    def fields(self, ploc):
+        """Non-dimensional (rho, ux, uy, uz, T) at the points ploc[..., ndims]."""
+        vm = self.vm
+        v = dict(self._vars)
+        v.update(zip('xyz', np.moveaxis(np.asarray(ploc, dtype=np.float64), -1, 0)))
+        shp = np.asarray(ploc).shape[:-1]
+        scale = {'rho': vm.rho0(), 'ux': vm.u0(), 'uy': vm.u0(), 'uz': vm.u0(), 'T': vm.T0()}
+        return [np.broadcast_to(np.asarray(npeval(self.cfg.getexpr(self.name, k), v),
+                                           dtype=np.float64), shp) / scale[k]
+                for k in ('rho', 'ux', 'uy', 'uz', 'T')]
+
+    def apply_init_vals(self, bank, ploc):
+        """bank[e][upt][:] <- the Maxwellian of the fields at ploc[e][upt]
+        (bdgfs_bgk_maxwellian from the rows (rho, rho u, E)); raises when a
+        point's density is not represented to 1e-5 (initcond.py:156-169)."""
+        vm = self.vm
+        rho, ux, uy, uz, T = (a.reshape(-1) for a in self.fields(ploc))
+        u2 = ux * ux + uy * uy + uz * uz
+        U = np.stack([rho, rho * ux, rho * uy, rho * uz, 1.5 * rho * T + rho * u2], axis=-1)
+        dev = bank.device
+        Ud = torch.as_tensor(U, dtype=torch.float64, device=dev).contiguous()
+        c0 = torch.as_tensor(vm.c0(), dtype=torch.float64, device=dev).contiguous()
+        n = vm.vsize()
+        _lib.check(_lib.lib().bdgfs_bgk_maxwellian(Ud.data_ptr(), bank.numel() // n, vm.Nv(),
+                                                   int(bank.dtype == torch.float64), c0.data_ptr(),
+                                                   bank.data_ptr(), _lib.stream_ptr()),
+                   'bdgfs_bgk_maxwellian')
+        bulk = bank.reshape(-1, n).double().sum(-1).cpu().numpy() * vm.cw()
+        if not np.allclose(rho, bulk, atol=1e-5):
+            raise ValueError('Bulk properties not conserved! Check Nv, dev')

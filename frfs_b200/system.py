@@ -26,7 +26,7 @@ from . import _lib
 from .initcond import DGFSInitCondition, DGFSMaxwellianInitCondition
 from .mesh import ElementGeometry
 from .scattering import DGFSScatteringModel
-from .util import subclass_where
+from .util import npeval, subclass_where
 from .velocitymesh import DGFSVelocityMesh
 
 
@@ -148,19 +148,15 @@ class DGFSWallDiffuseCylBCInters(DGFSBCInters):
 
     def load(self):
         cfg, vm, geo = self.cfg, self.vm, self.geo
-        subs = dict(cfg.items('constants'))
-        subs.update(abs='abs', pi=repr(np.pi))
         x = np.zeros((3, len(self.pts)))
         for i, w in enumerate(self.pts):
             e, f = geo.wall_fpts[w]
             x[:geo.ndims, i] = geo.plocfpts[e, f]
-        env = {'x': x[0], 'y': x[1], 'z': x[2], 'abs': np.abs, 'exp': np.exp, 'sin': np.sin,
-               'cos': np.cos, 'tanh': np.tanh, 'sqrt': np.sqrt, 'log': np.log, 'pi': np.pi}
+        env = cfg.items_as('constants', float)
+        env.update(x=x[0], y=x[1], z=x[2])
 
         def ev(k):
-            v = eval(cfg.getexpr(self.sect, k, subs={c: v for c, v in subs.items()
-                                                      if c not in ('abs', 'pi')}),
-                     {'__builtins__': {}}, env)
+            v = npeval(cfg.getexpr(self.sect, k), env)
             return np.broadcast_to(np.asarray(v, dtype=np.float64), (len(self.pts),))
         U = np.stack([ev('ux'), ev('uy'), ev('uz')]) / vm.u0()
         T = ev('T') / vm.T0()
@@ -335,8 +331,11 @@ class DGFSSystem:
         else:
             icn = cfg.get('soln-ics', 'type')
             ic = subclass_where(DGFSInitCondition, model=icn)(backend, cfg, self.vm, 'soln-ics')
-            f0 = backend.const(ic.get_init_vals())
-            self.eles_scal_upts_inb_full[0].copy_(f0.expand(E, U, nv))
+            if hasattr(ic, 'apply_init_vals'):
+                ic.apply_init_vals(self.eles_scal_upts_inb_full[0], self.geo.plocupts)
+            else:
+                f0 = backend.const(ic.get_init_vals())
+                self.eles_scal_upts_inb_full[0].copy_(f0.expand(E, U, nv))
         self._gen_kernels()
 
     # -- kernel registry ------------------------------------------------

@@ -117,3 +117,27 @@ def test_oracle_mirror_is_the_reflection():
     cr = o.cv[:2] - 2 * (n @ o.cv[:2]) * n[:, None]
     cr = np.clip(cr, c0[0], c0[-1])         # reflections off the grid: its nearest edge
     assert np.all(np.abs(o.cv[:2, m] - cr) <= (c0[1] - c0[0]) / 2 + 1e-12)
+
+
+def test_npeval_and_expression_initial_condition_fields():
+    from frfs_b200.initcond import DGFSMaxwellianExprInitCondition
+    from frfs_b200.util import npeval
+    x = np.linspace(0.0, 1.0, 5)
+    assert np.allclose(npeval('2 + (x < 0.5)*x + pow(x, 2)', {'x': x}), 2 + (x < 0.5) * x + x**2)
+    for bad in ('x**2', 'x.__class__', 'x; y', "__import__('os')"):
+        with pytest.raises(ValueError):
+            npeval(bad, {'x': x})
+    cfg = bc_cfg(16, 2, QUAD)
+    u0 = np.sqrt(2 * 8.3144598 / 39.96e-3 * 273.0)
+    cfg.set('constants', 'rl', '0.00011140244750324529')
+    for k, v in (('type', 'maxwellianExpr'), ('rho', 'rl*(1 + 0.1*sin(2*pi*x))'),
+                 ('ux', f'{0.1 * u0}*y'), ('uy', '0'), ('uz', '0'), ('T', '273*(1 + 0.05*x)')):
+        cfg.set('soln-ics', k, v)
+    vm = DGFSVelocityMesh(_CPUBackend(), cfg)
+    ic = DGFSMaxwellianExprInitCondition(_CPUBackend(), cfg, vm, 'soln-ics')
+    with pytest.raises(ValueError):
+        ic.get_init_vals()
+    p = np.array([[0.25, 0.5], [0.75, -0.5]])
+    rho, ux, uy, uz, T = ic.fields(p)
+    assert np.allclose(rho, [1.1, 0.9]) and np.allclose(ux, [0.05, -0.05])
+    assert np.allclose(T, [1.0125, 1.0375]) and not uy.any() and not uz.any()

@@ -103,3 +103,26 @@ def test_bc_steps_match_oracle(cuda, kind, bcs, nsteps):
         integ.tcurr += dt
     torch.cuda.synchronize()
     assert rel_l2(s.eles_scal_upts_inb_full[0].double().cpu().numpy(), u) < 1e-11
+
+
+@pytest.mark.parametrize('prec,tol', [('double', 1e-13), ('single', 1e-6)])
+def test_maxwellian_expr_initial_condition(cuda, prec, tol):
+    """'maxwellianExpr': every solution point holds the Maxwellian of the
+    expressions at its location."""
+    from helpers import maxwellian
+    cfg = bc_cfg(16, 2, QUAD, precision=prec)
+    u0 = np.sqrt(2 * 8.3144598 / 39.96e-3 * 273.0)
+    cfg.set('constants', 'rl', '0.00011140244750324529')
+    for k, v in (('type', 'maxwellianExpr'), ('rho', 'rl*(1 + 0.1*sin(2*pi*x))'),
+                 ('ux', f'{0.1 * u0}*y'), ('uy', f'{0.05 * u0}*x'), ('uz', '0'),
+                 ('T', '273*(1 + 0.05*x)')):
+        cfg.set('soln-ics', k, v)
+    be = CUDABackend(cfg)
+    s = DGFSSystem(be, StructuredMesh((3, 2), (0.0, -0.5), (1.0, 0.5)), cfg, nreg=2)
+    torch.cuda.synchronize()
+    cv = s.vm.cv()
+    p = s.geo.plocupts
+    want = np.stack([np.stack([maxwellian(cv, 1 + 0.1 * np.sin(2 * np.pi * x), [0.1 * y, 0.05 * x, 0],
+                                          1 + 0.05 * x) for x, y in pe]) for pe in p])
+    got = s.eles_scal_upts_inb_full[0].double().cpu().numpy()
+    assert rel_l2(got, want) < tol
