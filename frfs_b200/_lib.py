@@ -26,6 +26,7 @@ EXPORTS = (
     'bdgfs_hybrid_project_scatter', 'bdgfs_hybrid_heads',
     'bdgfs_bgk_moments', 'bdgfs_bgk_maxwellian', 'bdgfs_ars_stage',
     'bdgfs_esbgk_moments', 'bdgfs_esbgk_gaussian', 'bdgfs_shakov_moments', 'bdgfs_shakov_target',
+    'bdgfs_bdf_step',
 )
 
 
@@ -108,6 +109,17 @@ class ArsArgs(C.Structure):
                 ('model', C.c_int32), ('pad_', C.c_int32), ('Pr', C.c_double)]
 
 
+class BdfArgs(C.Structure):
+    _fields_ = [('ndof', C.c_int64), ('Nv', C.c_int32), ('fp64', C.c_int32),
+                ('c0', C.c_void_p), ('cw', C.c_double), ('prefac', C.c_double),
+                ('omega', C.c_double), ('dt', C.c_double), ('q', C.c_int32),
+                ('model', C.c_int32), ('Pr', C.c_double), ('a', C.c_double * 4),
+                ('g', C.c_double * 3), ('b', C.c_double), ('f', C.c_void_p * 3),
+                ('L', C.c_void_p * 3), ('U', C.c_void_p * 3), ('LU', C.c_void_p * 3),
+                ('Unew', C.c_void_p), ('fout', C.c_void_p), ('flags', C.c_int32),
+                ('pad_', C.c_int32)]
+
+
 _lib = None
 
 
@@ -157,6 +169,7 @@ def lib():
             'bdgfs_esbgk_gaussian': [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_double, vp, vp],
             'bdgfs_shakov_moments': [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_double, vp, vp],
             'bdgfs_shakov_target': [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_double, vp, vp],
+            'bdgfs_bdf_step': [vp, vp],
             'bdgfs_colsum': [vp, i64, i64, vp, vp],
             'bdgfs_adamw': [vp, vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float,
                             C.c_float, C.c_float, i64, vp],

@@ -23,6 +23,7 @@ from .system import DGFSSystem
 from .util import subclass_where  # noqa: F401
 
 ARS_MOM0, ARS_MOML, ARS_MOMU, ARS_DIST = 1, 2, 4, 8
+BDF_MOMN, BDF_MOMU, BDF_DIST = 1, 2, 4
 R0 = 8.3144598
 NA = 6.0221409e+23
 
@@ -106,6 +107,24 @@ class ADGFSBGKDirectGLLScatteringModel(ADGFSScatteringModel):
         for j, t in enumerate(LU):
             a.LU[j] = p(t)
         _lib.check(_lib.lib().bdgfs_ars_stage(C.byref(a), _lib.stream_ptr()), 'bdgfs_ars_stage')
+
+
+    def bdf_step(self, ndof, dt, q, flags, a, g, b, f, fout, L, U, LU, Unew):
+        """One fused IMEX-BDF step (bdgfs_bdf_step) over ndof distributions;
+        f, L, U, LU are lists of q tensors, oldest first (None where the
+        flags do not need them)."""
+        p = lambda t: t.data_ptr() if t is not None else None
+        x = _lib.BdfArgs(ndof=int(ndof), Nv=self.vm.Nv(), fp64=self.fp64, c0=self.c0.data_ptr(),
+                         cw=self.cw, prefac=self._prefactor, omega=self._omega, dt=float(dt),
+                         q=int(q), model=self.ars_model, Pr=self._Pr, b=float(b), flags=flags,
+                         Unew=p(Unew), fout=p(fout))
+        for j, v in enumerate(a):
+            x.a[j] = v
+        for j, v in enumerate(g):
+            x.g[j] = v
+        for j in range(q):
+            x.f[j], x.L[j], x.U[j], x.LU[j] = p(f[j]), p(L[j]), p(U[j]), p(LU[j])
+        _lib.check(_lib.lib().bdgfs_bdf_step(C.byref(x), _lib.stream_ptr()), 'bdgfs_bdf_step')
 
 
 class ADGFSESBGKDirectGLLScatteringModel(ADGFSBGKDirectGLLScatteringModel):
@@ -242,6 +261,46 @@ class ADGFSSystem(DGFSSystem):
         U = [self._mom(x) for x in args[3 * q:4 * q + 1]]
         F = [self._ref(x) for x in args[5 * q + 1:]]
         self.sm.ars_stage(self.ndof, dt, q, ARS_DIST, ae, ai, F[:q], F[q], L, U, [None] * q)
+
+    def updateMomentBDF(self, dt, *args):
+        """args = a_0, U_0, g_0, LU_0, ..., a_{q-1}, U_{q-1}, g_{q-1},
+        LU_{q-1}, a_q, U, b (system.py:108-111, updateMom{q}_BDF)."""
+        q = (len(args) - 3) // 4
+        if len(args) != 4 * q + 3:
+            raise ValueError('updateMomentBDF: inconsistent number of arguments')
+        a = [args[4 * i] for i in range(q)] + [args[4 * q]]
+        g = [args[4 * i + 2] for i in range(q)]
+        U = [self._mom(args[4 * i + 1]) for i in range(q)]
+        LU = [self._mom(args[4 * i + 3]) for i in range(q)]
+        self.sm.bdf_step(self.ndof, dt, q, BDF_MOMU, a, g, args[4 * q + 2], [None] * q, None,
+                         [None] * q, U, LU, self._mom(args[4 * q + 1]))
+
+    def updateDistBDF(self, dt, *args):
+        """args = a_0, f_0, g_0, L_0, ..., b, M (unused: the target is rebuilt
+        from U on the fly), a_q, U, f (system.py:113-121,
+        updateDistribution{q}_BDF)."""
+        q = (len(args) - 5) // 4
+        if len(args) != 4 * q + 5:
+            raise ValueError('updateDistBDF: inconsistent number of arguments')
+        a = [args[4 * i] for i in range(q)] + [args[4 * q + 2]]
+        g = [args[4 * i + 2] for i in range(q)]
+        f = [self._ref(args[4 * i + 1]) for i in range(q)]
+        L = [self._ref(args[4 * i + 3]) for i in range(q)]
+        self.sm.bdf_step(self.ndof, dt, q, BDF_DIST, a, g, args[4 * q], f,
+                         self._ref(args[4 * q + 4]), L, [None] * q, [None] * q,
+                         self._mom(args[4 * q + 3]))
+
+    def copy_dist(self, rdest, rsrc):
+        self._ref(rdest).copy_(self._ref(rsrc))
+
+    def copy_moms(self, rdest, rsrc):
+        self._mom(rdest).copy_(self._mom(rsrc))
+
+    def bdf_step(self, dt, q, flags, a, g, b, fbanks, foutbank, Lbanks, Umoms, LUmoms, Unew):
+        self.sm.bdf_step(self.ndof, dt, q, flags, a, g, b, [self._bank(x) for x in fbanks],
+                         self._bank(foutbank), [self._bank(x) for x in Lbanks],
+                         [self._mom(m) for m in Umoms], [self._mom(m) for m in LUmoms],
+                         self._mom(Unew))
 
     # fused stage used by the project's ARS steppers ------------------------
     def ars_stage(self, dt, ar, flags, ae, ai, fbanks, foutbank, Lbanks, Umoms, LUmoms):

@@ -477,6 +477,158 @@ __global__ void __launch_bounds__(256) ars_kernel(const bdgfs_ars_args g)
     }
 }
 
+// One IMEX-BDF step (updateMom{q}_BDF + constructMaxwellian +
+// updateDistribution{q}_BDF): with N = -sum_i (a_i X_i + g_i dt LX_i),
+//   U  = N / a_q for the conserved five; higher moments relax implicitly
+//        (ES-BGK second moments at b nu/Pr, Shakov second moments at b nu and
+//        the heat flux with denominator a_q + Pr b dt nu)
+//   f  = (N_f + b dt nu M[U]) / (a_q + b dt nu).
+// One CTA per distribution; the newest moment rows (of f_{q-1} and of
+// L_{q-1}) are reduced in the same launch when BDGFS_BDF_MOMN is set.
+template <typename T, int VEC, int NA>
+__global__ void __launch_bounds__(256) bdf_kernel(const bdgfs_bdf_args g)
+{
+    __shared__ double red[NA * 8];
+    __shared__ double cs[kMaxNv];
+    __shared__ double ex[3][kMaxNv];
+    __shared__ double gp[10];
+    __shared__ double am, nu;
+    const int64_t dof = blockIdx.x;
+    const int Nv = g.Nv, q = g.q, flags = g.flags;
+    const int n = Nv * Nv * Nv;
+    const int64_t off = dof * int64_t(n);
+    for (int i = threadIdx.x; i < Nv; i += blockDim.x) cs[i] = g.c0[i];
+    __syncthreads();
+
+    auto moments = [&](const T* row, double (&m)[NA]) {
+#pragma unroll
+        for (int i = 0; i < NA; ++i) m[i] = 0.0;
+        if constexpr (NA == 5) {
+            row_moments<T, VEC>(row, n, Nv, cs, m);
+        } else {
+            row_moments_hi<T, VEC, NA>(row, n, Nv, cs, m);
+        }
+        block_sum<NA>(m, red);
+#pragma unroll
+        for (int i = 0; i < NA; ++i) m[i] *= g.cw;
+    };
+    auto rate = [&](const double* u) {
+        double rho, ux, uy, uz, Tt;
+        double u5[5] = {u[0], u[1], u[2], u[3], u[4]};
+        row_state(u5, rho, ux, uy, uz, Tt);
+        return g.prefac * rho * pow(Tt, 1.0 - g.omega);
+    };
+
+    double Un[NA], LUn[NA], U[NA];
+    if (flags & BDGFS_BDF_MOMN) {
+        moments(static_cast<const T*>(g.f[q - 1]) + off, Un);
+        moments(static_cast<const T*>(g.L[q - 1]) + off, LUn);
+        if (threadIdx.x == 0)
+            for (int i = 0; i < NA; ++i) {
+                g.U[q - 1][dof * NA + i] = Un[i];
+                g.LU[q - 1][dof * NA + i] = LUn[i];
+            }
+    }
+    const double aq = g.a[q];
+    if (flags & BDGFS_BDF_MOMU) {
+        double N[NA];
+#pragma unroll
+        for (int k = 0; k < NA; ++k) {
+            double s = 0.0;
+            for (int i = 0; i < q; ++i) {
+                const bool fresh = i == q - 1 && (flags & BDGFS_BDF_MOMN);
+                const double ui = fresh ? Un[k] : g.U[i][dof * NA + k];
+                const double li = fresh ? LUn[k] : g.LU[i][dof * NA + k];
+                s -= g.a[i] * ui + g.g[i] * g.dt * li;
+            }
+            N[k] = s;
+        }
+#pragma unroll
+        for (int k = 0; k < 5; ++k) U[k] = N[k] / aq;
+        if constexpr (NA >= 11) {
+            const double w = g.b * g.dt * rate(U) * (NA == 11 ? 1.0 / g.Pr : 1.0);
+            double t[6];
+            maxwell_second(U, t);
+#pragma unroll
+            for (int k = 0; k < 6; ++k) U[5 + k] = (N[5 + k] + w * t[k]) / (aq + w);
+        }
+        if constexpr (NA == 14) {
+            const double w = g.b * g.dt * rate(U);
+            double h[3];
+            shakov_heat(U, g.Pr, h);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) U[11 + k] = (N[11 + k] + w * h[k]) / (aq + g.Pr * w);
+        }
+        if (threadIdx.x == 0)
+            for (int i = 0; i < NA; ++i) g.Unew[dof * NA + i] = U[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < NA; ++i) U[i] = g.Unew[dof * NA + i];
+    }
+    if (!(flags & BDGFS_BDF_DIST)) return;
+
+    // relaxation target of U and its collision frequency
+    if (threadIdx.x == 0) nu = rate(U);
+    if constexpr (NA == 11) {
+        if (threadIdx.x == 0) {
+            double gj[10];
+            es_params(U, g.Pr, gj);
+#pragma unroll
+            for (int i = 0; i < 10; ++i) gp[i] = gj[i];
+        }
+    } else {
+        double rho, ux, uy, uz, Tt;
+        double u5[5] = {U[0], U[1], U[2], U[3], U[4]};
+        row_state(u5, rho, ux, uy, uz, Tt);
+        if (threadIdx.x == 0) am = rho / pow(kPi * Tt, 1.5);
+        const double it = 1.0 / Tt;
+        for (int i = threadIdx.x; i < 3 * Nv; i += blockDim.x) {
+            const int d = i / Nv, k = i - d * Nv;
+            const double c = cs[k] - (d == 0 ? ux : d == 1 ? uy : uz);
+            ex[d][k] = exp(-c * c * it);
+        }
+        if constexpr (NA == 14) {
+            if (threadIdx.x == 0) {
+                double sj[7];
+                shakov_params(U, g.Pr, sj);
+#pragma unroll
+                for (int i = 0; i < 7; ++i) gp[i] = sj[i];
+            }
+        }
+    }
+    __syncthreads();
+    auto target = [&](uint32_t ix, uint32_t iy, uint32_t izq) -> double {
+        if constexpr (NA == 11) {
+            return es_eval(gp, cs[ix], cs[iy], cs[izq]);
+        } else {
+            const double m = am * ex[0][ix] * ex[1][iy] * ex[2][izq];
+            if constexpr (NA == 14) return m * shakov_factor(gp, cs[ix], cs[iy], cs[izq]);
+            else return m;
+        }
+    };
+    const double bdn = g.b * g.dt * nu;
+    const double inv = 1.0 / (aq + bdn);
+    for (int v = threadIdx.x * VEC; v < n; v += blockDim.x * VEC) {
+        uint32_t ix, iy, iz;
+        vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
+        double acc[VEC];
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) acc[j] = 0.0;
+        for (int i = 0; i < q; ++i) {
+            Chunk<T, VEC> cf, cl;
+            cf.load(static_cast<const T*>(g.f[i]) + off + v);
+            cl.load(static_cast<const T*>(g.L[i]) + off + v);
+            const double wa = g.a[i], wg = g.g[i] * g.dt;
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) acc[j] -= wa * double(cf.v[j]) + wg * double(cl.v[j]);
+        }
+        Chunk<T, VEC> o;
+#pragma unroll
+        for (int j = 0; j < VEC; ++j) o.v[j] = T((acc[j] + bdn * target(ix, iy, iz + j)) * inv);
+        o.store(static_cast<T*>(g.fout) + off + v);
+    }
+}
+
 }  // namespace bdgfs
 
 using namespace bdgfs;
@@ -621,4 +773,41 @@ extern "C" int32_t bdgfs_shakov_target(const double* U, int64_t ndof, int32_t Nv
                            int(Nv), c0, Pr, static_cast<double*>(S));
     return launch_rows(v4, shakov_target_kernel<float, 4>, shakov_target_kernel<float, 1>, ndof, st, U,
                        int(Nv), c0, Pr, static_cast<float*>(S));
+}
+
+extern "C" int32_t bdgfs_bdf_step(const bdgfs_bdf_args* a, void* stream)
+{
+    if (!a || a->ndof < 0 || a->ndof > 2147483647LL || a->Nv < 1 || a->Nv > kMaxNv || !a->c0 ||
+        a->q < 1 || a->q > 3 || (a->flags & ~7) || !a->Unew ||
+        (a->model != BDGFS_ARS_BGK && a->model != BDGFS_ARS_ESBGK && a->model != BDGFS_ARS_SHAKOV) ||
+        (a->model != BDGFS_ARS_BGK && !(a->Pr > 0.0)) || a->a[a->q] == 0.0)
+        return BDGFS_EINVAL;
+    const int q = a->q;
+    if (a->flags & BDGFS_BDF_MOMN) {
+        if (!a->f[q - 1] || !a->L[q - 1] || !a->U[q - 1] || !a->LU[q - 1]) return BDGFS_EINVAL;
+    }
+    if (a->flags & BDGFS_BDF_MOMU) {
+        for (int i = 0; i < q; ++i)
+            if (!a->U[i] || !a->LU[i]) return BDGFS_EINVAL;
+    }
+    bool v4 = a->Nv % 4 == 0;
+    if (a->flags & BDGFS_BDF_DIST) {
+        if (!a->fout) return BDGFS_EINVAL;
+        v4 = v4 && a16(a->fout);
+        for (int i = 0; i < q; ++i) {
+            if (!a->f[i] || !a->L[i]) return BDGFS_EINVAL;
+            v4 = v4 && a16(a->f[i]) && a16(a->L[i]);
+        }
+    } else if (a->flags & BDGFS_BDF_MOMN) {
+        v4 = v4 && a16(a->f[q - 1]) && a16(a->L[q - 1]);
+    }
+    if (a->ndof == 0) return BDGFS_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+#define BDF_GO(NA)                                                                                         \
+    return a->fp64 ? launch_rows(v4, bdf_kernel<double, 4, NA>, bdf_kernel<double, 1, NA>, a->ndof, st, *a) \
+                   : launch_rows(v4, bdf_kernel<float, 4, NA>, bdf_kernel<float, 1, NA>, a->ndof, st, *a);
+    if (a->model == BDGFS_ARS_SHAKOV) { BDF_GO(14) }
+    if (a->model == BDGFS_ARS_ESBGK) { BDF_GO(11) }
+    BDF_GO(5)
+#undef BDF_GO
 }

@@ -10,6 +10,8 @@ stepper chosen by ``[solver-time-integrator] scheme``:
 * 'adgfs-ars-111/222/443' (steppers.py:489-670): IMEX Runge-Kutta with the
                  FR advection explicit and the BGK relaxation implicit
                  ('adgfs' system, frfs_b200.adgfs)
+* 'adgfs-bdf-1/2/3' (steppers.py:675-860): IMEX backward differences
+                 (BDF-1 is ARS-111)
 
 Each stage is one ``collide`` launch (all DOFs) plus the disu / bc-update /
 fused-rhs launches; the register banks are those of the reference (r0, r1,
@@ -209,8 +211,124 @@ class ARS443AstdStepper(ARSabcAstdStepper):
     nregs = 8
 
 
+class BDF1AstdStepper(ARS111AstdStepper):
+    """'adgfs-bdf-1' is ARS-111 (steppers.py:675-676)."""
+    stepper_name = 'adgfs-bdf-1'
+
+
+class BDFqAstdStepper(BaseDGFSStepper):
+    """IMEX backward-difference schemes of order q for the 'adgfs' system
+    (BDF2AstdStepper / BDF3AstdStepper, steppers.py:680-860).  Per step:
+    L_n = L(f_n) (one FR launch) and one fused bdgfs_bdf_step launch that
+    reduces the moments of f_n and L_n, forms the new moments and writes
+    f_{n+1} over the oldest history bank.  The histories live in rings of q
+    banks (f, L) and moment rows (U, LU), so a step copies nothing; each of
+    the q ring phases is its own CUDA graph.  The first q - 1 calls each take
+    nstepsInit ARS-222 sub-steps (the reference's BDF3 takes both start-up
+    steps in its first call and none in its second; the state after two
+    calls is the same)."""
+    q = bdf_A = bdf_G = bdf_B = nstepsInit = None
+
+    def __init__(self, backend, system, cfg):
+        super().__init__(backend, system, cfg)
+        q = self.q
+        moms = system.get_nregs_moms(2 * q + 1)
+        self._FB = list(range(q))                 # f ring: bank 0 holds the solution at start
+        self._LB = list(range(q, 2 * q))
+        self._S = 2 * q                           # scratch F_1 of the ARS-222 start-up
+        self._UR, self._LR, self._UN = moms[:q], moms[q:2 * q], moms[2 * q]
+        self._nstart = 0
+        self._phase = 1
+        self._graphs = {}
+
+    def _ars222(self, t, dt):
+        """One ARS-222 sub-step of the solution in bank 0 (ARSabcAstdStepper)."""
+        from .adgfs import ARS_DIST, ARS_MOM0, ARS_MOML, ARS_MOMU
+        sysm, A = self.system, ARS222AstdStepper
+        F, L = [0, self._S, 0], self._LB[:2]
+        U, LU = [self._UR[0], self._UR[1], self._LR[0]], [self._LR[1], self._UN]
+        for i in range(2):
+            ar = i + 1
+            sysm.advect_combine(t, F[i], L[i], a=0.0, b=1.0)
+            flags = ARS_MOML | ARS_MOMU | ARS_DIST | (ARS_MOM0 if i == 0 else 0)
+            sysm.ars_stage(dt, ar, flags, A._A_expl(ar), A._A_impl(ar), F[:ar], F[ar], L[:ar],
+                           U[:ar + 1], LU[:ar])
+
+    def _startup(self, t, dt):
+        sysm, k = self.system, self._nstart
+        sysm._bank(self._FB[k + 1]).copy_(sysm._bank(0))       # keep f(t) as history
+        h = dt / self.nstepsInit
+        for j in range(self.nstepsInit):
+            self._ars222(t + j * h, h)
+        self._nstart += 1
+        if self._nstart == self.q - 1:
+            # history rows of the older states: L_i = L(f_i), U_i, LU_i
+            from .adgfs import BDF_MOMN
+            q, p = self.q, self._phase
+            for i in range(q - 1):
+                fb, lb = self._FB[(p + i) % q], self._LB[(p + i) % q]
+                sysm.advect_combine(t, fb, lb, a=0.0, b=1.0)
+                ii = (p + i) % q
+                sysm.bdf_step(dt, 1, BDF_MOMN, [0.0, 1.0], [0.0], 0.0, [fb], fb, [lb],
+                              [self._UR[ii]], [self._LR[ii]], self._UN)
+
+    def _bdf_kernels(self, t, dt, p):
+        from .adgfs import BDF_DIST, BDF_MOMN, BDF_MOMU
+        sysm, q = self.system, self.q
+        order = [(p + i) % q for i in range(q)]
+        fb = [self._FB[i] for i in order]
+        lb = [self._LB[i] for i in order]
+        sysm.advect_combine(t, fb[-1], lb[-1], a=0.0, b=1.0)             # L_n = L(f_n)
+        sysm.bdf_step(dt, q, BDF_MOMN | BDF_MOMU | BDF_DIST, self.bdf_A, [-x for x in self.bdf_G],
+                      self.bdf_B, fb, fb[0], lb, [self._UR[i] for i in order],
+                      [self._LR[i] for i in order], self._UN)
+
+    def step(self, t, dt):
+        if self._nstart < self.q - 1:
+            self._startup(t, dt)
+            return
+        p = self._phase
+        if not self.use_graph:
+            self._bdf_kernels(t, dt, p)
+        elif (p, dt) in self._graphs:
+            self._graphs[(p, dt)].replay()
+        else:
+            s = torch.cuda.Stream(device=self.backend.device)
+            s.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(s):
+                self._bdf_kernels(t, dt, p)                     # the real step
+            torch.cuda.current_stream().wait_stream(s)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._bdf_kernels(t, dt, p)
+            self._graphs[(p, dt)] = g
+        self._idxcurr = self._FB[p]
+        self._phase = (p + 1) % self.q
+
+
+class BDF2AstdStepper(BDFqAstdStepper):
+    stepper_name = 'adgfs-bdf-2'
+    order = q = 2
+    bdf_A = [1. / 3., -4. / 3., 1.]
+    bdf_G = [-2. / 3., 4. / 3.]
+    bdf_B = 2. / 3.
+    nstepsInit = 10
+    nregs = 5
+
+
+class BDF3AstdStepper(BDFqAstdStepper):
+    stepper_name = 'adgfs-bdf-3'
+    order = q = 3
+    bdf_A = [-2. / 11., 9. / 11., -18. / 11., 1.]
+    bdf_G = [6. / 11., -18. / 11., 18. / 11.]
+    bdf_B = 6. / 11.
+    nstepsInit = 100
+    nregs = 7
+
+
 STEPPERS = {c.stepper_name: c for c in (StdEulerDGFSStepper, StdTVDRK2DGFSStepper,
-                                        ARS111AstdStepper, ARS222AstdStepper, ARS443AstdStepper)}
+                                        ARS111AstdStepper, ARS222AstdStepper, ARS443AstdStepper,
+                                        BDF1AstdStepper, BDF2AstdStepper, BDF3AstdStepper)}
 
 
 def get_integrator(backend, system_or_factory, cfg):

@@ -437,6 +437,45 @@ int32_t bdgfs_esbgk_moments(const void* f, int64_t ndof, int32_t Nv,
 int32_t bdgfs_esbgk_gaussian(const double* U, int64_t ndof, int32_t Nv,
                              int32_t fp64, const double* c0, double Pr,
                              void* M, void* stream);
+/* One IMEX-BDF step of the 'adgfs' system (BDF2/BDF3AstdStepper.step,
+ * frfs/integrators/std/steppers.py:680-860: updateMom{q}_BDF,
+ * constructMaxwellian and updateDistribution{q}_BDF of
+ * kernels/scattering/{bgk,esbgk,shakov}-direct-gll.mako and
+ * linear-common-direct-gll.mako:40-88).  With X_0..X_{q-1} oldest to
+ * newest: N = -sum_i (a_i X_i + g_i dt LX_i); the new moments U = N/a_q for
+ * the conserved five (higher ones relax implicitly as in the reference) and
+ * f = (N_f + b dt nu M[U]) / (a_q + b dt nu).  g_i are the reference's
+ * arguments (the negated G coefficients). */
+#define BDGFS_BDF_MOMN 1     /* reduce U[q-1], LU[q-1] from f[q-1], L[q-1]  */
+#define BDGFS_BDF_MOMU 2     /* form Unew                                    */
+#define BDGFS_BDF_DIST 4     /* write fout                                   */
+typedef struct bdgfs_bdf_args {
+    int64_t ndof;
+    int32_t Nv;
+    int32_t fp64;
+    const double* c0;        /* [Nv] (FP64)                                  */
+    double cw;
+    double prefac;           /* nu = prefac rho T^(1 - omega)                */
+    double omega;
+    double dt;
+    int32_t q;               /* history length 1..3                          */
+    int32_t model;           /* BDGFS_ARS_BGK / _ESBGK / _SHAKOV             */
+    double Pr;
+    double a[4];             /* a_0..a_q                                     */
+    double g[3];             /* g_0..g_{q-1}                                 */
+    double b;
+    const void* f[3];        /* distributions f_0..f_{q-1} ([ndof][Nv^3])    */
+    const void* L[3];        /* explicit parts L_0..L_{q-1}                  */
+    double* U[3];            /* moment rows of f_i ([ndof][5, 11 or 14])     */
+    double* LU[3];           /* moment rows of L_i                           */
+    double* Unew;            /* new moment rows (written with MOMU, read
+                                otherwise)                                   */
+    void* fout;              /* new distribution (may alias f[0])            */
+    int32_t flags;
+    int32_t pad_;
+} bdgfs_bdf_args;
+int32_t bdgfs_bdf_step(const bdgfs_bdf_args* a, void* stream);
+
 /* Shakov ('shakov-direct-gll', frfs/solvers/adgfs/scattering.py,
  * ADGFSShakovDirectGLLScatteringModel): U[dof][14] = the 11 ES-BGK moments
  * followed by {|c|^2 c} cw, and S[dof] = M (1 + 2 (1 - Pr)/5 (q.d)/(rho T^2)

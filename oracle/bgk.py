@@ -287,3 +287,71 @@ def step_ars_sk(f0, dt, L, scheme, prefac, omega, Pr, cv, cw):
         num = num + A[ar][ar] * dt * nar * shakov_target(U[ar], Pr, cv)
         F.append(num / (1.0 + A[ar][ar] * dt * nar))
     return F[s]
+
+
+# ---------------------------------------------------------------------------
+# IMEX-BDF steppers ('adgfs-bdf-1/2/3', frfs/integrators/std/steppers.py:675-860)
+#   moments  N = -sum_i (a_i U_i + g_i dt LU_i); U = N / a_q (conserved five);
+#            second moments (ES-BGK: rate b nu/Pr, Shakov: b nu) and the Shakov
+#            heat flux (denominator a_q + Pr b dt nu) relax implicitly
+#            (updateMom{q}_BDF of the three scattering .mako files)
+#   dist     f = (-sum_i (a_i f_i + g_i dt L_i) + b dt nu M[U]) / (a_q + b dt nu)
+#            (updateDistribution{q}_BDF, linear-common-direct-gll.mako:40-88)
+#   start    the first q - 1 steps: nstepsInit ARS-222 sub-steps each
+BDF = {2: ([1. / 3., -4. / 3., 1.], [-2. / 3., 4. / 3.], 2. / 3., 10),
+       3: ([-2. / 11., 9. / 11., -18. / 11., 1.], [6. / 11., -18. / 11., 18. / 11.], 6. / 11., 100)}
+
+MODELS = {
+    'bgk': (moments5, lambda U, Pr, cv: maxwellian(U, cv)),
+    'esbgk': (moments11, es_gaussian),
+    'shakov': (moments14, shakov_target),
+}
+
+
+def bdf_update(fs, Ls, Us, LUs, a, g, b, dt, prefac, omega, Pr, cv, model):
+    """One BDF update from histories (oldest first); returns (U_new, f_new).
+    g are the coefficients as passed to the reference kernels (-G)."""
+    q = len(fs)
+    N = -sum(a[i] * Us[i] + g[i] * dt * LUs[i] for i in range(q))
+    U = N / a[q]
+    rate = nu(U, prefac, omega)[..., None]
+    if model == 'esbgk':
+        w = b * dt * rate / Pr
+        U[..., 5:11] = (N[..., 5:11] + w * _es_targets(U)) / (a[q] + w)
+    if model == 'shakov':
+        w = b * dt * rate
+        U[..., 5:11] = (N[..., 5:11] + w * _es_targets(U)) / (a[q] + w)
+        U[..., 11:14] = (N[..., 11:14] + w * _heat_targets(U, Pr)) / (a[q] + Pr * w)
+    M = MODELS[model][1](U, Pr, cv)
+    Nf = -sum(a[i] * fs[i] + g[i] * dt * Ls[i] for i in range(q))
+    return U, (Nf + b * dt * rate * M) / (a[q] + b * dt * rate)
+
+
+def run_bdf(f0, dt, L, nsteps, q, prefac, omega, Pr, cv, cw, model='bgk'):
+    """nsteps calls of the BDF-q stepper from f0: the first q - 1 calls take
+    nstepsInit ARS-222 sub-steps of dt / nstepsInit, then BDF steps."""
+    A, G, b, ninit = BDF[q]
+    g = [-x for x in G]
+    mom = MODELS[model][0]
+
+    def ars(f, h):
+        if model == 'bgk':
+            return step_ars(f, h, L, 'adgfs-ars-222', prefac, omega, cv, cw)
+        if model == 'esbgk':
+            return step_ars_es(f, h, L, 'adgfs-ars-222', prefac, omega, Pr, cv, cw)
+        return step_ars_sk(f, h, L, 'adgfs-ars-222', prefac, omega, Pr, cv, cw)
+    hist = [f0]
+    f = f0
+    for k in range(nsteps):
+        if k < q - 1:
+            for _ in range(ninit):
+                f = ars(f, dt / ninit)
+            hist.append(f)
+            continue
+        fs = hist[-q:]
+        Ls = [L(x) for x in fs]
+        Us = [mom(x, cv, cw) for x in fs]
+        LUs = [mom(x, cv, cw) for x in Ls]
+        _, f = bdf_update(fs, Ls, Us, LUs, A, g, b, dt, prefac, omega, Pr, cv, model)
+        hist.append(f)
+    return f

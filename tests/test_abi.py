@@ -38,6 +38,7 @@ STRUCTS = {
     'bdgfs_gemm_args': _lib.GemmArgs,
     'bdgfs_hybrid_args': _lib.HybridArgs,
     'bdgfs_ars_args': _lib.ArsArgs,
+    'bdgfs_bdf_args': _lib.BdfArgs,
 }
 
 

@@ -173,3 +173,20 @@ def test_shakov_ars_order(scheme, order):
     ref = run(512)
     rate = np.log2(np.linalg.norm(run(8) - ref) / np.linalg.norm(run(16) - ref))
     assert rate > order - 0.3, rate
+
+
+@pytest.mark.parametrize('q', [2, 3])
+@pytest.mark.parametrize('model', ['bgk', 'esbgk', 'shakov'])
+def test_bdf_order(q, model):
+    """The oracle BDF-q stepper (ARS-222 start-up) reaches order q."""
+    from oracle.bgk import run_bdf
+    cv, cw = _grid()
+    f0 = _f0(cv)[None]
+    L = lambda f: -0.7 * f
+    T = 0.4
+
+    def run(n):
+        return run_bdf(f0, T / n, L, n, q, 2.0, 0.81, 2.0 / 3.0, cv, cw, model)
+    ref = run(128)
+    rate = np.log2(np.linalg.norm(run(16) - ref) / np.linalg.norm(run(32) - ref))
+    assert rate > q - 0.3, rate

@@ -278,3 +278,58 @@ def test_shakov_single_precision_and_pr_one(cuda):
     ub = step_ars(u1, 2e-3, orc1.rhs, 'adgfs-ars-222', s1.sm._prefactor, s1.sm._omega, cv,
                   s1.vm.cw())
     assert rel_l2(s1.eles_scal_upts_inb_full[0].double().cpu().numpy(), ub) < 1e-11
+
+
+@pytest.mark.parametrize('scheme,model', [
+    ('adgfs-bdf-2', 'bgk-direct-gll'), ('adgfs-bdf-3', 'bgk-direct-gll'),
+    ('adgfs-bdf-2', 'esbgk-direct-gll'), ('adgfs-bdf-3', 'esbgk-direct-gll'),
+    ('adgfs-bdf-2', 'shakov-direct-gll'), ('adgfs-bdf-3', 'shakov-direct-gll')])
+def test_bdf_steps_match_oracle(cuda, scheme, model):
+    """BDF-2/3 (ARS-222 start-up, then graph-replayed BDF steps over every
+    ring phase) vs the oracle stepper, FP64."""
+    from oracle.bgk import run_bdf
+    from oracle.fr import velocities
+    from frfs_b200.integrators import STEPPERS
+    q = int(scheme[-1])
+    cfg = _cfg(scheme)
+    cfg.set('scattering-model', 'type', model)
+    be, s = _system(cfg, STEPPERS[scheme].nregs)
+    _perturb(s, 8)
+    orc = _fr_oracle(s, 'quad', 2)
+    cv = velocities(s.vm.c0())
+    u0 = s.eles_scal_upts_inb_full[0].double().cpu().numpy()
+    integ = get_integrator(be, s, cfg)
+    dt, nsteps = 2e-3, q + 3
+    for _ in range(nsteps):
+        integ.step(0.0, dt)
+    torch.cuda.synchronize()
+    mdl = {'bgk-direct-gll': 'bgk', 'esbgk-direct-gll': 'esbgk', 'shakov-direct-gll': 'shakov'}[model]
+    uo = run_bdf(u0, dt, orc.rhs, nsteps, q, s.sm._prefactor, s.sm._omega, s.sm._Pr, cv, s.vm.cw(),
+                 mdl)
+    assert rel_l2(integ.soln.double().cpu().numpy(), uo) < 1e-11
+
+
+def test_bdf_reference_methods_equal_fused_step(cuda):
+    """updateMomentBDF + updateDistBDF (the reference's calls, BDF2 order of
+    arguments) give the fused bdgfs_bdf_step's result."""
+    from frfs_b200.adgfs import BDF_DIST, BDF_MOMN, BDF_MOMU
+    from frfs_b200.integrators import BDF2AstdStepper as B
+    cfg = _es_cfg('adgfs-bdf-2')
+    be, s = _system(cfg, 6)
+    _perturb(s, 9)
+    s.get_nregs_moms(6)
+    s.eles_scal_upts_inb_full[1].copy_(s.eles_scal_upts_inb_full[0] * 0.97)
+    s.advect_combine(0.0, 0, 2, a=0.0, b=1.0)
+    s.advect_combine(0.0, 1, 3, a=0.0, b=1.0)
+    for f, m in ((0, 0), (2, 1), (1, 2), (3, 3)):
+        s.moment(0.0, f, m)
+    a, g, b, dt = B.bdf_A, [-x for x in B.bdf_G], B.bdf_B, 2e-3
+    # reference order: f_0 = bank 1 (older), f_1 = bank 0 (newer)
+    s.updateMomentBDF(dt, a[0], 2, g[0], 3, a[1], 0, g[1], 1, a[2], 4, b)
+    s.updateDistBDF(dt, a[0], 1, g[0], 3, a[1], 0, g[1], 2, b, None, a[2], 4, 4)
+    ref = s.eles_scal_upts_inb_full[4].clone()
+    Uref = s.eles_scal_upts_inb_moms[4].clone()
+    s.bdf_step(dt, 2, BDF_MOMN | BDF_MOMU | BDF_DIST, a, g, b, [1, 0], 5, [3, 2], [2, 0], [3, 1], 5)
+    torch.cuda.synchronize()
+    assert torch.equal(s.eles_scal_upts_inb_moms[5], Uref)
+    assert torch.equal(s.eles_scal_upts_inb_full[5], ref)
