@@ -26,7 +26,7 @@ EXPORTS = (
     'bdgfs_hybrid_project_scatter', 'bdgfs_hybrid_heads',
     'bdgfs_bgk_moments', 'bdgfs_bgk_maxwellian', 'bdgfs_ars_stage',
     'bdgfs_esbgk_moments', 'bdgfs_esbgk_gaussian', 'bdgfs_shakov_moments', 'bdgfs_shakov_target',
-    'bdgfs_bdf_step',
+    'bdgfs_bdf_step', 'bdgfs_vss_scratch_bytes', 'bdgfs_vss_collide',
 )
 
 
@@ -109,6 +109,14 @@ class ArsArgs(C.Structure):
                 ('model', C.c_int32), ('pad_', C.c_int32), ('Pr', C.c_double)]
 
 
+class VssArgs(C.Structure):
+    _fields_ = [('Nv', C.c_int32), ('nspcs', C.c_int32), ('Nrho', C.c_int32), ('M', C.c_int32),
+                ('ndof', C.c_int64), ('fp64', C.c_int32), ('pad_', C.c_int32),
+                ('f', C.c_void_p * 4), ('Q', C.c_void_p * 4), ('mfrac', C.c_void_p),
+                ('prefac', C.c_void_p), ('rfac', C.c_void_p), ('rw', C.c_void_p),
+                ('sz', C.c_void_p), ('b', C.c_void_p), ('c', C.c_void_p)]
+
+
 class BdfArgs(C.Structure):
     _fields_ = [('ndof', C.c_int64), ('Nv', C.c_int32), ('fp64', C.c_int32),
                 ('c0', C.c_void_p), ('cw', C.c_double), ('prefac', C.c_double),
@@ -131,6 +139,7 @@ def lib():
             raise BdgfsError(f'{LIBPATH} not built: run python -m frfs_b200.build')
         L = C.CDLL(LIBPATH)
         L.bdgfs_vhs_scratch_bytes.restype = C.c_size_t
+        L.bdgfs_vss_scratch_bytes.restype = C.c_size_t
         L.bdgfs_vhs_scratch_bytes.argtypes = [C.POINTER(VhsGrid), C.c_int32, C.c_int32]
         L.bdgfs_vhs_collide.restype = C.c_int32
         L.bdgfs_vhs_collide.argtypes = [C.POINTER(VhsGrid), C.c_int32, C.POINTER(VhsBatch),
@@ -170,6 +179,8 @@ def lib():
             'bdgfs_shakov_moments': [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_double, vp, vp],
             'bdgfs_shakov_target': [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_double, vp, vp],
             'bdgfs_bdf_step': [vp, vp],
+            'bdgfs_vss_scratch_bytes': [C.c_int32, C.c_int32, C.c_int32],
+            'bdgfs_vss_collide': [vp, vp, C.c_size_t, vp],
             'bdgfs_colsum': [vp, i64, i64, vp, vp],
             'bdgfs_adamw': [vp, vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float,
                             C.c_float, C.c_float, i64, vp],

@@ -1,0 +1,269 @@
+// Fast-spectral VSS collision operator of a gas mixture on one velocity grid:
+// Q_p = sum_q Q_pq(f_p, f_q) for every species p of every distribution.
+//
+// Reference: DGFSBiVSSGLLScatteringModel.Qij / fs (frfs/solvers/dgfsbi/
+// scattering.py:229-330) and its kernels r2z, cosSinMul_pq, prod,
+// computeQG, ax2, output_pq (frfs/solvers/dgfsbi/kernels/scattering/
+// vss-gll.mako:100-300).  Per pair (p, q), with F = FFT(f_p)/n,
+// G = FFT(f_q)/n and a = pi/L qz_r (s . l):
+//   t1 = e^{+i a m_q/(m_p+m_q)} F,  t2 = e^{-i a m_p/(m_p+m_q)} G
+//   G^ += w_r b_pq[r, s] FFT(IFFT(t1) IFFT(t2))          (all r, s)
+//   Q_pq = prefac_pq (Re IFFT(G^) - f_p Re IFFT(c_pq G))
+//
+// The reference runs 9 launches and 6 cuFFT executions per pair and
+// distribution, each over the full P = Nrho M slab of scratch.  Here one
+// persistent CTA owns a (distribution, species p) item and walks the P
+// slices one at a time through five pencil passes over CTA-private scratch
+// (L2 resident), with the DFTs in registers (generated codelets):
+//   A  x: phase (separable: e^{i a} = Ex[lx] Ey[ly] Ez[lz], tables in shared
+//         memory) and inverse DFT of t1 and t2
+//   B  y: inverse DFT of both
+//   C  z: inverse DFT of both, the product T, forward DFT of T
+//   D  y: forward DFT of T
+//   E  x: forward DFT of T and G^ += w_r prefac_pq b_pq T^
+// The gain and loss terms of all partners q are linear, so they are summed
+// in the spectral domain and transformed back once per item.
+#include "common.cuh"
+#include "fft_codelets.cuh"
+
+namespace bdgfs {
+
+namespace {
+
+template <typename T, int N>
+struct VssCfg {
+    static constexpr int n = N * N * N;
+    // one pencil per thread up to 256 pencils; 2 (24^3) or 4 (32^3) per
+    // thread above, so a pencil pass keeps its N complex values in registers
+    static constexpr int threads = sizeof(T) == 4 ? (N * N <= 256 ? N * N : N == 24 ? 288 : 256)
+                                                  : N * N / ((N * N + 255) / 256);
+};
+
+// pencil pc of axis AX: first element and stride ([x][y][z], z fastest)
+template <int N, int AX>
+__device__ __forceinline__ void pencil(int pc, int& base, int& stride)
+{
+    if constexpr (AX == 0) { base = pc; stride = N * N; }                            // (y, z)
+    else if constexpr (AX == 1) { base = (pc / N) * N * N + (pc % N); stride = N; }  // (x, z)
+    else { base = pc * N; stride = 1; }                                              // (x, y)
+}
+
+// DFT (SIGN < 0 forward, > 0 inverse, unnormalised) of every pencil of
+// axis AX of A, in place, times scale
+template <typename T, int N, int SIGN, int AX>
+__device__ __forceinline__ void pass(cpx<T>* __restrict__ A, T scale = T(1))
+{
+    for (int pc = threadIdx.x; pc < N * N; pc += blockDim.x) {
+        int b, s;
+        pencil<N, AX>(pc, b, s);
+        cpx<T> x[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) x[k] = A[b + k * s];
+        dft<N, SIGN>(x);
+#pragma unroll
+        for (int k = 0; k < N; ++k) A[b + k * s] = cpx<T>{x[k].x * scale, x[k].y * scale};
+    }
+}
+
+// 3-D forward DFT of a real row into A, scaled by 1/n
+template <typename T, int N>
+__device__ __forceinline__ void fft_real(const T* __restrict__ f, cpx<T>* __restrict__ A)
+{
+    for (int pc = threadIdx.x; pc < N * N; pc += blockDim.x) {
+        cpx<T> x[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) x[k] = cpx<T>{f[pc * N + k], T(0)};
+        dft<N, -1>(x);
+#pragma unroll
+        for (int k = 0; k < N; ++k) A[pc * N + k] = x[k];
+    }
+    __syncthreads();
+    pass<T, N, -1, 1>(A);
+    __syncthreads();
+    pass<T, N, -1, 0>(A, T(1.0 / double(N * N * N)));
+    __syncthreads();
+}
+
+__device__ __forceinline__ int lfreq(int k, int N) { return k < N / 2 ? k : k - N; }
+
+template <typename T>
+__device__ __forceinline__ cpx<T> cmul(cpx<T> a, cpx<T> b)
+{
+    return cpx<T>{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(VssCfg<T, N>::threads) vss_kernel(const bdgfs_vss_args g,
+                                                                     cpx<T>* __restrict__ scratch)
+{
+    constexpr int n = VssCfg<T, N>::n;
+    __shared__ cpx<T> E1[3][N], E2[3][N];
+    cpx<T>* F = scratch + size_t(blockIdx.x) * 6 * n;
+    cpx<T>* Gq = F + n;
+    cpx<T>* Z1 = F + 2 * n;
+    cpx<T>* Z2 = F + 3 * n;
+    cpx<T>* Ga = F + 4 * n;
+    cpx<T>* La = F + 5 * n;
+    const int S = g.nspcs, P = g.Nrho * g.M;
+    const int64_t nitems = g.ndof * S;
+    for (int64_t item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int p = int(item / g.ndof);
+        const int64_t dof = item - int64_t(p) * g.ndof;
+        const T* fp = static_cast<const T*>(g.f[p]) + dof * n;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            Ga[i] = cpx<T>{T(0), T(0)};
+            La[i] = cpx<T>{T(0), T(0)};
+        }
+        fft_real<T, N>(fp, F);
+        for (int q = 0; q < S; ++q) {
+            const int pq = p * S + q;
+            const cpx<T>* G = F;
+            if (q != p) {
+                fft_real<T, N>(static_cast<const T*>(g.f[q]) + dof * n, Gq);
+                G = Gq;
+            }
+            const T pref = T(g.prefac[pq]);
+            const cpx<T>* cq = static_cast<const cpx<T>*>(g.c) + size_t(pq) * n;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                const cpx<T> t = cmul(cq[i], G[i]);
+                La[i].x += pref * t.x;
+                La[i].y += pref * t.y;
+            }
+            const double mq = g.mfrac[pq], mp = 1.0 - mq;
+            const cpx<T>* bq = static_cast<const cpx<T>*>(g.b) + size_t(pq) * P * n;
+            for (int rs = 0; rs < P; ++rs) {
+                const int r = rs / g.M, s = rs - r * g.M;
+                __syncthreads();
+                // separable phase tables e^{+i mq a_d l}, e^{-i mp a_d l} per axis
+                for (int i = threadIdx.x; i < 6 * N; i += blockDim.x) {
+                    const int w = i / (3 * N), d = (i / N) % 3, k = i % N;
+                    const double ang = g.rfac[r] * g.sz[3 * s + d] * lfreq(k, N) * (w ? -mp : mq);
+                    double sn, cs;
+                    sincos(ang, &sn, &cs);
+                    (w ? E2 : E1)[d][k] = cpx<T>{T(cs), T(sn)};
+                }
+                __syncthreads();
+                // A: phases and inverse DFT along x
+                for (int pc = threadIdx.x; pc < N * N; pc += blockDim.x) {
+                    const int y = pc / N, z = pc % N;
+                    const cpx<T> e1 = cmul(E1[1][y], E1[2][z]), e2 = cmul(E2[1][y], E2[2][z]);
+                    cpx<T> x[N];
+#pragma unroll
+                    for (int k = 0; k < N; ++k) x[k] = cmul(cmul(E1[0][k], e1), F[pc + k * N * N]);
+                    dft<N, +1>(x);
+#pragma unroll
+                    for (int k = 0; k < N; ++k) Z1[pc + k * N * N] = x[k];
+#pragma unroll
+                    for (int k = 0; k < N; ++k) x[k] = cmul(cmul(E2[0][k], e2), G[pc + k * N * N]);
+                    dft<N, +1>(x);
+#pragma unroll
+                    for (int k = 0; k < N; ++k) Z2[pc + k * N * N] = x[k];
+                }
+                __syncthreads();
+                // B: inverse DFT along y
+                pass<T, N, +1, 1>(Z1);
+                pass<T, N, +1, 1>(Z2);
+                __syncthreads();
+                // C: inverse DFT along z, product, forward DFT along z
+                for (int pc = threadIdx.x; pc < N * N; pc += blockDim.x) {
+                    cpx<T> x[N];
+#pragma unroll
+                    for (int k = 0; k < N; ++k) x[k] = Z1[pc * N + k];
+                    dft<N, +1>(x);
+#pragma unroll
+                    for (int k = 0; k < N; ++k) Z1[pc * N + k] = x[k];
+#pragma unroll
+                    for (int k = 0; k < N; ++k) x[k] = Z2[pc * N + k];
+                    dft<N, +1>(x);
+#pragma unroll
+                    for (int k = 0; k < N; ++k) x[k] = cmul(Z1[pc * N + k], x[k]);
+                    dft<N, -1>(x);
+#pragma unroll
+                    for (int k = 0; k < N; ++k) Z1[pc * N + k] = x[k];
+                }
+                __syncthreads();
+                // D: forward DFT along y
+                pass<T, N, -1, 1>(Z1);
+                __syncthreads();
+                // E: forward DFT along x, weighted kernel product into G^
+                const T w = T(g.rw[r]) * pref;
+                const cpx<T>* brs = bq + size_t(rs) * n;
+                for (int pc = threadIdx.x; pc < N * N; pc += blockDim.x) {
+                    cpx<T> x[N];
+#pragma unroll
+                    for (int k = 0; k < N; ++k) x[k] = Z1[pc + k * N * N];
+                    dft<N, -1>(x);
+#pragma unroll
+                    for (int k = 0; k < N; ++k) {
+                        const int i = pc + k * N * N;
+                        const cpx<T> t = cmul(brs[i], x[k]);
+                        Ga[i].x += w * t.x;
+                        Ga[i].y += w * t.y;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        // back to velocity space: Q_p = Re IFFT(G^) - f_p Re IFFT(L^)
+        pass<T, N, +1, 2>(Ga);
+        pass<T, N, +1, 2>(La);
+        __syncthreads();
+        pass<T, N, +1, 1>(Ga);
+        pass<T, N, +1, 1>(La);
+        __syncthreads();
+        pass<T, N, +1, 0>(Ga);
+        pass<T, N, +1, 0>(La);
+        __syncthreads();
+        T* Qp = static_cast<T*>(g.Q[p]) + dof * n;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) Qp[i] = Ga[i].x - fp[i] * La[i].x;
+        __syncthreads();
+    }
+}
+
+template <typename T, int N>
+int vss_launch(const bdgfs_vss_args* a, void* scratch, size_t bytes, cudaStream_t st)
+{
+    constexpr int n = VssCfg<T, N>::n;
+    const size_t per = size_t(6) * n * sizeof(cpx<T>);
+    const int64_t nitems = a->ndof * a->nspcs;
+    const int64_t ctas = int64_t(bytes / per) < nitems ? int64_t(bytes / per) : nitems;
+    if (ctas < 1) return BDGFS_ESCRATCH;
+    vss_kernel<T, N><<<unsigned(ctas > 65535 ? 65535 : ctas), VssCfg<T, N>::threads, 0, st>>>(
+        *a, static_cast<cpx<T>*>(scratch));
+    return cuda_status(cudaGetLastError());
+}
+
+}  // namespace
+
+}  // namespace bdgfs
+
+using namespace bdgfs;
+
+extern "C" size_t bdgfs_vss_scratch_bytes(int32_t Nv, int32_t fp64, int32_t nctas)
+{
+    if (Nv < 1 || Nv > 32 || nctas < 1) return 0;
+    const size_t n = size_t(Nv) * Nv * Nv;
+    return size_t(nctas) * 6 * n * (fp64 ? 16 : 8);
+}
+
+extern "C" int32_t bdgfs_vss_collide(const bdgfs_vss_args* a, void* scratch, size_t bytes, void* stream)
+{
+    if (!a || !scratch || a->nspcs < 1 || a->nspcs > 4 || a->ndof < 0 || a->Nrho < 1 || a->M < 1 ||
+        !a->mfrac || !a->prefac || !a->rfac || !a->rw || !a->sz || !a->b || !a->c)
+        return BDGFS_EINVAL;
+    for (int p = 0; p < a->nspcs; ++p)
+        if (!a->f[p] || !a->Q[p]) return BDGFS_EINVAL;
+    if (a->ndof == 0) return BDGFS_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+#define VSS_GO(NN)                                                                          \
+    if (a->Nv == NN)                                                                        \
+        return a->fp64 ? vss_launch<double, NN>(a, scratch, bytes, st)                      \
+                       : vss_launch<float, NN>(a, scratch, bytes, st);
+    VSS_GO(8)
+    VSS_GO(12)
+    VSS_GO(16)
+    VSS_GO(24)
+    VSS_GO(32)
+#undef VSS_GO
+    return BDGFS_EUNSUPPORTED;
+}

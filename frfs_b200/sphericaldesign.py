@@ -19,6 +19,11 @@ Built in (closed form):
           M = 12 is supplied here.
 Any other M: pass ``ssrule`` as a file path with 2M rows "x y z" (the
 reference's file format), the first M rows are used.
+
+The gas-mixture operator integrates over the full sphere
+(frfs/solvers/dgfsbi/velocitymesh.py:158-166): ``full_sphere_design(M)``
+is the M-point antipodal design, a built-in half design of M/2 points and
+its antipodes, or the M rows of a design file.
 """
 import os
 
@@ -64,3 +69,16 @@ def half_sphere_design(M, ssrule='womersley'):
         return _octahedral_5design_half()
     raise ValueError('No suitable spherical quadrature rule found '
                      f'(built-in M in 1, 3, 6, 12; got M={M}); pass a file')
+
+
+def full_sphere_design(M, ssrule='womersley'):
+    """M points of an antipodal design on the whole sphere."""
+    if ssrule and os.path.isfile(str(ssrule)):
+        pts = np.loadtxt(ssrule)[:, :3]
+        if pts.shape[0] != M:
+            raise ValueError(f'design file has {pts.shape[0]} points, need {M}')
+        return pts.copy()
+    if M % 2:
+        raise ValueError(f'built-in full-sphere designs have an even number of points (got M={M})')
+    half = half_sphere_design(M // 2)
+    return np.concatenate([half, -half])

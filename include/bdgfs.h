@@ -437,6 +437,42 @@ int32_t bdgfs_esbgk_moments(const void* f, int64_t ndof, int32_t Nv,
 int32_t bdgfs_esbgk_gaussian(const double* U, int64_t ndof, int32_t Nv,
                              int32_t fp64, const double* c0, double Pr,
                              void* M, void* stream);
+/* ------------------------------------------------------------------------
+ * Gas mixtures: fast-spectral VSS collision operator on one velocity grid
+ * ---------------------------------------------------------------------- */
+
+/* Q_p = sum_q Q_pq(f_p, f_q) for every species p and distribution
+ * (DGFSBiVSSGLLScatteringModel.fs, frfs/solvers/dgfsbi/scattering.py:
+ * 229-330; kernels/scattering/vss-gll.mako:100-300).  Tables (built on the
+ * host from the reference's precompute_a / precompute_bc_pq):
+ *   rfac[r] = pi/L qz_r, rw[r] = qw_r sw / Nv^3, sz = the M full-sphere
+ *   directions, mfrac[p*S+q] = m_q/(m_p+m_q), prefac[p*S+q],
+ *   b[p*S+q][r*M+s][Nv^3] and c[p*S+q][Nv^3] complex in the state's
+ *   precision (interleaved re, im). */
+typedef struct bdgfs_vss_args {
+    int32_t Nv;              /* 8, 12, 16, 24 or 32                          */
+    int32_t nspcs;           /* species, 1..4                                */
+    int32_t Nrho;
+    int32_t M;
+    int64_t ndof;            /* distributions per species                    */
+    int32_t fp64;
+    int32_t pad_;
+    const void* f[4];        /* real [ndof][Nv^3] per species                */
+    void* Q[4];              /* real [ndof][Nv^3] per species (written)      */
+    const double* mfrac;
+    const double* prefac;
+    const double* rfac;
+    const double* rw;
+    const double* sz;        /* [M][3]                                       */
+    const void* b;
+    const void* c;
+} bdgfs_vss_args;
+/* Scratch for nctas persistent CTAs: 6 complex Nv^3 arrays each.  The
+ * launch uses as many CTAs as the scratch holds (at most ndof * nspcs). */
+size_t bdgfs_vss_scratch_bytes(int32_t Nv, int32_t fp64, int32_t nctas);
+int32_t bdgfs_vss_collide(const bdgfs_vss_args* a, void* scratch, size_t bytes,
+                          void* stream);
+
 /* One IMEX-BDF step of the 'adgfs' system (BDF2/BDF3AstdStepper.step,
  * frfs/integrators/std/steppers.py:680-860: updateMom{q}_BDF,
  * constructMaxwellian and updateDistribution{q}_BDF of

@@ -151,3 +151,70 @@ ux = 0
 uy = 0
 uz = 0
 """ + '\n'.join(sects))
+
+
+def vss_cfg(Nv, Nrho, M, Mpre, masses=(39.96e-3, 83.798e-3), alpha=1.3, omega=0.81, dev=5,
+            precision='double'):
+    """Gas-mixture config of the 'vss-gll' model: every ordered species pair
+    with the same VSS parameters."""
+    S = len(masses)
+    pairs = '\n'.join(f'alpha{p}{q} = {alpha}\nomega{p}{q} = {omega}\ndRef{p}{q} = 4.17e-10\n'
+                      f'Tref{p}{q} = 273' for p in range(S) for q in range(S))
+    mm = '\n'.join(f'molarMass{p + 1} = {m}' for p, m in enumerate(masses))
+    return Inifile(f"""
+[backend]
+precision = {precision}
+[constants]
+Nv = {Nv}
+Nrho = {Nrho}
+[non-dim]
+T0 = {NONDIM['T0']}
+H0 = {NONDIM['H0']}
+rho0 = {NONDIM['rho0']}
+molarMass0 = {NONDIM['molarMass0']}
+[velocity-mesh]
+dev = {dev}
+cmax = 0
+Tmax = 273
+{mm}
+[spherical-design-rule]
+ssrule = womersley
+M = {M}
+[scattering-model]
+type = vss-gll
+Mpre = {Mpre}
+ssrulepre = womersley
+{pairs}
+""")
+
+
+def vss_oracle_for(sm):
+    """The oracle on the model's mesh, directions and pair parameters."""
+    from oracle.vss import BiVelocityMesh, VSSOracle
+    vm = sm.vm
+    ovm = BiVelocityMesh(vm.Nv(), vm.Nrho(), vm.sz(), vm.masses(), cmax=0.0, Tmax=NONDIM['T0'],
+                         dev=vm.L(), **NONDIM)
+    pairs = {}
+    for p in range(vm.nspcs()):
+        for q in range(vm.nspcs()):
+            pq = f'{p}{q}'
+            c = sm.cfg
+            pairs[(p, q)] = dict(alpha=c.getfloat('scattering-model', 'alpha' + pq),
+                                 omega=c.getfloat('scattering-model', 'omega' + pq),
+                                 dRef=c.getfloat('scattering-model', 'dRef' + pq),
+                                 Tref=c.getfloat('scattering-model', 'Tref' + pq))
+    return VSSOracle(ovm, sm._szpre, pairs)
+
+
+def mixture(cv, masses, rng, k=2):
+    """Seeded non-equilibrium distributions of each species: sums of
+    Maxwellians n (m/(pi T))^1.5 exp(-m |c-u|^2/T)."""
+    out = []
+    for m in masses:
+        f = 0.0
+        for _ in range(k):
+            n, T = rng.uniform(0.3, 1.2), rng.uniform(0.7, 1.3)
+            u = rng.uniform(-0.3, 0.3, size=3)[:, None]
+            f = f + n * (m / (np.pi * T))**1.5 * np.exp(-m * np.sum((cv - u)**2, axis=0) / T)
+        out.append(f)
+    return out

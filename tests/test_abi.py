@@ -39,6 +39,7 @@ STRUCTS = {
     'bdgfs_hybrid_args': _lib.HybridArgs,
     'bdgfs_ars_args': _lib.ArsArgs,
     'bdgfs_bdf_args': _lib.BdfArgs,
+    'bdgfs_vss_args': _lib.VssArgs,
 }
 
 
