@@ -502,6 +502,131 @@ def small_fp64(flush, steps=20):
             'dtype': 'f64'}
 
 
+MIXTURE = dict(Nv=24, Nrho=12, M=12, Mpre=12, ndof=1024, masses=(39.96e-3, 83.798e-3),
+               alpha=1.3, omega=0.81, dev=6)
+
+
+def mixture_ini(w=MIXTURE):
+    """Binary argon-krypton mixture, 'vss-gll' with the same VSS parameters
+    for every ordered species pair, FP32 state."""
+    S = len(w['masses'])
+    pairs = '\n'.join(f"alpha{p}{q} = {w['alpha']}\nomega{p}{q} = {w['omega']}\n"
+                      f"dRef{p}{q} = 4.17e-10\nTref{p}{q} = {NONDIM['T0']}"
+                      for p in range(S) for q in range(S))
+    mm = '\n'.join(f'molarMass{p + 1} = {m}' for p, m in enumerate(w['masses']))
+    return f"""
+[backend]
+precision = single
+[constants]
+Nv = {w['Nv']}
+Nrho = {w['Nrho']}
+[non-dim]
+T0 = {NONDIM['T0']}
+H0 = {NONDIM['H0']}
+rho0 = {NONDIM['rho0']}
+molarMass0 = {NONDIM['molarMass0']}
+[velocity-mesh]
+dev = {w['dev']}
+cmax = 0
+Tmax = {NONDIM['T0']}
+{mm}
+[spherical-design-rule]
+ssrule = womersley
+M = {w['M']}
+[scattering-model]
+type = vss-gll
+Mpre = {w['Mpre']}
+ssrulepre = womersley
+{pairs}
+"""
+
+
+def vss_mixture(flush, peak=None, reps=3, ndof=None, check=True):
+    """Gas-mixture collision operator ('vss-gll', Q_p = sum_q Q_pq for both
+    species of ndof distribution pairs, one launch): Q_p evals/s, FLOP-model
+    roofline and the error of the FP32 launch against the FP64 oracle on two
+    seeded pairs.  FLOP per (distribution, species) item with S species,
+    P = Nrho M slices and n = Nv^3: (S (3 P + 1) + 2) 5 n log2 n for the
+    FFTs (F and the partners' transforms, three 3-D transforms per slice,
+    two inverse transforms at the end) + 38 S P n for the phase, product and
+    kernel-weight arithmetic."""
+    import numpy as np
+    import torch
+    from frfs_b200.backend import CUDABackend
+    from frfs_b200.dgfsbi import DGFSBiVelocityMesh, DGFSBiVSSGLLScatteringModel
+    from frfs_b200.inifile import Inifile
+    w = dict(MIXTURE)
+    if ndof is not None:
+        w['ndof'] = ndof
+    cfg = Inifile(mixture_ini(w))
+    be = CUDABackend(cfg)
+    S = len(w['masses'])
+    vm = DGFSBiVelocityMesh(be, cfg, S)
+    sm = DGFSBiVSSGLLScatteringModel(be, cfg, vm)
+    n, nd = vm.vsize(), w['ndof']
+    # seeded sums of two Maxwellians n (m/(pi T))^1.5 exp(-m |c-u|^2/T) per
+    # species, n ~ U(0.3, 1.2), T ~ U(0.7, 1.3), |u_i| < 0.3, built on the device
+    rng = np.random.default_rng(11)
+    cv = torch.as_tensor(vm.cv(), dtype=torch.float64, device=be.device)
+    fs = []
+    for m in vm.masses():
+        f = torch.zeros((nd, n), dtype=torch.float64, device=be.device)
+        for _ in range(2):
+            dn = torch.as_tensor(rng.uniform(0.3, 1.2, nd), device=be.device)[:, None]
+            T = torch.as_tensor(rng.uniform(0.7, 1.3, nd), device=be.device)[:, None]
+            u = torch.as_tensor(rng.uniform(-0.3, 0.3, (nd, 3, 1)), device=be.device)
+            f += dn * (m / (np.pi * T))**1.5 * torch.exp(-m * ((cv[None] - u)**2).sum(1) / T)
+        fs.append(f.float())
+        del f
+    Qs = [torch.empty_like(f) for f in fs]
+    st = torch.cuda.current_stream()
+    sm.collide(fs, Qs)
+    torch.cuda.synchronize()
+    tot = 0.0
+    for _ in range(reps):
+        flush.fill_(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        sm.collide(fs, Qs)
+        b.record(st)
+        torch.cuda.synchronize()
+        tot += a.elapsed_time(b)
+    ms = tot / reps
+    P = vm.Nrho() * vm.M()
+    flop_item = (S * (3 * P + 1) + 2) * 5 * n * math.log2(n) + 38 * S * P * n
+    flop = flop_item * S * nd
+    res = {'workload': (f"binary gas mixture (molar masses {w['masses'][0]}, {w['masses'][1]} kg/mol), "
+                        f"'vss-gll' alpha={w['alpha']} omega={w['omega']}, Nv={w['Nv']}^3 on "
+                        f"[-{w['dev']},{w['dev']}]^3, Nrho={w['Nrho']}, M={w['M']} full-sphere "
+                        f"directions, Mpre={w['Mpre']}; {nd} distribution pairs, Q_p = sum_q Q_pq "
+                        f"for both species in one launch, FP32"),
+           'launch_ms': ms, 'q_p_evals_per_s': S * nd / (ms * 1e-3),
+           'flop_per_launch': flop, 'achieved_tflops': flop / (ms * 1e-3) / 1e12}
+    if peak:
+        res['frac_of_fp32_fma_probe'] = res['achieved_tflops'] / peak
+    if check:
+        sys.path.insert(0, ROOT)
+        from oracle.vss import BiVelocityMesh, VSSOracle
+        ovm = BiVelocityMesh(vm.Nv(), vm.Nrho(), vm.sz(), vm.masses(), cmax=0.0, Tmax=NONDIM['T0'],
+                             dev=vm.L(), **NONDIM)
+        prm = dict(alpha=w['alpha'], omega=w['omega'], dRef=4.17e-10, Tref=NONDIM['T0'])
+        orc = VSSOracle(ovm, sm._szpre, {(p, q): prm for p in range(S) for q in range(S)})
+        err, t_or = 0.0, 0.0
+        for d in (0, nd - 1):
+            t0 = time.perf_counter()
+            want = orc.Q([fs[p][d].double().cpu().numpy() for p in range(S)])
+            t_or += time.perf_counter() - t0
+            for p in range(S):
+                got = Qs[p][d].double().cpu().numpy()
+                err = max(err, float(np.linalg.norm(got - want[p]) / np.linalg.norm(want[p])))
+        res['q_rel_l2_err_vs_fp64_oracle'] = err
+        res['error_sample'] = 'distribution pairs 0 and ndof-1, both species, FP64 oracle (1 host core)'
+        res['oracle_s_per_pair_1core'] = t_or / 2
+    del fs, Qs
+    torch.cuda.empty_cache()
+    return res
+
+
 def ars_bgk(flush, steps=20):
     """adgfs system: the Couette workload's mesh and velocity grid (16 x 8
     quads P3, Nv=24^3, FP32) with BGK relaxation (omega 0.81) and the
@@ -931,6 +1056,7 @@ def run_gpu(args):
         extra['batched_q'] = bq
         del arrays
         extra['ars_bgk'] = ars_bgk(flush)
+        extra['vss_mixture'] = vss_mixture(flush, peak)
     if ws == 1 and not args.no_surrogate:
         c4, c5 = surrogate_legs(flush)
         extra['surrogate'] = c4
@@ -1138,6 +1264,14 @@ def run_ars_only():
     print(json.dumps(ars_bgk(flush)))
 
 
+def run_vss_only(ndof):
+    """The gas-mixture collision launch alone on ndof distribution pairs
+    (profiling case, no oracle check)."""
+    import torch
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device='cuda')
+    print(json.dumps(vss_mixture(flush, reps=2, ndof=ndof, check=False)))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -1161,6 +1295,8 @@ def main():
                          '(random surrogate with zero head scales)')
     ap.add_argument('--ars-only', action='store_true',
                     help='profiling case: the adgfs ARS-222 leg alone')
+    ap.add_argument('--vss-only', type=int, default=0, metavar='NDOF',
+                    help='profiling case: the gas-mixture collision launch on NDOF pairs')
     ap.add_argument('--fr-only', choices=['couette', 'cavity'],
                     help='profiling case: the FR kernels of one RK stage')
     args = ap.parse_args()
@@ -1177,6 +1313,8 @@ def main():
         print(json.dumps(res))
     elif args.ars_only:
         run_ars_only()
+    elif args.vss_only:
+        run_vss_only(args.vss_only)
     elif args.fr_only:
         run_fr_only(args.fr_only)
     elif args.impl == 'reference':
