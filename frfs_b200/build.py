@@ -45,7 +45,7 @@ def build(force=False, verbose=False):
     gen = os.path.join(CSRC, 'gen_fft.py')
     subprocess.check_call([sys.executable, gen])
     os.makedirs(OUTDIR, exist_ok=True)
-    objs = []
+    cmds, objs = [], []
     for src in sources():
         obj = os.path.join(OUTDIR, os.path.basename(src)[:-3] + '.o')
         cmd = [_nvcc(), *NVCC_FLAGS, '-I', os.path.join(ROOT, 'include'),
@@ -53,8 +53,12 @@ def build(force=False, verbose=False):
         if verbose:
             cmd.insert(1, '-Xptxas=-v')
             print(' '.join(cmd), flush=True)
-        subprocess.check_call(cmd)
+        cmds.append(cmd)
         objs.append(obj)
+    # one nvcc process per source, as many at once as there are host cores
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        list(ex.map(subprocess.check_call, cmds))
     tmp = LIB + '.tmp'
     subprocess.check_call([_nvcc(), '-shared', '-gencode',
                            'arch=compute_100a,code=sm_100a', *objs, '-o', tmp,

@@ -23,6 +23,12 @@
 //   E  x: forward DFT of T and G^ += w_r prefac_pq b_pq T^
 // The gain and loss terms of all partners q are linear, so they are summed
 // in the spectral domain and transformed back once per item.
+//
+// FP32 at Nv <= 24 keeps the two working transforms Z1, Z2 of a slice in
+// shared memory (rows of N + 1 complex values, so that the z pencils of a
+// warp fall on distinct bank pairs; 231.5 KB at 24^3): passes B-D then touch
+// no global memory, and per slice only F, G, b_pq and G^ travel through L2.
+// Other grids keep Z1, Z2 in the CTA's global scratch (rows of N).
 #include "common.cuh"
 #include "fft_codelets.cuh"
 
@@ -37,25 +43,30 @@ struct VssCfg {
     // thread above, so a pencil pass keeps its N complex values in registers
     static constexpr int threads = sizeof(T) == 4 ? (N * N <= 256 ? N * N : N == 24 ? 288 : 256)
                                                   : N * N / ((N * N + 255) / 256);
+    // Z1, Z2 in shared memory (row pitch N + 1) or in global scratch (pitch N)
+    static constexpr bool smem = sizeof(T) == 4 && N <= 24;
+    static constexpr int RP = smem ? N + 1 : N;
+    static constexpr size_t smem_bytes = smem ? size_t(2) * N * N * RP * sizeof(cpx<T>) : 0;
 };
 
-// pencil pc of axis AX: first element and stride ([x][y][z], z fastest)
-template <int N, int AX>
+// pencil pc of axis AX: first element and stride ([x][y][z], z fastest,
+// rows of RP >= N elements)
+template <int N, int AX, int RP = N>
 __device__ __forceinline__ void pencil(int pc, int& base, int& stride)
 {
-    if constexpr (AX == 0) { base = pc; stride = N * N; }                            // (y, z)
-    else if constexpr (AX == 1) { base = (pc / N) * N * N + (pc % N); stride = N; }  // (x, z)
-    else { base = pc * N; stride = 1; }                                              // (x, y)
+    if constexpr (AX == 0) { base = (pc / N) * RP + (pc % N); stride = N * RP; }     // (y, z)
+    else if constexpr (AX == 1) { base = (pc / N) * N * RP + (pc % N); stride = RP; } // (x, z)
+    else { base = pc * RP; stride = 1; }                                              // (x, y)
 }
 
 // DFT (SIGN < 0 forward, > 0 inverse, unnormalised) of every pencil of
 // axis AX of A, in place, times scale
-template <typename T, int N, int SIGN, int AX>
+template <typename T, int N, int SIGN, int AX, int RP = N>
 __device__ __forceinline__ void pass(cpx<T>* __restrict__ A, T scale = T(1))
 {
     for (int pc = threadIdx.x; pc < N * N; pc += blockDim.x) {
         int b, s;
-        pencil<N, AX>(pc, b, s);
+        pencil<N, AX, RP>(pc, b, s);
         cpx<T> x[N];
 #pragma unroll
         for (int k = 0; k < N; ++k) x[k] = A[b + k * s];
@@ -97,11 +108,17 @@ __global__ void __launch_bounds__(VssCfg<T, N>::threads) vss_kernel(const bdgfs_
                                                                      cpx<T>* __restrict__ scratch)
 {
     constexpr int n = VssCfg<T, N>::n;
+    constexpr int RP = VssCfg<T, N>::RP;       // row pitch of Z1, Z2
     __shared__ cpx<T> E1[3][N], E2[3][N];
+    extern __shared__ __align__(16) unsigned char vss_smem[];
     cpx<T>* F = scratch + size_t(blockIdx.x) * 6 * n;
     cpx<T>* Gq = F + n;
     cpx<T>* Z1 = F + 2 * n;
     cpx<T>* Z2 = F + 3 * n;
+    if constexpr (VssCfg<T, N>::smem) {
+        Z1 = reinterpret_cast<cpx<T>*>(vss_smem);
+        Z2 = Z1 + N * N * RP;
+    }
     cpx<T>* Ga = F + 4 * n;
     cpx<T>* La = F + 5 * n;
     const int S = g.nspcs, P = g.Nrho * g.M;
@@ -146,52 +163,54 @@ __global__ void __launch_bounds__(VssCfg<T, N>::threads) vss_kernel(const bdgfs_
                 // A: phases and inverse DFT along x
                 for (int pc = threadIdx.x; pc < N * N; pc += blockDim.x) {
                     const int y = pc / N, z = pc % N;
+                    const int zb = y * RP + z;           // (0, y, z) in Z1, Z2
                     const cpx<T> e1 = cmul(E1[1][y], E1[2][z]), e2 = cmul(E2[1][y], E2[2][z]);
                     cpx<T> x[N];
 #pragma unroll
                     for (int k = 0; k < N; ++k) x[k] = cmul(cmul(E1[0][k], e1), F[pc + k * N * N]);
                     dft<N, +1>(x);
 #pragma unroll
-                    for (int k = 0; k < N; ++k) Z1[pc + k * N * N] = x[k];
+                    for (int k = 0; k < N; ++k) Z1[zb + k * N * RP] = x[k];
 #pragma unroll
                     for (int k = 0; k < N; ++k) x[k] = cmul(cmul(E2[0][k], e2), G[pc + k * N * N]);
                     dft<N, +1>(x);
 #pragma unroll
-                    for (int k = 0; k < N; ++k) Z2[pc + k * N * N] = x[k];
+                    for (int k = 0; k < N; ++k) Z2[zb + k * N * RP] = x[k];
                 }
                 __syncthreads();
                 // B: inverse DFT along y
-                pass<T, N, +1, 1>(Z1);
-                pass<T, N, +1, 1>(Z2);
+                pass<T, N, +1, 1, RP>(Z1);
+                pass<T, N, +1, 1, RP>(Z2);
                 __syncthreads();
                 // C: inverse DFT along z, product, forward DFT along z
                 for (int pc = threadIdx.x; pc < N * N; pc += blockDim.x) {
                     cpx<T> x[N];
 #pragma unroll
-                    for (int k = 0; k < N; ++k) x[k] = Z1[pc * N + k];
+                    for (int k = 0; k < N; ++k) x[k] = Z1[pc * RP + k];
                     dft<N, +1>(x);
 #pragma unroll
-                    for (int k = 0; k < N; ++k) Z1[pc * N + k] = x[k];
+                    for (int k = 0; k < N; ++k) Z1[pc * RP + k] = x[k];
 #pragma unroll
-                    for (int k = 0; k < N; ++k) x[k] = Z2[pc * N + k];
+                    for (int k = 0; k < N; ++k) x[k] = Z2[pc * RP + k];
                     dft<N, +1>(x);
 #pragma unroll
-                    for (int k = 0; k < N; ++k) x[k] = cmul(Z1[pc * N + k], x[k]);
+                    for (int k = 0; k < N; ++k) x[k] = cmul(Z1[pc * RP + k], x[k]);
                     dft<N, -1>(x);
 #pragma unroll
-                    for (int k = 0; k < N; ++k) Z1[pc * N + k] = x[k];
+                    for (int k = 0; k < N; ++k) Z1[pc * RP + k] = x[k];
                 }
                 __syncthreads();
                 // D: forward DFT along y
-                pass<T, N, -1, 1>(Z1);
+                pass<T, N, -1, 1, RP>(Z1);
                 __syncthreads();
                 // E: forward DFT along x, weighted kernel product into G^
                 const T w = T(g.rw[r]) * pref;
                 const cpx<T>* brs = bq + size_t(rs) * n;
                 for (int pc = threadIdx.x; pc < N * N; pc += blockDim.x) {
+                    const int zb = (pc / N) * RP + pc % N;
                     cpx<T> x[N];
 #pragma unroll
-                    for (int k = 0; k < N; ++k) x[k] = Z1[pc + k * N * N];
+                    for (int k = 0; k < N; ++k) x[k] = Z1[zb + k * N * RP];
                     dft<N, -1>(x);
 #pragma unroll
                     for (int k = 0; k < N; ++k) {
@@ -228,7 +247,13 @@ int vss_launch(const bdgfs_vss_args* a, void* scratch, size_t bytes, cudaStream_
     const int64_t nitems = a->ndof * a->nspcs;
     const int64_t ctas = int64_t(bytes / per) < nitems ? int64_t(bytes / per) : nitems;
     if (ctas < 1) return BDGFS_ESCRATCH;
-    vss_kernel<T, N><<<unsigned(ctas > 65535 ? 65535 : ctas), VssCfg<T, N>::threads, 0, st>>>(
+    constexpr size_t sm = VssCfg<T, N>::smem_bytes;
+    if constexpr (sm > 0) {
+        const cudaError_t e = cudaFuncSetAttribute(vss_kernel<T, N>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    vss_kernel<T, N><<<unsigned(ctas > 65535 ? 65535 : ctas), VssCfg<T, N>::threads, sm, st>>>(
         *a, static_cast<cpx<T>*>(scratch));
     return cuda_status(cudaGetLastError());
 }
