@@ -225,3 +225,265 @@ class DGFSBiVSSGLLScatteringModel(DGFSBiScatteringModel):
         if len(args) != 2 * S:
             raise ValueError('Need to be equal')
         self.collide([a[elem, upt] for a in args[:S]], [a[elem, upt] for a in args[S:]])
+
+
+# ---------------------------------------------------------------------------
+# The 'dgfsbi' system: one FR advection per species on the shared mesh and
+# velocity grid, the mixture collision operator across species.
+# ---------------------------------------------------------------------------
+from .mesh import ElementGeometry                                      # noqa: E402
+from .system import (DGFSBCInters, DGFSBoundaries, DGFSElements,       # noqa: E402
+                     DGFSSystem, DGFSWallSpecularBCInters)
+from .util import npeval, subclass_where                               # noqa: E402
+
+
+class SpeciesMesh:
+    """One species' view of the mixture velocity mesh: the shared grid,
+    with that species' molar mass for its Maxwellians."""
+
+    def __init__(self, vm, p):
+        self._vm, self.species = vm, p
+
+    def __getattr__(self, k):
+        return getattr(self._vm, k)
+
+    def mass(self):
+        return self._vm.masses()[self.species]
+
+
+def species_maxwellian(vm, m, nden, T, u):
+    """nden (m/(pi T))^1.5 exp(-m |c - u|^2 / T) on the grid (non-dimensional;
+    frfs/solvers/dgfsbi/initcond.py:68-76)."""
+    return nden * (m / (np.pi * T))**1.5 * np.exp(-m * np.sum((vm.cv() - u)**2, axis=0) / T)
+
+
+class DGFSBiMaxwellianInitCondition:
+    """'maxwellian' of the 'dgfsbi' system (frfs/solvers/dgfsbi/initcond.py:
+    47-117): per species the number density nden{p+1} (over n0), the shared
+    T and (ux, uy, uz); walls use nden = 1.  Raises ``ValueError`` when the
+    grid does not hold a species' number density, velocity and temperature
+    to 1e-5 (the reference's support test)."""
+    model = 'maxwellian'
+
+    def __init__(self, backend, cfg, vm, name, wall=False):
+        self.vm, S = vm, vm.nspcs()
+        u0 = vm.u0()
+        self._nden = [1.0] * S if wall else [cfg.getfloat(name, f'nden{p + 1}') / vm.n0()
+                                             for p in range(S)]
+        self._T = cfg.getfloat(name, 'T') / vm.T0()
+        self._u = np.array([cfg.getfloat(name, k) / u0 for k in ('ux', 'uy', 'uz')]).reshape(3, 1)
+        m, cv, cw = vm.masses(), vm.cv(), vm.cw()
+        self._init_vals = []
+        for p in range(S):
+            f = species_maxwellian(vm, m[p], self._nden[p], self._T, self._u)
+            mcw = m[p] * cw
+            rho = np.sum(f) * mcw
+            u = cv @ f * mcw / rho
+            T = np.sum(f * np.sum((cv - u[:, None])**2, axis=0)) * (2.0 / 3.0 * mcw * m[p]) / rho
+            ok = (np.isclose(self._nden[p], rho / m[p], rtol=1e-5, atol=1e-5)
+                  and np.allclose(self._u[:, 0] * u0, u * u0, rtol=1e-5, atol=1e-5)
+                  and np.isclose(self._T * vm.T0(), T * vm.T0(), rtol=1e-5, atol=1e-5))
+            if not ok:
+                raise ValueError(f'Bulk properties not conserved for species {p}! Check Nv, dev')
+            self._init_vals.append(f)
+
+    def get_init_vals(self):
+        return self._init_vals
+
+    def unondim(self):
+        return self._u
+
+
+class _BiMaxwellianRows:
+    """Wall / inflow rows of one species (frfs/solvers/dgfsbi/inters.py)."""
+    wall = True
+
+    def _maxwellian(self):
+        vm = self.vm
+        bc = DGFSBiMaxwellianInitCondition(self.be, self.cfg, vm._vm, self.sect, wall=self.wall)
+        return bc.unondim()[:, 0], bc.get_init_vals()[vm.species]
+
+
+class DGFSBiWallDiffuseBCInters(_BiMaxwellianRows, DGFSBCInters):
+    """'dgfsbi-wall-diffuse' (inters.py:176-283): the diffuse wall with each
+    species' wall Maxwellian (nden = 1, that species' mass)."""
+    type = 'dgfsbi-wall-diffuse'
+    oracle_type = 'dgfs-wall-diffuse'
+
+    def load(self):
+        self.rows = [self._maxwellian()]
+
+
+class DGFSBiWallDiffuseCylBCInters(DGFSBCInters):
+    """'dgfsbi-wall-diffuse-cyl' (inters.py:679-759): U_w, T_w expressions of
+    the face-point location; f_w = exp(-m |c - U_w|^2/T_w) per face point."""
+    type = 'dgfsbi-wall-diffuse-cyl'
+    oracle_type = 'dgfs-wall-diffuse'
+
+    def load(self):
+        cfg, vm, geo = self.cfg, self.vm, self.geo
+        x = np.zeros((3, len(self.pts)))
+        for i, w in enumerate(self.pts):
+            e, f = geo.wall_fpts[w]
+            x[:geo.ndims, i] = geo.plocfpts[e, f]
+        env = cfg.items_as('constants', float)
+        env.update(x=x[0], y=x[1], z=x[2])
+
+        def ev(k):
+            v = npeval(cfg.getexpr(self.sect, k), env)
+            return np.broadcast_to(np.asarray(v, dtype=np.float64), (len(self.pts),))
+        U = np.stack([ev('ux'), ev('uy'), ev('uz')]) / vm.u0()
+        T = ev('T') / vm.T0()
+        m, cv = vm.mass(), vm.cv()
+        self.rows = [(U[:, i].copy(), np.exp(-m * np.sum((cv - U[:, i:i + 1])**2, axis=0) / T[i]))
+                     for i in range(len(self.pts))]
+
+    def point_rows(self):
+        return np.arange(len(self.pts), dtype=np.int64)
+
+
+class DGFSBiWallSpecularBCInters(DGFSWallSpecularBCInters):
+    """'dgfsbi-wall-specular' (inters.py:286-421)."""
+    type = 'dgfsbi-wall-specular'
+
+
+class DGFSBiInletBCInters(_BiMaxwellianRows, DGFSBCInters):
+    """'dgfsbi-inlet' (inters.py:424-495): u_R = f_in,p where (c - U_in).n < 0,
+    f_in,p with the section's nden{p+1}."""
+    type = 'dgfsbi-inlet'
+    kind = _lib.BC_INLET
+    wall = False
+
+    def load(self):
+        self.rows = [self._maxwellian()]
+
+
+class DGFSBiInletNormalShockBCInters(_BiMaxwellianRows, DGFSBCInters):
+    """'dgfsbi-inlet-normalshock' (inters.py:498-560): u_R = f_in,p where c.n < 0."""
+    type = 'dgfsbi-inlet-normalshock'
+    kind = _lib.BC_INLET
+    wall = False
+
+    def load(self):
+        self.rows = [(np.zeros(3), self._maxwellian()[1])]
+
+
+class DGFSBiOutletBCInters(DGFSBCInters):
+    """'dgfsbi-outlet' (inters.py:563-617): u_R = u_L."""
+    type = 'dgfsbi-outlet'
+    kind = _lib.BC_OUTLET
+
+
+class DGFSBiVanishBCInters(DGFSBCInters):
+    """'dgfsbi-vanish' (inters.py:620-676): u_R = 0 where c.n < 0."""
+    type = 'dgfsbi-vanish'
+    kind = _lib.BC_INLET
+
+
+class DGFSBiSpecies(DGFSSystem):
+    """The FR advection of one species: the 'dgfs' system's kernels and fused
+    stage on the shared geometry and operators, with this species' boundary
+    rows and register banks; no collision model of its own."""
+
+    def __init__(self, bi, p, nreg):
+        be = bi.backend
+        self.backend, self.cfg, self.mesh = be, bi.cfg, bi.mesh
+        self.vm = SpeciesMesh(bi.vm, p)
+        self.geo, self.ele, self.ndims = bi.geo, bi.ele, bi.geo.ndims
+        self.domain, self.transport, self._send_rows = None, None, {}
+        self.walls = DGFSBoundaries(be, self.geo, self.vm, self.cfg, self.geo.wall_names)
+        self.unitCFLdt = bi.unitCFLdt
+        E, U, nv = self.ele.neles, self.ele.nupts, self.vm.vsize()
+        self.eles_scal_upts_inb_full = [be.empty(E, U, nv) for _ in range(nreg)]
+        self._uf_rows = be.empty(E * self.ele.nfpts, nv)
+        self._uf = self._uf_rows.view(E, self.ele.nfpts, nv)
+        self._gen_kernels()
+
+    def collide(self, t, uinbank, foutbank):
+        raise NotImplementedError('a species collides through DGFSBiSystem.collide')
+
+
+class DGFSBiSystem:
+    """Drop-in for ``DGFSBiSystem`` (frfs/solvers/dgfsbi/system.py:17-264,
+    name 'dgfsbi').  ``species[p]`` advects species p (banks
+    ``species[p].eles_scal_upts_inb_full[reg]``, each [neles][nupts][Nv^3]);
+    ``rhs`` / ``updatebc`` take the reference's species index ``idx`` ('0',
+    '1', ...), ``collide(t, regids)`` takes the reference's register list
+    (the S input registers, then the S output registers; or use
+    ``collide_banks``).  The species count is that of the
+    ``[velocity-mesh] molarMass{p}`` keys (the reference fixes it at 2)."""
+    name = 'dgfsbi'
+
+    def __init__(self, backend, mesh, cfg, nreg=3, initsoln=None):
+        self.backend, self.cfg, self.mesh = backend, cfg, mesh
+        S = 0
+        while cfg.hasopt('velocity-mesh', f'molarMass{S + 1}'):
+            S += 1
+        if S < 1:
+            raise ValueError('[velocity-mesh] needs molarMass1, molarMass2, ...')
+        self._nspcs = S
+        self.vm = DGFSBiVelocityMesh(backend, cfg, S)
+        self.geo = ElementGeometry(mesh, cfg.getint('solver', 'order'))
+        self.ele = DGFSElements(backend, self.geo, self.vm)
+        self.ndims = self.geo.ndims
+        # time-step estimate (system.py:58-75)
+        self.unitCFLdt = np.sqrt(np.min(self.geo.djac)) / self.vm.L() / self.ndims
+        smn = cfg.get('scattering-model', 'type')
+        self.sm = subclass_where(DGFSBiScatteringModel, scattering_model=smn)(backend, cfg, self.vm)
+        self.species = [DGFSBiSpecies(self, p, nreg) for p in range(S)]
+        if initsoln is not None:
+            for p in range(S):
+                self.species[p].eles_scal_upts_inb_full[0].copy_(
+                    torch.as_tensor(initsoln[p]).to(self.species[p].eles_scal_upts_inb_full[0]))
+        else:
+            icn = cfg.get('soln-ics', 'type')
+            if icn != 'maxwellian':
+                raise ValueError(f'unsupported initial condition {icn} for dgfsbi')
+            ic = DGFSBiMaxwellianInitCondition(backend, cfg, self.vm, 'soln-ics')
+            for p, f in enumerate(ic.get_init_vals()):
+                u = self.species[p].eles_scal_upts_inb_full[0]
+                u.copy_(backend.const(f).expand_as(u))
+
+    def nspcs(self):
+        return self._nspcs
+
+    def bank(self, p, reg):
+        return self.species[p].eles_scal_upts_inb_full[reg]
+
+    # -- reference system methods ----------------------------------------
+    def rhs(self, t, idx, uinbank, foutbank, batch=None, varidx=None):
+        """foutbank <- -div F(uinbank) of species int(idx) (system.py:179-218)."""
+        self.species[int(idx)].rhs(t, uinbank, foutbank, batch, varidx)
+
+    def updatebc(self, t, idx, uinbank, foutbank, batch=None, varidx=None):
+        """disu + update_bc of species int(idx) (system.py:221-238)."""
+        self.species[int(idx)].updatebc(t, uinbank, foutbank, batch, varidx)
+
+    def collide(self, t, regids):
+        """The reference's call (system.py:241-252): regids = the S input
+        registers then the S output registers."""
+        S = self._nspcs
+        if len(regids) != 2 * S:
+            raise ValueError(f'need {2 * S} registers')
+        self.sm.collide([self.bank(p, regids[p]) for p in range(S)],
+                        [self.bank(p, regids[S + p]) for p in range(S)])
+
+    def collide_banks(self, t, uinbank, foutbank):
+        """Q_p(uinbank) -> foutbank of every species p, one launch."""
+        S = self._nspcs
+        self.collide(t, [uinbank] * S + [foutbank] * S)
+
+    def invmass(self, uinbank, foutbank):
+        raise NotImplementedError('invmass is unused by the DGFS steppers')
+
+    def moments(self, bank):
+        """Per species and DOF (FP64 on the GPU, non-dimensional): number
+        density n = sum f cw, velocity U and temperature T = (2/3) m
+        sum |c - U|^2 f cw / n, the definitions of the reference's support
+        test (initcond.py:80-117)."""
+        from .system import macroscopic
+        out = []
+        for p in range(self._nspcs):
+            n, U, T, _, _ = macroscopic(self.bank(p, bank), self.species[p].vm)
+            out.append((n, U, T * self.vm.masses()[p]))
+        return out

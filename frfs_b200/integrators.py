@@ -12,6 +12,9 @@ stepper chosen by ``[solver-time-integrator] scheme``:
                  ('adgfs' system, frfs_b200.adgfs)
 * 'adgfs-bdf-1/2/3' (steppers.py:675-860): IMEX backward differences
                  (BDF-1 is ARS-111)
+* 'dgfsbi-euler', 'dgfsbi-tvd-rk2' (steppers.py:229-486): the same per
+                 species of the 'dgfsbi' gas-mixture system, the species
+                 coupled by the mixture collision operator
 
 Each stage is one ``collide`` launch (all DOFs) plus the disu / bc-update /
 fused-rhs launches; the register banks are those of the reference (r0, r1,
@@ -140,6 +143,84 @@ class StdTVDRK2DGFSStepper(BaseDGFSStepper):
         s.collide(t + dt, 1, 2)                                   # r2 = Q(r1)
         s.advect_combine(t + dt, 1, 0, a=0.5, b=0.5 * dt,         # r0 = r0/2 + r1/2
                          x1=2, c1=0.5 * dt, x2=0, c2=0.5)         #      + dt/2 (L+Q)(r1)
+
+
+class _DGFSBiStepperMixin:
+    """The 'dgfsbi' system's state is one bank per species; the residual
+    sums the species' norms and the NaN check covers every species."""
+
+    @property
+    def soln(self):
+        return [sp.eles_scal_upts_inb_full[self._idxcurr] for sp in self.system.species]
+
+    def _residual(self, prev):
+        out = torch.zeros(2, dtype=torch.float64, device=self.backend.device)
+        tot = torch.zeros(2, dtype=torch.float64, device=self.backend.device)
+        for cur, old in zip(self.soln, prev):
+            _lib.check(_lib.lib().bdgfs_residual(cur.data_ptr(), old.data_ptr(), cur.numel(),
+                                                 int(cur.dtype == torch.float64), out.data_ptr(),
+                                                 _lib.stream_ptr()), 'bdgfs_residual')
+            tot += out
+        o = tot.cpu()
+        return float((o[0] / o[1]).sqrt())
+
+    def advance_to(self, t):
+        while self.tcurr < t - 1e-12 * max(1.0, abs(t)):
+            dt = min(self._dt, t - self.tcurr)
+            need_resid = self.resid_nsteps and (self.nacptsteps + 1) % self.resid_nsteps == 0
+            if need_resid:
+                prev = [u.clone() for u in self.soln]
+            self.step(self.tcurr, dt)
+            self.tcurr += dt
+            self.nacptsteps += 1
+            if need_resid:
+                self.residuals.append((self.tcurr, self._residual(prev)))
+            if self.nancheck_nsteps and self.nacptsteps % self.nancheck_nsteps == 0:
+                self.nancheck()
+        return self.tcurr
+
+    def nancheck(self):
+        """Raise if any species' state holds NaN/Inf (plugins/nancheck.py)."""
+        self._status.zero_()
+        for u in self.soln:
+            _lib.check(_lib.lib().bdgfs_status_check(u.data_ptr(), u.numel(),
+                                                     int(u.dtype == torch.float64),
+                                                     self._status.data_ptr(), _lib.stream_ptr()),
+                       'bdgfs_status_check')
+        if int(self._status.item()):
+            raise RuntimeError(f'NaNs detected at t = {self.tcurr}')
+
+
+class StdEulerDGFSBiStepper(_DGFSBiStepperMixin, BaseDGFSStepper):
+    """'dgfsbi-euler' (steppers.py:229-326): u_p <- u_p + dt (L + Q_p)(u)
+    for every species, Q_p = sum_q Q_pq in one launch."""
+    stepper_name = 'dgfsbi-euler'
+    nregs = 2
+    order = 1
+
+    def _step_kernels(self, t, dt):
+        s = self.system
+        s.collide_banks(t, 0, 1)                                # r1_p = Q_p(r0)
+        for sp in s.species:
+            sp.advect_combine(t, 0, 0, a=1.0, b=dt, x1=1, c1=dt)
+
+
+class StdTVDRK2DGFSBiStepper(_DGFSBiStepperMixin, BaseDGFSStepper):
+    """'dgfsbi-tvd-rk2' (steppers.py:329-486): SSP-RK2 per species with the
+    mixture operator coupling the species at each stage."""
+    stepper_name = 'dgfsbi-tvd-rk2'
+    nregs = 3
+    order = 2
+
+    def _step_kernels(self, t, dt):
+        s = self.system
+        s.collide_banks(t, 0, 1)                                  # r1_p = Q_p(r0)
+        for sp in s.species:                                      # r1 = r0 + dt (L+Q)(r0)
+            sp.advect_combine(t, 0, 1, a=1.0, b=dt, x1=1, c1=dt)
+        s.collide_banks(t + dt, 1, 2)                             # r2_p = Q_p(r1)
+        for sp in s.species:                                      # r0 = r0/2 + r1/2
+            sp.advect_combine(t + dt, 1, 0, a=0.5, b=0.5 * dt,    #      + dt/2 (L+Q)(r1)
+                              x1=2, c1=0.5 * dt, x2=0, c2=0.5)
 
 
 class ARSabcAstdStepper(BaseDGFSStepper):
@@ -327,6 +408,7 @@ class BDF3AstdStepper(BDFqAstdStepper):
 
 
 STEPPERS = {c.stepper_name: c for c in (StdEulerDGFSStepper, StdTVDRK2DGFSStepper,
+                                        StdEulerDGFSBiStepper, StdTVDRK2DGFSBiStepper,
                                         ARS111AstdStepper, ARS222AstdStepper, ARS443AstdStepper,
                                         BDF1AstdStepper, BDF2AstdStepper, BDF3AstdStepper)}
 

@@ -188,6 +188,46 @@ ssrulepre = womersley
 """)
 
 
+def dgfsbi_cfg(Nv=16, Nrho=4, M=6, Mpre=6, order=2, precision='double', dev=4, uw=0.3,
+               scheme='dgfsbi-tvd-rk2', dt=2e-4, masses=(39.96e-3, 83.798e-3)):
+    """Gas mixture between diffuse walls at y = -+0.5 moving at -+uw
+    (non-dim), x periodic: the 'dgfsbi' system with 'vss-gll'."""
+    u0 = np.sqrt(2 * 8.3144598 / NONDIM['molarMass0'] * NONDIM['T0'])
+    n0 = NONDIM['rho0'] / NONDIM['molarMass0'] * 6.0221409e+23
+    cfg = vss_cfg(Nv, Nrho, M, Mpre, masses=masses, dev=dev, precision=precision)
+    extra = f"""
+[solver]
+system = dgfsbi
+order = {order}
+[solver-time-integrator]
+scheme = {scheme}
+controller = none
+tstart = 0.0
+tend = 1.0
+dt = {dt}
+[soln-ics]
+type = maxwellian
+{chr(10).join(f'nden{p + 1} = {n0 * (0.7 if p else 0.3)}' for p in range(len(masses)))}
+T = {NONDIM['T0']}
+ux = 0
+uy = 0
+uz = 0
+[soln-bcs-y-]
+type = dgfsbi-wall-diffuse
+T = {NONDIM['T0']}
+ux = {-uw * u0}
+uy = 0
+uz = 0
+[soln-bcs-y+]
+type = dgfsbi-wall-diffuse
+T = {NONDIM['T0'] * 1.1}
+ux = {uw * u0}
+uy = 0
+uz = 0
+"""
+    return Inifile(cfg.tostr() + extra)
+
+
 def vss_oracle_for(sm):
     """The oracle on the model's mesh, directions and pair parameters."""
     from oracle.vss import BiVelocityMesh, VSSOracle

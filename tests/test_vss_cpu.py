@@ -2,6 +2,7 @@
 kernel tables against the oracle, and the oracle's own properties."""
 import numpy as np
 import pytest
+import torch
 
 from frfs_b200.dgfsbi import DGFSBiVelocityMesh, DGFSBiVSSGLLScatteringModel
 
@@ -70,3 +71,59 @@ def test_oracle_mixture_equilibrium_and_conservation():
         errs.append((eq, mass, mom, en))
     assert all(x < 0.06 for x in errs[1])
     assert errs[1][0] < errs[0][0] and errs[1][3] < errs[0][3]
+
+
+def _bi_cfg(**kw):
+    from helpers import dgfsbi_cfg
+    return dgfsbi_cfg(**kw)
+
+
+def test_dgfsbi_maxwellian_and_support_check():
+    """Per-species Maxwellians n_p (m_p/(pi T))^1.5 exp(-m_p |c-u|^2/T) with
+    the reference's moment check; a grid too coarse for the heavy species
+    is refused."""
+    from frfs_b200.dgfsbi import DGFSBiMaxwellianInitCondition
+    cfg = _bi_cfg()
+    vm = DGFSBiVelocityMesh(_CPUBackend(), cfg, 2)
+    ic = DGFSBiMaxwellianInitCondition(None, cfg, vm, 'soln-ics')
+    cv, cw, m = vm.cv(), vm.cw(), vm.masses()
+    for p, f in enumerate(ic.get_init_vals()):
+        assert np.isclose(f.sum() * cw, 0.7 if p else 0.3, rtol=1e-6)
+        T = (2.0 / 3.0) * m[p] * np.sum(f * np.sum(cv * cv, axis=0)) * cw / (f.sum() * cw)
+        assert np.isclose(T, 1.0, rtol=1e-6)
+    wall = DGFSBiMaxwellianInitCondition(None, cfg, vm, 'soln-bcs-y+', wall=True)
+    fw = wall.get_init_vals()
+    assert np.isclose(fw[1].sum() * cw, 1.0, rtol=1e-6)
+    assert np.isclose(wall.unondim()[0, 0], 0.3)
+    coarse = _bi_cfg(Nv=8, dev=6)
+    with pytest.raises(ValueError):
+        DGFSBiMaxwellianInitCondition(None, coarse, DGFSBiVelocityMesh(_CPUBackend(), coarse, 2),
+                                      'soln-ics')
+
+
+def test_dgfsbi_species_wall_rows():
+    """Each species' diffuse-wall rows carry its own wall Maxwellian; the
+    boundary tables of the 'dgfsbi' types resolve on the host."""
+    from frfs_b200.dgfsbi import SpeciesMesh
+    from frfs_b200.mesh import ElementGeometry, StructuredMesh
+    from frfs_b200.system import DGFSBoundaries
+    cfg = _bi_cfg()
+    be = _CPUBackend()
+    be.fpdtype = torch.float64
+    vm = DGFSBiVelocityMesh(be, cfg, 2)
+    geo = ElementGeometry(StructuredMesh((2, 2), (0.0, -0.5), (1.0, 0.5), periodic='x'), 2)
+    walls = [DGFSBoundaries(be, geo, SpeciesMesh(vm, p), cfg, geo.wall_names) for p in range(2)]
+    cv, m = vm.cv(), vm.masses()
+    for p, w in enumerate(walls):
+        fw = w.fw.numpy()
+        U = w.uwall.numpy()
+        for r in range(fw.shape[0]):
+            T = 1.1 if U[r, 0] > 0 else 1.0
+            want = (m[p] / (np.pi * T))**1.5 * np.exp(-m[p] * np.sum((cv - U[r][:, None])**2, 0) / T)
+            assert np.allclose(fw[r], want, rtol=1e-12, atol=0)
+        assert w.has_diffuse
+
+
+def test_dgfsbi_steppers_registered():
+    from frfs_b200.integrators import STEPPERS
+    assert STEPPERS['dgfsbi-tvd-rk2'].nregs == 3 and STEPPERS['dgfsbi-euler'].nregs == 2
