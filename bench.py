@@ -627,6 +627,78 @@ def vss_mixture(flush, peak=None, reps=3, ndof=None, check=True):
     return res
 
 
+def dgfsbi_couette(flush, steps=3):
+    """'dgfsbi' system: the binary mixture of ``vss_mixture`` in the Couette
+    geometry (16 x 8 quads P3, 2048 DOFs per species, x periodic, diffuse
+    walls at y = -+0.5 moving at -+0.3 u0, T = 1), number densities 0.3 /
+    0.7 n0, dgfsbi-tvd-rk2 at dt = 5e-4 as one CUDA graph per step; DG
+    steps/s."""
+    import numpy as np
+    import torch
+    from frfs_b200.backend import CUDABackend
+    from frfs_b200.dgfsbi import DGFSBiSystem
+    from frfs_b200.inifile import Inifile
+    from frfs_b200.integrators import get_integrator
+    from frfs_b200.mesh import StructuredMesh
+    w = MIXTURE
+    u0 = np.sqrt(2 * 8.3144598 / NONDIM['molarMass0'] * NONDIM['T0'])
+    n0 = NONDIM['rho0'] / NONDIM['molarMass0'] * 6.0221409e+23
+    walls = ''.join(f"""
+[soln-bcs-{name}]
+type = dgfsbi-wall-diffuse
+T = {NONDIM['T0']}
+ux = {sgn * WORK['uw'] * u0}
+uy = 0
+uz = 0
+""" for name, sgn in (('y-', -1), ('y+', 1)))
+    cfg = Inifile(mixture_ini(w) + f"""
+[solver]
+system = dgfsbi
+order = {WORK['order']}
+[solver-time-integrator]
+scheme = dgfsbi-tvd-rk2
+controller = none
+tstart = 0.0
+tend = 1.0
+dt = {WORK['dt']}
+[soln-ics]
+type = maxwellian
+nden1 = {0.3 * n0}
+nden2 = {0.7 * n0}
+T = {NONDIM['T0']}
+ux = 0
+uy = 0
+uz = 0
+""" + walls)
+    be = CUDABackend(cfg)
+    mesh = StructuredMesh((WORK['nx'], WORK['ny']), (0.0, -0.5), (2.0, 0.5), periodic='x')
+    s = DGFSBiSystem(be, mesh, cfg, nreg=3)
+    integ = get_integrator(be, s, cfg)
+    dt = WORK['dt']
+    for _ in range(3):                      # warm-up: eager run, capture, one replay
+        integ.step(0.0, dt)
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    tot = 0.0
+    for _ in range(steps):
+        flush.fill_(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        integ.step(0.0, dt)
+        b.record(st)
+        torch.cuda.synchronize()
+        tot += a.elapsed_time(b)
+    ok = all(bool(torch.isfinite(u).all()) for u in integ.soln)
+    res = {'workload': (f"'dgfsbi' binary mixture Couette: 16 x 8 quads P3 (2048 DOFs per species), "
+                        f"the vss_mixture operator settings, diffuse walls -+0.3 u0 at T = 1, "
+                        f"nden 0.3 / 0.7 n0, dgfsbi-tvd-rk2 dt = {dt}, FP32"),
+           'dg_steps_per_s': steps / (tot * 1e-3), 'ms_per_step': tot / steps,
+           'finite': ok}
+    del s, integ
+    torch.cuda.empty_cache()
+    return res
+
+
 def ars_bgk(flush, steps=20):
     """adgfs system: the Couette workload's mesh and velocity grid (16 x 8
     quads P3, Nv=24^3, FP32) with BGK relaxation (omega 0.81) and the
@@ -1057,6 +1129,7 @@ def run_gpu(args):
         del arrays
         extra['ars_bgk'] = ars_bgk(flush)
         extra['vss_mixture'] = vss_mixture(flush, peak)
+        extra['dgfsbi_couette'] = dgfsbi_couette(flush)
     if ws == 1 and not args.no_surrogate:
         c4, c5 = surrogate_legs(flush)
         extra['surrogate'] = c4
@@ -1264,6 +1337,13 @@ def run_ars_only():
     print(json.dumps(ars_bgk(flush)))
 
 
+def run_dgfsbi_only():
+    """The 'dgfsbi' mixture Couette leg alone (profiling case)."""
+    import torch
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device='cuda')
+    print(json.dumps(dgfsbi_couette(flush)))
+
+
 def run_vss_only(ndof):
     """The gas-mixture collision launch alone on ndof distribution pairs
     (profiling case, no oracle check)."""
@@ -1295,6 +1375,8 @@ def main():
                          '(random surrogate with zero head scales)')
     ap.add_argument('--ars-only', action='store_true',
                     help='profiling case: the adgfs ARS-222 leg alone')
+    ap.add_argument('--dgfsbi-only', action='store_true',
+                    help='profiling case: the dgfsbi mixture Couette leg alone')
     ap.add_argument('--vss-only', type=int, default=0, metavar='NDOF',
                     help='profiling case: the gas-mixture collision launch on NDOF pairs')
     ap.add_argument('--fr-only', choices=['couette', 'cavity'],
@@ -1315,6 +1397,8 @@ def main():
         run_ars_only()
     elif args.vss_only:
         run_vss_only(args.vss_only)
+    elif args.dgfsbi_only:
+        run_dgfsbi_only()
     elif args.fr_only:
         run_fr_only(args.fr_only)
     elif args.impl == 'reference':
