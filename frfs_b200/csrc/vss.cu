@@ -29,8 +29,15 @@
 // warp fall on distinct bank pairs; 231.5 KB at 24^3): passes B-D then touch
 // no global memory, and per slice only F, G, b_pq and G^ travel through L2.
 // Other grids keep Z1, Z2 in the CTA's global scratch (rows of N).
+// At 24^3 FP32 the spectral gain accumulator G^ also stays on chip, in
+// tensor memory: each thread owns the 2 x-pencils it transforms in pass E,
+// so it keeps their 2 x 24 complex sums in its TMEM lane (96 columns; warp
+// w uses lanes 32 (w mod 4).. and columns 96 (w / 4)..; 512 columns per
+// CTA), read and written with tcgen05.ld / st, and G^ reaches global
+// scratch once per item for the back-transform.
 #include "common.cuh"
 #include "fft_codelets.cuh"
+#include "tcgen05.cuh"
 
 namespace bdgfs {
 
@@ -47,6 +54,13 @@ struct VssCfg {
     static constexpr bool smem = sizeof(T) == 4 && N <= 24;
     static constexpr int RP = smem ? N + 1 : N;
     static constexpr size_t smem_bytes = smem ? size_t(2) * N * N * RP * sizeof(cpx<T>) : 0;
+    // G^ in tensor memory: every thread owns PPT whole x-pencils
+    static constexpr bool tmem = sizeof(T) == 4 && N == 24;
+    static constexpr int PPT = (N * N) / threads;
+    static constexpr uint32_t tmem_cols = 512;
+    static_assert(!tmem || (PPT * threads == N * N && threads % 32 == 0 && N % 8 == 0 &&
+                            ((threads / 32 + 3) / 4) * PPT * 2 * N <= int(tmem_cols)),
+                  "TMEM accumulator layout");
 };
 
 // pencil pc of axis AX: first element and stride ([x][y][z], z fastest,
@@ -121,6 +135,18 @@ __global__ void __launch_bounds__(VssCfg<T, N>::threads) vss_kernel(const bdgfs_
     }
     cpx<T>* Ga = F + 4 * n;
     cpx<T>* La = F + 5 * n;
+    constexpr bool kTm = VssCfg<T, N>::tmem;
+    constexpr int PPT = VssCfg<T, N>::PPT;
+    __shared__ uint32_t s_tmem;
+    uint32_t tsv = 0;                             // this thread's TMEM lane, first column
+    if constexpr (kTm) {
+        if (threadIdx.x < 32) tc::tmem_alloc(&s_tmem, VssCfg<T, N>::tmem_cols);
+        tc::tc_fence_before();
+        __syncthreads();
+        tc::tc_fence_after();
+        const uint32_t warp = threadIdx.x >> 5;
+        tsv = s_tmem + (uint32_t(32 * (warp & 3)) << 16) + uint32_t(PPT * 2 * N * (warp >> 2));
+    }
     const int S = g.nspcs, P = g.Nrho * g.M;
     const int64_t nitems = g.ndof * S;
     for (int64_t item = blockIdx.x; item < nitems; item += gridDim.x) {
@@ -128,7 +154,7 @@ __global__ void __launch_bounds__(VssCfg<T, N>::threads) vss_kernel(const bdgfs_
         const int64_t dof = item - int64_t(p) * g.ndof;
         const T* fp = static_cast<const T*>(g.f[p]) + dof * n;
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            Ga[i] = cpx<T>{T(0), T(0)};
+            if constexpr (!kTm) Ga[i] = cpx<T>{T(0), T(0)};
             La[i] = cpx<T>{T(0), T(0)};
         }
         fft_real<T, N>(fp, F);
@@ -206,19 +232,71 @@ __global__ void __launch_bounds__(VssCfg<T, N>::threads) vss_kernel(const bdgfs_
                 // E: forward DFT along x, weighted kernel product into G^
                 const T w = T(g.rw[r]) * pref;
                 const cpx<T>* brs = bq + size_t(rs) * n;
-                for (int pc = threadIdx.x; pc < N * N; pc += blockDim.x) {
-                    const int zb = (pc / N) * RP + pc % N;
-                    cpx<T> x[N];
+                if constexpr (kTm) {
+                    const bool first = q == 0 && rs == 0;   // CTA-uniform
+                    tc::tmem_wait_st();
+#pragma unroll 1
+                    for (int j = 0; j < PPT; ++j) {         // every thread: PPT pencils
+                        const int pc = threadIdx.x + j * VssCfg<T, N>::threads;
+                        const int zb = (pc / N) * RP + pc % N;
+                        cpx<T> x[N];
 #pragma unroll
-                    for (int k = 0; k < N; ++k) x[k] = Z1[zb + k * N * RP];
-                    dft<N, -1>(x);
+                        for (int k = 0; k < N; ++k) x[k] = Z1[zb + k * N * RP];
+                        dft<N, -1>(x);
 #pragma unroll
-                    for (int k = 0; k < N; ++k) {
-                        const int i = pc + k * N * N;
-                        const cpx<T> t = cmul(brs[i], x[k]);
-                        Ga[i].x += w * t.x;
-                        Ga[i].y += w * t.y;
+                        for (int c = 0; c < N / 8; ++c) {
+                            uint32_t acc[16];
+                            const uint32_t col = tsv + uint32_t(j * 2 * N + 16 * c);
+                            if (!first) {
+                                tc::tmem_ld16_issue(col, acc);
+                                tc::tmem_wait();
+                            } else {
+#pragma unroll
+                                for (int e = 0; e < 16; ++e) acc[e] = 0u;
+                            }
+#pragma unroll
+                            for (int e = 0; e < 8; ++e) {
+                                const int k = 8 * c + e;
+                                const cpx<T> t = cmul(brs[pc + k * N * N], x[k]);
+                                acc[2 * e] = __float_as_uint(__uint_as_float(acc[2 * e]) + w * t.x);
+                                acc[2 * e + 1] = __float_as_uint(__uint_as_float(acc[2 * e + 1]) + w * t.y);
+                            }
+                            tc::tmem_st16(col, acc);
+                        }
                     }
+                } else {
+                    for (int pc = threadIdx.x; pc < N * N; pc += blockDim.x) {
+                        const int zb = (pc / N) * RP + pc % N;
+                        cpx<T> x[N];
+#pragma unroll
+                        for (int k = 0; k < N; ++k) x[k] = Z1[zb + k * N * RP];
+                        dft<N, -1>(x);
+#pragma unroll
+                        for (int k = 0; k < N; ++k) {
+                            const int i = pc + k * N * N;
+                            const cpx<T> t = cmul(brs[i], x[k]);
+                            Ga[i].x += w * t.x;
+                            Ga[i].y += w * t.y;
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if constexpr (kTm) {                      // G^: TMEM -> global scratch
+            tc::tmem_wait_st();
+#pragma unroll 1
+            for (int j = 0; j < PPT; ++j) {
+                const int pc = threadIdx.x + j * VssCfg<T, N>::threads;
+#pragma unroll
+                for (int c = 0; c < N / 8; ++c) {
+                    uint32_t acc[16];
+                    tc::tmem_ld16_issue(tsv + uint32_t(j * 2 * N + 16 * c), acc);
+                    tc::tmem_wait();
+#pragma unroll
+                    for (int e = 0; e < 8; ++e)
+                        Ga[pc + (8 * c + e) * N * N] =
+                            cpx<T>{__uint_as_float(acc[2 * e]), __uint_as_float(acc[2 * e + 1])};
                 }
             }
             __syncthreads();
@@ -236,6 +314,15 @@ __global__ void __launch_bounds__(VssCfg<T, N>::threads) vss_kernel(const bdgfs_
         T* Qp = static_cast<T*>(g.Q[p]) + dof * n;
         for (int i = threadIdx.x; i < n; i += blockDim.x) Qp[i] = Ga[i].x - fp[i] * La[i].x;
         __syncthreads();
+    }
+    if constexpr (kTm) {
+        tc::tmem_wait_st();
+        tc::tc_fence_before();
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            tc::tc_fence_after();
+            tc::tmem_dealloc(s_tmem, VssCfg<T, N>::tmem_cols);
+        }
     }
 }
 

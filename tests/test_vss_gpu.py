@@ -68,3 +68,12 @@ def test_vss_per_point_shim(cuda):
     for p in range(2):
         assert torch.equal(Q[p][1, 2], Qb[p])
         assert not Q[p][0].any() and not Q[p][1, :2].any()
+
+
+def test_vss_fp32_several_items_per_cta(cuda):
+    """Three persistent CTAs for ten (distribution, species) items: each CTA
+    restarts its on-chip accumulators for every item it takes."""
+    be, sm = _model(24, 4, 6, 6, precision='single')
+    sm._nctas = 3
+    sm._scratch = None
+    assert _run(be, sm, 5, 11) < 2e-4
