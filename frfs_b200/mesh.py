@@ -1,7 +1,7 @@
 """Structured quad/hex meshes, affine metrics and flux-point connectivity.
 
-The reference reads gmsh meshes converted to ``.frfsm`` (out of scope
-here); the DGFS workloads are boxes, so this module builds them in memory:
+Meshes come from ``StructuredMesh`` (boxes built in memory) or from a
+Gmsh 2.2 file (``frfs_b200.gmsh.GmshMesh``); both give ElementGeometry:
 ``eles`` (nspts, neles, ndims) corner coordinates in the reference's
 ``std_ele(1)`` order (x fastest), internal interfaces (periodic pairs
 included) and named boundary faces.
@@ -19,6 +19,15 @@ import itertools as it
 import numpy as np
 
 from .shapes import TensorShape
+
+
+def reference_faces(ndims):
+    """Face index -> (axis, side) of the quad / hex in the reference's face
+    order (the face of side s along axis a holds the corners whose bit a is
+    (s > 0))."""
+    if ndims == 2:
+        return [(1, -1), (0, +1), (1, +1), (0, -1)]
+    return [(2, -1), (1, -1), (0, +1), (1, +1), (0, -1), (2, +1)]
 
 
 class StructuredMesh:
@@ -54,9 +63,17 @@ class StructuredMesh:
 
     def faces(self):
         """Face index -> (axis, side) for the reference's face order."""
-        if self.ndims == 2:
-            return [(1, -1), (0, +1), (1, +1), (0, -1)]
-        return [(2, -1), (1, -1), (0, +1), (1, +1), (0, -1), (2, +1)]
+        return reference_faces(self.ndims)
+
+    def pair_shift(self, e, f, e2, f2):
+        """Location of face (e, f) minus that of its partner (e2, f2): the
+        box length along the axis for a periodic pair, else zero."""
+        a = self.faces()[f][0]
+        shift = np.zeros(self.ndims)
+        # periodic pair: the + side of the last cell meets the - side of cell 0
+        if self.cells[e][a] == self.shape[a] - 1 and self.cells[e2][a] == 0:
+            shift[a] = (self.hi - self.lo)[a]
+        return shift
 
     def interfaces(self):
         """Internal pairs [((e, f), (e', f'))] and boundaries {name: [(e, f)]}."""
@@ -145,13 +162,8 @@ class ElementGeometry:
         pairs, bcs = mesh.interfaces()
         E, nf = self.neles, self.nfpts
         nbr = np.full((E, nf), np.iinfo(np.int32).min, dtype=np.int64)
-        span = mesh.hi - mesh.lo
         for (e, f), (e2, f2) in pairs:
-            a = mesh.faces()[f][0]
-            shift = np.zeros(mesh.ndims)
-            # periodic pair: the + side of the last cell meets the - side of cell 0
-            if mesh.cells[e][a] == mesh.shape[a] - 1 and mesh.cells[e2][a] == 0:
-                shift[a] = span[a]
+            shift = mesh.pair_shift(e, f, e2, f2)
             l = self._sorted_face_fpts(e, f)
             r = self._sorted_face_fpts(e2, f2, shift=-shift)
             nbr[e, l] = e2 * nf + r
