@@ -29,12 +29,13 @@
 // warp fall on distinct bank pairs; 231.5 KB at 24^3): passes B-D then touch
 // no global memory, and per slice only F, G, b_pq and G^ travel through L2.
 // Other grids keep Z1, Z2 in the CTA's global scratch (rows of N).
-// At 24^3 FP32 the spectral gain accumulator G^ also stays on chip, in
-// tensor memory: each thread owns the 2 x-pencils it transforms in pass E,
-// so it keeps their 2 x 24 complex sums in its TMEM lane (96 columns; warp
-// w uses lanes 32 (w mod 4).. and columns 96 (w / 4)..; 512 columns per
-// CTA), read and written with tcgen05.ld / st, and G^ reaches global
-// scratch once per item for the back-transform.
+// In FP32 at Nv = 16, 24 and 32 the spectral gain accumulator G^ also
+// stays on chip, in tensor memory: each thread owns the PPT x-pencils it
+// transforms in pass E (1, 2, 4), so it keeps their complex sums in its
+// TMEM lane (2 N PPT columns; warp w uses lanes 32 (w mod 4).. and the
+// columns after those of warps w - 4, w - 8), read and written with
+// tcgen05.ld / st, and G^ reaches global scratch once per item for the
+// back-transform.
 #include "common.cuh"
 #include "fft_codelets.cuh"
 #include "tcgen05.cuh"
@@ -54,10 +55,11 @@ struct VssCfg {
     static constexpr bool smem = sizeof(T) == 4 && N <= 24;
     static constexpr int RP = smem ? N + 1 : N;
     static constexpr size_t smem_bytes = smem ? size_t(2) * N * N * RP * sizeof(cpx<T>) : 0;
-    // G^ in tensor memory: every thread owns PPT whole x-pencils
-    static constexpr bool tmem = sizeof(T) == 4 && N == 24;
+    // G^ in tensor memory: every thread owns PPT whole x-pencils (FP32,
+    // Nv = 16: 64 columns per CTA; 24: 288 of 512; 32: 512)
+    static constexpr bool tmem = sizeof(T) == 4 && N % 8 == 0 && N >= 16;
     static constexpr int PPT = (N * N) / threads;
-    static constexpr uint32_t tmem_cols = 512;
+    static constexpr uint32_t tmem_cols = N == 16 ? 64 : 512;
     static_assert(!tmem || (PPT * threads == N * N && threads % 32 == 0 && N % 8 == 0 &&
                             ((threads / 32 + 3) / 4) * PPT * 2 * N <= int(tmem_cols)),
                   "TMEM accumulator layout");

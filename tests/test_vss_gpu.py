@@ -45,7 +45,7 @@ def test_vss_three_species_and_equal_masses(cuda):
     assert _run(be, sm, 3, 1) < 1e-11
 
 
-@pytest.mark.parametrize('Nv,Nrho,M,Mpre', [(16, 6, 12, 12), (24, 6, 12, 12)])
+@pytest.mark.parametrize('Nv,Nrho,M,Mpre', [(16, 6, 12, 12), (24, 6, 12, 12), (32, 4, 6, 6)])
 def test_vss_fp32_matches_oracle(cuda, Nv, Nrho, M, Mpre):
     be, sm = _model(Nv, Nrho, M, Mpre, precision='single')
     assert _run(be, sm, 4, 7) < 2e-4
@@ -70,10 +70,11 @@ def test_vss_per_point_shim(cuda):
         assert not Q[p][0].any() and not Q[p][1, :2].any()
 
 
-def test_vss_fp32_several_items_per_cta(cuda):
+@pytest.mark.parametrize('Nv', [16, 24, 32])
+def test_vss_fp32_several_items_per_cta(cuda, Nv):
     """Three persistent CTAs for ten (distribution, species) items: each CTA
     restarts its on-chip accumulators for every item it takes."""
-    be, sm = _model(24, 4, 6, 6, precision='single')
+    be, sm = _model(Nv, 4, 6, 6, precision='single')
     sm._nctas = 3
     sm._scratch = None
     assert _run(be, sm, 5, 11) < 2e-4
