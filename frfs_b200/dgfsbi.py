@@ -390,13 +390,19 @@ class DGFSBiSpecies(DGFSSystem):
         self.backend, self.cfg, self.mesh = be, bi.cfg, bi.mesh
         self.vm = SpeciesMesh(bi.vm, p)
         self.geo, self.ele, self.ndims = bi.geo, bi.ele, bi.geo.ndims
-        self.domain, self.transport, self._send_rows = None, None, {}
+        self.domain, self.transport = bi.domain, bi.transport
         self.walls = DGFSBoundaries(be, self.geo, self.vm, self.cfg, self.geo.wall_names)
         self.unitCFLdt = bi.unitCFLdt
         E, U, nv = self.ele.neles, self.ele.nupts, self.vm.vsize()
         self.eles_scal_upts_inb_full = [be.empty(E, U, nv) for _ in range(nreg)]
-        self._uf_rows = be.empty(E * self.ele.nfpts, nv)
-        self._uf = self._uf_rows.view(E, self.ele.nfpts, nv)
+        # face values, then the ghost rows of a partitioned mesh
+        nghost = self.domain.nghost if self.domain is not None else 0
+        self._uf_rows = be.empty(E * self.ele.nfpts + nghost, nv)
+        self._uf = self._uf_rows[:E * self.ele.nfpts].view(E, self.ele.nfpts, nv)
+        self._send_rows = {}
+        if self.domain is not None:
+            for r, rows in self.domain.send.items():
+                self._send_rows[r] = torch.as_tensor(rows, dtype=torch.int64, device=be.device)
         self._gen_kernels()
 
     def collide(self, t, uinbank, foutbank):
@@ -414,8 +420,14 @@ class DGFSBiSystem:
     ``[velocity-mesh] molarMass{p}`` keys (the reference fixes it at 2)."""
     name = 'dgfsbi'
 
-    def __init__(self, backend, mesh, cfg, nreg=3, initsoln=None):
+    def __init__(self, backend, mesh, cfg, nreg=3, initsoln=None, partition=None,
+                 transport=None):
+        """partition = (parts, rank): this system owns the elements
+        parts[rank] of the mesh (frfs_b200.partition); transport exchanges
+        every species' face values with the neighbouring parts after disu
+        (species by species, in the same order on every rank)."""
         self.backend, self.cfg, self.mesh = backend, cfg, mesh
+        self.transport = transport
         S = 0
         while cfg.hasopt('velocity-mesh', f'molarMass{S + 1}'):
             S += 1
@@ -424,6 +436,10 @@ class DGFSBiSystem:
         self._nspcs = S
         self.vm = DGFSBiVelocityMesh(backend, cfg, S)
         self.geo = ElementGeometry(mesh, cfg.getint('solver', 'order'))
+        self.domain = None
+        if partition is not None:
+            from .partition import LocalDomain
+            self.domain = self.geo = LocalDomain(self.geo, *partition)
         self.ele = DGFSElements(backend, self.geo, self.vm)
         self.ndims = self.geo.ndims
         # time-step estimate (system.py:58-75)

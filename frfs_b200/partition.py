@@ -147,6 +147,33 @@ def step_rk2_virtual(systems, dt):
         s.advect_end(dt, 0.5, 0.5 * dt, x1=2, c1=0.5 * dt, x2=0, c2=0.5)
 
 
+def bind_local_transports_bi(systems):
+    """Virtual ranks of the 'dgfsbi' system in one process: species p of
+    every rank exchanges with species p of its neighbours."""
+    for p in range(systems[0].nspcs()):
+        tr = LocalTransport([b.species[p] for b in systems])
+        for b in systems:
+            b.species[p].transport = tr
+
+
+def step_rk2_virtual_bi(systems, dt):
+    """One dgfsbi-tvd-rk2 step of virtual ranks sharing one process."""
+    for b in systems:
+        b.collide_banks(0.0, 0, 1)
+        for sp in b.species:
+            sp.advect_begin(0, 1)
+    for b in systems:
+        for sp in b.species:
+            sp.advect_end(0.0, 1.0, dt, x1=1, c1=dt)
+    for b in systems:
+        b.collide_banks(dt, 1, 2)
+        for sp in b.species:
+            sp.advect_begin(1, 0)
+    for b in systems:
+        for sp in b.species:
+            sp.advect_end(dt, 0.5, 0.5 * dt, x1=2, c1=0.5 * dt, x2=0, c2=0.5)
+
+
 class NCCLTransport:
     """Halo exchange between processes: one batched send/recv per neighbour
     (torch.distributed; NCCL for CUDA tensors, gloo for CPU tensors)."""
