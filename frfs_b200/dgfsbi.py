@@ -492,6 +492,46 @@ class DGFSBiSystem:
     def invmass(self, uinbank, foutbank):
         raise NotImplementedError('invmass is unused by the DGFS steppers')
 
+    def macroscopic(self, bank):
+        """The per-species fields of the reference's mixture moment writer
+        (plugins/dgfsmomwriterbi.py:258-385), non-dimensional and FP64 on the
+        GPU, per DOF: mass density rho_p = m_p n_p, velocity U_p, temperature
+        T_p, heat flux q_p = m_p^2 sum f |c-U|^2 (c-U) cw and pressure tensor
+        P_p = 2 m_p^2 sum f (c-U)(c-U) cw (xx xy xz yy yz zz), both about the
+        mixture velocity U = sum rho_p U_p / sum rho_p; plus 'nden' = n_p.
+        Returns ([per-species dict], {'rho': mixture rho, 'U': U})."""
+        from .system import raw_moments
+        ij = ((0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2))
+        raws, out = [], []
+        for p in range(self._nspcs):
+            m = raw_moments(self.bank(p, bank), self.species[p].vm)
+            mp = self.vm.masses()[p]
+            n = m[:, 0]
+            U = m[:, 1:4] / n[:, None]
+            trS = m[:, 4] + m[:, 7] + m[:, 9]
+            c2 = trS - 2.0 * (U * m[:, 1:4]).sum(1) + (U * U).sum(1) * n
+            out.append({'nden': n, 'rho': mp * n, 'U': U, 'T': (2.0 / 3.0) * mp * c2 / n})
+            raws.append(m)
+        rho = sum(o['rho'] for o in out)
+        W = sum(o['rho'][:, None] * o['U'] for o in out) / rho[:, None]
+        W2 = (W * W).sum(1)
+        for p, (m, o) in enumerate(zip(raws, out)):
+            mp2 = self.vm.masses()[p]**2
+            m0, m1 = m[:, 0], m[:, 1:4]
+            S = torch.zeros(m.shape[0], 3, 3, dtype=torch.float64, device=m.device)
+            for k, (a, b) in enumerate(ij):
+                S[:, a, b] = S[:, b, a] = m[:, 4 + k]
+            trS = S[:, 0, 0] + S[:, 1, 1] + S[:, 2, 2]
+            # sum f (c-W)_a (c-W)_b and sum f |c-W|^2 (c-W)_a from the raw moments
+            C = (S - W[:, :, None] * m1[:, None, :] - m1[:, :, None] * W[:, None, :]
+                 + m0[:, None, None] * W[:, :, None] * W[:, None, :])
+            q = (m[:, 10:13] - trS[:, None] * W - 2.0 * torch.einsum('nab,nb->na', S, W)
+                 + 2.0 * W * (W * m1).sum(1, keepdim=True) + W2[:, None] * m1
+                 - (m0 * W2)[:, None] * W)
+            o['q'] = mp2 * q
+            o['P'] = torch.stack([2.0 * mp2 * C[:, a, b] for a, b in ij], 1)
+        return out, {'rho': rho, 'U': W}
+
     def moments(self, bank):
         """Per species and DOF (FP64 on the GPU, non-dimensional): number
         density n = sum f cw, velocity U and temperature T = (2/3) m

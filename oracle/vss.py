@@ -151,3 +151,30 @@ def full_sphere(half):
 def all_pairs(nspcs, alpha=1.0, omega=0.81, dRef=4.17e-10, Tref=273.0):
     return {(p, q): dict(alpha=alpha, omega=omega, dRef=dRef, Tref=Tref)
             for p, q in product(range(nspcs), repeat=2)}
+
+
+def mixture_moments(fs, cv, cw, masses):
+    """Per-species fields of one mixture distribution set, non-dimensional,
+    as plugins/dgfsmomwriterbi.py:258-385 forms them before its dimensional
+    scaling: rho_p = m_p sum f cw, U_p, T_p = (2/3) m_p sum f |c-U_p|^2 cw /
+    (sum f cw); heat flux m_p^2 sum f |c-U|^2 (c-U) cw and pressure tensor
+    2 m_p^2 sum f (c-U)_i (c-U)_j cw about the mixture velocity
+    U = sum rho_p U_p / sum rho_p."""
+    out = []
+    for f, m in zip(fs, masses):
+        mcw = m * cw
+        rho = np.sum(f) * mcw
+        U = cv @ f * mcw / rho
+        c = cv - U[:, None]
+        T = np.sum(f * np.sum(c * c, axis=0)) * (2.0 / 3.0 * mcw * m) / rho
+        out.append({'rho': rho, 'U': U, 'T': T, 'nden': rho / m})
+    rho = sum(o['rho'] for o in out)
+    W = sum(o['rho'] * o['U'] for o in out) / rho
+    c = cv - W[:, None]
+    c2 = np.sum(c * c, axis=0)
+    for f, m, o in zip(fs, masses, out):
+        mcw = m * cw
+        o['q'] = np.array([m * np.sum(f * c2 * c[a]) * mcw for a in range(3)])
+        o['P'] = np.array([2 * m * np.sum(f * c[a] * c[b]) * mcw
+                           for a, b in ((0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2))])
+    return out, {'rho': rho, 'U': W}

@@ -152,3 +152,29 @@ def test_dgfsbi_partitioned_virtual_ranks_equal_single_domain(cuda):
         idx = torch.as_tensor(parts[r], device=be.device)
         for p in range(s.nspcs()):
             assert torch.equal(b.bank(p, 0), s.bank(p, 0).index_select(0, idx)), (r, p)
+
+
+def test_dgfsbi_macroscopic_matches_oracle(cuda):
+    """The mixture moment writer's fields (per species rho, U, T, heat flux
+    and pressure tensor about the mixture velocity) from the FP64 device
+    moments equal the oracle's on a perturbed state."""
+    from oracle.vss import mixture_moments
+    cfg, be, s = _system()
+    _perturb(s, 13)
+    got, mix = s.macroscopic(0)
+    us = _state(s)
+    cv, cw, m = s.vm.cv(), s.vm.cw(), s.vm.masses()
+    E, U = us[0].shape[:2]
+    for e in range(E):
+        for j in range(U):
+            want, wmix = mixture_moments([u[e, j] for u in us], cv, cw, m)
+            d = e * U + j
+            assert np.isclose(float(mix['rho'][d]), wmix['rho'], rtol=1e-12)
+            assert np.allclose(mix['U'][d].cpu().numpy(), wmix['U'], rtol=0, atol=1e-12)
+            for p in range(len(us)):
+                for k in ('rho', 'T', 'nden'):
+                    assert np.isclose(float(got[p][k][d]), want[p][k], rtol=1e-12), k
+                for k in ('U', 'q', 'P'):
+                    w = np.asarray(want[p][k])
+                    assert np.allclose(got[p][k][d].cpu().numpy(), w, rtol=0,
+                                       atol=1e-11 * max(1.0, np.abs(w).max())), k
