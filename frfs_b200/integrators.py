@@ -146,23 +146,31 @@ class StdTVDRK2DGFSStepper(BaseDGFSStepper):
 
 
 class _DGFSBiStepperMixin:
-    """The 'dgfsbi' system's state is one bank per species; the residual
-    sums the species' norms and the NaN check covers every species."""
+    """The 'dgfsbi' system's state is one bank per species; the residual is
+    one value per species, ||f_p - f_p,prev|| / ||f_p,prev|| over all ranks
+    (plugins/dgfsresidualbi.py:33-80), and the NaN check covers every
+    species."""
+
+    def __init__(self, backend, system, cfg):
+        super().__init__(backend, system, cfg)
+        self.resid_nsteps = cfg.getint('soln-plugin-dgfsresidualbi', 'nsteps', self.resid_nsteps)
 
     @property
     def soln(self):
         return [sp.eles_scal_upts_inb_full[self._idxcurr] for sp in self.system.species]
 
     def _residual(self, prev):
-        out = torch.zeros(2, dtype=torch.float64, device=self.backend.device)
-        tot = torch.zeros(2, dtype=torch.float64, device=self.backend.device)
-        for cur, old in zip(self.soln, prev):
-            _lib.check(_lib.lib().bdgfs_residual(cur.data_ptr(), old.data_ptr(), cur.numel(),
-                                                 int(cur.dtype == torch.float64), out.data_ptr(),
+        cur = self.soln
+        out = torch.zeros(len(cur), 2, dtype=torch.float64, device=self.backend.device)
+        for p, (c, old) in enumerate(zip(cur, prev)):
+            _lib.check(_lib.lib().bdgfs_residual(c.data_ptr(), old.data_ptr(), c.numel(),
+                                                 int(c.dtype == torch.float64), out[p].data_ptr(),
                                                  _lib.stream_ptr()), 'bdgfs_residual')
-            tot += out
-        o = tot.cpu()
-        return float((o[0] / o[1]).sqrt())
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+            dist.all_reduce(out)                   # partitioned state: global norms
+        o = out.cpu()
+        return [float(v) for v in (o[:, 0] / o[:, 1]).sqrt()]
 
     def advance_to(self, t):
         while self.tcurr < t - 1e-12 * max(1.0, abs(t)):

@@ -178,3 +178,17 @@ def test_dgfsbi_macroscopic_matches_oracle(cuda):
                     w = np.asarray(want[p][k])
                     assert np.allclose(got[p][k][d].cpu().numpy(), w, rtol=0,
                                        atol=1e-11 * max(1.0, np.abs(w).max())), k
+
+
+def test_dgfsbi_residual_per_species(cuda):
+    """The residual plugin's value per species: ||f_p - f_p,prev|| / ||f_p,prev||."""
+    cfg, be, s = _system()
+    cfg.set('soln-plugin-dgfsresidualbi', 'nsteps', '1')
+    _perturb(s, 21)
+    integ = get_integrator(be, s, cfg)
+    before = _state(s)
+    integ.advance_to(2e-4)
+    after = _state(s)
+    (t, res), = integ.residuals
+    want = [np.linalg.norm(a - b) / np.linalg.norm(b) for a, b in zip(after, before)]
+    assert len(res) == 2 and np.allclose(res, want, rtol=1e-10, atol=0)
