@@ -26,7 +26,7 @@ EXPORTS = (
     'bdgfs_hybrid_project_scatter', 'bdgfs_hybrid_heads',
     'bdgfs_bgk_moments', 'bdgfs_bgk_maxwellian', 'bdgfs_ars_stage',
     'bdgfs_esbgk_moments', 'bdgfs_esbgk_gaussian', 'bdgfs_shakov_moments', 'bdgfs_shakov_target',
-    'bdgfs_bdf_step', 'bdgfs_vss_scratch_bytes', 'bdgfs_vss_collide',
+    'bdgfs_bdf_step', 'bdgfs_vss_scratch_bytes', 'bdgfs_vss_collide', 'bdgfs_vss_project',
 )
 
 
@@ -117,6 +117,12 @@ class VssArgs(C.Structure):
                 ('sz', C.c_void_p), ('b', C.c_void_p), ('c', C.c_void_p)]
 
 
+class VssProjArgs(C.Structure):
+    _fields_ = [('Nv', C.c_int32), ('nspcs', C.c_int32), ('ndof', C.c_int64),
+                ('fp64', C.c_int32), ('pad_', C.c_int32), ('Q', C.c_void_p * 4),
+                ('c0', C.c_void_p), ('mass', C.c_void_p), ('ginv', C.c_void_p)]
+
+
 class BdfArgs(C.Structure):
     _fields_ = [('ndof', C.c_int64), ('Nv', C.c_int32), ('fp64', C.c_int32),
                 ('c0', C.c_void_p), ('cw', C.c_double), ('prefac', C.c_double),
@@ -181,6 +187,7 @@ def lib():
             'bdgfs_bdf_step': [vp, vp],
             'bdgfs_vss_scratch_bytes': [C.c_int32, C.c_int32, C.c_int32],
             'bdgfs_vss_collide': [vp, vp, C.c_size_t, vp],
+            'bdgfs_vss_project': [vp, vp],
             'bdgfs_colsum': [vp, i64, i64, vp, vp],
             'bdgfs_adamw': [vp, vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float,
                             C.c_float, C.c_float, i64, vp],

@@ -347,11 +347,86 @@ int vss_launch(const bdgfs_vss_args* a, void* scratch, size_t bytes, cudaStream_
     return cuda_status(cudaGetLastError());
 }
 
+// FP64 conservation projection of a mixture's Q: per distribution, the
+// minimal-norm change of (Q_0 .. Q_{S-1}) that zeroes each species' mass
+// sum f cw, the total momentum sum_p m_p c Q_p cw and the total energy
+// sum_p m_p |c|^2 Q_p cw: Q_p -= lam_p + m_p (lam_S c + lam_{S+3} |c|^2),
+// lam = G^-1 r with r the current constraint sums.
+constexpr int VSS_PROJ_THREADS = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(VSS_PROJ_THREADS) vss_project_kernel(const bdgfs_vss_proj_args a)
+{
+    __shared__ double red[5 * 4 * (VSS_PROJ_THREADS / 32)];
+    const int N = a.Nv, S = a.nspcs, K = S + 4;
+    const int64_t n = int64_t(N) * N * N;
+    for (int64_t dof = blockIdx.x; dof < a.ndof; dof += gridDim.x) {
+        double m[20];
+#pragma unroll
+        for (int j = 0; j < 20; ++j) m[j] = 0.0;
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            if (p >= S) break;
+            const T* Q = static_cast<const T*>(a.Q[p]) + dof * n;
+            for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+                const double cx = a.c0[i / (N * N)], cy = a.c0[(i / N) % N], cz = a.c0[i % N];
+                const double q = double(Q[i]);
+                m[5 * p + 0] += q;
+                m[5 * p + 1] += cx * q;
+                m[5 * p + 2] += cy * q;
+                m[5 * p + 3] += cz * q;
+                m[5 * p + 4] += (cx * cx + cy * cy + cz * cz) * q;
+            }
+        }
+        block_sum<20>(m, red);
+        // constraint sums r and multipliers lam = G^-1 r (K <= 8)
+        double r[8], lam[8];
+        for (int k = 0; k < 8; ++k) r[k] = 0.0;
+        for (int p = 0; p < S; ++p) {
+            r[p] = m[5 * p];
+            for (int d = 0; d < 4; ++d) r[S + d] += a.mass[p] * m[5 * p + 1 + d];
+        }
+        for (int k = 0; k < K; ++k) {
+            double v = 0.0;
+            for (int l = 0; l < K; ++l) v += a.ginv[k * K + l] * r[l];
+            lam[k] = v;
+        }
+        for (int p = 0; p < S; ++p) {
+            T* Q = static_cast<T*>(a.Q[p]) + dof * n;
+            const double mp = a.mass[p];
+            for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+                const double cx = a.c0[i / (N * N)], cy = a.c0[(i / N) % N], cz = a.c0[i % N];
+                const double d = lam[p] + mp * (lam[S] * cx + lam[S + 1] * cy + lam[S + 2] * cz
+                                                + lam[S + 3] * (cx * cx + cy * cy + cz * cz));
+                Q[i] = T(double(Q[i]) - d);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 }  // namespace bdgfs
 
 using namespace bdgfs;
+
+extern "C" int32_t bdgfs_vss_project(const bdgfs_vss_proj_args* a, void* stream)
+{
+    if (!a || a->nspcs < 1 || a->nspcs > 4 || a->ndof < 0 || a->Nv < 1 || a->Nv > 64 || !a->c0 ||
+        !a->mass || !a->ginv)
+        return BDGFS_EINVAL;
+    for (int p = 0; p < a->nspcs; ++p)
+        if (!a->Q[p]) return BDGFS_EINVAL;
+    if (a->ndof == 0) return BDGFS_OK;
+    const int64_t grid = a->ndof < 148 * 8 ? a->ndof : 148 * 8;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (a->fp64)
+        vss_project_kernel<double><<<unsigned(grid), VSS_PROJ_THREADS, 0, st>>>(*a);
+    else
+        vss_project_kernel<float><<<unsigned(grid), VSS_PROJ_THREADS, 0, st>>>(*a);
+    return cuda_status(cudaGetLastError());
+}
 
 extern "C" size_t bdgfs_vss_scratch_bytes(int32_t Nv, int32_t fp64, int32_t nctas)
 {

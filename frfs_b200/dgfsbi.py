@@ -111,6 +111,23 @@ def _lgrid(N):
     return np.stack([l0[idx // (N * N)], l0[(idx // N) % N], l0[idx % N]])
 
 
+def mixture_gram_inverse(c0, masses):
+    """Inverse Gram matrix of the mixture's constraint functions over the
+    grid, the species' values concatenated: 1 on species p (one per
+    species), then m_p c_x, m_p c_y, m_p c_z and m_p |c|^2 on every species."""
+    S = len(masses)
+    cx, cy, cz = np.meshgrid(c0, c0, c0, indexing='ij')
+    phi = np.stack([np.ones_like(cx), cx, cy, cz, cx * cx + cy * cy + cz * cz]).reshape(5, -1)
+    G1 = phi @ phi.T                                   # per-species sums of phi_i phi_j
+    K = S + 4
+    G = np.zeros((K, K))
+    for p, m in enumerate(masses):
+        G[p, p] = G1[0, 0]
+        G[p, S:] = G[S:, p] = m * G1[0, 1:]
+        G[S:, S:] += m * m * G1[1:, 1:]
+    return np.linalg.inv(G)
+
+
 class DGFSBiScatteringModel:
     scattering_model = None
 
@@ -189,6 +206,12 @@ class DGFSBiVSSGLLScatteringModel(DGFSBiScatteringModel):
         nsm = torch.cuda.get_device_properties(dev).multi_processor_count if dev.type == 'cuda' else 1
         self._nctas = nsm
         self._scratch = None
+        # FP64 conservation projection (species masses, total momentum and
+        # energy); the reference's operator has none, so parity runs disable it
+        self._project = self.cfg.getbool('scattering-model', 'conservation-projection', True)
+        self.d_c0 = f64(vm.c0())
+        self.d_mass = f64(m)
+        self.d_ginv = f64(mixture_gram_inverse(vm.c0(), m).ravel())
 
     def _scratch_for(self, items):
         L = _lib.lib()
@@ -198,9 +221,11 @@ class DGFSBiVSSGLLScatteringModel(DGFSBiScatteringModel):
             self._scratch = torch.empty(nb, dtype=torch.uint8, device=self.backend.device)
         return self._scratch, nb
 
-    def collide(self, fs, Qs):
+    def collide(self, fs, Qs, project=None):
         """Qs[p][dof] <- sum_q Q_pq(fs[p][dof], fs[q][dof]) for every
-        distribution of the species banks fs (each [..., Nv^3])."""
+        distribution of the species banks fs (each [..., Nv^3]), then the
+        FP64 conservation projection unless disabled (``project`` or
+        ``[scattering-model] conservation-projection``)."""
         S, n = self._nspcs, self.vm.vsize()
         if len(fs) != S or len(Qs) != S:
             raise ValueError(f'need {S} species banks')
@@ -217,6 +242,14 @@ class DGFSBiVSSGLLScatteringModel(DGFSBiScatteringModel):
         scratch, nb = self._scratch_for(ndof * S)
         _lib.check(_lib.lib().bdgfs_vss_collide(C.byref(a), scratch.data_ptr(), nb,
                                                 _lib.stream_ptr()), 'bdgfs_vss_collide')
+        if self._project if project is None else project:
+            pa = _lib.VssProjArgs(Nv=self.vm.Nv(), nspcs=S, ndof=ndof, fp64=self.fp64,
+                                  c0=self.d_c0.data_ptr(), mass=self.d_mass.data_ptr(),
+                                  ginv=self.d_ginv.data_ptr())
+            for p in range(S):
+                pa.Q[p] = Qs[p].data_ptr()
+            _lib.check(_lib.lib().bdgfs_vss_project(C.byref(pa), _lib.stream_ptr()),
+                       'bdgfs_vss_project')
 
     def fs(self, elem, upt, *args):
         """The reference's per-point call: args = f_0..f_{S-1}, Q_0..Q_{S-1}

@@ -473,6 +473,26 @@ size_t bdgfs_vss_scratch_bytes(int32_t Nv, int32_t fp64, int32_t nctas);
 int32_t bdgfs_vss_collide(const bdgfs_vss_args* a, void* scratch, size_t bytes,
                           void* stream);
 
+/* FP64 conservation projection of a mixture's Q, in place, per
+ * distribution: the minimal-norm change of (Q_0 .. Q_{S-1}) that zeroes each
+ * species' mass and the total momentum and energy (species weighted by
+ * their masses).  ginv is the inverse (S+4) x (S+4) Gram matrix of the
+ * constraint functions (1 per species; m_p c; m_p |c|^2) over the grid.
+ * New relative to the reference's vss-gll operator (it has no projection);
+ * the counterpart of the VHS kernel's BDGFS_PROJECT for mixtures. */
+typedef struct bdgfs_vss_proj_args {
+    int32_t Nv;
+    int32_t nspcs;           /* 1..4                                          */
+    int64_t ndof;
+    int32_t fp64;
+    int32_t pad_;
+    void* Q[4];              /* real [ndof][Nv^3] per species (updated)       */
+    const double* c0;        /* [Nv]                                          */
+    const double* mass;      /* [nspcs] molar masses / molarMass0             */
+    const double* ginv;      /* [(nspcs+4)^2], row-major                      */
+} bdgfs_vss_proj_args;
+int32_t bdgfs_vss_project(const bdgfs_vss_proj_args* a, void* stream);
+
 /* One IMEX-BDF step of the 'adgfs' system (BDF2/BDF3AstdStepper.step,
  * frfs/integrators/std/steppers.py:680-860: updateMom{q}_BDF,
  * constructMaxwellian and updateDistribution{q}_BDF of

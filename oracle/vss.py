@@ -178,3 +178,24 @@ def mixture_moments(fs, cv, cw, masses):
         o['P'] = np.array([2 * m * np.sum(f * c[a] * c[b]) * mcw
                            for a, b in ((0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2))])
     return out, {'rho': rho, 'U': W}
+
+
+def project_mixture(Qs, cv, masses):
+    """Minimal-norm change of the concatenated (Q_0 .. Q_{S-1}) that zeroes
+    each species' mass and the total (mass-weighted) momentum and energy,
+    solved directly from the stacked constraint vectors (the checker of the
+    device projection; the reference has none)."""
+    S, n = len(Qs), cv.shape[1]
+    c2 = np.sum(cv * cv, axis=0)
+    rows = []
+    for p in range(S):
+        r = np.zeros(S * n)
+        r[p * n:(p + 1) * n] = 1.0
+        rows.append(r)
+    for phi in (cv[0], cv[1], cv[2], c2):
+        rows.append(np.concatenate([m * phi for m in masses]))
+    A = np.stack(rows)
+    q = np.concatenate(Qs)
+    lam = np.linalg.solve(A @ A.T, A @ q)
+    q = q - A.T @ lam
+    return [q[p * n:(p + 1) * n] for p in range(S)]

@@ -154,7 +154,7 @@ uz = 0
 
 
 def vss_cfg(Nv, Nrho, M, Mpre, masses=(39.96e-3, 83.798e-3), alpha=1.3, omega=0.81, dev=5,
-            precision='double'):
+            precision='double', project=False):
     """Gas-mixture config of the 'vss-gll' model: every ordered species pair
     with the same VSS parameters."""
     S = len(masses)
@@ -184,6 +184,7 @@ M = {M}
 type = vss-gll
 Mpre = {Mpre}
 ssrulepre = womersley
+conservation-projection = {'true' if project else 'false'}
 {pairs}
 """)
 

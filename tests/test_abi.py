@@ -40,6 +40,7 @@ STRUCTS = {
     'bdgfs_ars_args': _lib.ArsArgs,
     'bdgfs_bdf_args': _lib.BdfArgs,
     'bdgfs_vss_args': _lib.VssArgs,
+    'bdgfs_vss_proj_args': _lib.VssProjArgs,
 }
 
 

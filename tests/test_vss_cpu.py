@@ -127,3 +127,25 @@ def test_dgfsbi_species_wall_rows():
 def test_dgfsbi_steppers_registered():
     from frfs_b200.integrators import STEPPERS
     assert STEPPERS['dgfsbi-tvd-rk2'].nregs == 3 and STEPPERS['dgfsbi-euler'].nregs == 2
+
+
+def test_mixture_gram_inverse_projects_like_the_oracle():
+    """The host Gram inverse of the device projection gives the oracle's
+    least-squares projection (numpy, both species)."""
+    from frfs_b200.dgfsbi import mixture_gram_inverse
+    from oracle.vss import project_mixture
+    sm = _model()
+    o = vss_oracle_for(sm)
+    cv, m = o.vm.cv, o.vm.masses
+    rng = np.random.default_rng(2)
+    Q = [rng.standard_normal(cv.shape[1]) for _ in m]
+    Gi = mixture_gram_inverse(sm.vm.c0(), m)
+    S = len(m)
+    c2 = np.sum(cv * cv, 0)
+    r = np.array([q.sum() for q in Q] + [sum(mp * (phi @ q) for mp, q in zip(m, Q))
+                                         for phi in (cv[0], cv[1], cv[2], c2)])
+    lam = Gi @ r
+    got = [q - (lam[p] + m[p] * (lam[S] * cv[0] + lam[S + 1] * cv[1] + lam[S + 2] * cv[2]
+                                 + lam[S + 3] * c2)) for p, q in enumerate(Q)]
+    want = project_mixture(Q, cv, m)
+    assert all(np.allclose(g, w, rtol=0, atol=1e-12) for g, w in zip(got, want))

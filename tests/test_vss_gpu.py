@@ -78,3 +78,32 @@ def test_vss_fp32_several_items_per_cta(cuda, Nv):
     sm._nctas = 3
     sm._scratch = None
     assert _run(be, sm, 5, 11) < 2e-4
+
+
+@pytest.mark.parametrize('precision,tol', [('double', 1e-11), ('single', 2e-4)])
+def test_vss_conservation_projection(cuda, precision, tol):
+    """With the FP64 projection on, Q equals the oracle's Q after the same
+    minimal-norm projection, and (FP64) each species' mass, the total
+    momentum and the total energy of Q vanish to rounding."""
+    from oracle.vss import project_mixture
+    be, sm = _model(16, 6, 12, 12, precision=precision)
+    o = vss_oracle_for(sm)
+    rng = np.random.default_rng(8)
+    F = [mixture(o.vm.cv, o.vm.masses, rng) for _ in range(4)]
+    fs = [torch.tensor(np.stack([F[d][p] for d in range(4)]), dtype=be.fpdtype, device=be.device)
+          for p in range(2)]
+    Qs = [torch.empty_like(f) for f in fs]
+    sm.collide(fs, Qs, project=True)
+    torch.cuda.synchronize()
+    cv, m = o.vm.cv, o.vm.masses
+    for d in range(4):
+        want = project_mixture(o.Q(F[d]), cv, m)
+        got = [Qs[p][d].double().cpu().numpy() for p in range(2)]
+        assert max(rel_l2(got[p], want[p]) for p in range(2)) < tol
+        if precision == 'double':
+            scale = sum(np.abs(g).sum() for g in got)
+            assert max(abs(g.sum()) for g in got) < 1e-12 * scale
+            mom = sum(mp * (cv @ g) for mp, g in zip(m, got))
+            en = sum(mp * (np.sum(cv * cv, 0) @ g) for mp, g in zip(m, got))
+            assert np.abs(mom).max() < 1e-12 * scale * np.abs(cv).max()
+            assert abs(en) < 1e-12 * scale * np.sum(cv * cv, 0).max()
