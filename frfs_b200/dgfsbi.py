@@ -327,6 +327,53 @@ class DGFSBiMaxwellianInitCondition:
         return self._u
 
 
+class DGFSBiMaxwellianExprInitCondition:
+    """'maxwellianExpr' of the 'dgfsbi' system (frfs/solvers/dgfsbi/
+    initcond.py:138-212): per species p a Maxwellian of mass m_p whose
+    number density nden{p+1} and the shared ux, uy, uz, T are expressions of
+    x, y, z and the [constants], evaluated at every solution point; built on
+    the device (the species Maxwellian is the unit-mass one at T / m_p).
+    Raises ``ValueError`` when a point's number density is not represented
+    to 1e-5."""
+    model = 'maxwellianExpr'
+
+    def __init__(self, backend, cfg, vm, name):
+        self.cfg, self.vm, self.name = cfg, vm, name
+        self._vars = cfg.items_as('constants', float)
+        if any(d in self._vars for d in 'xyz'):
+            raise ValueError('Invalid constants (x, y, or z) in config file')
+
+    def fields(self, p, ploc):
+        """Non-dimensional (nden, ux, uy, uz, T) of species p at ploc[..., ndims]."""
+        vm = self.vm
+        v = dict(self._vars)
+        v.update(zip('xyz', np.moveaxis(np.asarray(ploc, dtype=np.float64), -1, 0)))
+        shp = np.asarray(ploc).shape[:-1]
+        keys = (f'nden{p + 1}', 'ux', 'uy', 'uz', 'T')
+        scale = (vm.n0(), vm.u0(), vm.u0(), vm.u0(), vm.T0())
+        return [np.broadcast_to(np.asarray(npeval(self.cfg.getexpr(self.name, k), v),
+                                           dtype=np.float64), shp) / sc
+                for k, sc in zip(keys, scale)]
+
+    def apply_init_vals(self, p, bank, ploc):
+        vm = self.vm
+        n, ux, uy, uz, T = (a.reshape(-1) for a in self.fields(p, ploc))
+        Tm = T / vm.masses()[p]
+        u2 = ux * ux + uy * uy + uz * uz
+        U = np.stack([n, n * ux, n * uy, n * uz, 1.5 * n * Tm + n * u2], axis=-1)
+        dev = bank.device
+        Ud = torch.as_tensor(U, dtype=torch.float64, device=dev).contiguous()
+        c0 = torch.as_tensor(vm.c0(), dtype=torch.float64, device=dev).contiguous()
+        nv = vm.vsize()
+        _lib.check(_lib.lib().bdgfs_bgk_maxwellian(Ud.data_ptr(), bank.numel() // nv, vm.Nv(),
+                                                   int(bank.dtype == torch.float64), c0.data_ptr(),
+                                                   bank.data_ptr(), _lib.stream_ptr()),
+                   'bdgfs_bgk_maxwellian')
+        bulk = bank.reshape(-1, nv).double().sum(-1).cpu().numpy() * vm.cw()
+        if not np.allclose(n, bulk, atol=1e-5):
+            raise ValueError(f'Bulk properties not conserved for species {p}! Check Nv, dev')
+
+
 class _BiMaxwellianRows:
     """Wall / inflow rows of one species (frfs/solvers/dgfsbi/inters.py)."""
     wall = True
@@ -486,12 +533,18 @@ class DGFSBiSystem:
                     torch.as_tensor(initsoln[p]).to(self.species[p].eles_scal_upts_inb_full[0]))
         else:
             icn = cfg.get('soln-ics', 'type')
-            if icn != 'maxwellian':
+            if icn == 'maxwellian':
+                ic = DGFSBiMaxwellianInitCondition(backend, cfg, self.vm, 'soln-ics')
+                for p, f in enumerate(ic.get_init_vals()):
+                    u = self.species[p].eles_scal_upts_inb_full[0]
+                    u.copy_(backend.const(f).expand_as(u))
+            elif icn == 'maxwellianExpr':
+                ic = DGFSBiMaxwellianExprInitCondition(backend, cfg, self.vm, 'soln-ics')
+                for p in range(S):
+                    ic.apply_init_vals(p, self.species[p].eles_scal_upts_inb_full[0],
+                                       self.geo.plocupts)
+            else:
                 raise ValueError(f'unsupported initial condition {icn} for dgfsbi')
-            ic = DGFSBiMaxwellianInitCondition(backend, cfg, self.vm, 'soln-ics')
-            for p, f in enumerate(ic.get_init_vals()):
-                u = self.species[p].eles_scal_upts_inb_full[0]
-                u.copy_(backend.const(f).expand_as(u))
 
     def nspcs(self):
         return self._nspcs

@@ -192,3 +192,32 @@ def test_dgfsbi_residual_per_species(cuda):
     (t, res), = integ.residuals
     want = [np.linalg.norm(a - b) / np.linalg.norm(b) for a, b in zip(after, before)]
     assert len(res) == 2 and np.allclose(res, want, rtol=1e-10, atol=0)
+
+
+@pytest.mark.parametrize('prec,tol', [('double', 1e-13), ('single', 1e-6)])
+def test_dgfsbi_maxwellian_expr_initial_condition(cuda, prec, tol):
+    """'maxwellianExpr': every solution point of species p holds
+    nden_p (m_p/(pi T))^1.5 exp(-m_p |c-u|^2/T) of the expressions there."""
+    cfg = dgfsbi_cfg(precision=prec)
+    u0 = np.sqrt(2 * 8.3144598 / 39.96e-3 * 273.0)
+    n0 = 0.00011140244750324529 / 39.96e-3 * 6.0221409e+23
+    cfg.set('constants', 'n0', repr(n0))
+    for k, v in (('type', 'maxwellianExpr'), ('nden1', 'n0*0.3*(1 + 0.1*sin(2*pi*x))'),
+                 ('nden2', 'n0*0.7*(1 - 0.05*y)'), ('ux', f'{0.1 * u0}*y'),
+                 ('uy', f'{0.05 * u0}*x'), ('uz', '0'), ('T', '273*(1 + 0.05*x)')):
+        cfg.set('soln-ics', k, v)
+    be = CUDABackend(cfg)
+    s = DGFSBiSystem(be, StructuredMesh((3, 2), (0.0, -0.5), (1.0, 0.5), periodic='x'), cfg)
+    torch.cuda.synchronize()
+    cv, m = s.vm.cv(), s.vm.masses()
+    pl = s.geo.plocupts
+    for p in range(2):
+        want = np.empty((pl.shape[0], pl.shape[1], cv.shape[1]))
+        for e in range(pl.shape[0]):
+            for j in range(pl.shape[1]):
+                x, y = pl[e, j]
+                n = 0.3 * (1 + 0.1 * np.sin(2 * np.pi * x)) if p == 0 else 0.7 * (1 - 0.05 * y)
+                u = np.array([0.1 * y, 0.05 * x, 0.0])[:, None]
+                T = 1 + 0.05 * x
+                want[e, j] = n * (m[p] / (np.pi * T))**1.5 * np.exp(-m[p] * np.sum((cv - u)**2, 0) / T)
+        assert rel_l2(s.bank(p, 0).double().cpu().numpy(), want) < tol
