@@ -95,7 +95,7 @@ class HybridArgs(C.Structure):
                 ('sur_rho2', C.c_void_p), ('spec_idx', C.c_void_p), ('flag', C.c_void_p),
                 ('eps', C.c_void_p), ('recheck_err', C.c_void_p), ('seed_dev', C.c_void_p),
                 ('dev_rows', C.c_void_p), ('feat', C.c_void_p), ('feat_ld', C.c_int64),
-                ('sur_s', C.c_void_p)]
+                ('sur_s', C.c_void_p), ('fb_idx', C.c_void_p)]
 
 
 class ArsArgs(C.Structure):

@@ -193,7 +193,16 @@ __global__ void __launch_bounds__(256) scatter_kernel(const bdgfs_hybrid_args h,
     const T* src = Qc + row * n;
     T* dst = Q + dof * n;
     if (h.flag[dof] != 2) {
-        for (int64_t v = threadIdx.x; v < n; v += blockDim.x) dst[v] = src[v];
+        int bad = 0;
+        for (int64_t v = threadIdx.x; v < n; v += blockDim.x) {
+            const T x = src[v];
+            bad |= !isfinite(x);
+            dst[v] = x;
+        }
+        // a non-finite row goes to the fallback list (the spectral launch
+        // that follows overwrites it)
+        if (__syncthreads_or(bad) && h.fb_idx && threadIdx.x == 0)
+            h.fb_idx[atomicAdd(reinterpret_cast<unsigned long long*>(h.counts + 3), 1ull)] = int32_t(dof);
         return;
     }
     double e[2] = {0, 0};
@@ -203,6 +212,7 @@ __global__ void __launch_bounds__(256) scatter_kernel(const bdgfs_hybrid_args h,
         e[1] += double(dst[v]) * double(dst[v]);
     }
     block_sum<2>(e, red);
+    if (!isfinite(e[0])) return;                       // the cell keeps its spectral Q
     if (threadIdx.x == 0 && h.recheck_err) {
         atomicAdd(h.recheck_err, e[0]);
         atomicAdd(h.recheck_err + 1, e[1]);
@@ -232,6 +242,15 @@ __global__ void __launch_bounds__(256) project_scatter_kernel(const bdgfs_hybrid
     double m[5] = {0, 0, 0, 0, 0};
     row_moments<T, VEC>(src, n, Nv, cs, m);
     block_sum<5>(m, red);
+    const bool re = h.flag[dof] == 2;
+    // a non-finite row (NaN / Inf anywhere makes its moments non-finite;
+    // uniform per block): nothing is written; a surrogate cell goes to the
+    // fallback list, a re-checked cell keeps its spectral Q
+    if (!isfinite(m[0] + m[1] + m[2] + m[3] + m[4])) {
+        if (!re && h.fb_idx && threadIdx.x == 0)
+            h.fb_idx[atomicAdd(reinterpret_cast<unsigned long long*>(h.counts + 3), 1ull)] = int32_t(dof);
+        return;
+    }
     double lam[5];
 #pragma unroll
     for (int i = 0; i < 5; ++i) {
@@ -240,7 +259,6 @@ __global__ void __launch_bounds__(256) project_scatter_kernel(const bdgfs_hybrid
         for (int j = 0; j < 5; ++j) t += h.ginv[i * 5 + j] * m[j];
         lam[i] = t;
     }
-    const bool re = h.flag[dof] == 2;
     double e[2] = {0, 0};
 #pragma unroll 2
     for (int v = threadIdx.x * VEC; v < n; v += blockDim.x * VEC) {
@@ -312,7 +330,8 @@ extern "C" int32_t bdgfs_hybrid_classify(const bdgfs_hybrid_args* h, const void*
         !h->flag)
         return BDGFS_EINVAL;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (cudaMemsetAsync(h->counts, 0, 3 * sizeof(int64_t), st) != cudaSuccess) return BDGFS_ECUDA;
+    if (cudaMemsetAsync(h->counts, 0, (h->fb_idx ? 4 : 3) * sizeof(int64_t), st) != cudaSuccess)
+        return BDGFS_ECUDA;
     if (h->recheck_err && cudaMemsetAsync(h->recheck_err, 0, 2 * sizeof(double), st) != cudaSuccess)
         return BDGFS_ECUDA;
     if (h->ndof == 0) return BDGFS_OK;

@@ -573,7 +573,8 @@ class HybridCollider:
         if self._n < ndof:
             dev = self.model.device
             n = self.model.n
-            self.counts = torch.zeros(3, dtype=torch.int64, device=dev)
+            self.counts = torch.zeros(4, dtype=torch.int64, device=dev)
+            self.fb_idx = torch.zeros(ndof, dtype=torch.int32, device=dev)
             self.sur_idx = torch.zeros(ndof, dtype=torch.int32, device=dev)
             self.spec_idx = torch.zeros(ndof, dtype=torch.int32, device=dev)
             self.inv_rho = torch.zeros(ndof, device=dev)
@@ -582,7 +583,7 @@ class HybridCollider:
             self.flag = torch.zeros(ndof, dtype=torch.uint8, device=dev)
             self.eps = torch.zeros(ndof, device=dev)
             self.recheck_err = torch.zeros(2, dtype=torch.float64, device=dev)
-            self.rc_counts = torch.zeros(3, dtype=torch.int64, device=dev)
+            self.rc_counts = torch.zeros(4, dtype=torch.int64, device=dev)
             self.seed_dev = torch.zeros(1, dtype=torch.int64, device=dev)
             self.dev_rows = torch.zeros(ndof, n, device=dev, dtype=torch.bfloat16)
             self._n = ndof
@@ -616,7 +617,7 @@ class HybridCollider:
             eps=self.eps.data_ptr(), recheck_err=self.recheck_err.data_ptr() if rc > 0 else 0,
             seed_dev=self.seed_dev.data_ptr() if seed is None else 0,
             dev_rows=self.dev_rows.data_ptr(), feat=feat, feat_ld=m.ldx,
-            sur_s=self.sur_s.data_ptr())
+            sur_s=self.sur_s.data_ptr(), fb_idx=self.fb_idx.data_ptr())
 
     def classify(self, fin, seed=None, recheck=None):
         f2 = fin.reshape(-1, self.model.n)
@@ -657,6 +658,10 @@ class HybridCollider:
         fn = L.bdgfs_hybrid_project_scatter if self.project else L.bdgfs_hybrid_scatter
         _lib.check(fn(C.byref(self.args), self.Qc.data_ptr(), q2.data_ptr(), _lib.stream_ptr()),
                    'bdgfs_hybrid_project_scatter')
+        # surrogate rows that came out NaN / Inf: the spectral operator on
+        # the device list the scatter built (no CTA has work when it is empty)
+        self.spectral([(0, f2, q2, None)], project=self.project, exact=False,
+                      index=self.fb_idx, count=self.counts[3:4])
 
     def collide_surrogate_only(self, fin, fout):
         """Every cell through the surrogate (evaluation helper)."""
@@ -674,4 +679,5 @@ class HybridCollider:
         r = self.rc_counts.cpu().tolist()
         e = self.recheck_err.cpu().tolist()
         return {'surrogate_cells': c[0], 'spectral_cells': c[1], 'rechecked_cells': r[2],
+                'fallback_cells': c[3],
                 'recheck_rel_l2': math.sqrt(e[0] / e[1]) if e[1] > 0 else None}

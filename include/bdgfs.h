@@ -334,7 +334,8 @@ typedef struct bdgfs_hybrid_args {
     float recheck;           /* fraction of surrogate cells re-checked     */
     uint64_t seed;           /* re-check sampling seed (e.g. step number)  */
     int64_t* counts;         /* [3] device: surrogate, spectral (incl.
-                                re-checks), re-checked                     */
+                                re-checks), re-checked; [4] with fb_idx:
+                                + fallback                                 */
     int32_t* sur_idx;        /* [ndof] surrogate cells                     */
     float* sur_inv_rho;      /* [ndof] 1/rho of each surrogate row         */
     float* sur_rho2;         /* [ndof] rho^2 of each surrogate row         */
@@ -352,6 +353,11 @@ typedef struct bdgfs_hybrid_args {
                                 gets (u_x, u_y, u_z, T - 1) at columns 0..3 */
     int64_t feat_ld;
     float* sur_s;            /* optional [ndof]: |d|_2 of surrogate row p   */
+    int32_t* fb_idx;         /* optional [ndof]: the scatter lists here the
+                                surrogate cells whose row is not finite
+                                (NaN / Inf) and writes nothing for them;
+                                counts[3] their number -- the caller runs
+                                the spectral operator on that list         */
 } bdgfs_hybrid_args;
 
 /* Indicator eps = |f - M[f]| / |f| per distribution and device-side lists. */

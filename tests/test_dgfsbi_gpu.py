@@ -221,3 +221,14 @@ def test_dgfsbi_maxwellian_expr_initial_condition(cuda, prec, tol):
                 T = 1 + 0.05 * x
                 want[e, j] = n * (m[p] / (np.pi * T))**1.5 * np.exp(-m[p] * np.sum((cv - u)**2, 0) / T)
         assert rel_l2(s.bank(p, 0).double().cpu().numpy(), want) < tol
+
+
+def test_dgfsbi_nancheck_covers_every_species(cuda):
+    cfg, be, s = _system(precision='single')
+    cfg.set('soln-plugin-nancheck', 'nsteps', '1')
+    integ = get_integrator(be, s, cfg)
+    integ.advance_to(2e-4)
+    integ.nancheck()
+    s.bank(1, integ._idxcurr)[0, 0, 5] = float('inf')
+    with pytest.raises(RuntimeError, match='NaNs detected'):
+        integ.nancheck()

@@ -276,3 +276,17 @@ def test_tensor_factored_rhs_matches_dense(cuda, kind, order, prec, tol):
     base = 0.5 * u + 0.25 * x1 - 0.5 * x2
     la, lb = (outs[0] - base).double(), (outs[1] - base).double()
     assert float((la - lb).norm() / la.norm()) < tol
+
+
+def test_nancheck_plugin_detects_injected_nan(cuda):
+    """[soln-plugin-nancheck] nsteps: a clean run passes; a NaN written into
+    the state on the host side is caught by the device status word at the
+    next check (plugins/nancheck.py:17-22), with RuntimeError."""
+    cfg, be, mesh, s = _system('quad', 2, 'single', Nv=8, Nrho=4, M=6)
+    cfg.set('soln-plugin-nancheck', 'nsteps', '1')
+    integ = get_integrator(be, s, cfg)
+    integ.advance_to(2 * 5e-4)
+    assert integ.nacptsteps == 2
+    integ.soln[1, 3, 17] = float('nan')
+    with pytest.raises(RuntimeError, match='NaNs detected'):
+        integ.advance_to(3 * 5e-4)

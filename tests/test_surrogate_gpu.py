@@ -284,3 +284,36 @@ def test_hybrid_recheck_every_second_call(small_fit):
     assert st1['rechecked_cells'] == 200 and st2['rechecked_cells'] == 200
     assert st2['spectral_cells'] == 0
     assert st2['recheck_rel_l2'] == st1['recheck_rel_l2']
+
+
+@pytest.mark.parametrize('project', [True, False])
+def test_nan_surrogate_falls_back_to_spectral(small_fit, project):
+    """Host-side fault injection: a NaN in the output layer makes every
+    surrogate row non-finite; the scatter lists those cells and the spectral
+    operator fills them, so the result equals the plain operator bitwise
+    (re-checked cells keep their spectral Q)."""
+    be, vm, sm, q = small_fit
+    gen = torch.Generator(device=be.device).manual_seed(11)
+    f = sample_family(vm.c0(), 200, gen, be.device)
+    plain = torch.empty_like(f)
+    sm.collide(f, plain, project=project, exact=False)
+    saved = q.W[3].clone()
+    try:
+        q.W[3][0, 0] = float('nan')
+        q._fold()
+        h = HybridCollider(q, threshold=float('inf'), recheck=0.1, project=project)
+        out = torch.full_like(f, 7.0)
+        h(f, out)
+        torch.cuda.synchronize()
+        st = h.stats()
+        assert st['surrogate_cells'] == 200 and st['rechecked_cells'] > 0
+        assert st['fallback_cells'] == 200 - st['rechecked_cells']
+        assert torch.equal(out, plain)
+    finally:
+        q.W[3].copy_(saved)
+        q._fold()
+    # a healthy surrogate falls back nowhere
+    h = HybridCollider(q, threshold=float('inf'), recheck=0.0, project=project)
+    h(f, torch.empty_like(f))
+    torch.cuda.synchronize()
+    assert h.stats()['fallback_cells'] == 0
