@@ -282,7 +282,7 @@ def test_nancheck_plugin_detects_injected_nan(cuda):
     """[soln-plugin-nancheck] nsteps: a clean run passes; a NaN written into
     the state on the host side is caught by the device status word at the
     next check (plugins/nancheck.py:17-22), with RuntimeError."""
-    cfg, be, mesh, s = _system('quad', 2, 'single', Nv=8, Nrho=4, M=6)
+    cfg, be, mesh, s = _system('quad', 2, 'single')
     cfg.set('soln-plugin-nancheck', 'nsteps', '1')
     integ = get_integrator(be, s, cfg)
     integ.advance_to(2 * 5e-4)
