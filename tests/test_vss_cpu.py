@@ -149,3 +149,40 @@ def test_mixture_gram_inverse_projects_like_the_oracle():
                                  + lam[S + 3] * c2)) for p, q in enumerate(Q)]
     want = project_mixture(Q, cv, m)
     assert all(np.allclose(g, w, rtol=0, atol=1e-12) for g, w in zip(got, want))
+
+
+def test_dgfsbi_other_boundary_types_resolve():
+    """Inlet rows carry each species' nden{p+1} Maxwellian, the normal-shock
+    inlet the same row with zero velocity shift; outlet / vanish / specular
+    resolve to their kernel kinds for every species."""
+    from frfs_b200 import _lib
+    from frfs_b200.dgfsbi import SpeciesMesh
+    from frfs_b200.mesh import ElementGeometry, StructuredMesh
+    from frfs_b200.system import DGFSBoundaries
+    cfg = _bi_cfg()
+    n0 = DGFSBiVelocityMesh(_CPUBackend(), cfg, 2).n0()
+    u0 = DGFSBiVelocityMesh(_CPUBackend(), cfg, 2).u0()
+    for name, t in (('x-', 'dgfsbi-inlet'), ('x+', 'dgfsbi-outlet'),
+                    ('y-', 'dgfsbi-wall-specular'), ('y+', 'dgfsbi-inlet-normalshock')):
+        cfg.set(f'soln-bcs-{name}', 'type', t)
+        for k, v in (('nden1', 0.2 * n0), ('nden2', 0.9 * n0), ('T', 273.0 * 1.2),
+                     ('ux', 0.1 * u0), ('uy', 0.0), ('uz', 0.0)):
+            cfg.set(f'soln-bcs-{name}', k, repr(float(v)))
+    be = _CPUBackend()
+    be.fpdtype = torch.float64
+    vm = DGFSBiVelocityMesh(be, cfg, 2)
+    geo = ElementGeometry(StructuredMesh((2, 2), (0.0, -0.5), (1.0, 0.5)), 2)
+    cv, m, cw = vm.cv(), vm.masses(), vm.cw()
+    for p in range(2):
+        w = DGFSBoundaries(be, geo, SpeciesMesh(vm, p), cfg, geo.wall_names)
+        kinds = dict(zip(w.types, w.kind.tolist()))
+        assert kinds['dgfsbi-outlet'] == _lib.BC_OUTLET
+        assert kinds['dgfsbi-inlet'] == _lib.BC_INLET == kinds['dgfsbi-inlet-normalshock']
+        assert kinds['dgfsbi-wall-specular'] == _lib.BC_SPECULAR_X + 1
+        r = w.types.index('dgfsbi-inlet')
+        want = (0.9 if p else 0.2) * (m[p] / (np.pi * 1.2))**1.5 * np.exp(
+            -m[p] * np.sum((cv - np.array([[0.1], [0.0], [0.0]]))**2, 0) / 1.2)
+        assert np.allclose(w.fw[r].numpy(), want, rtol=1e-12, atol=0)
+        assert np.isclose(w.fw[r].numpy().sum() * cw, 0.9 if p else 0.2, rtol=1e-6)
+        rs = w.types.index('dgfsbi-inlet-normalshock')
+        assert np.allclose(w.fw[rs].numpy(), want) and not w.uwall[rs].any()
