@@ -1080,24 +1080,39 @@ def run_gpu(args):
     torch.cuda.synchronize()
     pk_ms = a.elapsed_time(b)
     peak = nsm * 8 * 256 * iters * 16 * 8 * 2 / (pk_ms * 1e-3) / 1e12
-    # ---------------- e2e: host buffers, copies inside the timed region
+    # ---------------- e2e: host buffers, copies inside the timed region.  Every
+    # step uploads its input from pinned host memory and reads its result back;
+    # the result is first copied to a device staging bank, so its device->host
+    # read (copy stream) overlaps the next step's upload and compute.  One
+    # interval covers all steps, the L2 flushes and the last read-back.
     nbytes = fin.numel() * fin.element_size()
     host_in = torch.empty(fin.shape, dtype=fin.dtype, pin_memory=True)
     host_out = torch.empty(fin.shape, dtype=fin.dtype, pin_memory=True)
     host_in.copy_(fin)
+    stage = torch.empty_like(fin)
+    cs = torch.cuda.Stream(device=dev)
+    copied = None
     torch.cuda.synchronize()
-    e2e_ev = []
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
     for _ in range(args.steps):
         flush.fill_(1)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(st)
         fin.copy_(host_in, non_blocking=True)
         integ.step(integ.tcurr, dt)
-        host_out.copy_(fin, non_blocking=True)
-        b.record(st)
-        e2e_ev.append((a, b))
+        if copied is not None:
+            st.wait_event(copied)                  # the previous read-back has left stage
+        stage.copy_(fin)
+        done = torch.cuda.Event()
+        done.record(st)
+        cs.wait_event(done)
+        with torch.cuda.stream(cs):
+            host_out.copy_(stage, non_blocking=True)
+            copied = torch.cuda.Event()
+            copied.record(cs)
+    st.wait_event(copied)
+    b.record(st)
     torch.cuda.synchronize()
-    t_e2e = reduce_max(sum(x.elapsed_time(y) for x, y in e2e_ev) / 1e3, ws)
+    t_e2e = reduce_max(a.elapsed_time(b) / 1e3, ws)
     e2e = ws * args.steps / t_e2e
     # ---------------- CPU baseline (rank 0, N = 1): reference algorithm sample
     cpu = None
