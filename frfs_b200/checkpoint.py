@@ -25,9 +25,15 @@ def _banks(integ):
     return list(s) if isinstance(s, (list, tuple)) else [s]
 
 
+def _npz(path):
+    path = str(path)
+    return path if path.endswith('.npz') else path + '.npz'
+
+
 def save(path, integ):
     """Write the integrator's current solution, time and step count, and
-    the config it runs, to ``path`` (.npz)."""
+    the config it runs, to ``path`` ('.npz' is appended when missing)."""
+    path = _npz(path)
     sysm = integ.system
     banks = _banks(integ)
     arrays = {f'soln_{p}': b.detach().cpu().numpy() for p, b in enumerate(banks)}
@@ -41,6 +47,7 @@ class Checkpoint:
     ``tcurr``, ``nacptsteps`` and ``soln`` (one array per species)."""
 
     def __init__(self, path):
+        path = _npz(path)
         with np.load(path, allow_pickle=False) as z:
             if str(z['format']) != FORMAT:
                 raise ValueError(f'{path}: not a {FORMAT} file')

@@ -48,3 +48,10 @@ def test_shape_mismatch_and_foreign_files_are_refused(tmp_path):
     np.savez(tmp_path / 'other.npz', format=np.array('something-else'))
     with pytest.raises(ValueError):
         checkpoint.load(tmp_path / 'other.npz')
+
+
+def test_extension_is_added(tmp_path):
+    cfg = couette_cfg(8, 4, 6, 5, 2)
+    checkpoint.save(tmp_path / 'run', _Integ(cfg, [torch.ones(2, 9, 512)]))
+    assert (tmp_path / 'run.npz').exists()
+    assert checkpoint.load(tmp_path / 'run').nacptsteps == 7
