@@ -1,6 +1,7 @@
 // Shared definitions for the bdgfs CUDA kernels.
 #pragma once
 #include <cstdint>
+#include <mutex>
 #include <cuda_runtime.h>
 
 #include "../../include/bdgfs.h"
@@ -11,6 +12,29 @@ namespace bdgfs {
 static inline int cuda_status(cudaError_t e)
 {
     return e == cudaSuccess ? BDGFS_OK : BDGFS_ECUDA;
+}
+
+// Largest device ordinal the per-device records below cover.
+constexpr int kMaxDevices = 64;
+
+// Dynamic shared-memory opt-in of `func` on the current device.  The
+// attribute belongs to one (kernel, device) pair, so the caller keeps one
+// record per device (`done[dev]` = the largest size opted in there); the
+// attribute is set only when a size above that record is asked for, so that
+// calls made during CUDA-graph capture issue no attribute change.  Sizes up
+// to 48 KB need no opt-in.  Thread-safe.
+static inline int smem_optin(const void* func, size_t smem, size_t (&done)[kMaxDevices])
+{
+    if (smem <= 48 * 1024) return BDGFS_OK;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BDGFS_ECUDA;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (smem <= done[dev]) return BDGFS_OK;
+    if (cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+        return BDGFS_ECUDA;
+    done[dev] = smem;
+    return BDGFS_OK;
 }
 
 template <typename T>

@@ -1238,14 +1238,9 @@ static int launch(const bdgfs_vhs_grid* grids, int ngrids, const bdgfs_vhs_batch
     a.scratch_per_cta = per;
     a.counter = reinterpret_cast<unsigned long long*>(counter);
     auto k = vhs_collide_kernel<T, NT, V0, V1>;
-    // set once per instantiation (and again only if a larger M needs more), so
-    // that calls made during CUDA-graph capture issue no attribute change
-    static size_t smem_set = 0;
-    if (smem > smem_set) {
-        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
-            return BDGFS_ECUDA;
-        smem_set = smem;
-    }
+    // per device, once per instantiation (and again only if a larger M needs more)
+    static size_t smem_done[kMaxDevices] = {};
+    if (const int rc = smem_optin(reinterpret_cast<const void*>(k), smem, smem_done)) return rc;
     if (cudaMemsetAsync(counter, 0, sizeof(uint64_t), st) != cudaSuccess)
         return BDGFS_ECUDA;
     k<<<unsigned(nblk), NT, smem, st>>>(a);
@@ -1346,13 +1341,18 @@ extern "C" int32_t bdgfs_vhs_collide(const bdgfs_vhs_grid* grids, int32_t ngrids
 #define BDGFS_STATIC_SCRATCH_BYTES (size_t(16) << 20)
 static __device__ __align__(256) unsigned char g_vhs_static_scratch[BDGFS_STATIC_SCRATCH_BYTES];
 
-// Device address of the array, looked up once per device (the array's name
-// is only a host-side stand-in in host code).
+// Device address of the array, looked up once per device with that device
+// current (the array's name is only a host-side stand-in in host code).  The
+// lookup is serialised, so host threads may make their first calls at once.
+// The address is kept for the life of the process: after cudaDeviceReset the
+// module may load elsewhere, so this entry point must not be used across a
+// device reset.
 static void* static_scratch_addr(int dev)
 {
-    constexpr int kMaxDev = 64;
-    static void* addr[kMaxDev] = {};
-    if (dev < 0 || dev >= kMaxDev) return nullptr;
+    static std::mutex mu;
+    static void* addr[kMaxDevices] = {};
+    if (dev < 0 || dev >= kMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
     if (!addr[dev]) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_vhs_static_scratch) != cudaSuccess) return nullptr;

@@ -338,9 +338,9 @@ int vss_launch(const bdgfs_vss_args* a, void* scratch, size_t bytes, cudaStream_
     if (ctas < 1) return BDGFS_ESCRATCH;
     constexpr size_t sm = VssCfg<T, N>::smem_bytes;
     if constexpr (sm > 0) {
-        const cudaError_t e = cudaFuncSetAttribute(vss_kernel<T, N>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
-        if (e != cudaSuccess) return cuda_status(e);
+        static size_t smem_done[kMaxDevices] = {};
+        if (const int rc = smem_optin(reinterpret_cast<const void*>(vss_kernel<T, N>), sm, smem_done))
+            return rc;
     }
     vss_kernel<T, N><<<unsigned(ctas > 65535 ? 65535 : ctas), VssCfg<T, N>::threads, sm, st>>>(
         *a, static_cast<cpx<T>*>(scratch));

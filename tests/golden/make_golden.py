@@ -1,9 +1,9 @@
 """Generate golden fixtures from the reference's own Python modules.
 
-Run in a container that has the reference checkout (read-only) at
-REFERENCE_ROOT (default /root/reference):
+Run in a container that has the reference checkout (read-only), giving
+the checkout's root as the one argument:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <reference-root>
 
 It imports the reference's pure-numpy modules unchanged, with four alias
 shims for Python 3.12 / numpy 2 (``collections.Iterable``/``Sequence``,
@@ -33,7 +33,9 @@ import types
 
 import numpy as np
 
-REF = os.environ.get('REFERENCE_ROOT', '/root/reference')
+if len(sys.argv) != 2 or not os.path.isdir(os.path.join(sys.argv[1], 'frfs')):
+    sys.exit('usage: make_golden.py <reference-root>  (the directory holding frfs/)')
+REF = os.path.abspath(sys.argv[1])
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 # --- alias shims (no edits to the reference) -------------------------------

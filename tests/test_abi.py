@@ -73,3 +73,49 @@ def test_invalid_arguments_return_status_not_crash():
     assert L.bdgfs_fr_disu(None, None, None, None) == -1
     assert L.bdgfs_residual(None, None, 0, 0, None, None) == -1
     assert L.bdgfs_vhs_scratch_bytes(None, 0, 1) == 0
+
+
+def _header_params(name):
+    """Number of parameters of `name` as include/bdgfs.h declares it."""
+    txt = re.sub(r'/\*.*?\*/', '', open(HEADER).read(), flags=re.S)
+    m = re.search(r'\b' + name + r'\s*\(([^)]*)\)\s*;', txt)
+    assert m, name
+    args = m.group(1).strip()
+    return 0 if args in ('', 'void') else args.count(',') + 1
+
+
+def test_reference_side_binding_matches_header_and_notes(tmp_path):
+    """The stub INTEGRATION.md shows is frfs_b200/refbinding.py verbatim; its
+    structures have the header's layout and each bound entry point the
+    header's parameter count, and the library exports every one of them."""
+    from frfs_b200 import refbinding as rb
+    notes = open(os.path.join(ROOT, 'INTEGRATION.md')).read()
+    m = re.search(r'<!-- refbinding\.py begin -->\n```python\n(.*?)```\n<!-- refbinding\.py end -->',
+                  notes, flags=re.S)
+    assert m, 'INTEGRATION.md lost the binding block'
+    src = open(os.path.join(ROOT, 'frfs_b200', 'refbinding.py')).read()
+    assert m.group(1) == src
+    for name, (_, args) in rb.SIGNATURES.items():
+        assert _header_params(name) == len(args), name
+    L = rb.load(_lib.LIBPATH)
+    for name in rb.SIGNATURES:
+        assert hasattr(L, name)
+    if shutil.which('gcc') is None:
+        pytest.skip('no C compiler')
+    mirror = {'bdgfs_vhs_grid': rb.VhsGrid, 'bdgfs_vhs_batch': rb.VhsBatch,
+              'bdgfs_vss_args': rb.VssArgs}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"',
+             'int main(void) {']
+    for cname, cls in mirror.items():
+        lines.append(f'printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ['return 0;', '}']
+    (tmp_path / 'off.c').write_text('\n'.join(lines))
+    subprocess.check_call(['gcc', str(tmp_path / 'off.c'), '-o', str(tmp_path / 'off')])
+    import ctypes
+    for line in subprocess.check_output([str(tmp_path / 'off')], text=True).splitlines():
+        cname, field, val = line.split()
+        cls = mirror[cname]
+        got = ctypes.sizeof(cls) if field == 'sizeof' else getattr(cls, field).offset
+        assert got == int(val), (cname, field)
