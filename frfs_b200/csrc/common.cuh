@@ -1,7 +1,9 @@
 // Shared definitions for the bdgfs CUDA kernels.
 #pragma once
 #include <cstdint>
+#include <map>
 #include <mutex>
+#include <utility>
 #include <cuda_runtime.h>
 
 #include "../../include/bdgfs.h"
@@ -14,26 +16,28 @@ static inline int cuda_status(cudaError_t e)
     return e == cudaSuccess ? BDGFS_OK : BDGFS_ECUDA;
 }
 
-// Largest device ordinal the per-device records below cover.
+// Largest device ordinal the per-device records cover.
 constexpr int kMaxDevices = 64;
 
-// Dynamic shared-memory opt-in of `func` on the current device.  The
-// attribute belongs to one (kernel, device) pair, so the caller keeps one
-// record per device (`done[dev]` = the largest size opted in there); the
-// attribute is set only when a size above that record is asked for, so that
-// calls made during CUDA-graph capture issue no attribute change.  Sizes up
-// to 48 KB need no opt-in.  Thread-safe.
-static inline int smem_optin(const void* func, size_t smem, size_t (&done)[kMaxDevices])
+// Dynamic shared-memory opt-in of kernel `func` on the current device.  The
+// attribute belongs to one (kernel, device) pair, so the record is kept per
+// pair (the largest size opted in); the attribute is set only when a size
+// above that record is asked for, so that calls made during CUDA-graph
+// capture issue no attribute change.  Sizes up to 48 KB need no opt-in.
+// Thread-safe.
+static inline int smem_optin(const void* func, size_t smem)
 {
     if (smem <= 48 * 1024) return BDGFS_OK;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BDGFS_ECUDA;
     static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> done;
     std::lock_guard<std::mutex> lock(mu);
-    if (smem <= done[dev]) return BDGFS_OK;
+    size_t& have = done[{func, dev}];
+    if (smem <= have) return BDGFS_OK;
     if (cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
         return BDGFS_ECUDA;
-    done[dev] = smem;
+    have = smem;
     return BDGFS_OK;
 }
 

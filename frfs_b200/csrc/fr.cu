@@ -670,8 +670,7 @@ static int rhs_launch_vb(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl, cons
     auto k = TPP ? (uf ? rhs_kernel<T, ND, NU, NF, VB, false, RING, TPP>
                        : rhs_kernel<T, ND, NU, NF, VB, true, RING, TPP>)
                  : (fsel ? rhs_kernel<T, ND, NU, NF, VB, true, RING> : rhs_kernel<T, ND, NU, NF, VB, false, RING>);
-    static size_t smem_done[kMaxDevices] = {};
-    if (const int rc = smem_optin(reinterpret_cast<const void*>(k), smem, smem_done)) return rc;
+    if (const int rc = smem_optin(reinterpret_cast<const void*>(k), smem)) return rc;
     bdgfs_fr_walls w0{};
     const bdgfs_fr_tensor t0{};
     k<<<g, 128, smem, st>>>(*el, wl ? *wl : w0, static_cast<const T*>(u), static_cast<const T*>(uf),

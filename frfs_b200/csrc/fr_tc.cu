@@ -284,8 +284,7 @@ int launch(const bdgfs_fr_eles& el, const bdgfs_fr_walls& wl, const float* u, co
     if (bx > 65535 || el.neles > 65535) return BDGFS_EUNSUPPORTED;
     const size_t smem = S::BYTES + 1024;
     // dynamic shared-memory opt-in, once per device
-    static size_t smem_done[kMaxDevices] = {};
-    if (const int rc = smem_optin(reinterpret_cast<const void*>(rhs_tc_kernel<ND, NU, NF>), smem, smem_done))
+    if (const int rc = smem_optin(reinterpret_cast<const void*>(rhs_tc_kernel<ND, NU, NF>), smem))
         return rc;
     rhs_tc_kernel<ND, NU, NF><<<dim3(unsigned(bx), unsigned(el.neles)), THREADS, smem, st>>>(
         el, wl, u, uf, out, a, b, x1, c1, x2, c2, chunk, nullptr);

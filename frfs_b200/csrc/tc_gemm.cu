@@ -324,8 +324,7 @@ extern "C" int32_t bdgfs_gemm(const bdgfs_gemm_args* g, void* stream)
     const dim3 grid{static_cast<unsigned>(gx), static_cast<unsigned>(gy), 1u};
     const size_t smem = 4 * tc::TILE_BYTES;
     auto launch = [&](auto kern, auto a, auto b) -> int32_t {
-        static size_t smem_done[kMaxDevices] = {};
-        if (const int rc = smem_optin(reinterpret_cast<const void*>(kern), smem, smem_done)) return rc;
+        if (const int rc = smem_optin(reinterpret_cast<const void*>(kern), smem)) return rc;
         kern<<<grid, tc::THREADS, smem, st>>>(*g, a, b);
         return cuda_status(cudaGetLastError());
     };

@@ -1238,9 +1238,8 @@ static int launch(const bdgfs_vhs_grid* grids, int ngrids, const bdgfs_vhs_batch
     a.scratch_per_cta = per;
     a.counter = reinterpret_cast<unsigned long long*>(counter);
     auto k = vhs_collide_kernel<T, NT, V0, V1>;
-    // per device, once per instantiation (and again only if a larger M needs more)
-    static size_t smem_done[kMaxDevices] = {};
-    if (const int rc = smem_optin(reinterpret_cast<const void*>(k), smem, smem_done)) return rc;
+    // per device, once (and again only if a larger M needs more)
+    if (const int rc = smem_optin(reinterpret_cast<const void*>(k), smem)) return rc;
     if (cudaMemsetAsync(counter, 0, sizeof(uint64_t), st) != cudaSuccess)
         return BDGFS_ECUDA;
     k<<<unsigned(nblk), NT, smem, st>>>(a);

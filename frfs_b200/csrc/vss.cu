@@ -338,8 +338,7 @@ int vss_launch(const bdgfs_vss_args* a, void* scratch, size_t bytes, cudaStream_
     if (ctas < 1) return BDGFS_ESCRATCH;
     constexpr size_t sm = VssCfg<T, N>::smem_bytes;
     if constexpr (sm > 0) {
-        static size_t smem_done[kMaxDevices] = {};
-        if (const int rc = smem_optin(reinterpret_cast<const void*>(vss_kernel<T, N>), sm, smem_done))
+        if (const int rc = smem_optin(reinterpret_cast<const void*>(vss_kernel<T, N>), sm))
             return rc;
     }
     vss_kernel<T, N><<<unsigned(ctas > 65535 ? 65535 : ctas), VssCfg<T, N>::threads, sm, st>>>(
