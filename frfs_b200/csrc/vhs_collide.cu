@@ -659,9 +659,18 @@ __device__ __forceinline__ void p2_pass1_spectrum(int tr, const float4* ez, floa
     }
 }
 
+// SPLIT: the barrier that frees the work cube after the x-pass loads is an
+// mbarrier (arrive right after the loads, wait just before the next z-pass
+// stores), so the x-pass DFT, the S_p update and the next z-pass spectrum and
+// DFT of a warp overlap the other warps' loads instead of waiting at a CTA
+// barrier; two CTA barriers per transform remain (z stored, y stored).
+// wfree: that mbarrier (NT arrivals per phase), wpar: this thread's phase
+// parity, counter: the work counter, whose bit 62 a timed-out wait sets.
+template <bool SPLIT>
 __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict__ f,
                                float* __restrict__ Qout, double* mom, int flags,
-                               unsigned char* smem, unsigned char* scratch, uint32_t tmem)
+                               unsigned char* smem, unsigned char* scratch, uint32_t tmem,
+                               uint64_t* wfree, uint32_t& wpar, unsigned long long* counter)
 {
     using namespace p2;
     const int project = flags & BDGFS_PROJECT;
@@ -750,15 +759,15 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
         }
         __syncthreads();
 
-        for (int qt = 0; qt < M * ntr; ++qt) {
-            const int q = qt / ntr, tr = qt % ntr;
-            const cpx<float>* ep = ph + q * 3 * N;
-            // ---- pass 1: spectrum, inverse along z (pencil pairs of the table) ----
-            {
+        if constexpr (SPLIT) {
+            const int nq = M * ntr;
+            // pass 1 of transform qt: spectrum and inverse DFT along z (registers)
+            auto zpass = [&](int qt, float2 (&vr)[N], float2 (&vi)[N]) {
+                const int q = qt / ntr, tr = qt % ntr;
+                const cpx<float>* ep = ph + q * 3 * N;
                 float aA, bA, cA, aB, bB, cB;
                 p2_coef(ep, kxA, kyA, tr, aA, bA, cA);
                 p2_coef(ep, kxB, kyB, tr, aB, bB, cB);
-                float2 vr[N], vi[N];
                 if (single_warp)
                     p2_pass1_spectrum<true>(tr, ezz + q * N, f2(aA, aB), f2(bA, bB), f2(cA, cB),
                                             fa, fb, single, vr, vi);
@@ -766,6 +775,8 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
                     p2_pass1_spectrum<false>(tr, ezz + q * N, f2(aA, aB), f2(bA, bB), f2(cA, cB),
                                              fa, fb, single, vr, vi);
                 dft_p2<N, +1>(vr, vi);
+            };
+            auto zstore = [&](const float2 (&vr)[N], const float2 (&vi)[N]) {
 #pragma unroll
                 for (int z = 0; z < N; z += 2) {
                     st2(Wr + offA + z, f2(vr[z].x, vr[z + 1].x));
@@ -773,49 +784,140 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
                     st2(Wr + offB + z, f2(vr[z].y, vr[z + 1].y));
                     st2(Wi + offB + z, f2(vi[z].y, vi[z + 1].y));
                 }
-            }
-            __syncthreads();
-            // ---- pass 2: inverse along y ----
+            };
             {
                 float2 vr[N], vi[N];
-#pragma unroll
-                for (int j = 0; j < N; ++j) { vr[j] = ld2(Wr + ybase + j * RS); vi[j] = ld2(Wi + ybase + j * RS); }
-                dft_p2<N, +1>(vr, vi);
-#pragma unroll
-                for (int j = 0; j < N; ++j) { st2(Wr + ybase + j * RS, vr[j]); st2(Wi + ybase + j * RS, vi[j]); }
+                zpass(0, vr, vi);
+                zstore(vr, vi);
             }
-            __syncthreads();
-            // ---- pass 3: inverse along x, S_p += Re(w^2) = (re + im)(re - im) ----
-            {
-                float2 vr[N], vi[N];
+            for (int qt = 0; qt < nq; ++qt) {
+                const int tr = qt % ntr;
+                __syncthreads();                            // z-pass of qt stored
+                {                                           // pass 2: inverse along y
+                    float2 vr[N], vi[N];
 #pragma unroll
-                for (int i = 0; i < N; ++i) { vr[i] = ld2(Wr + i * PS + xbase); vi[i] = ld2(Wi + i * PS + xbase); }
-                dft_p2<N, +1>(vr, vi);
-                const float2 m1 = f2(-1.f, -1.f);
-                tc::tmem_wait_st();
+                    for (int j = 0; j < N; ++j) { vr[j] = ld2(Wr + ybase + j * RS); vi[j] = ld2(Wi + ybase + j * RS); }
+                    dft_p2<N, +1>(vr, vi);
 #pragma unroll
-                for (int c = 0; c < N / 8; ++c) {
-                    uint32_t r[16];
-                    if (qt > 0) {
-                        tc::tmem_ld16_issue(ts + 16 * c, r);
-                        tc::tmem_wait();
-                    } else {
+                    for (int j = 0; j < N; ++j) { st2(Wr + ybase + j * RS, vr[j]); st2(Wi + ybase + j * RS, vi[j]); }
+                }
+                __syncthreads();                            // y-pass stored
+                const bool more = qt + 1 < nq;
+                {                                           // pass 3: inverse along x, S_p += Re(w^2)
+                    float2 vr[N], vi[N];
 #pragma unroll
-                        for (int k = 0; k < 16; ++k) r[k] = 0u;
+                    for (int i = 0; i < N; ++i) { vr[i] = ld2(Wr + i * PS + xbase); vi[i] = ld2(Wi + i * PS + xbase); }
+                    if (more) tc::mbar_arrive(wfree);       // this thread is done reading W
+                    dft_p2<N, +1>(vr, vi);
+                    const float2 m1 = f2(-1.f, -1.f);
+                    tc::tmem_wait_st();
+#pragma unroll
+                    for (int c = 0; c < N / 8; ++c) {
+                        uint32_t r[16];
+                        if (qt > 0) {
+                            tc::tmem_ld16_issue(ts + 16 * c, r);
+                            tc::tmem_wait();
+                        } else {
+#pragma unroll
+                            for (int k = 0; k < 16; ++k) r[k] = 0u;
+                        }
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) {
+                            const int x = 8 * c + k;
+                            const float2 d = tr == 0 ? __ffma2_rn(vi[x], m1, vr[x]) : __ffma2_rn(vr[x], m1, vi[x]);
+                            const float2 sv = __ffma2_rn(__fadd2_rn(vr[x], vi[x]), d,
+                                                         f2(__uint_as_float(r[2 * k]), __uint_as_float(r[2 * k + 1])));
+                            r[2 * k] = __float_as_uint(sv.x);
+                            r[2 * k + 1] = __float_as_uint(sv.y);
+                        }
+                        tc::tmem_st16(ts + 16 * c, r);
                     }
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        const int x = 8 * c + k;
-                        const float2 d = tr == 0 ? __ffma2_rn(vi[x], m1, vr[x]) : __ffma2_rn(vr[x], m1, vi[x]);
-                        const float2 sv = __ffma2_rn(__fadd2_rn(vr[x], vi[x]), d,
-                                                     f2(__uint_as_float(r[2 * k]), __uint_as_float(r[2 * k + 1])));
-                        r[2 * k] = __float_as_uint(sv.x);
-                        r[2 * k + 1] = __float_as_uint(sv.y);
+                }
+                if (more) {                                 // pass 1 of the next transform
+                    float2 vr[N], vi[N];
+                    zpass(qt + 1, vr, vi);
+                    // every thread's x-pass loads done: W is free (bounded wait;
+                    // on expiry bit 62 of the work counter ends the launch)
+                    uint32_t spins = 0;
+                    while (!tc::mbar_try(wfree, wpar)) {
+                        if (++spins == (1u << 22)) {
+                            atomicOr(counter, 1ull << 62);
+                            break;
+                        }
                     }
-                    tc::tmem_st16(ts + 16 * c, r);
+                    wpar ^= 1u;
+                    zstore(vr, vi);
                 }
             }
-            __syncthreads();
+            __syncthreads();                                // last x-pass loads done
+        } else {
+            for (int qt = 0; qt < M * ntr; ++qt) {
+                const int q = qt / ntr, tr = qt % ntr;
+                const cpx<float>* ep = ph + q * 3 * N;
+                // ---- pass 1: spectrum, inverse along z (pencil pairs of the table) ----
+                {
+                    float aA, bA, cA, aB, bB, cB;
+                    p2_coef(ep, kxA, kyA, tr, aA, bA, cA);
+                    p2_coef(ep, kxB, kyB, tr, aB, bB, cB);
+                    float2 vr[N], vi[N];
+                    if (single_warp)
+                        p2_pass1_spectrum<true>(tr, ezz + q * N, f2(aA, aB), f2(bA, bB), f2(cA, cB),
+                                                fa, fb, single, vr, vi);
+                    else
+                        p2_pass1_spectrum<false>(tr, ezz + q * N, f2(aA, aB), f2(bA, bB), f2(cA, cB),
+                                                 fa, fb, single, vr, vi);
+                    dft_p2<N, +1>(vr, vi);
+#pragma unroll
+                    for (int z = 0; z < N; z += 2) {
+                        st2(Wr + offA + z, f2(vr[z].x, vr[z + 1].x));
+                        st2(Wi + offA + z, f2(vi[z].x, vi[z + 1].x));
+                        st2(Wr + offB + z, f2(vr[z].y, vr[z + 1].y));
+                        st2(Wi + offB + z, f2(vi[z].y, vi[z + 1].y));
+                    }
+                }
+                __syncthreads();
+                // ---- pass 2: inverse along y ----
+                {
+                    float2 vr[N], vi[N];
+#pragma unroll
+                    for (int j = 0; j < N; ++j) { vr[j] = ld2(Wr + ybase + j * RS); vi[j] = ld2(Wi + ybase + j * RS); }
+                    dft_p2<N, +1>(vr, vi);
+#pragma unroll
+                    for (int j = 0; j < N; ++j) { st2(Wr + ybase + j * RS, vr[j]); st2(Wi + ybase + j * RS, vi[j]); }
+                }
+                __syncthreads();
+                // ---- pass 3: inverse along x, S_p += Re(w^2) = (re + im)(re - im) ----
+                {
+                    float2 vr[N], vi[N];
+#pragma unroll
+                    for (int i = 0; i < N; ++i) { vr[i] = ld2(Wr + i * PS + xbase); vi[i] = ld2(Wi + i * PS + xbase); }
+                    dft_p2<N, +1>(vr, vi);
+                    const float2 m1 = f2(-1.f, -1.f);
+                    tc::tmem_wait_st();
+#pragma unroll
+                    for (int c = 0; c < N / 8; ++c) {
+                        uint32_t r[16];
+                        if (qt > 0) {
+                            tc::tmem_ld16_issue(ts + 16 * c, r);
+                            tc::tmem_wait();
+                        } else {
+#pragma unroll
+                            for (int k = 0; k < 16; ++k) r[k] = 0u;
+                        }
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) {
+                            const int x = 8 * c + k;
+                            const float2 d = tr == 0 ? __ffma2_rn(vi[x], m1, vr[x]) : __ffma2_rn(vr[x], m1, vi[x]);
+                            const float2 sv = __ffma2_rn(__fadd2_rn(vr[x], vi[x]), d,
+                                                         f2(__uint_as_float(r[2 * k]), __uint_as_float(r[2 * k + 1])));
+                            r[2 * k] = __float_as_uint(sv.x);
+                            r[2 * k + 1] = __float_as_uint(sv.y);
+                        }
+                        tc::tmem_st16(ts + 16 * c, r);
+                    }
+                }
+                __syncthreads();
+            }
         }
 
         // ---- Gh += gw_p * FFT(S_p) (kx <= N/2) ----
@@ -1002,15 +1104,16 @@ template <typename T, int N, int NT, bool WG, bool SG, int GR = 0, bool SL = fal
 struct Variant {
     using L = QLayout<T, N, NT, WG, SG, SL>;
     static constexpr int n = N;
-    static constexpr bool wg = WG, sg = SG, sl = SL, pk = false;
+    static constexpr bool wg = WG, sg = SG, sl = SL, pk = false, split = false;
     static constexpr int gr = GR;
 };
 
-// packed Nv = 24 FP32 variant (288 threads)
+// packed Nv = 24 FP32 variant (288 threads); SPLIT: split work-cube barrier
+template <bool SPLIT = false>
 struct VariantP2 {
     using L = QLayoutP2;
     static constexpr int n = p2::N;
-    static constexpr bool wg = false, sg = false, sl = false, pk = true;
+    static constexpr bool wg = false, sg = false, sl = false, pk = true, split = SPLIT;
     static constexpr int gr = 0;
 };
 
@@ -1023,11 +1126,14 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
     __shared__ int64_t s_item;
     __shared__ int64_t s_start[5];
     __shared__ uint32_t s_tmem;
+    __shared__ __align__(8) uint64_t s_wfree;
     constexpr bool kPacked = V0::pk || V1::pk;
     if constexpr (kPacked) {
         if (threadIdx.x < 32) tc::tmem_alloc(&s_tmem, p2::TMEM_COLS);
+        if (threadIdx.x == 0) tc::mbar_init(&s_wfree, NT);
         tc::tc_fence_before();
     }
+    uint32_t wpar = 0;
     unsigned char* scratch = a.scratch + size_t(blockIdx.x) * a.scratch_per_cta;
     if (threadIdx.x == 0) {
         // per-batch counts: the host size, or a device count when given
@@ -1067,14 +1173,16 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
         double* mom = bt.moments ? bt.moments + dof * 10 : nullptr;
         if (g.Nv == V0::n) {
             if constexpr (V0::pk)
-                collide_one_p2(g, f, Q, mom, a.flags, smem, scratch, tmem);
+                collide_one_p2<V0::split>(g, f, Q, mom, a.flags, smem, scratch, tmem, &s_wfree, wpar,
+                                          a.counter);
             else
                 collide_one<T, V0::n, NT, V0::wg, V0::sg, V0::gr, V0::sl>(
                     g, f, Q, mom, a.flags, smem, scratch);
         } else if constexpr (V1::n > 0) {
             if (g.Nv == V1::n) {
                 if constexpr (V1::pk)
-                    collide_one_p2(g, f, Q, mom, a.flags, smem, scratch, tmem);
+                    collide_one_p2<V1::split>(g, f, Q, mom, a.flags, smem, scratch, tmem, &s_wfree,
+                                              wpar, a.counter);
                 else
                     collide_one<T, V1::n, NT, V1::wg, V1::sg, V1::gr, V1::sl>(
                         g, f, Q, mom, a.flags, smem, scratch);
@@ -1094,7 +1202,7 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
 
 struct NoVariant {
     static constexpr int n = 0;
-    static constexpr bool wg = false, sg = false, sl = false, pk = false;
+    static constexpr bool wg = false, sg = false, sl = false, pk = false, split = false;
     static constexpr int gr = 0;
     struct L {
         static constexpr int WS = 0;
@@ -1173,8 +1281,11 @@ static const Entry kEntries[] = {
      &launch<float, 256, VARIANT(float, 24, 256, false, false), VARIANTS(float, 256)>,
      &entry_per_cta<float, 256, VARIANT(float, 24, 256, false, false), VARIANTS(float, 256)>},
     // 24^3 packed: two pencils per thread on f32x2 arithmetic
-    {0, 24, 0, 288, &launch<float, 288, VariantP2, NoVariant>,
-     &entry_per_cta<float, 288, VariantP2, NoVariant>},
+    {0, 24, 0, 288, &launch<float, 288, VariantP2<>, NoVariant>,
+     &entry_per_cta<float, 288, VariantP2<>, NoVariant>},
+    // the same with the split work-cube barrier
+    {0, 24, 0, 288, &launch<float, 288, VariantP2<true>, NoVariant>,
+     &entry_per_cta<float, 288, VariantP2<true>, NoVariant>},
 };
 static constexpr int kNumEntries = int(sizeof(kEntries) / sizeof(kEntries[0]));
 
