@@ -85,6 +85,34 @@ class FROracle:
             bc[w, 1] = np.sum(np.where(fac < 0, fac * fw * self.cw, 0.0))
         return bc
 
+    def update_bc_from_state(self, u):
+        """update_bc from the solution itself, with the face values formed
+        only at the wall points (the same sums as ``update_bc(disu(u))``;
+        keeps the full velocity set without a mesh-wide face array)."""
+        g = self.geo
+        uf = {}
+        for e, f in g.wall_fpts:
+            if (e, f) not in uf:
+                uf[e, f] = self.M0[f] @ u[e]
+
+        class _Faces:
+            def __getitem__(_, ef):
+                return uf[ef]
+        return self.update_bc(_Faces())
+
+    def restrict(self, vsel):
+        """The same operator on the velocity subset vsel.  The FR operator
+        acts on every velocity separately; only the diffuse-wall sums couple
+        them, so pass ``bc`` from the full set (``update_bc_from_state``) to
+        ``rhs`` of the restricted oracle."""
+        import copy
+        if any(kind == 'dgfs-wall-specular' for _, _, kind in self.walls):
+            raise ValueError('the specular wall couples velocities: no restriction')
+        sub = copy.copy(self)
+        sub.cv = self.cv[:, vsel]
+        sub.walls = [(Uw, np.asarray(fw)[vsel], kind) for Uw, fw, kind in self.walls]
+        return sub
+
     def _rusanov(self, ul, ur, n):
         nc = sum(n[j] * self.cv[j] for j in range(self.ndims))
         return 0.5 * nc * (ul + ur) + 0.5 * np.abs(nc) * (ul - ur)

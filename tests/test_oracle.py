@@ -130,3 +130,35 @@ def test_bkw_known_answer():
     scale = np.dot(q, dfdt) / np.dot(dfdt, dfdt)
     assert scale > 0
     assert rel_l2(q, scale * dfdt) < 2e-2
+
+
+def test_fr_oracle_velocity_restriction_and_wall_sums():
+    """The restricted FR oracle on a velocity subset, with the diffuse-wall
+    sums taken from the full set at the wall points only, equals the full
+    oracle on that subset (velocities are independent in the FR operator)."""
+    from frfs_b200.mesh import ElementGeometry, StructuredMesh
+    from oracle.fr import FROracle
+    g = np.load(os.path.join(GOLD, 'shapes_quad_p2.npz'))
+    geo = ElementGeometry(StructuredMesh((3, 2), (0.0, -0.5), (1.0, 0.5), periodic='x'), 2)
+    c0 = np.linspace(-3, 3, 6)
+    N = len(c0)
+    idx = np.arange(N**3)
+    cv = np.stack([c0[idx // (N * N)], c0[(idx // N) % N], c0[idx % N]])
+    fw = np.exp(-np.sum(cv**2, axis=0))
+    walls = [(np.array([-0.3, 0, 0]), fw, 'dgfs-wall-diffuse'),
+             (np.array([0.3, 0, 0]), fw, 'dgfs-wall-diffuse')]
+    nw = len(geo.wall_fpts)
+    bcid = np.asarray(geo.wall_bcid)
+    assert set(bcid.tolist()) == {0, 1}
+    orc = FROracle({'M0': g['M0'], 'M132': g['M132'], 'M3': g['M3']}, geo, c0, 0.1, walls,
+                   bcid=bcid)
+    rng = np.random.default_rng(1)
+    u = fw[None, None, :] * (1 + 0.2 * rng.uniform(size=(geo.smats.shape[0], 9, N**3)))
+    assert nw > 0
+    bc_full = orc.update_bc(orc.disu(u))
+    bc_state = orc.update_bc_from_state(u)
+    assert np.allclose(bc_full, bc_state, rtol=1e-14, atol=0)
+    vsel = np.sort(rng.choice(N**3, size=40, replace=False))
+    L_full = orc.rhs(u)
+    L_sub = orc.restrict(vsel).rhs(u[:, :, vsel], bc=bc_state)
+    assert np.allclose(L_sub, L_full[:, :, vsel], rtol=1e-13, atol=1e-14 * np.abs(L_full).max())
