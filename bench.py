@@ -216,13 +216,17 @@ def _oracle_q_keyed(item):
     import numpy as np
     key, F = item
     orc, scale = _ORCS[key]
+    if len(F) == 0:
+        return key, np.zeros((0, orc.vm.vsize))
     return key, np.stack([scale * orc.Q(f) for f in F])
 
 
-def batched_q_error(arrays, per_grid=16, seed=5):
+def batched_q_error(arrays, per_grid=64, seed=5, counts=None):
     """Relative L2 error of the batched launch's Q against the FP64 reference
     algorithm on a seeded sample of per_grid distributions of each grid
-    (host cores, spawned pool)."""
+    (host cores, spawned pool), and the host cores' Q evaluations per second
+    for the workload's mix of grids (counts: distributions per grid),
+    timed per grid on that sample and extrapolated."""
     import multiprocessing as mp
     from concurrent.futures import ProcessPoolExecutor
     import numpy as np
@@ -231,7 +235,7 @@ def batched_q_error(arrays, per_grid=16, seed=5):
     grids, fs, qs = arrays
     w = BATCHED
     rng = np.random.default_rng(seed)
-    cfgs, items, picks = [], [], {}
+    cfgs, items, picks = [], {}, {}
     for gi, (g, mass) in enumerate(zip(grids, (1.0, w['mass2']))):
         key = f'Nv{g.Nv}'
         from frfs_b200.inifile import Inifile
@@ -245,23 +249,35 @@ def batched_q_error(arrays, per_grid=16, seed=5):
         idx = np.sort(rng.choice(fs[gi].shape[0], size=per_grid, replace=False))
         picks[key] = (gi, idx)
         F = fs[gi][idx].double().cpu().numpy()
-        items += [(key, c) for c in np.array_split(F, max(1, per_grid // 2))]
-    ncores = min(os.cpu_count() or 1, len(items))
+        items[key] = [(key, c) for c in np.array_split(F, per_grid)]
+    ncores = min(os.cpu_count() or 1, per_grid)
+    err, secs = {}, {}
     with ProcessPoolExecutor(max_workers=ncores, mp_context=mp.get_context('spawn'),
                              initializer=_oracle_init_multi, initargs=(cfgs,)) as pool:
-        outs = list(pool.map(_oracle_q_keyed, items))
-    err = {}
-    for key, (gi, idx) in picks.items():
-        Qo = np.concatenate([q for k, q in outs if k == key])
-        # the same conservation projection as the kernel, applied in FP64
-        c0 = grids[gi].c0.double().cpu().numpy()
-        cx, cy, cz = np.meshgrid(c0, c0, c0, indexing='ij')
-        Phi = np.stack([np.ones_like(cx), cx, cy, cz, cx * cx + cy * cy + cz * cz]).reshape(5, -1)
-        lam = np.linalg.solve(Phi @ Phi.T, Phi @ Qo.T)
-        Qo = Qo - (Phi.T @ lam).T
-        Qg = qs[gi][idx].double().cpu().numpy()
-        err[key] = float(np.linalg.norm(Qg - Qo) / np.linalg.norm(Qo))
-    return err
+        list(pool.map(_oracle_q_keyed, [(cfgs[0][0], []) for _ in range(ncores)]))  # start
+        for key, (gi, idx) in picks.items():
+            t0 = time.perf_counter()
+            outs = list(pool.map(_oracle_q_keyed, items[key]))
+            secs[key] = (time.perf_counter() - t0) / per_grid       # wall s per Q, all cores
+            Qo = np.concatenate([q for _, q in outs])
+            # the same conservation projection as the kernel, applied in FP64
+            c0 = grids[gi].c0.double().cpu().numpy()
+            cx, cy, cz = np.meshgrid(c0, c0, c0, indexing='ij')
+            Phi = np.stack([np.ones_like(cx), cx, cy, cz, cx * cx + cy * cy + cz * cz]).reshape(5, -1)
+            lam = np.linalg.solve(Phi @ Phi.T, Phi @ Qo.T)
+            Qo = Qo - (Phi.T @ lam).T
+            Qg = qs[gi][idx].double().cpu().numpy()
+            err[key] = float(np.linalg.norm(Qg - Qo) / np.linalg.norm(Qo))
+    cpu = None
+    if counts is not None:
+        keys = list(picks)
+        t = sum(counts[i] * secs[k] for i, k in enumerate(keys))
+        cpu = {'value': sum(counts) / t, 'unit': 'Q evals/s', 'cores': ncores, 'kind': 'port',
+               'sample': (f'{per_grid} seeded distributions of each grid (reference algorithm, '
+                          '3+3*M*Nrho FP64 FFTs each, spread over the host cores), wall time '
+                          'per distribution extrapolated to the workload mix '
+                          f'{dict(zip(keys, counts))}')}
+    return err, cpu
 
 
 def make_pool(ncores, Nv, Nrho, sz, dev, omega):
@@ -299,6 +315,79 @@ def make_fr_oracle(system):
     ops = {'M0': shp.opmat('M0'), 'M132': shp.opmat('M1 - M3*M2'), 'M3': shp.opmat('M3')}
     walls, rows = system.walls.oracle_walls()
     return FROracle(ops, system.geo, system.vm.c0(), system.vm.cw(), walls, bcid=rows)
+
+
+def _oracle_gl_worker(F):
+    """(Q, loss term) of the reference algorithm for each row of F."""
+    import numpy as np
+    if len(F) == 0:
+        return np.zeros((0, 0)), np.zeros((0, 0))
+    out = [_ORC.gain_loss(f) for f in F]
+    return (np.stack([g - l for g, l in out]), np.stack([l for _, l in out]))
+
+
+def upt_weights(geo):
+    """Quadrature weight x |J| of every solution point, [E * nupts] (the
+    tensor-product GLL rule of the element's solution points)."""
+    import numpy as np
+    shp = geo.shape
+    pts, wts = np.asarray(shp.pts1), np.asarray(shp.wts1)
+    w = np.prod([wts[np.argmin(np.abs(pts[None, :] - shp.upts[:, d:d + 1]), axis=1)]
+                 for d in range(shp.upts.shape[1])], axis=0)
+    return (geo.djac * w[None, :]).reshape(-1)
+
+
+def state_totals(system, bank):
+    """Mesh integrals, in FP64, of the mass, momentum and energy (sum of
+    |c|^2 f cw) of a solution bank."""
+    import torch
+    from frfs_b200.system import raw_moments
+    m = raw_moments(system.eles_scal_upts_inb_full[bank], system.vm)
+    dens = torch.stack([m[:, 0], m[:, 1], m[:, 2], m[:, 3], m[:, 4] + m[:, 7] + m[:, 9]], 1)
+    w = torch.as_tensor(upt_weights(system.geo), dtype=torch.float64, device=m.device)
+    return (w[:, None] * dens).sum(0).cpu().numpy()
+
+
+def drift(before, after, conserved=(0, 1, 2, 3, 4)):
+    """Relative change of the conserved totals over one step: mass and
+    energy relative to themselves, momentum relative to the mass (unit
+    speed)."""
+    out = {}
+    names = ['mass', 'momentum_x', 'momentum_y', 'momentum_z', 'energy']
+    for k in conserved:
+        ref = abs(before[0]) if 1 <= k <= 3 else abs(before[k])
+        out[names[k]] = float(abs(after[k] - before[k]) / ref)
+    return out
+
+
+def q_conservation(collide, f, q, c0, cw, chunk=2048):
+    """Conservation of one collision launch over every distribution of f:
+    the FP64 moments C.Q the launch reports before and after its projection
+    (after: FP64, before the cast to the state's type) and the FP64 moments
+    of the Q it wrote, each relative to C.|Q| (C = cw {1, c, |c|^2}); max
+    over distributions and the five moments."""
+    import torch
+    n3 = c0.numel()**3
+    f2, q2 = f.reshape(-1, n3), q.reshape(-1, n3)
+    ndof = f2.shape[0]
+    mom = torch.empty(ndof, 10, dtype=torch.float64, device=f.device)
+    collide(f2, q2, mom)
+    cx, cy, cz = torch.meshgrid(c0, c0, c0, indexing='ij')
+    phi = torch.stack([torch.ones_like(cx), cx, cy, cz, cx * cx + cy * cy + cz * cz]).reshape(5, -1)
+    worst = {'projected_fp64': 0.0, 'written': 0.0, 'unprojected': 0.0}
+    for i0 in range(0, ndof, chunk):
+        Q = q2[i0:i0 + chunk].double()
+        scale = (Q.abs() @ phi.abs().T) * cw
+        wr = (Q @ phi.T) * cw
+        m = mom[i0:i0 + chunk]
+        worst['projected_fp64'] = max(worst['projected_fp64'], float((m[:, 5:].abs() / scale).max()))
+        worst['written'] = max(worst['written'], float((wr.abs() / scale).max()))
+        worst['unprojected'] = max(worst['unprojected'], float((m[:, :5].abs() / scale).max()))
+    return {'max_rel_' + k: v for k, v in worst.items()} | {
+        'definition': 'max over distributions and moments of |cw sum phi Q| / (cw sum |phi| |Q|), '
+                      'phi = {1, c, |c|^2}: FP64 sums of the launch before its projection '
+                      '(unprojected), after it (projected_fp64, before the cast) and of the '
+                      'FP32 Q it wrote'}
 
 
 def run_reference(args):
@@ -367,8 +456,9 @@ def config_block(n):
 # ---------------------------------------------------------------- other configs
 BATCHED = dict(n24=24576, n32=8192, Nrho=16, M=12, dev=6, omega=0.81, mass2=2.0)
 # DRAM bytes (read + write) of one collision launch on the 2048-DOF Couette
-# state, from an ncu capture of the packed Nv=24 variant (114.6 MB + 99.5 MB)
-Q_LAUNCH_DRAM_BYTES = 114.58e6 + 99.50e6
+# state, from an ncu capture of the packed Nv=24 variant with the split
+# work-cube barrier (114.7 MB + 96.3 MB)
+Q_LAUNCH_DRAM_BYTES = 114.69e6 + 96.25e6
 SMALL64 = dict(Nv=16, Nrho=8, M=6, dev=5, omega=0.5, order=2, nx=4, ny=4, dt=1e-3)
 
 
@@ -444,13 +534,17 @@ def batched_q(flush, reps=3, sizes=None):
         ms.append(a.elapsed_time(b))
     t = sum(ms) / len(ms)
     ndof = w['n24'] + w['n32']
+    cons = {}
+    for gi, g in enumerate(grids):
+        cons[f'Nv{g.Nv}'] = q_conservation(lambda f2, q2, m, gi=gi: col([(gi, f2, q2, m)]),
+                                           fs[gi], qs[gi], g.c0.double(), float(g.struct.cw))
     return {'workload': f"two species, {w['n24']} x 24^3 + {w['n32']} x 32^3, mass ratio 2, Nrho=16, M=12, "
                         'one persistent launch in a CUDA graph, FP32 + FP64 projection',
             'q_evals_per_s': ndof / (t * 1e-3), 'ms_per_launch': t,
-            'tiles': [int(x.struct.tile) for x in grids]}, (grids, fs, qs)
+            'tiles': [int(x.struct.tile) for x in grids], 'conservation': cons}, (grids, fs, qs)
 
 
-def small_fp64(flush, steps=20):
+def small_fp64(flush, steps=20, ncores=0):
     """Plain FP64 method: 4x4 periodic quads P2 (144 DOFs), Nv=16, hard
     spheres, Nrho=8, M=6, two seeded Maxwellians per DOF, SSP-RK2 dt=1e-3."""
     import numpy as np
@@ -483,6 +577,39 @@ def small_fp64(flush, steps=20):
             F[e, j] = f
     u.copy_(torch.from_numpy(F))
     integ = get_integrator(be, s, cfg)
+    # one step from the seeded state: conservation, and the same step of the
+    # reference algorithm (FP64 oracle, whole mesh, its Q followed by the
+    # launch's FP64 projection) on the host cores, timed and compared
+    tot0 = state_totals(s, 0)
+    integ.step(0.0, w['dt'])
+    torch.cuda.synchronize()
+    tot1 = state_totals(s, 0)
+    got = s.eles_scal_upts_inb_full[0].cpu().numpy()
+    cpu = err = None
+    if ncores:
+        from oracle.fr import step_rk2
+        from frfs_b200.sphericaldesign import half_sphere_design
+        pool = make_pool(ncores, w['Nv'], w['Nrho'], half_sphere_design(w['M']), w['dev'], w['omega'])
+        orc = make_fr_oracle(s)
+        c0 = s.vm.c0().astype(np.float64)
+        cx, cy, cz = np.meshgrid(c0, c0, c0, indexing='ij')
+        Phi = np.stack([np.ones_like(cx), cx, cy, cz, cx * cx + cy * cy + cz * cz]).reshape(5, -1)
+        E, J, n = F.shape
+
+        def Qo(x):
+            rows = x.reshape(E * J, n)
+            q = np.concatenate(list(pool.map(_oracle_q_worker, np.array_split(rows, ncores))))
+            q -= (Phi.T @ np.linalg.solve(Phi @ Phi.T, Phi @ q.T)).T
+            return q.reshape(E, J, n)
+        t0 = time.perf_counter()
+        uo = step_rk2(F, w['dt'], orc.rhs, Qo)
+        t_cpu = time.perf_counter() - t0
+        pool.shutdown()
+        err = float(np.linalg.norm(got - uo) / np.linalg.norm(uo - F))
+        cpu = {'value': 1.0 / t_cpu, 'unit': 'DG steps/s', 'cores': ncores, 'kind': 'port',
+               'sample': ('one whole SSP-RK2 step of the same state (288 Q evaluations, '
+                          '3+3*M*Nrho FP64 FFTs each, on the host cores + the FR operator '
+                          'twice), no extrapolation')}
     for _ in range(3):
         integ.step(0.0, w['dt'])
     torch.cuda.synchronize()
@@ -496,10 +623,20 @@ def small_fp64(flush, steps=20):
         b.record(st)
         torch.cuda.synchronize()
         tot += a.elapsed_time(b)
+    c0t = torch.as_tensor(s.vm.c0(), dtype=torch.float64, device=be.device)
+    qc = q_conservation(lambda f, q, m: s.sm.collide(f, q, moments=m),
+                        s.eles_scal_upts_inb_full[0], s.eles_scal_upts_inb_full[2], c0t, s.vm.cw())
     return {'workload': '4x4 periodic quads P2 (144 DOFs), Nv=16^3 on [-5,5]^3, hard sphere, '
                         'Nrho=8, M=6, SSP-RK2 dt=1e-3, FP64 (exact-Nyquist collision operator)',
             'dg_steps_per_s': steps / (tot * 1e-3), 'ms_per_step': tot / steps,
-            'dtype': 'f64'}
+            'dtype': 'f64',
+            'step_rel_l2_err_vs_fp64_oracle': err,
+            'error_definition': ('|u_gpu - u_oracle| / |u_oracle - u_0| after one step from the '
+                                 'seeded state (relative to the change the step makes)'),
+            'conservation': {'collision': qc,
+                             'state_drift_per_step': drift(tot0, tot1),
+                             'state_totals': 'GLL-quadrature integrals over the periodic mesh'},
+            'cpu_baseline': cpu}
 
 
 MIXTURE = dict(Nv=24, Nrho=12, M=12, Mpre=12, ndof=1024, masses=(39.96e-3, 83.798e-3),
@@ -842,11 +979,69 @@ def run_hybrid_steps(nsteps, nwarm=3):
                       'surrogate_cells_per_call': stt['surrogate_cells']}))
 
 
-def surrogate_legs(flush, log=None):
+def fp64_subcheck(pool, ncores, f, outs, c0):
+    """Errors of device Q arrays (outs: name -> [m][n]) on the distributions
+    f against the FP64 oracle (reference algorithm + the launch's FP64
+    projection), relative to the oracle's Q and to its loss term
+    prefac f (IFFT(bb2 F^)) (the collision frequency times f)."""
+    import numpy as np
+    F = f.double().cpu().numpy()
+    t0 = time.perf_counter()
+    res = list(pool.map(_oracle_gl_worker, [c for c in np.array_split(F, 4 * ncores) if len(c)]))
+    t = time.perf_counter() - t0
+    Qo = np.concatenate([r[0] for r in res])
+    Lo = np.concatenate([r[1] for r in res])
+    c0 = np.asarray(c0, np.float64)
+    cx, cy, cz = np.meshgrid(c0, c0, c0, indexing='ij')
+    Phi = np.stack([np.ones_like(cx), cx, cy, cz, cx * cx + cy * cy + cz * cz]).reshape(5, -1)
+    Qo = Qo - (Phi.T @ np.linalg.solve(Phi @ Phi.T, Phi @ Qo.T)).T
+    out = {'n': int(F.shape[0]), 'oracle_s': t}
+    for name, q in outs.items():
+        d = q.double().cpu().numpy() - Qo
+        row = np.linalg.norm(d, axis=1) / np.linalg.norm(Qo, axis=1)
+        out[name] = {'rel_l2_vs_q': float(np.linalg.norm(d) / np.linalg.norm(Qo)),
+                     'rel_l2_vs_loss_term': float(np.linalg.norm(d) / np.linalg.norm(Lo)),
+                     'per_row_median': float(np.median(row)),
+                     'per_row_p90': float(np.percentile(row, 90))}
+    return out
+
+
+def cavity_cpu_step(s5, bank, pool, ncores, nq=128, nv=512):
+    """Host cores: one SSP-RK2 step of the reference algorithm on the cavity
+    state, from a bounded sample: Q of nq seeded DOFs (pool) and the FR
+    operator on nv seeded velocities (velocities are independent there),
+    each extrapolated to the whole state."""
+    import numpy as np
+    import torch
+    u = s5.eles_scal_upts_inb_full[bank]
+    E, J, n = u.shape
+    rng = np.random.default_rng(6)
+    pick = np.sort(rng.choice(E * J, nq, replace=False))
+    F = u.reshape(-1, n)[torch.as_tensor(pick, device=u.device)].double().cpu().numpy()
+    t0 = time.perf_counter()
+    list(pool.map(_oracle_q_worker, [c for c in np.array_split(F, ncores) if len(c)]))
+    tq = time.perf_counter() - t0
+    orc = make_fr_oracle(s5)
+    vsel = np.sort(rng.choice(n, nv, replace=False))
+    uh = u[:, :, torch.as_tensor(vsel, device=u.device)].double().cpu().numpy()
+    full = u.cpu().numpy()
+    t1 = time.perf_counter()
+    bc = orc.update_bc_from_state(full)
+    orc.restrict(vsel).rhs(uh, bc=bc)
+    tfr = time.perf_counter() - t1
+    t_step = 2.0 * (tq * (E * J) / nq + tfr * n / nv)
+    return {'value': 1.0 / t_step, 'unit': 'DG steps/s', 'cores': ncores, 'kind': 'port',
+            'sample': (f'Q of {nq} seeded DOFs ({tq:.1f} s on {ncores} processes, reference '
+                       f'algorithm) and the FR operator on {nv} of {n} velocities ({tfr:.2f} s, '
+                       'wall sums over all), each extrapolated to the whole state, 2 stages')}
+
+
+def surrogate_legs(flush, log=None, pool=None, ncores=0):
     """Config 4 (surrogate trained on the Couette family, evaluated on 50000
     held-out seeded distributions) and config 5 (8^3 hex P2 lid-driven
     cavity: plain FP32 spectral vs surrogate hybrid, DG steps/s)."""
     import time
+    import numpy as np
     import torch
     from frfs_b200.backend import CUDABackend
     from frfs_b200.inifile import Inifile
@@ -909,6 +1104,17 @@ def surrogate_legs(flush, log=None):
           'heldout_rel_l2_vs_spectral_q': q.test_err,
           'surrogate_q_evals_per_s': 8192 / (t_sur * 1e-3),
           'spectral_q_evals_per_s': 8192 / (t_spec * 1e-3)}
+    if pool is not None:
+        # 1000 further held-out distributions against the FP64 oracle
+        fo = sample_family(vm.c0(), 1000, torch.Generator(device=be.device).manual_seed(987654),
+                           be.device)
+        qs, qh = torch.empty_like(fo), torch.empty_like(fo)
+        sm.collide(fo, qs, project=True, exact=False)
+        h.collide_surrogate_only(fo, qh)
+        c4['fp64_oracle_subcheck'] = fp64_subcheck(pool, ncores, fo, {'surrogate': qh,
+                                                                      'fp32_spectral': qs},
+                                                   vm.c0())
+
     # ---- config 5: lid-driven cavity
     ini, names = cavity_ini()
     # surrogate for the cavity's near-equilibrium cells (CAVITY family)
@@ -961,6 +1167,23 @@ def surrogate_legs(flush, log=None):
             res[mode].update({'surrogate_cells_per_call': sur / k, 'rechecked_cells_per_step': rec / k,
                               'spectral_cells_per_step': spc / k,
                               'recheck_rel_l2': math.sqrt(num / den) if den > 0 else None})
+        if mode == 'plain' and pool is not None:
+            res[mode]['cpu_baseline'] = cavity_cpu_step(s5, integ._idxcurr, pool, ncores)
+        if hc is not None and pool is not None:
+            # the surrogate on 64 seeded cells it handles in the final state,
+            # against the FP64 oracle: relative to Q and to the loss term
+            fin = s5.eles_scal_upts_inb_full[integ._idxcurr].reshape(-1, s5.vm.vsize())
+            hc.classify(fin, seed=1, recheck=0.0)
+            nsur = int(hc.counts[0])
+            pick = torch.as_tensor(np.sort(np.random.default_rng(4).choice(nsur, min(64, nsur),
+                                                                           replace=False)),
+                                   device=fin.device)
+            fsel = fin.index_select(0, hc.sur_idx[:nsur].long()[pick]).contiguous()
+            qs, qh = torch.empty_like(fsel), torch.empty_like(fsel)
+            sm.collide(fsel, qs, project=True, exact=False)
+            HybridCollider(qc, threshold=float('inf'), recheck=0.0).collide_surrogate_only(fsel, qh)
+            res[mode]['surrogate_cells_fp64_oracle_check'] = fp64_subcheck(
+                pool, ncores, fsel, {'surrogate': qh, 'fp32_spectral': qs}, s5.vm.c0())
         rho, U, T, _, _ = s5.moments(integ._idxcurr)
         fields[mode] = (rho.cpu(), U.cpu(), T.cpu())
         del s5, integ, hc
@@ -1049,9 +1272,22 @@ def run_gpu(args):
     t_max = reduce_max(t_dev, ws)
     value = ws * args.steps / t_max
     ms_per_step = t_max / args.steps * 1e3
-    # ---------------- dominant kernel: Q alone, events on its stream
+    # ---------------- conservation: one more step's state totals, one launch's moments
     fin = system.eles_scal_upts_inb_full[0]
     qout = system.eles_scal_upts_inb_full[2]
+    conservation = None
+    if ws == 1:
+        tot0 = state_totals(system, 0)
+        integ.step(integ.tcurr, dt)
+        tot1 = state_totals(system, 0)
+        c0t = torch.as_tensor(system.vm.c0(), dtype=torch.float64, device=dev)
+        conservation = {
+            'collision': q_conservation(lambda f, q, m: system.sm.collide(f, q, moments=m),
+                                        fin, qout, c0t, system.vm.cw()),
+            'state_drift_per_step': drift(tot0, tot1, conserved=(0,)),
+            'state_totals': ('GLL-quadrature integrals over the mesh; the diffuse walls exchange '
+                             'momentum and energy with the gas, so mass is the conserved total')}
+    # ---------------- dominant kernel: Q alone, events on its stream
     for _ in range(2):
         system.sm.collide(fin, qout)
     torch.cuda.synchronize()
@@ -1133,14 +1369,14 @@ def run_gpu(args):
                'sample': (f'Q of {len(idx)} random DOFs of the same state (reference algorithm, '
                           f'3+3*M*Nrho FP64 FFTs each, {tq:.1f} s on {ncores} processes) + FR '
                           f'operator on the full mesh ({tfr:.2f} s), extrapolated to one step')}
-        pool.shutdown()
     # other measured configurations of the metric (rank 0, single GPU)
     extra = {}
     if ws == 1 and not args.no_extra:
-        extra['plain_fp64_small'] = small_fp64(flush)
+        extra['plain_fp64_small'] = small_fp64(flush, ncores=0 if args.no_cpu else ncores)
         bq, arrays = batched_q(flush)
-        bq['q_rel_l2_err_vs_fp64_reference'] = batched_q_error(arrays)
-        bq['error_sample'] = ('16 seeded distributions per grid, FP64 reference algorithm on the '
+        bq['q_rel_l2_err_vs_fp64_reference'], bq['cpu_baseline'] = batched_q_error(
+            arrays, counts=[BATCHED['n24'], BATCHED['n32']])
+        bq['error_sample'] = ('64 seeded distributions per grid, FP64 reference algorithm on the '
                               'host cores followed by the same conservation projection as the '
                               'kernel (applied in FP64)')
         extra['batched_q'] = bq
@@ -1149,9 +1385,11 @@ def run_gpu(args):
         extra['vss_mixture'] = vss_mixture(flush, peak)
         extra['dgfsbi_couette'] = dgfsbi_couette(flush)
     if ws == 1 and not args.no_surrogate:
-        c4, c5 = surrogate_legs(flush)
+        c4, c5 = surrogate_legs(flush, pool=pool, ncores=ncores)
         extra['surrogate'] = c4
         extra['hybrid_lid_cavity'] = c5
+    if pool is not None:
+        pool.shutdown()
     # gpu launches per step: 2 stages x (collide [+ disu] [+ bc_update] + rhs); the
     # one-part GLL system reads face values from the state (no disu)
     gathers = system.ele.fsel is not None and system.domain is None
@@ -1170,15 +1408,17 @@ def run_gpu(args):
                      'peak_source': 'measured FP32 FMA probe on this GPU (MEASURED_PEAKS.json has '
                                     'no FP32 CUDA-core figure)',
                      'flop_per_launch': flop, 'launch_ms': q_ms,
-                     # dram__bytes_read.sum + dram__bytes_write.sum of one captured launch
-                     # of the same kernel variant on 2048 Nv=24 cubes (ncu --set full);
                      # algorithmic: f in + Q out = 2 x 113 MB
-                     'traffic': Q_LAUNCH_DRAM_BYTES, 'traffic_alg': 2 * 4 * ndof * 24**3},
+                     'traffic': Q_LAUNCH_DRAM_BYTES, 'traffic_alg': 2 * 4 * ndof * 24**3,
+                     'traffic_source': ('not measured in this run: dram__bytes_read.sum + '
+                                        'dram__bytes_write.sum of one ncu capture of this '
+                                        'kernel variant on the same 2048 Couette cubes')},
         'e2e': {'value': e2e, 'unit': 'DG steps/s', 'h2d_bytes_per_step': nbytes,
                 'd2h_bytes_per_step': nbytes},
         'gpu_launches': launches,
         'clocks': clocks,
         'cpu_baseline': cpu,
+        'conservation': conservation,
         **extra,
     }
     if rank == 0:

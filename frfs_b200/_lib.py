@@ -17,7 +17,7 @@ _ERRORS = {-1: 'invalid argument', -2: 'CUDA error', -3: 'unsupported grid/preci
 # Every symbol include/bdgfs.h declares (tests check the export list).
 EXPORTS = (
     'bdgfs_vhs_scratch_bytes', 'bdgfs_vhs_collide', 'bdgfs_vhs_tiles', 'bdgfs_fma_probe',
-    'bdgfs_vhs_collide_static',
+    'bdgfs_vhs_collide_static', 'bdgfs_wait_probe',
     'bdgfs_fr_disu', 'bdgfs_fr_bc_update', 'bdgfs_fr_rhs', 'bdgfs_fr_rhs_gather',
     'bdgfs_fr_bc_update_gather', 'bdgfs_fr_rhs_tensor',
     'bdgfs_moments', 'bdgfs_residual', 'bdgfs_status_check',
@@ -189,6 +189,7 @@ def lib():
             'bdgfs_vss_collide': [vp, vp, C.c_size_t, vp],
             'bdgfs_vss_project': [vp, vp],
             'bdgfs_colsum': [vp, i64, i64, vp, vp],
+            'bdgfs_wait_probe': [C.c_uint32, i32, vp, vp],
             'bdgfs_adamw': [vp, vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float,
                             C.c_float, C.c_float, i64, vp],
         }

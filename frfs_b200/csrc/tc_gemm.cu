@@ -36,9 +36,21 @@ constexpr uint32_t kIdesc = idesc_bf16(BM, BN);
 
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase)
 {
-    for (uint32_t it = 0; it < kWaitLimit; ++it)
-        if (mbar_try(bar, phase)) return true;
-    return false;
+    return mbar_wait_bounded(bar, phase, kWaitLimit);
+}
+
+// Bounded-wait probe: one thread waits on an mbarrier of one expected
+// arrival; with arrive = 0 nothing arrives, so the wait runs out after
+// `limit` polls and the status word gets BDGFS_ETIMEOUT (no copy or MMA is
+// in flight, no TMEM is held); with arrive = 1 the thread arrives first and
+// the wait succeeds (BDGFS_OK).
+__global__ void wait_probe_kernel(uint32_t limit, int arrive, int32_t* status)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    if (arrive) mbar_arrive(&bar);
+    *status = mbar_wait_bounded(&bar, 0, limit) ? BDGFS_OK : BDGFS_ETIMEOUT;
 }
 
 __device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
@@ -340,6 +352,13 @@ extern "C" int32_t bdgfs_gemm(const bdgfs_gemm_args* g, void* stream)
                       static_cast<const __nv_bfloat16*>(g->B));
     return launch(tc_gemm_kernel<float, float>, static_cast<const float*>(g->A),
                   static_cast<const float*>(g->B));
+}
+
+extern "C" int32_t bdgfs_wait_probe(uint32_t limit, int32_t arrive, int32_t* status, void* stream)
+{
+    if (!status || limit < 1) return BDGFS_EINVAL;
+    tc::wait_probe_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(limit, arrive ? 1 : 0, status);
+    return cuda_status(cudaGetLastError());
 }
 
 extern "C" int32_t bdgfs_colsum(const float* X, int64_t M, int64_t N, float* out, void* stream)

@@ -30,6 +30,15 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity)
     return done != 0;
 }
 
+// Poll the mbarrier phase `parity` at most `limit` times; false when the
+// phase did not complete within them (the caller records BDGFS_ETIMEOUT).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t limit)
+{
+    for (uint32_t it = 0; it < limit; ++it)
+        if (mbar_try(bar, parity)) return true;
+    return false;
+}
+
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");

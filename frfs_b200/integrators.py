@@ -127,8 +127,9 @@ class StdEulerDGFSStepper(BaseDGFSStepper):
 
     def _step_kernels(self, t, dt):
         s = self.system
+        s.advect_begin(0, 0)                                 # face values (+ halo posted)
         s.collide(t, 0, 1)                                   # r1 = Q(r0)
-        s.advect_combine(t, 0, 0, a=1.0, b=dt, x1=1, c1=dt)  # r0 += dt (L + Q)
+        s.advect_end(t, a=1.0, b=dt, x1=1, c1=dt)            # r0 += dt (L + Q)
 
 
 class StdTVDRK2DGFSStepper(BaseDGFSStepper):
@@ -138,11 +139,16 @@ class StdTVDRK2DGFSStepper(BaseDGFSStepper):
 
     def _step_kernels(self, t, dt):
         s = self.system
+        # each stage: face values first (their halo exchange, when the mesh is
+        # partitioned, overlaps the collision launch), then Q, then the
+        # fused FR residual + combination
+        s.advect_begin(0, 1)
         s.collide(t, 0, 1)                                        # r1 = Q(r0)
-        s.advect_combine(t, 0, 1, a=1.0, b=dt, x1=1, c1=dt)       # r1 = r0 + dt (L+Q)(r0)
+        s.advect_end(t, a=1.0, b=dt, x1=1, c1=dt)                 # r1 = r0 + dt (L+Q)(r0)
+        s.advect_begin(1, 0)
         s.collide(t + dt, 1, 2)                                   # r2 = Q(r1)
-        s.advect_combine(t + dt, 1, 0, a=0.5, b=0.5 * dt,         # r0 = r0/2 + r1/2
-                         x1=2, c1=0.5 * dt, x2=0, c2=0.5)         #      + dt/2 (L+Q)(r1)
+        s.advect_end(t + dt, a=0.5, b=0.5 * dt,                   # r0 = r0/2 + r1/2
+                     x1=2, c1=0.5 * dt, x2=0, c2=0.5)             #      + dt/2 (L+Q)(r1)
 
 
 class _DGFSBiStepperMixin:

@@ -367,7 +367,13 @@ class DGFSSystem:
                    'bdgfs_fr_bc_update')
 
     def _exchange(self):
-        if self.transport is not None:
+        """Complete the halo exchange of the face values: the one posted by
+        ``advect_begin`` when the transport is asynchronous, else a blocking
+        one now."""
+        pending, self._pending = getattr(self, '_pending', None), None
+        if pending is not None:
+            self.transport.wait(pending)
+        elif self.transport is not None:
             self.transport.exchange(self)
 
     def _fused_rhs(self, a=0.0, b=1.0, x1=None, c1=0.0, x2=None, c2=0.0, out=None, **kw):
@@ -425,10 +431,14 @@ class DGFSSystem:
                 and self._active[0] != self._active[1])
 
     def advect_begin(self, uinbank, outbank):
-        """First half of a stage: face values of the stage input."""
+        """First half of a stage: face values of the stage input, and (with
+        an asynchronous transport) the halo exchange posted, to be completed
+        by ``advect_end``; work queued in between overlaps it."""
         self._active = (uinbank, outbank)
         if not self._gathers():
             self._disu()
+            if self.transport is not None and hasattr(self.transport, 'start'):
+                self._pending = self.transport.start(self)
 
     def advect_end(self, t, a, b, x1=None, c1=0.0, x2=None, c2=0.0):
         """Second half: halo exchange, wall update, fused FR + combination."""

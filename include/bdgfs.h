@@ -106,6 +106,14 @@ int32_t bdgfs_vhs_collide_static(const bdgfs_vhs_grid* grids, int32_t ngrids,
                                  const bdgfs_vhs_batch* batches, int32_t nbatch,
                                  int32_t flags, void* stream);
 
+/* Bounded-wait probe: one thread waits on an mbarrier with the polling
+ * loop the tensor-core kernels use for their waits, at most `limit` polls.
+ * arrive = 0: nothing arrives, the wait runs out and *status (device) is set
+ * to BDGFS_ETIMEOUT; arrive = 1: the barrier completes and *status is
+ * BDGFS_OK.  Tests the timeout path without a device fault.  No counterpart
+ * in the reference. */
+int32_t bdgfs_wait_probe(uint32_t limit, int32_t arrive, int32_t* status, void* stream);
+
 /* Measured FP32 FMA throughput probe: runs iters dependent-free FMA chains
  * per thread on nblocks x 256 threads and writes a checksum to out[0]. */
 int32_t bdgfs_fma_probe(float* out, int32_t nblocks, int32_t iters,

@@ -117,7 +117,11 @@ class FROracle:
         nc = sum(n[j] * self.cv[j] for j in range(self.ndims))
         return 0.5 * nc * (ul + ur) + 0.5 * np.abs(nc) * (ul - ur)
 
-    def rhs(self, u, bc=None):
+    def rhs(self, u, bc=None, ghost=None):
+        """L(u).  ghost: face values of neighbours owned by other parts of a
+        partitioned mesh (rows E*nfpts + i of the local neighbour table);
+        their faces get the one-sided flux the reference's MPI interfaces
+        compute (frfs/solvers/dgfs/inters.py:61-112)."""
         g = self.geo
         d = self.ndims
         E, nupts, nv = u.shape
@@ -139,7 +143,10 @@ class FROracle:
                 n = g.norm_pnorm[e, f]
                 mag = g.mag_pnorm[e, f]
                 ul = uf[e, f]
-                if nb >= 0:
+                if nb >= E * nf:
+                    fn = self._rusanov(ul, ghost[int(nb) - E * nf], n)
+                    Fh[e, f] = mag * fn
+                elif nb >= 0:
                     e2, f2 = divmod(int(nb), nf)
                     fn = self._rusanov(ul, uf[e2, f2], n)
                     Fh[e, f] = mag * fn

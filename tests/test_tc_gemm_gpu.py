@@ -124,3 +124,28 @@ def test_tma_engine_gelu_grad_and_plain(cuda):
     cdf = 0.5 * (1 + torch.erf(z / math.sqrt(2)))
     assert _rel(D, _ref(A, B) * (cdf + z * phi)) < 1e-5
     assert _rel(P, _ref(A, B)) < 1e-5
+
+
+def test_bounded_wait_times_out_then_next_calls_are_correct(cuda):
+    """The mbarrier polling loop of the tensor-core kernels, given a small
+    limit on a barrier that nothing completes, gives up and reports
+    BDGFS_ETIMEOUT (-4) instead of hanging; the context stays usable: the
+    same wait on a completed barrier reports success and a GEMM that follows
+    is correct."""
+    from frfs_b200 import _lib
+    L = _lib.lib()
+    status = torch.full((1,), 99, dtype=torch.int32, device=cuda)
+    assert L.bdgfs_wait_probe(1000, 0, status.data_ptr(), _lib.stream_ptr()) == 0
+    torch.cuda.synchronize()
+    assert int(status.item()) == -4
+    assert L.bdgfs_wait_probe(1000, 1, status.data_ptr(), _lib.stream_ptr()) == 0
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    assert L.bdgfs_wait_probe(0, 0, status.data_ptr(), _lib.stream_ptr()) == -1
+    g = torch.Generator(device=cuda).manual_seed(9)
+    A = torch.randn(300, 130, device=cuda, generator=g).bfloat16()
+    B = torch.randn(200, 130, device=cuda, generator=g).bfloat16()
+    C = torch.empty(300, 200, device=cuda)
+    gemm(A, B, out=C)
+    torch.cuda.synchronize()
+    assert _rel(C, _ref(A, B)) < 1e-5
