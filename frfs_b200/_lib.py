@@ -23,7 +23,8 @@ EXPORTS = (
     'bdgfs_moments', 'bdgfs_residual', 'bdgfs_status_check',
     'bdgfs_gemm', 'bdgfs_colsum', 'bdgfs_adamw', 'bdgfs_relmse',
     'bdgfs_hybrid_classify', 'bdgfs_hybrid_project', 'bdgfs_hybrid_scatter',
-    'bdgfs_hybrid_project_scatter', 'bdgfs_hybrid_heads',
+    'bdgfs_hybrid_project_scatter', 'bdgfs_hybrid_heads', 'bdgfs_hybrid_shift',
+    'bdgfs_hybrid_tfeatures',
     'bdgfs_bgk_moments', 'bdgfs_bgk_maxwellian', 'bdgfs_ars_stage',
     'bdgfs_esbgk_moments', 'bdgfs_esbgk_gaussian', 'bdgfs_shakov_moments', 'bdgfs_shakov_target',
     'bdgfs_bdf_step', 'bdgfs_vss_scratch_bytes', 'bdgfs_vss_collide', 'bdgfs_vss_project',
@@ -95,7 +96,8 @@ class HybridArgs(C.Structure):
                 ('sur_rho2', C.c_void_p), ('spec_idx', C.c_void_p), ('flag', C.c_void_p),
                 ('eps', C.c_void_p), ('recheck_err', C.c_void_p), ('seed_dev', C.c_void_p),
                 ('dev_rows', C.c_void_p), ('feat', C.c_void_p), ('feat_ld', C.c_int64),
-                ('sur_s', C.c_void_p), ('fb_idx', C.c_void_p)]
+                ('sur_s', C.c_void_p), ('fb_idx', C.c_void_p), ('sur_uT', C.c_void_p),
+                ('center', C.c_int32), ('pad2_', C.c_int32)]
 
 
 class ArsArgs(C.Structure):
@@ -177,6 +179,8 @@ def lib():
             'bdgfs_hybrid_scatter': [vp, vp, vp, vp],
             'bdgfs_hybrid_project_scatter': [vp, vp, vp, vp],
             'bdgfs_hybrid_heads': [vp, vp, C.c_int64, C.c_int64, C.c_int32, vp, C.c_int64, vp],
+            'bdgfs_hybrid_shift': [vp, vp, i32, vp, i32, C.c_float, vp],
+            'bdgfs_hybrid_tfeatures': [vp, vp, i64, i64, i64, i64, vp],
             'bdgfs_bgk_moments': [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_double, vp, vp],
             'bdgfs_bgk_maxwellian': [vp, C.c_int64, C.c_int32, C.c_int32, vp, vp, vp],
             'bdgfs_ars_stage': [vp, vp],

@@ -95,11 +95,17 @@ __global__ void __launch_bounds__(256) indicator_kernel(const bdgfs_hybrid_args 
             h.sur_rho2[p] = float(rho * rho);
             s_pos = p;
             if (h.sur_s) h.sur_s[p] = float(sqrt(e[0]) / rho);
+            if (h.sur_uT) {
+                h.sur_uT[4 * p + 0] = float(ux);
+                h.sur_uT[4 * p + 1] = float(uy);
+                h.sur_uT[4 * p + 2] = float(uz);
+                h.sur_uT[4 * p + 3] = float(Tt);
+            }
             if (h.feat) {
                 __nv_bfloat16* fr = static_cast<__nv_bfloat16*>(h.feat) + p * h.feat_ld;
-                fr[0] = __float2bfloat16_rn(float(ux));
-                fr[1] = __float2bfloat16_rn(float(uy));
-                fr[2] = __float2bfloat16_rn(float(uz));
+                fr[0] = __float2bfloat16_rn(h.center ? 0.f : float(ux));
+                fr[1] = __float2bfloat16_rn(h.center ? 0.f : float(uy));
+                fr[2] = __float2bfloat16_rn(h.center ? 0.f : float(uz));
                 fr[3] = __float2bfloat16_rn(float(Tt - 1.0));
             }
         }
@@ -294,6 +300,95 @@ __global__ void __launch_bounds__(256) project_scatter_kernel(const bdgfs_hybrid
     }
 }
 
+template <typename T>
+__device__ __forceinline__ float to_f32(T x) { return float(x); }
+template <>
+__device__ __forceinline__ float to_f32<__nv_bfloat16>(__nv_bfloat16 x) { return __bfloat162float(x); }
+template <typename T>
+__device__ __forceinline__ T from_f32(float x) { return T(x); }
+template <>
+__device__ __forceinline__ __nv_bfloat16 from_f32<__nv_bfloat16>(float x) { return __float2bfloat16_rn(x); }
+
+// Spectral shift of compact rows (bdgfs_hybrid_shift).  Along one axis the
+// shift by a is the circulant g_i = sum_j w[(i - j) mod N] f_j with
+//   w[k] = (1/N) sum_{m=-N/2}^{N/2-1} cos(2 pi m (k + a/h) / N)
+// (the real part of the trigonometric interpolant on the periodic grid);
+// the three axes are applied in turn on the row staged in shared memory
+// (z-stride padded to N + 1: the three pencil directions are free of bank
+// conflicts).  Grid-stride over the rows below the device count.
+template <int N, typename TI, typename TO>
+__global__ void __launch_bounds__(256) shift_kernel(const bdgfs_hybrid_args h, const TI* in, TO* out,
+                                                    float sign)
+{
+    extern __shared__ float sh[];
+    constexpr int S = N + 1;
+    constexpr int n = N * N * N;
+    float* cube = sh;
+    float* wt = sh + N * N * S;
+    const int64_t cnt = *h.counts;
+    const double hg = h.c0[1] - h.c0[0];
+    for (int64_t row = blockIdx.x; row < cnt; row += gridDim.x) {
+        const TI* src = in + row * int64_t(n);
+        TO* dst = out + row * int64_t(n);
+        for (int i = threadIdx.x; i < 3 * N; i += blockDim.x) {
+            const int d = i / N, k = i - d * N;
+            const double a = double(sign) * double(h.sur_uT[4 * row + d]) / hg;
+            double w = 0.0;
+            for (int m = -N / 2; m < N / 2; ++m) w += cospi(2.0 * double(m) * (double(k) + a) / double(N));
+            wt[i] = float(w / double(N));
+        }
+        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+            const int xy = v / N;
+            cube[xy * S + (v - xy * N)] = to_f32(src[v]);
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int d = 2; d >= 0; --d) {              // z, y, x
+            float w[N];
+#pragma unroll
+            for (int k = 0; k < N; ++k) w[k] = wt[d * N + k];
+            for (int p = threadIdx.x; p < N * N; p += blockDim.x) {
+                const int p0 = p / N, p1 = p - p0 * N;
+                int base, stride;
+                if (d == 2) { base = p * S; stride = 1; }                    // (x, y)
+                else if (d == 1) { base = p0 * N * S + p1; stride = S; }     // (x, z)
+                else { base = p0 * S + p1; stride = N * S; }                 // (y, z)
+                float v[N];
+#pragma unroll
+                for (int j = 0; j < N; ++j) v[j] = cube[base + j * stride];
+#pragma unroll
+                for (int i = 0; i < N; ++i) {
+                    float acc = 0.f;
+#pragma unroll
+                    for (int j = 0; j < N; ++j) acc = fmaf(w[(i - j + N) % N], v[j], acc);
+                    cube[base + i * stride] = acc;
+                }
+            }
+            __syncthreads();
+        }
+        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+            const int xy = v / N;
+            dst[v] = from_f32<TO>(cube[xy * S + (v - xy * N)]);
+        }
+        __syncthreads();                             // cube and wt reused by the next row
+    }
+}
+
+__global__ void __launch_bounds__(256) tfeat_kernel(const bdgfs_hybrid_args h, __nv_bfloat16* xc, int64_t ld,
+                                                    int64_t x0, int64_t x1, int64_t k)
+{
+    const int64_t cnt = *h.counts;
+    for (int64_t row = blockIdx.x; row < cnt; row += gridDim.x) {
+        const float t = h.sur_uT[4 * row + 3] - 1.f;
+        __nv_bfloat16* r = xc + row * ld;
+        for (int64_t j = threadIdx.x; j < k; j += blockDim.x) {
+            const float x = __bfloat162float(r[x0 + j]);
+            r[x1 + j] = __float2bfloat16_rn(t * x);
+            r[x1 + k + j] = __float2bfloat16_rn(t * t * x);
+        }
+    }
+}
+
 // out[m][i*k + j] = s_m^i Y[m][i*k + j]
 __global__ void __launch_bounds__(128) heads_kernel(const bdgfs_hybrid_args h, const float* __restrict__ Y,
                                                     int64_t ldy, int64_t k, int nheads,
@@ -423,3 +518,75 @@ extern "C" int32_t bdgfs_hybrid_heads(const bdgfs_hybrid_args* h, const float* Y
         *h, Y, ldy, k, nheads, static_cast<__nv_bfloat16*>(out), ldo);
     return cuda_status(cudaGetLastError());
 }
+
+template <int N, typename TI, typename TO>
+static int shift_launch(const bdgfs_hybrid_args* h, const void* in, void* out, float sign, cudaStream_t st)
+{
+    const size_t smem = sizeof(float) * (size_t(N) * N * (N + 1) + 3 * N);
+    if (const int rc = smem_optin(reinterpret_cast<const void*>(shift_kernel<N, TI, TO>), smem)) return rc;
+    int dev = 0, nsm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return BDGFS_ECUDA;
+    int64_t grid = int64_t(nsm) * 4;
+    if (grid > h->ndof) grid = h->ndof;
+    shift_kernel<N, TI, TO><<<unsigned(grid), 256, smem, st>>>(*h, static_cast<const TI*>(in),
+                                                               static_cast<TO*>(out), sign);
+    return cuda_status(cudaGetLastError());
+}
+
+template <int N>
+static int shift_types(const bdgfs_hybrid_args* h, const void* in, int in_bf16, void* out, int out_bf16,
+                       float sign, cudaStream_t st)
+{
+    using B = __nv_bfloat16;
+    if (h->fp64) {
+        if (in_bf16 && out_bf16) return shift_launch<N, B, B>(h, in, out, sign, st);
+        if (in_bf16) return shift_launch<N, B, double>(h, in, out, sign, st);
+        if (out_bf16) return shift_launch<N, double, B>(h, in, out, sign, st);
+        return shift_launch<N, double, double>(h, in, out, sign, st);
+    }
+    if (in_bf16 && out_bf16) return shift_launch<N, B, B>(h, in, out, sign, st);
+    if (in_bf16) return shift_launch<N, B, float>(h, in, out, sign, st);
+    if (out_bf16) return shift_launch<N, float, B>(h, in, out, sign, st);
+    return shift_launch<N, float, float>(h, in, out, sign, st);
+}
+
+extern "C" int32_t bdgfs_hybrid_shift(const bdgfs_hybrid_args* h, const void* in, int32_t in_bf16,
+                                      void* out, int32_t out_bf16, float sign, void* stream)
+{
+    int rc = check_h(h);
+    if (rc) return rc;
+    if (!in || !out || !h->counts || !h->sur_uT || h->Nv < 2) return BDGFS_EINVAL;
+    if (h->ndof == 0) return BDGFS_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    switch (h->Nv) {
+    case 8: return shift_types<8>(h, in, in_bf16, out, out_bf16, sign, st);
+    case 12: return shift_types<12>(h, in, in_bf16, out, out_bf16, sign, st);
+    case 16: return shift_types<16>(h, in, in_bf16, out, out_bf16, sign, st);
+    case 24: return shift_types<24>(h, in, in_bf16, out, out_bf16, sign, st);
+    case 32: return shift_types<32>(h, in, in_bf16, out, out_bf16, sign, st);
+    default: return BDGFS_EUNSUPPORTED;
+    }
+}
+
+extern "C" int32_t bdgfs_hybrid_tfeatures(const bdgfs_hybrid_args* h, void* xc, int64_t ld, int64_t x0,
+                                          int64_t x1, int64_t k, void* stream)
+{
+    int rc = check_h(h);
+    if (rc) return rc;
+    if (!xc || !h->counts || !h->sur_uT || k < 1 || x0 < 0 || x1 < 0 || x0 + k > ld || x1 + 2 * k > ld ||
+        (x1 < x0 + k && x0 < x1 + 2 * k))
+        return BDGFS_EINVAL;
+    if (h->ndof == 0) return BDGFS_OK;
+    int dev = 0, nsm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return BDGFS_ECUDA;
+    int64_t grid = int64_t(nsm) * 8;
+    if (grid > h->ndof) grid = h->ndof;
+    tfeat_kernel<<<unsigned(grid), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        *h, static_cast<__nv_bfloat16*>(xc), ld, x0, x1, k);
+    return cuda_status(cudaGetLastError());
+}
+

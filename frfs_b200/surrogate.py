@@ -165,22 +165,35 @@ class QSurrogate:
     """Basis projection + MLP with output heads (BF16 weights, FP32
     accumulation on the tensor cores) for Q."""
 
-    def __init__(self, grid, nmodes=512, width=1024, device=None, family=COUETTE):
+    def __init__(self, grid, nmodes=512, width=1024, device=None, family=COUETTE, center=True):
+        """center: the network sees every distribution re-centred at zero
+        velocity (spectral shift by -u) and its Q is shifted back by +u;
+        the collision operator commutes with the shift, so the drift drops
+        out of what is learned, and the input gains the temperature
+        features (T-1) x and (T-1)^2 x of the deviation modes x, which make
+        the linear skip path the exact form of the linearised operator's
+        smooth temperature dependence."""
         self.grid = grid                    # scattering.VHSGrid (tables, c0, ginv)
         self.Nv = grid.Nv
         self.n = grid.Nv**3
         self.k = nmodes
         self.w = width
         self.family = family
+        self.center = bool(center)
         self.device = device or grid.phase.device
         self.trained = False
         self.history = []
 
     @property
+    def kfeat(self):
+        """Columns of the deviation modes and NFEAT features, padded to 16."""
+        return (self.k + NFEAT + 15) // 16 * 16
+
+    @property
     def kin(self):
         """Input width: k deviation modes, NFEAT features, zero padding to a
-        multiple of 16."""
-        return (self.k + NFEAT + 15) // 16 * 16
+        multiple of 16, then (centred model) the 2k temperature features."""
+        return self.kfeat + (2 * self.k if self.center else 0)
 
     @property
     def ldx(self):
@@ -328,6 +341,8 @@ class QSurrogate:
         m = nbasis
         idx = enc.sur_idx[:m].long()
         fb = fb.index_select(0, idx)
+        if self.center:
+            enc.shift(fb, False, fb, False, 1.0)           # rows at zero drift
         Xd = enc.dev_rows[:m].float()
         heads = self._head_labels(fb, enc.dev_rows[:m], col)
         del fb
@@ -364,7 +379,10 @@ class QSurrogate:
             f = sample_family(c0, m, gen, dev, family=self.family)
             x, _, _, idx = self.encode(f, enc)
             X[i0:i0 + m] = x
-            heads = self._head_labels(f.index_select(0, idx.long()), enc.dev_rows[:m], col)
+            fc = f.index_select(0, idx.long())
+            if self.center:
+                enc.shift(fc, False, fc, False, 1.0)
+            heads = self._head_labels(fc, enc.dev_rows[:m], col)
             for hd, y in enumerate(heads):
                 gemm(y.contiguous(), self.Bq[hd * self.k:(hd + 1) * self.k],
                      out=Cc[i0:i0 + m, hd * self.k:(hd + 1) * self.k], engine=1)
@@ -475,6 +493,11 @@ class QSurrogate:
     def project_input(self, enc, M):
         gemm(enc.dev_rows[:M], self.BdT_bf16, bias=self.bias_in, mcount=enc.counts[0:1],
              out_bf16=enc.xc[:M, self.w:self.w + self.k])
+        if self.center:
+            x1 = self.w + self.kfeat
+            _lib.check(_lib.lib().bdgfs_hybrid_tfeatures(C.byref(enc.args), enc.xc.data_ptr(),
+                                                         self.ldx, self.w, x1, self.k,
+                                                         _lib.stream_ptr()), 'bdgfs_hybrid_tfeatures')
 
     def infer(self, enc, M):
         """Compact surrogate Q of the rows the indicator selected (device
@@ -493,6 +516,8 @@ class QSurrogate:
                                                  enc.yb.data_ptr(), NHEADS * self.k,
                                                  _lib.stream_ptr()), 'bdgfs_hybrid_heads')
         gemm(enc.yb[:M], self.BqT_bf16, row_scale=enc.rho2, mcount=cnt, out=enc.Qc[:M])
+        if self.center:
+            enc.shift(enc.Qc, False, enc.Qc, False, -1.0)           # back to the cell's drift
 
     def evaluate(self, nsamples, seed=1, chunk=8192, family=None):
         """Relative L2 error of the surrogate (with conservation projection)
@@ -526,7 +551,7 @@ class QSurrogate:
         keys = ('Bd', 'Bq', 'mu', 'sigma', 'hscale')
         d = {k: getattr(self, k).cpu() for k in keys}
         d.update(W=[w.cpu() for w in self.W], b=[b.cpu() for b in self.b],
-                 k=self.k, w=self.w, Nv=self.Nv)
+                 k=self.k, w=self.w, Nv=self.Nv, center=self.center)
         return d
 
     def load_state_dict(self, d):
@@ -534,6 +559,7 @@ class QSurrogate:
         for k in ('Bd', 'Bq', 'mu', 'sigma', 'hscale'):
             setattr(self, k, d[k].to(dev))
         self.k, self.w = int(d['k']), int(d['w'])
+        self.center = bool(d.get('center', False))
         self.W = [w.to(dev) for w in d['W']]
         self.b = [b.to(dev) for b in d['b']]
         self._sync_bf16()
@@ -585,6 +611,7 @@ class HybridCollider:
             self.recheck_err = torch.zeros(2, dtype=torch.float64, device=dev)
             self.rc_counts = torch.zeros(4, dtype=torch.int64, device=dev)
             self.seed_dev = torch.zeros(1, dtype=torch.int64, device=dev)
+            self.sur_uT = torch.zeros(ndof, 4, device=dev)
             self.dev_rows = torch.zeros(ndof, n, device=dev, dtype=torch.bfloat16)
             self._n = ndof
             self._net = None
@@ -617,7 +644,8 @@ class HybridCollider:
             eps=self.eps.data_ptr(), recheck_err=self.recheck_err.data_ptr() if rc > 0 else 0,
             seed_dev=self.seed_dev.data_ptr() if seed is None else 0,
             dev_rows=self.dev_rows.data_ptr(), feat=feat, feat_ld=m.ldx,
-            sur_s=self.sur_s.data_ptr(), fb_idx=self.fb_idx.data_ptr())
+            sur_s=self.sur_s.data_ptr(), fb_idx=self.fb_idx.data_ptr(),
+            sur_uT=self.sur_uT.data_ptr(), center=int(m.center))
 
     def classify(self, fin, seed=None, recheck=None):
         f2 = fin.reshape(-1, self.model.n)
@@ -626,7 +654,16 @@ class HybridCollider:
         self.args = self._args(ndof, seed, recheck)
         _lib.check(_lib.lib().bdgfs_hybrid_classify(C.byref(self.args), f2.data_ptr(),
                                                     _lib.stream_ptr()), 'bdgfs_hybrid_classify')
+        if self.model.center:                    # deviation directions at zero drift
+            self.shift(self.dev_rows, True, self.dev_rows, True, 1.0)
         return ndof
+
+    def shift(self, src, src_bf16, dst, dst_bf16, sign):
+        """The first counts[0] compact rows of src at velocities c + sign*u
+        (u of each surrogate row) into dst (bdgfs_hybrid_shift)."""
+        _lib.check(_lib.lib().bdgfs_hybrid_shift(C.byref(self.args), src.data_ptr(), int(src_bf16),
+                                                 dst.data_ptr(), int(dst_bf16), float(sign),
+                                                 _lib.stream_ptr()), 'bdgfs_hybrid_shift')
 
     def __call__(self, fin, fout, seed=None):
         """Q for every distribution of fin [ndof][n] into fout."""

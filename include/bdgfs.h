@@ -366,6 +366,12 @@ typedef struct bdgfs_hybrid_args {
                                 (NaN / Inf) and writes nothing for them;
                                 counts[3] their number -- the caller runs
                                 the spectral operator on that list         */
+    float* sur_uT;           /* optional [ndof][4]: (u_x, u_y, u_z, T) of
+                                surrogate row p (FP32)                      */
+    int32_t center;          /* nonzero: the feature columns get
+                                (0, 0, 0, T - 1), the rows being re-centred
+                                at zero velocity by bdgfs_hybrid_shift     */
+    int32_t pad2_;
 } bdgfs_hybrid_args;
 
 /* Indicator eps = |f - M[f]| / |f| per distribution and device-side lists. */
@@ -382,6 +388,24 @@ int32_t bdgfs_hybrid_scatter(const bdgfs_hybrid_args* h, const void* Qc,
  * projected on the fly and written to Q; Qc itself is left unchanged). */
 int32_t bdgfs_hybrid_project_scatter(const bdgfs_hybrid_args* h,
                                      const void* Qc, void* Q, void* stream);
+/* Spectral velocity shift of the first counts[0] compact rows: row p of out
+ * is row p of in evaluated at the velocities c + sign * u_p, u_p =
+ * sur_uT[p][0..2], by trigonometric interpolation on the periodic Nv^3 grid
+ * of spacing c0[1] - c0[0] (one circulant pass along each axis; exact for
+ * band-limited rows, its own inverse with the opposite sign up to the
+ * Nyquist terms).  sign = +1 centres a row at zero velocity, -1 moves it
+ * back.  in / out: bf16 (flag 1) or the state's real type, [rows][Nv^3];
+ * they may be the same array.  Nv in {8, 12, 16, 24, 32}.  No counterpart
+ * in the reference (the surrogate works on rows centred at zero velocity,
+ * where the collision operator's dependence on the drift is removed
+ * exactly). */
+int32_t bdgfs_hybrid_shift(const bdgfs_hybrid_args* h, const void* in, int32_t in_bf16,
+                           void* out, int32_t out_bf16, float sign, void* stream);
+/* Temperature features of the first counts[0] rows of the bf16 network
+ * input xc (leading dimension ld): columns [x1, x1+k) <- (T-1) * columns
+ * [x0, x0+k) and [x1+k, x1+2k) <- (T-1)^2 * the same, T = sur_uT[p][3]. */
+int32_t bdgfs_hybrid_tfeatures(const bdgfs_hybrid_args* h, void* xc, int64_t ld, int64_t x0,
+                               int64_t x1, int64_t k, void* stream);
 /* Scale the network's output heads of the first counts[0] rows:
  * out[m][i*k + j] = sur_s[m]^i * Y[m][i*k + j], i < nheads, j < k
  * (Y float, leading dimension ldy; out bf16, leading dimension ldo). */

@@ -18,12 +18,70 @@ from helpers import vhs_cfg
 pytestmark = pytest.mark.gpu
 
 
-def _model(Nv=16, Nrho=8, M=6, dev=5, k=64, w=128):
+def _model(Nv=16, Nrho=8, M=6, dev=5, k=64, w=128, center=True):
     cfg = vhs_cfg(Nv, Nrho, M, dev, precision='single')
     be = CUDABackend(cfg)
     vm = DGFSVelocityMesh(be, cfg)
     sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
-    return be, vm, sm, QSurrogate(sm.grid, nmodes=k, width=w)
+    return be, vm, sm, QSurrogate(sm.grid, nmodes=k, width=w, center=center)
+
+
+def _fft_shift(F, u, c0):
+    """Rows of F at velocities c + u by FFT (FP64 test restatement of the
+    trigonometric-interpolation shift)."""
+    N = c0.numel()
+    om = 2 * math.pi * torch.fft.fftfreq(N, d=float(c0[1] - c0[0])).to(F.device).double()
+    G = torch.fft.fftn(F.double().view(-1, N, N, N), dim=(1, 2, 3))
+    ph = torch.exp(1j * (om.view(1, -1, 1, 1) * u[:, 0].view(-1, 1, 1, 1)
+                         + om.view(1, 1, -1, 1) * u[:, 1].view(-1, 1, 1, 1)
+                         + om.view(1, 1, 1, -1) * u[:, 2].view(-1, 1, 1, 1)))
+    return torch.fft.ifftn(G * ph, dim=(1, 2, 3)).real.reshape(F.shape[0], -1)
+
+
+@pytest.mark.parametrize('Nv', [16, 24])
+def test_spectral_shift_of_rows(cuda, Nv):
+    """bdgfs_hybrid_shift: rows at c + u equal the FFT restatement, the
+    shift back returns the row, the centred rows have zero drift; the
+    centred model's deviation rows are the raw ones shifted, its features
+    (0, 0, 0, T - 1)."""
+    be, vm, sm, q = _model(Nv=Nv, Nrho=4, M=6, dev=5 if Nv == 16 else 6, k=32, w=64)
+    gen = torch.Generator(device=be.device).manual_seed(21)
+    f = sample_family(vm.c0(), 40, gen, be.device)
+    h = HybridCollider(q, threshold=float('inf'), recheck=0.0)
+    h.classify(f)
+    torch.cuda.synchronize()
+    m = int(h.counts[0])
+    assert m == 40
+    rows = f.index_select(0, h.sur_idx[:m].long()).contiguous()
+    c0 = torch.as_tensor(vm.c0(), dtype=torch.float64, device=be.device)
+    u = h.sur_uT[:m, :3].double()
+    out = torch.empty_like(rows)
+    h.shift(rows, False, out, False, 1.0)
+    back = torch.empty_like(rows)
+    h.shift(out, False, back, False, -1.0)
+    torch.cuda.synchronize()
+    ref = _fft_shift(rows, u, c0)
+    rel = lambda a, b: float((a.double() - b.double()).norm() / b.double().norm())
+    assert rel(out, ref) < 2e-6
+    assert rel(back, rows) < 1e-4
+    N = Nv
+    Fc = out.double().view(-1, N, N, N)
+    drift = torch.stack([(Fc * c0.view(1, -1, 1, 1)).sum((1, 2, 3)),
+                         (Fc * c0.view(1, 1, -1, 1)).sum((1, 2, 3)),
+                         (Fc * c0.view(1, 1, 1, -1)).sum((1, 2, 3))], 1) / Fc.sum((1, 2, 3))[:, None]
+    assert float(drift.abs().max()) < 1e-3 < float(u.abs().max())
+    # centred deviation rows = the raw ones (uncentred model) shifted
+    q0 = QSurrogate(sm.grid, nmodes=32, width=64, center=False)
+    h0 = HybridCollider(q0, threshold=float('inf'), recheck=0.0)
+    h0.classify(f)
+    torch.cuda.synchronize()
+    o0, o1 = torch.argsort(h0.sur_idx[:m]), torch.argsort(h.sur_idx[:m])
+    raw = h0.dev_rows[:m][o0].float()
+    assert rel(h.dev_rows[:m][o1].float(), _fft_shift(raw, u[o1], c0)) < 6e-3     # bf16 rows
+    feat = h.xc[:m, q.w + q.k:q.w + q.k + 4].double()
+    assert float(feat[:, :3].abs().max()) == 0.0
+    T = h.sur_uT[:m, 3].double()
+    assert float((feat[:, 3] - (T - 1)).abs().max()) < 4e-3
 
 
 def test_training_gradients_match_fp64_oracle(cuda):
@@ -60,7 +118,7 @@ def test_indicator_rows_features_and_heads(cuda):
     FP64 restatement; the head-combination and fused project-scatter
     kernels against their unfused forms."""
     from frfs_b200 import _lib
-    be, vm, sm, q = _model(k=64, w=128)
+    be, vm, sm, q = _model(k=64, w=128, center=False)
     gen = torch.Generator(device=be.device).manual_seed(4)
     f = sample_family(vm.c0(), 50, gen, be.device)
     h = HybridCollider(q, threshold=float('inf'), recheck=0.0)
@@ -126,7 +184,7 @@ def test_head_labels_recombine_to_q(cuda):
     at each sample's own deviation size s, to the spectral Q of the sample
     (up to FP32 rounding and the bf16 rounding of d^)."""
     from frfs_b200.scattering import VHSCollider
-    be, vm, sm, q = _model(k=64, w=128)
+    be, vm, sm, q = _model(k=64, w=128, center=False)
     gen = torch.Generator(device=be.device).manual_seed(12)
     f = sample_family(vm.c0(), 64, gen, be.device)
     h = HybridCollider(q, threshold=float('inf'), recheck=0.0)
