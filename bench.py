@@ -948,7 +948,7 @@ def run_hybrid_steps(nsteps, nwarm=3):
     be = CUDABackend(cfg)
     mesh = StructuredMesh((8, 8, 8), (0, 0, 0), (1, 1, 1), periodic='', bcnames=names)
     s5 = DGFSSystem(be, mesh, cfg, nreg=3)
-    q = QSurrogate(s5.sm.grid, nmodes=512, width=1024)
+    q = QSurrogate(s5.sm.grid, nmodes=256, width=1024)
     dev = be.device
     g = torch.Generator(device=dev).manual_seed(0)
     n = q.n
@@ -1056,7 +1056,7 @@ def surrogate_legs(flush, log=None, pool=None, ncores=0):
     vm = DGFSVelocityMesh(be, cfg)
     sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
     t0 = time.time()
-    q = QSurrogate(sm.grid, nmodes=512, width=1024)
+    q = QSurrogate(sm.grid, nmodes=256, width=1024)
     q.fit(nsamples=200000, ntest=50000, epochs=20, lr=3e-4, batch=1024, seed=0)
     t_fit = time.time() - t0
     # surrogate vs spectral throughput on near-equilibrium cells
@@ -1088,11 +1088,13 @@ def surrogate_legs(flush, log=None, pool=None, ncores=0):
     lin = q.evaluate(10000, seed=1)
     q.W[3].copy_(saved)
     q._fold()
-    c4 = {'workload': ('surrogate of Q on Nv=24^3 (M=Nrho=12): 512-mode bases (randomised SVD) '
-                       'of the Maxwellian-deviation direction and of Q/rho^2, 4-layer GELU MLP '
-                       'width 1024 with a linear skip and 3 output heads '
+    c4 = {'workload': ('surrogate of Q on Nv=24^3 (M=Nrho=12): every cell re-centred at zero '
+                       'velocity by a spectral shift (Q shifted back), 256-mode bases '
+                       '(randomised SVD) of the Maxwellian-deviation direction and of Q/rho^2, '
+                       'input = modes x, (T-1) x, (T-1)^2 x, products of the 24 leading modes, '
+                       'T-1; 4-layer GELU MLP width 1024 with a linear skip and 3 output heads '
                        '(Q/rho^2 = y0 + s y1 + s^2 y2, s the deviation size), BF16 weights / '
-                       'FP32 accumulation on tcgen05, least-squares start of the skip path, '
+                       'FP32 accumulation on tcgen05, least-squares skip path (kept fixed), '
                        'AdamW lr 3e-4, 20 epochs, 200000 training / 50000 held-out seeded '
                        'distributions of the Couette family, FP64 conservation projection'),
           'modes': q.k, 'train_steps': q.steps, 'train_s': q.train_seconds,
@@ -1119,7 +1121,7 @@ def surrogate_legs(flush, log=None, pool=None, ncores=0):
     ini, names = cavity_ini()
     # surrogate for the cavity's near-equilibrium cells (CAVITY family)
     t0 = time.time()
-    qc = QSurrogate(sm.grid, nmodes=512, width=1024, family=CAVITY)
+    qc = QSurrogate(sm.grid, nmodes=256, width=1024, family=CAVITY)
     qc.fit(nsamples=200000, ntest=20000, epochs=20, lr=3e-4, batch=1024, seed=10)
     t_fit_c = time.time() - t0
     res, fields = {}, {}
@@ -1455,7 +1457,7 @@ def run_q_only(ndof):
 
 def run_surrogate_call(ndof, reps=2):
     """Profiling case: all-surrogate hybrid calls on ndof Couette-family
-    cells with a randomly initialised 512-mode / width-1024 network (the
+    cells with a randomly initialised 256-mode / width-1024 network (the
     kernels and shapes of inference; timing only)."""
     import torch
     from frfs_b200.backend import CUDABackend
@@ -1467,7 +1469,7 @@ def run_surrogate_call(ndof, reps=2):
     be = CUDABackend(cfg)
     vm = DGFSVelocityMesh(be, cfg)
     sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
-    q = QSurrogate(sm.grid, nmodes=512, width=1024)
+    q = QSurrogate(sm.grid, nmodes=256, width=1024)
     dev = be.device
     g = torch.Generator(device=dev).manual_seed(0)
     n = q.n

@@ -24,7 +24,7 @@ EXPORTS = (
     'bdgfs_gemm', 'bdgfs_colsum', 'bdgfs_adamw', 'bdgfs_relmse',
     'bdgfs_hybrid_classify', 'bdgfs_hybrid_project', 'bdgfs_hybrid_scatter',
     'bdgfs_hybrid_project_scatter', 'bdgfs_hybrid_heads', 'bdgfs_hybrid_shift',
-    'bdgfs_hybrid_tfeatures',
+    'bdgfs_hybrid_tfeatures', 'bdgfs_hybrid_heads_split',
     'bdgfs_bgk_moments', 'bdgfs_bgk_maxwellian', 'bdgfs_ars_stage',
     'bdgfs_esbgk_moments', 'bdgfs_esbgk_gaussian', 'bdgfs_shakov_moments', 'bdgfs_shakov_target',
     'bdgfs_bdf_step', 'bdgfs_vss_scratch_bytes', 'bdgfs_vss_collide', 'bdgfs_vss_project',
@@ -180,7 +180,8 @@ def lib():
             'bdgfs_hybrid_project_scatter': [vp, vp, vp, vp],
             'bdgfs_hybrid_heads': [vp, vp, C.c_int64, C.c_int64, C.c_int32, vp, C.c_int64, vp],
             'bdgfs_hybrid_shift': [vp, vp, i32, vp, i32, C.c_float, vp],
-            'bdgfs_hybrid_tfeatures': [vp, vp, i64, i64, i64, i64, vp],
+            'bdgfs_hybrid_heads_split': [vp, vp, C.c_int64, C.c_int64, C.c_int32, vp, C.c_int64, vp],
+            'bdgfs_hybrid_tfeatures': [vp, vp, i64, i64, i64, i64, i32, i64, vp],
             'bdgfs_bgk_moments': [vp, C.c_int64, C.c_int32, C.c_int32, vp, C.c_double, vp, vp],
             'bdgfs_bgk_maxwellian': [vp, C.c_int64, C.c_int32, C.c_int32, vp, vp, vp],
             'bdgfs_ars_stage': [vp, vp],

@@ -375,9 +375,11 @@ __global__ void __launch_bounds__(256) shift_kernel(const bdgfs_hybrid_args h, c
 }
 
 __global__ void __launch_bounds__(256) tfeat_kernel(const bdgfs_hybrid_args h, __nv_bfloat16* xc, int64_t ld,
-                                                    int64_t x0, int64_t x1, int64_t k)
+                                                    int64_t x0, int64_t x1, int64_t k, int k2, int64_t xq)
 {
+    __shared__ float xs[64];
     const int64_t cnt = *h.counts;
+    const int nq = k2 * (k2 + 1) / 2;
     for (int64_t row = blockIdx.x; row < cnt; row += gridDim.x) {
         const float t = h.sur_uT[4 * row + 3] - 1.f;
         __nv_bfloat16* r = xc + row * ld;
@@ -385,7 +387,16 @@ __global__ void __launch_bounds__(256) tfeat_kernel(const bdgfs_hybrid_args h, _
             const float x = __bfloat162float(r[x0 + j]);
             r[x1 + j] = __float2bfloat16_rn(t * x);
             r[x1 + k + j] = __float2bfloat16_rn(t * t * x);
+            if (j < k2) xs[j] = x;
         }
+        __syncthreads();
+        // products x_i x_j, i <= j < k2, row-major over the upper triangle
+        for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+            int i = 0, rem = q;
+            while (rem >= k2 - i) { rem -= k2 - i; ++i; }
+            r[xq + q] = __float2bfloat16_rn(xs[i] * xs[i + rem]);
+        }
+        __syncthreads();
     }
 }
 
@@ -402,6 +413,36 @@ __global__ void __launch_bounds__(128) heads_kernel(const bdgfs_hybrid_args h, c
     for (int i = 0; i < nheads; ++i) {
         for (int64_t j = threadIdx.x; j < k; j += blockDim.x)
             out[row * ldo + i * k + j] = __float2bfloat16_rn(p * y[i * k + j]);
+        p *= s;
+    }
+}
+
+// Split-bf16 heads: v = s_m^i Y[m][i*k + j] as hi = bf16(v), lo = bf16(v - hi),
+// written at columns c, K + c and 2K + c (K = nheads * k, c = i*k + j) as
+// [hi | hi | lo], to meet an output basis stored as [B_hi | B_lo | B_hi]:
+// one GEMM then sums hi*B_hi + hi*B_lo + lo*B_hi (the bf16 x bf16 terms of
+// an FP32-accurate product; lo*B_lo is below FP32 rounding).
+__global__ void __launch_bounds__(128) heads_split_kernel(const bdgfs_hybrid_args h,
+                                                          const float* __restrict__ Y, int64_t ldy,
+                                                          int64_t k, int nheads,
+                                                          __nv_bfloat16* __restrict__ out, int64_t ldo)
+{
+    const int64_t row = blockIdx.x;
+    if (row >= *h.counts) return;
+    const float s = h.sur_s[row];
+    const float* y = Y + row * ldy;
+    const int64_t K = int64_t(nheads) * k;
+    __nv_bfloat16* o = out + row * ldo;
+    float p = 1.f;
+    for (int i = 0; i < nheads; ++i) {
+        for (int64_t j = threadIdx.x; j < k; j += blockDim.x) {
+            const float v = p * y[i * k + j];
+            const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+            const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+            o[i * k + j] = hi;
+            o[K + i * k + j] = hi;
+            o[2 * K + i * k + j] = lo;
+        }
         p *= s;
     }
 }
@@ -571,12 +612,15 @@ extern "C" int32_t bdgfs_hybrid_shift(const bdgfs_hybrid_args* h, const void* in
 }
 
 extern "C" int32_t bdgfs_hybrid_tfeatures(const bdgfs_hybrid_args* h, void* xc, int64_t ld, int64_t x0,
-                                          int64_t x1, int64_t k, void* stream)
+                                          int64_t x1, int64_t k, int32_t k2, int64_t xq, void* stream)
 {
     int rc = check_h(h);
     if (rc) return rc;
+    const int64_t nq = int64_t(k2) * (k2 + 1) / 2;
     if (!xc || !h->counts || !h->sur_uT || k < 1 || x0 < 0 || x1 < 0 || x0 + k > ld || x1 + 2 * k > ld ||
-        (x1 < x0 + k && x0 < x1 + 2 * k))
+        (x1 < x0 + k && x0 < x1 + 2 * k) || k2 < 0 || k2 > 64 || k2 > k ||
+        (k2 > 0 && (xq < 0 || xq + nq > ld || (xq < x0 + k && x0 < xq + nq) ||
+                    (xq < x1 + 2 * k && x1 < xq + nq))))
         return BDGFS_EINVAL;
     if (h->ndof == 0) return BDGFS_OK;
     int dev = 0, nsm = 0;
@@ -586,7 +630,22 @@ extern "C" int32_t bdgfs_hybrid_tfeatures(const bdgfs_hybrid_args* h, void* xc, 
     int64_t grid = int64_t(nsm) * 8;
     if (grid > h->ndof) grid = h->ndof;
     tfeat_kernel<<<unsigned(grid), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        *h, static_cast<__nv_bfloat16*>(xc), ld, x0, x1, k);
+        *h, static_cast<__nv_bfloat16*>(xc), ld, x0, x1, k, k2, xq);
+    return cuda_status(cudaGetLastError());
+}
+
+extern "C" int32_t bdgfs_hybrid_heads_split(const bdgfs_hybrid_args* h, const float* Y, int64_t ldy,
+                                            int64_t k, int32_t nheads, void* out, int64_t ldo,
+                                            void* stream)
+{
+    int rc = check_h(h);
+    if (rc) return rc;
+    if (!Y || !out || !h->counts || !h->sur_s || k < 1 || nheads < 1 || ldy < nheads * k ||
+        ldo < 3 * nheads * k)
+        return BDGFS_EINVAL;
+    if (h->ndof == 0) return BDGFS_OK;
+    heads_split_kernel<<<unsigned(h->ndof), 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        *h, Y, ldy, k, nheads, static_cast<__nv_bfloat16*>(out), ldo);
     return cuda_status(cudaGetLastError());
 }
 

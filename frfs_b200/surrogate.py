@@ -165,7 +165,8 @@ class QSurrogate:
     """Basis projection + MLP with output heads (BF16 weights, FP32
     accumulation on the tensor cores) for Q."""
 
-    def __init__(self, grid, nmodes=512, width=1024, device=None, family=COUETTE, center=True):
+    def __init__(self, grid, nmodes=256, width=1024, device=None, family=COUETTE, center=True,
+                 split_out=False, nquad=None):
         """center: the network sees every distribution re-centred at zero
         velocity (spectral shift by -u) and its Q is shifted back by +u;
         the collision operator commutes with the shift, so the drift drops
@@ -180,6 +181,10 @@ class QSurrogate:
         self.w = width
         self.family = family
         self.center = bool(center)
+        self.split_out = bool(split_out)
+        # quadratic features of the leading deviation modes (centred model):
+        # the s^2 head is the collision operator's bilinear term in d^
+        self.nquad = (24 if self.center else 0) if nquad is None else int(nquad)
         self.device = device or grid.phase.device
         self.trained = False
         self.history = []
@@ -190,10 +195,16 @@ class QSurrogate:
         return (self.k + NFEAT + 15) // 16 * 16
 
     @property
+    def nq(self):
+        """Columns of the quadratic features, padded to 16."""
+        return (self.nquad * (self.nquad + 1) // 2 + 15) // 16 * 16
+
+    @property
     def kin(self):
         """Input width: k deviation modes, NFEAT features, zero padding to a
-        multiple of 16, then (centred model) the 2k temperature features."""
-        return self.kfeat + (2 * self.k if self.center else 0)
+        multiple of 16, then (centred model) the 2k temperature features and
+        the quadratic features."""
+        return self.kfeat + (2 * self.k + self.nq if self.center else 0)
 
     @property
     def ldx(self):
@@ -321,7 +332,7 @@ class QSurrogate:
         return y0, y1, y2
 
     def fit(self, nsamples=200000, ntest=50000, epochs=20, lr=3e-4, batch=1024, seed=0,
-            nbasis=16384, chunk=8192, log=None, ridge=1e-6, head_weights=(0.1, 1.0, 1.0)):
+            nbasis=16384, chunk=8192, log=None, ridge=1e-6, head_weights=None, freeze_skip=None):
         """Generate data, fit the bases, train the network (all on the
         device).  head_weights scale each head's share of the loss (its
         targets are divided by hscale_h / weight_h); y0 = Q(M)/rho^2 is
@@ -329,6 +340,10 @@ class QSurrogate:
         and weighting it 0.1 lowers the held-out error of Q (2.44 % -> 2.14 %
         on 20000 Couette-family samples)."""
         from .scattering import VHSCollider
+        if head_weights is None:
+            head_weights = (0.03, 1.0, 0.1) if self.center else (0.1, 1.0, 1.0)
+        if freeze_skip is None:
+            freeze_skip = self.center
         dev = self.device
         gen = torch.Generator(device=dev).manual_seed(seed)
         col = VHSCollider([self.grid], dev)
@@ -398,6 +413,11 @@ class QSurrogate:
         self._init_params(gen)
         t1 = time.time()
         self.ridge_residual = self._ridge_init(X, Tt, ridge)
+        if freeze_skip:
+            # the least-squares skip path stays as solved; the hidden layers
+            # learn what it leaves
+            skip = self.W[3][:, self.w:].clone()
+            skip_bf16 = self.Wb[3][:, self.w:].clone()
         # 4. AdamW
         loss = torch.zeros(1, dtype=torch.float64, device=dev)
         tot = torch.zeros(1, dtype=torch.float64, device=dev)
@@ -419,6 +439,9 @@ class QSurrogate:
                              0.01 + 0.99 * 0.5 * (1 + math.cos(math.pi * (step - warm) /
                                                                 max(1, nsteps - warm))))
                 self.train_step(xc, Tt[idb].contiguous(), dY, loss, step, lr_t)
+                if freeze_skip:
+                    self.W[3][:, self.w:] = skip
+                    self.Wb[3][:, self.w:] = skip_bf16
                 tot += loss
                 nb += 1
             self.history.append(float(tot.item()) / max(nb, 1))
@@ -479,7 +502,15 @@ class QSurrogate:
         b3 = self.b[3] * sc[:, 0]
         self.inf_W = [w.bfloat16().contiguous() for w in self.W[:3]] + [W3.bfloat16().contiguous()]
         self.inf_b = [b.contiguous() for b in self.b[:3]] + [b3.contiguous()]
-        self.BqT_bf16 = self.Bq.t().bfloat16().contiguous()                    # n x 3k
+        B = self.Bq.t().contiguous()                                            # n x 3k
+        if self.split_out:
+            # [B_hi | B_lo | B_hi] against heads [y_hi | y_hi | y_lo]: one bf16
+            # GEMM with FP32-level accuracy of the reconstruction
+            hi = B.bfloat16()
+            lo = (B - hi.float()).bfloat16()
+            self.BqT_bf16 = torch.cat([hi, lo, hi], dim=1).contiguous()         # n x 9k
+        else:
+            self.BqT_bf16 = B.bfloat16().contiguous()
 
     # inference ------------------------------------------------------------
     def encode(self, f, enc):
@@ -496,8 +527,9 @@ class QSurrogate:
         if self.center:
             x1 = self.w + self.kfeat
             _lib.check(_lib.lib().bdgfs_hybrid_tfeatures(C.byref(enc.args), enc.xc.data_ptr(),
-                                                         self.ldx, self.w, x1, self.k,
-                                                         _lib.stream_ptr()), 'bdgfs_hybrid_tfeatures')
+                                                         self.ldx, self.w, x1, self.k, self.nquad,
+                                                         x1 + 2 * self.k, _lib.stream_ptr()),
+                       'bdgfs_hybrid_tfeatures')
 
     def infer(self, enc, M):
         """Compact surrogate Q of the rows the indicator selected (device
@@ -511,10 +543,9 @@ class QSurrogate:
             gemm(h, self.inf_W[l], bias=self.inf_b[l], act=ACT_GELU, mcount=cnt, out_bf16=hn)
             h = hn
         gemm(xc, self.inf_W[3], bias=self.inf_b[3], mcount=cnt, out=enc.Y[:M])
-        _lib.check(_lib.lib().bdgfs_hybrid_heads(C.byref(enc.args), enc.Y.data_ptr(),
-                                                 NHEADS * self.k, self.k, NHEADS,
-                                                 enc.yb.data_ptr(), NHEADS * self.k,
-                                                 _lib.stream_ptr()), 'bdgfs_hybrid_heads')
+        heads = _lib.lib().bdgfs_hybrid_heads_split if self.split_out else _lib.lib().bdgfs_hybrid_heads
+        _lib.check(heads(C.byref(enc.args), enc.Y.data_ptr(), NHEADS * self.k, self.k, NHEADS,
+                         enc.yb.data_ptr(), enc.yb.shape[1], _lib.stream_ptr()), 'bdgfs_hybrid_heads')
         gemm(enc.yb[:M], self.BqT_bf16, row_scale=enc.rho2, mcount=cnt, out=enc.Qc[:M])
         if self.center:
             enc.shift(enc.Qc, False, enc.Qc, False, -1.0)           # back to the cell's drift
@@ -551,7 +582,8 @@ class QSurrogate:
         keys = ('Bd', 'Bq', 'mu', 'sigma', 'hscale')
         d = {k: getattr(self, k).cpu() for k in keys}
         d.update(W=[w.cpu() for w in self.W], b=[b.cpu() for b in self.b],
-                 k=self.k, w=self.w, Nv=self.Nv, center=self.center)
+                 k=self.k, w=self.w, Nv=self.Nv, center=self.center, split_out=self.split_out,
+                 nquad=self.nquad)
         return d
 
     def load_state_dict(self, d):
@@ -560,6 +592,8 @@ class QSurrogate:
             setattr(self, k, d[k].to(dev))
         self.k, self.w = int(d['k']), int(d['w'])
         self.center = bool(d.get('center', False))
+        self.split_out = bool(d.get('split_out', False))
+        self.nquad = int(d.get('nquad', 0))
         self.W = [w.to(dev) for w in d['W']]
         self.b = [b.to(dev) for b in d['b']]
         self._sync_bf16()
@@ -616,14 +650,15 @@ class HybridCollider:
             self._n = ndof
             self._net = None
         m = self.model
-        shape = (self._n, m.k, m.w, m.kin)
+        shape = (self._n, m.k, m.w, m.kin, m.split_out, m.nquad)
         if self._net != shape:
             dev = m.device
             ndof = self._n
             self.xc = torch.zeros(ndof, m.ldx, device=dev, dtype=torch.bfloat16)
             self.h = [torch.empty(ndof, m.w, device=dev, dtype=torch.bfloat16) for _ in range(2)]
             self.Y = torch.empty(ndof, NHEADS * m.k, device=dev)
-            self.yb = torch.empty(ndof, NHEADS * m.k, device=dev, dtype=torch.bfloat16)
+            self.yb = torch.empty(ndof, (3 if m.split_out else 1) * NHEADS * m.k, device=dev,
+                                  dtype=torch.bfloat16)
             self.Qc = torch.empty(ndof, m.n, device=dev, dtype=self.grid.dtype)
             self._net = shape
 

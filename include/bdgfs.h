@@ -388,6 +388,13 @@ int32_t bdgfs_hybrid_scatter(const bdgfs_hybrid_args* h, const void* Qc,
  * projected on the fly and written to Q; Qc itself is left unchanged). */
 int32_t bdgfs_hybrid_project_scatter(const bdgfs_hybrid_args* h,
                                      const void* Qc, void* Q, void* stream);
+/* bdgfs_hybrid_heads with each value split into bf16 hi and lo parts,
+ * written as [hi | hi | lo] column blocks of width nheads*k (ldo >=
+ * 3*nheads*k): against an output basis stored as [B_hi | B_lo | B_hi], one
+ * bf16 GEMM reconstructs Q to about FP32 accuracy. */
+int32_t bdgfs_hybrid_heads_split(const bdgfs_hybrid_args* h, const float* Y, int64_t ldy,
+                                 int64_t k, int32_t nheads, void* out, int64_t ldo,
+                                 void* stream);
 /* Spectral velocity shift of the first counts[0] compact rows: row p of out
  * is row p of in evaluated at the velocities c + sign * u_p, u_p =
  * sur_uT[p][0..2], by trigonometric interpolation on the periodic Nv^3 grid
@@ -401,11 +408,15 @@ int32_t bdgfs_hybrid_project_scatter(const bdgfs_hybrid_args* h,
  * exactly). */
 int32_t bdgfs_hybrid_shift(const bdgfs_hybrid_args* h, const void* in, int32_t in_bf16,
                            void* out, int32_t out_bf16, float sign, void* stream);
-/* Temperature features of the first counts[0] rows of the bf16 network
- * input xc (leading dimension ld): columns [x1, x1+k) <- (T-1) * columns
- * [x0, x0+k) and [x1+k, x1+2k) <- (T-1)^2 * the same, T = sur_uT[p][3]. */
+/* Features of the first counts[0] rows of the bf16 network input xc
+ * (leading dimension ld) from its deviation modes x = columns [x0, x0+k):
+ * columns [x1, x1+k) <- (T-1) x and [x1+k, x1+2k) <- (T-1)^2 x (T =
+ * sur_uT[p][3]; the linearised operator's temperature dependence), and the
+ * k2 (k2+1)/2 products x_i x_j, i <= j < k2, row-major over the upper
+ * triangle, at columns [xq, ...) (the quadratic term of the collision
+ * operator in the deviation; k2 <= 64, 0 for none). */
 int32_t bdgfs_hybrid_tfeatures(const bdgfs_hybrid_args* h, void* xc, int64_t ld, int64_t x0,
-                               int64_t x1, int64_t k, void* stream);
+                               int64_t x1, int64_t k, int32_t k2, int64_t xq, void* stream);
 /* Scale the network's output heads of the first counts[0] rows:
  * out[m][i*k + j] = sur_s[m]^i * Y[m][i*k + j], i < nheads, j < k
  * (Y float, leading dimension ldy; out bf16, leading dimension ldo). */
