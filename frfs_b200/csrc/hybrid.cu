@@ -309,68 +309,300 @@ __device__ __forceinline__ T from_f32(float x) { return T(x); }
 template <>
 __device__ __forceinline__ __nv_bfloat16 from_f32<__nv_bfloat16>(float x) { return __float2bfloat16_rn(x); }
 
-// Spectral shift of compact rows (bdgfs_hybrid_shift).  Along one axis the
-// shift by a is the circulant g_i = sum_j w[(i - j) mod N] f_j with
+// Spectral shift (bdgfs_hybrid_shift).  Along one axis the shift by a is
+// the circulant g_i = sum_j w[(i - j) mod N] f_j with
 //   w[k] = (1/N) sum_{m=-N/2}^{N/2-1} cos(2 pi m (k + a/h) / N)
 // (the real part of the trigonometric interpolant on the periodic grid);
-// the three axes are applied in turn on the row staged in shared memory
-// (z-stride padded to N + 1: the three pencil directions are free of bank
-// conflicts).  Grid-stride over the rows below the device count.
+// the three axes are applied in turn on a row staged in shared memory as a
+// padded cube, element (x, y, z) at (x*N + y)*(N + 1) + z (the three pencil
+// directions are then free of bank conflicts).  u: the shift per axis,
+// sign * u[d] / h in grid units; wt: 3N floats.  Ends with a barrier.
+template <int N>
+__device__ __forceinline__ int cube_at(int v)
+{
+    const int xy = v / N;
+    return xy * (N + 1) + (v - xy * N);
+}
+
+template <int N>
+__device__ void cube_shift(float* cube, float* wt, const float* u, double sign, double hg)
+{
+    constexpr int S = N + 1;
+    for (int i = threadIdx.x; i < 3 * N; i += blockDim.x) {
+        const int d = i / N, k = i - d * N;
+        const double a = sign * double(u[d]) / hg;
+        double w = 0.0;
+        for (int m = -N / 2; m < N / 2; ++m) w += cospi(2.0 * double(m) * (double(k) + a) / double(N));
+        wt[i] = float(w / double(N));
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int d = 2; d >= 0; --d) {                  // z, y, x
+        float w[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) w[k] = wt[d * N + k];
+        for (int p = threadIdx.x; p < N * N; p += blockDim.x) {
+            const int p0 = p / N, p1 = p - p0 * N;
+            int base, stride;
+            if (d == 2) { base = p * S; stride = 1; }                    // (x, y)
+            else if (d == 1) { base = p0 * N * S + p1; stride = S; }     // (x, z)
+            else { base = p0 * S + p1; stride = N * S; }                 // (y, z)
+            float v[N];
+#pragma unroll
+            for (int j = 0; j < N; ++j) v[j] = cube[base + j * stride];
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                float acc = 0.f;
+#pragma unroll
+                for (int j = 0; j < N; ++j) acc = fmaf(w[(i - j + N) % N], v[j], acc);
+                cube[base + i * stride] = acc;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <int N>
+constexpr size_t cube_smem_bytes()
+{
+    return sizeof(float) * (size_t(N) * N * (N + 1) + 3 * N);
+}
+
+// Grid-stride over the rows below the device count.
 template <int N, typename TI, typename TO>
 __global__ void __launch_bounds__(256) shift_kernel(const bdgfs_hybrid_args h, const TI* in, TO* out,
                                                     float sign)
 {
     extern __shared__ float sh[];
-    constexpr int S = N + 1;
     constexpr int n = N * N * N;
     float* cube = sh;
-    float* wt = sh + N * N * S;
+    float* wt = sh + N * N * (N + 1);
     const int64_t cnt = *h.counts;
     const double hg = h.c0[1] - h.c0[0];
     for (int64_t row = blockIdx.x; row < cnt; row += gridDim.x) {
         const TI* src = in + row * int64_t(n);
         TO* dst = out + row * int64_t(n);
-        for (int i = threadIdx.x; i < 3 * N; i += blockDim.x) {
-            const int d = i / N, k = i - d * N;
-            const double a = double(sign) * double(h.sur_uT[4 * row + d]) / hg;
-            double w = 0.0;
-            for (int m = -N / 2; m < N / 2; ++m) w += cospi(2.0 * double(m) * (double(k) + a) / double(N));
-            wt[i] = float(w / double(N));
-        }
-        for (int v = threadIdx.x; v < n; v += blockDim.x) {
-            const int xy = v / N;
-            cube[xy * S + (v - xy * N)] = to_f32(src[v]);
-        }
-        __syncthreads();
-#pragma unroll 1
-        for (int d = 2; d >= 0; --d) {              // z, y, x
-            float w[N];
-#pragma unroll
-            for (int k = 0; k < N; ++k) w[k] = wt[d * N + k];
-            for (int p = threadIdx.x; p < N * N; p += blockDim.x) {
-                const int p0 = p / N, p1 = p - p0 * N;
-                int base, stride;
-                if (d == 2) { base = p * S; stride = 1; }                    // (x, y)
-                else if (d == 1) { base = p0 * N * S + p1; stride = S; }     // (x, z)
-                else { base = p0 * S + p1; stride = N * S; }                 // (y, z)
-                float v[N];
-#pragma unroll
-                for (int j = 0; j < N; ++j) v[j] = cube[base + j * stride];
-#pragma unroll
-                for (int i = 0; i < N; ++i) {
-                    float acc = 0.f;
-#pragma unroll
-                    for (int j = 0; j < N; ++j) acc = fmaf(w[(i - j + N) % N], v[j], acc);
-                    cube[base + i * stride] = acc;
-                }
-            }
-            __syncthreads();
-        }
-        for (int v = threadIdx.x; v < n; v += blockDim.x) {
-            const int xy = v / N;
-            dst[v] = from_f32<TO>(cube[xy * S + (v - xy * N)]);
-        }
+        for (int v = threadIdx.x; v < n; v += blockDim.x) cube[cube_at<N>(v)] = to_f32(src[v]);
+        cube_shift<N>(cube, wt, h.sur_uT + 4 * row, double(sign), hg);
+        for (int v = threadIdx.x; v < n; v += blockDim.x) dst[v] = from_f32<TO>(cube[cube_at<N>(v)]);
         __syncthreads();                             // cube and wt reused by the next row
+    }
+}
+
+// Indicator with the row staged once in shared memory (FP32 state): the
+// moments, the Maxwellian deviation and the deviation row are computed
+// from shared memory, so f is read from HBM once; with h.center the
+// deviation row is also re-centred at zero velocity (cube_shift by +u)
+// before its bf16 copy is written.  Same lists, counts and per-row outputs
+// as indicator_kernel.
+template <int N, bool CENTER>
+__global__ void __launch_bounds__(256) indicator_smem_kernel(const bdgfs_hybrid_args h,
+                                                             const float* __restrict__ f)
+{
+    extern __shared__ float sh[];
+    constexpr int n = N * N * N;
+    float* cube = sh;
+    float* wt = sh + N * N * (N + 1);
+    __shared__ double red[8 * 8];
+    __shared__ double cs[N], ex[3][N];
+    __shared__ int64_t s_pos;
+    __shared__ float s_u[3];
+    const int64_t dof = blockIdx.x;
+    const float* fd = f + dof * int64_t(n);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) cs[i] = h.c0[i];
+    for (int v = 4 * threadIdx.x; v < n; v += 4 * blockDim.x) {       // 16-byte loads
+        const float4 x = *reinterpret_cast<const float4*>(fd + v);
+        float* c = cube + cube_at<N>(v);                               // N % 4 == 0: one row
+        c[0] = x.x; c[1] = x.y; c[2] = x.z; c[3] = x.w;
+    }
+    __syncthreads();
+    double m[5] = {0, 0, 0, 0, 0};
+    for (int v = threadIdx.x; v < n; v += blockDim.x) {
+        uint32_t ix, iy, iz;
+        vsplit(uint32_t(v), uint32_t(N), ix, iy, iz);
+        const double x = double(cube[cube_at<N>(v)]);
+        const double cx = cs[ix], cy = cs[iy], cz = cs[iz];
+        m[0] += x;
+        m[1] += cx * x;
+        m[2] += cy * x;
+        m[3] += cz * x;
+        m[4] += (cx * cx + cy * cy + cz * cz) * x;
+    }
+    block_sum<5>(m, red);
+    const double rho = m[0] * h.cw;
+    const double ux = m[1] / m[0], uy = m[2] / m[0], uz = m[3] / m[0];
+    const double Tt = (m[4] / m[0] - (ux * ux + uy * uy + uz * uz)) * (2.0 / 3.0);
+    const bool ok = rho > 0.0 && Tt > 0.0;
+    const double a = ok ? rho / pow(3.141592653589793 * Tt, 1.5) : 0.0;
+    if (ok) {
+        const double it = 1.0 / Tt;
+        for (int i = threadIdx.x; i < 3 * N; i += blockDim.x) {
+            const int d = i / N, j = i - d * N;
+            const double c = cs[j] - (d == 0 ? ux : d == 1 ? uy : uz);
+            ex[d][j] = exp(-c * c * it);
+        }
+    }
+    __syncthreads();
+    double e[2] = {0, 0};
+    if (ok) {
+        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+            uint32_t ix, iy, iz;
+            vsplit(uint32_t(v), uint32_t(N), ix, iy, iz);
+            const double x = double(cube[cube_at<N>(v)]);
+            const double d = x - a * ex[0][ix] * ex[1][iy] * ex[2][iz];
+            e[0] += d * d;
+            e[1] += x * x;
+        }
+    }
+    block_sum<2>(e, red);
+    if (threadIdx.x == 0) {
+        const double eps = (ok && e[1] > 0.0) ? sqrt(e[0] / e[1]) : 1e30;
+        s_pos = -1;
+        if (h.eps) h.eps[dof] = float(eps);
+        const bool sur = eps < double(h.threshold);
+        const uint64_t seed = h.seed_dev ? *h.seed_dev : h.seed;
+        const bool re = sur && (double(mix32(seed * 0x100000001B3ull + uint64_t(dof))) <
+                                double(h.recheck) * 4294967296.0);
+        if (h.flag) h.flag[dof] = uint8_t(sur ? (re ? 2 : 1) : 0);
+        if (sur) {
+            const int64_t p = int64_t(atomicAdd(reinterpret_cast<unsigned long long*>(h.counts), 1ull));
+            h.sur_idx[p] = int32_t(dof);
+            h.sur_inv_rho[p] = float(1.0 / rho);
+            h.sur_rho2[p] = float(rho * rho);
+            s_pos = p;
+            if (h.sur_s) h.sur_s[p] = float(sqrt(e[0]) / rho);
+            if (h.sur_uT) {
+                h.sur_uT[4 * p + 0] = float(ux);
+                h.sur_uT[4 * p + 1] = float(uy);
+                h.sur_uT[4 * p + 2] = float(uz);
+                h.sur_uT[4 * p + 3] = float(Tt);
+            }
+            if (h.feat) {
+                __nv_bfloat16* fr = static_cast<__nv_bfloat16*>(h.feat) + p * h.feat_ld;
+                fr[0] = __float2bfloat16_rn(h.center ? 0.f : float(ux));
+                fr[1] = __float2bfloat16_rn(h.center ? 0.f : float(uy));
+                fr[2] = __float2bfloat16_rn(h.center ? 0.f : float(uz));
+                fr[3] = __float2bfloat16_rn(float(Tt - 1.0));
+            }
+            s_u[0] = float(ux);
+            s_u[1] = float(uy);
+            s_u[2] = float(uz);
+        }
+        if (!sur || re) {
+            const int64_t p = int64_t(atomicAdd(reinterpret_cast<unsigned long long*>(h.counts + 1), 1ull));
+            h.spec_idx[p] = int32_t(dof);
+        }
+        if (re) atomicAdd(reinterpret_cast<unsigned long long*>(h.counts + 2), 1ull);
+    }
+    __syncthreads();
+    const int64_t p = s_pos;
+    if (p < 0 || !h.dev_rows) return;                  // uniform per block
+    const double inv = (ok && e[0] > 0.0) ? 1.0 / sqrt(e[0]) : 0.0;
+    for (int v = threadIdx.x; v < n; v += blockDim.x) {
+        uint32_t ix, iy, iz;
+        vsplit(uint32_t(v), uint32_t(N), ix, iy, iz);
+        float* c = cube + cube_at<N>(v);
+        *c = ok ? float((double(*c) - a * ex[0][ix] * ex[1][iy] * ex[2][iz]) * inv) : 0.f;
+    }
+    __syncthreads();
+    if constexpr (CENTER) cube_shift<N>(cube, wt, s_u, 1.0, cs[1] - cs[0]);
+    __nv_bfloat16* out = static_cast<__nv_bfloat16*>(h.dev_rows) + p * int64_t(n);
+    for (int v = 4 * threadIdx.x; v < n; v += 4 * blockDim.x) {
+        const float* c = cube + cube_at<N>(v);
+        __align__(8) __nv_bfloat162 hv[2] = {__floats2bfloat162_rn(c[0], c[1]),
+                                             __floats2bfloat162_rn(c[2], c[3])};
+        *reinterpret_cast<uint2*>(out + v) = *reinterpret_cast<const uint2*>(hv);
+    }
+}
+
+// project_scatter for the centred surrogate (FP32): each compact row is
+// staged in shared memory, moved back to its cell's drift (cube_shift by
+// -u), then projected in FP64 and scattered exactly as
+// project_scatter_kernel does.  Qc is left unchanged.
+template <int N>
+__global__ void __launch_bounds__(256) shift_project_scatter_kernel(const bdgfs_hybrid_args h,
+                                                                    const float* __restrict__ Qc,
+                                                                    float* __restrict__ Q)
+{
+    extern __shared__ float sh[];
+    constexpr int n = N * N * N;
+    float* cube = sh;
+    float* wt = sh + N * N * (N + 1);
+    __shared__ double red[5 * 8];
+    __shared__ double cs[N];
+    const int64_t row = blockIdx.x;
+    if (row == 0 && threadIdx.x == 0 && h.seed_dev) *h.seed_dev += 1;   // next step's sample
+    const int64_t cnt = *h.counts;
+    if (row >= cnt) return;
+    const float* src = Qc + row * int64_t(n);
+    const int64_t dof = h.sur_idx[row];
+    float* dst = Q + dof * int64_t(n);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) cs[i] = h.c0[i];
+    for (int v = 4 * threadIdx.x; v < n; v += 4 * blockDim.x) {
+        const float4 x = *reinterpret_cast<const float4*>(src + v);
+        float* c = cube + cube_at<N>(v);
+        c[0] = x.x; c[1] = x.y; c[2] = x.z; c[3] = x.w;
+    }
+    __syncthreads();
+    cube_shift<N>(cube, wt, h.sur_uT + 4 * row, -1.0, cs[1] - cs[0]);
+    double m[5] = {0, 0, 0, 0, 0};
+    for (int v = threadIdx.x; v < n; v += blockDim.x) {
+        uint32_t ix, iy, iz;
+        vsplit(uint32_t(v), uint32_t(N), ix, iy, iz);
+        const double x = double(cube[cube_at<N>(v)]);
+        const double cx = cs[ix], cy = cs[iy], cz = cs[iz];
+        m[0] += x;
+        m[1] += cx * x;
+        m[2] += cy * x;
+        m[3] += cz * x;
+        m[4] += (cx * cx + cy * cy + cz * cz) * x;
+    }
+    block_sum<5>(m, red);
+    const bool re = h.flag[dof] == 2;
+    if (!isfinite(m[0] + m[1] + m[2] + m[3] + m[4])) {
+        if (!re && h.fb_idx && threadIdx.x == 0)
+            h.fb_idx[atomicAdd(reinterpret_cast<unsigned long long*>(h.counts + 3), 1ull)] = int32_t(dof);
+        return;
+    }
+    double lam[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        double t = 0.0;
+#pragma unroll
+        for (int j = 0; j < 5; ++j) t += h.ginv[i * 5 + j] * m[j];
+        lam[i] = t;
+    }
+    double e[2] = {0, 0};
+    for (int v = 4 * threadIdx.x; v < n; v += 4 * blockDim.x) {
+        uint32_t ix, iy, iz;
+        vsplit(uint32_t(v), uint32_t(N), ix, iy, iz);
+        const double cx = cs[ix], cy = cs[iy];
+        const double lxy = lam[0] + lam[1] * cx + lam[2] * cy + lam[4] * (cx * cx + cy * cy);
+        const float* c = cube + cube_at<N>(v);
+        float o[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double cz = cs[iz + j];
+            o[j] = float(double(c[j]) - (lxy + lam[3] * cz + lam[4] * cz * cz));
+        }
+        if (!re) {
+            *reinterpret_cast<float4*>(dst + v) = make_float4(o[0], o[1], o[2], o[3]);
+        } else {
+            const float4 sp = *reinterpret_cast<const float4*>(dst + v);
+            const float spv[4] = {sp.x, sp.y, sp.z, sp.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const double d = double(o[j]) - double(spv[j]);
+                e[0] += d * d;
+                e[1] += double(spv[j]) * double(spv[j]);
+            }
+        }
+    }
+    if (!re) return;                                   // uniform per block
+    block_sum<2>(e, red);
+    if (threadIdx.x == 0 && h.recheck_err) {
+        atomicAdd(h.recheck_err, e[0]);
+        atomicAdd(h.recheck_err + 1, e[1]);
     }
 }
 
@@ -458,6 +690,47 @@ static int check_h(const bdgfs_hybrid_args* h)
     return BDGFS_OK;
 }
 
+static int shift_any(const bdgfs_hybrid_args* h, const void* in, int in_bf16, void* out, int out_bf16,
+                     float sign, cudaStream_t st);
+
+static bool cube_grid(int Nv)
+{
+    return Nv == 8 || Nv == 12 || Nv == 16 || Nv == 24 || Nv == 32;
+}
+
+template <int N, bool CENTER>
+static int indicator_smem_launch(const bdgfs_hybrid_args* h, const float* f, cudaStream_t st)
+{
+    constexpr size_t smem = cube_smem_bytes<N>();
+    if (const int rc = smem_optin(reinterpret_cast<const void*>(indicator_smem_kernel<N, CENTER>), smem))
+        return rc;
+    indicator_smem_kernel<N, CENTER><<<unsigned(h->ndof), 256, smem, st>>>(*h, f);
+    return cuda_status(cudaGetLastError());
+}
+
+template <bool CENTER>
+static int indicator_smem_dispatch(const bdgfs_hybrid_args* h, const float* f, cudaStream_t st)
+{
+    switch (h->Nv) {
+    case 8: return indicator_smem_launch<8, CENTER>(h, f, st);
+    case 12: return indicator_smem_launch<12, CENTER>(h, f, st);
+    case 16: return indicator_smem_launch<16, CENTER>(h, f, st);
+    case 24: return indicator_smem_launch<24, CENTER>(h, f, st);
+    case 32: return indicator_smem_launch<32, CENTER>(h, f, st);
+    default: return BDGFS_EUNSUPPORTED;
+    }
+}
+
+template <int N>
+static int shift_project_scatter_launch(const bdgfs_hybrid_args* h, const float* Qc, float* Q, cudaStream_t st)
+{
+    constexpr size_t smem = cube_smem_bytes<N>();
+    if (const int rc = smem_optin(reinterpret_cast<const void*>(shift_project_scatter_kernel<N>), smem))
+        return rc;
+    shift_project_scatter_kernel<N><<<unsigned(h->ndof), 256, smem, st>>>(*h, Qc, Q);
+    return cuda_status(cudaGetLastError());
+}
+
 extern "C" int32_t bdgfs_hybrid_classify(const bdgfs_hybrid_args* h, const void* f, void* stream)
 {
     int rc = check_h(h);
@@ -473,6 +746,13 @@ extern "C" int32_t bdgfs_hybrid_classify(const bdgfs_hybrid_args* h, const void*
     if (h->ndof == 0) return BDGFS_OK;
     const bool v4 = h->Nv % 4 == 0 && (reinterpret_cast<uintptr_t>(f) & 15u) == 0 &&
                     (!h->dev_rows || (reinterpret_cast<uintptr_t>(h->dev_rows) & 7u) == 0);
+    if (h->center && (!h->sur_uT || !h->dev_rows)) return BDGFS_EINVAL;
+    if (!h->fp64 && v4 && cube_grid(h->Nv)) {
+        // the row staged once in shared memory; with center the deviation
+        // rows are re-centred in the same launch
+        return h->center ? indicator_smem_dispatch<true>(h, static_cast<const float*>(f), st)
+                         : indicator_smem_dispatch<false>(h, static_cast<const float*>(f), st);
+    }
     if (h->fp64) {
         if (v4)
             indicator_kernel<double, 4><<<unsigned(h->ndof), 256, 0, st>>>(*h, static_cast<const double*>(f));
@@ -484,7 +764,9 @@ extern "C" int32_t bdgfs_hybrid_classify(const bdgfs_hybrid_args* h, const void*
         else
             indicator_kernel<float, 1><<<unsigned(h->ndof), 256, 0, st>>>(*h, static_cast<const float*>(f));
     }
-    return cuda_status(cudaGetLastError());
+    if (cudaGetLastError() != cudaSuccess) return BDGFS_ECUDA;
+    if (h->center) return shift_any(h, h->dev_rows, 1, h->dev_rows, 1, 1.f, st);
+    return BDGFS_OK;
 }
 
 extern "C" int32_t bdgfs_hybrid_project(const bdgfs_hybrid_args* h, void* Qc, void* stream)
@@ -509,6 +791,10 @@ extern "C" int32_t bdgfs_hybrid_scatter(const bdgfs_hybrid_args* h, const void* 
     if (!Qc || !Q || !h->counts || !h->sur_idx || !h->flag) return BDGFS_EINVAL;
     if (h->ndof == 0) return BDGFS_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (h->center) {                   // back to each cell's drift, in place
+        if (!h->sur_uT) return BDGFS_EINVAL;
+        if (const int r = shift_any(h, Qc, 0, const_cast<void*>(Qc), 0, -1.f, st)) return r;
+    }
     if (h->fp64)
         scatter_kernel<double><<<unsigned(h->ndof), 256, 0, st>>>(*h, static_cast<const double*>(Qc),
                                                                   static_cast<double*>(Q));
@@ -528,6 +814,21 @@ extern "C" int32_t bdgfs_hybrid_project_scatter(const bdgfs_hybrid_args* h, cons
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const bool v4 = h->Nv % 4 == 0 && (reinterpret_cast<uintptr_t>(Qc) & 15u) == 0 &&
                     (reinterpret_cast<uintptr_t>(Q) & 15u) == 0;
+    if (h->center) {
+        if (!h->sur_uT) return BDGFS_EINVAL;
+        if (!h->fp64 && v4 && cube_grid(h->Nv)) {     // shift back, project, scatter: one pass
+            const float* q = static_cast<const float*>(Qc);
+            float* o = static_cast<float*>(Q);
+            switch (h->Nv) {
+            case 8: return shift_project_scatter_launch<8>(h, q, o, st);
+            case 12: return shift_project_scatter_launch<12>(h, q, o, st);
+            case 16: return shift_project_scatter_launch<16>(h, q, o, st);
+            case 24: return shift_project_scatter_launch<24>(h, q, o, st);
+            default: return shift_project_scatter_launch<32>(h, q, o, st);
+            }
+        }
+        if (const int r = shift_any(h, Qc, 0, const_cast<void*>(Qc), 0, -1.f, st)) return r;
+    }
     if (h->fp64) {
         if (v4)
             project_scatter_kernel<double, 4><<<unsigned(h->ndof), 256, 0, st>>>(
@@ -563,7 +864,7 @@ extern "C" int32_t bdgfs_hybrid_heads(const bdgfs_hybrid_args* h, const float* Y
 template <int N, typename TI, typename TO>
 static int shift_launch(const bdgfs_hybrid_args* h, const void* in, void* out, float sign, cudaStream_t st)
 {
-    const size_t smem = sizeof(float) * (size_t(N) * N * (N + 1) + 3 * N);
+    constexpr size_t smem = cube_smem_bytes<N>();
     if (const int rc = smem_optin(reinterpret_cast<const void*>(shift_kernel<N, TI, TO>), smem)) return rc;
     int dev = 0, nsm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
@@ -600,7 +901,12 @@ extern "C" int32_t bdgfs_hybrid_shift(const bdgfs_hybrid_args* h, const void* in
     if (rc) return rc;
     if (!in || !out || !h->counts || !h->sur_uT || h->Nv < 2) return BDGFS_EINVAL;
     if (h->ndof == 0) return BDGFS_OK;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return shift_any(h, in, in_bf16, out, out_bf16, sign, static_cast<cudaStream_t>(stream));
+}
+
+static int shift_any(const bdgfs_hybrid_args* h, const void* in, int in_bf16, void* out, int out_bf16,
+                     float sign, cudaStream_t st)
+{
     switch (h->Nv) {
     case 8: return shift_types<8>(h, in, in_bf16, out, out_bf16, sign, st);
     case 12: return shift_types<12>(h, in, in_bf16, out, out_bf16, sign, st);

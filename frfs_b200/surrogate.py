@@ -547,8 +547,8 @@ class QSurrogate:
         _lib.check(heads(C.byref(enc.args), enc.Y.data_ptr(), NHEADS * self.k, self.k, NHEADS,
                          enc.yb.data_ptr(), enc.yb.shape[1], _lib.stream_ptr()), 'bdgfs_hybrid_heads')
         gemm(enc.yb[:M], self.BqT_bf16, row_scale=enc.rho2, mcount=cnt, out=enc.Qc[:M])
-        if self.center:
-            enc.shift(enc.Qc, False, enc.Qc, False, -1.0)           # back to the cell's drift
+        # (centred model: Qc holds Q at zero drift; the scatter launch moves
+        # each row back to its cell's drift)
 
     def evaluate(self, nsamples, seed=1, chunk=8192, family=None):
         """Relative L2 error of the surrogate (with conservation projection)
@@ -689,8 +689,8 @@ class HybridCollider:
         self.args = self._args(ndof, seed, recheck)
         _lib.check(_lib.lib().bdgfs_hybrid_classify(C.byref(self.args), f2.data_ptr(),
                                                     _lib.stream_ptr()), 'bdgfs_hybrid_classify')
-        if self.model.center:                    # deviation directions at zero drift
-            self.shift(self.dev_rows, True, self.dev_rows, True, 1.0)
+        # with model.center the indicator launch also re-centres the
+        # deviation rows at zero velocity
         return ndof
 
     def shift(self, src, src_bf16, dst, dst_bf16, sign):

@@ -368,9 +368,15 @@ typedef struct bdgfs_hybrid_args {
                                 the spectral operator on that list         */
     float* sur_uT;           /* optional [ndof][4]: (u_x, u_y, u_z, T) of
                                 surrogate row p (FP32)                      */
-    int32_t center;          /* nonzero: the feature columns get
-                                (0, 0, 0, T - 1), the rows being re-centred
-                                at zero velocity by bdgfs_hybrid_shift     */
+    int32_t center;          /* nonzero (needs sur_uT and dev_rows): the
+                                surrogate works at zero drift --
+                                bdgfs_hybrid_classify writes the deviation
+                                rows re-centred at zero velocity and the
+                                features (0, 0, 0, T - 1); the scatter
+                                entries move each compact row of Qc back to
+                                its cell's drift first (FP32 rows: fused with
+                                the projection, Qc unchanged; otherwise Qc
+                                is shifted in place)                        */
     int32_t pad2_;
 } bdgfs_hybrid_args;
 
