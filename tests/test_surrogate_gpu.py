@@ -206,10 +206,14 @@ def test_head_labels_recombine_to_q(cuda):
     assert float(err.max()) < 1e-2, float(err.max())
 
 
+SMALL = dict(Nv=24, Nrho=8, M=6, dev=6, k=64, w=256)
+SMALL_FIT = dict(nsamples=32768, ntest=2048, epochs=8, lr=1e-3, batch=512, nbasis=4096, chunk=4096)
+
+
 @pytest.fixture(scope='module')
 def small_fit(cuda):
-    be, vm, sm, q = _model(k=64, w=256)
-    q.fit(nsamples=16384, ntest=2048, epochs=6, lr=1e-3, batch=512, nbasis=4096, chunk=4096)
+    be, vm, sm, q = _model(**SMALL)
+    q.fit(**SMALL_FIT)
     return be, vm, sm, q
 
 
@@ -232,8 +236,8 @@ def test_small_fit_learns_and_gains(small_fit):
     q._fold()
     print(f'small fit: trained {trained:.3e}, linear path {linear:.3e}')
     assert trained < 1.1 * linear, (trained, linear)
-    q_raw = QSurrogate(sm.grid, nmodes=64, width=256, center=False)
-    q_raw.fit(nsamples=16384, ntest=2048, epochs=6, lr=1e-3, batch=512, nbasis=4096, chunk=4096)
+    q_raw = QSurrogate(sm.grid, nmodes=SMALL['k'], width=SMALL['w'], center=False)
+    q_raw.fit(**SMALL_FIT)
     print(f'raw rows: {q_raw.test_err["aggregate"]:.3e}')
     assert trained < 0.7 * q_raw.test_err['aggregate'], (trained, q_raw.test_err)
     f = sample_family(vm.c0(), 2048, torch.Generator(device=be.device).manual_seed(8), be.device)
