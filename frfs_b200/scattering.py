@@ -239,6 +239,15 @@ class DGFSVHSGLLHybridScatteringModel(DGFSVHSGLLScatteringModel):
                            trained and saved there when absent
       surrogate-family     training distributions: 'couette' (default) or
                            'cavity' (see frfs_b200.surrogate)
+      surrogate-center     true: the network works on rows re-centred at
+                           zero velocity (QSurrogate center=True: 3x lower
+                           Q error on the Couette family); default false,
+                           because at 24^3 the spectral operator is not
+                           shift-equivariant to better than 0.3-1 % of Q,
+                           and on near-equilibrium cells -- whose Q is
+                           mostly that operator's own error on a drifting
+                           Maxwellian -- the raw-row model follows the
+                           spectral solve more closely
       surrogate-nsamples / -epochs / -modes / -width / -lr / -seed
                            training settings (200000 / 20 / 512 / 1024 /
                            3e-4 / 0)
@@ -257,7 +266,8 @@ class DGFSVHSGLLHybridScatteringModel(DGFSVHSGLLScatteringModel):
         self.surrogate = QSurrogate(self.grid,
                                     nmodes=cfg.getint(sect, 'surrogate-modes', 512),
                                     width=cfg.getint(sect, 'surrogate-width', 1024),
-                                    family=fams[fam])
+                                    family=fams[fam],
+                                    center=cfg.getbool(sect, 'surrogate-center', False))
         path = cfg.get(sect, 'surrogate-file', '')
         if path and os.path.exists(path):
             self.surrogate.load_state_dict(torch.load(path, map_location='cpu'))
