@@ -948,7 +948,7 @@ def run_hybrid_steps(nsteps, nwarm=3):
     be = CUDABackend(cfg)
     mesh = StructuredMesh((8, 8, 8), (0, 0, 0), (1, 1, 1), periodic='', bcnames=names)
     s5 = DGFSSystem(be, mesh, cfg, nreg=3)
-    q = QSurrogate(s5.sm.grid, nmodes=256, width=1024)
+    q = QSurrogate(s5.sm.grid, nmodes=512, width=1024, center=False)   # the cavity hybrid's model
     dev = be.device
     g = torch.Generator(device=dev).manual_seed(0)
     n = q.n
