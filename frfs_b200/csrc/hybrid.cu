@@ -416,17 +416,22 @@ __global__ void __launch_bounds__(256) indicator_smem_kernel(const bdgfs_hybrid_
         c[0] = x.x; c[1] = x.y; c[2] = x.z; c[3] = x.w;
     }
     __syncthreads();
+    // every pass walks chunks of 4 consecutive z (one index split per chunk)
+    constexpr int NC = n / 4, NZ = N / 4;
     double m[5] = {0, 0, 0, 0, 0};
-    for (int v = threadIdx.x; v < n; v += blockDim.x) {
-        uint32_t ix, iy, iz;
-        vsplit(uint32_t(v), uint32_t(N), ix, iy, iz);
-        const double x = double(cube[cube_at<N>(v)]);
-        const double cx = cs[ix], cy = cs[iy], cz = cs[iz];
-        m[0] += x;
-        m[1] += cx * x;
-        m[2] += cy * x;
-        m[3] += cz * x;
-        m[4] += (cx * cx + cy * cy + cz * cz) * x;
+    for (int c = threadIdx.x; c < NC; c += blockDim.x) {
+        const int xy = c / NZ, z0 = 4 * (c - xy * NZ), ix = xy / N, iy = xy - ix * N;
+        const float* q = cube + xy * (N + 1) + z0;
+        const double cx = cs[ix], cy = cs[iy], b = cx * cx + cy * cy;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double x = double(q[j]), cz = cs[z0 + j];
+            m[0] += x;
+            m[1] += cx * x;
+            m[2] += cy * x;
+            m[3] += cz * x;
+            m[4] += (b + cz * cz) * x;
+        }
     }
     block_sum<5>(m, red);
     const double rho = m[0] * h.cw;
@@ -445,13 +450,17 @@ __global__ void __launch_bounds__(256) indicator_smem_kernel(const bdgfs_hybrid_
     __syncthreads();
     double e[2] = {0, 0};
     if (ok) {
-        for (int v = threadIdx.x; v < n; v += blockDim.x) {
-            uint32_t ix, iy, iz;
-            vsplit(uint32_t(v), uint32_t(N), ix, iy, iz);
-            const double x = double(cube[cube_at<N>(v)]);
-            const double d = x - a * ex[0][ix] * ex[1][iy] * ex[2][iz];
-            e[0] += d * d;
-            e[1] += x * x;
+        for (int c = threadIdx.x; c < NC; c += blockDim.x) {
+            const int xy = c / NZ, z0 = 4 * (c - xy * NZ), ix = xy / N, iy = xy - ix * N;
+            const float* q = cube + xy * (N + 1) + z0;
+            const double axy = a * ex[0][ix] * ex[1][iy];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const double x = double(q[j]);
+                const double d = x - axy * ex[2][z0 + j];
+                e[0] += d * d;
+                e[1] += x * x;
+            }
         }
     }
     block_sum<2>(e, red);
@@ -498,11 +507,13 @@ __global__ void __launch_bounds__(256) indicator_smem_kernel(const bdgfs_hybrid_
     const int64_t p = s_pos;
     if (p < 0 || !h.dev_rows) return;                  // uniform per block
     const double inv = (ok && e[0] > 0.0) ? 1.0 / sqrt(e[0]) : 0.0;
-    for (int v = threadIdx.x; v < n; v += blockDim.x) {
-        uint32_t ix, iy, iz;
-        vsplit(uint32_t(v), uint32_t(N), ix, iy, iz);
-        float* c = cube + cube_at<N>(v);
-        *c = ok ? float((double(*c) - a * ex[0][ix] * ex[1][iy] * ex[2][iz]) * inv) : 0.f;
+    for (int c = threadIdx.x; c < NC; c += blockDim.x) {
+        const int xy = c / NZ, z0 = 4 * (c - xy * NZ), ix = xy / N, iy = xy - ix * N;
+        float* q = cube + xy * (N + 1) + z0;
+        const double axy = a * ex[0][ix] * ex[1][iy];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            q[j] = ok ? float((double(q[j]) - axy * ex[2][z0 + j]) * inv) : 0.f;
     }
     __syncthreads();
     if constexpr (CENTER) cube_shift<N>(cube, wt, s_u, 1.0, cs[1] - cs[0]);
@@ -515,11 +526,12 @@ __global__ void __launch_bounds__(256) indicator_smem_kernel(const bdgfs_hybrid_
     }
 }
 
-// project_scatter for the centred surrogate (FP32): each compact row is
-// staged in shared memory, moved back to its cell's drift (cube_shift by
-// -u), then projected in FP64 and scattered exactly as
-// project_scatter_kernel does.  Qc is left unchanged.
-template <int N>
+// project_scatter with each compact row staged once in shared memory
+// (FP32; Qc read from HBM once); SHIFT (centred surrogate): the row is first
+// moved back to its cell's drift (cube_shift by -u).  Then projected in
+// FP64 and scattered exactly as project_scatter_kernel does.  Qc is left
+// unchanged.
+template <int N, bool SHIFT>
 __global__ void __launch_bounds__(256) shift_project_scatter_kernel(const bdgfs_hybrid_args h,
                                                                     const float* __restrict__ Qc,
                                                                     float* __restrict__ Q)
@@ -544,18 +556,22 @@ __global__ void __launch_bounds__(256) shift_project_scatter_kernel(const bdgfs_
         c[0] = x.x; c[1] = x.y; c[2] = x.z; c[3] = x.w;
     }
     __syncthreads();
-    cube_shift<N>(cube, wt, h.sur_uT + 4 * row, -1.0, cs[1] - cs[0]);
+    if constexpr (SHIFT) cube_shift<N>(cube, wt, h.sur_uT + 4 * row, -1.0, cs[1] - cs[0]);
+    constexpr int NC = n / 4, NZ = N / 4;
     double m[5] = {0, 0, 0, 0, 0};
-    for (int v = threadIdx.x; v < n; v += blockDim.x) {
-        uint32_t ix, iy, iz;
-        vsplit(uint32_t(v), uint32_t(N), ix, iy, iz);
-        const double x = double(cube[cube_at<N>(v)]);
-        const double cx = cs[ix], cy = cs[iy], cz = cs[iz];
-        m[0] += x;
-        m[1] += cx * x;
-        m[2] += cy * x;
-        m[3] += cz * x;
-        m[4] += (cx * cx + cy * cy + cz * cz) * x;
+    for (int c = threadIdx.x; c < NC; c += blockDim.x) {
+        const int xy = c / NZ, z0 = 4 * (c - xy * NZ), ix = xy / N, iy = xy - ix * N;
+        const float* q = cube + xy * (N + 1) + z0;
+        const double cx = cs[ix], cy = cs[iy], b = cx * cx + cy * cy;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double x = double(q[j]), cz = cs[z0 + j];
+            m[0] += x;
+            m[1] += cx * x;
+            m[2] += cy * x;
+            m[3] += cz * x;
+            m[4] += (b + cz * cz) * x;
+        }
     }
     block_sum<5>(m, red);
     const bool re = h.flag[dof] == 2;
@@ -574,11 +590,10 @@ __global__ void __launch_bounds__(256) shift_project_scatter_kernel(const bdgfs_
     }
     double e[2] = {0, 0};
     for (int v = 4 * threadIdx.x; v < n; v += 4 * blockDim.x) {
-        uint32_t ix, iy, iz;
-        vsplit(uint32_t(v), uint32_t(N), ix, iy, iz);
+        const int xy = v / N, iz = v - xy * N, ix = xy / N, iy = xy - ix * N;
         const double cx = cs[ix], cy = cs[iy];
         const double lxy = lam[0] + lam[1] * cx + lam[2] * cy + lam[4] * (cx * cx + cy * cy);
-        const float* c = cube + cube_at<N>(v);
+        const float* c = cube + xy * (N + 1) + iz;
         float o[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -721,14 +736,26 @@ static int indicator_smem_dispatch(const bdgfs_hybrid_args* h, const float* f, c
     }
 }
 
-template <int N>
+template <int N, bool SHIFT>
 static int shift_project_scatter_launch(const bdgfs_hybrid_args* h, const float* Qc, float* Q, cudaStream_t st)
 {
     constexpr size_t smem = cube_smem_bytes<N>();
-    if (const int rc = smem_optin(reinterpret_cast<const void*>(shift_project_scatter_kernel<N>), smem))
+    if (const int rc = smem_optin(reinterpret_cast<const void*>(shift_project_scatter_kernel<N, SHIFT>), smem))
         return rc;
-    shift_project_scatter_kernel<N><<<unsigned(h->ndof), 256, smem, st>>>(*h, Qc, Q);
+    shift_project_scatter_kernel<N, SHIFT><<<unsigned(h->ndof), 256, smem, st>>>(*h, Qc, Q);
     return cuda_status(cudaGetLastError());
+}
+
+template <bool SHIFT>
+static int staged_project_scatter(const bdgfs_hybrid_args* h, const float* q, float* o, cudaStream_t st)
+{
+    switch (h->Nv) {
+    case 8: return shift_project_scatter_launch<8, SHIFT>(h, q, o, st);
+    case 12: return shift_project_scatter_launch<12, SHIFT>(h, q, o, st);
+    case 16: return shift_project_scatter_launch<16, SHIFT>(h, q, o, st);
+    case 24: return shift_project_scatter_launch<24, SHIFT>(h, q, o, st);
+    default: return shift_project_scatter_launch<32, SHIFT>(h, q, o, st);
+    }
 }
 
 extern "C" int32_t bdgfs_hybrid_classify(const bdgfs_hybrid_args* h, const void* f, void* stream)
@@ -747,11 +774,11 @@ extern "C" int32_t bdgfs_hybrid_classify(const bdgfs_hybrid_args* h, const void*
     const bool v4 = h->Nv % 4 == 0 && (reinterpret_cast<uintptr_t>(f) & 15u) == 0 &&
                     (!h->dev_rows || (reinterpret_cast<uintptr_t>(h->dev_rows) & 7u) == 0);
     if (h->center && (!h->sur_uT || !h->dev_rows)) return BDGFS_EINVAL;
-    if (!h->fp64 && v4 && cube_grid(h->Nv)) {
-        // the row staged once in shared memory; with center the deviation
-        // rows are re-centred in the same launch
-        return h->center ? indicator_smem_dispatch<true>(h, static_cast<const float*>(f), st)
-                         : indicator_smem_dispatch<false>(h, static_cast<const float*>(f), st);
+    if (h->center && !h->fp64 && v4 && cube_grid(h->Nv)) {
+        // the row staged once in shared memory and the deviation row
+        // re-centred in the same launch (without centring the streaming
+        // kernel below is faster: more CTAs per SM keep more loads in flight)
+        return indicator_smem_dispatch<true>(h, static_cast<const float*>(f), st);
     }
     if (h->fp64) {
         if (v4)
@@ -816,17 +843,8 @@ extern "C" int32_t bdgfs_hybrid_project_scatter(const bdgfs_hybrid_args* h, cons
                     (reinterpret_cast<uintptr_t>(Q) & 15u) == 0;
     if (h->center) {
         if (!h->sur_uT) return BDGFS_EINVAL;
-        if (!h->fp64 && v4 && cube_grid(h->Nv)) {     // shift back, project, scatter: one pass
-            const float* q = static_cast<const float*>(Qc);
-            float* o = static_cast<float*>(Q);
-            switch (h->Nv) {
-            case 8: return shift_project_scatter_launch<8>(h, q, o, st);
-            case 12: return shift_project_scatter_launch<12>(h, q, o, st);
-            case 16: return shift_project_scatter_launch<16>(h, q, o, st);
-            case 24: return shift_project_scatter_launch<24>(h, q, o, st);
-            default: return shift_project_scatter_launch<32>(h, q, o, st);
-            }
-        }
+        if (!h->fp64 && v4 && cube_grid(h->Nv))       // shift back, project, scatter: one pass
+            return staged_project_scatter<true>(h, static_cast<const float*>(Qc), static_cast<float*>(Q), st);
         if (const int r = shift_any(h, Qc, 0, const_cast<void*>(Qc), 0, -1.f, st)) return r;
     }
     if (h->fp64) {

@@ -485,7 +485,7 @@ __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
             if (project) {
                 Qs[idx] = qv;
             } else {
-                Qout[idx] = qv;
+                __stcs(Qout + idx, qv);           // streaming: keep L2 for the scratch
             }
             if (need_m) {
                 const double cx = g.c0[x], dq = double(qv);
@@ -518,7 +518,7 @@ __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
                 const double c2 = cx * cx + cy * cy + cz * cz;
                 const double qc = double(Qs[idx]) - (lam[0] + lam[1] * cx + lam[2] * cy
                                                      + lam[3] * cz + lam[4] * c2);
-                Qout[idx] = T(qc);
+                __stcs(Qout + idx, T(qc));
                 m2[0] += qc;
                 m2[1] += cx * qc;
                 m2[2] += cy * qc;
@@ -1070,7 +1070,7 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
                 const double c2 = cx * cx + cy * cy + cz * cz;
                 const double qc = double(Qs[idx]) - (lam[0] + lam[1] * cx + lam[2] * cy
                                                      + lam[3] * cz + lam[4] * c2);
-                Qout[idx] = float(qc);
+                __stcs(Qout + idx, float(qc));   // streaming: keep L2 for the scratch
                 m2[0] += qc;
                 m2[1] += cx * qc;
                 m2[2] += cy * qc;
