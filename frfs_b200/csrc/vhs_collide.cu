@@ -578,7 +578,7 @@ struct QLayoutP2 {
         b += size_t(p2::NH) * p2::N * p2::FS * sizeof(cpx<float>);        // Fh
         b += size_t(M) * 3 * p2::N * sizeof(cpx<float>);                  // phase
         b += size_t(M) * p2::N * sizeof(float4);                          // (Ez.x, Ez.x, Ez.y, Ez.y)
-        b += 10 * (p2::NT / 32) * sizeof(double) + 16;
+        b += 10 * 10 * sizeof(double) + 16;                                // up to 10 warps
         return b;
     }
     // global scratch per CTA: Gh as two float planes [kz][kx <= N/2][ky]
@@ -666,7 +666,15 @@ __device__ __forceinline__ void p2_pass1_spectrum(int tr, const float4* ez, floa
 // barrier; two CTA barriers per transform remain (z stored, y stored).
 // wfree: that mbarrier (NT arrivals per phase), wpar: this thread's phase
 // parity, counter: the work counter, whose bit 62 a timed-out wait sets.
-template <bool SPLIT>
+// BAL (with SPLIT, 320 threads): in the transform loop warps 0-7 carry the
+// pencil pairs 0..255 on f32x2 arithmetic and warps 8-9 the remaining 32
+// pairs as 64 single pencils on scalar arithmetic (thread 256 + 2e + s:
+// pencil s of pair 256 + e).  With 9 pair-warps one SM sub-partition runs
+// three of them and the others two, so its FP32 pipe bounds the kernel at
+// 3/4 of the SM's; here the sub-partitions carry 5, 5, 4 and 4 pipe units
+// of work (a pair warp 2, a scalar warp 1): a bound of 9/10.  The other
+// stages run on threads 0..287 as without BAL.
+template <bool SPLIT, bool BAL = false>
 __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict__ f,
                                float* __restrict__ Qout, double* mom, int flags,
                                unsigned char* smem, unsigned char* scratch, uint32_t tmem,
@@ -687,22 +695,38 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
     float* Ghi = Ghr + N * NH * N;
 
     // lane tables: z-pass pencil pair, y-pass pair (natural), x-pass pair
-    const int kxA = p2tab::zpen[tid][0], kyA = p2tab::zpen[tid][1];
-    const int kxB = p2tab::zpen[tid][2], kyB = p2tab::zpen[tid][3];
+    // (threads beyond the 288 pairs -- BAL -- read the last entry and take
+    // no part in the stages that use them)
+    const int te = tid < NT ? tid : NT - 1;
+    const bool pt = tid < NT;                              // a pair thread outside the loop
+    const int kxA = p2tab::zpen[te][0], kyA = p2tab::zpen[te][1];
+    const int kxB = p2tab::zpen[te][2], kyB = p2tab::zpen[te][3];
     const bool single = tid == p2tab::SINGLE_AT || tid == p2tab::SINGLE_AT + 1;
     const bool single_warp = (tid >> 5) == p2tab::SINGLE_AT / 32;
     static_assert(p2tab::SINGLE_AT % 32 < 31, "self-conjugate pairs in one warp");
     const int offA = kxA * PS + kyA * RS, offB = kxB * PS + kyB * RS;
     const cpx<float>* fa = Fh + (kxA * N + kyA) * FS;
     const cpx<float>* fb = Fh + (kxB < NH ? kxB * N + kyB : 0) * FS;
-    const int ybase = (tid / NP2) * PS + 2 * (tid % NP2);      // + j*RS
-    const int xbase = p2tab::xpen[tid][0] * RS + 2 * p2tab::xpen[tid][1];   // + i*PS
+    const int ybase = (te / NP2) * PS + 2 * (te % NP2);        // + j*RS
+    const int xbase = p2tab::xpen[te][0] * RS + 2 * p2tab::xpen[te][1];     // + i*PS
+    // BAL: the transform loop's single-pencil threads
+    static_assert(!BAL || SPLIT, "balanced split needs the split barrier");
+    static_assert(p2tab::SINGLE_AT + 1 < 256, "self-conjugate pairs among the pair threads");
+    const bool sc = BAL && tid >= 256;                      // single-pencil thread
+    const int es = sc ? 256 + ((tid - 256) >> 1) : 0, ss = sc ? ((tid - 256) & 1) : 0;
+    const int s_kx = ss ? p2tab::zpen[es][2] : p2tab::zpen[es][0];
+    const int s_ky = ss ? p2tab::zpen[es][3] : p2tab::zpen[es][1];
+    const int s_off = s_kx * PS + s_ky * RS;
+    const cpx<float>* s_fa = Fh + (p2tab::zpen[es][0] * N + p2tab::zpen[es][1]) * FS;
+    const int s_ybase = (es / NP2) * PS + 2 * (es % NP2) + ss;
+    const int s_xbase = p2tab::xpen[es][0] * RS + 2 * p2tab::xpen[es][1] + ss;
+    const bool lp = !BAL || tid < 256;                      // a pair thread in the loop
     const float inv_n = 1.f / float(N * N * N);
     const int warp = tid >> 5;
     const uint32_t ts = tmem + (uint32_t(32 * (warp & 3)) << 16) + uint32_t(2 * N * (warp >> 2));
 
     // ---- Fh = FFT(f) / n (kx <= N/2) ----
-    {
+    if (pt) {
         const int y = tid / NP2, z = 2 * (tid % NP2);      // x-pass, real input
         float2 vr[N], vi[N];
 #pragma unroll
@@ -751,7 +775,7 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
     const float* gw = static_cast<const float*>(g.gw);
 
     for (int p = 0; p < Nrho; ++p) {
-        for (int e = tid; e < M * 3 * N; e += NT) {
+        for (int e = tid; e < M * 3 * N; e += int(blockDim.x)) {
             const cpx<float> v = phase[size_t(p) * M * 3 * N + e];
             ph[e] = v;
             const int q = e / (3 * N), r = e - q * 3 * N;
@@ -785,25 +809,71 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
                     st2(Wi + offB + z, f2(vi[z].y, vi[z + 1].y));
                 }
             };
-            {
+            // the same for one pencil (BAL single-pencil threads): pencil B of
+            // a pair is the conjugate partner, F_B(kz) = conj(F_A(-kz))
+            auto zpass_s = [&](int qt, cpx<float> (&v)[N]) {
+                const int q = qt / ntr, tr = qt % ntr;
+                float a, b, c;
+                p2_coef(ph + q * 3 * N, s_kx, s_ky, tr, a, b, c);
+                const float4* ez = ezz + q * N;
+#pragma unroll
+                for (int kz = 0; kz < N; ++kz) {
+                    const float4 e = ez[kz];
+                    const float m = fmaf(a, e.x, (kz == N / 2 ? c : b) * e.z);
+                    const cpx<float> F = ss ? conjc(s_fa[(N - kz) % N]) : s_fa[kz];
+                    v[kz] = tr == 0 ? cpx<float>{m * F.x, m * F.y} : cpx<float>{-m * F.y, m * F.x};
+                }
+                dft<N, +1>(v);
+            };
+            auto zstore_s = [&](const cpx<float> (&v)[N]) {
+#pragma unroll
+                for (int z = 0; z < N; ++z) {
+                    Wr[s_off + z] = v[z].x;
+                    Wi[s_off + z] = v[z].y;
+                }
+            };
+            // every thread's x-pass loads done: W is free (bounded wait; on
+            // expiry bit 62 of the work counter ends the launch)
+            auto wait_free = [&]() {
+                uint32_t spins = 0;
+                while (!tc::mbar_try(wfree, wpar)) {
+                    if (++spins == (1u << 22)) {
+                        atomicOr(counter, 1ull << 62);
+                        break;
+                    }
+                }
+                wpar ^= 1u;
+            };
+            if (lp) {
                 float2 vr[N], vi[N];
                 zpass(0, vr, vi);
                 zstore(vr, vi);
+            } else {
+                cpx<float> v[N];
+                zpass_s(0, v);
+                zstore_s(v);
             }
             for (int qt = 0; qt < nq; ++qt) {
                 const int tr = qt % ntr;
                 __syncthreads();                            // z-pass of qt stored
-                {                                           // pass 2: inverse along y
+                if (lp) {                                   // pass 2: inverse along y
                     float2 vr[N], vi[N];
 #pragma unroll
                     for (int j = 0; j < N; ++j) { vr[j] = ld2(Wr + ybase + j * RS); vi[j] = ld2(Wi + ybase + j * RS); }
                     dft_p2<N, +1>(vr, vi);
 #pragma unroll
                     for (int j = 0; j < N; ++j) { st2(Wr + ybase + j * RS, vr[j]); st2(Wi + ybase + j * RS, vi[j]); }
+                } else {
+                    cpx<float> v[N];
+#pragma unroll
+                    for (int j = 0; j < N; ++j) v[j] = {Wr[s_ybase + j * RS], Wi[s_ybase + j * RS]};
+                    dft<N, +1>(v);
+#pragma unroll
+                    for (int j = 0; j < N; ++j) { Wr[s_ybase + j * RS] = v[j].x; Wi[s_ybase + j * RS] = v[j].y; }
                 }
                 __syncthreads();                            // y-pass stored
                 const bool more = qt + 1 < nq;
-                {                                           // pass 3: inverse along x, S_p += Re(w^2)
+                if (lp) {                                   // pass 3: inverse along x, S_p += Re(w^2)
                     float2 vr[N], vi[N];
 #pragma unroll
                     for (int i = 0; i < N; ++i) { vr[i] = ld2(Wr + i * PS + xbase); vi[i] = ld2(Wi + i * PS + xbase); }
@@ -832,21 +902,46 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
                         }
                         tc::tmem_st16(ts + 16 * c, r);
                     }
+                } else {                                    // one pencil: 24 S_p values, 2 x 16 columns
+                    cpx<float> v[N];
+#pragma unroll
+                    for (int i = 0; i < N; ++i) v[i] = {Wr[i * PS + s_xbase], Wi[i * PS + s_xbase]};
+                    if (more) tc::mbar_arrive(wfree);
+                    dft<N, +1>(v);
+                    tc::tmem_wait_st();
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        uint32_t r[16];
+                        if (qt > 0) {
+                            tc::tmem_ld16_issue(ts + 16 * c, r);
+                            tc::tmem_wait();
+                        } else {
+#pragma unroll
+                            for (int k = 0; k < 16; ++k) r[k] = 0u;
+                        }
+#pragma unroll
+                        for (int k = 0; k < 16; ++k) {
+                            const int x = 16 * c + k;
+                            if (x < N) {
+                                const float d = tr == 0 ? fmaf(v[x].y, -1.f, v[x].x) : fmaf(v[x].x, -1.f, v[x].y);
+                                r[k] = __float_as_uint(fmaf(v[x].x + v[x].y, d, __uint_as_float(r[k])));
+                            }
+                        }
+                        tc::tmem_st16(ts + 16 * c, r);
+                    }
                 }
                 if (more) {                                 // pass 1 of the next transform
-                    float2 vr[N], vi[N];
-                    zpass(qt + 1, vr, vi);
-                    // every thread's x-pass loads done: W is free (bounded wait;
-                    // on expiry bit 62 of the work counter ends the launch)
-                    uint32_t spins = 0;
-                    while (!tc::mbar_try(wfree, wpar)) {
-                        if (++spins == (1u << 22)) {
-                            atomicOr(counter, 1ull << 62);
-                            break;
-                        }
+                    if (lp) {
+                        float2 vr[N], vi[N];
+                        zpass(qt + 1, vr, vi);
+                        wait_free();
+                        zstore(vr, vi);
+                    } else {
+                        cpx<float> v[N];
+                        zpass_s(qt + 1, v);
+                        wait_free();
+                        zstore_s(v);
                     }
-                    wpar ^= 1u;
-                    zstore(vr, vi);
                 }
             }
             __syncthreads();                                // last x-pass loads done
@@ -921,7 +1016,7 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
         }
 
         // ---- Gh += gw_p * FFT(S_p) (kx <= N/2) ----
-        {
+        if (lp) {
             float2 vr[N], vi[N];                            // x-pass, real input
             tc::tmem_wait_st();
 #pragma unroll
@@ -938,6 +1033,21 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
             dft_p2<N, -1>(vr, vi);
 #pragma unroll
             for (int kx = 0; kx < NH; ++kx) { st2(Wr + kx * PS + xbase, vr[kx]); st2(Wi + kx * PS + xbase, vi[kx]); }
+        } else {                                            // BAL single pencil
+            cpx<float> v[N];
+            tc::tmem_wait_st();
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                uint32_t r[16];
+                tc::tmem_ld16_issue(ts + 16 * c, r);
+                tc::tmem_wait();
+#pragma unroll
+                for (int k = 0; k < 16; ++k)
+                    if (16 * c + k < N) v[16 * c + k] = {__uint_as_float(r[k]), 0.f};
+            }
+            dft<N, -1>(v);
+#pragma unroll
+            for (int kx = 0; kx < NH; ++kx) { Wr[kx * PS + s_xbase] = v[kx].x; Wi[kx * PS + s_xbase] = v[kx].y; }
         }
         __syncthreads();
         if (tid < NH * NP2) {                               // y-pass
@@ -979,7 +1089,7 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
 
     // ---- QG + i*fC = IFFT(Gh + i*bb2*Fh) ----
     const float* bb2 = static_cast<const float*>(g.bb2);
-    {
+    if (pt) {
         auto spec = [&](int kx, int ky, int kz) -> cpx<float> {
             const bool direct = kx < NH;
             const int pkx = direct ? kx : N - kx;
@@ -1009,7 +1119,7 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
         }
     }
     __syncthreads();
-    {
+    if (pt) {
         float2 vr[N], vi[N];
 #pragma unroll
         for (int j = 0; j < N; ++j) { vr[j] = ld2(Wr + ybase + j * RS); vi[j] = ld2(Wi + ybase + j * RS); }
@@ -1023,7 +1133,7 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
     const bool need_m = project || mom;
     float* Qs = reinterpret_cast<float*>(Fh);          // Fh is free from here on
     double m[5] = {0, 0, 0, 0, 0};
-    {
+    if (pt) {
         const int y = tid / NP2, z = 2 * (tid % NP2);
         float2 vr[N], vi[N];
 #pragma unroll
@@ -1061,7 +1171,7 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
             for (int j = 0; j < 5; ++j) s += g.ginv[i * 5 + j] * m[j];
             lam[i] = s;
         }
-        for (int pid = tid; pid < N * N; pid += NT) {
+        for (int pid = tid; pid < N * N; pid += int(blockDim.x)) {
             const int y = pid / N, z = pid % N;
             const double cy = g.c0[y], cz = g.c0[z];
             for (int x = 0; x < N; ++x) {
@@ -1104,16 +1214,16 @@ template <typename T, int N, int NT, bool WG, bool SG, int GR = 0, bool SL = fal
 struct Variant {
     using L = QLayout<T, N, NT, WG, SG, SL>;
     static constexpr int n = N;
-    static constexpr bool wg = WG, sg = SG, sl = SL, pk = false, split = false;
+    static constexpr bool wg = WG, sg = SG, sl = SL, pk = false, split = false, bal = false;
     static constexpr int gr = GR;
 };
 
 // packed Nv = 24 FP32 variant (288 threads); SPLIT: split work-cube barrier
-template <bool SPLIT = false>
+template <bool SPLIT = false, bool BAL = false>
 struct VariantP2 {
     using L = QLayoutP2;
     static constexpr int n = p2::N;
-    static constexpr bool wg = false, sg = false, sl = false, pk = true, split = SPLIT;
+    static constexpr bool wg = false, sg = false, sl = false, pk = true, split = SPLIT, bal = BAL;
     static constexpr int gr = 0;
 };
 
@@ -1173,7 +1283,7 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
         double* mom = bt.moments ? bt.moments + dof * 10 : nullptr;
         if (g.Nv == V0::n) {
             if constexpr (V0::pk)
-                collide_one_p2<V0::split>(g, f, Q, mom, a.flags, smem, scratch, tmem, &s_wfree, wpar,
+                collide_one_p2<V0::split, V0::bal>(g, f, Q, mom, a.flags, smem, scratch, tmem, &s_wfree, wpar,
                                           a.counter);
             else
                 collide_one<T, V0::n, NT, V0::wg, V0::sg, V0::gr, V0::sl>(
@@ -1181,7 +1291,7 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
         } else if constexpr (V1::n > 0) {
             if (g.Nv == V1::n) {
                 if constexpr (V1::pk)
-                    collide_one_p2<V1::split>(g, f, Q, mom, a.flags, smem, scratch, tmem, &s_wfree,
+                    collide_one_p2<V1::split, V1::bal>(g, f, Q, mom, a.flags, smem, scratch, tmem, &s_wfree,
                                               wpar, a.counter);
                 else
                     collide_one<T, V1::n, NT, V1::wg, V1::sg, V1::gr, V1::sl>(
@@ -1202,7 +1312,7 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
 
 struct NoVariant {
     static constexpr int n = 0;
-    static constexpr bool wg = false, sg = false, sl = false, pk = false, split = false;
+    static constexpr bool wg = false, sg = false, sl = false, pk = false, split = false, bal = false;
     static constexpr int gr = 0;
     struct L {
         static constexpr int WS = 0;
@@ -1286,6 +1396,9 @@ static const Entry kEntries[] = {
     // the same with the split work-cube barrier
     {0, 24, 0, 288, &launch<float, 288, VariantP2<true>, NoVariant>,
      &entry_per_cta<float, 288, VariantP2<true>, NoVariant>},
+    // split barrier, 8 pair-warps + 2 single-pencil warps in the transform loop
+    {0, 24, 0, 320, &launch<float, 320, VariantP2<true, true>, NoVariant>,
+     &entry_per_cta<float, 320, VariantP2<true, true>, NoVariant>},
 };
 static constexpr int kNumEntries = int(sizeof(kEntries) / sizeof(kEntries[0]));
 
