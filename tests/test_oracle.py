@@ -162,3 +162,19 @@ def test_fr_oracle_velocity_restriction_and_wall_sums():
     L_full = orc.rhs(u)
     L_sub = orc.restrict(vsel).rhs(u[:, :, vsel], bc=bc_state)
     assert np.allclose(L_sub, L_full[:, :, vsel], rtol=1e-13, atol=1e-14 * np.abs(L_full).max())
+
+
+@pytest.mark.parametrize('tag', ['nv16', 'nv24'])
+def test_oracle_q_equals_reference_kernels(tag):
+    """The oracle's Q against the reference's own vhs-gll CUDA kernels and
+    cuFFT (frfs/solvers/dgfs/kernels/scattering/vhs-gll.mako rendered,
+    driven in the order of frfs/solvers/dgfs/scattering.py:227-286; golden
+    vectors written by tests/golden/make_reference_q.py on a GPU)."""
+    from oracle.ref_vhs.build import GRIDS, grid_tables
+    d = np.load(os.path.join(GOLD, f'reference_q_{tag}.npz'))
+    g = GRIDS[tag]
+    assert int(d['Nv']) == g['Nv'] and int(d['M']) == g['M'] and int(d['Nrho']) == g['Nrho']
+    vm, _, _ = grid_tables(g)
+    orc = VHSOracle(vm, g['omega'], 4.17e-10, 273.0)
+    Qo = np.stack([orc.Q(f) for f in d['f']])
+    assert rel_l2(Qo, d['Q']) < 1e-12

@@ -195,3 +195,29 @@ def test_two_grids_one_launch_equals_separate(cuda):
             err = float((qa[i].double() - qb[i].double()).norm() / qb[i].double().norm())
             assert err < 1e-6, (t, i, err)
     grids[0].struct.tile = 0
+
+
+@pytest.mark.parametrize('tag,prec,tol', [('nv16', 'double', 1e-10), ('nv24', 'double', 1e-10),
+                                          ('nv16', 'single', 1e-3), ('nv24', 'single', 1e-3)])
+def test_q_equals_reference_kernels(cuda, tag, prec, tol):
+    """Q of the collision launch against the reference's own vhs-gll CUDA
+    kernels and cuFFT (golden vectors of tests/golden/make_reference_q.py,
+    the reference's host order of frfs/solvers/dgfs/scattering.py:227-286;
+    no conservation projection, as there).  FP64 with the exact-Nyquist
+    option: rounding only; FP32: the collision tolerance."""
+    import os
+    from oracle.ref_vhs.build import GRIDS
+    g = GRIDS[tag]
+    d = np.load(os.path.join(os.path.dirname(__file__), 'golden', f'reference_q_{tag}.npz'))
+    cfg = vhs_cfg(g['Nv'], g['Nrho'], g['M'], g['dev'], omega=g['omega'], precision=prec)
+    be = CUDABackend(cfg)
+    vm = DGFSVelocityMesh(be, cfg)
+    sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
+    dt = torch.float64 if prec == 'double' else torch.float32
+    fin = torch.from_numpy(d['f']).to(device=be.device, dtype=dt)
+    q = torch.empty_like(fin)
+    sm.collide(fin, q, project=False, exact=(prec == 'double'))
+    torch.cuda.synchronize()
+    err = rel_l2(q.double().cpu().numpy(), d['Q'])
+    print(f'{tag} {prec}: {err:.2e}')
+    assert err < tol
