@@ -221,3 +221,34 @@ def test_q_equals_reference_kernels(cuda, tag, prec, tol):
     err = rel_l2(q.double().cpu().numpy(), d['Q'])
     print(f'{tag} {prec}: {err:.2e}')
     assert err < tol
+
+
+def test_q_equals_reference_kernels_live(cuda):
+    """The collision launch and the reference's own vhs-gll kernels (built in
+    oracle/_ref by python -m oracle.ref_vhs.build; skipped where they were
+    not built) on the same fresh seeded distributions on the same GPU."""
+    import ctypes as C
+    import json
+    import os
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    so = os.path.join(root, 'oracle', '_ref', 'libref_vhs_nv24.so')
+    if not os.path.exists(so):
+        pytest.skip('reference kernels not built (oracle/_ref)')
+    with open(os.path.join(root, 'oracle', '_ref', 'ref_vhs_nv24.json')) as fh:
+        g = json.load(fh)
+    cfg = vhs_cfg(g['Nv'], g['Nrho'], g['M'], g['dev'], omega=g['omega'], precision='double')
+    be = CUDABackend(cfg)
+    vm = DGFSVelocityMesh(be, cfg)
+    sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
+    rng = np.random.default_rng(31337)
+    F = np.ascontiguousarray(np.stack([mixed_maxwellians(vm.cv(), rng) for _ in range(3)]))
+    Qr = np.zeros_like(F)
+    lib = C.CDLL(so)
+    lib.ref_vhs_q.restype = C.c_int
+    lib.ref_vhs_q.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    assert lib.ref_vhs_q(g['Nv'], g['Nrho'], g['M'], 3, F.ctypes.data, Qr.ctypes.data) == 0
+    fin = torch.from_numpy(F).to(be.device)
+    q = torch.empty_like(fin)
+    sm.collide(fin, q, project=False, exact=True)
+    torch.cuda.synchronize()
+    assert rel_l2(q.cpu().numpy(), Qr) < 1e-10
