@@ -17,8 +17,11 @@ are pinned against fixtures produced by the reference's own Python modules
 (``tests/golden/make_golden.py``); the VHS precompute tables are pinned
 against the reference's own numpy formulation of them (the docstring block
 in ``frfs/solvers/dgfs/scattering.py:94-126``, executed by the same
-script).  The collision operator itself cannot be run from the reference
-here (it needs PyCUDA, Mako and cuFFT), so Q is pinned by known-answer
-tests instead: Q(Maxwellian) ~ 0, conservation of mass/momentum/energy,
-and the Bobylev-Krook-Wu analytic solution for Maxwell molecules.
+script).  The collision operator is pinned against the reference's own
+CUDA kernels: ``oracle/ref_vhs`` renders its vhs-gll template and drives
+the kernels with cuFFT in its host order (test infrastructure, built into
+``oracle/_ref``); the oracle's Q matches the golden vectors they wrote to
+1.8e-14 (16^3) and 5.5e-15 (24^3) relative L2.  Known-answer tests add
+Q(Maxwellian) ~ 0, conservation of mass/momentum/energy and the
+Bobylev-Krook-Wu analytic solution for Maxwell molecules.
 """
