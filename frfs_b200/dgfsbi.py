@@ -18,6 +18,7 @@ in one ``bdgfs_vss_collide`` launch, and ``fs`` is the reference's
 per-point call.
 """
 import ctypes as C
+from fractions import Fraction
 from itertools import product
 from math import gamma as _gamma
 
@@ -164,6 +165,25 @@ class DGFSBiVSSGLLScatteringModel(DGFSBiScatteringModel):
             self._prefactor[pq] = invKn * alpha / (np.sqrt(1. + m[p] / m[q]) * mu**(omega - 0.5)
                                                    * 2.**(1 + alpha) * _gamma(2.5 - omega) * np.pi)
 
+    @staticmethod
+    def one_plus_cos(sz, szpre):
+        """1 + s . t for every direction s of sz [M, 3] and t of szpre
+        [Mpre, 3], rounded as the reference's precompute_bc_pq evaluates it
+        on the GPU (vss-gll.mako:80-82: 1 + s_x t_x + s_y t_y + s_z t_z,
+        contracted into three fused multiply-adds, each rounded once).  Where
+        t = -s the exact value is 0 and the rounded one is noise of order
+        1e-16 that (.)^(alpha - 1) lifts to order 1e-5; rounding it the same
+        way keeps B, and Q, equal to the reference's.  A negative rounded value
+        (the reference's pow then gives NaN) is taken as the exact 0."""
+        def fma(a, b, c):
+            return float(Fraction(a) * Fraction(b) + Fraction(c))
+        sz, szpre = np.asarray(sz, dtype=np.float64), np.asarray(szpre, dtype=np.float64)
+        out = np.empty((sz.shape[0], szpre.shape[0]))
+        for y, s in enumerate(sz.tolist()):
+            for t, u in enumerate(szpre.tolist()):
+                out[y, t] = fma(s[2], u[2], fma(s[1], u[1], fma(s[0], u[0], 1.0)))
+        return np.maximum(out, 0.0)
+
     def kernel_tables(self, p, q):
         """b_pq[r*M+s][l], c_pq[l] (precompute_bc_pq, vss-gll.mako:53-95), FP64."""
         vm = self.vm
@@ -171,7 +191,7 @@ class DGFSBiVSSGLLScatteringModel(DGFSBiScatteringModel):
         m = vm.masses()
         mq = m[q] / (m[p] + m[q])
         sz, szpre = vm.sz(), self._szpre
-        Bst = (1.0 + sz @ szpre.T)**self._eta[pq]               # [M, Mpre]
+        Bst = self.one_plus_cos(sz, szpre)**self._eta[pq]        # [M, Mpre]
         tl = szpre @ _lgrid(vm.Nv())                            # [Mpre, n]
         b = np.empty((vm.Nrho() * vm.M(), vm.vsize()), complex)
         c = np.zeros(vm.vsize(), complex)

@@ -21,7 +21,11 @@ script).  The collision operator is pinned against the reference's own
 CUDA kernels: ``oracle/ref_vhs`` renders its vhs-gll template and drives
 the kernels with cuFFT in its host order (test infrastructure, built into
 ``oracle/_ref``); the oracle's Q matches the golden vectors they wrote to
-1.8e-14 (16^3) and 5.5e-15 (24^3) relative L2.  Known-answer tests add
+1.8e-14 (16^3) and 5.5e-15 (24^3) relative L2.  The gas-mixture
+operator likewise: ``oracle/ref_vss`` renders the vss-gll template; the
+mixture oracle's Q_p matches its golden vectors to 5.4e-15 (two species,
+16^3), with 1 + s.t in B rounded as the kernel evaluates it (three fused
+multiply-adds).  Known-answer tests add
 Q(Maxwellian) ~ 0, conservation of mass/momentum/energy and the
 Bobylev-Krook-Wu analytic solution for Maxwell molecules.
 """

@@ -35,6 +35,9 @@ extern "C" int ref_vhs_q(int Nv, int Nrho, int M, int ndof, const double* f, dou
 {
     if (Nv < 2 || Nrho < 1 || M < 1 || ndof < 0 || !f || !Q) return -1;
     const int vsize = Nv * Nv * Nv;
+    // computeQG stores outside its idx < vsize guard (vhs-gll.mako:205): the
+    // grid must cover vsize exactly
+    if (vsize % 256) return -1;
     const dim3 block(256), grid((vsize + 255) / 256);
     int rc = 0;
     double *lx = nullptr, *ly = nullptr, *lz = nullptr, *aa = nullptr, *bb1 = nullptr, *bb2 = nullptr;

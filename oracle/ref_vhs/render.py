@@ -1,16 +1,35 @@
-"""Render the reference's vhs-gll Mako template (test infrastructure).
+"""Render the reference's collision-kernel Mako templates (test infrastructure).
 
-The template (frfs/solvers/dgfs/kernels/scattering/vhs-gll.mako) uses a
-small part of Mako: a module block ``<%! ... %>``, one-line code blocks
-``<% ... %>``, control lines ``% for ...:`` / ``% endfor`` (and the if
-forms) and ``${expression}`` substitutions rendered with ``str``.  This
-renderer translates exactly those into a Python function, as Mako itself
-does, and runs it with the template arguments the reference passes
-(frfs/solvers/dgfs/scattering.py:154-160).
+The templates (frfs/solvers/dgfs/kernels/scattering/vhs-gll.mako,
+frfs/solvers/dgfsbi/kernels/scattering/vss-gll.mako) use a small part of
+Mako: a module block ``<%! ... %>``, code blocks ``<% ... %>`` (one line or
+several), control lines ``% for ...:`` / ``% endfor`` and the if forms, and
+``${expression}`` substitutions rendered with ``str``.  This renderer
+translates exactly those into a Python function, as Mako itself does, and
+runs it with the template arguments the reference passes
+(frfs/solvers/dgfs/scattering.py:154-160, frfs/solvers/dgfsbi/scattering.py:
+153-163).
 """
-import re
+import textwrap
 
-_EXPR = re.compile(r'\$\{(.*?)\}')
+
+def _subst(line):
+    """Python expression joining the literal text of a line with its
+    ${...} substitutions (braces inside an expression are matched)."""
+    parts, pos = [], 0
+    while True:
+        i = line.find('${', pos)
+        if i < 0:
+            break
+        depth, j = 1, i + 2
+        while depth:
+            depth += {'{': 1, '}': -1}.get(line[j], 0)
+            j += 1
+        parts.append(repr(line[pos:i]))
+        parts.append('str(' + line[i + 2:j - 1] + ')')
+        pos = j
+    parts.append(repr(line[pos:] + '\n'))
+    return ' + '.join(parts)
 
 
 def _compile(src):
@@ -23,15 +42,21 @@ def _compile(src):
     while i < len(lines):
         line = lines[i]
         st = line.strip()
-        if st.startswith('<%!'):                           # module-level block
-            body = []
-            rest = st[3:]
-            while '%>' not in rest:
-                body.append(rest)
+        if st.startswith('<%') and '%>' not in st:
+            # module block, or a code block over several lines
+            module = st.startswith('<%!')
+            body = [st[3:] if module else st[2:]]
+            while True:
                 i += 1
-                rest = lines[i]
-            body.append(rest[:rest.index('%>')])
-            mod.extend(b.strip() for b in body if b.strip())
+                if '%>' in lines[i]:
+                    body.append(lines[i][:lines[i].index('%>')])
+                    break
+                body.append(lines[i])
+            code = textwrap.dedent('\n'.join(body)).strip('\n')
+            if module:
+                mod.extend(c for c in code.split('\n') if c.strip())
+            else:
+                out.extend('    ' * depth + c for c in code.split('\n') if c.strip())
             i += 1
             continue
         if st.startswith('%') and not st.startswith('%%'):  # control line
@@ -46,20 +71,14 @@ def _compile(src):
                 depth += 1
             i += 1
             continue
-        if st.startswith('<%') and st.endswith('%>') and not st.startswith('<%!'):
+        if st.startswith('<%') and st.endswith('%>'):
             out.append('    ' * depth + st[2:-2].strip())   # one-line code block
             i += 1
             continue
         if st.startswith('##'):                            # template comment
             i += 1
             continue
-        parts, pos = [], 0
-        for m in _EXPR.finditer(line):
-            parts.append(repr(line[pos:m.start()]))
-            parts.append('str(' + m.group(1) + ')')
-            pos = m.end()
-        parts.append(repr(line[pos:] + '\n'))
-        out.append('    ' * depth + '__buf.append(' + ' + '.join(parts) + ')')
+        out.append('    ' * depth + '__buf.append(' + _subst(line) + ')')
         i += 1
     out.append("    return ''.join(__buf)")
     return '\n'.join(mod + out)

@@ -20,6 +20,7 @@ step by step, with the reference's operation order:
                                                           (precompute_bc_pq)
 Test infrastructure only.
 """
+from fractions import Fraction
 from itertools import product
 from math import gamma as _gamma
 
@@ -77,6 +78,21 @@ def vss_parameters(vm, pairs):
     return out
 
 
+def one_plus_cos(sz, szpre):
+    """The base of B in precompute_bc_pq (vss-gll.mako:80-82),
+    1 + szx[y] t_x + szy[y] t_y + szz[y] t_z, as the GPU evaluates the
+    expression: three fused multiply-adds (the compiler's default
+    contraction), each rounded once (emulated exactly with rationals).  At
+    t = -s the exact value is 0 and this rounding decides B there."""
+    def fma(a, b, c):
+        return float(Fraction(a) * Fraction(b) + Fraction(c))
+    out = np.empty((sz.shape[0], szpre.shape[0]))
+    for y, s in enumerate(np.asarray(sz, dtype=np.float64).tolist()):
+        for t, u in enumerate(np.asarray(szpre, dtype=np.float64).tolist()):
+            out[y, t] = fma(s[2], u[2], fma(s[1], u[1], fma(s[0], u[0], 1.0)))
+    return out
+
+
 def precompute_bc(vm, szpre, gamma_pq, eta_pq, mq_frac):
     """precompute_bc_pq (vss-gll.mako:53-95): b[r*M+s, l] and c[l], complex."""
     l = lgrid(vm.Nv)
@@ -85,7 +101,7 @@ def precompute_bc(vm, szpre, gamma_pq, eta_pq, mq_frac):
     P = vm.Nrho * vm.M
     b = np.zeros((P, vm.vsize), complex)
     c = np.zeros(vm.vsize, complex)
-    Bst = (1.0 + vm.sz @ szpre.T)**eta_pq                     # [M, Mpre]
+    Bst = one_plus_cos(vm.sz, szpre)**eta_pq                  # [M, Mpre]
     tl = szpre @ l                                            # [Mpre, n]
     for r in range(vm.Nrho):
         fac = np.pi / vm.L * vm.qz[r]

@@ -178,3 +178,24 @@ def test_oracle_q_equals_reference_kernels(tag):
     orc = VHSOracle(vm, g['omega'], 4.17e-10, 273.0)
     Qo = np.stack([orc.Q(f) for f in d['f']])
     assert rel_l2(Qo, d['Q']) < 1e-12
+
+
+def test_oracle_mixture_q_equals_reference_kernels():
+    """The mixture oracle's Q_p = sum_q Q_pq against the reference's own
+    vss-gll CUDA kernels and cuFFT (frfs/solvers/dgfsbi/kernels/scattering/
+    vss-gll.mako rendered, driven in the order of frfs/solvers/dgfsbi/
+    scattering.py:256-330; golden vectors written by
+    tests/golden/make_reference_q.py on a GPU): two species (argon, krypton),
+    every pair VSS with alpha = 1.3, omega = 0.81, Nv = 16."""
+    from oracle.ref_vss.build import GRIDS, grid_tables
+    from oracle.vss import VSSOracle
+    d = np.load(os.path.join(GOLD, 'reference_qbi_bi16.npz'))
+    g = GRIDS['bi16']
+    assert int(d['Nv']) == g['Nv'] and int(d['M']) == g['M'] and int(d['Mpre']) == g['Mpre']
+    vm, szpre, pairs, _ = grid_tables(g)
+    orc = VSSOracle(vm, szpre, pairs)
+    Qo = np.stack([np.stack(orc.Q(list(f))) for f in d['f']])
+    assert rel_l2(Qo, d['Q']) < 1e-12
+    # each species' own Q too (the lighter species' Q is not swamped)
+    for p in range(2):
+        assert rel_l2(Qo[:, p], d['Q'][:, p]) < 1e-12

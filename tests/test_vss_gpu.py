@@ -107,3 +107,65 @@ def test_vss_conservation_projection(cuda, precision, tol):
             en = sum(mp * (np.sum(cv * cv, 0) @ g) for mp, g in zip(m, got))
             assert np.abs(mom).max() < 1e-12 * scale * np.abs(cv).max()
             assert abs(en) < 1e-12 * scale * np.sum(cv * cv, 0).max()
+
+
+def _reference_model(g, prec):
+    return _model(g['Nv'], g['Nrho'], g['M'], g['Mpre'], precision=prec,
+                  masses=tuple(g['molar']), alpha=g['alpha'], omega=g['omega'], dev=g['dev'])
+
+
+def _collide(be, sm, F):
+    """Q of the mixture launch for F [dof][species][Nv^3] (FP64 numpy)."""
+    S = F.shape[1]
+    fs = [torch.tensor(np.ascontiguousarray(F[:, p]), dtype=be.fpdtype, device=be.device)
+          for p in range(S)]
+    Qs = [torch.full_like(f, float('nan')) for f in fs]
+    sm.collide(fs, Qs)
+    torch.cuda.synchronize()
+    return np.stack([Q.double().cpu().numpy() for Q in Qs], axis=1)
+
+
+@pytest.mark.parametrize('prec,tol', [('double', 1e-11), ('single', 2e-4)])
+def test_vss_equals_reference_kernels(cuda, prec, tol):
+    """Q of the mixture launch against the reference's own vss-gll CUDA
+    kernels and cuFFT (golden vectors of tests/golden/make_reference_q.py,
+    the reference's host order of frfs/solvers/dgfsbi/scattering.py:256-330;
+    no conservation projection, as there): FP64 to rounding, FP32 to the
+    mixture operator's FP32 tolerance."""
+    import os
+    from oracle.ref_vss.build import GRIDS
+    g = GRIDS['bi16']
+    d = np.load(os.path.join(os.path.dirname(__file__), 'golden', 'reference_qbi_bi16.npz'))
+    be, sm = _reference_model(g, prec)
+    got = _collide(be, sm, d['f'])
+    for p in range(2):
+        err = rel_l2(got[:, p], d['Q'][:, p])
+        print(f'bi16 {prec} species {p}: {err:.2e}')
+        assert err < tol
+
+
+def test_vss_equals_reference_kernels_live(cuda):
+    """The mixture launch and the reference's own vss-gll kernels (built in
+    oracle/_ref by python -m oracle.ref_vss.build; skipped where they were not
+    built) on the same fresh seeded distributions on the same GPU, FP64."""
+    import json
+    import os
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    so = os.path.join(root, 'oracle', '_ref', 'libref_vss_bi16.so')
+    if not os.path.exists(so):
+        pytest.skip('reference kernels not built (oracle/_ref)')
+    sys.path.insert(0, os.path.join(root, 'tests', 'golden'))
+    from make_reference_q import run_vss
+    from oracle.ref_vss.build import grid_tables
+    with open(os.path.join(root, 'oracle', '_ref', 'ref_vss_bi16.json')) as fh:
+        g = json.load(fh)
+    vm, _, _, par = grid_tables(g)
+    rng = np.random.default_rng(4242)
+    F = np.stack([np.stack(mixture(vm.cv, vm.masses, rng, k=3)) for _ in range(2)])
+    Qr = run_vss(so, g, vm, par, F)
+    be, sm = _reference_model(g, 'double')
+    got = _collide(be, sm, F)
+    err = max(rel_l2(got[:, p], Qr[:, p]) for p in range(2))
+    print(f'live bi16 double: {err:.2e}')
+    assert err < 1e-11
