@@ -890,10 +890,7 @@ def ars_bgk(flush, steps=20):
     kt /= reps
     elems = s.ndof * s.vm.vsize()
     nbytes = elems * 4 * 6                       # 5 reads + 1 write of FP32 rows
-    peak = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)),
-                                       'MEASURED_PEAKS.json')))['hbm_gbs'] \
-        if os.path.exists(os.path.join(os.path.dirname(os.path.abspath(__file__)),
-                                       'MEASURED_PEAKS.json')) else 6650.0
+    peak = hbm_peak_gbs()
     ach = nbytes / (kt * 1e-3) / 1e9
     return {'workload': ('adgfs: 16x8 quads P3 (2048 DOFs), Nv=24^3, BGK (bgk-direct-gll, '
                          'omega 0.81), ARS-222, dt=5e-4, FP32 state / FP64 moments'),
@@ -1499,6 +1496,15 @@ def run_surrogate_call(ndof, reps=2):
     print(json.dumps({'surrogate_call_ndof': ndof, 'ms': ms, 'q_evals_per_s': ndof / ms * 1e3}))
 
 
+def hbm_peak_gbs():
+    """HBM copy bandwidth of MEASURED_PEAKS.json (measured on this pool's
+    B200s), else the pool's earlier measurement, 6650 GB/s."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'MEASURED_PEAKS.json')
+    if os.path.exists(path):
+        return json.load(open(path))['hbm_gbs']
+    return 6650.0
+
+
 def run_fr_only(kind, reps=10):
     """Profiling case: the FR kernels of one SSP-RK2 stage (disu, wall
     update, fused rhs with two combination operands) on the Couette
@@ -1557,8 +1563,7 @@ uz = 0
         out.data_ptr(), 0.5, 2.5e-4, x1.data_ptr(), 2.5e-4, x2.data_ptr(), 0.5, _lb.stream_ptr()))
     E, U, F, nv = s.ele.neles, s.ele.nupts, s.ele.nfpts, s.vm.vsize()
     nbytes = 4 * nv * E * (4 * U + 2 * F)          # u, x1, x2 in + out; own and neighbour faces
-    peak = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)),
-                                       'MEASURED_PEAKS.json')))['hbm_gbs']
+    peak = hbm_peak_gbs()
     res = {'fr_only': kind, 'neles': E, 'nupts': U, 'nfpts': F, 'nv': nv,
            'disu_ms': t_disu, 'bc_update_ms': t_bc, 'rhs_ms': t_rhs,
            'rhs_bytes': nbytes, 'rhs_gbs': nbytes / (t_rhs * 1e-3) / 1e9,
