@@ -25,7 +25,10 @@ the kernels with cuFFT in its host order (test infrastructure, built into
 operator likewise: ``oracle/ref_vss`` renders the vss-gll template; the
 mixture oracle's Q_p matches its golden vectors to 5.4e-15 (two species,
 16^3), with 1 + s.t in B rounded as the kernel evaluates it (three fused
-multiply-adds).  Known-answer tests add
+multiply-adds).  The BGK, ES-BGK and Shakov relaxation steps likewise:
+``oracle/ref_adgfs`` renders the reference's *-direct-gll templates and
+runs its ARS stepper's kernel sequence; the oracle's ARS steps match to
+3.7e-14 of the step's change.  Known-answer tests add
 Q(Maxwellian) ~ 0, conservation of mass/momentum/energy and the
 Bobylev-Krook-Wu analytic solution for Maxwell molecules.
 """

@@ -32,6 +32,22 @@ def _subst(line):
     return ' + '.join(parts)
 
 
+def _open_subst(text):
+    """True when a ${ in text is not closed within it."""
+    pos = 0
+    while True:
+        i = text.find('${', pos)
+        if i < 0:
+            return False
+        depth, j = 1, i + 2
+        while depth and j < len(text):
+            depth += {'{': 1, '}': -1}.get(text[j], 0)
+            j += 1
+        if depth:
+            return True
+        pos = j
+
+
 def _compile(src):
     """Python source of a function render(ctx) -> str for the template."""
     out = ['def __render(__ctx):', '    globals().update(__ctx)', '    __buf = []']
@@ -42,6 +58,11 @@ def _compile(src):
     while i < len(lines):
         line = lines[i]
         st = line.strip()
+        if st.startswith('<%include') and st.endswith('/>'):
+            name = st.split('file=', 1)[1].split('"')[1]
+            out.append('    ' * depth + f'__buf.append(__include({name!r}, __ctx))')
+            i += 1
+            continue
         if st.startswith('<%') and '%>' not in st:
             # module block, or a code block over several lines
             module = st.startswith('<%!')
@@ -78,15 +99,26 @@ def _compile(src):
         if st.startswith('##'):                            # template comment
             i += 1
             continue
+        while _open_subst(line) and i + 1 < len(lines):     # ${...} over several lines
+            i += 1
+            line = line + '\n' + lines[i]
         out.append('    ' * depth + '__buf.append(' + _subst(line) + ')')
         i += 1
     out.append("    return ''.join(__buf)")
     return '\n'.join(mod + out)
 
 
-def render(src, **args):
-    ns = {}
-    exec(compile(_compile(src), '<vhs-gll.mako>', 'exec'), ns)
+def render(src, lookup_dir=None, **args):
+    """Render template text with the given arguments; <%include file="x"/>
+    renders lookup_dir/x.mako with the same arguments."""
+    import os
+
+    def include(name, ctx):
+        with open(os.path.join(lookup_dir, name + '.mako')) as fh:
+            return render(fh.read(), lookup_dir, **{k: v for k, v in ctx.items()
+                                                    if not k.startswith('__')})
+    ns = {'__include': include}
+    exec(compile(_compile(src), '<template>', 'exec'), ns)
     return ns['__render'](dict(args))
 
 

@@ -190,3 +190,36 @@ def test_bdf_order(q, model):
     ref = run(128)
     rate = np.log2(np.linalg.norm(run(16) - ref) / np.linalg.norm(run(32) - ref))
     assert rate > q - 0.3, rate
+
+
+@pytest.mark.parametrize('model', ['bgk', 'esbgk', 'shakov'])
+@pytest.mark.parametrize('scheme', ['adgfs-ars-111', 'adgfs-ars-222', 'adgfs-ars-443'])
+def test_oracle_ars_step_equals_reference_kernels(model, scheme):
+    """One ARS step of the oracle's steppers against the reference's own
+    bgk-, esbgk- and shakov-direct-gll kernels (rendered; the call sequence
+    of frfs/integrators/std/steppers.py:538-585; golden vectors written by
+    tests/golden/make_reference_ars.py on a GPU): 4 of its 32 seeded
+    distributions on a 16^3 grid, a given explicit part L, dt nu ~ 1, FP64."""
+    import os
+    import sys
+    from oracle.bgk import step_ars, step_ars_es, step_ars_sk
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), 'golden'))
+    from make_reference_ars import grid, inputs
+    d = np.load(os.path.join(os.path.dirname(__file__), 'golden', 'reference_ars.npz'))
+    cv, cw = grid()
+    rows = d['rows']
+    f0, L = inputs(cv)                      # the generator's seeded inputs
+    f0, L = f0[rows], L[rows]
+    assert np.allclose(f0.sum(1), d['f0_rows_sum'], rtol=1e-15, atol=0)
+    dt, prefac = float(d['dt']), float(d['prefac'])
+    Lf = lambda f: L
+    if model == 'bgk':
+        got = step_ars(f0, dt, Lf, scheme, prefac, 0.81, cv, cw)
+    elif model == 'esbgk':
+        got = step_ars_es(f0, dt, Lf, scheme, prefac, 0.81, 2.0 / 3.0, cv, cw)
+    else:
+        got = step_ars_sk(f0, dt, Lf, scheme, prefac, 0.81, 2.0 / 3.0, cv, cw)
+    want = d[f'{model}:{scheme}']
+    # relative to the change the step makes
+    err = np.linalg.norm(got - want) / np.linalg.norm(want - f0)
+    assert err < 1e-12, err

@@ -333,3 +333,59 @@ def test_bdf_reference_methods_equal_fused_step(cuda):
     torch.cuda.synchronize()
     assert torch.equal(s.eles_scal_upts_inb_moms[5], Uref)
     assert torch.equal(s.eles_scal_upts_inb_full[5], ref)
+
+
+@pytest.mark.parametrize('model', ['bgk', 'esbgk', 'shakov'])
+@pytest.mark.parametrize('scheme', ['adgfs-ars-111', 'adgfs-ars-222', 'adgfs-ars-443'])
+def test_ars_stages_equal_reference_kernels(cuda, model, scheme):
+    """bdgfs_ars_stage, driven stage by stage as the reference's ARS stepper
+    (frfs/integrators/std/steppers.py:538-585) with a given explicit part
+    L, against the reference's own bgk-, esbgk- and shakov-direct-gll
+    kernels (golden vectors of tests/golden/make_reference_ars.py): FP64,
+    relative to the change the step makes."""
+    import ctypes as C
+    import os
+    import sys
+    from frfs_b200 import _lib
+    from oracle.bgk import ARS
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), 'golden'))
+    from make_reference_ars import grid, inputs
+    d = np.load(os.path.join(os.path.dirname(__file__), 'golden', 'reference_ars.npz'))
+    cv, cw = grid()
+    rows = d['rows']
+    f0, L = inputs(cv)
+    f0, L = f0[rows], L[rows]
+    Nv, n = 16, f0.shape[0]
+    dev = torch.device('cuda')
+    nalph = {'bgk': 5, 'esbgk': 11, 'shakov': 14}[model]
+    c0 = torch.as_tensor(np.linspace(-5 + 5 / Nv, 5 - 5 / Nv, Nv), dtype=torch.float64, device=dev)
+    F = [torch.as_tensor(f0, device=dev)]
+    Ld = torch.as_tensor(L, device=dev)
+    U = [torch.zeros(n, nalph, dtype=torch.float64, device=dev) for _ in range(5)]
+    LU = [torch.zeros(n, nalph, dtype=torch.float64, device=dev) for _ in range(4)]
+    _A, A = ARS[scheme]
+    s = len(_A) - 1
+    for i in range(s):
+        ar = i + 1
+        F.append(torch.empty_like(F[0]))
+        a = _lib.ArsArgs(ndof=n, Nv=Nv, fp64=1, c0=c0.data_ptr(), cw=cw, prefac=float(d['prefac']),
+                         omega=0.81, dt=float(d['dt']), stage=ar,
+                         flags=(1 if ar == 1 else 0) | 2 | 4 | 8,
+                         model={'bgk': 0, 'esbgk': 1, 'shakov': 2}[model],
+                         Pr=1.0 if model == 'bgk' else 2.0 / 3.0)
+        for j in range(ar):
+            a.ae[j] = _A[ar][j]
+            a.ai[j] = A[ar][j + 1]
+            a.f[j] = F[j].data_ptr()
+            a.L[j] = Ld.data_ptr()
+            a.LU[j] = LU[j].data_ptr()
+        for j in range(ar + 1):
+            a.U[j] = U[j].data_ptr()
+        a.fout = F[ar].data_ptr()
+        _lib.check(_lib.lib().bdgfs_ars_stage(C.byref(a), _lib.stream_ptr()), 'bdgfs_ars_stage')
+    torch.cuda.synchronize()
+    got = F[s].cpu().numpy()
+    want = d[f'{model}:{scheme}']
+    err = np.linalg.norm(got - want) / np.linalg.norm(want - f0)
+    print(f'{model} {scheme}: {err:.1e}')
+    assert err < 1e-12
