@@ -27,8 +27,8 @@ mixture oracle's Q_p matches its golden vectors to 5.4e-15 (two species,
 16^3), with 1 + s.t in B rounded as the kernel evaluates it (three fused
 multiply-adds).  The BGK, ES-BGK and Shakov relaxation steps likewise:
 ``oracle/ref_adgfs`` renders the reference's *-direct-gll templates and
-runs its ARS stepper's kernel sequence; the oracle's ARS steps match to
-3.7e-14 of the step's change.  Known-answer tests add
+runs its ARS and BDF steppers' kernel sequences; the oracle's ARS steps
+and BDF updates match to 4.7e-14 of the step's change.  Known-answer tests add
 Q(Maxwellian) ~ 0, conservation of mass/momentum/energy and the
 Bobylev-Krook-Wu analytic solution for Maxwell molecules.
 """

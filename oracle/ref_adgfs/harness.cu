@@ -151,3 +151,101 @@ extern "C" int ref_ars_step(int s, const double* At, const double* Ai, double dt
     cudaFree(dc);
     return rc;
 }
+
+// One update of the reference's IMEX-BDF stepper (BDF2AstdStepper.step,
+// frfs/integrators/std/steppers.py:700-760; BDF3 likewise) for q = 2 or 3
+// histories, oldest first: Us, LUs = moments of fs, Ls;
+// updateMom{q}_BDF(prefac, lda, dt, a_0, U_0, g_0, LU_0, ..., a_q, U, b);
+// constructMaxwellian(U); updateDistribution{q}_BDF(prefac, nupts, ldim,
+// nvars, neles, dt, a_0, f_0, g_0, L_0, ..., b, M, a_q, U, f).  a[0..q],
+// g[0..q-1] as passed to the kernels (g = -G of the stepper's tables).
+// fs, Ls: [q][32][nv]; fout: [32][nv]; Uout: [32][nalph].
+extern "C" int ref_bdf_update(int q, const double* a, const double* g, double b, double dt, double prefac,
+                              int nalph, int nv, const double* mat, const double* c, const double* fs,
+                              const double* Ls, double* fout, double* Uout)
+{
+    if ((q != 2 && q != 3) || nalph != NALPH || nv < 1 || !a || !g || !mat || !c || !fs || !Ls || !fout ||
+        !Uout)
+        return -1;
+    const int nupts = 1, neles = kElems, nvars = nv, ldim = kElems * nv, lda = nupts * neles;
+    const size_t nf = size_t(kElems) * nv, nu = size_t(kElems) * NALPH;
+    const dim3 block(256), gridf(unsigned((nf + 255) / 256)), gridu(unsigned((lda + 255) / 256));
+    std::vector<double> h(nf), hu(nu);
+    double *dF[3] = {}, *dL[3] = {}, *dU[3] = {}, *dLU[3] = {}, *dUn = nullptr, *dUt = nullptr, *dM = nullptr,
+           *dout = nullptr, *dc = nullptr;
+    int rc = 0;
+    auto moment = [&](const double* dsrc, double* ddst) -> int {
+        int r = ok(cudaMemcpy(h.data(), dsrc, nf * sizeof(double), cudaMemcpyDeviceToHost));
+        if (r) return r;
+        for (int e = 0; e < kElems; ++e)
+            for (int k = 0; k < NALPH; ++k) {
+                double acc = 0.0;
+                for (int v = 0; v < nv; ++v) acc += h[size_t(v) * kElems + e] * mat[size_t(k) * nv + v];
+                hu[size_t(e) * NALPH + k] = acc;
+            }
+        return ok(cudaMemcpy(ddst, hu.data(), nu * sizeof(double), cudaMemcpyHostToDevice));
+    };
+    auto upload = [&](const double* src, double* ddst) -> int {
+        for (int e = 0; e < kElems; ++e)
+            for (int v = 0; v < nv; ++v) h[size_t(v) * kElems + e] = src[size_t(e) * nv + v];
+        return ok(cudaMemcpy(ddst, h.data(), nf * sizeof(double), cudaMemcpyHostToDevice));
+    };
+    do {
+        for (int i = 0; i < q && !rc; ++i) {
+            rc = ok(cudaMalloc(&dF[i], nf * sizeof(double)));
+            if (!rc) rc = ok(cudaMalloc(&dL[i], nf * sizeof(double)));
+            if (!rc) rc = ok(cudaMalloc(&dU[i], nu * sizeof(double)));
+            if (!rc) rc = ok(cudaMalloc(&dLU[i], nu * sizeof(double)));
+        }
+        if (rc) break;
+        if ((rc = ok(cudaMalloc(&dUn, nu * sizeof(double))))) break;
+        if ((rc = ok(cudaMalloc(&dUt, nu * sizeof(double))))) break;
+        if ((rc = ok(cudaMalloc(&dM, nf * sizeof(double))))) break;
+        if ((rc = ok(cudaMalloc(&dout, nf * sizeof(double))))) break;
+        if ((rc = ok(cudaMalloc(&dc, 3 * size_t(nv) * sizeof(double))))) break;
+        if ((rc = ok(cudaMemcpy(dc, c, 3 * size_t(nv) * sizeof(double), cudaMemcpyHostToDevice)))) break;
+        for (int i = 0; i < q && !rc; ++i) {
+            if ((rc = upload(fs + size_t(i) * nf, dF[i]))) break;
+            if ((rc = upload(Ls + size_t(i) * nf, dL[i]))) break;
+            if ((rc = moment(dF[i], dU[i]))) break;
+            rc = moment(dL[i], dLU[i]);
+        }
+        if (rc) break;
+        if (q == 2)
+            updateMom2_BDF<<<gridu, block>>>(prefac, lda, dt, a[0], dU[0], g[0], dLU[0], a[1], dU[1], g[1], dLU[1],
+                                             a[2], dUn, b);
+        else
+            updateMom3_BDF<<<gridu, block>>>(prefac, lda, dt, a[0], dU[0], g[0], dLU[0], a[1], dU[1], g[1], dLU[1],
+                                             a[2], dU[2], g[2], dLU[2], a[3], dUn, b);
+#ifdef HAS_MOMENT_NORM
+        momentNorm<<<gridu, block>>>(lda, dUn, dUt);
+        cmaxwellian<<<gridf, block>>>(nupts, ldim, nvars, neles, dc, dc + nv, dc + 2 * nv, dM, dUt);
+#else
+        cmaxwellian<<<gridf, block>>>(nupts, ldim, nvars, neles, dc, dc + nv, dc + 2 * nv, dM, dUn);
+#endif
+        if (q == 2)
+            updateDistribution2_BDF<<<gridf, block>>>(prefac, nupts, ldim, nvars, neles, dt, a[0], dF[0], g[0],
+                                                      dL[0], a[1], dF[1], g[1], dL[1], b, dM, a[2], dUn, dout);
+        else
+            updateDistribution3_BDF<<<gridf, block>>>(prefac, nupts, ldim, nvars, neles, dt, a[0], dF[0], g[0],
+                                                      dL[0], a[1], dF[1], g[1], dL[1], a[2], dF[2], g[2], dL[2],
+                                                      b, dM, a[3], dUn, dout);
+        if ((rc = ok(cudaGetLastError()))) break;
+        if ((rc = ok(cudaMemcpy(h.data(), dout, nf * sizeof(double), cudaMemcpyDeviceToHost)))) break;
+        for (int e = 0; e < kElems; ++e)
+            for (int v = 0; v < nv; ++v) fout[size_t(e) * nv + v] = h[size_t(v) * kElems + e];
+        rc = ok(cudaMemcpy(Uout, dUn, nu * sizeof(double), cudaMemcpyDeviceToHost));
+    } while (false);
+    for (int i = 0; i < 3; ++i) {
+        cudaFree(dF[i]);
+        cudaFree(dL[i]);
+        cudaFree(dU[i]);
+        cudaFree(dLU[i]);
+    }
+    cudaFree(dUn);
+    cudaFree(dUt);
+    cudaFree(dM);
+    cudaFree(dout);
+    cudaFree(dc);
+    return rc;
+}

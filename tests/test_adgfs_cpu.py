@@ -198,7 +198,7 @@ def test_oracle_ars_step_equals_reference_kernels(model, scheme):
     """One ARS step of the oracle's steppers against the reference's own
     bgk-, esbgk- and shakov-direct-gll kernels (rendered; the call sequence
     of frfs/integrators/std/steppers.py:538-585; golden vectors written by
-    tests/golden/make_reference_ars.py on a GPU): 4 of its 32 seeded
+    tests/golden/make_reference_ars.py on a GPU): 2 of its 32 seeded
     distributions on a 16^3 grid, a given explicit part L, dt nu ~ 1, FP64."""
     import os
     import sys
@@ -223,3 +223,32 @@ def test_oracle_ars_step_equals_reference_kernels(model, scheme):
     # relative to the change the step makes
     err = np.linalg.norm(got - want) / np.linalg.norm(want - f0)
     assert err < 1e-12, err
+
+
+@pytest.mark.parametrize('model', ['bgk', 'esbgk', 'shakov'])
+@pytest.mark.parametrize('q', [2, 3])
+def test_oracle_bdf_update_equals_reference_kernels(model, q):
+    """One IMEX-BDF-q update of the oracle (oracle/bgk.py:bdf_update)
+    against the reference's own updateMom{q}_BDF / cmaxwellian /
+    updateDistribution{q}_BDF kernels of the *-direct-gll templates (the
+    call sequence of BDF2AstdStepper.step, frfs/integrators/std/
+    steppers.py:700-760; golden vectors of tests/golden/
+    make_reference_ars.py): new moments and distribution, FP64."""
+    import os
+    import sys
+    from oracle.bgk import BDF, MODELS, bdf_update
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), 'golden'))
+    from make_reference_ars import bdf_inputs, grid
+    d = np.load(os.path.join(os.path.dirname(__file__), 'golden', 'reference_ars.npz'))
+    cv, cw = grid()
+    rows = d['rows']
+    fs, Ls = bdf_inputs(cv, q)
+    fs, Ls = fs[:, rows], Ls[:, rows]
+    mom = MODELS[model][0]
+    A, G, b, _ = BDF[q]
+    Pr = 1.0 if model == 'bgk' else 2.0 / 3.0
+    U, f = bdf_update(list(fs), list(Ls), [mom(x, cv, cw) for x in fs], [mom(x, cv, cw) for x in Ls],
+                      A, [-x for x in G], b, float(d['dt']), float(d['prefac']), 0.81, Pr, cv, model)
+    wf, wU = d[f'{model}:bdf{q}:f'], d[f'{model}:bdf{q}:U']
+    assert np.linalg.norm(f - wf) / np.linalg.norm(wf - fs[-1]) < 1e-12
+    assert np.abs(U - wU).max() / np.abs(wU).max() < 1e-13

@@ -389,3 +389,56 @@ def test_ars_stages_equal_reference_kernels(cuda, model, scheme):
     err = np.linalg.norm(got - want) / np.linalg.norm(want - f0)
     print(f'{model} {scheme}: {err:.1e}')
     assert err < 1e-12
+
+
+@pytest.mark.parametrize('model', ['bgk', 'esbgk', 'shakov'])
+@pytest.mark.parametrize('q', [2, 3])
+def test_bdf_step_equals_reference_kernels(cuda, model, q):
+    """bdgfs_bdf_step (moments of the newest history level reduced in the
+    launch, the others given) against the reference's own BDF-q update
+    kernels (golden vectors of tests/golden/make_reference_ars.py): new
+    distribution and moments, FP64."""
+    import ctypes as C
+    import os
+    import sys
+    from frfs_b200 import _lib
+    from oracle.bgk import BDF, MODELS
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), 'golden'))
+    from make_reference_ars import bdf_inputs, grid
+    d = np.load(os.path.join(os.path.dirname(__file__), 'golden', 'reference_ars.npz'))
+    cv, cw = grid()
+    rows = d['rows']
+    fs, Ls = bdf_inputs(cv, q)
+    fs, Ls = fs[:, rows], Ls[:, rows]
+    Nv, n = 16, fs.shape[1]
+    dev = torch.device('cuda')
+    mom = MODELS[model][0]
+    c0 = torch.as_tensor(np.linspace(-5 + 5 / Nv, 5 - 5 / Nv, Nv), dtype=torch.float64, device=dev)
+    F = [torch.as_tensor(x, device=dev) for x in fs]
+    Ld = [torch.as_tensor(x, device=dev) for x in Ls]
+    U = [torch.as_tensor(mom(x, cv, cw), device=dev) for x in fs]
+    LU = [torch.as_tensor(mom(x, cv, cw), device=dev) for x in Ls]
+    U[-1].zero_()
+    LU[-1].zero_()                               # reduced by the launch (MOMN)
+    Unew = torch.zeros_like(U[0])
+    fout = torch.empty_like(F[0])
+    A, G, b, _ = BDF[q]
+    x = _lib.BdfArgs(ndof=n, Nv=Nv, fp64=1, c0=c0.data_ptr(), cw=cw, prefac=float(d['prefac']), omega=0.81,
+                     dt=float(d['dt']), q=q, model={'bgk': 0, 'esbgk': 1, 'shakov': 2}[model],
+                     Pr=1.0 if model == 'bgk' else 2.0 / 3.0, b=b, Unew=Unew.data_ptr(),
+                     fout=fout.data_ptr(), flags=1 | 2 | 4)
+    for i in range(q + 1):
+        x.a[i] = A[i]
+    for i in range(q):
+        x.g[i] = -G[i]
+        x.f[i] = F[i].data_ptr()
+        x.L[i] = Ld[i].data_ptr()
+        x.U[i] = U[i].data_ptr()
+        x.LU[i] = LU[i].data_ptr()
+    _lib.check(_lib.lib().bdgfs_bdf_step(C.byref(x), _lib.stream_ptr()), 'bdgfs_bdf_step')
+    torch.cuda.synchronize()
+    wf, wU = d[f'{model}:bdf{q}:f'], d[f'{model}:bdf{q}:U']
+    ef = np.linalg.norm(fout.cpu().numpy() - wf) / np.linalg.norm(wf - fs[-1])
+    eU = np.abs(Unew.cpu().numpy() - wU).max() / np.abs(wU).max()
+    print(f'{model} BDF-{q}: f {ef:.1e}, U {eU:.1e}')
+    assert ef < 1e-12 and eU < 1e-13
