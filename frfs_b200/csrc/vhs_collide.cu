@@ -659,6 +659,33 @@ __device__ __forceinline__ void p2_pass1_spectrum(int tr, const float4* ez, floa
     }
 }
 
+// p2_pass1_spectrum from tensor memory: the thread's pencil spectra A[kz]
+// (columns ft..ft+47, re/im interleaved) and B[kz] (ft+48..ft+95): the
+// same values p2_pass1_spectrum reads from Fh (B = the conjugate partner,
+// or the own pencil of a self-conjugate pair), so the result is the same.
+__device__ __forceinline__ void p2_pass1_spectrum_tm(int tr, const float4* ez, float2 al, float2 be,
+                                                     float2 be2, uint32_t ft, float2 (&vr)[p2::N],
+                                                     float2 (&vi)[p2::N])
+{
+    constexpr int N = p2::N;
+#pragma unroll
+    for (int c = 0; c < N / 8; ++c) {
+        uint32_t ra[16], rb[16];
+        tc::tmem_ld16_issue(ft + 16 * c, ra);
+        tc::tmem_ld16_issue(ft + 48 + 16 * c, rb);
+        tc::tmem_wait();
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int kz = 8 * c + k;
+            const float4 e = ez[kz];
+            const float2 m = __ffma2_rn(al, f2(e.x, e.y), __fmul2_rn(kz == N / 2 ? be2 : be, f2(e.z, e.w)));
+            const cpx<float> A = {__uint_as_float(ra[2 * k]), __uint_as_float(ra[2 * k + 1])};
+            const cpx<float> B = {__uint_as_float(rb[2 * k]), __uint_as_float(rb[2 * k + 1])};
+            p2_spec(tr, m, A, B, vr[kz], vi[kz]);
+        }
+    }
+}
+
 // SPLIT: the barrier that frees the work cube after the x-pass loads is an
 // mbarrier (arrive right after the loads, wait just before the next z-pass
 // stores), so the x-pass DFT, the S_p update and the next z-pass spectrum and
@@ -674,7 +701,7 @@ __device__ __forceinline__ void p2_pass1_spectrum(int tr, const float4* ez, floa
 // 3/4 of the SM's; here the sub-partitions carry 5, 5, 4 and 4 pipe units
 // of work (a pair warp 2, a scalar warp 1): a bound of 9/10.  The other
 // stages run on threads 0..287 as without BAL.
-template <bool SPLIT, bool BAL = false>
+template <bool SPLIT, bool BAL = false, bool FHT = false>
 __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict__ f,
                                float* __restrict__ Qout, double* mom, int flags,
                                unsigned char* smem, unsigned char* scratch, uint32_t tmem,
@@ -724,6 +751,11 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
     const float inv_n = 1.f / float(N * N * N);
     const int warp = tid >> 5;
     const uint32_t ts = tmem + (uint32_t(32 * (warp & 3)) << 16) + uint32_t(2 * N * (warp >> 2));
+    // FHT: the z-pass spectra in the upper 256 columns: pair warps 96 columns
+    // each (A and B), the single-pencil warps 48
+    static_assert(!FHT || (SPLIT && BAL), "spectra in tensor memory with the balanced split variant");
+    const uint32_t ft = tmem + (uint32_t(32 * (warp & 3)) << 16) +
+                        (lp ? TMEM_COLS + uint32_t(4 * N * (warp >> 2)) : TMEM_COLS + uint32_t(8 * N));
 
     // ---- Fh = FFT(f) / n (kx <= N/2) ----
     if (pt) {
@@ -792,7 +824,9 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
                 float aA, bA, cA, aB, bB, cB;
                 p2_coef(ep, kxA, kyA, tr, aA, bA, cA);
                 p2_coef(ep, kxB, kyB, tr, aB, bB, cB);
-                if (single_warp)
+                if constexpr (FHT)
+                    p2_pass1_spectrum_tm(tr, ezz + q * N, f2(aA, aB), f2(bA, bB), f2(cA, cB), ft, vr, vi);
+                else if (single_warp)
                     p2_pass1_spectrum<true>(tr, ezz + q * N, f2(aA, aB), f2(bA, bB), f2(cA, cB),
                                             fa, fb, single, vr, vi);
                 else
@@ -816,12 +850,29 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
                 float a, b, c;
                 p2_coef(ph + q * 3 * N, s_kx, s_ky, tr, a, b, c);
                 const float4* ez = ezz + q * N;
+                if constexpr (FHT) {
 #pragma unroll
-                for (int kz = 0; kz < N; ++kz) {
-                    const float4 e = ez[kz];
-                    const float m = fmaf(a, e.x, (kz == N / 2 ? c : b) * e.z);
-                    const cpx<float> F = ss ? conjc(s_fa[(N - kz) % N]) : s_fa[kz];
-                    v[kz] = tr == 0 ? cpx<float>{m * F.x, m * F.y} : cpx<float>{-m * F.y, m * F.x};
+                    for (int cc = 0; cc < N / 8; ++cc) {
+                        uint32_t r[16];
+                        tc::tmem_ld16_issue(ft + 16 * cc, r);
+                        tc::tmem_wait();
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) {
+                            const int kz = 8 * cc + k;
+                            const float4 e = ez[kz];
+                            const float m = fmaf(a, e.x, (kz == N / 2 ? c : b) * e.z);
+                            const cpx<float> F = {__uint_as_float(r[2 * k]), __uint_as_float(r[2 * k + 1])};
+                            v[kz] = tr == 0 ? cpx<float>{m * F.x, m * F.y} : cpx<float>{-m * F.y, m * F.x};
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int kz = 0; kz < N; ++kz) {
+                        const float4 e = ez[kz];
+                        const float m = fmaf(a, e.x, (kz == N / 2 ? c : b) * e.z);
+                        const cpx<float> F = ss ? conjc(s_fa[(N - kz) % N]) : s_fa[kz];
+                        v[kz] = tr == 0 ? cpx<float>{m * F.x, m * F.y} : cpx<float>{-m * F.y, m * F.x};
+                    }
                 }
                 dft<N, +1>(v);
             };
@@ -844,6 +895,35 @@ __device__ void collide_one_p2(const bdgfs_vhs_grid& g, const float* __restrict_
                 }
                 wpar ^= 1u;
             };
+            if constexpr (FHT) {
+                if (p == 0) {
+                    // the distribution's spectra, once: A[kz] = Fh of the pencil,
+                    // B[kz] = its partner's (see p2_pass1_spectrum)
+#pragma unroll
+                    for (int cc = 0; cc < N / 8; ++cc) {
+                        uint32_t r[16], rb[16];
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) {
+                            const int kz = 8 * cc + k, kn = (N - kz) % N;
+                            cpx<float> A, B;
+                            if (lp) {
+                                A = fa[kz];
+                                B = (single_warp && single) ? fb[kz] : conjc(fa[kn]);
+                            } else {
+                                A = ss ? conjc(s_fa[kn]) : s_fa[kz];
+                                B = A;
+                            }
+                            r[2 * k] = __float_as_uint(A.x);
+                            r[2 * k + 1] = __float_as_uint(A.y);
+                            rb[2 * k] = __float_as_uint(B.x);
+                            rb[2 * k + 1] = __float_as_uint(B.y);
+                        }
+                        tc::tmem_st16(ft + 16 * cc, r);
+                        if (lp) tc::tmem_st16(ft + 48 + 16 * cc, rb);
+                    }
+                    tc::tmem_wait_st();
+                }
+            }
             if (lp) {
                 float2 vr[N], vi[N];
                 zpass(0, vr, vi);
@@ -1214,16 +1294,17 @@ template <typename T, int N, int NT, bool WG, bool SG, int GR = 0, bool SL = fal
 struct Variant {
     using L = QLayout<T, N, NT, WG, SG, SL>;
     static constexpr int n = N;
-    static constexpr bool wg = WG, sg = SG, sl = SL, pk = false, split = false, bal = false;
+    static constexpr bool wg = WG, sg = SG, sl = SL, pk = false, split = false, bal = false, fht = false;
     static constexpr int gr = GR;
 };
 
-// packed Nv = 24 FP32 variant (288 threads); SPLIT: split work-cube barrier
-template <bool SPLIT = false, bool BAL = false>
+// packed Nv = 24 FP32 variant (288 threads); SPLIT: split work-cube barrier;
+// FHT: each thread's z-pass spectra held in tensor memory (see collide_one_p2)
+template <bool SPLIT = false, bool BAL = false, bool FHT = false>
 struct VariantP2 {
     using L = QLayoutP2;
     static constexpr int n = p2::N;
-    static constexpr bool wg = false, sg = false, sl = false, pk = true, split = SPLIT, bal = BAL;
+    static constexpr bool wg = false, sg = false, sl = false, pk = true, split = SPLIT, bal = BAL, fht = FHT;
     static constexpr int gr = 0;
 };
 
@@ -1238,8 +1319,9 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
     __shared__ uint32_t s_tmem;
     __shared__ __align__(8) uint64_t s_wfree;
     constexpr bool kPacked = V0::pk || V1::pk;
+    constexpr uint32_t kTmemCols = (V0::fht || V1::fht) ? 2 * p2::TMEM_COLS : p2::TMEM_COLS;
     if constexpr (kPacked) {
-        if (threadIdx.x < 32) tc::tmem_alloc(&s_tmem, p2::TMEM_COLS);
+        if (threadIdx.x < 32) tc::tmem_alloc(&s_tmem, kTmemCols);
         if (threadIdx.x == 0) tc::mbar_init(&s_wfree, NT);
         tc::tc_fence_before();
     }
@@ -1283,7 +1365,7 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
         double* mom = bt.moments ? bt.moments + dof * 10 : nullptr;
         if (g.Nv == V0::n) {
             if constexpr (V0::pk)
-                collide_one_p2<V0::split, V0::bal>(g, f, Q, mom, a.flags, smem, scratch, tmem, &s_wfree, wpar,
+                collide_one_p2<V0::split, V0::bal, V0::fht>(g, f, Q, mom, a.flags, smem, scratch, tmem, &s_wfree, wpar,
                                           a.counter);
             else
                 collide_one<T, V0::n, NT, V0::wg, V0::sg, V0::gr, V0::sl>(
@@ -1291,7 +1373,7 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
         } else if constexpr (V1::n > 0) {
             if (g.Nv == V1::n) {
                 if constexpr (V1::pk)
-                    collide_one_p2<V1::split, V1::bal>(g, f, Q, mom, a.flags, smem, scratch, tmem, &s_wfree,
+                    collide_one_p2<V1::split, V1::bal, V1::fht>(g, f, Q, mom, a.flags, smem, scratch, tmem, &s_wfree,
                                               wpar, a.counter);
                 else
                     collide_one<T, V1::n, NT, V1::wg, V1::sg, V1::gr, V1::sl>(
@@ -1305,14 +1387,15 @@ __global__ void __launch_bounds__(NT, 1) __maxnreg__(65536 / NT / 8 * 8 > 255 ? 
         __syncthreads();
         if (threadIdx.x < 32) {
             tc::tc_fence_after();
-            tc::tmem_dealloc(tmem, p2::TMEM_COLS);
+            tc::tmem_dealloc(tmem, kTmemCols);
         }
     }
 }
 
 struct NoVariant {
     static constexpr int n = 0;
-    static constexpr bool wg = false, sg = false, sl = false, pk = false, split = false, bal = false;
+    static constexpr bool wg = false, sg = false, sl = false, pk = false, split = false, bal = false,
+                          fht = false;
     static constexpr int gr = 0;
     struct L {
         static constexpr int WS = 0;
@@ -1399,6 +1482,9 @@ static const Entry kEntries[] = {
     // split barrier, 8 pair-warps + 2 single-pencil warps in the transform loop
     {0, 24, 0, 320, &launch<float, 320, VariantP2<true, true>, NoVariant>,
      &entry_per_cta<float, 320, VariantP2<true, true>, NoVariant>},
+    // the same with each thread's z-pass spectra in tensor memory
+    {0, 24, 0, 320, &launch<float, 320, VariantP2<true, true, true>, NoVariant>,
+     &entry_per_cta<float, 320, VariantP2<true, true, true>, NoVariant>},
 };
 static constexpr int kNumEntries = int(sizeof(kEntries) / sizeof(kEntries[0]));
 
