@@ -561,7 +561,9 @@ __device__ void collide_one(const bdgfs_vhs_grid& g, const T* __restrict__ f,
 // S_p (48 floats per thread) lives in tensor memory: with 9 warps per CTA
 // three share an SM sub-partition, which caps registers at 168, and the
 // x-pass needs 96 for its two pencils.  Warp w owns TMEM lanes
-// 32*(w%4).. and columns 48*(w/4).. of a 256-column allocation.
+// 32*(w%4).. and columns 48*(w/4).. of a 256-column allocation; the
+// spectra-in-TMEM variant allocates 512 columns and keeps the z-pass
+// spectra in the upper 256 (see collide_one_p2).
 namespace p2 {
 constexpr int N = p2tab::N, NH = N / 2 + 1, NP2 = N / 2, NT = 288;
 constexpr uint32_t TMEM_COLS = 256;
