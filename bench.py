@@ -1318,23 +1318,44 @@ def run_gpu(args):
     pk_ms = a.elapsed_time(b)
     peak = nsm * 8 * 256 * iters * 16 * 8 * 2 / (pk_ms * 1e-3) / 1e12
     # ---------------- e2e: host buffers, copies inside the timed region.  Every
-    # step uploads its input from pinned host memory and reads its result back;
-    # the result is first copied to a device staging bank, so its device->host
-    # read (copy stream) overlaps the next step's upload and compute.  One
-    # interval covers all steps, the L2 flushes and the last read-back.
+    # step uploads its input from pinned host memory and reads its result back.
+    # Uploads go to one of two device input buffers on their own copy stream,
+    # so the next step's upload overlaps this step's compute (the first one
+    # does not); the step starts from its buffer with a device copy.  The
+    # result is first copied to a device staging bank, so its device->host
+    # read (a second copy stream) overlaps the next step too.  One interval
+    # covers all steps, the L2 flushes and the last read-back.
     nbytes = fin.numel() * fin.element_size()
     host_in = torch.empty(fin.shape, dtype=fin.dtype, pin_memory=True)
     host_out = torch.empty(fin.shape, dtype=fin.dtype, pin_memory=True)
     host_in.copy_(fin)
     stage = torch.empty_like(fin)
+    dev_in = [torch.empty_like(fin), torch.empty_like(fin)]
     cs = torch.cuda.Stream(device=dev)
+    cu = torch.cuda.Stream(device=dev)
+    uploaded, consumed = [None, None], [None, None]
+
+    def upload(k):
+        with torch.cuda.stream(cu):
+            if consumed[k % 2] is not None:
+                cu.wait_event(consumed[k % 2])     # its previous input has been taken
+            dev_in[k % 2].copy_(host_in, non_blocking=True)
+            uploaded[k % 2] = torch.cuda.Event()
+            uploaded[k % 2].record(cu)
     copied = None
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(st)
-    for _ in range(args.steps):
+    cu.wait_event(a)
+    upload(0)
+    for k in range(args.steps):
         flush.fill_(1)
-        fin.copy_(host_in, non_blocking=True)
+        if k + 1 < args.steps:
+            upload(k + 1)
+        st.wait_event(uploaded[k % 2])
+        fin.copy_(dev_in[k % 2])
+        consumed[k % 2] = torch.cuda.Event()
+        consumed[k % 2].record(st)
         integ.step(integ.tcurr, dt)
         if copied is not None:
             st.wait_event(copied)                  # the previous read-back has left stage
