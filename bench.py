@@ -1475,6 +1475,39 @@ def run_q_only(ndof):
     print(json.dumps({'q_only_ndof': ndof, 'finite': bool(torch.isfinite(q).all())}))
 
 
+def run_surrogate_curve(modes=(64, 128, 256, 384, 512)):
+    """Analysis case: the Couette-family surrogate (drift-free rows, the
+    config-4 model and training) at several basis sizes: held-out error
+    against the FP32 spectral Q (50000 distributions), the bases'
+    truncation of the heads, and the error of the fixed linear path alone
+    (the hidden layers' output zeroed), one JSON line per size."""
+    import time
+    from frfs_b200.backend import CUDABackend
+    from frfs_b200.inifile import Inifile
+    from frfs_b200.scattering import DGFSVHSGLLScatteringModel
+    from frfs_b200.surrogate import QSurrogate
+    from frfs_b200.velocitymesh import DGFSVelocityMesh
+    cfg = Inifile(couette_ini('single'))
+    be = CUDABackend(cfg)
+    vm = DGFSVelocityMesh(be, cfg)
+    sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
+    for k in modes:
+        t0 = time.time()
+        q = QSurrogate(sm.grid, nmodes=k, width=1024)
+        q.fit(nsamples=200000, ntest=50000, epochs=20, lr=3e-4, batch=1024, seed=0)
+        saved = q.W[3].clone()
+        q.W[3][:, :q.w] = 0.0
+        q._fold()
+        lin = q.evaluate(10000, seed=1)
+        q.W[3].copy_(saved)
+        q._fold()
+        print(json.dumps({'modes': k, 'heldout_rel_l2_vs_spectral_q': q.test_err,
+                          'basis_truncation_heads': q.basis_err_heads,
+                          'heldout_rel_l2_linear_skip_only': lin, 'fit_s': time.time() - t0}),
+              flush=True)
+        del q
+
+
 def run_surrogate_call(ndof, reps=2):
     """Profiling case: all-surrogate hybrid calls on ndof Couette-family
     cells with a randomly initialised 256-mode / width-1024 network (the
@@ -1655,6 +1688,8 @@ def main():
                     help='profiling case: 3 launches of the collision kernel on NDOF cubes')
     ap.add_argument('--surrogate-call', type=int, default=0, metavar='NDOF',
                     help='profiling case: all-surrogate hybrid calls on NDOF cells')
+    ap.add_argument('--surrogate-curve', action='store_true',
+                    help='analysis case: the Couette surrogate at 64..512 modes')
     ap.add_argument('--q-batched', type=int, default=0, metavar='NDOF24',
                     help='profiling case: the two-species collision launch on NDOF24 24^3 and '
                          'NDOF24/3 32^3 cubes')
@@ -1674,6 +1709,8 @@ def main():
         run_q_only(args.q_only)
     elif args.surrogate_call:
         run_surrogate_call(args.surrogate_call)
+    elif args.surrogate_curve:
+        run_surrogate_curve()
     elif args.hybrid_steps:
         run_hybrid_steps(args.hybrid_steps)
     elif args.q_batched:
