@@ -456,9 +456,9 @@ def config_block(n):
 # ---------------------------------------------------------------- other configs
 BATCHED = dict(n24=24576, n32=8192, Nrho=16, M=12, dev=6, omega=0.81, mass2=2.0)
 # DRAM bytes (read + write) of one collision launch on the 2048-DOF Couette
-# state, from an ncu capture of the packed Nv=24 variant with the split
-# work-cube barrier (114.7 MB + 96.3 MB)
-Q_LAUNCH_DRAM_BYTES = 114.69e6 + 96.25e6
+# state, from an ncu capture of the tuner's Nv=24 variant (the balanced
+# packed variant with the z-pass spectra in tensor memory: 114.2 MB + 93.5 MB)
+Q_LAUNCH_DRAM_BYTES = 114.22e6 + 93.46e6
 SMALL64 = dict(Nv=16, Nrho=8, M=6, dev=5, omega=0.5, order=2, nx=4, ny=4, dt=1e-3)
 
 
@@ -1434,7 +1434,8 @@ def run_gpu(args):
                      'traffic': Q_LAUNCH_DRAM_BYTES, 'traffic_alg': 2 * 4 * ndof * 24**3,
                      'traffic_source': ('not measured in this run: dram__bytes_read.sum + '
                                         'dram__bytes_write.sum of one ncu capture of this '
-                                        'kernel variant on the same 2048 Couette cubes')},
+                                        'kernel variant on the same 2048 Couette cubes '
+                                        '(profiles/vhs_collide_nv24.md)')},
         'e2e': {'value': e2e, 'unit': 'DG steps/s', 'h2d_bytes_per_step': nbytes,
                 'd2h_bytes_per_step': nbytes},
         'gpu_launches': launches,
