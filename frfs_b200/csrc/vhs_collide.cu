@@ -664,7 +664,9 @@ __device__ __forceinline__ void p2_pass1_spectrum(int tr, const float4* ez, floa
 // p2_pass1_spectrum from tensor memory: the thread's pencil spectra A[kz]
 // (columns ft..ft+47, re/im interleaved) and B[kz] (ft+48..ft+95): the
 // same values p2_pass1_spectrum reads from Fh (B = the conjugate partner,
-// or the own pencil of a self-conjugate pair), so the result is the same.
+// or the own pencil of a self-conjugate pair) and the same operations; the
+// result agrees to rounding (the compiler may contract the spectrum
+// products into the DFT's first additions differently).
 __device__ __forceinline__ void p2_pass1_spectrum_tm(int tr, const float4* ez, float2 al, float2 be,
                                                      float2 be2, uint32_t ft, float2 (&vr)[p2::N],
                                                      float2 (&vi)[p2::N])
