@@ -18,7 +18,7 @@ _ERRORS = {-1: 'invalid argument', -2: 'CUDA error', -3: 'unsupported grid/preci
 EXPORTS = (
     'bdgfs_vhs_scratch_bytes', 'bdgfs_vhs_collide', 'bdgfs_vhs_tiles', 'bdgfs_fma_probe',
     'bdgfs_vhs_collide_static', 'bdgfs_wait_probe',
-    'bdgfs_fr_disu', 'bdgfs_fr_bc_update', 'bdgfs_fr_rhs', 'bdgfs_fr_rhs_gather',
+    'bdgfs_fr_disu', 'bdgfs_fr_invmass', 'bdgfs_fr_bc_update', 'bdgfs_fr_rhs', 'bdgfs_fr_rhs_gather',
     'bdgfs_fr_bc_update_gather', 'bdgfs_fr_rhs_tensor',
     'bdgfs_moments', 'bdgfs_residual', 'bdgfs_status_check',
     'bdgfs_gemm', 'bdgfs_colsum', 'bdgfs_adamw', 'bdgfs_relmse',
@@ -164,6 +164,7 @@ def lib():
         vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
         sig = {
             'bdgfs_fr_disu': [vp, vp, vp, vp],
+            'bdgfs_fr_invmass': [vp, vp, vp, vp, vp],
             'bdgfs_fr_bc_update': [vp, vp, vp, vp],
             'bdgfs_fr_rhs': [vp, vp, vp, vp, vp, dbl, dbl, vp, dbl, vp, dbl, vp],
             'bdgfs_fr_rhs_gather': [vp, vp, vp, vp, vp, dbl, dbl, vp, dbl, vp, dbl, vp],

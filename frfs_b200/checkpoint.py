@@ -8,9 +8,9 @@ system takes the stored solution as ``initsoln`` (solvers/dgfs/system.py:
 (integrators/base.py:36-40).  HDF5 is not available here, so the same
 content -- the config text, tcurr, the accepted-step count and the
 solution bank of every species -- is stored in one ``.npz`` file.  A
-restart needs the same mesh, order and velocity grid (the reference also
-interpolates between solution bases; that is not done here and a mismatch
-raises ``ValueError``).
+restart needs the same mesh and velocity grid; a solution of another order
+is interpolated onto the current solution points, as the reference does
+(solvers/dgfs/system.py:96-107).
 """
 import numpy as np
 import torch
@@ -75,9 +75,8 @@ def restart(backend, mesh, ckpt, cfg=None):
         from .dgfsbi import DGFSBiSystem
 
         def make(nreg):
-            for a in ckpt.soln:
-                _check_shape(mesh, cfg, a)
-            return DGFSBiSystem(backend, mesh, cfg, nreg=nreg, initsoln=ckpt.soln)
+            soln = [interp_soln(mesh, cfg, ckpt.cfg, a) for a in ckpt.soln]
+            return DGFSBiSystem(backend, mesh, cfg, nreg=nreg, initsoln=soln)
     else:
         if name == 'adgfs':
             from .adgfs import ADGFSSystem as cls
@@ -87,18 +86,37 @@ def restart(backend, mesh, ckpt, cfg=None):
             raise ValueError(f'unknown system {name}')
 
         def make(nreg):
-            _check_shape(mesh, cfg, ckpt.soln[0])
-            return cls(backend, mesh, cfg, nreg=nreg, initsoln=ckpt.soln[0])
+            soln = interp_soln(mesh, cfg, ckpt.cfg, ckpt.soln[0])
+            return cls(backend, mesh, cfg, nreg=nreg, initsoln=soln)
     integ = get_integrator(backend, make, cfg)
     integ.tcurr = ckpt.tcurr
     integ.nacptsteps = ckpt.nacptsteps
     return integ
 
 
-def _check_shape(mesh, cfg, arr):
-    from .mesh import ElementGeometry
-    geo = ElementGeometry(mesh, cfg.getint('solver', 'order'))
+def interp_soln(mesh, cfg, solncfg, arr):
+    """The stored solution ``arr`` ([neles][nupts of the stored order][Nv^3],
+    written under ``solncfg``) on the solution points of the order ``cfg``
+    asks for: the stored nodal basis evaluated at the current points applied
+    per element (solvers/dgfs/system.py:96-107), in FP64 and returned in
+    the stored dtype.  Mesh and velocity grid must match (the reference
+    checks the field names, i.e. the velocity count)."""
+    from .shapes import TensorShape
+    order = cfg.getint('solver', 'order')
+    sorder = solncfg.getint('solver', 'order', order)
     Nv = cfg.getint('constants', 'Nv')
-    want = (geo.neles, geo.nupts, Nv**3)
-    if tuple(arr.shape) != want:
-        raise ValueError(f'checkpoint solution {arr.shape} does not fit the system {want}')
+    if arr.ndim != 3 or arr.shape[0] != mesh.neles or arr.shape[2] != Nv**3:
+        raise ValueError(f'checkpoint solution {arr.shape} does not fit the system '
+                         f'({mesh.neles}, *, {Nv**3})')
+    src = TensorShape(mesh.etype, sorder)
+    if arr.shape[1] != src.nupts:
+        raise ValueError(f'checkpoint solution {arr.shape} does not fit its order {sorder}')
+    if sorder == order:
+        return arr
+    op = TensorShape(mesh.etype, order).interp_from(sorder)      # (nupts, src.nupts)
+    out = np.empty((arr.shape[0], op.shape[0], arr.shape[2]), dtype=arr.dtype)
+    step = max(1, (1 << 26) // max(1, arr.shape[1] * arr.shape[2]))
+    for e0 in range(0, arr.shape[0], step):
+        blk = arr[e0:e0 + step].astype(np.float64)
+        out[e0:e0 + step] = np.einsum('ij,ejv->eiv', op, blk)
+    return out

@@ -123,19 +123,21 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// u_f = M0 u.  Each CTA (128 threads) owns one element and a chunk of
-// velocities, each thread VB consecutive velocities per step.  When every
-// row of M0 is a unit vector (flux points on solution points, as with GLL
-// points) the product is a gather: uf[f] = u[sel[f]], pure data movement;
-// otherwise the dense product with the operator read from shared memory.
+// u_f = M0 u (gm0 = M0, NF flux points), or any other per-element operator
+// with NF rows (the inverse mass matrix: NF = NU).  Each CTA (128 threads)
+// owns one element and a chunk of velocities, each thread VB consecutive
+// velocities per step.  When every row of the operator is a unit vector
+// (flux points on solution points, as with GLL points) the product is a
+// gather: uf[f] = u[sel[f]], pure data movement; otherwise the dense product
+// with the operator read from shared memory.
 template <typename T, int NU, int NF, int VB>
-__global__ void __launch_bounds__(128) disu_kernel(const bdgfs_fr_eles el, const T* __restrict__ u,
-                                                   T* __restrict__ uf, int64_t chunk)
+__global__ void __launch_bounds__(128) disu_kernel(const bdgfs_fr_eles el, const T* __restrict__ gm0,
+                                                   const T* __restrict__ u, T* __restrict__ uf,
+                                                   int64_t chunk)
 {
     __shared__ T m0[NF * NU];
     __shared__ int sel[NF];
     __shared__ int gather;
-    const T* gm0 = static_cast<const T*>(el.m0);                                  // [NF][NU]
     for (int i = threadIdx.x; i < NF * NU; i += blockDim.x) m0[i] = gm0[i];
     if (threadIdx.x == 0) gather = 1;
     __syncthreads();
@@ -697,23 +699,25 @@ static int rhs_launch(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl, const v
 }
 
 template <typename T, int NU, int NF, int VB>
-static int disu_launch_vb(const bdgfs_fr_eles* el, const void* u, void* uf, cudaStream_t st)
+static int disu_launch_vb(const bdgfs_fr_eles* el, const void* op, const void* u, void* uf,
+                          cudaStream_t st)
 {
     const int64_t chunk = fr_chunk(el->nv, el->neles, VB);
     dim3 g;
     if (grid_v(el->nv, el->neles, chunk, &g) != BDGFS_OK) return BDGFS_EINVAL;
-    disu_kernel<T, NU, NF, VB><<<g, 128, 0, st>>>(*el, static_cast<const T*>(u), static_cast<T*>(uf),
-                                                  chunk);
+    disu_kernel<T, NU, NF, VB><<<g, 128, 0, st>>>(*el, static_cast<const T*>(op), static_cast<const T*>(u),
+                                                  static_cast<T*>(uf), chunk);
     return cuda_status(cudaGetLastError());
 }
 
+// op: [NF][NU] operator (M0 for disu, the inverse mass matrix for invmass)
 template <typename T, int NU, int NF>
-static int disu_launch(const bdgfs_fr_eles* el, const void* u, void* uf, cudaStream_t st)
+static int disu_launch(const bdgfs_fr_eles* el, const void* op, const void* u, void* uf, cudaStream_t st)
 {
     const void* ptrs[] = {u, uf};
     constexpr int VBW = sizeof(T) == 4 ? 4 : 2;
-    if (vec_width<T>(el->nv, ptrs, 2) == VBW) return disu_launch_vb<T, NU, NF, VBW>(el, u, uf, st);
-    return disu_launch_vb<T, NU, NF, 1>(el, u, uf, st);
+    if (vec_width<T>(el->nv, ptrs, 2) == VBW) return disu_launch_vb<T, NU, NF, VBW>(el, op, u, uf, st);
+    return disu_launch_vb<T, NU, NF, 1>(el, op, u, uf, st);
 }
 
 #define BDGFS_FR_SHAPES(X)                                                          \
@@ -750,8 +754,24 @@ extern "C" int32_t bdgfs_fr_disu(const bdgfs_fr_eles* el, const void* u, void* u
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 #define GO(D, U, F)                                                                         \
     if (el->ndims == D && el->nupts == U && el->nfpts == F)                                 \
-        return el->fp64 ? disu_launch<double, U, F>(el, u, uf, st)                          \
-                        : disu_launch<float, U, F>(el, u, uf, st);
+        return el->fp64 ? disu_launch<double, U, F>(el, el->m0, u, uf, st)                 \
+                        : disu_launch<float, U, F>(el, el->m0, u, uf, st);
+    BDGFS_FR_SHAPES(GO)
+#undef GO
+    return BDGFS_EUNSUPPORTED;
+}
+
+extern "C" int32_t bdgfs_fr_invmass(const bdgfs_fr_eles* el, const void* minv, const void* u, void* out,
+                                    void* stream)
+{
+    int rc = check_eles(el);
+    if (rc != BDGFS_OK) return rc;
+    if (!minv || !u || !out || u == out) return BDGFS_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+#define GO(D, U, F)                                                                         \
+    if (el->ndims == D && el->nupts == U && el->nfpts == F)                                 \
+        return el->fp64 ? disu_launch<double, U, U>(el, minv, u, out, st)                   \
+                        : disu_launch<float, U, U>(el, minv, u, out, st);
     BDGFS_FR_SHAPES(GO)
 #undef GO
     return BDGFS_EUNSUPPORTED;

@@ -596,7 +596,9 @@ class DGFSBiSystem:
         self.collide(t, [uinbank] * S + [foutbank] * S)
 
     def invmass(self, uinbank, foutbank):
-        raise NotImplementedError('invmass is unused by the DGFS steppers')
+        """foutbank <- M12 uinbank of every species (dgfsbi/system.py:253-263)."""
+        for sp in self.species:
+            sp.invmass(uinbank, foutbank)
 
     def macroscopic(self, bank):
         """The per-species fields of the reference's mixture moment writer

@@ -144,8 +144,30 @@ class TensorShape:
             K *= _kernel_1d(n, self.upts[:, a][:, None], self.fpts[:, a][None, :])
         return K * self.fpts_wts[None, :]
 
+    @property
+    def m12(self):
+        """Inverse of the nodal mass matrix, V^T V with V[k][u] the
+        orthonormal basis (products of sqrt(k + 1/2) P_k) at the solution
+        points (shapes.py:163-166); a product of 1-D factors per axis."""
+        n = self.n1
+        V1 = np.array([np.sqrt(k + 0.5) * npleg.legval(self.pts1, [0] * k + [1])
+                       for k in range(n)])
+        m1 = V1.T @ V1
+        idx = np.array([p[::-1] for p in it.product(range(n), repeat=self.ndims)])
+        M = np.ones((self.nupts, self.nupts))
+        for a in range(self.ndims):
+            M *= m1[np.ix_(idx[:, a], idx[:, a])]
+        return M
+
+    def interp_from(self, order):
+        """(nupts, nupts of order) values at these solution points of the
+        nodal basis of order ``order``: the restart interpolation of
+        solvers/dgfs/system.py:100-104."""
+        return TensorShape(self.name, order).nodal_at(self.upts)[0]
+
     def opmat(self, expr):
-        mats = {'M0': self.m0, 'M1': self.m1, 'M2': self.m2, 'M3': self.m3}
+        mats = {'M0': self.m0, 'M1': self.m1, 'M2': self.m2, 'M3': self.m3,
+                'M12': self.m12}
         if expr == 'M1 - M3*M2':
             return mats['M1'] - mats['M3'] @ mats['M2']
         return mats[expr]

@@ -48,6 +48,7 @@ class DGFSElements:
         self.tensor = self._tensor_form(shp, m0, c) if unit else None
         self.dcorr = c(shp.opmat('M1 - M3*M2'))
         self.m3 = c(shp.opmat('M3'))
+        self.minv = c(shp.opmat('M12'))
         self.smats = c(geo.smats)
         self.rcpdjac = c(geo.rcpdjac)
         self.pnorm = c(geo.norm_pnorm)
@@ -416,7 +417,13 @@ class DGFSSystem:
         self.sm.collide(self._bank(uinbank), self._bank(foutbank))
 
     def invmass(self, uinbank, foutbank):
-        raise NotImplementedError('invmass is unused by the DGFS steppers')
+        """foutbank <- M12 uinbank per element, M12 the inverse mass matrix
+        (system.py:221-231, kernel elements.py:161-164).  The DGFS steppers
+        do not call it; the banks must differ."""
+        u, out = self._bank(uinbank), self._bank(foutbank)
+        _lib.check(_lib.lib().bdgfs_fr_invmass(_lib.ref(self.ele.struct), _lib.ptr(self.ele.minv),
+                                               _lib.ptr(u), _lib.ptr(out), _lib.stream_ptr()),
+                   'bdgfs_fr_invmass')
 
     # -- fused stage used by the steppers ---------------------------------
     def advect_combine(self, t, uinbank, outbank, a, b, x1=None, c1=0.0, x2=None, c2=0.0):

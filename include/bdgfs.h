@@ -189,6 +189,13 @@ typedef struct bdgfs_fr_walls {
 int32_t bdgfs_fr_disu(const bdgfs_fr_eles* el, const void* u, void* uf,
                       void* stream);
 
+/* out = minv u per element, minv real [nupts][nupts] in el's precision: the
+ * inverse mass matrix M12 (frfs/shapes.py:163-166).  out must not alias u.
+ * Replaces kernels['eles', 'invmass'] (solvers/dgfs/elements.py:161-164),
+ * which system.invmass (solvers/dgfs/system.py:221-231) launches. */
+int32_t bdgfs_fr_invmass(const bdgfs_fr_eles* el, const void* minv,
+                         const void* u, void* out, void* stream);
+
 /* bc0/bc1 of every diffuse-wall face point from uf.  Replaces
  * kernels['bcint', 'update_bc'] (solvers/dgfs/inters.py:221-229,
  * kernels/bccupdate.mako, kernels/bcs/dgfs-wall-diffuse-update.mako),

@@ -12,7 +12,9 @@ shims for Python 3.12 / numpy 2 (``collections.Iterable``/``Sequence``,
 ``tests/golden/*.npz``:
 
 * ``shapes_<kind>_p<order>.npz``  upts, fpts, M0, M1, M2, M3, M1-M3*M2,
-  norm_fpts from ``frfs/shapes.py`` (QuadShape / HexShape, GLL points);
+  norm_fpts, M12 (the inverse mass matrix) from ``frfs/shapes.py``
+  (QuadShape / HexShape, GLL points), and ``interp_from_p<q>`` for q =
+  order -+ 1, the restart interpolation of ``solvers/dgfs/system.py:100-104``;
 * ``metrics_<kind>_p<order>.npz``  smats, rcpdjac, pnorms, ploc for a small
   affine mesh via ``frfs/solvers/base/elements.py``;
 * ``vmesh_<case>.npz``  cv, cw, L, qz, qw, sz, sw from
@@ -96,7 +98,13 @@ def shapes():
                  M0=s.opmat('M0'), M1=s.opmat('M1'), M2=s.opmat('M2'),
                  M3=s.opmat('M3'), M132=s.opmat('M1 - M3*M2'),
                  norm_fpts=np.array(s.norm_fpts),
-                 nfacefpts=np.array(s.nfacefpts))
+                 nfacefpts=np.array(s.nfacefpts), M12=s.opmat('M12'))
+        # restart interpolation onto this basis from a solution of order q
+        # (solvers/dgfs/system.py:100-104: the stored basis' nodal_basis_at
+        # of the current solution points)
+        for q in (order - 1, order + 1):
+            solnb = cls(None, _cfg(q))
+            d[f'interp_from_p{q}'] = solnb.ubasis.nodal_basis_at(s.upts)
         name = f'shapes_{cls.name}_p{order}.npz'
         np.savez(os.path.join(OUT, name), **d)
         out[(cls.name, order)] = (cls, cfg)

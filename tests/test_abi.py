@@ -71,6 +71,7 @@ def test_invalid_arguments_return_status_not_crash():
     L = _lib.lib()
     assert L.bdgfs_vhs_collide(None, 0, None, 0, 0, None, 0, None, None) == -1
     assert L.bdgfs_fr_disu(None, None, None, None) == -1
+    assert L.bdgfs_fr_invmass(None, None, None, None, None) == -1
     assert L.bdgfs_residual(None, None, 0, 0, None, None) == -1
     assert L.bdgfs_vhs_scratch_bytes(None, 0, 1) == 0
 

@@ -290,3 +290,23 @@ def test_nancheck_plugin_detects_injected_nan(cuda):
     integ.soln[1, 3, 17] = float('nan')
     with pytest.raises(RuntimeError, match='NaNs detected'):
         integ.advance_to(3 * 5e-4)
+
+
+@pytest.mark.parametrize('kind,order,prec,tol', [('quad', 2, 'double', 1e-14), ('quad', 3, 'single', 1e-6),
+                                                 ('hex', 2, 'single', 1e-6), ('hex', 2, 'double', 1e-14)])
+def test_invmass_equals_reference_operator(cuda, kind, order, prec, tol):
+    """system.invmass (solvers/dgfs/system.py:221-231): out = M12 u per
+    element with the reference's own M12 (frfs/shapes.py:163-166, golden
+    fixture); the banks must differ."""
+    from frfs_b200._lib import BdgfsError
+    cfg, be, mesh, s = _system(kind, order, prec)
+    _perturb(s, 3)
+    m12 = np.load(f'{GOLD}/shapes_{kind}_p{order}.npz')['M12']
+    s.invmass(0, 1)
+    torch.cuda.synchronize()
+    u = s.eles_scal_upts_inb_full[0].double().cpu().numpy()
+    want = np.einsum('ij,ejv->eiv', m12, u)
+    got = s.eles_scal_upts_inb_full[1].double().cpu().numpy()
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) < tol
+    with pytest.raises(BdgfsError):
+        s.invmass(0, 0)

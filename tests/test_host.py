@@ -24,8 +24,11 @@ def test_operator_matrices_match_reference(kind, order):
     s = TensorShape(kind, order)
     assert np.allclose(s.upts, g['upts'], atol=1e-15)
     assert np.allclose(s.fpts, g['fpts'], atol=1e-15)
-    for m in ('M0', 'M1', 'M2', 'M3'):
+    for m in ('M0', 'M1', 'M2', 'M3', 'M12'):
         assert np.allclose(s.opmat(m), g[m], atol=1e-13), m
+    for k in g.files:
+        if k.startswith('interp_from_p'):
+            assert np.allclose(s.interp_from(int(k[len('interp_from_p'):])), g[k], atol=1e-14), k
     assert np.allclose(s.opmat('M1 - M3*M2'), g['M132'], atol=1e-13)
     assert np.array_equal(s.norm_fpts, g['norm_fpts'])
 
