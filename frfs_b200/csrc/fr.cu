@@ -223,8 +223,10 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
     constexpr int NUP = (NU + 3) / 4 * 4;
     extern __shared__ __align__(16) unsigned char smraw[];
     // [RING][128][VB] row ring (see below), then the operators
+    // (M1 - M3 M2) is read only by the dense residual (TPP == 0)
+    constexpr int NDT = TPP ? 0 : ND * NU * NUP;
     T* dT = reinterpret_cast<T*>(smraw) + RING * 128 * VB;   // [ND*NU][NUP]  (M1 - M3 M2) transposed
-    T* m3T = dT + ND * NU * NUP;                        // [NF][NUP]
+    T* m3T = dT + NDT;                                  // [NF][NUP]
     T* sm = m3T + NF * NUP;                             // [NU][ND][ND]
     T* rj = sm + NU * ND * ND;                          // [NU]
     T* pn = rj + NU;                                    // [NF][ND]
@@ -236,12 +238,14 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
     int* fdm = fs + NF;                                 // [NF] (TPP)
     const int64_t e = blockIdx.y;
     {
-        for (int i = threadIdx.x; i < (ND * NU + NF) * NUP; i += blockDim.x) dT[i] = T(0);
+        for (int i = threadIdx.x; i < NDT + NF * NUP; i += blockDim.x) dT[i] = T(0);
         __syncthreads();
-        const T* gd = static_cast<const T*>(el.dcorr);   // [NU][ND*NU], read coalesced
-        for (int i = threadIdx.x; i < NU * ND * NU; i += blockDim.x) {
-            const int row = i / (ND * NU), col = i - row * (ND * NU);
-            dT[col * NUP + row] = gd[i];
+        if constexpr (NDT > 0) {
+            const T* gd = static_cast<const T*>(el.dcorr);   // [NU][ND*NU], read coalesced
+            for (int i = threadIdx.x; i < NU * ND * NU; i += blockDim.x) {
+                const int row = i / (ND * NU), col = i - row * (ND * NU);
+                dT[col * NUP + row] = gd[i];
+            }
         }
         const T* gm3 = static_cast<const T*>(el.m3);     // [NU][NF]
         for (int i = threadIdx.x; i < NU * NF; i += blockDim.x) {
@@ -666,8 +670,8 @@ static int rhs_launch_vb(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl, cons
     dim3 g;
     if (grid_v(el->nv, el->neles, chunk, &g) != BDGFS_OK) return BDGFS_EINVAL;
     constexpr int RING = 8;
-    const size_t smem = sizeof(T) * (size_t(RING) * 128 * VB + (ND * NU + NF) * NUP + NU * ND * ND + NU
-                                     + NF * ND + NF + (TPP ? ND * NU * 4 + NF : 0))
+    const size_t smem = sizeof(T) * (size_t(RING) * 128 * VB + ((TPP ? 0 : ND * NU) + NF) * NUP + NU * ND * ND
+                                     + NU + NF * ND + NF + (TPP ? ND * NU * 4 + NF : 0))
                         + sizeof(int) * 3 * NF + 16;
     auto k = TPP ? (uf ? rhs_kernel<T, ND, NU, NF, VB, false, RING, TPP>
                        : rhs_kernel<T, ND, NU, NF, VB, true, RING, TPP>)

@@ -239,7 +239,8 @@ def test_stepper_gather_path_equals_disu_path(cuda):
 
 
 @pytest.mark.parametrize('kind,order,prec,tol', [('quad', 3, 'single', 2e-6), ('hex', 2, 'single', 2e-6),
-                                                 ('hex', 2, 'double', 1e-13), ('quad', 2, 'double', 1e-13)])
+                                                 ('hex', 2, 'double', 1e-13), ('quad', 2, 'double', 1e-13),
+                                                 ('hex', 1, 'single', 1e-5), ('hex', 1, 'double', 1e-13)])
 def test_tensor_factored_rhs_matches_dense(cuda, kind, order, prec, tol):
     """The factored residual R = M1 F~ + M3 (F^n - M2 F~) of
     bdgfs_fr_rhs_tensor against bdgfs_fr_rhs_gather (dense M1 - M3 M2):
