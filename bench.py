@@ -1053,7 +1053,7 @@ def surrogate_legs(flush, log=None, pool=None, ncores=0):
     vm = DGFSVelocityMesh(be, cfg)
     sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
     t0 = time.time()
-    q = QSurrogate(sm.grid, nmodes=256, width=1024)
+    q = QSurrogate(sm.grid, nmodes=512, width=1024)
     q.fit(nsamples=200000, ntest=50000, epochs=20, lr=3e-4, batch=1024, seed=0)
     t_fit = time.time() - t0
     # surrogate vs spectral throughput on near-equilibrium cells
@@ -1086,7 +1086,7 @@ def surrogate_legs(flush, log=None, pool=None, ncores=0):
     q.W[3].copy_(saved)
     q._fold()
     c4 = {'workload': ('surrogate of Q on Nv=24^3 (M=Nrho=12): every cell re-centred at zero '
-                       'velocity by a spectral shift (Q shifted back), 256-mode bases '
+                       'velocity by a spectral shift (Q shifted back), 512-mode bases '
                        '(randomised SVD) of the Maxwellian-deviation direction and of Q/rho^2, '
                        'input = modes x, (T-1) x, (T-1)^2 x, products of the 24 leading modes, '
                        'T-1; 4-layer GELU MLP width 1024 with a linear skip and 3 output heads '
@@ -1523,7 +1523,7 @@ def run_surrogate_call(ndof, reps=2):
     be = CUDABackend(cfg)
     vm = DGFSVelocityMesh(be, cfg)
     sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
-    q = QSurrogate(sm.grid, nmodes=256, width=1024)
+    q = QSurrogate(sm.grid, nmodes=512, width=1024)
     dev = be.device
     g = torch.Generator(device=dev).manual_seed(0)
     n = q.n

@@ -165,7 +165,7 @@ class QSurrogate:
     """Basis projection + MLP with output heads (BF16 weights, FP32
     accumulation on the tensor cores) for Q."""
 
-    def __init__(self, grid, nmodes=256, width=1024, device=None, family=COUETTE, center=True,
+    def __init__(self, grid, nmodes=512, width=1024, device=None, family=COUETTE, center=True,
                  split_out=False, nquad=None):
         """center: the network sees every distribution re-centred at zero
         velocity (spectral shift by -u) and its Q is shifted back by +u;

@@ -395,7 +395,7 @@ def test_nan_surrogate_falls_back_to_spectral(small_fit, project):
 
 
 def test_couette_surrogate_fp64_oracle_subcheck(cuda):
-    """The Couette-family surrogate at full size (256 modes, width 1024,
+    """The Couette-family surrogate at full size (512 modes, width 1024,
     200000 training samples, 20 epochs, drift-free rows) on 1000 held-out
     seeded distributions, measured against the FP64 oracle (reference
     algorithm + the same FP64 conservation projection) as well as against
@@ -409,7 +409,7 @@ def test_couette_surrogate_fp64_oracle_subcheck(cuda):
     be = CUDABackend(cfg)
     vm = DGFSVelocityMesh(be, cfg)
     sm = DGFSVHSGLLScatteringModel(be, cfg, vm)
-    q = QSurrogate(sm.grid, nmodes=256, width=1024)
+    q = QSurrogate(sm.grid, nmodes=512, width=1024)
     q.fit(nsamples=200000, ntest=2000, epochs=20, lr=3e-4, batch=1024, seed=0)
     gen = torch.Generator(device=be.device).manual_seed(987654)     # not a training seed
     f = sample_family(vm.c0(), 1000, gen, be.device)
