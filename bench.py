@@ -97,6 +97,15 @@ def q_flops_per_eval(Nv, Nrho, M):
     return (M * Nrho + Nrho + 2) * 5.0 * n * math.log2(n) + 8.0 * M * Nrho * n
 
 
+def q_flops_reference_equivalent(Nv, Nrho, M):
+    """FLOP of the reference's own evaluation of one Q (scattering.py:
+    239-281): 3 M Nrho + 3 complex FFTs at 5 n log2 n, n = Nv^3.  Reported
+    beside the roofline only as context; the roofline uses the packed count."""
+    import math
+    n = Nv**3
+    return (3 * M * Nrho + 3) * 5.0 * n * math.log2(n)
+
+
 class ClockSampler:
     """nvidia-smi clocks/throttle reasons sampled during the timed region."""
 
@@ -1430,6 +1439,11 @@ def run_gpu(args):
                      'peak_source': 'measured FP32 FMA probe on this GPU (MEASURED_PEAKS.json has '
                                     'no FP32 CUDA-core figure)',
                      'flop_per_launch': flop, 'launch_ms': q_ms,
+                     'reference_equivalent': {
+                         'flop_per_launch': ndof * q_flops_reference_equivalent(24, 12, 12),
+                         'tflops': ndof * q_flops_reference_equivalent(24, 12, 12) / (q_ms * 1e-3) / 1e12,
+                         'note': ("the reference's 3 M Nrho + 3 FFTs per Q in the same launch time; "
+                                  'context only (above the peak: the packed algorithm does fewer)')},
                      # algorithmic: f in + Q out = 2 x 113 MB
                      'traffic': Q_LAUNCH_DRAM_BYTES, 'traffic_alg': 2 * 4 * ndof * 24**3,
                      'traffic_source': ('not measured in this run: dram__bytes_read.sum + '
