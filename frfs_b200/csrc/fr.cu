@@ -82,27 +82,71 @@ struct Vec {
     }
 };
 
-// y[i] += col[i] * s[q] for i < NU, col a shared-memory column padded to a
-// multiple of 4 (read as 16-byte broadcasts for float)
-template <typename T, int NU, int NUP, int VB>
-__device__ __forceinline__ void axpy_col(const T* __restrict__ col, const T (&s)[VB], T (&R)[VB][NU])
+// Residual accumulators R(q, i) of a thread's VB velocities at the NU
+// solution points.  FP32 with an even VB (PK): consecutive solution points
+// in float2 pairs, so that the operator columns, read as 16-byte
+// broadcasts, feed sm_100 f32x2 FMAs: half the FMA instructions of scalar
+// code and the same rounding (each lane is one fused multiply-add).
+template <typename T, int NU, int VB, bool PK = false>
+struct Racc {
+    T r[VB][NU];
+    __device__ __forceinline__ T& operator()(int q, int i) { return r[q][i]; }
+};
+template <int NU, int VB>
+struct Racc<float, NU, VB, true> {
+    static constexpr int NPR = NU / 2;               // pairs (i, i+1), i even < 2 NPR
+    float2 p[VB][NPR];
+    float l[VB];                                     // i = NU - 1 when NU is odd
+    __device__ __forceinline__ float& operator()(int q, int i)
+    {
+        return i < 2 * NPR ? ((i & 1) ? p[q][i >> 1].y : p[q][i >> 1].x) : l[q];
+    }
+};
+
+// R(q, i) += col[i] * s[q] for i < NU, col a shared-memory column padded to
+// a multiple of 4 (read as 16-byte broadcasts for float)
+template <typename T, int NU, int NUP, int VB, bool PK>
+__device__ __forceinline__ void axpy_col(const T* __restrict__ col, const T (&s)[VB], Racc<T, NU, VB, PK>& R)
 {
+    if constexpr (PK) {
+        constexpr int NPR = Racc<T, NU, VB, PK>::NPR;
+        float2 s2[VB];
 #pragma unroll
-    for (int i4 = 0; i4 < NUP; i4 += 4) {
-        T w[4];
-        if constexpr (sizeof(T) == 4) {
+        for (int q = 0; q < VB; ++q) s2[q] = make_float2(s[q], s[q]);
+#pragma unroll
+        for (int i4 = 0; i4 < NUP; i4 += 4) {
             const float4 x = *reinterpret_cast<const float4*>(col + i4);
-            w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
-        } else {
-            const double2 x0 = *reinterpret_cast<const double2*>(col + i4);
-            const double2 x1 = *reinterpret_cast<const double2*>(col + i4 + 2);
-            w[0] = x0.x; w[1] = x0.y; w[2] = x1.x; w[3] = x1.y;
+            const float2 w2[2] = {make_float2(x.x, x.y), make_float2(x.z, x.w)};
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int i = i4 + 2 * h;
+                if (i + 1 < 2 * NPR) {
+#pragma unroll
+                    for (int q = 0; q < VB; ++q) R.p[q][i >> 1] = __ffma2_rn(w2[h], s2[q], R.p[q][i >> 1]);
+                } else if (i < NU) {
+#pragma unroll
+                    for (int q = 0; q < VB; ++q) R(q, i) += w2[h].x * s[q];
+                }
+            }
         }
+    } else {
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-            if (i4 + t < NU) {
+        for (int i4 = 0; i4 < NUP; i4 += 4) {
+            T w[4];
+            if constexpr (sizeof(T) == 4) {
+                const float4 x = *reinterpret_cast<const float4*>(col + i4);
+                w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
+            } else {
+                const double2 x0 = *reinterpret_cast<const double2*>(col + i4);
+                const double2 x1 = *reinterpret_cast<const double2*>(col + i4 + 2);
+                w[0] = x0.x; w[1] = x0.y; w[2] = x1.x; w[3] = x1.y;
+            }
 #pragma unroll
-                for (int q = 0; q < VB; ++q) R[q][i4 + t] += w[t] * s[q];
+            for (int t = 0; t < 4; ++t) {
+                if (i4 + t < NU) {
+#pragma unroll
+                    for (int q = 0; q < VB; ++q) R(q, i4 + t) += w[t] * s[q];
+                }
             }
         }
     }
@@ -221,6 +265,7 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
                                                   T c2, int64_t chunk)
 {
     constexpr int NUP = (NU + 3) / 4 * 4;
+    constexpr bool PK = sizeof(T) == 4 && VB % 2 == 0 && TPP > 0;    // f32x2 accumulation
     extern __shared__ __align__(16) unsigned char smraw[];
     // [RING][128][VB] row ring (see below), then the operators
     // (M1 - M3 M2) is read only by the dense residual (TPP == 0)
@@ -336,11 +381,11 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
         T c[VB][3];
 #pragma unroll
         for (int q = 0; q < VB; ++q) vel(c0, el.Nv, v0 + q, c[q]);
-        T R[VB][NU];
+        Racc<T, NU, VB, PK> R;
 #pragma unroll
         for (int q = 0; q < VB; ++q)
 #pragma unroll
-            for (int i = 0; i < NU; ++i) R[q][i] = T(0);
+            for (int i = 0; i < NU; ++i) R(q, i) = T(0);
 #pragma unroll
         for (int k = 0; k < RING - 1; ++k) issue(k, v0);
         if constexpr (TPP > 0) {
@@ -366,7 +411,7 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
                     for (int t = 0; t < TPP; ++t) {
                         const T wt = w[t];
 #pragma unroll
-                        for (int q = 0; q < VB; ++q) R[q][base + t * st] += wt * ft[q];
+                        for (int q = 0; q < VB; ++q) R(q, base + t * st) += wt * ft[q];
                     }
                 }
             }
@@ -386,7 +431,7 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
                     for (int k = 0; k < ND; ++k) al += sm[(j * ND + d) * ND + k] * c[q][k];
                     ft[q] = al * uj.v[q];
                 }
-                axpy_col<T, NU, NUP, VB>(dT + (d * NU + j) * NUP, ft, R);
+                axpy_col<T, NU, NUP, VB, PK>(dT + (d * NU + j) * NUP, ft, R);
             }
         }
         }
@@ -447,7 +492,7 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
                     fh[q] -= sg * al * ul.v[q];
                 }
             }
-            axpy_col<T, NU, NUP, VB>(m3T + f * NUP, fh, R);
+            axpy_col<T, NU, NUP, VB, PK>(m3T + f * NUP, fh, R);
         }
         // combination rows u, x1, x2: out = a u + b L(u) + c1 x1 + c2 x2
 #pragma unroll
@@ -461,7 +506,7 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
             const Vec<T, VB> y2 = take(k + 2);
             Vec<T, VB> o;
 #pragma unroll
-            for (int q = 0; q < VB; ++q) o.v[q] = a * ui.v[q] + b * (-rj[i] * R[q][i]);
+            for (int q = 0; q < VB; ++q) o.v[q] = a * ui.v[q] + b * (-rj[i] * R(q, i));
             if (x1) {
 #pragma unroll
                 for (int q = 0; q < VB; ++q) o.v[q] += c1 * y1.v[q];
