@@ -256,8 +256,9 @@ __device__ __forceinline__ int64_t mirror_chunk(int64_t v0, int Nv, int kind, in
     return v0 - iz + (N - iz - VB);
 }
 
+
 template <typename T, int ND, int NU, int NF, int VB, bool GATHER = false, int RING = 8, int TPP = 0>
-__global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, const bdgfs_fr_walls wl,
+__global__ void __launch_bounds__(128, (NU <= 16 && sizeof(T) == 4) ? 4 : 3) rhs_kernel(const bdgfs_fr_eles el, const bdgfs_fr_walls wl,
                                                   const T* __restrict__ u, const T* __restrict__ uf,
                                                   const int32_t* __restrict__ fsel,
                                                   const bdgfs_fr_tensor tp,
@@ -365,8 +366,41 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
         const T* base = w == 0 ? u : (w == 1 ? (x1 ? x1 : u) : (x2 ? x2 : u));
         return base + (e * NU + i) * nv + v0;
     };
+    // Sources of the rows past the volume rows (k >= NU), the same for every
+    // thread of the CTA, looked up once: the row at velocity 0 and, for a
+    // specular wall, its mirror kind (the row is then read at the mirrored
+    // velocity chunk).  The volume rows are addressed directly.
+    // rowm: 0, or 1 + the mirrored axis; moff[m][thread]: the thread's
+    // velocity offset for that kind (0 for m = 0; the others set per
+    // velocity step when a specular wall is present)
+    __shared__ const T* rowp[NR - NU];
+    __shared__ unsigned char rowm[NR - NU];
+    __shared__ int64_t moff[4][128];
+    for (int k = NU + int(threadIdx.x); k < NR; k += int(blockDim.x)) {
+        const int kk = k - NU;
+        unsigned char m = 0;
+        if (kk < 2 * NF && (kk & 1) && nb[kk >> 1] < 0) {
+            const int bid = wl.bcid[-1 - nb[kk >> 1]];
+            const int kd = wl.kind ? wl.kind[bid] : BDGFS_BC_DIFFUSE;
+            if (kd >= BDGFS_BC_SPECULAR_X) m = static_cast<unsigned char>(1 + kd - BDGFS_BC_SPECULAR_X);
+        }
+        rowp[kk] = m ? lsrc(kk >> 1, 0) : rowptr(k, 0);
+        rowm[kk] = m;
+    }
+    moff[0][threadIdx.x] = 0;
+    const bool mirrors = wl.kind && (wl.kinds_used & ((1 << BDGFS_BC_SPECULAR_X) | (1 << BDGFS_BC_SPECULAR_Y) |
+                                                      (1 << BDGFS_BC_SPECULAR_Z)));
+    __syncthreads();
     auto issue = [&](int k, int64_t v0) {
-        if (k < NR) cp_async<VB * sizeof(T)>(ring + size_t(k % RING) * 128 * VB, rowptr(k, v0));
+        if (k < NR) {
+            const T* src;
+            if (k < NU) {
+                src = u + (e * NU + k) * nv + v0;
+            } else {
+                src = rowp[k - NU] + v0 + moff[rowm[k - NU]][threadIdx.x];
+            }
+            cp_async<VB * sizeof(T)>(ring + size_t(k % RING) * 128 * VB, src);
+        }
         cp_async_commit();
     };
     auto take = [&](int k) {
@@ -381,6 +415,11 @@ __global__ void __launch_bounds__(128, 3) rhs_kernel(const bdgfs_fr_eles el, con
         T c[VB][3];
 #pragma unroll
         for (int q = 0; q < VB; ++q) vel(c0, el.Nv, v0 + q, c[q]);
+        if (mirrors) {                                   // the thread's own slots only
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                moff[1 + a][threadIdx.x] = mirror_chunk(v0, el.Nv, BDGFS_BC_SPECULAR_X + a, VB) - v0;
+        }
         Racc<T, NU, VB, PK> R;
 #pragma unroll
         for (int q = 0; q < VB; ++q)
