@@ -82,6 +82,30 @@ struct Vec {
     }
 };
 
+// r[0..N) = p[0..N) from shared memory in one vector load (p aligned to
+// N * sizeof(T); N = 2 or 4)
+template <typename T, int N>
+__device__ __forceinline__ void lds_vec(const T* __restrict__ p, T (&r)[N])
+{
+    if constexpr (sizeof(T) == 4 && N == 4) {
+        const float4 x = *reinterpret_cast<const float4*>(p);
+        r[0] = x.x; r[1] = x.y; r[2] = x.z; r[3] = x.w;
+    } else if constexpr (sizeof(T) == 4 && N == 2) {
+        const float2 x = *reinterpret_cast<const float2*>(p);
+        r[0] = x.x; r[1] = x.y;
+    } else if constexpr (sizeof(T) == 8 && N == 4) {
+        const double2 x0 = *reinterpret_cast<const double2*>(p);
+        const double2 x1 = *reinterpret_cast<const double2*>(p + 2);
+        r[0] = x0.x; r[1] = x0.y; r[2] = x1.x; r[3] = x1.y;
+    } else if constexpr (sizeof(T) == 8 && N == 2) {
+        const double2 x = *reinterpret_cast<const double2*>(p);
+        r[0] = x.x; r[1] = x.y;
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) r[i] = p[i];
+    }
+}
+
 // Residual accumulators R(q, i) of a thread's VB velocities at the NU
 // solution points.  FP32 with an even VB (PK): consecutive solution points
 // in float2 pairs, so that the operator columns, read as 16-byte
@@ -272,14 +296,16 @@ __global__ void __launch_bounds__(128, (NU <= 16 && sizeof(T) == 4) ? 4 : 3) rhs
     // (M1 - M3 M2) is read only by the dense residual (TPP == 0)
     constexpr int NDT = TPP ? 0 : ND * NU * NUP;
     T* dT = reinterpret_cast<T*>(smraw) + RING * 128 * VB;   // [ND*NU][NUP]  (M1 - M3 M2) transposed
+    // rows of the metric terms, the normals and M1's line values are padded
+    // to 4 (2 for smats in 2-D) entries, read with one vector load each
+    constexpr int SR = ND == 3 ? 4 : ND;
     T* m3T = dT + NDT;                                  // [NF][NUP]
-    T* sm = m3T + NF * NUP;                             // [NU][ND][ND]
-    T* rj = sm + NU * ND * ND;                          // [NU]
-    T* pn = rj + NU;                                    // [NF][ND]
-    T* mg = pn + NF * ND;                               // [NF]
-    T* m1l = mg + NF;                                   // [ND][NU][4] (TPP)
+    T* sm = m3T + NF * NUP;                             // [NU][ND][SR]  smats
+    T* pn = sm + NU * ND * SR;                          // [NF][4]: unit normal (ND), |n| at 3
+    T* m1l = pn + NF * 4;                               // [ND][NU][4] (TPP)
     T* fsg = m1l + (TPP ? ND * NU * 4 : 0);             // [NF] (TPP)
-    int* nb = reinterpret_cast<int*>(fsg + (TPP ? NF : 0));   // [NF]
+    T* rj = fsg + (TPP ? NF : 0);                       // [NU]
+    int* nb = reinterpret_cast<int*>(rj + NU);          // [NF]
     int* fs = nb + NF;                                  // [NF] (GATHER)
     int* fdm = fs + NF;                                 // [NF] (TPP)
     const int64_t e = blockIdx.y;
@@ -299,14 +325,19 @@ __global__ void __launch_bounds__(128, (NU <= 16 && sizeof(T) == 4) ? 4 : 3) rhs
             m3T[f * NUP + row] = gm3[i];
         }
         const T* gs = static_cast<const T*>(el.smats) + e * NU * ND * ND;
-        for (int i = threadIdx.x; i < NU * ND * ND; i += blockDim.x) sm[i] = gs[i];
+        for (int i = threadIdx.x; i < NU * ND * SR; i += blockDim.x) {
+            const int row = i / SR, k = i - row * SR;
+            sm[i] = k < ND ? gs[row * ND + k] : T(0);
+        }
         const T* gr = static_cast<const T*>(el.rcpdjac) + e * NU;
         for (int i = threadIdx.x; i < NU; i += blockDim.x) rj[i] = gr[i];
         const T* gp = static_cast<const T*>(el.pnorm) + e * NF * ND;
-        for (int i = threadIdx.x; i < NF * ND; i += blockDim.x) pn[i] = gp[i];
         const T* gg = static_cast<const T*>(el.magn) + e * NF;
+        for (int i = threadIdx.x; i < NF * 4; i += blockDim.x) {
+            const int f = i >> 2, k = i & 3;
+            pn[i] = k < ND ? gp[f * ND + k] : (k == 3 ? gg[f] : T(0));
+        }
         for (int i = threadIdx.x; i < NF; i += blockDim.x) {
-            mg[i] = gg[i];
             nb[i] = el.nbr[e * NF + i];
             // table entries clamped into range (a malformed table gives wrong
             // values, never an out-of-range access)
@@ -435,17 +466,20 @@ __global__ void __launch_bounds__(128, (NU <= 16 && sizeof(T) == 4) ? 4 : 3) rhs
                 const Vec<T, VB> uj = take(j);
 #pragma unroll
                 for (int d = 0; d < ND; ++d) {
+                    // scalar reads here: this loop is unrolled over every (j, d)
+                    // and vector reads of the padded rows measured slower
+                    const T* srow = sm + (j * ND + d) * SR;
+                    const T* w = m1l + (d * NU + j) * 4;
                     T ft[VB];
 #pragma unroll
                     for (int q = 0; q < VB; ++q) {
                         T al = T(0);
 #pragma unroll
-                        for (int k = 0; k < ND; ++k) al += sm[(j * ND + d) * ND + k] * c[q][k];
+                        for (int k = 0; k < ND; ++k) al += srow[k] * c[q][k];
                         ft[q] = al * uj.v[q];
                     }
                     const int st = d == 0 ? 1 : (d == 1 ? TPP : TPP * TPP);
                     const int base = j - ((j / st) % TPP) * st;
-                    const T* w = m1l + (d * NU + j) * 4;
 #pragma unroll
                     for (int t = 0; t < TPP; ++t) {
                         const T wt = w[t];
@@ -462,12 +496,14 @@ __global__ void __launch_bounds__(128, (NU <= 16 && sizeof(T) == 4) ? 4 : 3) rhs
             const Vec<T, VB> uj = take(j);
 #pragma unroll
             for (int d = 0; d < ND; ++d) {
+                T srow[SR];
+                lds_vec<T, SR>(sm + (j * ND + d) * SR, srow);
                 T ft[VB];
 #pragma unroll
                 for (int q = 0; q < VB; ++q) {
                     T al = T(0);
 #pragma unroll
-                    for (int k = 0; k < ND; ++k) al += sm[(j * ND + d) * ND + k] * c[q][k];
+                    for (int k = 0; k < ND; ++k) al += srow[k] * c[q][k];
                     ft[q] = al * uj.v[q];
                 }
                 axpy_col<T, NU, NUP, VB, PK>(dT + (d * NU + j) * NUP, ft, R);
@@ -483,12 +519,14 @@ __global__ void __launch_bounds__(128, (NU <= 16 && sizeof(T) == 4) ? 4 : 3) rhs
             issue(k + RING, v0);
             Vec<T, VB> ur = take(k + 1);
             const int n = nb[f];
+            T prow[4];                                       // unit normal, |n| at 3
+            lds_vec<T, 4>(pn + f * 4, prow);
             T nc[VB];
 #pragma unroll
             for (int q = 0; q < VB; ++q) {
                 nc[q] = T(0);
 #pragma unroll
-                for (int d = 0; d < ND; ++d) nc[q] += pn[f * ND + d] * c[q][d];
+                for (int d = 0; d < ND; ++d) nc[q] += prow[d] * c[q][d];
             }
             if (n < 0) {                                     // boundary: ur holds f_w or the mirrored row
                 const int w = -1 - n;
@@ -509,7 +547,7 @@ __global__ void __launch_bounds__(128, (NU <= 16 && sizeof(T) == 4) ? 4 : 3) rhs
                     for (int q = 0; q < VB; ++q) {
                         T fac = T(0);
 #pragma unroll
-                        for (int d = 0; d < ND; ++d) fac += (c[q][d] - uw[bid * 3 + d]) * pn[f * ND + d];
+                        for (int d = 0; d < ND; ++d) fac += (c[q][d] - uw[bid * 3 + d]) * prow[d];
                         ur.v[q] = (fac < T(0)) ? ur.v[q] * sc : ul.v[q];
                     }
                 }
@@ -518,16 +556,18 @@ __global__ void __launch_bounds__(128, (NU <= 16 && sizeof(T) == 4) ? 4 : 3) rhs
 #pragma unroll
             for (int q = 0; q < VB; ++q) {
                 const T fn = T(0.5) * nc[q] * (ul.v[q] + ur.v[q]) + T(0.5) * fabs(nc[q]) * (ul.v[q] - ur.v[q]);
-                fh[q] = mg[f] * fn;
+                fh[q] = prow[3] * fn;
             }
             if constexpr (TPP > 0) {                         // F^n - M2 F~ (ul is u at fsel[f])
                 const int jf = fs[f], df = fdm[f];
                 const T sg = fsg[f];
+                T srow[SR];
+                lds_vec<T, SR>(sm + (jf * ND + df) * SR, srow);
 #pragma unroll
                 for (int q = 0; q < VB; ++q) {
                     T al = T(0);
 #pragma unroll
-                    for (int k = 0; k < ND; ++k) al += sm[(jf * ND + df) * ND + k] * c[q][k];
+                    for (int k = 0; k < ND; ++k) al += srow[k] * c[q][k];
                     fh[q] -= sg * al * ul.v[q];
                 }
             }
@@ -754,8 +794,9 @@ static int rhs_launch_vb(const bdgfs_fr_eles* el, const bdgfs_fr_walls* wl, cons
     dim3 g;
     if (grid_v(el->nv, el->neles, chunk, &g) != BDGFS_OK) return BDGFS_EINVAL;
     constexpr int RING = 8;
-    const size_t smem = sizeof(T) * (size_t(RING) * 128 * VB + ((TPP ? 0 : ND * NU) + NF) * NUP + NU * ND * ND
-                                     + NU + NF * ND + NF + (TPP ? ND * NU * 4 + NF : 0))
+    constexpr int SR = ND == 3 ? 4 : ND;
+    const size_t smem = sizeof(T) * (size_t(RING) * 128 * VB + ((TPP ? 0 : ND * NU) + NF) * NUP + NU * ND * SR
+                                     + NF * 4 + (TPP ? ND * NU * 4 + NF : 0) + NU)
                         + sizeof(int) * 3 * NF + 16;
     auto k = TPP ? (uf ? rhs_kernel<T, ND, NU, NF, VB, false, RING, TPP>
                        : rhs_kernel<T, ND, NU, NF, VB, true, RING, TPP>)
