@@ -30,20 +30,21 @@ __device__ __forceinline__ uint32_t mix32(uint64_t x)
     return uint32_t(x >> 32);
 }
 
-template <typename T, int VEC>
+// NVC > 0: the grid size at compile time (h.Nv == NVC)
+template <typename T, int VEC, int NVC = 0>
 __global__ void __launch_bounds__(256) indicator_kernel(const bdgfs_hybrid_args h, const T* __restrict__ f)
 {
     __shared__ double red[8 * 8];
     __shared__ double cs[kMaxNv], ex[3][kMaxNv];
     __shared__ int64_t s_pos;
     const int64_t dof = blockIdx.x;
-    const int Nv = h.Nv;
+    const int Nv = NVC > 0 ? NVC : h.Nv;
     const int n = Nv * Nv * Nv;
     const T* fd = f + dof * int64_t(n);
     for (int i = threadIdx.x; i < Nv; i += blockDim.x) cs[i] = h.c0[i];
     __syncthreads();
     double m[5] = {0, 0, 0, 0, 0};
-    row_moments<T, VEC>(fd, n, Nv, cs, m);
+    row_moments<T, VEC, NVC>(fd, n, Nv, cs, m);
     block_sum<5>(m, red);
     const double rho = m[0] * h.cw;
     const double ux = m[1] / m[0], uy = m[2] / m[0], uz = m[3] / m[0];
@@ -67,7 +68,7 @@ __global__ void __launch_bounds__(256) indicator_kernel(const bdgfs_hybrid_args 
             Chunk<T, VEC> c;
             c.load(fd + v);
             uint32_t ix, iy, iz;
-            vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
+            vsplit<NVC>(uint32_t(v), uint32_t(Nv), ix, iy, iz);
             const double axy = a * ex[0][ix] * ex[1][iy];
 #pragma unroll
             for (int j = 0; j < VEC; ++j) {
@@ -127,7 +128,7 @@ __global__ void __launch_bounds__(256) indicator_kernel(const bdgfs_hybrid_args 
             Chunk<T, VEC> c;
             c.load(fd + v);
             uint32_t ix, iy, iz;
-            vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
+            vsplit<NVC>(uint32_t(v), uint32_t(Nv), ix, iy, iz);
             const double axy = a * ex[0][ix] * ex[1][iy];
             float d[VEC];
 #pragma unroll
@@ -786,7 +787,9 @@ extern "C" int32_t bdgfs_hybrid_classify(const bdgfs_hybrid_args* h, const void*
         else
             indicator_kernel<double, 1><<<unsigned(h->ndof), 256, 0, st>>>(*h, static_cast<const double*>(f));
     } else {
-        if (v4)
+        if (v4 && h->Nv == 24)
+            indicator_kernel<float, 4, 24><<<unsigned(h->ndof), 256, 0, st>>>(*h, static_cast<const float*>(f));
+        else if (v4)
             indicator_kernel<float, 4><<<unsigned(h->ndof), 256, 0, st>>>(*h, static_cast<const float*>(f));
         else
             indicator_kernel<float, 1><<<unsigned(h->ndof), 256, 0, st>>>(*h, static_cast<const float*>(f));

@@ -7,13 +7,16 @@ namespace bdgfs {
 
 constexpr int kMaxNv = 64;
 
-// velocity index v = (ix*Nv + iy)*Nv + iz, 32-bit arithmetic
+// velocity index v = (ix*Nv + iy)*Nv + iz, 32-bit arithmetic; NVC > 0: Nv
+// known at compile time (the divisions become multiplications)
+template <int NVC = 0>
 __device__ __forceinline__ void vsplit(uint32_t v, uint32_t Nv, uint32_t& ix, uint32_t& iy, uint32_t& iz)
 {
-    const uint32_t q = v / Nv;
-    iz = v - q * Nv;
-    ix = q / Nv;
-    iy = q - ix * Nv;
+    const uint32_t N = NVC > 0 ? uint32_t(NVC) : Nv;
+    const uint32_t q = v / N;
+    iz = v - q * N;
+    ix = q / N;
+    iy = q - ix * N;
 }
 
 // Four consecutive values (same x, y; z..z+3) of a row: one 16-byte load
@@ -48,7 +51,7 @@ struct Chunk {
 };
 
 // FP64 raw moments {sum x, sum c x, sum |c|^2 x} of one row (block-wide)
-template <typename T, int VEC>
+template <typename T, int VEC, int NVC = 0>
 __device__ __forceinline__ void row_moments(const T* __restrict__ row, int n, int Nv, const double* cs,
                                             double (&m)[5])
 {
@@ -57,7 +60,7 @@ __device__ __forceinline__ void row_moments(const T* __restrict__ row, int n, in
         Chunk<T, VEC> c;
         c.load(row + v);
         uint32_t ix, iy, iz;
-        vsplit(uint32_t(v), uint32_t(Nv), ix, iy, iz);
+        vsplit<NVC>(uint32_t(v), uint32_t(Nv), ix, iy, iz);
         const double cx = cs[ix], cy = cs[iy], b = cx * cx + cy * cy;
 #pragma unroll
         for (int j = 0; j < VEC; ++j) {
