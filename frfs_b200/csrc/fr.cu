@@ -608,6 +608,7 @@ __global__ void __launch_bounds__(256) bc_update_kernel(const bdgfs_fr_eles el,
                                                         const int32_t* __restrict__ fsel)
 {
     __shared__ double red[2 * 8];
+    __shared__ T cs[1024];                                    // cell-centre velocities (Nv <= 1024)
     const int w = blockIdx.x;
     const int e = wl.fpt[2 * w], f = wl.fpt[2 * w + 1];
     const int bid = wl.bcid[w];
@@ -626,19 +627,32 @@ __global__ void __launch_bounds__(256) bc_update_kernel(const bdgfs_fr_eles el,
     const T* ul = fsel ? uf + (int64_t(e) * el.nupts + fsel[f]) * el.nv
                        : uf + (int64_t(e) * el.nfpts + f) * el.nv;
     const T* c0 = static_cast<const T*>(el.c0);
+    for (int i = threadIdx.x; i < el.Nv; i += blockDim.x) cs[i] = c0[i];
+    __syncthreads();
     double s0 = 0.0, s1 = 0.0;
-    // four velocities per step (16-byte loads) when rows are aligned
+    // four velocities per step (16-byte loads) when rows are aligned; with
+    // Nv % 4 == 0 the four share one z line (one index split per step)
     const bool v4 = sizeof(T) == 4 && el.nv % 4 == 0 && (reinterpret_cast<uintptr_t>(ul) & 15u) == 0 &&
                     (reinterpret_cast<uintptr_t>(fw) & 15u) == 0;
+    const bool zline = el.Nv % 4 == 0;
     const int64_t nv4 = v4 ? el.nv : 0;
     for (int64_t v0 = int64_t(threadIdx.x) * 4; v0 < nv4; v0 += int64_t(blockDim.x) * 4) {
         Vec<T, 4> a, b;
         a.load(ul + v0);
         b.load(fw + v0);
+        const uint32_t vv = uint32_t(v0), nn = uint32_t(el.Nv);    // v < Nv^3 <= 2^30
+        const uint32_t qq = vv / nn, iz0 = vv - qq * nn;
+        const uint32_t ix = qq / nn, iy = qq - ix * nn;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             T c[3];
-            vel(c0, el.Nv, v0 + q, c);
+            if (zline) {
+                c[0] = cs[ix];
+                c[1] = cs[iy];
+                c[2] = cs[iz0 + q];
+            } else {
+                vel(cs, el.Nv, v0 + q, c);
+            }
             T fac = T(0);
             for (int d = 0; d < ND; ++d) fac += (c[d] - uw[d]) * pn[d];
             if (fac >= T(0)) s0 += double(fac * a.v[q]);
@@ -647,7 +661,7 @@ __global__ void __launch_bounds__(256) bc_update_kernel(const bdgfs_fr_eles el,
     }
     for (int64_t v = nv4 + threadIdx.x; v < el.nv; v += blockDim.x) {
         T c[3];
-        vel(c0, el.Nv, v, c);
+        vel(cs, el.Nv, v, c);
         T fac = T(0);
         for (int d = 0; d < ND; ++d) fac += (c[d] - uw[d]) * pn[d];
         if (fac >= T(0)) s0 += double(fac * ul[v]);
