@@ -397,13 +397,13 @@ __global__ void __launch_bounds__(128, (NU <= 16 && sizeof(T) == 4) ? 4 : 3) rhs
         const T* base = w == 0 ? u : (w == 1 ? (x1 ? x1 : u) : (x2 ? x2 : u));
         return base + (e * NU + i) * nv + v0;
     };
-    // Sources of the rows past the volume rows (k >= NU), the same for every
-    // thread of the CTA, looked up once: the row at velocity 0 and, for a
-    // specular wall, its mirror kind (the row is then read at the mirrored
-    // velocity chunk).  The volume rows are addressed directly.
-    // rowm: 0, or 1 + the mirrored axis; moff[m][thread]: the thread's
-    // velocity offset for that kind (0 for m = 0; the others set per
-    // velocity step when a specular wall is present)
+    // Sources of the rows past the volume rows (k >= NU) are the same for
+    // every thread of the CTA and are looked up once: rowp, the row at
+    // velocity 0, and rowm, 0 or 1 + the mirrored axis of a specular wall
+    // (that row is read at the mirrored velocity chunk).  moff[m][thread]
+    // holds the thread's velocity offset for kind m (128 threads per CTA):
+    // 0 for m = 0, the others set per velocity step when a specular wall is
+    // present.  The volume rows are addressed directly.
     __shared__ const T* rowp[NR - NU];
     __shared__ unsigned char rowm[NR - NU];
     __shared__ int64_t moff[4][128];
