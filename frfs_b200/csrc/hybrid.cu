@@ -32,7 +32,8 @@ __device__ __forceinline__ uint32_t mix32(uint64_t x)
 
 // NVC > 0: the grid size at compile time (h.Nv == NVC)
 template <typename T, int VEC, int NVC = 0>
-__global__ void __launch_bounds__(256) indicator_kernel(const bdgfs_hybrid_args h, const T* __restrict__ f)
+__global__ void __launch_bounds__(256, NVC > 0 ? 5 : 0) indicator_kernel(const bdgfs_hybrid_args h,
+                                                                         const T* __restrict__ f)
 {
     __shared__ double red[8 * 8];
     __shared__ double cs[kMaxNv], ex[3][kMaxNv];
