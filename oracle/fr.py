@@ -22,6 +22,8 @@ Restates, interface by interface as the reference does:
               is the diffuse wall with a per-point f_w (its own U, T)
   tdivtconf   R += M3 Fhat                       (elements.py:85-88)
   negdivconf  R = -rcpdjac R                     (kernels/negdivconf.mako:5-13)
+  invmass     M12 u, M12 the inverse mass matrix (elements.py:161-164,
+                                                  shapes.py:163-166)
 and the steppers dgfs-euler / dgfs-tvd-rk2 (frfs/integrators/std/steppers.py:20-225).
 Arrays are element-major: u[e][upt][v].  Test infrastructure only.
 """
@@ -175,6 +177,35 @@ class FROracle:
                 done[e, f] = True
         R = R + np.einsum('uf,efv->euv', self.M3, Fh)
         return -g.rcpdjac[:, :, None] * R
+
+
+def inverse_mass(ndims, order):
+    """M12 of frfs/shapes.py:163-166 (V^T V, V the orthonormal basis at the
+    solution points) restated as the inverse of the nodal mass matrix
+    M_ij = int l_i l_j over [-1, 1]^ndims (l the Lagrange basis at the GLL
+    solution points, x index fastest), integrated exactly by a Gauss-Legendre
+    product rule: for an orthonormal basis V^T V = M^-1."""
+    from numpy.polynomial import legendre as L
+    n = order + 1
+    c = np.zeros(n)
+    c[-1] = 1.0
+    x = np.concatenate([[-1.0], np.sort(L.legroots(L.legder(c))), [1.0]])
+    xq, wq = L.leggauss(n + 1)                     # exact for degree 2n + 1
+    lag = np.ones((len(xq), n))
+    for i in range(n):
+        for j in range(n):
+            if j != i:
+                lag[:, i] *= (xq - x[j]) / (x[i] - x[j])
+    m1 = lag.T @ (wq[:, None] * lag)
+    M = m1
+    for _ in range(ndims - 1):
+        M = np.kron(m1, M)                         # slower index on the left
+    return np.linalg.inv(M)
+
+
+def invmass(minv, u):
+    """system.invmass (solvers/dgfs/system.py:221-231): minv u per element."""
+    return np.einsum('ij,ejv->eiv', minv, u)
 
 
 def step_rk2(u, dt, L, Q):

@@ -199,3 +199,16 @@ def test_oracle_mixture_q_equals_reference_kernels():
     # each species' own Q too (the lighter species' Q is not swamped)
     for p in range(2):
         assert rel_l2(Qo[:, p], d['Q'][:, p]) < 1e-12
+
+
+@pytest.mark.parametrize('kind,ndims,order', [('quad', 2, 2), ('quad', 2, 3), ('hex', 3, 2)])
+def test_oracle_inverse_mass_equals_reference(kind, ndims, order):
+    """The oracle's inverse mass matrix (the exact nodal mass matrix,
+    inverted) equals the reference's own M12 = V^T V (golden fixture written
+    from frfs/shapes.py:163-166)."""
+    from oracle.fr import inverse_mass, invmass
+    ref = np.load(os.path.join(GOLD, f'shapes_{kind}_p{order}.npz'))['M12']
+    mine = inverse_mass(ndims, order)
+    assert np.abs(mine - ref).max() < 1e-12 * np.abs(ref).max()
+    u = np.random.default_rng(order).standard_normal((3, ref.shape[0], 7))
+    assert np.allclose(invmass(mine, u), np.einsum('ij,ejv->eiv', ref, u), rtol=0, atol=1e-12)
